@@ -1,0 +1,310 @@
+"""Python binding of libcmg.so (the C ABI in include/cmg.h).
+
+Mirrors the reference's solver interface (src/AMGSolver.h, src/HAGrid.h) so
+that a caller written against Cirrus-amg reads the same:
+
+    grid = HADeviceGrid(1/8, 10)                 # HADeviceGrid(h0, log2hash per level)
+    grid.set_tile_host(0, (0, 0, 0), LEAF)       # setTileHost
+    grid.rebuild()
+    grid.iterative_refine(level_target)          # or grid.refine_case(...)
+    solver = AMGSolver(coeff_channel, 0.5, 1, 1)
+    solver.prepareTypesAndCoeffs(grid)
+    iters, rel = solver.solve(grid, False, 100, 1e-6, 2, 10, 1, False)
+
+The library is required: there is no CPU path.  Importing this module on a
+machine without libcmg.so raises; calling a device function without a CUDA
+device returns the CUDA error as an exception.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcmg.so")
+
+LEAF, NONLEAF, GHOST = 1, 2, 4
+DIRICHLET, INTERIOR, NEUMANN = 1, 2, 4
+CASE_UNIFORM, CASE_CENTER_POINT, CASE_SPHERE_EMPTY, CASE_SPHERE_SOLID = 0, 1, 2, 3
+CASE_STAR_EMPTY, CASE_STAR_SOLID, CASE_SHELL, CASE_MULTI_SPHERE = 4, 5, 6, 7
+
+# names of every entry point include/cmg.h declares
+EXPORTS = [
+    "cmg_last_error", "cmg_version",
+    "cmg_grid_create", "cmg_grid_destroy", "cmg_grid_set_tile", "cmg_grid_rebuild", "cmg_grid_iterative_refine",
+    "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
+    "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
+    "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
+    "cmg_grid_synchronize",
+    "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
+    "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_full_neg_lap", "cmg_amg_dot",
+    "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solve",
+    "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
+]
+
+TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE, "-j4"], check=True)
+
+
+def lib():
+    """The loaded library.  Raises if libcmg.so has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, F, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_size_t
+        PP = ctypes.POINTER(ctypes.c_void_p)
+        sig = {
+            "cmg_last_error": (ctypes.c_char_p, []),
+            "cmg_version": (I, []),
+            "cmg_grid_create": (I, [F, I, I, PP]),
+            "cmg_grid_destroy": (I, [P]),
+            "cmg_grid_set_tile": (I, [P, I, I, I, I, I]),
+            "cmg_grid_rebuild": (I, [P]),
+            "cmg_grid_iterative_refine": (I, [P, TARGET_FN, P, P]),
+            "cmg_grid_refine_case": (I, [P, I, P, I, P]),
+            "cmg_grid_info": (I, [P, P, P, P]),
+            "cmg_grid_tiles": (I, [P, P, P, P]),
+            "cmg_grid_tables": (I, [P, P, P]),
+            "cmg_grid_channel_ptr": (I, [P, I, PP]),
+            "cmg_grid_cell_type_ptr": (I, [P, PP]),
+            "cmg_grid_upload_channel": (I, [P, I, P, S]),
+            "cmg_grid_download_channel": (I, [P, I, P, S]),
+            "cmg_grid_upload_cell_types": (I, [P, P, S]),
+            "cmg_grid_download_cell_types": (I, [P, P, S]),
+            "cmg_grid_fill_channel": (I, [P, I, F]),
+            "cmg_grid_set_leaf_cell_types_case": (I, [P, I, P, I]),
+            "cmg_grid_set_stream": (I, [P, P]),
+            "cmg_grid_synchronize": (I, [P]),
+            "cmg_amg_prepare_types_and_coeffs": (I, [P, I, F]),
+            "cmg_amg_prepare_system": (I, [P, I, F]),
+            "cmg_amg_cutcell_sphere_coeffs": (I, [P, I, F, I, P]),
+            "cmg_amg_face_velocity_fourier": (I, [P, I, I, P, P, P]),
+            "cmg_amg_divergence": (I, [P, I, I, I]),
+            "cmg_amg_full_neg_lap": (I, [P, I, I, I]),
+            "cmg_amg_dot": (I, [P, I, I, P]),
+            "cmg_amg_solver_create": (I, [I, F, F, F, PP]),
+            "cmg_amg_solver_destroy": (I, [P]),
+            "cmg_amg_solver_set_smoother": (I, [P, D, I]),
+            "cmg_amg_solve": (I, [P, P, I, I, D, I, I, I, I, P, P]),
+            "cmg_amg_solve_host": (I, [P, P, P, P, S, I, D, I, I, I, I, P, P]),
+            "cmg_amg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
+            "cmg_amg_fas_mu_cycle": (I, [P, P, I, I, I, I, I]),
+            "cmg_amg_last_solve_ms": (I, [P, P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class CmgError(RuntimeError):
+    pass
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib().cmg_last_error()
+        raise CmgError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class HADeviceGrid:
+    """Octree of 8^3 tiles on the device (src/HAGrid.h:357)."""
+
+    def __init__(self, h0=0.125, num_levels=10, num_channels=16):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        _check(self.L.cmg_grid_create(h0, num_levels, num_channels, ctypes.byref(h)), "cmg_grid_create")
+        self.h = h
+        self.h0 = h0
+        self.num_channels = num_channels
+        self._cb = None
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.cmg_grid_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def set_tile_host(self, level, coord, ttype):
+        _check(self.L.cmg_grid_set_tile(self.h, level, int(coord[0]), int(coord[1]), int(coord[2]), ttype), "set_tile")
+
+    def rebuild(self):
+        _check(self.L.cmg_grid_rebuild(self.h), "rebuild")
+
+    def iterative_refine(self, level_target):
+        """level_target(level, i, j, k) -> target level of that tile."""
+        cb = TARGET_FN(lambda user, l, i, j, k: int(level_target(l, i, j, k)))
+        self._cb = cb
+        steps = ctypes.c_int(0)
+        _check(self.L.cmg_grid_iterative_refine(self.h, cb, None, ctypes.byref(steps)), "iterative_refine")
+        return steps.value
+
+    def refine_case(self, case_id, params):
+        prm = np.asarray(params, dtype=np.float64)
+        steps = ctypes.c_int(0)
+        _check(self.L.cmg_grid_refine_case(self.h, case_id, _p(prm), len(prm), ctypes.byref(steps)), "refine_case")
+        return steps.value
+
+    def info(self):
+        n, ml, nl = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(self.L.cmg_grid_info(self.h, ctypes.byref(n), ctypes.byref(ml), ctypes.byref(nl)), "info")
+        return n.value, ml.value, nl.value
+
+    @property
+    def num_tiles(self):
+        return self.info()[0]
+
+    @property
+    def max_level(self):
+        return self.info()[1]
+
+    def tiles(self):
+        n = self.num_tiles
+        lv = np.zeros(n, np.int32)
+        ijk = np.zeros((n, 3), np.int32)
+        ty = np.zeros(n, np.uint8)
+        _check(self.L.cmg_grid_tiles(self.h, _p(lv), _p(ijk), _p(ty)), "tiles")
+        return lv, ijk, ty
+
+    def tables(self):
+        n = self.num_tiles
+        nb = np.zeros((n, 8), np.int32)
+        ch = np.zeros((n, 8), np.int32)
+        _check(self.L.cmg_grid_tables(self.h, _p(nb), _p(ch)), "tables")
+        return nb, ch
+
+    def channel_ptr(self, ch):
+        p = ctypes.c_void_p()
+        _check(self.L.cmg_grid_channel_ptr(self.h, ch, ctypes.byref(p)), "channel_ptr")
+        return p.value
+
+    def upload(self, ch, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float32).reshape(-1)
+        _check(self.L.cmg_grid_upload_channel(self.h, ch, _p(a), a.size), "upload_channel")
+
+    def download(self, ch):
+        a = np.zeros((self.num_tiles, 512), np.float32)
+        _check(self.L.cmg_grid_download_channel(self.h, ch, _p(a), a.size), "download_channel")
+        return a
+
+    def upload_cell_types(self, arr):
+        a = np.ascontiguousarray(arr, dtype=np.uint8).reshape(-1)
+        _check(self.L.cmg_grid_upload_cell_types(self.h, _p(a), a.size), "upload_cell_types")
+
+    def download_cell_types(self):
+        a = np.zeros((self.num_tiles, 512), np.uint8)
+        _check(self.L.cmg_grid_download_cell_types(self.h, _p(a), a.size), "download_cell_types")
+        return a
+
+    def fill(self, ch, value):
+        _check(self.L.cmg_grid_fill_channel(self.h, ch, value), "fill_channel")
+
+    def set_leaf_cell_types_case(self, case_id, params=(0, 0)):
+        prm = np.asarray(params, dtype=np.float64)
+        _check(self.L.cmg_grid_set_leaf_cell_types_case(self.h, case_id, _p(prm), len(prm)), "set_leaf_cell_types")
+
+    def set_stream(self, stream_ptr):
+        _check(self.L.cmg_grid_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "set_stream")
+
+    def synchronize(self):
+        _check(self.L.cmg_grid_synchronize(self.h), "synchronize")
+
+    # operator set-up and rhs (src/AMGSolver.cu, cirrus_cutcell/MeshCutCell.cu)
+    def prepare_system(self, coeff_ch, R_matrix):
+        _check(self.L.cmg_amg_prepare_system(self.h, coeff_ch, R_matrix), "prepare_system")
+
+    def cutcell_sphere_coeffs(self, coeff_ch, spheres, R_matrix=0.5):
+        s = np.ascontiguousarray(np.asarray(spheres, dtype=np.float32).reshape(-1, 4))
+        _check(self.L.cmg_amg_cutcell_sphere_coeffs(self.h, coeff_ch, R_matrix, s.shape[0], _p(s)), "cutcell_sphere_coeffs")
+
+    def face_velocity_fourier(self, u_ch, k, amp, phase):
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        amp = np.ascontiguousarray(amp, dtype=np.float64)
+        phase = np.ascontiguousarray(phase, dtype=np.float64)
+        _check(self.L.cmg_amg_face_velocity_fourier(self.h, u_ch, len(phase), _p(k), _p(amp), _p(phase)), "face_velocity")
+
+    def divergence(self, u_ch, coeff_ch, out_ch):
+        _check(self.L.cmg_amg_divergence(self.h, u_ch, coeff_ch, out_ch), "divergence")
+
+    def full_neg_lap(self, x_ch, coeff_ch, ax_ch):
+        _check(self.L.cmg_amg_full_neg_lap(self.h, x_ch, coeff_ch, ax_ch), "full_neg_lap")
+
+    def dot(self, a_ch, b_ch):
+        out = ctypes.c_double(0)
+        _check(self.L.cmg_amg_dot(self.h, a_ch, b_ch, ctypes.byref(out)), "dot")
+        return out.value
+
+
+class AMGSolver:
+    """AMGSolver (src/AMGSolver.h:19-75): FAS mu-cycle preconditioned CG."""
+
+    def __init__(self, coeff_channel, R_matrix_coeff=1.0, R_restrict_coeff=1.0, P_coeff=1.0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        _check(self.L.cmg_amg_solver_create(coeff_channel, R_matrix_coeff, R_restrict_coeff, P_coeff, ctypes.byref(h)),
+               "cmg_amg_solver_create")
+        self.h = h
+        self.coeff_channel = coeff_channel
+        self.R_matrix_coeff = R_matrix_coeff
+        self.omega = 1.5
+        self.mu_cycle_repeat_times = 2
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.cmg_amg_solver_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def _sync_params(self):
+        _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")
+
+    def prepareTypesAndCoeffs(self, grid):
+        _check(self.L.cmg_amg_prepare_types_and_coeffs(grid.h, self.coeff_channel, self.R_matrix_coeff), "prepareTypesAndCoeffs")
+
+    def solve(self, grid, verbose, max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride, is_pure_neumann):
+        self._sync_params()
+        it, rel = ctypes.c_int(0), ctypes.c_double(0)
+        _check(self.L.cmg_amg_solve(self.h, grid.h, int(verbose), max_iters, relative_tolerance, level_iters, coarsest_iters,
+                                    sync_stride, int(is_pure_neumann), ctypes.byref(it), ctypes.byref(rel)), "solve")
+        return it.value, rel.value
+
+    def solve_host(self, grid, b_host_ptr, x_host_ptr, count, max_iters, relative_tolerance, level_iters, coarsest_iters,
+                   sync_stride=1, is_pure_neumann=False):
+        """Solve with host buffers (pointers, e.g. pinned memory): b copied in, x copied out."""
+        self._sync_params()
+        it, rel = ctypes.c_int(0), ctypes.c_double(0)
+        _check(self.L.cmg_amg_solve_host(self.h, grid.h, ctypes.c_void_p(b_host_ptr), ctypes.c_void_p(x_host_ptr), count,
+                                         max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride,
+                                         int(is_pure_neumann), ctypes.byref(it), ctypes.byref(rel)), "solve_host")
+        return it.value, rel.value
+
+    def gauss_seidel(self, grid, iters, order, level, x_ch, rhs_ch):
+        self._sync_params()
+        _check(self.L.cmg_amg_gauss_seidel(self.h, grid.h, iters, order, level, x_ch, rhs_ch), "gauss_seidel")
+
+    def fas_mu_cycle(self, grid, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters):
+        self._sync_params()
+        _check(self.L.cmg_amg_fas_mu_cycle(self.h, grid.h, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters), "fas_mu_cycle")
+
+    def last_solve_ms(self):
+        ms = ctypes.c_float(0)
+        _check(self.L.cmg_amg_last_solve_ms(self.h, ctypes.byref(ms)), "last_solve_ms")
+        return ms.value

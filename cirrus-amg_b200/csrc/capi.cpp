@@ -1,0 +1,362 @@
+// extern "C" entry points declared in include/cmg.h.
+#include "cmg.h"
+
+#include <cstring>
+#include <exception>
+#include <new>
+#include <vector>
+
+#include "cmg_impl.hpp"
+
+struct cmg_grid {
+    cmg::Grid g;
+    cmg_grid(float h0, int nl, int nc) : g(h0, nl, nc) {}
+};
+struct cmg_amg_solver {
+    cmg::Solver s;
+    cmg_amg_solver(int c, float rm, float rr, float p) : s(c, rm, rr, p) {}
+};
+
+namespace {
+
+int fail(int code, const char* msg) {
+    cmg::set_error(msg);
+    return code;
+}
+#define GUARD_BEGIN try {
+#define GUARD_END                                                   \
+    }                                                               \
+    catch (const std::bad_alloc&) { return fail(CMG_ERR_INVALID, "host allocation failed"); } \
+    catch (const std::exception& e) { return fail(CMG_ERR_INVALID, e.what()); }
+#define CKC(call)                                                    \
+    do {                                                             \
+        int _rc = cmg::check_cuda((call), #call);                    \
+        if (_rc) return _rc;                                         \
+    } while (0)
+
+bool host_ready(cmg_grid* g) { return g && g->g.built && g->g.topo.size() > 0; }
+// topology built and its device copy current (uploads it on first use)
+bool grid_ready(cmg_grid* g) { return host_ready(g) && g->g.ensure_device() == 0; }
+bool chan_ok(cmg_grid* g, int ch) { return ch >= 0 && ch < g->g.nch; }
+
+// per-grid reduction scratch for stand-alone dot products
+struct DotScratch {
+    double* partial = nullptr;
+    cmg::PcgScalars* s = nullptr;
+    int cap = 0;
+};
+DotScratch& dot_scratch(cmg_grid* g) {
+    static thread_local std::vector<std::pair<cmg_grid*, DotScratch>> v;
+    for (auto& p : v)
+        if (p.first == g) return p.second;
+    v.push_back({g, DotScratch{}});
+    return v.back().second;
+}
+
+int prepare_system(cmg::Grid& G, int coeff_ch, float R) {
+    const cmg::DevGrid d = G.dev();
+    for (int L = G.max_level(); L > 0; --L)
+        cmg::launch_coarsen_offdiag(d, G.level_begin(L), G.level_end(L) - G.level_begin(L), coeff_ch, R, G.stream);
+    for (int L = G.max_level(); L >= 0; --L) cmg::launch_diag(d, G.level_begin(L), G.level_end(L) - G.level_begin(L), coeff_ch, R, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "prepare_system");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cmg_last_error(void) { return cmg::last_error(); }
+int cmg_version(void) { return 1; }
+
+int cmg_grid_create(float h0, int num_levels, int num_channels, cmg_grid** out) {
+    GUARD_BEGIN
+    if (!out || !(h0 > 0) || num_levels < 1 || num_levels > 16 || num_channels < 1) return fail(CMG_ERR_INVALID, "cmg_grid_create: bad argument");
+    *out = new cmg_grid(h0, num_levels, num_channels);
+    return CMG_OK;
+    GUARD_END
+}
+int cmg_grid_destroy(cmg_grid* g) {
+    delete g;
+    return CMG_OK;
+}
+int cmg_grid_set_tile(cmg_grid* g, int level, int i, int j, int k, int tile_type) {
+    GUARD_BEGIN
+    if (!g || (tile_type != CMG_LEAF && tile_type != CMG_NONLEAF && tile_type != CMG_GHOST)) return fail(CMG_ERR_INVALID, "cmg_grid_set_tile: bad type");
+    if (g->g.topo.set(level, i, j, k, tile_type) < 0) return fail(CMG_ERR_INVALID, "cmg_grid_set_tile: level out of range");
+    return CMG_OK;
+    GUARD_END
+}
+int cmg_grid_rebuild(cmg_grid* g) {
+    GUARD_BEGIN
+    if (!g) return fail(CMG_ERR_INVALID, "null grid");
+    return g->g.rebuild();
+    GUARD_END
+}
+int cmg_grid_iterative_refine(cmg_grid* g, cmg_level_target_fn fn, void* user, int* steps) {
+    GUARD_BEGIN
+    if (!g || !fn) return fail(CMG_ERR_INVALID, "cmg_grid_iterative_refine: null argument");
+    int st = g->g.topo.iterative_refine([&](int level, int i, int j, int k) { return fn(user, level, i, j, k); });
+    if (steps) *steps = st;
+    return g->g.rebuild();
+    GUARD_END
+}
+int cmg_grid_refine_case(cmg_grid* g, int case_id, const double* params, int nparams, int* steps) {
+    GUARD_BEGIN
+    if (!g || !params || nparams < 2 || case_id < 0 || case_id > 7) return fail(CMG_ERR_INVALID, "cmg_grid_refine_case: bad argument");
+    std::vector<double> prm(params, params + nparams);
+    const float h0 = g->g.topo.h0();
+    int st = g->g.topo.iterative_refine([&](int level, int i, int j, int k) {
+        const int c[3] = {i, j, k};
+        return cmg::case_target(case_id, prm.data(), (int)prm.size(), h0, level, c);
+    });
+    if (steps) *steps = st;
+    return g->g.rebuild();
+    GUARD_END
+}
+int cmg_grid_info(cmg_grid* g, int* num_tiles, int* max_level, int* num_leaf_tiles) {
+    if (!g) return fail(CMG_ERR_INVALID, "null grid");
+    if (num_tiles) *num_tiles = g->g.built ? g->g.topo.size() : 0;
+    if (max_level) *max_level = g->g.max_level();
+    if (num_leaf_tiles) *num_leaf_tiles = g->g.built ? (int)g->g.topo.leaf_list.size() : 0;
+    return CMG_OK;
+}
+int cmg_grid_tiles(cmg_grid* g, int* level, int* ijk, uint8_t* type) {
+    if (!host_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_tiles: grid not built");
+    const auto& T = g->g.topo.tiles();
+    for (int t = 0; t < g->g.topo.size(); ++t) {
+        if (level) level[t] = T[t].level;
+        if (ijk)
+            for (int d = 0; d < 3; ++d) ijk[3 * t + d] = T[t].c[d];
+        if (type) type[t] = (uint8_t)T[t].type;
+    }
+    return CMG_OK;
+}
+int cmg_grid_tables(cmg_grid* g, int* nb, int* child) {
+    if (!host_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_tables: grid not built");
+    if (nb) std::memcpy(nb, g->g.topo.nb.data(), sizeof(int) * 8 * g->g.topo.size());
+    if (child) std::memcpy(child, g->g.topo.child.data(), sizeof(int) * 8 * g->g.topo.size());
+    return CMG_OK;
+}
+int cmg_grid_channel_ptr(cmg_grid* g, int ch, float** dev_ptr) {
+    if (!grid_ready(g) || !dev_ptr) return fail(CMG_ERR_STATE, "cmg_grid_channel_ptr: grid not built");
+    if (!chan_ok(g, ch)) return fail(CMG_ERR_INVALID, "channel out of range");
+    *dev_ptr = g->g.plane(ch);
+    return CMG_OK;
+}
+int cmg_grid_cell_type_ptr(cmg_grid* g, uint8_t** dev_ptr) {
+    if (!grid_ready(g) || !dev_ptr) return fail(CMG_ERR_STATE, "cmg_grid_cell_type_ptr: grid not built");
+    *dev_ptr = g->g.ctype;
+    return CMG_OK;
+}
+int cmg_grid_upload_channel(cmg_grid* g, int ch, const float* host, size_t count) {
+    if (!grid_ready(g) || !host) return fail(CMG_ERR_STATE, "cmg_grid_upload_channel: grid not built");
+    if (!chan_ok(g, ch) || count != (size_t)g->g.n * 512) return fail(CMG_ERR_INVALID, "cmg_grid_upload_channel: bad channel or count");
+    CKC(cudaMemcpyAsync(g->g.plane(ch), host, sizeof(float) * count, cudaMemcpyHostToDevice, g->g.stream));
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return CMG_OK;
+}
+int cmg_grid_download_channel(cmg_grid* g, int ch, float* host, size_t count) {
+    if (!grid_ready(g) || !host) return fail(CMG_ERR_STATE, "cmg_grid_download_channel: grid not built");
+    if (!chan_ok(g, ch) || count != (size_t)g->g.n * 512) return fail(CMG_ERR_INVALID, "cmg_grid_download_channel: bad channel or count");
+    CKC(cudaMemcpyAsync(host, g->g.plane(ch), sizeof(float) * count, cudaMemcpyDeviceToHost, g->g.stream));
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return CMG_OK;
+}
+int cmg_grid_upload_cell_types(cmg_grid* g, const uint8_t* host, size_t count) {
+    if (!grid_ready(g) || !host) return fail(CMG_ERR_STATE, "cmg_grid_upload_cell_types: grid not built");
+    if (count != (size_t)g->g.n * 512) return fail(CMG_ERR_INVALID, "cmg_grid_upload_cell_types: bad count");
+    CKC(cudaMemcpyAsync(g->g.ctype, host, count, cudaMemcpyHostToDevice, g->g.stream));
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return CMG_OK;
+}
+int cmg_grid_download_cell_types(cmg_grid* g, uint8_t* host, size_t count) {
+    if (!grid_ready(g) || !host) return fail(CMG_ERR_STATE, "cmg_grid_download_cell_types: grid not built");
+    if (count != (size_t)g->g.n * 512) return fail(CMG_ERR_INVALID, "cmg_grid_download_cell_types: bad count");
+    CKC(cudaMemcpyAsync(host, g->g.ctype, count, cudaMemcpyDeviceToHost, g->g.stream));
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return CMG_OK;
+}
+int cmg_grid_fill_channel(cmg_grid* g, int ch, float value) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_fill_channel: grid not built");
+    if (!chan_ok(g, ch)) return fail(CMG_ERR_INVALID, "channel out of range");
+    cmg::launch_fill(g->g.plane(ch), (size_t)g->g.n * 512, value, g->g.stream);
+    return cmg::check_cuda(cudaGetLastError(), "fill");
+}
+int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams) {
+    GUARD_BEGIN
+    (void)params;
+    (void)nparams;
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    const int n = g->g.n;
+    std::vector<uint8_t> ty((size_t)n * 512);
+    CKC(cudaMemcpy(ty.data(), g->g.ctype, ty.size(), cudaMemcpyDeviceToHost));
+    const auto& T = g->g.topo.tiles();
+    for (int t = 0; t < n; ++t) {
+        if (T[t].type != cmg::kLeaf) continue;
+        for (int v = 0; v < 512; ++v) ty[(size_t)t * 512 + v] = cmg::case_cell_type(case_id, g->g.topo.h0(), T[t].level, T[t].c, v);
+    }
+    CKC(cudaMemcpy(g->g.ctype, ty.data(), ty.size(), cudaMemcpyHostToDevice));
+    return CMG_OK;
+    GUARD_END
+}
+int cmg_grid_set_stream(cmg_grid* g, void* s) {
+    if (!g) return fail(CMG_ERR_INVALID, "null grid");
+    g->g.stream = (cudaStream_t)s;
+    return CMG_OK;
+}
+int cmg_grid_synchronize(cmg_grid* g) {
+    if (!g) return fail(CMG_ERR_INVALID, "null grid");
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return cmg::check_cuda(cudaGetLastError(), "synchronize");
+}
+
+int cmg_amg_prepare_types_and_coeffs(cmg_grid* g, int coeff_ch, float R) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (coeff_ch < 0 || coeff_ch + 4 > g->g.nch) return fail(CMG_ERR_INVALID, "coefficient channels out of range");
+    const cmg::DevGrid d = g->g.dev();
+    cmg::launch_ghost_types(d, 0, g->g.n, g->g.stream);
+    cmg::launch_face_coeffs(d, 0, g->g.n, coeff_ch, 0, nullptr, g->g.stream);
+    return prepare_system(g->g, coeff_ch, R);
+}
+int cmg_amg_prepare_system(cmg_grid* g, int coeff_ch, float R) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (coeff_ch < 0 || coeff_ch + 4 > g->g.nch) return fail(CMG_ERR_INVALID, "coefficient channels out of range");
+    return prepare_system(g->g, coeff_ch, R);
+}
+int cmg_amg_cutcell_sphere_coeffs(cmg_grid* g, int coeff_ch, float R, int nspheres, const float* spheres) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (coeff_ch < 0 || coeff_ch + 4 > g->g.nch || nspheres < 1 || nspheres > 64 || !spheres)
+        return fail(CMG_ERR_INVALID, "cmg_amg_cutcell_sphere_coeffs: bad argument");
+    cmg::Grid& G = g->g;
+    if (!G.spheres) CKC(cudaMalloc(&G.spheres, sizeof(float) * 4 * 64));
+    CKC(cudaMemcpyAsync(G.spheres, spheres, sizeof(float) * 4 * nspheres, cudaMemcpyHostToDevice, G.stream));
+    const cmg::DevGrid d = G.dev();
+    cmg::launch_cutcell_neumann(d, G.leaf, G.nleaf, nspheres, G.spheres, G.stream);
+    cmg::launch_ghost_types(d, 0, G.n, G.stream);
+    cmg::launch_face_coeffs(d, 0, G.n, coeff_ch, nspheres, G.spheres, G.stream);
+    int rc = prepare_system(G, coeff_ch, R);
+    if (rc) return rc;
+    CKC(cudaStreamSynchronize(G.stream));
+    return CMG_OK;
+}
+int cmg_amg_face_velocity_fourier(cmg_grid* g, int u_ch, int nmodes, const double* k, const double* amp, const double* phase) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (u_ch < 0 || u_ch + 3 > g->g.nch || nmodes < 1 || nmodes > 256 || !k || !amp || !phase)
+        return fail(CMG_ERR_INVALID, "cmg_amg_face_velocity_fourier: bad argument");
+    cmg::Grid& G = g->g;
+    if (!G.modes) CKC(cudaMalloc(&G.modes, sizeof(double) * 7 * 256));
+    CKC(cudaMemcpyAsync(G.modes, k, sizeof(double) * 3 * nmodes, cudaMemcpyHostToDevice, G.stream));
+    CKC(cudaMemcpyAsync(G.modes + 3 * nmodes, amp, sizeof(double) * 3 * nmodes, cudaMemcpyHostToDevice, G.stream));
+    CKC(cudaMemcpyAsync(G.modes + 6 * nmodes, phase, sizeof(double) * nmodes, cudaMemcpyHostToDevice, G.stream));
+    cmg::launch_face_velocity(G.dev(), G.leaf, G.nleaf, u_ch, nmodes, G.modes, G.stream);
+    CKC(cudaStreamSynchronize(G.stream));
+    return cmg::check_cuda(cudaGetLastError(), "face velocity");
+}
+int cmg_amg_divergence(cmg_grid* g, int u_ch, int coeff_ch, int out_ch) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (u_ch < 0 || u_ch + 3 > g->g.nch || coeff_ch < 0 || coeff_ch + 4 > g->g.nch || !chan_ok(g, out_ch))
+        return fail(CMG_ERR_INVALID, "cmg_amg_divergence: channel out of range");
+    cmg::Grid& G = g->g;
+    const cmg::DevGrid d = G.dev();
+    for (int a = 0; a < 3; ++a) cmg::launch_propagate_ghost(d, 0, G.n, u_ch + a, G.stream);
+    cmg::launch_accumulate_faces(d, G.leaf, G.nleaf, u_ch, G.stream);
+    cmg::launch_divergence(d, G.leaf, G.nleaf, u_ch, coeff_ch, out_ch, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "divergence");
+}
+int cmg_amg_full_neg_lap(cmg_grid* g, int x_ch, int coeff_ch, int ax_ch) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (!chan_ok(g, x_ch) || !chan_ok(g, ax_ch) || coeff_ch < 0 || coeff_ch + 4 > g->g.nch)
+        return fail(CMG_ERR_INVALID, "cmg_amg_full_neg_lap: channel out of range");
+    cmg::Grid& G = g->g;
+    cmg::ReduceScratch rs{nullptr, nullptr, nullptr};
+    cmg::launch_leaf_apply(G.dev(), G.leaf, G.nleaf, G.plane(x_ch), G.plane(ax_ch), coeff_ch, false, rs, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "full_neg_lap");
+}
+int cmg_amg_dot(cmg_grid* g, int a_ch, int b_ch, double* out) {
+    if (!grid_ready(g) || !out) return fail(CMG_ERR_STATE, "grid not built");
+    if (!chan_ok(g, a_ch) || !chan_ok(g, b_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_dot: channel out of range");
+    cmg::Grid& G = g->g;
+    DotScratch& D = dot_scratch(g);
+    if (D.cap < G.nleaf) {
+        if (D.partial) cudaFree(D.partial);
+        CKC(cudaMalloc(&D.partial, sizeof(double) * (G.nleaf + 1)));
+        D.cap = G.nleaf;
+    }
+    if (!D.s) {
+        CKC(cudaMalloc(&D.s, sizeof(cmg::PcgScalars)));
+        CKC(cudaMemset(D.s, 0, sizeof(cmg::PcgScalars)));
+    }
+    if (!G.dot_out) CKC(cudaMalloc(&G.dot_out, sizeof(double)));
+    cmg::launch_dot(G.dev(), G.leaf, G.nleaf, G.plane(a_ch), G.plane(b_ch), cmg::kDotStore, G.dot_out,
+                    cmg::ReduceScratch{D.partial, nullptr, D.s}, G.stream);
+    CKC(cudaMemcpyAsync(out, G.dot_out, sizeof(double), cudaMemcpyDeviceToHost, G.stream));
+    CKC(cudaStreamSynchronize(G.stream));
+    return CMG_OK;
+}
+
+int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float P, cmg_amg_solver** out) {
+    GUARD_BEGIN
+    if (!out || coeff_ch < 0) return fail(CMG_ERR_INVALID, "cmg_amg_solver_create: bad argument");
+    cmg_amg_solver* s = new cmg_amg_solver(coeff_ch, R_matrix, R_restrict, P);
+    int rc = s->s.init();
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return CMG_OK;
+    GUARD_END
+}
+int cmg_amg_solver_destroy(cmg_amg_solver* s) {
+    delete s;
+    return CMG_OK;
+}
+int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu) {
+    if (!s || mu < 0 || !(omega > 0)) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_smoother: bad argument");
+    s->s.omega = omega;
+    s->s.mu = mu;
+    return CMG_OK;
+}
+int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
+                  int pure_neumann, int* iters, double* rel_res) {
+    GUARD_BEGIN
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_amg_solve: solver or grid not ready");
+    return s->s.solve(g->g, verbose != 0, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, iters, rel_res);
+    GUARD_END
+}
+int cmg_amg_solve_host(cmg_amg_solver* s, cmg_grid* g, const float* b_host, float* x_host, size_t count, int max_iters, double tol,
+                       int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, int* iters, double* rel_res) {
+    GUARD_BEGIN
+    if (!s || !grid_ready(g) || !b_host || !x_host) return fail(CMG_ERR_STATE, "cmg_amg_solve_host: bad argument");
+    cmg::Grid& G = g->g;
+    if (count != (size_t)G.n * 512 || G.nch < 5) return fail(CMG_ERR_INVALID, "cmg_amg_solve_host: count must be num_tiles*512");
+    CKC(cudaMemcpyAsync(G.plane(1), b_host, sizeof(float) * count, cudaMemcpyHostToDevice, G.stream));
+    int rc = s->s.solve(G, false, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, iters, rel_res);
+    if (rc) return rc;
+    CKC(cudaMemcpyAsync(x_host, G.plane(0), sizeof(float) * count, cudaMemcpyDeviceToHost, G.stream));
+    CKC(cudaStreamSynchronize(G.stream));
+    return CMG_OK;
+    GUARD_END
+}
+int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (level < 0 || level > g->g.max_level() || !chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || (order != 0 && order != 1))
+        return fail(CMG_ERR_INVALID, "cmg_amg_gauss_seidel: bad argument");
+    s->s.enqueue_gs(g->g, level, iters, order, g->g.plane(x_ch), g->g.plane(rhs_ch), g->g.stream);
+    return cmg::check_cuda(cudaGetLastError(), "gauss_seidel");
+}
+int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (!chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || !chan_ok(g, x0_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_fas_mu_cycle: channel out of range");
+    if (int rc = cmg::validate_solver_topology(g->g)) return rc;
+    const cmg::MuArgs A = s->s.mu_args(g->g, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters);
+    s->s.enqueue_mu_cycle(g->g, A, g->g.stream);
+    return cmg::check_cuda(cudaGetLastError(), "fas_mu_cycle");
+}
+int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms) {
+    if (!s || !ms) return fail(CMG_ERR_INVALID, "null argument");
+    *ms = s->s.last_ms;
+    return CMG_OK;
+}
+
+}  // extern "C"

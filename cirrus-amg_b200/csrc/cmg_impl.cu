@@ -1,0 +1,400 @@
+// Device octree and AMG solver (see cmg_impl.hpp).
+#include "cmg_impl.hpp"
+
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <unordered_map>
+
+namespace cmg {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+int check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return 0;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return 2;
+}
+#define CK(call)                                      \
+    do {                                              \
+        int _rc = check_cuda((call), #call);          \
+        if (_rc) return _rc;                          \
+    } while (0)
+
+template <class T>
+static void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+Grid::~Grid() {
+    dfree(chan);
+    dfree(ctype);
+    dfree(meta);
+    dfree(nb);
+    dfree(child);
+    dfree(leaf);
+    dfree(spheres);
+    dfree(modes);
+    dfree(dot_out);
+}
+
+static unsigned long long tile_key(const TileRec& r) {
+    return ((unsigned long long)(r.level & 0xff) << 56) | ((unsigned long long)((r.c[0] + 4) & 0x3ffff) << 36) |
+           ((unsigned long long)((r.c[1] + 4) & 0x3ffff) << 18) | (unsigned long long)((r.c[2] + 4) & 0x3ffff);
+}
+
+// HADeviceGrid::rebuild (src/HAGrid.h:892): spawn ghosts, put the tiles in
+// device order and build the tables (host side only).
+int Grid::rebuild() {
+    topo.spawn_ghosts();
+    topo.canonicalize();
+    built = true;
+    ++host_version;
+    return 0;
+}
+
+// syncHostAndDevice (src/HAGrid.h:653): allocate the channel planes of the
+// current topology and upload its tables.  Tiles that already had device
+// storage keep their channel values and cell types; new tiles start at zero.
+int Grid::ensure_device() {
+    if (!built) {
+        set_error("grid not built: call rebuild or refine first");
+        return 3;
+    }
+    if (dev_version == host_version && n > 0) return 0;
+    const int n_old = n;
+    const int n_new = topo.size();
+    std::unordered_map<unsigned long long, int> old_index;
+    old_index.reserve(2 * dev_keys.size() + 1);
+    for (int t = 0; t < (int)dev_keys.size(); ++t) old_index.emplace(dev_keys[t], t);
+    std::vector<int> old_of_new(n_new);
+    std::vector<unsigned long long> keys(n_new);
+    for (int t = 0; t < n_new; ++t) {
+        keys[t] = tile_key(topo.tiles()[t]);
+        auto it = old_index.find(keys[t]);
+        old_of_new[t] = it == old_index.end() ? -1 : it->second;
+    }
+
+    float* chan_new = nullptr;
+    uint8_t* ct_new = nullptr;
+    const size_t cells = (size_t)n_new * kCells;
+    CK(cudaMalloc(&chan_new, sizeof(float) * cells * nch + 16));
+    CK(cudaMalloc(&ct_new, cells + 16));
+    int* d_map = nullptr;
+    CK(cudaMalloc(&d_map, sizeof(int) * (n_new + 1)));
+    CK(cudaMemcpy(d_map, old_of_new.data(), sizeof(int) * n_new, cudaMemcpyHostToDevice));
+    if (n_old > 0) {
+        launch_remap(chan, chan_new, d_map, n_new, nch, n_old, stream);
+        launch_remap_types(ctype, ct_new, d_map, n_new, stream);
+    } else {
+        CK(cudaMemsetAsync(chan_new, 0, sizeof(float) * cells * nch, stream));
+        CK(cudaMemsetAsync(ct_new, 0, cells, stream));
+    }
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaGetLastError());
+    cudaFree(d_map);
+    dfree(chan);
+    dfree(ctype);
+    chan = chan_new;
+    ctype = ct_new;
+
+    std::vector<int4> hm(n_new);
+    for (int t = 0; t < n_new; ++t) {
+        const TileRec& r = topo.tiles()[t];
+        hm[t] = make_int4(r.level | (r.type << 8), r.c[0], r.c[1], r.c[2]);
+    }
+    dfree(meta);
+    dfree(nb);
+    dfree(child);
+    dfree(leaf);
+    CK(cudaMalloc(&meta, sizeof(int4) * (n_new + 1)));
+    CK(cudaMalloc(&nb, sizeof(int) * 8 * (n_new + 1)));
+    CK(cudaMalloc(&child, sizeof(int) * 8 * (n_new + 1)));
+    CK(cudaMalloc(&leaf, sizeof(int) * (topo.leaf_list.size() + 1)));
+    CK(cudaMemcpy(meta, hm.data(), sizeof(int4) * n_new, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(nb, topo.nb.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(child, topo.child.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(leaf, topo.leaf_list.data(), sizeof(int) * topo.leaf_list.size(), cudaMemcpyHostToDevice));
+    n = n_new;
+    nleaf = (int)topo.leaf_list.size();
+    dev_keys.swap(keys);
+    dev_version = host_version;
+    ++version;
+    return 0;
+}
+
+// The stencil kernels rely on three properties of a tree built by
+// refineStep + spawnGhostTiles; a grid assembled by hand is checked here.
+//  1. every GHOST tile has a LEAF parent tile;
+//  2. where a LEAF tile touches a same-level NONLEAF tile, the NONLEAF cells on
+//     that face have LEAF children (the reference reads them after a one-step
+//     children-to-parent average, src/AMGSolver.cu:607);
+//  3. levels 0 and 1 hold no GHOST tiles (they run in the coarse kernel).
+int validate_solver_topology(const Grid& G) {
+    const auto& T = G.topo.tiles();
+    for (int t = 0; t < G.n; ++t) {
+        const TileRec& r = T[t];
+        if (r.type == kGhost) {
+            const int p = G.topo.nb[8 * t + 6];
+            if (p < 0 || !(T[p].type & kLeaf)) {
+                set_error("GHOST tile without a LEAF parent");
+                return 4;
+            }
+            if (r.level <= 1) {
+                set_error("GHOST tile on level 0 or 1");
+                return 4;
+            }
+        }
+        if (r.type != kLeaf) continue;
+        for (int a = 0; a < 6; ++a) {
+            const int q = G.topo.nb[8 * t + a];
+            if (q < 0 || T[q].type != kNonLeaf) continue;
+            const int axis = a % 3, plus = a / 3;
+            for (int ci = 0; ci < 8; ++ci) {
+                const int bit = axis == 0 ? (ci >> 2) : axis == 1 ? ((ci >> 1) & 1) : (ci & 1);
+                if (bit != (plus ? 0 : 1)) continue;  // children on the shared face
+                const int c = G.topo.child[8 * q + ci];
+                if (c < 0 || T[c].type != kLeaf) {
+                    set_error("octree is not 2:1 face-balanced next to a LEAF tile");
+                    return 4;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+Solver::~Solver() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    dfree(partial);
+    dfree(partial2);
+    dfree(s);
+    if (h_s) cudaFreeHost(h_s);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+}
+
+int Solver::init() {
+    CK(cudaMalloc(&s, sizeof(PcgScalars)));
+    CK(cudaMemset(s, 0, sizeof(PcgScalars)));
+    CK(cudaMallocHost(&h_s, sizeof(PcgScalars)));
+    std::memset(h_s, 0, sizeof(PcgScalars));
+    CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    init_kernel_attributes();
+    return check_cuda(cudaGetLastError(), "kernel attributes");
+}
+
+int Solver::ensure_scratch(int nl) {
+    if (nl <= partial_cap) return 0;
+    dfree(partial);
+    dfree(partial2);
+    CK(cudaMalloc(&partial, sizeof(double) * (nl + 1)));
+    CK(cudaMalloc(&partial2, sizeof(double) * (nl + 1)));
+    partial_cap = nl;
+    // captured graphs hold the old scratch pointers
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+    return 0;
+}
+
+MuArgs Solver::mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) const {
+    MuArgs A;
+    A.X = G.plane(x_ch);
+    A.RHS = G.plane(rhs_ch);
+    A.X0 = G.plane(x0_ch);
+    A.coeff_ch = coeff_ch;
+    A.mu = mu;
+    A.level_iters = level_iters;
+    A.coarsest_iters = coarsest_iters;
+    A.omega = omega;
+    A.Rr = R_restrict;
+    A.P = P;
+    return A;
+}
+
+// GaussSeidelAMG (src/AMGSolver.cu:887-894) on the LEAF and NONLEAF tiles of one level
+void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    const int t0 = G.level_begin(level), nt = G.ghost_begin(level) - t0;
+    for (int it = 0; it < iters; ++it) {
+        launch_gs(d, t0, nt, X, RHS, coeff_ch, order, omega, st);
+        launch_gs(d, t0, nt, X, RHS, coeff_ch, 1 - order, omega, st);
+    }
+}
+
+// AMGSolver::FASMuCycleStep (src/AMGSolver.cu:1257-1277).  Levels 0 and 1 run
+// as a single coarse-kernel launch.
+void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    if (l <= 1) {
+        launch_coarse_step(d, l, G.level_end(l), 1, A.X, A.RHS, A.X0, A.coeff_ch, A.mu,
+                           A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P, st);
+        return;
+    }
+    enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st);
+    launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
+    launch_fas_save(d, G.nonleaf_begin(l - 1), G.ghost_begin(l - 1) - G.nonleaf_begin(l - 1), A.X, A.RHS, A.X0, A.coeff_ch, st);
+    for (int r = 0; r < A.mu; ++r) enqueue_mu_step(G, l - 1, A, st);
+    launch_prolong(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), A.X, A.X0, A.P, st);
+    enqueue_gs(G, l, A.level_iters, 1, A.X, A.RHS, st);
+}
+
+// AMGSolver::FASMuCycle (src/AMGSolver.cu:1279-1292): zero x everywhere, then the top step
+void Solver::enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const {
+    launch_fill(A.X, (size_t)G.n * kCells, 0.0f, st);
+    enqueue_mu_step(G, G.max_level(), A, st);
+}
+
+static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
+    cudaStreamCaptureStatus stt;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &stt, nullptr, nullptr, &deps, &nd));
+    tail.assign(deps, deps + nd);
+    return 0;
+}
+
+// The whole of AMGSolver::solve (src/AMGSolver.cu:1399-1549) as one graph:
+//   x = 0; rr0 = r.r; [recenter]; z = M r; p = z; gamma = z.r; gate
+//   WHILE (not done):  Ap = A p (+ alpha);  x, r update (+ r.r, convergence)
+//                      IF (not done): [recenter]; z = M r; beta; p = z + beta p
+int Solver::build_graph(Grid& G, const Key& k, cudaGraphExec_t* out) {
+    const DevGrid d = G.dev();
+    const ReduceScratch rs = scratch();
+    float* X = G.plane(0);
+    float* R = G.plane(1);
+    float* Pp = G.plane(2);
+    float* AP = G.plane(3);
+    float* Z = G.plane(4);
+    const MuArgs A = mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters);
+    cudaStream_t cs = cap_stream;
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+
+    cudaGraph_t top;
+    CK(cudaGraphCreate(&top, 0));
+    cudaGraphConditionalHandle loop_h = 0, body_h = 0;
+    CK(cudaGraphConditionalHandleCreate(&loop_h, top, 1, cudaGraphCondAssignDefault));
+
+    CK(cudaStreamBeginCaptureToGraph(cs, top, nullptr, nullptr, 0, mode));
+    launch_leaf_fill(d, G.leaf, G.nleaf, X, 0.0f, cs);
+    if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, R, R, kDotRR0, nullptr, rs, cs);
+    if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, R, rs, cs);
+    enqueue_mu_cycle(G, A, cs);
+    launch_leaf_copy(d, G.leaf, G.nleaf, Pp, Z, cs);
+    launch_dot(d, G.leaf, G.nleaf, Z, R, kDotGammaInit, nullptr, rs, cs);
+    launch_loop_gate(rs, loop_h, cs);
+    std::vector<cudaGraphNode_t> tail;
+    if (int rc = capture_tail(cs, tail)) return rc;
+    CK(cudaStreamEndCapture(cs, &top));
+
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = loop_h;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, top, tail.data(), tail.size(), &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    CK(cudaGraphConditionalHandleCreate(&body_h, body, 0, cudaGraphCondAssignDefault));
+
+    CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
+    launch_leaf_apply(d, G.leaf, G.nleaf, Pp, AP, coeff_ch, true, rs, cs);
+    launch_xr_update(d, G.leaf, G.nleaf, X, R, Pp, AP, rs, loop_h, body_h, true, cs);
+    if (int rc = capture_tail(cs, tail)) return rc;
+    CK(cudaStreamEndCapture(cs, &body));
+
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = body_h;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    CK(cudaGraphAddNode(&inode, body, tail.data(), tail.size(), &ip));
+    cudaGraph_t ibody = ip.conditional.phGraph_out[0];
+
+    CK(cudaStreamBeginCaptureToGraph(cs, ibody, nullptr, nullptr, 0, mode));
+    if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, R, rs, cs);
+    enqueue_mu_cycle(G, A, cs);
+    launch_dot(d, G.leaf, G.nleaf, R, Z, kDotBeta, nullptr, rs, cs);
+    launch_p_update(d, G.leaf, G.nleaf, Pp, Z, rs, cs);
+    CK(cudaStreamEndCapture(cs, &ibody));
+
+    cudaGraphExec_t exec;
+    CK(cudaGraphInstantiate(&exec, top, 0));
+    cudaGraphDestroy(top);
+    *out = exec;
+    return 0;
+}
+
+int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann,
+                  int* iters, double* rel) {
+    if (G.n == 0 || G.nleaf == 0) {
+        set_error("solve: grid has no LEAF tiles (rebuild first)");
+        return 3;
+    }
+    if (G.nch < 5 || coeff_ch < 5 || coeff_ch + 4 > G.nch) {
+        set_error("solve: needs channels 0..4 and coefficient channels coeff..coeff+3 (coeff >= 5)");
+        return 1;
+    }
+    if (max_iters < 0 || level_iters < 0 || coarsest_iters < 0 || mu < 0) {
+        set_error("solve: negative iteration count");
+        return 1;
+    }
+    if (int rc = validate_solver_topology(G)) return rc;
+    if (int rc = ensure_scratch(G.nleaf)) return rc;
+    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, sync_stride > 0 ? 1 : 0, omega};
+    cudaGraphExec_t exec;
+    auto it = graphs.find(k);
+    if (it == graphs.end()) {
+        if (int rc = build_graph(G, k, &exec)) return rc;
+        graphs[k] = exec;
+    } else {
+        exec = it->second;
+    }
+    std::memset(h_s, 0, sizeof(PcgScalars));
+    h_s->max_iters = max_iters;
+    h_s->sync_stride = sync_stride;
+    h_s->thr = -1.0;
+    h_s->tol = tol;  // the gate kernel turns it into max(tol^2 rr0, DBL_MIN)
+    cudaStream_t st = G.stream;
+    CK(cudaMemcpyAsync(s, h_s, sizeof(PcgScalars), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(ev0, st));
+    CK(cudaGraphLaunch(exec, st));
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    cudaEventElapsedTime(&last_ms, ev0, ev1);
+    const PcgScalars& r = *h_s;
+    int n_it = r.iter;
+    double rel_res;
+    if (sync_stride > 0) {
+        if (r.rr0 == 0.0) {
+            n_it = 0;
+            rel_res = 0.0;
+        } else if (n_it == 0) {
+            rel_res = 1.0;
+        } else {
+            rel_res = std::sqrt(r.rr / r.rr0);
+        }
+    } else {
+        rel_res = -1.0;
+    }
+    if (iters) *iters = n_it;
+    if (rel) *rel = rel_res;
+    if (verbose) std::printf("cmg AMG-PCG: %d iterations, relative residual %.6e, %.3f ms\n", n_it, rel_res, last_ms);
+    if (r.nonfinite) {
+        set_error("solve: non-finite value in a PCG reduction");
+        return 5;
+    }
+    return 0;
+}
+
+}  // namespace cmg

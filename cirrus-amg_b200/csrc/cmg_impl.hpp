@@ -1,0 +1,121 @@
+// Host objects behind the C ABI: the device octree (cmg_grid) and the AMG
+// solver (cmg_amg_solver).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "kernels.hpp"
+#include "topology.hpp"
+
+namespace cmg {
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+// Device octree: HADeviceGrid's role (src/HAGrid.h:357).
+struct Grid {
+    Topology topo;
+    int nch;
+    cudaStream_t stream = nullptr;
+
+    int n = 0;  // tiles on the device
+    bool built = false;                   // host topology ordered and tabled
+    unsigned long long host_version = 0;  // bumps on every rebuild
+    unsigned long long dev_version = 0;   // host_version the device copy matches
+    std::vector<unsigned long long> dev_keys;
+    float* chan = nullptr;
+    uint8_t* ctype = nullptr;
+    int4* meta = nullptr;
+    int* nb = nullptr;
+    int* child = nullptr;
+    int* leaf = nullptr;
+    int nleaf = 0;
+    unsigned long long version = 0;
+    float* spheres = nullptr;  // device scratch for set-up calls
+    double* modes = nullptr;
+    double* dot_out = nullptr;
+
+    Grid(float h0, int num_levels, int num_channels) : topo(h0, num_levels), nch(num_channels) {}
+    ~Grid();
+    int rebuild();        // host: ghosts, order, tables
+    int ensure_device();  // device: storage and tables of the current topology
+    DevGrid dev() const {
+        DevGrid d;
+        d.n = n;
+        d.nch = nch;
+        d.h0 = topo.h0();
+        d.chan = chan;
+        d.ctype = ctype;
+        d.meta = meta;
+        d.nb = nb;
+        d.child = child;
+        return d;
+    }
+    float* plane(int c) const { return chan + (size_t)c * (size_t)n * kCells; }
+    int max_level() const { return topo.max_level(); }
+    int level_begin(int l) const { return topo.level_begin[l]; }
+    int level_end(int l) const { return topo.level_end[l]; }
+    int nonleaf_begin(int l) const { return topo.nonleaf_begin[l]; }
+    int ghost_begin(int l) const { return topo.ghost_begin[l]; }
+};
+
+struct MuArgs {
+    float* X;
+    float* RHS;
+    float* X0;
+    int coeff_ch, mu, level_iters, coarsest_iters;
+    double omega;
+    float Rr, P;
+};
+
+// AMGSolver (src/AMGSolver.h:19-75)
+struct Solver {
+    int coeff_ch;
+    float R_matrix, R_restrict, P;
+    double omega = 1.5;
+    int mu = 2;
+
+    double* partial = nullptr;
+    double* partial2 = nullptr;
+    int partial_cap = 0;
+    PcgScalars* s = nullptr;
+    PcgScalars* h_s = nullptr;  // pinned mirror
+    cudaStream_t cap_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.0f;
+    bool conditional_ok = true;
+
+    struct Key {
+        const Grid* g;
+        unsigned long long version;
+        int level_iters, coarsest_iters, pure_neumann, mu, sync;
+        double omega;
+        bool operator<(const Key& o) const {
+            return std::tie(g, version, level_iters, coarsest_iters, pure_neumann, mu, sync, omega) <
+                   std::tie(o.g, o.version, o.level_iters, o.coarsest_iters, o.pure_neumann, o.mu, o.sync, o.omega);
+        }
+    };
+    std::map<Key, cudaGraphExec_t> graphs;
+
+    Solver(int c, float rm, float rr, float p) : coeff_ch(c), R_matrix(rm), R_restrict(rr), P(p) {}
+    ~Solver();
+    int init();
+    int ensure_scratch(int nleaf);
+    ReduceScratch scratch() const { return ReduceScratch{partial, partial2, s}; }
+    MuArgs mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) const;
+    void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
+    void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st) const;
+    void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
+    int build_graph(Grid& G, const Key& k, cudaGraphExec_t* out);
+    int solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
+              bool pure_neumann, int* iters, double* rel);
+};
+
+int check_cuda(cudaError_t e, const char* what);
+int validate_solver_topology(const Grid& G);
+
+}  // namespace cmg

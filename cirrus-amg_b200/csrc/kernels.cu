@@ -1,0 +1,949 @@
+// Device kernels of the octree MG-preconditioned CG solve (sm_100a).
+//
+// Launch shape: one 128-thread block per 8^3 tile; every thread owns four
+// consecutive cells along k (one float4 of each channel plane), so each
+// channel of a tile moves as one fully coalesced 2 KB transaction set.  Tile
+// and halo values are staged in a shared-memory snapshot (device.cuh).
+// Reductions are deterministic: one double per block, summed in a fixed order
+// by the last block to finish, which then applies the scalar update the
+// reference does with one-thread kernels (TernaryOnArray, src/GPUUtils.h:72).
+#include "kernels.hpp"
+
+#include <algorithm>
+#include <cfloat>
+
+namespace cmg {
+
+namespace {
+
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    return is_last;
+}
+__device__ __forceinline__ double sum_partials(const double* part, int n, double* red) {
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += 128) s += __ldcg(part + i);
+    return block_sum128(s, red);
+}
+// products of four cells summed in float, the reference's Dot128Kernel (src/PoissonGrid.cu:168-172)
+__device__ __forceinline__ double dot4(const float4& a, const float4& b) {
+    float f = __fmul_rn(a.x, b.x);
+    f = __fmaf_rn(a.y, b.y, f);
+    f = __fmaf_rn(a.z, b.z, f);
+    f = __fmaf_rn(a.w, b.w, f);
+    return (double)f;
+}
+
+// ---------------------------------------------------------------------------
+// multigrid
+// ---------------------------------------------------------------------------
+// NegativeLaplacianAndGaussSeidelSameLevelAMG128Kernel (src/AMGSolver.cu:838-877)
+template <bool kExactOmega>
+__global__ void __launch_bounds__(128) k_gs(DevGrid g, int t0, float* X, const float* B, int coeff_ch, int color, float om,
+                                            double omega) {
+    __shared__ Snap S;
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    float4 xr, dg;
+    uchar4 ty;
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg);
+    const float4 b = ld4(B + Q.base);
+    float4 out = xr;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int k = Q.k0 + u;
+        if (((Q.i + Q.j + k) & 1) != color) continue;
+        const float d = f4get(dg, u);
+        const float ax = snap_neg_lap(S, Q.i, Q.j, k, d);
+        const float delta = (t4get(ty, u) & dInterior) ? __fdiv_rn(__fsub_rn(f4get(b, u), ax), d) : 0.0f;
+        const float xs = S.x[sx(Q.i, Q.j, k)];
+        f4set(out, u, kExactOmega ? __fmaf_rn(delta, om, xs) : (float)((double)xs + (double)delta * omega));
+    }
+    st4(X + Q.base, out);
+}
+
+// ResidualAndRestrictAMG128Kernel (src/AMGSolver.cu:896-960)
+__global__ void __launch_bounds__(128) k_restrict(DevGrid g, int t0, float* X, float* RHS, int coeff_ch, float Rr) {
+    __shared__ Snap S;
+    __shared__ float res[kCells];
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    float4 xr, dg;
+    uchar4 ty;
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg);
+    const float4 rh = ld4(RHS + Q.base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) res[4 * Q.q + u] = __fsub_rn(f4get(rh, u), snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u)));
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        const int b = threadIdx.x;
+        const int f0 = (b >> 4) * 2, f1 = ((b >> 2) & 3) * 2, f2 = (b & 3) * 2;
+        float rs = 0.0f, xs = 0.0f;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    rs = __fadd_rn(rs, res[cell_index(f0 + ii, f1 + jj, f2 + kk)]);
+                    xs = __fadd_rn(xs, S.x[sx(f0 + ii, f1 + jj, f2 + kk)]);
+                }
+        const int p = g.nb[8 * t + 6];
+        if (p >= 0) {
+            const int4 m = g.meta[t];
+            const size_t o = (size_t)p * kCells + cell_index(parent_local(m.y, f0), parent_local(m.z, f1), parent_local(m.w, f2));
+            RHS[o] = __fmul_rn(rs, Rr);
+            X[o] = __fdiv_rn(xs, 8.0f);
+        }
+    }
+}
+
+// FASSaveSolutionAndUpdateSource128Kernel (src/AMGSolver.cu:1176-1206)
+__global__ void __launch_bounds__(128) k_fas_save(DevGrid g, int t0, const float* X, float* RHS, float* X0, int coeff_ch) {
+    __shared__ Snap S;
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    float4 xr, dg;
+    uchar4 ty;
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg);
+    float4 rh = ld4(RHS + Q.base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (t4get(ty, u) & dInterior) {
+            f4set(rh, u, __fadd_rn(f4get(rh, u), snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u))));
+            X0[Q.base + u] = f4get(xr, u);
+        } else {
+            f4set(rh, u, 0.0f);
+        }
+    }
+    st4(RHS + Q.base, rh);
+}
+
+// FASProlongateAndUpdateAMG128Kernel (src/AMGSolver.cu:1216-1248)
+__global__ void __launch_bounds__(128) k_prolong(DevGrid g, int t0, float* X, const float* X0, float P) {
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    const int4 m = g.meta[t];
+    const bool ghost = (m.x >> 8) & dGhost;
+    const int p = g.nb[8 * t + 6];
+    const float4 xr = ld4(X + Q.base);
+    const uchar4 ty = ldt4(g.ctype + Q.base);
+    const int pi = parent_local(m.y, Q.i), pj = parent_local(m.z, Q.j);
+    float4 out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        float cx = 0.0f, cx0 = 0.0f;
+        if (p >= 0) {
+            const size_t o = (size_t)p * kCells + cell_index(pi, pj, parent_local(m.w, Q.k0 + u));
+            cx = X[o];
+            cx0 = X0[o];
+        }
+        const bool in = t4get(ty, u) & dInterior;
+        f4set(out, u, ghost ? (in ? cx : 0.0f) : (in ? __fmaf_rn(P, __fsub_rn(cx, cx0), f4get(xr, u)) : 0.0f));
+    }
+    st4(X + Q.base, out);
+}
+
+// ---------------------------------------------------------------------------
+// Coarse levels: FASMuCycleStep (src/AMGSolver.cu:1257-1277) of level 0 or 1
+// in one 1024-thread block.  Level 0 is the root tile and level 1 its eight
+// children, so the whole sub-cycle (all mu recursions and the 2*coarsest_iters
+// colour sweeps of every coarsest visit) runs out of shared memory with block
+// barriers instead of ~50 kernel launches.  Neither level can hold GHOST
+// tiles (a level-1 ghost would need a LEAF root, which has no active children).
+// ---------------------------------------------------------------------------
+struct CoarseArgs {
+    int top, ntiles, l1b, coeff_ch, mu, level_iters, coarsest_iters, exact;
+    float om, Rr, P;
+    double omega;
+};
+
+struct CoarseSmem {
+    float *x, *rhs, *x0, *c;
+    uint8_t* ty;
+    int* nb;     // [ntiles][6]
+    int* child;  // root children [8]
+    int4* meta;  // [ntiles]
+    int T;
+    float h[2];
+    __device__ float xm(int t, int v) const { return ty[t * kCells + v] == dInterior ? x[t * kCells + v] : 0.0f; }
+    __device__ float coef(int a, int t, int v) const { return c[(a * T + t) * kCells + v]; }
+    // negativeLap with the coarse-level halo (only empty or same-level active neighbours)
+    __device__ float neg_lap(int t, int v) const {
+        const float d = coef(3, t, v);
+        if (d == 0.0f) return 0.0f;
+        const int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+        const int stride[3] = {64, 8, 1};
+        float s = xm(t, v) * d;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int sg = 0; sg < 2; ++sg) {
+                int nt = t, nv = v;
+                if (sg == 0) {
+                    if (l[a] > 0) nv = v - stride[a];
+                    else { nt = nb[t * 6 + a]; nv = v + 7 * stride[a]; }
+                } else {
+                    if (l[a] < 7) nv = v + stride[a];
+                    else { nt = nb[t * 6 + 3 + a]; nv = v - 7 * stride[a]; }
+                }
+                float cf, xv;
+                if (sg == 0) cf = coef(a, t, v);
+                else cf = (nt < 0) ? h[tile_lvl(t)] : coef(a, nt, nv);
+                xv = (nt < 0) ? 0.0f : xm(nt, nv);
+                s = __fmaf_rn(cf, xv, s);
+            }
+        }
+        return s;
+    }
+    __device__ int tile_lvl(int t) const { return meta[t].x & 0xff; }
+};
+
+__device__ void coarse_gs_pass(CoarseSmem& M, const CoarseArgs& A, int lb, int le, int color) {
+    const int total = (le - lb) * kCells;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int t = lb + (idx >> 9), v = idx & 511;
+        if ((((v >> 6) + ((v >> 3) & 7) + (v & 7)) & 1) != color) continue;
+        const float d = M.coef(3, t, v);
+        const float ax = M.neg_lap(t, v);
+        const float delta = (M.ty[t * kCells + v] & dInterior) ? __fdiv_rn(__fsub_rn(M.rhs[t * kCells + v], ax), d) : 0.0f;
+        const float xs = M.xm(t, v);
+        M.x[t * kCells + v] = A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega);
+    }
+    __syncthreads();
+}
+__device__ void coarse_gs(CoarseSmem& M, const CoarseArgs& A, int level, int iters, int order) {
+    const int lb = level == 0 ? 0 : A.l1b, le = level == 0 ? A.l1b : A.ntiles;
+    for (int it = 0; it < iters; ++it) {
+        coarse_gs_pass(M, A, lb, le, order);
+        coarse_gs_pass(M, A, lb, le, 1 - order);
+    }
+}
+__device__ void coarse_step0(CoarseSmem& M, const CoarseArgs& A) {
+    coarse_gs(M, A, 0, A.coarsest_iters / 2, 0);
+    coarse_gs(M, A, 0, A.coarsest_iters / 2, 1);
+}
+
+__global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float* X, float* RHS, float* X0) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int T = A.ntiles;
+    CoarseSmem M;
+    M.T = T;
+    M.x = reinterpret_cast<float*>(smraw);
+    M.rhs = M.x + T * kCells;
+    M.x0 = M.rhs + T * kCells;
+    M.c = M.x0 + T * kCells;
+    M.meta = reinterpret_cast<int4*>(M.c + 4 * T * kCells);
+    M.nb = reinterpret_cast<int*>(M.meta + T);
+    M.child = M.nb + 6 * T;
+    M.ty = reinterpret_cast<uint8_t*>(M.child + 8);
+    M.h[0] = voxel_size(g.h0, 0);
+    M.h[1] = voxel_size(g.h0, 1);
+    const int tot = T * kCells;
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+        M.x[i] = X[i];
+        M.rhs[i] = RHS[i];
+        M.x0[i] = X0[i];
+        M.ty[i] = g.ctype[i];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) M.c[a * tot + i] = g.plane(A.coeff_ch + a)[i];
+    }
+    for (int i = threadIdx.x; i < 6 * T; i += blockDim.x) {
+        const int nq = g.nb[8 * (i / 6) + (i % 6)];
+        M.nb[i] = (nq >= 0 && nq < T) ? nq : -1;
+    }
+    if (threadIdx.x < 8) M.child[threadIdx.x] = g.child[threadIdx.x];
+    for (int i = threadIdx.x; i < T; i += blockDim.x) M.meta[i] = g.meta[i];
+    __syncthreads();
+
+    if (A.top == 0) {
+        coarse_step0(M, A);
+    } else {
+        coarse_gs(M, A, 1, A.level_iters, 0);
+        // residual on level 1 restricted to the root (ResidualAndRestrictAMG128Kernel)
+        for (int v0 = threadIdx.x; v0 < kCells; v0 += blockDim.x) {
+            const int l0 = v0 >> 6, l1 = (v0 >> 3) & 7, l2 = v0 & 7;
+            const int ct = M.child[(l0 >> 2) * 4 + (l1 >> 2) * 2 + (l2 >> 2)];
+            if (ct < A.l1b || ct >= T) continue;
+            const int b0 = (l0 & 3) << 1, b1 = (l1 & 3) << 1, b2 = (l2 & 3) << 1;
+            float rs = 0.0f, xs = 0.0f;
+            for (int ii = 0; ii < 2; ++ii)
+                for (int jj = 0; jj < 2; ++jj)
+                    for (int kk = 0; kk < 2; ++kk) {
+                        const int cv = cell_index(b0 + ii, b1 + jj, b2 + kk);
+                        rs = __fadd_rn(rs, __fsub_rn(M.rhs[ct * kCells + cv], M.neg_lap(ct, cv)));
+                        xs = __fadd_rn(xs, M.xm(ct, cv));
+                    }
+            M.rhs[v0] = __fmul_rn(rs, A.Rr);
+            M.x[v0] = __fdiv_rn(xs, 8.0f);
+        }
+        __syncthreads();
+        // FASSaveSolutionAndUpdateSource on the root
+        for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+            if (M.ty[v] & dInterior) {
+                const float lap = M.neg_lap(0, v);
+                M.rhs[v] = __fadd_rn(M.rhs[v], lap);
+                M.x0[v] = M.x[v];
+            } else {
+                M.rhs[v] = 0.0f;
+            }
+        }
+        __syncthreads();
+        for (int r = 0; r < A.mu; ++r) coarse_step0(M, A);
+        // FASProlongateAndUpdate on level 1 (LEAF or NONLEAF tiles only)
+        const int n1 = (T - A.l1b) * kCells;
+        for (int idx = threadIdx.x; idx < n1; idx += blockDim.x) {
+            const int t = A.l1b + (idx >> 9), v = idx & 511;
+            const int4 m = M.meta[t];
+            const int pv = cell_index(parent_local(m.y, v >> 6), parent_local(m.z, (v >> 3) & 7), parent_local(m.w, v & 7));
+            const float cx = M.x[pv], cx0 = M.x0[pv];
+            const int o = t * kCells + v;
+            M.x[o] = (M.ty[o] & dInterior) ? __fmaf_rn(A.P, __fsub_rn(cx, cx0), M.x[o]) : 0.0f;
+        }
+        __syncthreads();
+        coarse_gs(M, A, 1, A.level_iters, 1);
+    }
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+        X[i] = M.x[i];
+        RHS[i] = M.rhs[i];
+        X0[i] = M.x0[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PCG on LEAF tiles
+// ---------------------------------------------------------------------------
+// AMGFullNegativeLaplacianOnLeafs (src/AMGSolver.cu:589-632) with the p.Ap dot
+// (src/AMGSolver.cu:1455) and alpha = gamma / pAp (src/AMGSolver.cu:1457) fused.
+__global__ void __launch_bounds__(128) k_leaf_apply(DevGrid g, const int* leaf, const float* P, float* AP, int coeff_ch, int fuse,
+                                                    ReduceScratch rs) {
+    __shared__ Snap S;
+    __shared__ double red[4];
+    const int t = leaf[blockIdx.x];
+    const Quad Q(t, threadIdx.x);
+    float4 xr, dg;
+    uchar4 ty;
+    load_snap(g, t, P, coeff_ch, LeafHalo{P, g.ctype}, S, Q, xr, ty, dg);
+    float4 ap;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        f4set(ap, u, t4get(ty, u) == dInterior ? snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u)) : 0.0f);
+    st4(AP + Q.base, ap);
+    if (!fuse) return;
+    const double bs = block_sum128(dot4(xr, ap), red);
+    if (threadIdx.x == 0) rs.partial[blockIdx.x] = bs;
+    if (last_block(&rs.s->counter[0])) {
+        const double tot = sum_partials(rs.partial, gridDim.x, red);
+        if (threadIdx.x == 0) {
+            PcgScalars* s = rs.s;
+            s->pAp = tot;
+            s->alpha = s->gamma / tot;
+            s->counter[0] = 0;
+        }
+    }
+}
+
+// x += alpha p, r -= alpha Ap on INTERIOR cells (src/AMGSolver.cu:1462-1485),
+// r.r (src/AMGSolver.cu:1488) and the convergence test (src/AMGSolver.cu:1487-1496)
+__global__ void __launch_bounds__(128) k_xr_update(DevGrid g, const int* leaf, float* X, float* R, const float* P, const float* AP,
+                                                   ReduceScratch rs, cudaGraphConditionalHandle loop_h,
+                                                   cudaGraphConditionalHandle body_h, int use_handles) {
+    __shared__ double red[4];
+    const int t = leaf[blockIdx.x];
+    const Quad Q(t, threadIdx.x);
+    const float alpha = (float)rs.s->alpha;
+    float4 x = ld4(X + Q.base), r = ld4(R + Q.base);
+    const float4 p = ld4(P + Q.base), ap = ld4(AP + Q.base);
+    const uchar4 ty = ldt4(g.ctype + Q.base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (t4get(ty, u) & dInterior) {
+            f4set(x, u, __fmaf_rn(alpha, f4get(p, u), f4get(x, u)));
+            f4set(r, u, __fmaf_rn(-alpha, f4get(ap, u), f4get(r, u)));
+        }
+    }
+    st4(X + Q.base, x);
+    st4(R + Q.base, r);
+    const double bs = block_sum128(dot4(r, r), red);
+    if (threadIdx.x == 0) rs.partial[blockIdx.x] = bs;
+    if (last_block(&rs.s->counter[1])) {
+        const double rr = sum_partials(rs.partial, gridDim.x, red);
+        if (threadIdx.x == 0) {
+            PcgScalars* s = rs.s;
+            s->rr = rr;
+            const int it = ++s->iter;
+            const bool bad = !isfinite(rr) || !isfinite(s->alpha);
+            const bool conv = s->sync_stride > 0 && (it % s->sync_stride) == 0 && rr < s->thr;
+            const bool done = conv || bad || it >= s->max_iters;
+            s->converged = conv;
+            s->nonfinite = bad;
+            s->done = done;
+            s->counter[1] = 0;
+            if (use_handles) {
+                cudaGraphSetConditional(loop_h, done ? 0u : 1u);
+                cudaGraphSetConditional(body_h, done ? 0u : 1u);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_dot(const int* leaf, const float* A, const float* B, int mode, double* out, ReduceScratch rs) {
+    __shared__ double red[4];
+    const int t = leaf[blockIdx.x];
+    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
+    const double bs = block_sum128(dot4(ld4(A + base), ld4(B + base)), red);
+    if (threadIdx.x == 0) rs.partial[blockIdx.x] = bs;
+    if (last_block(&rs.s->counter[2])) {
+        const double d = sum_partials(rs.partial, gridDim.x, red);
+        if (threadIdx.x == 0) {
+            PcgScalars* s = rs.s;
+            if (mode == kDotStore) *out = d;
+            else if (mode == kDotRR0) s->rr0 = d;
+            else if (mode == kDotGammaInit) s->gamma = d;
+            else {  // src/AMGSolver.cu:1513-1520
+                s->gamma_old = s->gamma;
+                s->gamma = d;
+                s->beta = d / s->gamma_old;
+            }
+            s->counter[2] = 0;
+        }
+    }
+}
+
+// p = z + beta p on INTERIOR cells (src/AMGSolver.cu:1525-1536)
+__global__ void __launch_bounds__(128) k_p_update(DevGrid g, const int* leaf, float* P, const float* Z, ReduceScratch rs) {
+    const int t = leaf[blockIdx.x];
+    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
+    const float beta = (float)rs.s->beta;
+    float4 p = ld4(P + base);
+    const float4 z = ld4(Z + base);
+    const uchar4 ty = ldt4(g.ctype + base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (t4get(ty, u) & dInterior) f4set(p, u, __fmaf_rn(beta, f4get(p, u), f4get(z, u)));
+    st4(P + base, p);
+}
+
+__global__ void k_leaf_fill(const int* leaf, float* X, float v) {
+    const size_t base = (size_t)leaf[blockIdx.x] * kCells + 4 * threadIdx.x;
+    st4(X + base, make_float4(v, v, v, v));
+}
+__global__ void k_leaf_copy(const int* leaf, float* D, const float* Sx) {
+    const size_t base = (size_t)leaf[blockIdx.x] * kCells + 4 * threadIdx.x;
+    st4(D + base, ld4(Sx + base));
+}
+
+// ReCenterLeafCells (src/PoissonGrid.cu:889-921)
+__global__ void __launch_bounds__(128) k_mean_partial(DevGrid g, const int* leaf, const float* R, ReduceScratch rs) {
+    __shared__ double red[4];
+    const size_t base = (size_t)leaf[blockIdx.x] * kCells + 4 * threadIdx.x;
+    const float4 r = ld4(R + base);
+    const uchar4 ty = ldt4(g.ctype + base);
+    float f = 0.0f;
+    int c = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const bool in = t4get(ty, u) & dInterior;
+        const float v = in ? f4get(r, u) : 0.0f;
+        f = (u == 0) ? v : __fadd_rn(f, v);
+        c += in;
+    }
+    const double bs = block_sum128((double)f, red);
+    const double bc = block_sum128((double)c, red);
+    if (threadIdx.x == 0) {
+        rs.partial[blockIdx.x] = bs;
+        rs.partial2[blockIdx.x] = bc;
+    }
+    if (last_block(&rs.s->counter[3])) {
+        const double sum = sum_partials(rs.partial, gridDim.x, red);
+        const double cnt = sum_partials(rs.partial2, gridDim.x, red);
+        if (threadIdx.x == 0) {
+            rs.s->mean = sum / cnt;
+            rs.s->count = cnt;
+            rs.s->counter[3] = 0;
+        }
+    }
+}
+__global__ void k_sub_mean(DevGrid g, const int* leaf, float* R, ReduceScratch rs) {
+    const size_t base = (size_t)leaf[blockIdx.x] * kCells + 4 * threadIdx.x;
+    const double mean = rs.s->mean;
+    float4 r = ld4(R + base);
+    const uchar4 ty = ldt4(g.ctype + base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (t4get(ty, u) & dInterior) f4set(r, u, (float)((double)f4get(r, u) - mean));
+    st4(R + base, r);
+}
+
+// threshold (epsilon |b|)^2 and the b == 0 exit (src/AMGSolver.cu:1410-1426), then the loop condition
+__global__ void k_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h) {
+    PcgScalars* s = rs.s;
+    if (s->sync_stride > 0) {
+        const double t = s->tol * s->tol * s->rr0;
+        s->thr = t > DBL_MIN ? t : DBL_MIN;
+        if (s->rr0 == 0.0) s->done = 1;
+    }
+    cudaGraphSetConditional(loop_h, (s->done == 0 && s->iter < s->max_iters) ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------
+// operator set-up
+// ---------------------------------------------------------------------------
+// GHOST cell type := parent cell type (src/AMGSolver.cu:265-274)
+__global__ void k_ghost_types(DevGrid g, int t0) {
+    const int t = t0 + blockIdx.x;
+    const int4 m = g.meta[t];
+    if (!((m.x >> 8) & dGhost)) return;
+    const int p = g.nb[8 * t + 6];
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        uint8_t ty = dDirichlet;
+        if (p >= 0)
+            ty = g.ctype[(size_t)p * kCells + cell_index(parent_local(m.y, v >> 6), parent_local(m.z, (v >> 3) & 7), parent_local(m.w, v & 7))];
+        g.ctype[(size_t)t * kCells + v] = ty;
+    }
+}
+
+// NegativeLaplacianCoeff (src/AMGSolver.cu:12-24)
+__device__ __forceinline__ bool face_valid(int tt0, int tt1, int c0, int c1) {
+    const bool both_leafs = (tt0 & dLeaf) && (tt1 & dLeaf);
+    const bool leaf_ghost = ((tt0 & dLeaf) && (tt1 & dGhost)) || ((tt0 & dGhost) && (tt1 & dLeaf));
+    const bool has_neumann = (c0 & dNeumann) || (c1 & dNeumann);
+    const bool has_interior = (c0 & dInterior) || (c1 & dInterior);
+    return (both_leafs || leaf_ghost) && !has_neumann && has_interior;
+}
+// FracInside (cirrus_cutcell/MeshCutCell.cu:262-272)
+__device__ __forceinline__ float frac_inside(float a, float b) {
+    if (a < 0.0f && b < 0.0f) return 0.0f;
+    if (a < 0.0f && b >= 0.0f) return __fdiv_rn(b, __fsub_rn(b, a));
+    if (a >= 0.0f && b < 0.0f) return __fdiv_rn(a, __fsub_rn(a, b));
+    return 1.0f;
+}
+// Fluid fraction of a face from its four corner SDFs in cyclic order: the
+// marching-squares area rule of FaceFluidRatio (MeshCutCell.cu:305-408).
+__device__ float face_fluid_ratio(const float phi[4]) {
+    int in[4], nin = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        in[i] = phi[i] < 0.0f;
+        nin += in[i];
+    }
+    float ret;
+    if (nin == 4) ret = 0.0f;
+    else if (nin == 0) ret = 1.0f;
+    else if (nin == 3) {
+        int m = 0;
+        while (in[m]) ++m;
+        ret = (float)(0.5 * (double)frac_inside(phi[m], phi[(m + 3) & 3]) * (double)frac_inside(phi[m], phi[(m + 1) & 3]));
+    } else if (nin == 1) {
+        int m = 0;
+        while (!in[m]) ++m;
+        const float e1 = (float)(1.0 - (double)frac_inside(phi[m], phi[(m + 1) & 3]));
+        const float e2 = (float)(1.0 - (double)frac_inside(phi[m], phi[(m + 3) & 3]));
+        ret = (float)(1.0 - 0.5 * (double)e1 * (double)e2);
+    } else if (in[0] == in[2]) {
+        const int f0 = in[0] ? 1 : 0, f1 = f0 + 2;
+        const double t0 = 0.5 * (double)frac_inside(phi[f0], phi[(f0 + 3) & 3]) * (double)frac_inside(phi[f0], phi[(f0 + 1) & 3]);
+        const double t1 = 0.5 * (double)frac_inside(phi[f1], phi[(f1 + 3) & 3]) * (double)frac_inside(phi[f1], phi[(f1 + 1) & 3]);
+        ret = (float)(t0 + t1);
+    } else {
+        double s = 0;
+        for (int i = 0; i < 4; ++i) {
+            if (in[i]) continue;
+            const int nbc = in[(i + 1) & 3] ? ((i + 1) & 3) : ((i + 3) & 3);
+            s += (double)frac_inside(phi[i], phi[nbc]);
+        }
+        ret = (float)(0.5 * s);
+    }
+    if (ret < 0.1f && ret != 0.0f) ret = 0.1f;
+    return ret;
+}
+// node SDF of a union of spheres at global node (gi, gj, gk) of a level with voxel size h
+__device__ __forceinline__ float node_sdf(int gi, int gj, int gk, float h, int ns, const float* sp) {
+    const float px = __fmul_rn((float)gi, h), py = __fmul_rn((float)gj, h), pz = __fmul_rn((float)gk, h);
+    float best = FLT_MAX;
+    for (int s = 0; s < ns; ++s) {
+        const float dx = __fsub_rn(px, sp[4 * s]), dy = __fsub_rn(py, sp[4 * s + 1]), dz = __fsub_rn(pz, sp[4 * s + 2]);
+        const float d = __fsub_rn(__fsqrt_rn(__fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)))), sp[4 * s + 3]);
+        best = fminf(best, d);
+    }
+    return best;
+}
+
+// Face coefficients of LEAF and GHOST cells, 0 on NONLEAF (src/AMGSolver.cu:277-315);
+// with spheres, -h times the face fluid fraction (MeshCutCell.cu:452-540).
+__global__ void k_face_coeffs(DevGrid g, int t0, int coeff_ch, int ns, const float* sp) {
+    const int t = t0 + blockIdx.x;
+    const int4 m = g.meta[t];
+    const int tt0 = (m.x >> 8) & 0xff, level = m.x & 0xff;
+    const float h = voxel_size(g.h0, level);
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        const int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+        const int stride[3] = {64, 8, 1};
+        const int c0 = g.ctype[(size_t)t * kCells + v];
+        for (int a = 0; a < 3; ++a) {
+            float c = 0.0f;
+            if (tt0 != dNonLeaf) {
+                int q = t, nv = v - stride[a];
+                if (l[a] == 0) {
+                    q = g.nb[8 * t + a];
+                    nv = v + 7 * stride[a];
+                }
+                const int tt1 = q < 0 ? tt0 : tile_type(g, q);
+                const int c1 = q < 0 ? dDirichlet : g.ctype[(size_t)q * kCells + nv];
+                if (face_valid(tt0, tt1, c0, c1)) {
+                    if (ns == 0) c = -h;
+                    else {
+                        // corners of the negative face in cyclic order (FaceCornerSDFs, MeshCutCell.cu:274-303)
+                        const int gi = m.y * 8 + l[0], gj = m.z * 8 + l[1], gk = m.w * 8 + l[2];
+                        float phi[4];
+                        if (a == 0) {
+                            phi[0] = node_sdf(gi, gj, gk, h, ns, sp); phi[1] = node_sdf(gi, gj, gk + 1, h, ns, sp);
+                            phi[2] = node_sdf(gi, gj + 1, gk + 1, h, ns, sp); phi[3] = node_sdf(gi, gj + 1, gk, h, ns, sp);
+                        } else if (a == 1) {
+                            phi[0] = node_sdf(gi, gj, gk, h, ns, sp); phi[1] = node_sdf(gi, gj, gk + 1, h, ns, sp);
+                            phi[2] = node_sdf(gi + 1, gj, gk + 1, h, ns, sp); phi[3] = node_sdf(gi + 1, gj, gk, h, ns, sp);
+                        } else {
+                            phi[0] = node_sdf(gi, gj, gk, h, ns, sp); phi[1] = node_sdf(gi, gj + 1, gk, h, ns, sp);
+                            phi[2] = node_sdf(gi + 1, gj + 1, gk, h, ns, sp); phi[3] = node_sdf(gi + 1, gj, gk, h, ns, sp);
+                        }
+                        c = -__fmul_rn(h, face_fluid_ratio(phi));
+                    }
+                }
+            }
+            g.plane(coeff_ch + a)[(size_t)t * kCells + v] = c;
+        }
+    }
+}
+
+// LEAF cells with all eight corners inside the solid become NEUMANN (MeshCutCell.cu:421-429)
+__global__ void k_cutcell_neumann(DevGrid g, const int* leaf, int ns, const float* sp) {
+    const int t = leaf[blockIdx.x];
+    const int4 m = g.meta[t];
+    const float h = voxel_size(g.h0, m.x & 0xff);
+    const float eps = __fmul_rn(h, 1e-3f);
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        const int gi = m.y * 8 + (v >> 6), gj = m.z * 8 + ((v >> 3) & 7), gk = m.w * 8 + (v & 7);
+        int cnt = 0;
+        for (int d = 0; d < 8; ++d)
+            if (__fsub_rn(node_sdf(gi + (d >> 2), gj + ((d >> 1) & 1), gk + (d & 1), h, ns, sp), eps) < 0.0f) ++cnt;
+        if (cnt == 8) g.ctype[(size_t)t * kCells + v] = dNeumann;
+    }
+}
+
+// coarse face += R * (sum of the 4 fine faces) (CoarsenOffDiagCoefficientsOneStepKernel, src/AMGSolver.cu:27-78)
+__global__ void k_coarsen_offdiag(DevGrid g, int t0, int coeff_ch, float R) {
+    const int t = t0 + blockIdx.x;
+    const int b = threadIdx.x;  // 64 threads: one 2x2x2 block each
+    const int p = g.nb[8 * t + 6];
+    if (p < 0) return;
+    const int4 m = g.meta[t];
+    const int f[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
+    const size_t pv = (size_t)p * kCells + cell_index(parent_local(m.y, f[0]), parent_local(m.z, f[1]), parent_local(m.w, f[2]));
+    for (int a = 0; a < 3; ++a) {
+        const float* C = g.plane(coeff_ch + a) + (size_t)t * kCells;
+        float s = 0.0f;
+        for (int jj = 0; jj < 2; ++jj)
+            for (int kk = 0; kk < 2; ++kk) {
+                int o[3];
+                o[a] = 0;
+                o[(a + 1) % 3] = jj;
+                o[(a + 2) % 3] = kk;
+                s = __fadd_rn(s, C[cell_index(f[0] + o[0], f[1] + o[1], f[2] + o[2])]);
+            }
+        float* cc = g.plane(coeff_ch + a) + pv;
+        *cc = __fmaf_rn(s, R, *cc);
+    }
+}
+
+// diagonal coefficients and NONLEAF cell types (src/AMGSolver.cu:124-253), one level
+__global__ void k_diag(DevGrid g, int t0, int coeff_ch, float R) {
+    const int t = t0 + blockIdx.x;
+    const int4 m = g.meta[t];
+    const int tt = (m.x >> 8) & 0xff;
+    const float h = voxel_size(g.h0, m.x & 0xff);
+    float* D = g.plane(coeff_ch + 3) + (size_t)t * kCells;
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        const int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+        const int stride[3] = {64, 8, 1};
+        if (tt & (dLeaf | dGhost)) {
+            float d = 0.0f;
+            if (g.ctype[(size_t)t * kCells + v] & dInterior) {
+                for (int a = 0; a < 3; ++a) {
+                    d = __fsub_rn(d, g.plane(coeff_ch + a)[(size_t)t * kCells + v]);
+                    int q = t, nv = v + stride[a];
+                    if (l[a] == 7) {
+                        q = g.nb[8 * t + 3 + a];
+                        nv = v - 7 * stride[a];
+                    }
+                    const float c1 = q < 0 ? -h : g.plane(coeff_ch + a)[(size_t)q * kCells + nv];
+                    d = __fsub_rn(d, c1);
+                }
+            }
+            D[v] = d;
+        } else {
+            const int q = g.child[8 * t + (l[0] >> 2) * 4 + (l[1] >> 2) * 2 + (l[2] >> 2)];
+            int ct[8];
+            float off[3][8];
+            float dsum = 0.0f;
+            int interior_cnt = 0;
+            for (int ci = 0; ci < 8; ++ci) {
+                if (q >= 0) {
+                    const size_t cv = (size_t)q * kCells + cell_index(((l[0] & 3) << 1) + (ci >> 2), ((l[1] & 3) << 1) + ((ci >> 1) & 1),
+                                                                       ((l[2] & 3) << 1) + (ci & 1));
+                    dsum = __fadd_rn(dsum, g.plane(coeff_ch + 3)[cv]);
+                    ct[ci] = g.ctype[cv];
+                    interior_cnt += (ct[ci] == dInterior);
+                    for (int a = 0; a < 3; ++a) off[a][ci] = g.plane(coeff_ch + a)[cv];
+                } else {
+                    ct[ci] = dDirichlet;
+                    for (int a = 0; a < 3; ++a) off[a][ci] = 0.0f;
+                }
+            }
+            // internal child faces, each counted from both sides of the pair
+            for (int ci = 0; ci < 8; ++ci) {
+                const int x = ci >> 2, y = (ci >> 1) & 1, z = ci & 1;
+                if (ct[0 * 4 + y * 2 + z] == dInterior && ct[1 * 4 + y * 2 + z] == dInterior) dsum = __fadd_rn(dsum, off[0][4 + y * 2 + z]);
+                if (ct[x * 4 + 0 * 2 + z] == dInterior && ct[x * 4 + 1 * 2 + z] == dInterior) dsum = __fadd_rn(dsum, off[1][x * 4 + 2 + z]);
+                if (ct[x * 4 + y * 2 + 0] == dInterior && ct[x * 4 + y * 2 + 1] == dInterior) dsum = __fadd_rn(dsum, off[2][x * 4 + y * 2 + 1]);
+            }
+            g.ctype[(size_t)t * kCells + v] = interior_cnt > 0 ? dInterior : dDirichlet;
+            D[v] = __fmul_rn(dsum, R);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// right-hand side: face velocity of Fourier modes and its divergence
+// ---------------------------------------------------------------------------
+__global__ void k_face_velocity(DevGrid g, const int* leaf, int u_ch, int nm, const double* modes) {
+    const int t = leaf[blockIdx.x];
+    const int4 m = g.meta[t];
+    const double h = (double)voxel_size(g.h0, m.x & 0xff);
+    const double two_pi = 6.283185307179586;
+    const double* kv = modes;
+    const double* amp = modes + 3 * nm;
+    const double* ph = modes + 6 * nm;
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        const int gc[3] = {m.y * 8 + (v >> 6), m.z * 8 + ((v >> 3) & 7), m.w * 8 + (v & 7)};
+        for (int a = 0; a < 3; ++a) {
+            double p[3];
+            for (int d = 0; d < 3; ++d) p[d] = ((double)gc[d] + (d == a ? 0.0 : 0.5)) * h;
+            double u = 0;
+            for (int q = 0; q < nm; ++q) {
+                const double arg = two_pi * (kv[3 * q] * p[0] + kv[3 * q + 1] * p[1] + kv[3 * q + 2] * p[2]) + ph[q];
+                u += amp[3 * q + a] * sin(arg);
+            }
+            g.plane(u_ch + a)[(size_t)t * kCells + v] = (float)u;
+        }
+    }
+}
+// GHOST value := parent value (PropagateToChildren, src/PoissonGrid.cu:377-405)
+__global__ void k_propagate_ghost(DevGrid g, int t0, int ch) {
+    const int t = t0 + blockIdx.x;
+    const int4 m = g.meta[t];
+    if (!((m.x >> 8) & dGhost)) return;
+    const int p = g.nb[8 * t + 6];
+    float* X = g.plane(ch);
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        if (!(g.ctype[(size_t)t * kCells + v] & (dInterior | dDirichlet | dNeumann))) continue;
+        float val = 0.0f;
+        if (p >= 0) {
+            const size_t o = (size_t)p * kCells + cell_index(parent_local(m.y, v >> 6), parent_local(m.z, (v >> 3) & 7), parent_local(m.w, v & 7));
+            if (g.ctype[o] & (dInterior | dDirichlet | dNeumann)) val = X[o];
+        }
+        X[(size_t)t * kCells + v] = val;
+    }
+}
+// coarse face := 1/4 sum of the 4 fine faces of LEAF tiles (AccumulateFacesToParentsOneStepKernel, src/PoissonGrid.cu:523-566)
+__global__ void k_accumulate_faces(DevGrid g, const int* leaf, int u_ch) {
+    const int t = leaf[blockIdx.x];
+    const int b = threadIdx.x;
+    const int p = g.nb[8 * t + 6];
+    if (p < 0) return;
+    const int4 m = g.meta[t];
+    const int f[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
+    const size_t pv = (size_t)p * kCells + cell_index(parent_local(m.y, f[0]), parent_local(m.z, f[1]), parent_local(m.w, f[2]));
+    for (int a = 0; a < 3; ++a) {
+        const float* U = g.plane(u_ch + a) + (size_t)t * kCells;
+        float s = 0.0f;
+        for (int jj = 0; jj < 2; ++jj)
+            for (int kk = 0; kk < 2; ++kk) {
+                int o[3];
+                o[a] = 0;
+                o[(a + 1) % 3] = jj;
+                o[(a + 2) % 3] = kk;
+                const int v = cell_index(f[0] + o[0], f[1] + o[1], f[2] + o[2]);
+                s = __fadd_rn(s, (g.ctype[(size_t)t * kCells + v] & (dInterior | dDirichlet | dNeumann)) ? U[v] : 0.0f);
+            }
+        g.plane(u_ch + a)[pv] = __fmul_rn(s, 0.25f);
+    }
+}
+// AMGVolumeWeightedDivergenceOnLeafs (src/AMGSolver.cu:797-834)
+__global__ void k_divergence(DevGrid g, const int* leaf, int u_ch, int coeff_ch, int out_ch) {
+    const int t = leaf[blockIdx.x];
+    const int4 m = g.meta[t];
+    const float h = voxel_size(g.h0, m.x & 0xff);
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
+        const int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+        const int stride[3] = {64, 8, 1};
+        float sum = 0.0f;
+        for (int a = 0; a < 3; ++a) {
+            const size_t o = (size_t)t * kCells + v;
+            sum = __fmaf_rn(__fmul_rn(g.plane(u_ch + a)[o], g.plane(coeff_ch + a)[o]), h, sum);
+            int q = t, nv = v + stride[a];
+            if (l[a] == 7) {
+                q = g.nb[8 * t + 3 + a];
+                nv = v - 7 * stride[a];
+            }
+            float u1 = 0.0f, c1 = 0.0f;
+            if (q >= 0) {
+                u1 = g.plane(u_ch + a)[(size_t)q * kCells + nv];
+                c1 = g.plane(coeff_ch + a)[(size_t)q * kCells + nv];
+            }
+            sum = __fmaf_rn(__fmul_rn(-u1, c1), h, sum);
+        }
+        g.plane(out_ch)[(size_t)t * kCells + v] = (g.ctype[(size_t)t * kCells + v] & dInterior) ? sum : 0.0f;
+    }
+}
+
+__global__ void k_remap(const float* src, float* dst, const int* old_of_new, int n_new, int n_old) {
+    const int t = blockIdx.x, c = blockIdx.y;
+    const int o = old_of_new[t];
+    const size_t dbase = ((size_t)c * n_new + t) * kCells;
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x)
+        dst[dbase + v] = (o >= 0) ? src[((size_t)c * n_old + o) * kCells + v] : 0.0f;
+}
+__global__ void k_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new) {
+    const int t = blockIdx.x;
+    const int o = old_of_new[t];
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x) dst[(size_t)t * kCells + v] = (o >= 0) ? src[(size_t)o * kCells + v] : 0;
+}
+__global__ void k_fill(float* p, size_t n, float v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_count_bad_diag(DevGrid g, int t0, int coeff_ch, int* out) {
+    const int t = t0 + blockIdx.x;
+    const float* D = g.plane(coeff_ch + 3) + (size_t)t * kCells;
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x)
+        if ((g.ctype[(size_t)t * kCells + v] & dInterior) && !(D[v] != 0.0f)) atomicAdd(out, 1);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st) {
+    if (nt <= 0) return;
+    const float om = (float)omega;
+    if ((double)om == omega) k_gs<true><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
+    else k_gs<false><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
+}
+void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st) {
+    if (nt > 0) k_restrict<<<nt, 128, 0, st>>>(g, t0, X, RHS, coeff_ch, Rr);
+}
+void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st) {
+    if (nt > 0) k_fas_save<<<nt, 128, 0, st>>>(g, t0, X, RHS, X0, coeff_ch);
+}
+void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st) {
+    if (nt > 0) k_prolong<<<nt, 128, 0, st>>>(g, t0, X, X0, P);
+}
+size_t coarse_step_smem_bytes(int ntiles) {
+    return (size_t)ntiles * kCells * (7 * sizeof(float) + 1) + sizeof(int) * (6 * ntiles + 8) + sizeof(int4) * ntiles + 16;
+}
+void launch_coarse_step(const DevGrid& g, int top, int ntiles, int level1_begin, float* X, float* RHS, float* X0, int coeff_ch, int mu,
+                        int level_iters, int coarsest_iters, double omega, float Rr, float P, cudaStream_t st) {
+    CoarseArgs A;
+    A.top = top;
+    A.ntiles = ntiles;
+    A.l1b = level1_begin;
+    A.coeff_ch = coeff_ch;
+    A.mu = mu;
+    A.level_iters = level_iters;
+    A.coarsest_iters = coarsest_iters;
+    A.om = (float)omega;
+    A.exact = ((double)A.om == omega);
+    A.omega = omega;
+    A.Rr = Rr;
+    A.P = P;
+    const size_t smem = coarse_step_smem_bytes(ntiles);
+    k_coarse<<<1, 1024, smem, st>>>(g, A, X, RHS, X0);
+}
+void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
+                       ReduceScratch rs, cudaStream_t st) {
+    if (nleaf > 0) k_leaf_apply<<<nleaf, 128, 0, st>>>(g, leaf, P, AP, coeff_ch, fuse_alpha ? 1 : 0, rs);
+}
+void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,
+                      ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool use_handles,
+                      cudaStream_t st) {
+    if (nleaf > 0) k_xr_update<<<nleaf, 128, 0, st>>>(g, leaf, X, R, P, AP, rs, loop_h, body_h, use_handles ? 1 : 0);
+}
+void launch_dot(const DevGrid& g, const int* leaf, int nleaf, const float* A, const float* B, int mode, double* out, ReduceScratch rs,
+                cudaStream_t st) {
+    (void)g;
+    if (nleaf > 0) k_dot<<<nleaf, 128, 0, st>>>(leaf, A, B, mode, out, rs);
+}
+void launch_p_update(const DevGrid& g, const int* leaf, int nleaf, float* P, const float* Z, ReduceScratch rs, cudaStream_t st) {
+    if (nleaf > 0) k_p_update<<<nleaf, 128, 0, st>>>(g, leaf, P, Z, rs);
+}
+void launch_leaf_fill(const DevGrid& g, const int* leaf, int nleaf, float* X, float value, cudaStream_t st) {
+    (void)g;
+    if (nleaf > 0) k_leaf_fill<<<nleaf, 128, 0, st>>>(leaf, X, value);
+}
+void launch_leaf_copy(const DevGrid& g, const int* leaf, int nleaf, float* dst, const float* src, cudaStream_t st) {
+    (void)g;
+    if (nleaf > 0) k_leaf_copy<<<nleaf, 128, 0, st>>>(leaf, dst, src);
+}
+void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, ReduceScratch rs, cudaStream_t st) {
+    if (nleaf <= 0) return;
+    k_mean_partial<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
+    k_sub_mean<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
+}
+void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st) { k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h); }
+void init_kernel_attributes() { cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); }
+
+void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st) {
+    if (nt > 0) k_ghost_types<<<nt, 128, 0, st>>>(g, t0);
+}
+void launch_face_coeffs(const DevGrid& g, int t0, int nt, int coeff_ch, int ns, const float* sp, cudaStream_t st) {
+    if (nt > 0) k_face_coeffs<<<nt, 128, 0, st>>>(g, t0, coeff_ch, ns, sp);
+}
+void launch_cutcell_neumann(const DevGrid& g, const int* leaf, int nleaf, int ns, const float* sp, cudaStream_t st) {
+    if (nleaf > 0) k_cutcell_neumann<<<nleaf, 128, 0, st>>>(g, leaf, ns, sp);
+}
+void launch_coarsen_offdiag(const DevGrid& g, int t0, int nt, int coeff_ch, float R, cudaStream_t st) {
+    if (nt > 0) k_coarsen_offdiag<<<nt, 64, 0, st>>>(g, t0, coeff_ch, R);
+}
+void launch_diag(const DevGrid& g, int t0, int nt, int coeff_ch, float R, cudaStream_t st) {
+    if (nt > 0) k_diag<<<nt, 128, 0, st>>>(g, t0, coeff_ch, R);
+}
+void launch_face_velocity(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int nm, const double* modes, cudaStream_t st) {
+    if (nleaf > 0) k_face_velocity<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, nm, modes);
+}
+void launch_propagate_ghost(const DevGrid& g, int t0, int nt, int ch, cudaStream_t st) {
+    if (nt > 0) k_propagate_ghost<<<nt, 128, 0, st>>>(g, t0, ch);
+}
+void launch_accumulate_faces(const DevGrid& g, const int* leaf, int nleaf, int u_ch, cudaStream_t st) {
+    if (nleaf > 0) k_accumulate_faces<<<nleaf, 64, 0, st>>>(g, leaf, u_ch);
+}
+void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int coeff_ch, int out_ch, cudaStream_t st) {
+    if (nleaf > 0) k_divergence<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, coeff_ch, out_ch);
+}
+void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st) {
+    if (n_new > 0 && nch > 0) k_remap<<<dim3(n_new, nch), 128, 0, st>>>(src, dst, old_of_new, n_new, n_old);
+}
+void launch_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new, int n_new, cudaStream_t st) {
+    if (n_new > 0) k_remap_types<<<n_new, 128, 0, st>>>(src, dst, old_of_new);
+}
+void launch_fill(float* p, size_t n, float v, cudaStream_t st) {
+    if (n > 0) k_fill<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p, n, v);
+}
+void launch_count_bad_diag(const DevGrid& g, int t0, int nt, int coeff_ch, int* out, cudaStream_t st) {
+    if (nt > 0) k_count_bad_diag<<<nt, 128, 0, st>>>(g, t0, coeff_ch, out);
+}
+
+}  // namespace cmg

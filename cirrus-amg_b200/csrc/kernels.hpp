@@ -1,0 +1,68 @@
+// Host launchers of the device kernels (kernels.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace cmg {
+
+// device-resident scalars of one PCG solve (the reference keeps them in a
+// thrust::device_vector<double>(7), src/AMGSolver.h:309-318)
+struct PcgScalars {
+    double gamma, gamma_old, beta, alpha, pAp, rr, rr0, thr, tol;
+    double mean, count;
+    int iter, done, converged, nonfinite;
+    int max_iters, sync_stride;
+    unsigned int counter[8];
+};
+
+struct ReduceScratch {
+    double* partial;  // one double per tile (LEAF tiles at most)
+    double* partial2;
+    PcgScalars* s;
+};
+
+// --- multigrid ---
+void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
+void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float R_restrict, cudaStream_t st);
+void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st);
+void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st);
+// Whole FASMuCycleStep of level `top` (0 or 1) in one thread block, the
+// coarse levels resident in shared memory.  ntiles = tiles of levels 0..top.
+void launch_coarse_step(const DevGrid& g, int top, int ntiles, int level1_begin, float* X, float* RHS, float* X0, int coeff_ch,
+                        int mu, int level_iters, int coarsest_iters, double omega, float R_restrict, float P, cudaStream_t st);
+size_t coarse_step_smem_bytes(int ntiles);
+
+// --- PCG on LEAF tiles (tile list) ---
+enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3 };
+void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
+                       ReduceScratch rs, cudaStream_t st);
+void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,
+                      ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool use_handles,
+                      cudaStream_t st);
+void launch_dot(const DevGrid& g, const int* leaf, int nleaf, const float* A, const float* B, int mode, double* out,
+                ReduceScratch rs, cudaStream_t st);
+void launch_p_update(const DevGrid& g, const int* leaf, int nleaf, float* P, const float* Z, ReduceScratch rs, cudaStream_t st);
+void launch_leaf_fill(const DevGrid& g, const int* leaf, int nleaf, float* X, float value, cudaStream_t st);
+void launch_leaf_copy(const DevGrid& g, const int* leaf, int nleaf, float* dst, const float* src, cudaStream_t st);
+void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, ReduceScratch rs, cudaStream_t st);
+void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st);
+void init_kernel_attributes();
+
+// --- operator set-up and right-hand side ---
+void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st);
+void launch_face_coeffs(const DevGrid& g, int t0, int nt, int coeff_ch, int nspheres, const float* spheres_dev, cudaStream_t st);
+void launch_cutcell_neumann(const DevGrid& g, const int* leaf, int nleaf, int nspheres, const float* spheres_dev, cudaStream_t st);
+void launch_coarsen_offdiag(const DevGrid& g, int t0, int nt, int coeff_ch, float R, cudaStream_t st);
+void launch_diag(const DevGrid& g, int t0, int nt, int coeff_ch, float R, cudaStream_t st);
+void launch_face_velocity(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int nmodes, const double* modes_dev, cudaStream_t st);
+void launch_propagate_ghost(const DevGrid& g, int t0, int nt, int ch, cudaStream_t st);
+void launch_accumulate_faces(const DevGrid& g, const int* leaf, int nleaf, int u_ch, cudaStream_t st);
+void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int coeff_ch, int out_ch, cudaStream_t st);
+void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st);
+void launch_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new, int n_new, cudaStream_t st);
+void launch_fill(float* p, size_t n, float v, cudaStream_t st);
+void launch_count_bad_diag(const DevGrid& g, int t0, int nt, int coeff_ch, int* out, cudaStream_t st);
+
+}  // namespace cmg

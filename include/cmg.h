@@ -1,0 +1,152 @@
+/*
+ * cmg.h -- C ABI of the B200 octree multigrid pressure-Poisson solver.
+ *
+ * Plain pointers, sizes and status codes only; no C++ or torch types cross
+ * this boundary.  Each entry point names the Cirrus-amg interface it stands
+ * in for (file:line relative to that project's root).  Every function
+ * returns CMG_OK (0) or a CMG_ERR_* code; cmg_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Object model (the reference's, re-laid-out for the GPU):
+ *   cmg_grid   <-> HADeviceGrid<PoissonTile<float,15>> (src/HAGrid.h:357):
+ *                  an octree of 8^3-cell tiles, LEAF / NONLEAF / GHOST tiles
+ *                  per level, num_channels float channels per cell and one
+ *                  uint8 cell type per cell.  On the device every channel is
+ *                  a plane of num_tiles*512 floats, tile-major, cell index
+ *                  i*64 + j*8 + k inside a tile (src/HAAccessor.h:32).  Tiles
+ *                  are ordered by (level, tile type, Morton code).
+ *   cmg_amg_solver <-> AMGSolver (src/AMGSolver.h:19-75).
+ *
+ * Channel conventions of the solve follow PoissonTile (src/PoissonTile.h:13-18):
+ * x = 0, b = r = 1 (overwritten by the residual), p = 2, Ap = 3, z = 4.
+ */
+#ifndef CMG_H
+#define CMG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* tile types (src/HATileInfo.h:10) */
+#define CMG_LEAF 1
+#define CMG_NONLEAF 2
+#define CMG_GHOST 4
+/* cell types (src/PoissonTile.h:7) */
+#define CMG_DIRICHLET 1
+#define CMG_INTERIOR 2
+#define CMG_NEUMANN 4
+
+/* status codes */
+#define CMG_OK 0
+#define CMG_ERR_INVALID 1    /* bad argument (channel, level, pointer, size) */
+#define CMG_ERR_CUDA 2       /* a CUDA call failed; see cmg_last_error() */
+#define CMG_ERR_STATE 3      /* call order: e.g. solve before prepare */
+#define CMG_ERR_TOPOLOGY 4   /* octree not 2:1 face-balanced where the operator needs it */
+#define CMG_ERR_NONFINITE 5  /* a NaN/Inf reached a reduction */
+
+/* built-in refinement targets (tests/TestGrids.cuh:33-142 and the
+ * adaptive-sphere workloads); params[0] = min level, params[1] = max level. */
+#define CMG_CASE_UNIFORM 0
+#define CMG_CASE_CENTER_POINT 1
+#define CMG_CASE_SPHERE_EMPTY 2
+#define CMG_CASE_SPHERE_SOLID 3
+#define CMG_CASE_STAR_EMPTY 4
+#define CMG_CASE_STAR_SOLID 5
+#define CMG_CASE_SHELL 6        /* + mid level, centre xyz, radius, fine band, mid band */
+#define CMG_CASE_MULTI_SPHERE 7 /* + band, count, then (x, y, z, r) per sphere */
+
+typedef struct cmg_grid cmg_grid;
+typedef struct cmg_amg_solver cmg_amg_solver;
+
+/* Refinement target of a tile: the level it should reach (the device lambda
+ * passed to HADeviceGrid::iterativeRefine, src/HAGrid.h:1173). */
+typedef int (*cmg_level_target_fn)(void* user, int level, int i, int j, int k);
+
+const char* cmg_last_error(void);
+int cmg_version(void);
+
+/* ---- grid: HADeviceGrid ------------------------------------------------ */
+/* HADeviceGrid(h0, levels_log2_hash) (src/HAGrid.h:416); num_levels = number
+ * of hash levels there, num_channels = PoissonTile NUMCHNLS (15). */
+int cmg_grid_create(float h0, int num_levels, int num_channels, cmg_grid** out);
+int cmg_grid_destroy(cmg_grid* g);
+/* setTileHost (src/HAGrid.h:526): add a tile or change its type. */
+int cmg_grid_set_tile(cmg_grid* g, int level, int i, int j, int k, int tile_type);
+/* rebuild (src/HAGrid.h:892): spawn GHOST tiles, order tiles, upload tables.
+ * Channel data of tiles that survive is kept; new tiles start at zero. */
+int cmg_grid_rebuild(cmg_grid* g);
+/* iterativeRefine (src/HAGrid.h:1173) with a host callback or a built-in case. */
+int cmg_grid_iterative_refine(cmg_grid* g, cmg_level_target_fn fn, void* user, int* steps);
+int cmg_grid_refine_case(cmg_grid* g, int case_id, const double* params, int nparams, int* steps);
+/* numTotalTiles / mMaxLevel (src/HAGrid.h:504, 366) */
+int cmg_grid_info(cmg_grid* g, int* num_tiles, int* max_level, int* num_leaf_tiles);
+/* tile list in device order: level[n], ijk[3n], type[n] (host buffers) */
+int cmg_grid_tiles(cmg_grid* g, int* level, int* ijk, uint8_t* type);
+/* device tables: nb[8n] (-x,-y,-z,+x,+y,+z, parent, -1), child[8n] (dx*4+dy*2+dz) */
+int cmg_grid_tables(cmg_grid* g, int* nb, int* child);
+/* device pointers of channel planes / the cell-type plane (num_tiles*512 each) */
+int cmg_grid_channel_ptr(cmg_grid* g, int ch, float** dev_ptr);
+int cmg_grid_cell_type_ptr(cmg_grid* g, uint8_t** dev_ptr);
+/* host <-> device copies of a whole channel plane or the cell types */
+int cmg_grid_upload_channel(cmg_grid* g, int ch, const float* host, size_t count);
+int cmg_grid_download_channel(cmg_grid* g, int ch, float* host, size_t count);
+int cmg_grid_upload_cell_types(cmg_grid* g, const uint8_t* host, size_t count);
+int cmg_grid_download_cell_types(cmg_grid* g, uint8_t* host, size_t count);
+int cmg_grid_fill_channel(cmg_grid* g, int ch, float value);
+/* CreateTestGrid cell types of LEAF tiles (tests/TestGrids.cuh:161-167) */
+int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams);
+/* stream used by every later call on this grid (NULL = legacy default) */
+int cmg_grid_set_stream(cmg_grid* g, void* cuda_stream);
+int cmg_grid_synchronize(cmg_grid* g);
+
+/* ---- operator set-up: AMGSolver.cu / MeshCutCell.cu ------------------- */
+/* CoarsenTypesAndAMGCoeffs (src/AMGSolver.cu:256-318), the body of
+ * AMGSolver::prepareTypesAndCoeffs (src/AMGSolver.cu:1394). */
+int cmg_amg_prepare_types_and_coeffs(cmg_grid* g, int coeff_ch, float R_matrix);
+/* PrepareLaplacianSystemFromLeafAndGhostCellTypesAndFaceCoeffs (src/AMGSolver.cu:89) */
+int cmg_amg_prepare_system(cmg_grid* g, int coeff_ch, float R_matrix);
+/* CreateAMGLaplacianSystemWithSolidCutOnNodeSDF (cirrus_cutcell/MeshCutCell.cu:416)
+ * with the node SDF of a union of spheres (x, y, z, r per sphere). */
+int cmg_amg_cutcell_sphere_coeffs(cmg_grid* g, int coeff_ch, float R_matrix, int nspheres, const float* spheres);
+/* face velocity u = sum_m amp_m sin(2 pi k_m . x + phase_m) on LEAF faces (k[3m], amp[3m], phase[m]) */
+int cmg_amg_face_velocity_fourier(cmg_grid* g, int u_ch, int nmodes, const double* k, const double* amp, const double* phase);
+/* AMGVolumeWeightedDivergenceOnLeafs (src/AMGSolver.cu:790) */
+int cmg_amg_divergence(cmg_grid* g, int u_ch, int coeff_ch, int out_ch);
+/* AMGFullNegativeLaplacianOnLeafs (src/AMGSolver.cu:589): Ax on LEAF tiles */
+int cmg_amg_full_neg_lap(cmg_grid* g, int x_ch, int coeff_ch, int ax_ch);
+/* Dot over LEAF tiles (src/PoissonGrid.cu:203) */
+int cmg_amg_dot(cmg_grid* g, int a_ch, int b_ch, double* out);
+
+/* ---- solver: AMGSolver ------------------------------------------------- */
+/* AMGSolver(coeff_channel, R_matrix, R_restrict, P) (src/AMGSolver.h:309);
+ * omega = 1.5, mu = 2 as there (src/AMGSolver.h:306-307). */
+int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float P, cmg_amg_solver** out);
+int cmg_amg_solver_destroy(cmg_amg_solver* s);
+/* public fields omega / mu_cycle_repeat_times (src/AMGSolver.h:306-307) */
+int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
+/* AMGSolver::solve (src/AMGSolver.cu:1399): solves -lap x = b, b read from
+ * channel 1 and overwritten by the residual, x written to channel 0.
+ * iters/rel_res are the reference's (num_iters, relative_residual), with
+ * rel_res = -1 when sync_stride <= 0.  The PCG loop runs on the device as a
+ * CUDA-graph while-loop; no host synchronisation happens inside it. */
+int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double relative_tolerance,
+                  int level_iters, int coarsest_iters, int sync_stride, int is_pure_neumann,
+                  int* iters, double* rel_res);
+/* The same solve with host buffers: b (num_tiles*512 floats, device order)
+ * is copied in, x copied out; the copies are part of the call. */
+int cmg_amg_solve_host(cmg_amg_solver* s, cmg_grid* g, const float* b_host, float* x_host, size_t count,
+                       int max_iters, double relative_tolerance, int level_iters, int coarsest_iters,
+                       int sync_stride, int is_pure_neumann, int* iters, double* rel_res);
+/* GaussSeidelAMG (src/AMGSolver.cu:887) on one level */
+int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
+/* AMGSolver::FASMuCycle (src/AMGSolver.cu:1279) */
+int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters);
+/* device time of the last cmg_amg_solve, milliseconds (CUDA events) */
+int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

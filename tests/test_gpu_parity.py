@@ -1,0 +1,167 @@
+"""Parity of the CUDA product (through the C ABI) with the CPU oracle.
+
+Tolerances: the operator set-up is integer/elementwise float work and must be
+bit-identical; single stencil passes follow the same float operation order
+and are compared at 1e-6 relative to the field's magnitude; whole
+multigrid cycles and solves are FP32 iterations and are compared at 1e-5
+relative L2, with PCG iteration counts within +-1 (the reference's
+tolerance for this path), against both the oracle's float run and the FP64
+CSR solution of the same operator.
+"""
+import numpy as np
+import pytest
+
+import cmg
+from oracle import oracle as O
+from workloads import COEFF, U, setup_uniform, setup_shell, shell_params, build_product, build_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def leaf_mask(G):
+    return G.tiles()[2] == cmg.LEAF
+
+
+def fp64_solution(g, b_leaf_tiles, method):
+    rp, ci, va, rt, rc = g.assemble(COEFF)
+    bb = b_leaf_tiles[rt, rc].astype(np.float64)
+    x, its, rel = O.csr_solve(rp, ci, va, bb, 1e-12, 50000, method)
+    assert rel < 1e-10
+    return x, rt, rc
+
+
+def test_uniform_coefficients_bitwise():
+    G, g, solver, b = setup_uniform(3)
+    assert np.array_equal(G.download_cell_types(), g.cell_types())
+    for a in range(4):
+        assert np.array_equal(G.download(COEFF + a), g.channel(COEFF + a)), f"coefficient channel {a}"
+
+
+def test_uniform_laplacian_matches_oracle():
+    G, g, solver, b = setup_uniform(3)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((G.num_tiles, 512)).astype(np.float32)
+    G.upload(2, x)
+    g.channel(2)[:] = x
+    G.full_neg_lap(2, COEFF, 3)
+    g.full_neg_lap_leafs(2, COEFF, 3)
+    m = leaf_mask(G)
+    ax, axo = G.download(3)[m], g.channel(3)[m]
+    assert np.max(np.abs(ax - axo)) <= 1e-6 * np.max(np.abs(axo))
+
+
+@pytest.mark.parametrize("level", [3, 2, 1, 0])
+def test_uniform_gauss_seidel_matches_oracle(level):
+    G, g, solver, b = setup_uniform(3)
+    rng = np.random.default_rng(7 + level)
+    x = rng.standard_normal((G.num_tiles, 512)).astype(np.float32)
+    r = rng.standard_normal((G.num_tiles, 512)).astype(np.float32)
+    for ch, v in ((4, x), (1, r)):
+        G.upload(ch, v)
+        g.channel(ch)[:] = v
+    solver.gauss_seidel(G, 2, 0, level, 4, 1)
+    g.gauss_seidel(2, 0, level, 4, COEFF, 1, 1.5)
+    lv = G.tiles()[0]
+    sel = lv == level
+    xd, xo = G.download(4)[sel], g.channel(4)[sel]
+    assert np.max(np.abs(xd - xo)) <= 1e-6 * np.max(np.abs(xo))
+
+
+def test_uniform_mu_cycle_matches_oracle():
+    G, g, solver, b = setup_uniform(3)
+    solver.fas_mu_cycle(G, 4, 1, 3, 2, 10)
+    g.fas_mu_cycle(2, 4, 1, 3, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    m = leaf_mask(G)
+    assert rel_l2(G.download(4)[m], g.channel(4)[m]) <= 1e-5
+
+
+@pytest.mark.parametrize("mu", [2, 1])
+def test_uniform_solve_matches_oracle_and_fp64(mu):
+    G, g, solver, b = setup_uniform(3)
+    solver.mu_cycle_repeat_times = mu
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    ito, relo = g.amg_solve(COEFF, omega=1.5, mu=mu, max_iters=100, tol=1e-6, level_iters=2, coarsest_iters=10)
+    assert rel <= 1e-6 and relo <= 1e-6
+    assert abs(it - ito) <= 1
+    m = leaf_mask(G)
+    x = G.download(0)
+    assert rel_l2(x[m], g.channel(0)[m]) <= 1e-5
+    xs, rt, rc = fp64_solution(g, b, 0)
+    assert rel_l2(x[rt, rc], xs) <= 1e-5
+
+
+def test_solve_zero_rhs_returns_zero():
+    G, g, solver, b = setup_uniform(3, with_oracle=False)
+    G.fill(1, 0.0)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    assert (it, rel) == (0, 0.0)
+    assert not np.any(G.download(0)[leaf_mask(G)])
+
+
+def test_sync_stride_semantics():
+    G, g, solver, b = setup_uniform(3)
+    it, rel = solver.solve(G, False, 5, 1e-6, 2, 10, -1, False)
+    assert (it, rel) == (5, -1.0)
+    G.upload(1, b)
+    it3, rel3 = solver.solve(G, False, 100, 1e-6, 2, 10, 3, False)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6, sync_stride=3)
+    assert it3 % 3 == 0 and it3 == ito and rel3 <= 1e-6
+
+
+def test_shell_setup_matches_oracle():
+    prm = shell_params(coarse=3, mid=4, fine=5)
+    G, g, solver = setup_shell(prm)
+    assert np.array_equal(G.download_cell_types(), g.cell_types())
+    for a in range(4):
+        d, o = G.download(COEFF + a), g.channel(COEFF + a)
+        assert np.array_equal(d, o), f"coefficient channel {a}: max diff {np.max(np.abs(d - o))}"
+    bd, bo = G.download(1), g.channel(1)
+    assert np.max(np.abs(bd - bo)) <= 1e-5 * np.max(np.abs(bo))
+
+
+def test_shell_solve_matches_oracle_and_fp64():
+    prm = shell_params(coarse=3, mid=4, fine=5)
+    G, g, solver = setup_shell(prm)
+    b = G.download(1)
+    g.channel(1)[:] = b  # identical rhs on both sides
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    assert rel <= 1e-6 and abs(it - ito) <= 1
+    m = leaf_mask(G)
+    x = G.download(0)
+    assert rel_l2(x[m], g.channel(0)[m]) <= 1e-5
+    xs, rt, rc = fp64_solution(g, b, 1)
+    assert rel_l2(x[rt, rc], xs) <= 1e-5
+
+
+@pytest.mark.parametrize("case_id,prm", [(cmg.CASE_SPHERE_SOLID, [2, 4]), (cmg.CASE_STAR_EMPTY, [2, 4]), (cmg.CASE_CENTER_POINT, [2, 5])])
+def test_reference_test_grids_solve(case_id, prm):
+    """Octrees of tests/TestGrids.cuh solved by both sides (Dirichlet walls, random rhs on INTERIOR cells)."""
+    G = build_product(case_id, prm)
+    G.set_leaf_cell_types_case(case_id)
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    solver.prepareTypesAndCoeffs(G)
+    g = build_oracle(case_id, prm)
+    g.set_leaf_cell_types_case(case_id)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    assert np.array_equal(G.download_cell_types(), g.cell_types())
+    for a in range(4):
+        assert np.array_equal(G.download(COEFF + a), g.channel(COEFF + a))
+    ct = g.cell_types()
+    rng = np.random.default_rng(11)
+    b = rng.standard_normal(ct.shape).astype(np.float32)
+    b[(G.tiles()[2] != cmg.LEAF)] = 0
+    b[ct != cmg.INTERIOR] = 0
+    G.upload(1, b)
+    g.channel(1)[:] = b
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    assert rel <= 1e-6 and abs(it - ito) <= 1
+    m = leaf_mask(G)
+    assert rel_l2(G.download(0)[m], g.channel(0)[m]) <= 1e-5

@@ -1,0 +1,93 @@
+"""Seeded workloads shared by the tests: the same octree and right-hand side
+built by the CUDA product (through the C ABI) and by the CPU oracle.
+
+Workloads (synthetic, seeded; the reference publishes no dataset):
+  uniform(L)   uniform (8*2^L)^3 grid, all INTERIOR, Dirichlet walls, rhs N(0,1)
+               from numpy default_rng(seed), mean removed (64^3 is L = 3).
+  shell(...)   octree refined to `fine` within `bf` of a solid sphere surface,
+               to `mid` within `bm`, else `coarse`; the sphere is a Neumann
+               cut-cell boundary; rhs = divergence of 16 random Fourier modes.
+"""
+import numpy as np
+
+import cmg
+from oracle import oracle as O
+
+COEFF = 6  # coefficient channels 6..9 (the reference tests use 6, SolverTests.cu:1857)
+U = 10     # face-velocity channels 10..12
+
+
+def fourier_modes(seed, n=16):
+    rng = np.random.default_rng(seed)
+    k = rng.integers(1, 9, size=(n, 3)).astype(np.float64)
+    amp = rng.standard_normal((n, 3))
+    ph = rng.uniform(0.0, 2.0 * np.pi, n)
+    return k, amp, ph
+
+
+def shell_params(coarse=4, mid=5, fine=6, center=(0.5, 0.5, 0.5), r=0.1, bf=0.05, bm=0.15):
+    return [coarse, fine, mid, center[0], center[1], center[2], r, bf, bm]
+
+
+def build_product(case_id, params, h0=0.125, nlev=10, nch=16):
+    G = cmg.HADeviceGrid(h0, nlev, nch)
+    G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
+    G.rebuild()
+    G.refine_case(case_id, params)
+    return G
+
+
+def build_oracle(case_id, params, h0=0.125, nlev=10, nch=16):
+    g = O.Grid(h0, nlev)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(case_id, params)
+    g.alloc(nch)
+    return g
+
+
+def uniform_rhs(leaf_mask, seed=0):
+    rng = np.random.default_rng(seed)
+    n = int(leaf_mask.sum())
+    v = rng.standard_normal(n * 512).astype(np.float32)
+    v -= v.mean(dtype=np.float64).astype(np.float32)
+    b = np.zeros((leaf_mask.size, 512), np.float32)
+    b[leaf_mask] = v.reshape(n, 512)
+    return b
+
+
+def setup_uniform(L=3, seed=0, with_oracle=True):
+    """64^3 for L = 3: both sides prepared, rhs uploaded into channel 1."""
+    prm = [L, L]
+    G = build_product(cmg.CASE_UNIFORM, prm)
+    lv, ijk, ty = G.tiles()
+    G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    solver.prepareTypesAndCoeffs(G)
+    b = uniform_rhs(ty == cmg.LEAF, seed)
+    G.upload(1, b)
+    g = None
+    if with_oracle:
+        g = build_oracle(cmg.CASE_UNIFORM, prm)
+        g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+        g.coarsen_types_and_coeffs(COEFF, 0.5)
+        g.channel(1)[:] = b
+    return G, g, solver, b
+
+
+def setup_shell(params, seed=1, spheres=((0.5, 0.5, 0.5, 0.1),), with_oracle=True):
+    G = build_product(cmg.CASE_SHELL, params)
+    G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
+    G.cutcell_sphere_coeffs(COEFF, spheres, 0.5)
+    k, amp, ph = fourier_modes(seed)
+    G.face_velocity_fourier(U, k, amp, ph)
+    G.divergence(U, COEFF, 1)
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    g = None
+    if with_oracle:
+        g = build_oracle(cmg.CASE_SHELL, params)
+        g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+        g.cutcell_sphere_coeffs(COEFF, spheres, 0.5)
+        g.face_velocity_fourier(U, k, amp, ph)
+        g.divergence(U, COEFF, 1)
+    return G, g, solver
