@@ -35,12 +35,13 @@ EXPORTS = [
     "cmg_grid_create", "cmg_grid_destroy", "cmg_grid_set_tile", "cmg_grid_rebuild", "cmg_grid_iterative_refine",
     "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
     "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
-    "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
+    "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_copy_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
     "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_full_neg_lap", "cmg_amg_dot",
     "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
+    "cmg_amg_last_solve_launches",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -80,6 +81,7 @@ def lib():
             "cmg_grid_upload_cell_types": (I, [P, P, S]),
             "cmg_grid_download_cell_types": (I, [P, P, S]),
             "cmg_grid_fill_channel": (I, [P, I, F]),
+            "cmg_grid_copy_channel": (I, [P, I, I]),
             "cmg_grid_set_leaf_cell_types_case": (I, [P, I, P, I]),
             "cmg_grid_set_stream": (I, [P, P]),
             "cmg_grid_synchronize": (I, [P]),
@@ -98,6 +100,7 @@ def lib():
             "cmg_amg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
             "cmg_amg_fas_mu_cycle": (I, [P, P, I, I, I, I, I]),
             "cmg_amg_last_solve_ms": (I, [P, P]),
+            "cmg_amg_last_solve_launches": (I, [P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -215,6 +218,9 @@ class HADeviceGrid:
     def fill(self, ch, value):
         _check(self.L.cmg_grid_fill_channel(self.h, ch, value), "fill_channel")
 
+    def copy(self, src_ch, dst_ch):
+        _check(self.L.cmg_grid_copy_channel(self.h, src_ch, dst_ch), "copy_channel")
+
     def set_leaf_cell_types_case(self, case_id, params=(0, 0)):
         prm = np.asarray(params, dtype=np.float64)
         _check(self.L.cmg_grid_set_leaf_cell_types_case(self.h, case_id, _p(prm), len(prm)), "set_leaf_cell_types")
@@ -308,3 +314,8 @@ class AMGSolver:
         ms = ctypes.c_float(0)
         _check(self.L.cmg_amg_last_solve_ms(self.h, ctypes.byref(ms)), "last_solve_ms")
         return ms.value
+
+    def last_solve_launches(self):
+        n = ctypes.c_longlong(0)
+        _check(self.L.cmg_amg_last_solve_launches(self.h, ctypes.byref(n)), "last_solve_launches")
+        return n.value

@@ -182,6 +182,14 @@ int cmg_grid_fill_channel(cmg_grid* g, int ch, float value) {
     cmg::launch_fill(g->g.plane(ch), (size_t)g->g.n * 512, value, g->g.stream);
     return cmg::check_cuda(cudaGetLastError(), "fill");
 }
+int cmg_grid_copy_channel(cmg_grid* g, int src_ch, int dst_ch) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_copy_channel: grid not built");
+    if (!chan_ok(g, src_ch) || !chan_ok(g, dst_ch)) return fail(CMG_ERR_INVALID, "channel out of range");
+    if (src_ch == dst_ch) return CMG_OK;
+    CKC(cudaMemcpyAsync(g->g.plane(dst_ch), g->g.plane(src_ch), sizeof(float) * (size_t)g->g.n * 512, cudaMemcpyDeviceToDevice,
+                        g->g.stream));
+    return CMG_OK;
+}
 int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams) {
     GUARD_BEGIN
     (void)params;
@@ -356,6 +364,11 @@ int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, i
 int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms) {
     if (!s || !ms) return fail(CMG_ERR_INVALID, "null argument");
     *ms = s->s.last_ms;
+    return CMG_OK;
+}
+int cmg_amg_last_solve_launches(cmg_amg_solver* s, long long* launches) {
+    if (!s || !launches) return fail(CMG_ERR_INVALID, "null argument");
+    *launches = s->s.last_launches;
     return CMG_OK;
 }
 

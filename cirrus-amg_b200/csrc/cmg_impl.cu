@@ -169,7 +169,7 @@ int validate_solver_topology(const Grid& G) {
 }
 
 Solver::~Solver() {
-    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
     dfree(partial);
     dfree(partial2);
     dfree(s);
@@ -199,7 +199,7 @@ int Solver::ensure_scratch(int nl) {
     CK(cudaMalloc(&partial2, sizeof(double) * (nl + 1)));
     partial_cap = nl;
     // captured graphs hold the old scratch pointers
-    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
     graphs.clear();
     return 0;
 }
@@ -265,7 +265,7 @@ static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
 //   x = 0; rr0 = r.r; [recenter]; z = M r; p = z; gamma = z.r; gate
 //   WHILE (not done):  Ap = A p (+ alpha);  x, r update (+ r.r, convergence)
 //                      IF (not done): [recenter]; z = M r; beta; p = z + beta p
-int Solver::build_graph(Grid& G, const Key& k, cudaGraphExec_t* out) {
+int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
     float* X = G.plane(0);
@@ -282,6 +282,7 @@ int Solver::build_graph(Grid& G, const Key& k, cudaGraphExec_t* out) {
     cudaGraphConditionalHandle loop_h = 0, body_h = 0;
     CK(cudaGraphConditionalHandleCreate(&loop_h, top, 1, cudaGraphCondAssignDefault));
 
+    const long long c0 = kernel_launch_count();
     CK(cudaStreamBeginCaptureToGraph(cs, top, nullptr, nullptr, 0, mode));
     launch_leaf_fill(d, G.leaf, G.nleaf, X, 0.0f, cs);
     if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, R, R, kDotRR0, nullptr, rs, cs);
@@ -304,6 +305,7 @@ int Solver::build_graph(Grid& G, const Key& k, cudaGraphExec_t* out) {
     cudaGraph_t body = wp.conditional.phGraph_out[0];
     CK(cudaGraphConditionalHandleCreate(&body_h, body, 0, cudaGraphCondAssignDefault));
 
+    const long long c1 = kernel_launch_count();
     CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
     launch_leaf_apply(d, G.leaf, G.nleaf, Pp, AP, coeff_ch, true, rs, cs);
     launch_xr_update(d, G.leaf, G.nleaf, X, R, Pp, AP, rs, loop_h, body_h, true, cs);
@@ -319,6 +321,7 @@ int Solver::build_graph(Grid& G, const Key& k, cudaGraphExec_t* out) {
     CK(cudaGraphAddNode(&inode, body, tail.data(), tail.size(), &ip));
     cudaGraph_t ibody = ip.conditional.phGraph_out[0];
 
+    const long long c2 = kernel_launch_count();
     CK(cudaStreamBeginCaptureToGraph(cs, ibody, nullptr, nullptr, 0, mode));
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, R, rs, cs);
     enqueue_mu_cycle(G, A, cs);
@@ -326,10 +329,11 @@ int Solver::build_graph(Grid& G, const Key& k, cudaGraphExec_t* out) {
     launch_p_update(d, G.leaf, G.nleaf, Pp, Z, rs, cs);
     CK(cudaStreamEndCapture(cs, &ibody));
 
-    cudaGraphExec_t exec;
-    CK(cudaGraphInstantiate(&exec, top, 0));
+    out->k_pre = (int)(c1 - c0);
+    out->k_body = (int)(c2 - c1);
+    out->k_if = (int)(kernel_launch_count() - c2);
+    CK(cudaGraphInstantiate(&out->exec, top, 0));
     cudaGraphDestroy(top);
-    *out = exec;
     return 0;
 }
 
@@ -350,14 +354,15 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
     Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, sync_stride > 0 ? 1 : 0, omega};
-    cudaGraphExec_t exec;
+    Plan plan;
     auto it = graphs.find(k);
     if (it == graphs.end()) {
-        if (int rc = build_graph(G, k, &exec)) return rc;
-        graphs[k] = exec;
+        if (int rc = build_graph(G, k, &plan)) return rc;
+        graphs[k] = plan;
     } else {
-        exec = it->second;
+        plan = it->second;
     }
+    cudaGraphExec_t exec = plan.exec;
     std::memset(h_s, 0, sizeof(PcgScalars));
     h_s->max_iters = max_iters;
     h_s->sync_stride = sync_stride;
@@ -389,6 +394,8 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     }
     if (iters) *iters = n_it;
     if (rel) *rel = rel_res;
+    // the IF body runs on every iteration except the one that ends the loop
+    last_launches = plan.k_pre + (long long)r.iter * plan.k_body + (long long)(r.iter > 0 ? r.iter - 1 : 0) * plan.k_if;
     if (verbose) std::printf("cmg AMG-PCG: %d iterations, relative residual %.6e, %.3f ms\n", n_it, rel_res, last_ms);
     if (r.nonfinite) {
         set_error("solve: non-finite value in a PCG reduction");

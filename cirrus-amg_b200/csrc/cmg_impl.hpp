@@ -99,7 +99,12 @@ struct Solver {
                    std::tie(o.g, o.version, o.level_iters, o.coarsest_iters, o.pure_neumann, o.mu, o.sync, o.omega);
         }
     };
-    std::map<Key, cudaGraphExec_t> graphs;
+    struct Plan {
+        cudaGraphExec_t exec;
+        int k_pre, k_body, k_if;  // kernel nodes before the loop, per iteration, in the per-iteration IF body
+    };
+    std::map<Key, Plan> graphs;
+    long long last_launches = 0;
 
     Solver(int c, float rm, float rr, float p) : coeff_ch(c), R_matrix(rm), R_restrict(rr), P(p) {}
     ~Solver();
@@ -110,7 +115,7 @@ struct Solver {
     void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
     void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
-    int build_graph(Grid& G, const Key& k, cudaGraphExec_t* out);
+    int build_graph(Grid& G, const Key& k, Plan* out);
     int solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
               bool pure_neumann, int* iters, double* rel);
 };

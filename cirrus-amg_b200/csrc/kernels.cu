@@ -10,6 +10,7 @@
 #include "kernels.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 
 namespace cmg {
@@ -837,20 +838,24 @@ __global__ void k_count_bad_diag(DevGrid g, int t0, int coeff_ch, int* out) {
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+static std::atomic<long long> g_launches{0};
+static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st) {
     if (nt <= 0) return;
     const float om = (float)omega;
-    if ((double)om == omega) k_gs<true><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
-    else k_gs<false><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
+    if ((double)om == omega) count_launch(), k_gs<true><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
+    else count_launch(), k_gs<false><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
 }
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st) {
-    if (nt > 0) k_restrict<<<nt, 128, 0, st>>>(g, t0, X, RHS, coeff_ch, Rr);
+    if (nt > 0) count_launch(), k_restrict<<<nt, 128, 0, st>>>(g, t0, X, RHS, coeff_ch, Rr);
 }
 void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st) {
-    if (nt > 0) k_fas_save<<<nt, 128, 0, st>>>(g, t0, X, RHS, X0, coeff_ch);
+    if (nt > 0) count_launch(), k_fas_save<<<nt, 128, 0, st>>>(g, t0, X, RHS, X0, coeff_ch);
 }
 void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st) {
-    if (nt > 0) k_prolong<<<nt, 128, 0, st>>>(g, t0, X, X0, P);
+    if (nt > 0) count_launch(), k_prolong<<<nt, 128, 0, st>>>(g, t0, X, X0, P);
 }
 size_t coarse_step_smem_bytes(int ntiles) {
     return (size_t)ntiles * kCells * (7 * sizeof(float) + 1) + sizeof(int) * (6 * ntiles + 8) + sizeof(int4) * ntiles + 16;
@@ -871,79 +876,79 @@ void launch_coarse_step(const DevGrid& g, int top, int ntiles, int level1_begin,
     A.Rr = Rr;
     A.P = P;
     const size_t smem = coarse_step_smem_bytes(ntiles);
-    k_coarse<<<1, 1024, smem, st>>>(g, A, X, RHS, X0);
+    count_launch(), k_coarse<<<1, 1024, smem, st>>>(g, A, X, RHS, X0);
 }
 void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
                        ReduceScratch rs, cudaStream_t st) {
-    if (nleaf > 0) k_leaf_apply<<<nleaf, 128, 0, st>>>(g, leaf, P, AP, coeff_ch, fuse_alpha ? 1 : 0, rs);
+    if (nleaf > 0) count_launch(), k_leaf_apply<<<nleaf, 128, 0, st>>>(g, leaf, P, AP, coeff_ch, fuse_alpha ? 1 : 0, rs);
 }
 void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,
                       ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool use_handles,
                       cudaStream_t st) {
-    if (nleaf > 0) k_xr_update<<<nleaf, 128, 0, st>>>(g, leaf, X, R, P, AP, rs, loop_h, body_h, use_handles ? 1 : 0);
+    if (nleaf > 0) count_launch(), k_xr_update<<<nleaf, 128, 0, st>>>(g, leaf, X, R, P, AP, rs, loop_h, body_h, use_handles ? 1 : 0);
 }
 void launch_dot(const DevGrid& g, const int* leaf, int nleaf, const float* A, const float* B, int mode, double* out, ReduceScratch rs,
                 cudaStream_t st) {
     (void)g;
-    if (nleaf > 0) k_dot<<<nleaf, 128, 0, st>>>(leaf, A, B, mode, out, rs);
+    if (nleaf > 0) count_launch(), k_dot<<<nleaf, 128, 0, st>>>(leaf, A, B, mode, out, rs);
 }
 void launch_p_update(const DevGrid& g, const int* leaf, int nleaf, float* P, const float* Z, ReduceScratch rs, cudaStream_t st) {
-    if (nleaf > 0) k_p_update<<<nleaf, 128, 0, st>>>(g, leaf, P, Z, rs);
+    if (nleaf > 0) count_launch(), k_p_update<<<nleaf, 128, 0, st>>>(g, leaf, P, Z, rs);
 }
 void launch_leaf_fill(const DevGrid& g, const int* leaf, int nleaf, float* X, float value, cudaStream_t st) {
     (void)g;
-    if (nleaf > 0) k_leaf_fill<<<nleaf, 128, 0, st>>>(leaf, X, value);
+    if (nleaf > 0) count_launch(), k_leaf_fill<<<nleaf, 128, 0, st>>>(leaf, X, value);
 }
 void launch_leaf_copy(const DevGrid& g, const int* leaf, int nleaf, float* dst, const float* src, cudaStream_t st) {
     (void)g;
-    if (nleaf > 0) k_leaf_copy<<<nleaf, 128, 0, st>>>(leaf, dst, src);
+    if (nleaf > 0) count_launch(), k_leaf_copy<<<nleaf, 128, 0, st>>>(leaf, dst, src);
 }
 void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, ReduceScratch rs, cudaStream_t st) {
     if (nleaf <= 0) return;
-    k_mean_partial<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
-    k_sub_mean<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
+    count_launch(), k_mean_partial<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
+    count_launch(), k_sub_mean<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
 }
-void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st) { k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h); }
+void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st) { count_launch(), k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h); }
 void init_kernel_attributes() { cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); }
 
 void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st) {
-    if (nt > 0) k_ghost_types<<<nt, 128, 0, st>>>(g, t0);
+    if (nt > 0) count_launch(), k_ghost_types<<<nt, 128, 0, st>>>(g, t0);
 }
 void launch_face_coeffs(const DevGrid& g, int t0, int nt, int coeff_ch, int ns, const float* sp, cudaStream_t st) {
-    if (nt > 0) k_face_coeffs<<<nt, 128, 0, st>>>(g, t0, coeff_ch, ns, sp);
+    if (nt > 0) count_launch(), k_face_coeffs<<<nt, 128, 0, st>>>(g, t0, coeff_ch, ns, sp);
 }
 void launch_cutcell_neumann(const DevGrid& g, const int* leaf, int nleaf, int ns, const float* sp, cudaStream_t st) {
-    if (nleaf > 0) k_cutcell_neumann<<<nleaf, 128, 0, st>>>(g, leaf, ns, sp);
+    if (nleaf > 0) count_launch(), k_cutcell_neumann<<<nleaf, 128, 0, st>>>(g, leaf, ns, sp);
 }
 void launch_coarsen_offdiag(const DevGrid& g, int t0, int nt, int coeff_ch, float R, cudaStream_t st) {
-    if (nt > 0) k_coarsen_offdiag<<<nt, 64, 0, st>>>(g, t0, coeff_ch, R);
+    if (nt > 0) count_launch(), k_coarsen_offdiag<<<nt, 64, 0, st>>>(g, t0, coeff_ch, R);
 }
 void launch_diag(const DevGrid& g, int t0, int nt, int coeff_ch, float R, cudaStream_t st) {
-    if (nt > 0) k_diag<<<nt, 128, 0, st>>>(g, t0, coeff_ch, R);
+    if (nt > 0) count_launch(), k_diag<<<nt, 128, 0, st>>>(g, t0, coeff_ch, R);
 }
 void launch_face_velocity(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int nm, const double* modes, cudaStream_t st) {
-    if (nleaf > 0) k_face_velocity<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, nm, modes);
+    if (nleaf > 0) count_launch(), k_face_velocity<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, nm, modes);
 }
 void launch_propagate_ghost(const DevGrid& g, int t0, int nt, int ch, cudaStream_t st) {
-    if (nt > 0) k_propagate_ghost<<<nt, 128, 0, st>>>(g, t0, ch);
+    if (nt > 0) count_launch(), k_propagate_ghost<<<nt, 128, 0, st>>>(g, t0, ch);
 }
 void launch_accumulate_faces(const DevGrid& g, const int* leaf, int nleaf, int u_ch, cudaStream_t st) {
-    if (nleaf > 0) k_accumulate_faces<<<nleaf, 64, 0, st>>>(g, leaf, u_ch);
+    if (nleaf > 0) count_launch(), k_accumulate_faces<<<nleaf, 64, 0, st>>>(g, leaf, u_ch);
 }
 void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int coeff_ch, int out_ch, cudaStream_t st) {
-    if (nleaf > 0) k_divergence<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, coeff_ch, out_ch);
+    if (nleaf > 0) count_launch(), k_divergence<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, coeff_ch, out_ch);
 }
 void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st) {
-    if (n_new > 0 && nch > 0) k_remap<<<dim3(n_new, nch), 128, 0, st>>>(src, dst, old_of_new, n_new, n_old);
+    if (n_new > 0 && nch > 0) count_launch(), k_remap<<<dim3(n_new, nch), 128, 0, st>>>(src, dst, old_of_new, n_new, n_old);
 }
 void launch_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new, int n_new, cudaStream_t st) {
-    if (n_new > 0) k_remap_types<<<n_new, 128, 0, st>>>(src, dst, old_of_new);
+    if (n_new > 0) count_launch(), k_remap_types<<<n_new, 128, 0, st>>>(src, dst, old_of_new);
 }
 void launch_fill(float* p, size_t n, float v, cudaStream_t st) {
-    if (n > 0) k_fill<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p, n, v);
+    if (n > 0) count_launch(), k_fill<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p, n, v);
 }
 void launch_count_bad_diag(const DevGrid& g, int t0, int nt, int coeff_ch, int* out, cudaStream_t st) {
-    if (nt > 0) k_count_bad_diag<<<nt, 128, 0, st>>>(g, t0, coeff_ch, out);
+    if (nt > 0) count_launch(), k_count_bad_diag<<<nt, 128, 0, st>>>(g, t0, coeff_ch, out);
 }
 
 }  // namespace cmg

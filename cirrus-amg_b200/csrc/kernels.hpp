@@ -49,6 +49,7 @@ void launch_leaf_copy(const DevGrid& g, const int* leaf, int nleaf, float* dst, 
 void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, ReduceScratch rs, cudaStream_t st);
 void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st);
 void init_kernel_attributes();
+long long kernel_launch_count();  // kernels enqueued (or captured) by this library so far
 
 // --- operator set-up and right-hand side ---
 void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st);

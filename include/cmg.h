@@ -95,6 +95,9 @@ int cmg_grid_download_channel(cmg_grid* g, int ch, float* host, size_t count);
 int cmg_grid_upload_cell_types(cmg_grid* g, const uint8_t* host, size_t count);
 int cmg_grid_download_cell_types(cmg_grid* g, uint8_t* host, size_t count);
 int cmg_grid_fill_channel(cmg_grid* g, int ch, float value);
+/* device-to-device copy of a whole channel plane (Copy over all tiles and
+ * cells, src/PoissonGrid.cu:87, without the cell-type mask) */
+int cmg_grid_copy_channel(cmg_grid* g, int src_ch, int dst_ch);
 /* CreateTestGrid cell types of LEAF tiles (tests/TestGrids.cuh:161-167) */
 int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams);
 /* stream used by every later call on this grid (NULL = legacy default) */
@@ -145,6 +148,10 @@ int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, i
 int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters);
 /* device time of the last cmg_amg_solve, milliseconds (CUDA events) */
 int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms);
+/* number of this library's kernels the last cmg_amg_solve executed (counted
+ * from the kernel nodes of its graph times the loop trips); no counterpart in
+ * the reference, which launches each kernel from the host */
+int cmg_amg_last_solve_launches(cmg_amg_solver* s, long long* launches);
 
 #ifdef __cplusplus
 }
