@@ -150,6 +150,9 @@ def make_solver(cmg):
     s = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
     s.omega = SOLVE["omega"]
     s.mu_cycle_repeat_times = SOLVE["mu"]
+    # CMG_SOLVE_MODE=stream launches kernel by kernel (for ncu launch lists)
+    if os.environ.get("CMG_SOLVE_MODE", "graph") == "stream":
+        s.set_launch_mode(False)
     return s
 
 

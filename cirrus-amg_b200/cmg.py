@@ -39,7 +39,8 @@ EXPORTS = [
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
     "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_full_neg_lap", "cmg_amg_dot",
-    "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solve",
+    "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solver_set_launch_mode",
+    "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
     "cmg_amg_last_solve_launches",
 ]
@@ -95,6 +96,7 @@ def lib():
             "cmg_amg_solver_create": (I, [I, F, F, F, PP]),
             "cmg_amg_solver_destroy": (I, [P]),
             "cmg_amg_solver_set_smoother": (I, [P, D, I]),
+            "cmg_amg_solver_set_launch_mode": (I, [P, I]),
             "cmg_amg_solve": (I, [P, P, I, I, D, I, I, I, I, P, P]),
             "cmg_amg_solve_host": (I, [P, P, P, P, S, I, D, I, I, I, I, P, P]),
             "cmg_amg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
@@ -278,6 +280,10 @@ class AMGSolver:
                 self.h = None
         except Exception:
             pass
+
+    def set_launch_mode(self, use_graph):
+        """True: one CUDA graph per solve (default); False: kernel-by-kernel launches."""
+        _check(self.L.cmg_amg_solver_set_launch_mode(self.h, int(bool(use_graph))), "set_launch_mode")
 
     def _sync_params(self):
         _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")

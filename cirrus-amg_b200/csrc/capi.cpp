@@ -325,6 +325,11 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu) {
     s->s.mu = mu;
     return CMG_OK;
 }
+int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int use_graph) {
+    if (!s) return fail(CMG_ERR_INVALID, "null solver");
+    s->s.use_graph = use_graph != 0;
+    return CMG_OK;
+}
 int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
                   int pure_neumann, int* iters, double* rel_res) {
     GUARD_BEGIN

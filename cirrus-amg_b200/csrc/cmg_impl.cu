@@ -265,15 +265,36 @@ static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
 //   x = 0; rr0 = r.r; [recenter]; z = M r; p = z; gamma = z.r; gate
 //   WHILE (not done):  Ap = A p (+ alpha);  x, r update (+ r.r, convergence)
 //                      IF (not done): [recenter]; z = M r; beta; p = z + beta p
-int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
+// x = 0; rr0 = r.r; [recenter]; z = M r; p = z; gamma = z.r; loop gate (src/AMGSolver.cu:1405-1442)
+void Solver::enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_h, bool graph, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
-    float* X = G.plane(0);
-    float* R = G.plane(1);
-    float* Pp = G.plane(2);
-    float* AP = G.plane(3);
-    float* Z = G.plane(4);
-    const MuArgs A = mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters);
+    launch_leaf_fill(d, G.leaf, G.nleaf, G.plane(0), 0.0f, st);
+    if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(1), kDotRR0, nullptr, rs, st);
+    if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
+    enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
+    launch_leaf_copy(d, G.leaf, G.nleaf, G.plane(2), G.plane(4), st);
+    launch_dot(d, G.leaf, G.nleaf, G.plane(4), G.plane(1), kDotGammaInit, nullptr, rs, st);
+    launch_loop_gate(rs, loop_h, graph, st);
+}
+// Ap = A p with alpha; x += alpha p, r -= alpha Ap with r.r and the convergence test (src/AMGSolver.cu:1449-1499)
+void Solver::enqueue_body(Grid& G, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool graph, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    const ReduceScratch rs = scratch();
+    launch_leaf_apply(d, G.leaf, G.nleaf, G.plane(2), G.plane(3), coeff_ch, true, rs, st);
+    launch_xr_update(d, G.leaf, G.nleaf, G.plane(0), G.plane(1), G.plane(2), G.plane(3), rs, loop_h, body_h, graph, st);
+}
+// [recenter]; z = M r; gamma_old, gamma, beta; p = z + beta p (src/AMGSolver.cu:1500-1536)
+void Solver::enqueue_tail(Grid& G, const Key& k, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    const ReduceScratch rs = scratch();
+    if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
+    enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
+    launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(4), kDotBeta, nullptr, rs, st);
+    launch_p_update(d, G.leaf, G.nleaf, G.plane(2), G.plane(4), rs, st);
+}
+
+int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
     cudaStream_t cs = cap_stream;
     const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
 
@@ -284,13 +305,7 @@ int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
 
     const long long c0 = kernel_launch_count();
     CK(cudaStreamBeginCaptureToGraph(cs, top, nullptr, nullptr, 0, mode));
-    launch_leaf_fill(d, G.leaf, G.nleaf, X, 0.0f, cs);
-    if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, R, R, kDotRR0, nullptr, rs, cs);
-    if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, R, rs, cs);
-    enqueue_mu_cycle(G, A, cs);
-    launch_leaf_copy(d, G.leaf, G.nleaf, Pp, Z, cs);
-    launch_dot(d, G.leaf, G.nleaf, Z, R, kDotGammaInit, nullptr, rs, cs);
-    launch_loop_gate(rs, loop_h, cs);
+    enqueue_pre(G, k, loop_h, true, cs);
     std::vector<cudaGraphNode_t> tail;
     if (int rc = capture_tail(cs, tail)) return rc;
     CK(cudaStreamEndCapture(cs, &top));
@@ -307,8 +322,7 @@ int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
 
     const long long c1 = kernel_launch_count();
     CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, mode));
-    launch_leaf_apply(d, G.leaf, G.nleaf, Pp, AP, coeff_ch, true, rs, cs);
-    launch_xr_update(d, G.leaf, G.nleaf, X, R, Pp, AP, rs, loop_h, body_h, true, cs);
+    enqueue_body(G, loop_h, body_h, true, cs);
     if (int rc = capture_tail(cs, tail)) return rc;
     CK(cudaStreamEndCapture(cs, &body));
 
@@ -323,10 +337,7 @@ int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
 
     const long long c2 = kernel_launch_count();
     CK(cudaStreamBeginCaptureToGraph(cs, ibody, nullptr, nullptr, 0, mode));
-    if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, R, rs, cs);
-    enqueue_mu_cycle(G, A, cs);
-    launch_dot(d, G.leaf, G.nleaf, R, Z, kDotBeta, nullptr, rs, cs);
-    launch_p_update(d, G.leaf, G.nleaf, Pp, Z, rs, cs);
+    enqueue_tail(G, k, cs);
     CK(cudaStreamEndCapture(cs, &ibody));
 
     out->k_pre = (int)(c1 - c0);
@@ -354,15 +365,16 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
     Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, sync_stride > 0 ? 1 : 0, omega};
-    Plan plan;
-    auto it = graphs.find(k);
-    if (it == graphs.end()) {
-        if (int rc = build_graph(G, k, &plan)) return rc;
-        graphs[k] = plan;
-    } else {
-        plan = it->second;
+    Plan plan{};
+    if (use_graph) {
+        auto it = graphs.find(k);
+        if (it == graphs.end()) {
+            if (int rc = build_graph(G, k, &plan)) return rc;
+            graphs[k] = plan;
+        } else {
+            plan = it->second;
+        }
     }
-    cudaGraphExec_t exec = plan.exec;
     std::memset(h_s, 0, sizeof(PcgScalars));
     h_s->max_iters = max_iters;
     h_s->sync_stride = sync_stride;
@@ -371,7 +383,26 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     cudaStream_t st = G.stream;
     CK(cudaMemcpyAsync(s, h_s, sizeof(PcgScalars), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(ev0, st));
-    CK(cudaGraphLaunch(exec, st));
+    long long stream_launches = -1;
+    if (use_graph) {
+        CK(cudaGraphLaunch(plan.exec, st));
+    } else {
+        // the same kernels launched one by one, the loop test read back on the
+        // host after every update (for profilers that do not enter graphs)
+        const long long c0 = kernel_launch_count();
+        enqueue_pre(G, k, 0, false, st);
+        for (;;) {
+            CK(cudaMemcpyAsync(&h_s->done, &s->done, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (h_s->done) break;
+            enqueue_body(G, 0, 0, false, st);
+            CK(cudaMemcpyAsync(&h_s->done, &s->done, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (h_s->done) break;
+            enqueue_tail(G, k, st);
+        }
+        stream_launches = kernel_launch_count() - c0;
+    }
     CK(cudaEventRecord(ev1, st));
     CK(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -395,7 +426,8 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     if (iters) *iters = n_it;
     if (rel) *rel = rel_res;
     // the IF body runs on every iteration except the one that ends the loop
-    last_launches = plan.k_pre + (long long)r.iter * plan.k_body + (long long)(r.iter > 0 ? r.iter - 1 : 0) * plan.k_if;
+    last_launches = use_graph ? plan.k_pre + (long long)r.iter * plan.k_body + (long long)(r.iter > 0 ? r.iter - 1 : 0) * plan.k_if
+                              : stream_launches;
     if (verbose) std::printf("cmg AMG-PCG: %d iterations, relative residual %.6e, %.3f ms\n", n_it, rel_res, last_ms);
     if (r.nonfinite) {
         set_error("solve: non-finite value in a PCG reduction");

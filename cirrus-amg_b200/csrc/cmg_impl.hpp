@@ -115,6 +115,10 @@ struct Solver {
     void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
     void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
+    bool use_graph = true;  // false: launch kernel by kernel from the host (profiling)
+    void enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_h, bool graph, cudaStream_t st) const;
+    void enqueue_body(Grid& G, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool graph, cudaStream_t st) const;
+    void enqueue_tail(Grid& G, const Key& k, cudaStream_t st) const;
     int build_graph(Grid& G, const Key& k, Plan* out);
     int solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
               bool pure_neumann, int* iters, double* rel);

@@ -481,14 +481,15 @@ __global__ void k_sub_mean(DevGrid g, const int* leaf, float* R, ReduceScratch r
 }
 
 // threshold (epsilon |b|)^2 and the b == 0 exit (src/AMGSolver.cu:1410-1426), then the loop condition
-__global__ void k_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h) {
+__global__ void k_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, int use_handle) {
     PcgScalars* s = rs.s;
     if (s->sync_stride > 0) {
         const double t = s->tol * s->tol * s->rr0;
         s->thr = t > DBL_MIN ? t : DBL_MIN;
         if (s->rr0 == 0.0) s->done = 1;
     }
-    cudaGraphSetConditional(loop_h, (s->done == 0 && s->iter < s->max_iters) ? 1u : 0u);
+    if (s->iter >= s->max_iters) s->done = 1;
+    if (use_handle) cudaGraphSetConditional(loop_h, s->done == 0 ? 1u : 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -908,7 +909,9 @@ void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, Red
     count_launch(), k_mean_partial<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
     count_launch(), k_sub_mean<<<nleaf, 128, 0, st>>>(g, leaf, R, rs);
 }
-void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st) { count_launch(), k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h); }
+void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, bool use_handle, cudaStream_t st) {
+    count_launch(), k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h, use_handle ? 1 : 0);
+}
 void init_kernel_attributes() { cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); }
 
 void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st) {

@@ -47,7 +47,7 @@ void launch_p_update(const DevGrid& g, const int* leaf, int nleaf, float* P, con
 void launch_leaf_fill(const DevGrid& g, const int* leaf, int nleaf, float* X, float value, cudaStream_t st);
 void launch_leaf_copy(const DevGrid& g, const int* leaf, int nleaf, float* dst, const float* src, cudaStream_t st);
 void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, ReduceScratch rs, cudaStream_t st);
-void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaStream_t st);
+void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, bool use_handle, cudaStream_t st);
 void init_kernel_attributes();
 long long kernel_launch_count();  // kernels enqueued (or captured) by this library so far
 

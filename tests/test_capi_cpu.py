@@ -1,0 +1,95 @@
+"""CPU checks of the native library: it loads, exports every entry point the
+header declares, builds the octree topology on the host identically to the
+oracle, and rejects bad arguments with status codes.  No device call is made."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cmg
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "cmg.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(cmg_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(cmg.LIB_PATH)
+    names = header_functions()
+    assert len(names) >= 38
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert sorted(cmg.EXPORTS) == names
+
+
+@pytest.mark.parametrize("case_id,prm", [
+    (cmg.CASE_UNIFORM, [3, 3]),
+    (cmg.CASE_CENTER_POINT, [2, 6]),
+    (cmg.CASE_SPHERE_EMPTY, [2, 5]),
+    (cmg.CASE_SPHERE_SOLID, [2, 5]),
+    (cmg.CASE_STAR_EMPTY, [3, 6]),
+    (cmg.CASE_STAR_SOLID, [2, 5]),
+    (cmg.CASE_SHELL, [4, 6, 5, 0.5, 0.5, 0.5, 0.1, 0.05, 0.15]),
+    (cmg.CASE_MULTI_SPHERE, [3, 5, 0.05, 2, 0.3, 0.3, 0.4, 0.08, 0.7, 0.6, 0.5, 0.12]),
+])
+def test_host_topology_matches_oracle(case_id, prm):
+    G = cmg.HADeviceGrid(0.125, 10, 16)
+    G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
+    G.rebuild()
+    G.refine_case(case_id, prm)
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(case_id, prm)
+    for a, b in zip(G.tiles(), g.tiles()):
+        assert np.array_equal(a, b)
+    nb, ch = G.tables()
+    onb, opar, och = g.tables()
+    assert np.array_equal(nb[:, :6], onb)
+    assert np.array_equal(nb[:, 6], opar)
+    assert np.all(nb[:, 7] == -1)
+    assert np.array_equal(ch, och)
+
+
+def test_callback_refinement_equals_builtin_case():
+    """iterativeRefine with a host callback reproduces the built-in uniform case."""
+    G = cmg.HADeviceGrid(0.125, 10, 16)
+    G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
+    G.rebuild()
+    G.iterative_refine(lambda l, i, j, k: 3)
+    H = cmg.HADeviceGrid(0.125, 10, 16)
+    H.set_tile_host(0, (0, 0, 0), cmg.LEAF)
+    H.rebuild()
+    H.refine_case(cmg.CASE_UNIFORM, [3, 3])
+    for a, b in zip(G.tiles(), H.tiles()):
+        assert np.array_equal(a, b)
+
+
+def test_refinement_respects_level_capacity():
+    G = cmg.HADeviceGrid(0.125, 3, 16)  # levels 0..2 only
+    G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
+    G.rebuild()
+    G.refine_case(cmg.CASE_UNIFORM, [5, 5])
+    assert G.max_level == 2
+
+
+def test_bad_arguments_return_status_codes():
+    L = cmg.lib()
+    h = ctypes.c_void_p()
+    assert L.cmg_grid_create(-1.0, 10, 16, ctypes.byref(h)) == 1
+    assert L.cmg_grid_create(0.125, 0, 16, ctypes.byref(h)) == 1
+    G = cmg.HADeviceGrid(0.125, 10, 16)
+    assert L.cmg_grid_set_tile(G.h, 0, 0, 0, 0, 3) == 1          # not a tile type
+    assert L.cmg_grid_set_tile(G.h, 12, 0, 0, 0, 1) == 1         # level beyond capacity
+    p = ctypes.c_void_p()
+    assert L.cmg_grid_channel_ptr(G.h, 0, ctypes.byref(p)) == 3  # not built yet
+    prm = np.array([3.0, 3.0])
+    assert L.cmg_grid_refine_case(G.h, 99, prm.ctypes.data_as(ctypes.c_void_p), 2, None) == 1
+    assert b"not built" in L.cmg_last_error() or b"bad argument" in L.cmg_last_error()

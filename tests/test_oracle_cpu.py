@@ -1,0 +1,169 @@
+"""CPU checks of the oracle against the reference's own known-answer tests.
+
+The reference stores no golden vectors for this path; its tests are analytic
+(tests/SolverTests.cu).  These restate them on the oracle:
+  * operator structure on a uniform grid (7-point, -h off-diagonal, 6h diagonal
+    with Dirichlet walls folded in, symmetric);
+  * discrete-Laplacian truncation error against an analytic -lap f * h^3
+    (TestDiscretizedLaplacian, tests/SolverTests.cu:1282-1361): second order;
+  * refinement rules: 2:1 face balance, GHOST parents are LEAF
+    (src/HAGrid.h:856-889, 1088-1170);
+  * the oracle's FAS mu-cycle PCG converges to 1e-6 and agrees with the FP64
+    CSR solution of the same operator (the north-star 1e-5 bar).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+COEFF = 6
+
+
+def uniform_grid(L):
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(O.CASE_UNIFORM, [L, L])
+    g.alloc(16)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    return g
+
+
+def cell_centres(g):
+    lv, ijk, ty = g.tiles()
+    v = np.arange(512)
+    l = np.stack([v >> 6, (v >> 3) & 7, v & 7], axis=1)
+    h = 0.125 / (2.0 ** lv)
+    gc = ijk[:, None, :] * 8 + l[None, :, :]
+    return (gc + 0.5) * h[:, None, None], h
+
+
+def test_uniform_tile_counts():
+    g = uniform_grid(3)
+    lv, ijk, ty = g.tiles()
+    assert g.n == 585
+    for L, (nleaf, nnon) in enumerate([(0, 1), (0, 8), (0, 64), (512, 0)]):
+        assert int(((lv == L) & (ty == O.LEAF)).sum()) == nleaf
+        assert int(((lv == L) & (ty == O.NONLEAF)).sum()) == nnon
+    assert not np.any(ty == O.GHOST)
+
+
+def test_uniform_operator_values_and_symmetry():
+    g = uniform_grid(3)
+    lv, ijk, ty = g.tiles()
+    leaf = ty == O.LEAF
+    h = 0.125 / 8
+    assert np.all(g.channel(COEFF + 3)[leaf] == np.float32(6 * h))
+    for a in range(3):
+        assert set(np.unique(g.channel(COEFF + a)[leaf]).tolist()) == {np.float32(-h)}
+    # NONLEAF levels: scaled Galerkin coarsening keeps the 7-point form at 2h
+    lev2 = lv == 2
+    assert np.all(g.channel(COEFF + 3)[lev2] == np.float32(6 * 2 * h))
+    rp, ci, va, rt, rc = g.assemble(COEFF)
+    import scipy.sparse as sp
+
+    n = len(rp) - 1
+    A = sp.csr_matrix((va, ci, rp), shape=(n, n))
+    assert n == 64 ** 3
+    assert abs(A - A.T).max() == 0.0
+    # row sums: 0 inside, k*h for a cell touching k Dirichlet walls
+    rs = np.asarray(A.sum(axis=1)).ravel()
+    assert np.allclose(np.unique(np.round(rs / h, 6)), [0, 1, 2, 3])
+
+
+@pytest.mark.parametrize("L", [2])
+def test_truncation_error_second_order(L):
+    """A f versus -lap f * h^3 for f = sin(pi x) sin(pi y) sin(pi z) (zero on the walls).
+    Levels 2 -> 3: finer than that the float32 operator apply (the stencil cancels
+    ~6/(3 pi^2 h^2) = O(1e3)) reaches round-off."""
+    errs = []
+    for lev in (L, L + 1):
+        g = uniform_grid(lev)
+        xc, h = cell_centres(g)
+        f = np.sin(np.pi * xc[..., 0]) * np.sin(np.pi * xc[..., 1]) * np.sin(np.pi * xc[..., 2])
+        g.channel(2)[:] = f.astype(np.float32)
+        g.full_neg_lap_leafs(2, COEFF, 3)
+        lv, ijk, ty = g.tiles()
+        leaf = ty == O.LEAF
+        exact = 3 * np.pi ** 2 * f * (h[:, None] ** 3)
+        # the Dirichlet wall sits at the empty neighbour's cell centre (AMGSolver.cu:489-493),
+        # a first-order boundary treatment; the second-order rate holds away from the walls
+        far = np.all((xc > 2 * h[:, None, None]) & (xc < 1 - 2 * h[:, None, None]), axis=-1)
+        sel = leaf[:, None] & far
+        e = np.abs(g.channel(3)[sel] - exact[sel]).mean() / np.abs(exact[sel]).mean()
+        errs.append(e)
+    assert errs[1] < errs[0] / 3.0, errs  # halving h cuts the error ~4x
+
+
+@pytest.mark.parametrize("case_id,prm", [(O.CASE_SPHERE_EMPTY, [2, 5]), (O.CASE_STAR_SOLID, [2, 5]), (O.CASE_SHELL, [3, 5, 4, 0.5, 0.5, 0.5, 0.1, 0.05, 0.15])])
+def test_refinement_rules(case_id, prm):
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(case_id, prm)
+    lv, ijk, ty = g.tiles()
+    nbr, par, ch = g.tables()
+    for t in range(g.n):
+        if ty[t] == O.GHOST:
+            assert par[t] >= 0 and ty[par[t]] == O.LEAF
+        if ty[t] == O.LEAF:
+            for a in range(6):
+                q = nbr[t, a]
+                if q >= 0 and ty[q] == O.NONLEAF:
+                    axis, plus = a % 3, a // 3
+                    for ci in range(8):
+                        bit = (ci >> (2 - axis)) & 1
+                        if bit == (0 if plus else 1):
+                            assert ty[ch[q, ci]] == O.LEAF
+    # every LEAF tile's face neighbours are within one level (2:1 balance across faces)
+    key = {(int(lv[t]), *map(int, ijk[t])): t for t in range(g.n)}
+    for t in np.nonzero(ty == O.LEAF)[0]:
+        L = int(lv[t])
+        for a in range(6):
+            c = list(map(int, ijk[t]))
+            c[a % 3] += 1 if a >= 3 else -1
+            if (L, *c) in key:
+                continue
+            # neighbour region not at this level: must be covered by a LEAF one level up
+            pc = [x >> 1 for x in c]
+            assert (L - 1, *pc) in key or min(c) < 0 or max(c) >= 2 ** L
+
+
+def test_oracle_solve_matches_fp64():
+    g = uniform_grid(2)
+    lv, ijk, ty = g.tiles()
+    leaf = ty == O.LEAF
+    rng = np.random.default_rng(0)
+    b = np.zeros((g.n, 512), np.float32)
+    b[leaf] = rng.standard_normal((int(leaf.sum()), 512)).astype(np.float32)
+    g.channel(1)[:] = b
+    it, rel = g.amg_solve(COEFF, omega=1.5, mu=2, max_iters=100, tol=1e-6, level_iters=2, coarsest_iters=10)
+    assert rel < 1e-6 and 3 <= it <= 12
+    rp, ci, va, rt, rc = g.assemble(COEFF)
+    xs, its, rr = O.csr_solve(rp, ci, va, b[rt, rc].astype(np.float64), 1e-12, 5000, 0)
+    x = g.channel(0)[rt, rc]
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-5
+
+
+def test_cutcell_face_fraction_rules():
+    """Face fluid fractions: 0 inside the solid, 1 in open fluid, clamped to >= 0.1 when cut (MeshCutCell.cu:405)."""
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(O.CASE_SHELL, [3, 4, 3, 0.5, 0.5, 0.5, 0.2, 0.05, 0.05])
+    g.alloc(16)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.cutcell_sphere_coeffs(COEFF, [[0.5, 0.5, 0.5, 0.2]], 0.5)
+    lv, ijk, ty = g.tiles()
+    ct = g.cell_types()
+    leaf = ty == O.LEAF
+    h = (0.125 / 2.0 ** lv)[:, None]
+    for a in range(3):
+        c = g.channel(COEFF + a)
+        ratio = (-c / h)[leaf]
+        assert np.all(ratio >= 0) and np.all(ratio <= 1.0 + 1e-6)
+        cut = (ratio > 0) & (ratio < 1)
+        assert np.all(ratio[cut] >= 0.1 - 1e-7)
+    assert np.any(ct[leaf] == O.NEUMANN)
+    assert np.all(g.channel(COEFF + 3)[leaf][ct[leaf] == O.NEUMANN] == 0)
