@@ -234,7 +234,7 @@ void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, cons
 void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) const {
     const DevGrid d = G.dev();
     if (l <= 1) {
-        launch_coarse_step(d, l, G.level_end(l), 1, A.X, A.RHS, A.X0, A.coeff_ch, A.mu,
+        launch_coarse_step(d, l, A.X, A.RHS, A.X0, A.coeff_ch, A.mu,
                            A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P, st);
         return;
     }

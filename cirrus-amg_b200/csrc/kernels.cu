@@ -151,167 +151,211 @@ __global__ void __launch_bounds__(128) k_prolong(DevGrid g, int t0, float* X, co
 
 // ---------------------------------------------------------------------------
 // Coarse levels: FASMuCycleStep (src/AMGSolver.cu:1257-1277) of level 0 or 1
-// in one 1024-thread block.  Level 0 is the root tile and level 1 its eight
-// children, so the whole sub-cycle (all mu recursions and the 2*coarsest_iters
-// colour sweeps of every coarsest visit) runs out of shared memory with block
-// barriers instead of ~50 kernel launches.  Neither level can hold GHOST
-// tiles (a level-1 ghost would need a LEAF root, which has no active children).
+// in one 1024-thread block.  A NONLEAF root has all eight children and
+// neither level can hold GHOST tiles, so the root and its children are
+// complete 8^3 and 16^3 grids.  Both are staged in shared memory as dense
+// arrays with a zero halo: the stencil needs no neighbour tables, every
+// thread of a colour sweep has a cell, and all mu recursions with their
+// 2*coarsest_iters sweeps run between block barriers instead of ~50 kernel
+// launches.  A zero halo value is exactly the reference's empty-neighbour rule
+// (x = 0, src/AMGSolver.cu:489-493); x is held masked to INTERIOR cells, which
+// is how every read of it in the reference sees it.
 // ---------------------------------------------------------------------------
 struct CoarseArgs {
-    int top, ntiles, l1b, coeff_ch, mu, level_iters, coarsest_iters, exact;
+    int top, coeff_ch, mu, level_iters, coarsest_iters, exact;
     float om, Rr, P;
     double omega;
 };
 
-struct CoarseSmem {
-    float *x, *rhs, *x0, *c;
+template <int N>  // cells per axis: 16 for level 1, 8 for level 0
+struct DenseLevel {
+    static constexpr int PD = N + 2;  // padded extent of x
+    float* x;                         // PD^3, zero halo
+    float* c0;                        // [N+1][N][N]: -x face of cell i (face N: domain boundary, 0)
+    float* c1;                        // [N][N+1][N]
+    float* c2;                        // [N][N][N+1]
+    float* d;                         // [N][N][N]
+    float* rhs;
     uint8_t* ty;
-    int* nb;     // [ntiles][6]
-    int* child;  // root children [8]
-    int4* meta;  // [ntiles]
-    int T;
-    float h[2];
-    __device__ float xm(int t, int v) const { return ty[t * kCells + v] == dInterior ? x[t * kCells + v] : 0.0f; }
-    __device__ float coef(int a, int t, int v) const { return c[(a * T + t) * kCells + v]; }
-    // negativeLap with the coarse-level halo (only empty or same-level active neighbours)
-    __device__ float neg_lap(int t, int v) const {
-        const float d = coef(3, t, v);
-        if (d == 0.0f) return 0.0f;
-        const int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
-        const int stride[3] = {64, 8, 1};
-        float s = xm(t, v) * d;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-#pragma unroll
-            for (int sg = 0; sg < 2; ++sg) {
-                int nt = t, nv = v;
-                if (sg == 0) {
-                    if (l[a] > 0) nv = v - stride[a];
-                    else { nt = nb[t * 6 + a]; nv = v + 7 * stride[a]; }
-                } else {
-                    if (l[a] < 7) nv = v + stride[a];
-                    else { nt = nb[t * 6 + 3 + a]; nv = v - 7 * stride[a]; }
-                }
-                float cf, xv;
-                if (sg == 0) cf = coef(a, t, v);
-                else cf = (nt < 0) ? h[tile_lvl(t)] : coef(a, nt, nv);
-                xv = (nt < 0) ? 0.0f : xm(nt, nv);
-                s = __fmaf_rn(cf, xv, s);
-            }
-        }
+    __device__ static int xi(int i, int j, int k) { return ((i + 1) * PD + (j + 1)) * PD + (k + 1); }
+    __device__ static int ci(int i, int j, int k) { return (i * N + j) * N + k; }
+    __device__ float neg_lap(int i, int j, int k) const {
+        const float dd = d[ci(i, j, k)];
+        if (dd == 0.0f) return 0.0f;
+        const int q = xi(i, j, k);
+        float s = x[q] * dd;
+        s = __fmaf_rn(c0[(i * N + j) * N + k], x[q - PD * PD], s);
+        s = __fmaf_rn(c0[((i + 1) * N + j) * N + k], x[q + PD * PD], s);
+        s = __fmaf_rn(c1[(i * (N + 1) + j) * N + k], x[q - PD], s);
+        s = __fmaf_rn(c1[(i * (N + 1) + j + 1) * N + k], x[q + PD], s);
+        s = __fmaf_rn(c2[(i * N + j) * (N + 1) + k], x[q - 1], s);
+        s = __fmaf_rn(c2[(i * N + j) * (N + 1) + k + 1], x[q + 1], s);
         return s;
     }
-    __device__ int tile_lvl(int t) const { return meta[t].x & 0xff; }
+    // one colour: the N^3/2 cells with (i+j+k)%2 == color, one per thread
+    __device__ void gs_pass(int color, const CoarseArgs& A) {
+        constexpr int half = N * N * N / 2;
+        for (int idx = threadIdx.x; idx < half; idx += blockDim.x) {
+            const int i = idx / (N * N / 2), j = (idx / (N / 2)) % N, kh = idx % (N / 2);
+            const int k = 2 * kh + ((i + j + color) & 1);
+            const int c = ci(i, j, k);
+            const float ax = neg_lap(i, j, k);
+            const float delta = (ty[c] & dInterior) ? __fdiv_rn(__fsub_rn(rhs[c], ax), d[c]) : 0.0f;
+            const float xs = x[xi(i, j, k)];
+            x[xi(i, j, k)] = A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega);
+        }
+        __syncthreads();
+    }
+    __device__ void gs(int iters, int order, const CoarseArgs& A) {
+        for (int it = 0; it < iters; ++it) {
+            gs_pass(order, A);
+            gs_pass(1 - order, A);
+        }
+    }
+    __device__ void clear_boundary_faces() {
+        for (int q = threadIdx.x; q < N * N; q += blockDim.x) {
+            const int a = q / N, b = q % N;
+            c0[(N * N + a) * N + b] = 0.0f;
+            c1[(a * (N + 1) + N) * N + b] = 0.0f;
+            c2[(a * N + b) * (N + 1) + N] = 0.0f;
+        }
+    }
 };
-
-__device__ void coarse_gs_pass(CoarseSmem& M, const CoarseArgs& A, int lb, int le, int color) {
-    const int total = (le - lb) * kCells;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int t = lb + (idx >> 9), v = idx & 511;
-        if ((((v >> 6) + ((v >> 3) & 7) + (v & 7)) & 1) != color) continue;
-        const float d = M.coef(3, t, v);
-        const float ax = M.neg_lap(t, v);
-        const float delta = (M.ty[t * kCells + v] & dInterior) ? __fdiv_rn(__fsub_rn(M.rhs[t * kCells + v], ax), d) : 0.0f;
-        const float xs = M.xm(t, v);
-        M.x[t * kCells + v] = A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega);
-    }
-    __syncthreads();
-}
-__device__ void coarse_gs(CoarseSmem& M, const CoarseArgs& A, int level, int iters, int order) {
-    const int lb = level == 0 ? 0 : A.l1b, le = level == 0 ? A.l1b : A.ntiles;
-    for (int it = 0; it < iters; ++it) {
-        coarse_gs_pass(M, A, lb, le, order);
-        coarse_gs_pass(M, A, lb, le, 1 - order);
-    }
-}
-__device__ void coarse_step0(CoarseSmem& M, const CoarseArgs& A) {
-    coarse_gs(M, A, 0, A.coarsest_iters / 2, 0);
-    coarse_gs(M, A, 0, A.coarsest_iters / 2, 1);
-}
+constexpr int kCoarseFloats = 18 * 18 * 18 + 3 * 17 * 16 * 16 + 3 * 4096 + 10 * 10 * 10 + 3 * 9 * 8 * 8 + 3 * 512;
+constexpr size_t kCoarseSmem = sizeof(float) * kCoarseFloats + sizeof(int) * 8 + 4096 + 512;
 
 __global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float* X, float* RHS, float* X0) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    const int T = A.ntiles;
-    CoarseSmem M;
-    M.T = T;
-    M.x = reinterpret_cast<float*>(smraw);
-    M.rhs = M.x + T * kCells;
-    M.x0 = M.rhs + T * kCells;
-    M.c = M.x0 + T * kCells;
-    M.meta = reinterpret_cast<int4*>(M.c + 4 * T * kCells);
-    M.nb = reinterpret_cast<int*>(M.meta + T);
-    M.child = M.nb + 6 * T;
-    M.ty = reinterpret_cast<uint8_t*>(M.child + 8);
-    M.h[0] = voxel_size(g.h0, 0);
-    M.h[1] = voxel_size(g.h0, 1);
-    const int tot = T * kCells;
-    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-        M.x[i] = X[i];
-        M.rhs[i] = RHS[i];
-        M.x0[i] = X0[i];
-        M.ty[i] = g.ctype[i];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) M.c[a * tot + i] = g.plane(A.coeff_ch + a)[i];
+    float* f = reinterpret_cast<float*>(smraw);
+    DenseLevel<16> L1;
+    DenseLevel<8> L0;
+    L1.x = f; f += 18 * 18 * 18;
+    L1.c0 = f; f += 17 * 256;
+    L1.c1 = f; f += 17 * 256;
+    L1.c2 = f; f += 17 * 256;
+    L1.d = f; f += 4096;
+    L1.rhs = f; f += 4096;
+    float* res = f; f += 4096;
+    L0.x = f; f += 1000;
+    L0.c0 = f; f += 576;
+    L0.c1 = f; f += 576;
+    L0.c2 = f; f += 576;
+    L0.d = f; f += 512;
+    L0.rhs = f; f += 512;
+    float* x00 = f; f += 512;
+    int* child = reinterpret_cast<int*>(f);
+    L1.ty = reinterpret_cast<uint8_t*>(child + 8);
+    L0.ty = L1.ty + 4096;
+    const int tid = threadIdx.x;
+    const float* C0 = g.plane(A.coeff_ch);
+    const float* C1 = g.plane(A.coeff_ch + 1);
+    const float* C2 = g.plane(A.coeff_ch + 2);
+    const float* C3 = g.plane(A.coeff_ch + 3);
+
+    for (int q = tid; q < 18 * 18 * 18; q += blockDim.x) L1.x[q] = 0.0f;
+    for (int q = tid; q < 1000; q += blockDim.x) L0.x[q] = 0.0f;
+    if (tid < 8) child[tid] = g.child[tid];
+    L1.clear_boundary_faces();
+    L0.clear_boundary_faces();
+    __syncthreads();
+    // root tile (tile 0)
+    for (int v = tid; v < kCells; v += blockDim.x) {
+        const int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+        const uint8_t t = g.ctype[v];
+        L0.ty[v] = t;
+        L0.d[v] = C3[v];
+        L0.c0[(i * 8 + j) * 8 + k] = C0[v];
+        L0.c1[(i * 9 + j) * 8 + k] = C1[v];
+        L0.c2[(i * 8 + j) * 9 + k] = C2[v];
+        L0.rhs[v] = RHS[v];
+        x00[v] = X0[v];
+        L0.x[DenseLevel<8>::xi(i, j, k)] = t == dInterior ? X[v] : 0.0f;
     }
-    for (int i = threadIdx.x; i < 6 * T; i += blockDim.x) {
-        const int nq = g.nb[8 * (i / 6) + (i % 6)];
-        M.nb[i] = (nq >= 0 && nq < T) ? nq : -1;
+    // the eight level-1 tiles as one 16^3 grid
+    if (A.top == 1) {
+        for (int idx = tid; idx < 8 * kCells; idx += blockDim.x) {
+            const int tci = idx >> 9, v = idx & 511;
+            const int tile = child[tci];
+            if (tile < 0) continue;
+            const size_t o = (size_t)tile * kCells + v;
+            const int I = ((tci >> 2) << 3) | (v >> 6), J = (((tci >> 1) & 1) << 3) | ((v >> 3) & 7), K = ((tci & 1) << 3) | (v & 7);
+            const int c = DenseLevel<16>::ci(I, J, K);
+            const uint8_t t = g.ctype[o];
+            L1.ty[c] = t;
+            L1.d[c] = C3[o];
+            L1.rhs[c] = RHS[o];
+            L1.c0[(I * 16 + J) * 16 + K] = C0[o];
+            L1.c1[(I * 17 + J) * 16 + K] = C1[o];
+            L1.c2[(I * 16 + J) * 17 + K] = C2[o];
+            L1.x[DenseLevel<16>::xi(I, J, K)] = t == dInterior ? X[o] : 0.0f;
+        }
     }
-    if (threadIdx.x < 8) M.child[threadIdx.x] = g.child[threadIdx.x];
-    for (int i = threadIdx.x; i < T; i += blockDim.x) M.meta[i] = g.meta[i];
     __syncthreads();
 
     if (A.top == 0) {
-        coarse_step0(M, A);
+        L0.gs(A.coarsest_iters / 2, 0, A);
+        L0.gs(A.coarsest_iters / 2, 1, A);
     } else {
-        coarse_gs(M, A, 1, A.level_iters, 0);
-        // residual on level 1 restricted to the root (ResidualAndRestrictAMG128Kernel)
-        for (int v0 = threadIdx.x; v0 < kCells; v0 += blockDim.x) {
-            const int l0 = v0 >> 6, l1 = (v0 >> 3) & 7, l2 = v0 & 7;
-            const int ct = M.child[(l0 >> 2) * 4 + (l1 >> 2) * 2 + (l2 >> 2)];
-            if (ct < A.l1b || ct >= T) continue;
-            const int b0 = (l0 & 3) << 1, b1 = (l1 & 3) << 1, b2 = (l2 & 3) << 1;
+        L1.gs(A.level_iters, 0, A);
+        // residual on level 1 (ResidualAndRestrictAMG128Kernel) ...
+        for (int c = tid; c < 4096; c += blockDim.x) {
+            const int I = c >> 8, J = (c >> 4) & 15, K = c & 15;
+            res[c] = __fsub_rn(L1.rhs[c], L1.neg_lap(I, J, K));
+        }
+        __syncthreads();
+        // ... restricted to the root: rhs = R * sum of 8 residuals, x = mean of 8 x
+        for (int v = tid; v < kCells; v += blockDim.x) {
+            const int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
             float rs = 0.0f, xs = 0.0f;
             for (int ii = 0; ii < 2; ++ii)
                 for (int jj = 0; jj < 2; ++jj)
                     for (int kk = 0; kk < 2; ++kk) {
-                        const int cv = cell_index(b0 + ii, b1 + jj, b2 + kk);
-                        rs = __fadd_rn(rs, __fsub_rn(M.rhs[ct * kCells + cv], M.neg_lap(ct, cv)));
-                        xs = __fadd_rn(xs, M.xm(ct, cv));
+                        rs = __fadd_rn(rs, res[DenseLevel<16>::ci(2 * i + ii, 2 * j + jj, 2 * k + kk)]);
+                        xs = __fadd_rn(xs, L1.x[DenseLevel<16>::xi(2 * i + ii, 2 * j + jj, 2 * k + kk)]);
                     }
-            M.rhs[v0] = __fmul_rn(rs, A.Rr);
-            M.x[v0] = __fdiv_rn(xs, 8.0f);
+            L0.rhs[v] = __fmul_rn(rs, A.Rr);
+            L0.x[DenseLevel<8>::xi(i, j, k)] = L0.ty[v] == dInterior ? __fdiv_rn(xs, 8.0f) : 0.0f;
         }
         __syncthreads();
         // FASSaveSolutionAndUpdateSource on the root
-        for (int v = threadIdx.x; v < kCells; v += blockDim.x) {
-            if (M.ty[v] & dInterior) {
-                const float lap = M.neg_lap(0, v);
-                M.rhs[v] = __fadd_rn(M.rhs[v], lap);
-                M.x0[v] = M.x[v];
+        for (int v = tid; v < kCells; v += blockDim.x) {
+            const int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+            if (L0.ty[v] & dInterior) {
+                L0.rhs[v] = __fadd_rn(L0.rhs[v], L0.neg_lap(i, j, k));
+                x00[v] = L0.x[DenseLevel<8>::xi(i, j, k)];
             } else {
-                M.rhs[v] = 0.0f;
+                L0.rhs[v] = 0.0f;
             }
         }
         __syncthreads();
-        for (int r = 0; r < A.mu; ++r) coarse_step0(M, A);
-        // FASProlongateAndUpdate on level 1 (LEAF or NONLEAF tiles only)
-        const int n1 = (T - A.l1b) * kCells;
-        for (int idx = threadIdx.x; idx < n1; idx += blockDim.x) {
-            const int t = A.l1b + (idx >> 9), v = idx & 511;
-            const int4 m = M.meta[t];
-            const int pv = cell_index(parent_local(m.y, v >> 6), parent_local(m.z, (v >> 3) & 7), parent_local(m.w, v & 7));
-            const float cx = M.x[pv], cx0 = M.x0[pv];
-            const int o = t * kCells + v;
-            M.x[o] = (M.ty[o] & dInterior) ? __fmaf_rn(A.P, __fsub_rn(cx, cx0), M.x[o]) : 0.0f;
+        for (int r = 0; r < A.mu; ++r) {
+            L0.gs(A.coarsest_iters / 2, 0, A);
+            L0.gs(A.coarsest_iters / 2, 1, A);
+        }
+        // FASProlongateAndUpdate on level 1
+        for (int c = tid; c < 4096; c += blockDim.x) {
+            const int I = c >> 8, J = (c >> 4) & 15, K = c & 15;
+            const int q = DenseLevel<16>::xi(I, J, K);
+            const float cx = L0.x[DenseLevel<8>::xi(I >> 1, J >> 1, K >> 1)];
+            const float cx0 = x00[DenseLevel<8>::ci(I >> 1, J >> 1, K >> 1)];
+            L1.x[q] = (L1.ty[c] & dInterior) ? __fmaf_rn(A.P, __fsub_rn(cx, cx0), L1.x[q]) : 0.0f;
         }
         __syncthreads();
-        coarse_gs(M, A, 1, A.level_iters, 1);
+        L1.gs(A.level_iters, 1, A);
     }
-    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-        X[i] = M.x[i];
-        RHS[i] = M.rhs[i];
-        X0[i] = M.x0[i];
+    for (int v = tid; v < kCells; v += blockDim.x) {
+        X[v] = L0.x[DenseLevel<8>::xi(v >> 6, (v >> 3) & 7, v & 7)];
+        RHS[v] = L0.rhs[v];
+        X0[v] = x00[v];
+    }
+    if (A.top == 1) {
+        for (int idx = tid; idx < 8 * kCells; idx += blockDim.x) {
+            const int tci = idx >> 9, v = idx & 511;
+            const int tile = child[tci];
+            if (tile < 0) continue;
+            const int I = ((tci >> 2) << 3) | (v >> 6), J = (((tci >> 1) & 1) << 3) | ((v >> 3) & 7), K = ((tci & 1) << 3) | (v & 7);
+            X[(size_t)tile * kCells + v] = L1.x[DenseLevel<16>::xi(I, J, K)];
+        }
     }
 }
 
@@ -858,15 +902,11 @@ void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RH
 void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st) {
     if (nt > 0) count_launch(), k_prolong<<<nt, 128, 0, st>>>(g, t0, X, X0, P);
 }
-size_t coarse_step_smem_bytes(int ntiles) {
-    return (size_t)ntiles * kCells * (7 * sizeof(float) + 1) + sizeof(int) * (6 * ntiles + 8) + sizeof(int4) * ntiles + 16;
-}
-void launch_coarse_step(const DevGrid& g, int top, int ntiles, int level1_begin, float* X, float* RHS, float* X0, int coeff_ch, int mu,
-                        int level_iters, int coarsest_iters, double omega, float Rr, float P, cudaStream_t st) {
+size_t coarse_step_smem_bytes() { return kCoarseSmem; }
+void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters,
+                        int coarsest_iters, double omega, float Rr, float P, cudaStream_t st) {
     CoarseArgs A;
     A.top = top;
-    A.ntiles = ntiles;
-    A.l1b = level1_begin;
     A.coeff_ch = coeff_ch;
     A.mu = mu;
     A.level_iters = level_iters;
@@ -876,8 +916,7 @@ void launch_coarse_step(const DevGrid& g, int top, int ntiles, int level1_begin,
     A.omega = omega;
     A.Rr = Rr;
     A.P = P;
-    const size_t smem = coarse_step_smem_bytes(ntiles);
-    count_launch(), k_coarse<<<1, 1024, smem, st>>>(g, A, X, RHS, X0);
+    count_launch(), k_coarse<<<1, 1024, kCoarseSmem, st>>>(g, A, X, RHS, X0);
 }
 void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
                        ReduceScratch rs, cudaStream_t st) {
@@ -912,7 +951,7 @@ void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, Red
 void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, bool use_handle, cudaStream_t st) {
     count_launch(), k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h, use_handle ? 1 : 0);
 }
-void init_kernel_attributes() { cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); }
+void init_kernel_attributes() { cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmem); }
 
 void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st) {
     if (nt > 0) count_launch(), k_ghost_types<<<nt, 128, 0, st>>>(g, t0);

@@ -29,10 +29,10 @@ void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int
 void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st);
 void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st);
 // Whole FASMuCycleStep of level `top` (0 or 1) in one thread block, the
-// coarse levels resident in shared memory.  ntiles = tiles of levels 0..top.
-void launch_coarse_step(const DevGrid& g, int top, int ntiles, int level1_begin, float* X, float* RHS, float* X0, int coeff_ch,
-                        int mu, int level_iters, int coarsest_iters, double omega, float R_restrict, float P, cudaStream_t st);
-size_t coarse_step_smem_bytes(int ntiles);
+// root and its eight children resident in shared memory as dense grids.
+void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters,
+                        int coarsest_iters, double omega, float R_restrict, float P, cudaStream_t st);
+size_t coarse_step_smem_bytes();
 
 // --- PCG on LEAF tiles (tile list) ---
 enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3 };

@@ -165,3 +165,26 @@ def test_reference_test_grids_solve(case_id, prm):
     assert rel <= 1e-6 and abs(it - ito) <= 1
     m = leaf_mask(G)
     assert rel_l2(G.download(0)[m], g.channel(0)[m]) <= 1e-5
+
+
+@pytest.mark.parametrize("L", [0, 1, 2])
+def test_shallow_trees_match_oracle(L):
+    """Trees of 1, 9 and 73 tiles: the coarse-level kernel runs the whole cycle (levels 0 and 1)."""
+    G, g, solver, b = setup_uniform(L)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    assert abs(it - ito) <= 1 and rel <= 1e-6
+    m = leaf_mask(G)
+    assert rel_l2(G.download(0)[m], g.channel(0)[m]) <= 1e-5
+
+
+def test_graph_and_stream_launch_modes_agree():
+    G, g, solver, b = setup_uniform(3, with_oracle=False)
+    it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x1 = G.download(0)
+    G.upload(1, b)
+    solver.set_launch_mode(False)
+    it2, rel2 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x2 = G.download(0)
+    assert it1 == it2 and rel1 == rel2
+    assert np.array_equal(x1, x2)
