@@ -152,7 +152,7 @@ def make_solver(cmg):
     s.mu_cycle_repeat_times = SOLVE["mu"]
     # CMG_SOLVE_MODE=stream launches kernel by kernel (for ncu launch lists)
     if os.environ.get("CMG_SOLVE_MODE", "graph") == "stream":
-        s.set_launch_mode(False)
+        s.set_launch_mode(use_graph=False)
     return s
 
 

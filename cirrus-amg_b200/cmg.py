@@ -281,9 +281,11 @@ class AMGSolver:
         except Exception:
             pass
 
-    def set_launch_mode(self, use_graph):
-        """True: one CUDA graph per solve (default); False: kernel-by-kernel launches."""
-        _check(self.L.cmg_amg_solver_set_launch_mode(self.h, int(bool(use_graph))), "set_launch_mode")
+    def set_launch_mode(self, use_graph=True, persistent=False):
+        """use_graph: one CUDA graph per solve (default) or kernel-by-kernel launches;
+        persistent: levels 2-3 of each cycle in one cooperative kernel (off by default)."""
+        flags = (1 if use_graph else 0) | (2 if persistent else 0)
+        _check(self.L.cmg_amg_solver_set_launch_mode(self.h, flags), "set_launch_mode")
 
     def _sync_params(self):
         _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")

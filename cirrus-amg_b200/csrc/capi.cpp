@@ -325,9 +325,10 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu) {
     s->s.mu = mu;
     return CMG_OK;
 }
-int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int use_graph) {
-    if (!s) return fail(CMG_ERR_INVALID, "null solver");
-    s->s.use_graph = use_graph != 0;
+int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags) {
+    if (!s || (flags & ~3)) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_launch_mode: bad argument");
+    s->s.use_graph = (flags & CMG_LAUNCH_GRAPH) != 0;
+    s->s.use_persist = (flags & CMG_LAUNCH_PERSISTENT) != 0 && s->s.persist_nblocks > 0;
     return CMG_OK;
 }
 int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,

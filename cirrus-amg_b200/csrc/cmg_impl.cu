@@ -36,6 +36,7 @@ Grid::~Grid() {
     dfree(meta);
     dfree(nb);
     dfree(child);
+    dfree(nbx);
     dfree(leaf);
     dfree(spheres);
     dfree(modes);
@@ -107,10 +108,19 @@ int Grid::ensure_device() {
         const TileRec& r = topo.tiles()[t];
         hm[t] = make_int4(r.level | (r.type << 8), r.c[0], r.c[1], r.c[2]);
     }
+    std::vector<int> hx((size_t)8 * n_new, 0);
+    for (int t = 0; t < n_new; ++t)
+        for (int f = 0; f < 6; ++f) {
+            const int q = topo.nb[8 * t + f];
+            if (q >= 0) hx[8 * t + f] = ((q + 1) << 3) | topo.tiles()[q].type;
+        }
     dfree(meta);
     dfree(nb);
     dfree(child);
+    dfree(nbx);
     dfree(leaf);
+    CK(cudaMalloc(&nbx, sizeof(int) * 8 * (n_new + 1)));
+    CK(cudaMemcpy(nbx, hx.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
     CK(cudaMalloc(&meta, sizeof(int4) * (n_new + 1)));
     CK(cudaMalloc(&nb, sizeof(int) * 8 * (n_new + 1)));
     CK(cudaMalloc(&child, sizeof(int) * 8 * (n_new + 1)));
@@ -174,6 +184,8 @@ Solver::~Solver() {
     dfree(partial2);
     dfree(s);
     if (h_s) cudaFreeHost(h_s);
+    if (h_bar) cudaFreeHost(h_bar);
+    dfree(bar);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -187,7 +199,12 @@ int Solver::init() {
     CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
+    CK(cudaMalloc(&bar, sizeof(unsigned int) * 4));
+    CK(cudaMemset(bar, 0, sizeof(unsigned int) * 4));
+    CK(cudaMallocHost(&h_bar, sizeof(unsigned int) * 4));
     init_kernel_attributes();
+    persist_nblocks = persist_blocks();
+    if (persist_nblocks <= 0) use_persist = false;
     return check_cuda(cudaGetLastError(), "kernel attributes");
 }
 
@@ -236,6 +253,19 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) c
     if (l <= 1) {
         launch_coarse_step(d, l, A.X, A.RHS, A.X0, A.coeff_ch, A.mu,
                            A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P, st);
+        return;
+    }
+    if (use_persist && l <= 3) {
+        int lb[4], ab[4], le[4], nlb[4];
+        for (int q = 0; q < 4; ++q) {
+            const bool has = q <= G.max_level();
+            lb[q] = has ? G.level_begin(q) : 0;
+            ab[q] = has ? G.ghost_begin(q) : 0;
+            le[q] = has ? G.level_end(q) : 0;
+            nlb[q] = has ? G.nonleaf_begin(q) : 0;
+        }
+        launch_persist_step(d, l, lb, ab, le, nlb, A.X, A.RHS, A.X0, A.coeff_ch, A.mu, A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P,
+                            bar, persist_nblocks, st);
         return;
     }
     enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st);
@@ -364,7 +394,7 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     }
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
-    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, sync_stride > 0 ? 1 : 0, omega};
+    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0), omega};
     Plan plan{};
     if (use_graph) {
         auto it = graphs.find(k);
@@ -405,6 +435,7 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     }
     CK(cudaEventRecord(ev1, st));
     CK(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_bar, bar, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     cudaEventElapsedTime(&last_ms, ev0, ev1);
@@ -429,6 +460,11 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     last_launches = use_graph ? plan.k_pre + (long long)r.iter * plan.k_body + (long long)(r.iter > 0 ? r.iter - 1 : 0) * plan.k_if
                               : stream_launches;
     if (verbose) std::printf("cmg AMG-PCG: %d iterations, relative residual %.6e, %.3f ms\n", n_it, rel_res, last_ms);
+    if (h_bar[2]) {
+        cudaMemsetAsync(bar, 0, sizeof(unsigned int) * 4, st);
+        set_error("solve: grid barrier of the persistent multigrid kernel timed out");
+        return 2;
+    }
     if (r.nonfinite) {
         set_error("solve: non-finite value in a PCG reduction");
         return 5;

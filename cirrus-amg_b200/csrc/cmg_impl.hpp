@@ -32,6 +32,7 @@ struct Grid {
     int4* meta = nullptr;
     int* nb = nullptr;
     int* child = nullptr;
+    int* nbx = nullptr;  // packed face neighbours, see DevGrid::nbx
     int* leaf = nullptr;
     int nleaf = 0;
     unsigned long long version = 0;
@@ -53,6 +54,7 @@ struct Grid {
         d.meta = meta;
         d.nb = nb;
         d.child = child;
+        d.nbx = nbx;
         return d;
     }
     float* plane(int c) const { return chan + (size_t)c * (size_t)n * kCells; }
@@ -115,7 +117,11 @@ struct Solver {
     void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
     void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
-    bool use_graph = true;  // false: launch kernel by kernel from the host (profiling)
+    bool use_graph = true;    // false: launch kernel by kernel from the host (profiling)
+    bool use_persist = false;  // levels 2-3 in one cooperative kernel per visit
+    int persist_nblocks = 0;
+    unsigned int* bar = nullptr;  // grid-barrier words of the persistent kernel
+    unsigned int* h_bar = nullptr;
     void enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_h, bool graph, cudaStream_t st) const;
     void enqueue_body(Grid& G, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool graph, cudaStream_t st) const;
     void enqueue_tail(Grid& G, const Key& k, cudaStream_t st) const;

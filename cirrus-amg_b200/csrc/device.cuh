@@ -27,6 +27,7 @@ struct DevGrid {
     const int4* meta;
     const int* nb;
     const int* child;
+    const int* nbx;  // [n][8]: face neighbours packed as (tile + 1) << 3 | tile type, 0 = none
     __host__ __device__ float* plane(int c) const { return chan + (size_t)c * (size_t)n * kCells; }
 };
 
@@ -81,6 +82,10 @@ struct Quad {
 };
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+// loads of fields other blocks of the same kernel may have written (the
+// persistent multi-level kernel): straight from L2, never a stale L1 line
+__device__ __forceinline__ float4 ldcg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ uchar4 ldt4(const uint8_t* p) { return *reinterpret_cast<const uchar4*>(p); }
 __device__ __forceinline__ float f4get(const float4& v, int u) { return u == 0 ? v.x : u == 1 ? v.y : u == 2 ? v.z : v.w; }
@@ -98,9 +103,10 @@ struct MgHalo {
     const uint8_t* ct;
     __device__ __forceinline__ float active(const DevGrid&, int qn, int nl, int) const {
         const size_t o = (size_t)qn * kCells + nl;
-        return ct[o] == dInterior ? X[o] : 0.0f;
+        const float v = ldcg(X + o);
+        return ct[o] == dInterior ? v : 0.0f;
     }
-    __device__ __forceinline__ float ghost(const DevGrid&, int qn, int nl) const { return X[(size_t)qn * kCells + nl]; }
+    __device__ __forceinline__ float ghost(const DevGrid&, int qn, int nl) const { return ldcg(X + (size_t)qn * kCells + nl); }
 };
 // LeafHalo: A*p on LEAF tiles.  The reference first writes GHOST cells from
 // their LEAF parents (PropagateToChildren, src/PoissonGrid.cu:377) and NONLEAF
@@ -111,7 +117,7 @@ struct LeafHalo {
     const uint8_t* ct;
     __device__ __forceinline__ float active(const DevGrid& g, int qn, int nl, int ntype) const {
         const size_t o = (size_t)qn * kCells + nl;
-        if (ntype & dLeaf) return ct[o] == dInterior ? X[o] : 0.0f;
+        if (ntype & dLeaf) return ct[o] == dInterior ? ldcg(X + o) : 0.0f;
         if (ct[o] != dInterior) return 0.0f;
         const int l0 = nl >> 6, l1 = (nl >> 3) & 7, l2 = nl & 7;
         const int c = g.child[8 * qn + (l0 >> 2) * 4 + (l1 >> 2) * 2 + (l2 >> 2)];
@@ -124,7 +130,7 @@ struct LeafHalo {
 #pragma unroll
             for (int jj = 0; jj < 2; ++jj)
 #pragma unroll
-                for (int kk = 0; kk < 2; ++kk) s = __fadd_rn(s, Xc[cell_index(b0 + ii, b1 + jj, b2 + kk)]);
+                for (int kk = 0; kk < 2; ++kk) s = __fadd_rn(s, ldcg(Xc + cell_index(b0 + ii, b1 + jj, b2 + kk)));
         return __fmul_rn(s, 0.125f);
     }
     __device__ __forceinline__ float ghost(const DevGrid& g, int qn, int nl) const {
@@ -132,24 +138,66 @@ struct LeafHalo {
         if (p < 0) return 0.0f;
         const int4 m = g.meta[qn];
         const int pv = cell_index(parent_local(m.y, nl >> 6), parent_local(m.z, (nl >> 3) & 7), parent_local(m.w, nl & 7));
-        return X[(size_t)p * kCells + pv];
+        return ldcg(X + (size_t)p * kCells + pv);
     }
+};
+
+// Barrier scopes of the tile code: the whole block (one tile per block) or
+// one 128-thread slot of a block that works on several tiles at once.
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct SlotSync {
+    int id;  // named barrier 1..15
+    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 };
 
 // Load the snapshot of tile t (128 threads).  Returns the thread's raw x,
 // cell types and diagonal for its four cells.  LoadAMGLaplacianTileData,
-// src/AMGSolver.cu:419-543.
-template <class Halo>
+// src/AMGSolver.cu:419-543.  Latency: the neighbour descriptors are the only
+// loads the halo values depend on, so the tile's own loads and the halo loads
+// are all in flight before the first barrier; only the GHOST extrapolation,
+// which needs the tile's own values, waits for it.
+template <class Halo, class Sync>
 __device__ __forceinline__ void load_snap(const DevGrid& g, int t, const float* X, int coeff_ch, const Halo& halo, Snap& S,
-                                          const Quad& Q, float4& xr, uchar4& ty, float4& dg) {
+                                          const Quad& Q, float4& xr, uchar4& ty, float4& dg, const Sync& sync) {
     const float* C0 = g.plane(coeff_ch);
     const float* C1 = g.plane(coeff_ch + 1);
     const float* C2 = g.plane(coeff_ch + 2);
     const float* C3 = g.plane(coeff_ch + 3);
-    xr = ld4(X + Q.base);
+    // halo cell r of this thread: face f = hh / 64 (axis f/2, side f%2), cell (a, b) on the face
+    int desc[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int f = (Q.q + 128 * r) >> 6;
+        desc[r] = g.nbx[8 * t + (f >> 1) + 3 * (f & 1)];
+    }
+    xr = ldcg4(X + Q.base);
     ty = ldt4(g.ctype + Q.base);
     const float4 a0 = ld4(C0 + Q.base), a1 = ld4(C1 + Q.base), a2 = ld4(C2 + Q.base);
     dg = ld4(C3 + Q.base);
+    const float h = voxel_size(g.h0, tile_level(g, t));
+    float hv[3], hc[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int hh = Q.q + 128 * r;
+        const int f = hh >> 6, fi = hh & 63;
+        const int axis = f >> 1, s = f & 1;
+        const int a = fi >> 3, b = fi & 7;
+        int nlc[3];
+        nlc[axis] = s ? 0 : 7;
+        if (axis == 0) { nlc[1] = a; nlc[2] = b; }
+        else if (axis == 1) { nlc[0] = a; nlc[2] = b; }
+        else { nlc[0] = a; nlc[1] = b; }
+        const int nl = cell_index(nlc[0], nlc[1], nlc[2]);
+        hv[r] = 0.0f;
+        hc[r] = h;
+        if (desc[r] != 0) {
+            const int qn = (desc[r] >> 3) - 1, ntype = desc[r] & 7;
+            hv[r] = (ntype & dGhost) ? halo.ghost(g, qn, nl) : halo.active(g, qn, nl, ntype);
+            if (s) hc[r] = g.plane(coeff_ch + axis)[(size_t)qn * kCells + nl];
+        }
+    }
     const int s0 = sx(Q.i, Q.j, Q.k0);
     S.x[s0 + 0] = ty.x == dInterior ? xr.x : 0.0f;
     S.x[s0 + 1] = ty.y == dInterior ? xr.y : 0.0f;
@@ -162,9 +210,8 @@ __device__ __forceinline__ void load_snap(const DevGrid& g, int t, const float* 
     S.c2[c2o + 1] = a2.y;
     S.c2[c2o + 2] = a2.z;
     S.c2[c2o + 3] = a2.w;
-    __syncthreads();
+    sync();
 
-    const float h = voxel_size(g.h0, tile_level(g, t));
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         const int hh = Q.q + 128 * r;
@@ -178,36 +225,26 @@ __device__ __forceinline__ void load_snap(const DevGrid& g, int t, const float* 
         else { fl[0] = a; fl[1] = b; fl[2] = axk; }
         cl[0] = fl[0]; cl[1] = fl[1]; cl[2] = fl[2];
         cl[axis] = s ? 7 : 0;
-        int nlc[3] = {cl[0], cl[1], cl[2]};
-        nlc[axis] = s ? 0 : 7;
-        const int nl = cell_index(nlc[0], nlc[1], nlc[2]);
         const int fx = sx(fl[0], fl[1], fl[2]);
-        const int qn = g.nb[8 * t + axis + 3 * s];
-        float* cslot = nullptr;
-        if (s) cslot = axis == 0 ? &S.c0[8 * 64 + a * 8 + b] : axis == 1 ? &S.c1[a * 72 + 64 + b] : &S.c2[a * 72 + b * 9 + 8];
-        if (qn < 0) {
-            S.x[fx] = 0.0f;
-            if (s) *cslot = h;
-        } else {
-            const int ntype = tile_type(g, qn);
-            if (ntype & dGhost) {
-                float avg = 0.0f;
+        float v = hv[r];
+        if (desc[r] != 0 && (desc[r] & dGhost)) {
+            float avg = 0.0f;
 #pragma unroll
-                for (int di = 0; di < 2; ++di)
+            for (int di = 0; di < 2; ++di)
 #pragma unroll
-                    for (int dj = 0; dj < 2; ++dj)
+                for (int dj = 0; dj < 2; ++dj)
 #pragma unroll
-                        for (int dk = 0; dk < 2; ++dk) avg = __fadd_rn(avg, S.x[sx(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)]);
-                avg = __fdiv_rn(avg, 8.0f);
-                const float V1 = halo.ghost(g, qn, nl);
-                S.x[fx] = __fmaf_rn(0.5f, __fsub_rn(V1, avg), S.x[sx(cl[0], cl[1], cl[2])]);
-            } else {
-                S.x[fx] = halo.active(g, qn, nl, ntype);
-            }
-            if (s) *cslot = g.plane(coeff_ch + axis)[(size_t)qn * kCells + nl];
+                    for (int dk = 0; dk < 2; ++dk) avg = __fadd_rn(avg, S.x[sx(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)]);
+            avg = __fdiv_rn(avg, 8.0f);
+            v = __fmaf_rn(0.5f, __fsub_rn(hv[r], avg), S.x[sx(cl[0], cl[1], cl[2])]);
+        }
+        S.x[fx] = v;
+        if (s) {
+            float* cslot = axis == 0 ? &S.c0[8 * 64 + a * 8 + b] : axis == 1 ? &S.c1[a * 72 + 64 + b] : &S.c2[a * 72 + b * 9 + 8];
+            *cslot = hc[r];
         }
     }
-    __syncthreads();
+    sync();
 }
 
 // Block-wide deterministic double reduction for 128 threads; result valid in thread 0.

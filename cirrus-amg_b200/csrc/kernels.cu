@@ -40,19 +40,26 @@ __device__ __forceinline__ double dot4(const float4& a, const float4& b) {
 }
 
 // ---------------------------------------------------------------------------
-// multigrid
+// multigrid: one 8^3 tile per 128-thread group.  The tile_* functions are
+// shared by the one-tile-per-block kernels and the persistent kernel that
+// runs several tiles per block; `sync` is the barrier of the 128 threads.
+// Each ends with a barrier so the snapshot can be reused for the next tile.
 // ---------------------------------------------------------------------------
+struct SmoothArgs {
+    int coeff_ch, exact;
+    float om;
+    double omega;
+};
+
 // NegativeLaplacianAndGaussSeidelSameLevelAMG128Kernel (src/AMGSolver.cu:838-877)
-template <bool kExactOmega>
-__global__ void __launch_bounds__(128) k_gs(DevGrid g, int t0, float* X, const float* B, int coeff_ch, int color, float om,
-                                            double omega) {
-    __shared__ Snap S;
-    const int t = t0 + blockIdx.x;
-    const Quad Q(t, threadIdx.x);
+template <class Sync>
+__device__ __forceinline__ void tile_gs(const DevGrid& g, int t, int tid, float* X, const float* B, int color, const SmoothArgs& A,
+                                        Snap& S, const Sync& sync) {
+    const Quad Q(t, tid);
     float4 xr, dg;
     uchar4 ty;
-    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg);
-    const float4 b = ld4(B + Q.base);
+    load_snap(g, t, X, A.coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg, sync);
+    const float4 b = ldcg4(B + Q.base);
     float4 out = xr;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -62,26 +69,26 @@ __global__ void __launch_bounds__(128) k_gs(DevGrid g, int t0, float* X, const f
         const float ax = snap_neg_lap(S, Q.i, Q.j, k, d);
         const float delta = (t4get(ty, u) & dInterior) ? __fdiv_rn(__fsub_rn(f4get(b, u), ax), d) : 0.0f;
         const float xs = S.x[sx(Q.i, Q.j, k)];
-        f4set(out, u, kExactOmega ? __fmaf_rn(delta, om, xs) : (float)((double)xs + (double)delta * omega));
+        f4set(out, u, A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega));
     }
     st4(X + Q.base, out);
+    sync();
 }
 
 // ResidualAndRestrictAMG128Kernel (src/AMGSolver.cu:896-960)
-__global__ void __launch_bounds__(128) k_restrict(DevGrid g, int t0, float* X, float* RHS, int coeff_ch, float Rr) {
-    __shared__ Snap S;
-    __shared__ float res[kCells];
-    const int t = t0 + blockIdx.x;
-    const Quad Q(t, threadIdx.x);
+template <class Sync>
+__device__ __forceinline__ void tile_restrict(const DevGrid& g, int t, int tid, float* X, float* RHS, int coeff_ch, float Rr, Snap& S,
+                                              float* res, const Sync& sync) {
+    const Quad Q(t, tid);
     float4 xr, dg;
     uchar4 ty;
-    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg);
-    const float4 rh = ld4(RHS + Q.base);
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg, sync);
+    const float4 rh = ldcg4(RHS + Q.base);
 #pragma unroll
     for (int u = 0; u < 4; ++u) res[4 * Q.q + u] = __fsub_rn(f4get(rh, u), snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u)));
-    __syncthreads();
-    if (threadIdx.x < 64) {
-        const int b = threadIdx.x;
+    sync();
+    if (tid < 64) {
+        const int b = tid;
         const int f0 = (b >> 4) * 2, f1 = ((b >> 2) & 3) * 2, f2 = (b & 3) * 2;
         float rs = 0.0f, xs = 0.0f;
 #pragma unroll
@@ -101,17 +108,18 @@ __global__ void __launch_bounds__(128) k_restrict(DevGrid g, int t0, float* X, f
             X[o] = __fdiv_rn(xs, 8.0f);
         }
     }
+    sync();
 }
 
 // FASSaveSolutionAndUpdateSource128Kernel (src/AMGSolver.cu:1176-1206)
-__global__ void __launch_bounds__(128) k_fas_save(DevGrid g, int t0, const float* X, float* RHS, float* X0, int coeff_ch) {
-    __shared__ Snap S;
-    const int t = t0 + blockIdx.x;
-    const Quad Q(t, threadIdx.x);
+template <class Sync>
+__device__ __forceinline__ void tile_fas_save(const DevGrid& g, int t, int tid, const float* X, float* RHS, float* X0, int coeff_ch,
+                                              Snap& S, const Sync& sync) {
+    const Quad Q(t, tid);
     float4 xr, dg;
     uchar4 ty;
-    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg);
-    float4 rh = ld4(RHS + Q.base);
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg, sync);
+    float4 rh = ldcg4(RHS + Q.base);
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         if (t4get(ty, u) & dInterior) {
@@ -122,16 +130,16 @@ __global__ void __launch_bounds__(128) k_fas_save(DevGrid g, int t0, const float
         }
     }
     st4(RHS + Q.base, rh);
+    sync();
 }
 
-// FASProlongateAndUpdateAMG128Kernel (src/AMGSolver.cu:1216-1248)
-__global__ void __launch_bounds__(128) k_prolong(DevGrid g, int t0, float* X, const float* X0, float P) {
-    const int t = t0 + blockIdx.x;
-    const Quad Q(t, threadIdx.x);
+// FASProlongateAndUpdateAMG128Kernel (src/AMGSolver.cu:1216-1248); no snapshot
+__device__ __forceinline__ void tile_prolong(const DevGrid& g, int t, int tid, float* X, const float* X0, float P) {
+    const Quad Q(t, tid);
     const int4 m = g.meta[t];
     const bool ghost = (m.x >> 8) & dGhost;
     const int p = g.nb[8 * t + 6];
-    const float4 xr = ld4(X + Q.base);
+    const float4 xr = ldcg4(X + Q.base);
     const uchar4 ty = ldt4(g.ctype + Q.base);
     const int pi = parent_local(m.y, Q.i), pj = parent_local(m.z, Q.j);
     float4 out;
@@ -140,13 +148,30 @@ __global__ void __launch_bounds__(128) k_prolong(DevGrid g, int t0, float* X, co
         float cx = 0.0f, cx0 = 0.0f;
         if (p >= 0) {
             const size_t o = (size_t)p * kCells + cell_index(pi, pj, parent_local(m.w, Q.k0 + u));
-            cx = X[o];
-            cx0 = X0[o];
+            cx = ldcg(X + o);
+            cx0 = ldcg(X0 + o);
         }
         const bool in = t4get(ty, u) & dInterior;
         f4set(out, u, ghost ? (in ? cx : 0.0f) : (in ? __fmaf_rn(P, __fsub_rn(cx, cx0), f4get(xr, u)) : 0.0f));
     }
     st4(X + Q.base, out);
+}
+
+__global__ void __launch_bounds__(128) k_gs(DevGrid g, int t0, float* X, const float* B, int color, SmoothArgs A) {
+    __shared__ Snap S;
+    tile_gs(g, t0 + blockIdx.x, threadIdx.x, X, B, color, A, S, BlockSync{});
+}
+__global__ void __launch_bounds__(128) k_restrict(DevGrid g, int t0, float* X, float* RHS, int coeff_ch, float Rr) {
+    __shared__ Snap S;
+    __shared__ float res[kCells];
+    tile_restrict(g, t0 + blockIdx.x, threadIdx.x, X, RHS, coeff_ch, Rr, S, res, BlockSync{});
+}
+__global__ void __launch_bounds__(128) k_fas_save(DevGrid g, int t0, const float* X, float* RHS, float* X0, int coeff_ch) {
+    __shared__ Snap S;
+    tile_fas_save(g, t0 + blockIdx.x, threadIdx.x, X, RHS, X0, coeff_ch, S, BlockSync{});
+}
+__global__ void __launch_bounds__(128) k_prolong(DevGrid g, int t0, float* X, const float* X0, float P) {
+    tile_prolong(g, t0 + blockIdx.x, threadIdx.x, X, X0, P);
 }
 
 // ---------------------------------------------------------------------------
@@ -224,8 +249,8 @@ struct DenseLevel {
 constexpr int kCoarseFloats = 18 * 18 * 18 + 3 * 17 * 16 * 16 + 3 * 4096 + 10 * 10 * 10 + 3 * 9 * 8 * 8 + 3 * 512;
 constexpr size_t kCoarseSmem = sizeof(float) * kCoarseFloats + sizeof(int) * 8 + 4096 + 512;
 
-__global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float* X, float* RHS, float* X0) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+// the whole coarse sub-cycle by the calling block (any multiple of 32 threads)
+__device__ void coarse_dense(const DevGrid& g, const CoarseArgs& A, float* X, float* RHS, float* X0, unsigned char* smraw) {
     float* f = reinterpret_cast<float*>(smraw);
     DenseLevel<16> L1;
     DenseLevel<8> L0;
@@ -267,9 +292,9 @@ __global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float*
         L0.c0[(i * 8 + j) * 8 + k] = C0[v];
         L0.c1[(i * 9 + j) * 8 + k] = C1[v];
         L0.c2[(i * 8 + j) * 9 + k] = C2[v];
-        L0.rhs[v] = RHS[v];
-        x00[v] = X0[v];
-        L0.x[DenseLevel<8>::xi(i, j, k)] = t == dInterior ? X[v] : 0.0f;
+        L0.rhs[v] = ldcg(RHS + v);
+        x00[v] = ldcg(X0 + v);
+        L0.x[DenseLevel<8>::xi(i, j, k)] = t == dInterior ? ldcg(X + v) : 0.0f;
     }
     // the eight level-1 tiles as one 16^3 grid
     if (A.top == 1) {
@@ -283,11 +308,11 @@ __global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float*
             const uint8_t t = g.ctype[o];
             L1.ty[c] = t;
             L1.d[c] = C3[o];
-            L1.rhs[c] = RHS[o];
+            L1.rhs[c] = ldcg(RHS + o);
             L1.c0[(I * 16 + J) * 16 + K] = C0[o];
             L1.c1[(I * 17 + J) * 16 + K] = C1[o];
             L1.c2[(I * 16 + J) * 17 + K] = C2[o];
-            L1.x[DenseLevel<16>::xi(I, J, K)] = t == dInterior ? X[o] : 0.0f;
+            L1.x[DenseLevel<16>::xi(I, J, K)] = t == dInterior ? ldcg(X + o) : 0.0f;
         }
     }
     __syncthreads();
@@ -357,6 +382,125 @@ __global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float*
             X[(size_t)tile * kCells + v] = L1.x[DenseLevel<16>::xi(I, J, K)];
         }
     }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float* X, float* RHS, float* X0) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    coarse_dense(g, A, X, RHS, X0, smraw);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent kernel for the middle of the hierarchy: FASMuCycleStep of level
+// 2 or 3 (all of its mu-recursions) in one cooperative launch.  Each block
+// runs four 128-thread slots on four tiles at once; phases (a colour sweep,
+// restriction, FAS update, prolongation of one level) are separated by a
+// grid barrier, and levels 0-1 run in block 0 with the dense coarse code.
+// The barrier spin is bounded: past the limit the kernel records an error
+// and every block returns.
+// ---------------------------------------------------------------------------
+struct PersistArgs {
+    int top;
+    int lb[4], ab[4], le[4], nlb[4];  // level begin, active end (first GHOST), level end, first NONLEAF
+    int mu, level_iters, coarsest_iters;
+    SmoothArgs sm;
+    CoarseArgs co;
+    float Rr, P;
+    float *X, *RHS, *X0;
+    unsigned int* bar;  // [0] arrivals, [1] generation, [2] error flag
+};
+constexpr int kSlots = 4;
+constexpr size_t kPersistSmem = kCoarseSmem + kSlots * (sizeof(Snap) + sizeof(float) * kCells);
+
+__device__ bool grid_sync(const PersistArgs& A) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = A.bar + 1;
+        const unsigned int g0 = *gen;
+        __threadfence();
+        if (atomicAdd(A.bar, 1u) == gridDim.x - 1) {
+            A.bar[0] = 0;
+            __threadfence();
+            atomicAdd(A.bar + 1, 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*gen == g0) {
+                if (++spins > (1u << 24)) {  // ~1 s
+                    atomicExch(A.bar + 2, 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *((volatile unsigned int*)A.bar + 2) == 0;
+}
+
+struct PersistCtx {
+    DevGrid g;
+    PersistArgs A;
+    Snap* S;
+    float* res;
+    unsigned char* coarse_smem;
+    int slot, tid, gslot, nslot;
+    SlotSync sync;
+};
+
+__device__ bool p_gs(PersistCtx& C, int l, int iters, int order) {
+    for (int it = 0; it < iters; ++it)
+        for (int h = 0; h < 2; ++h) {
+            const int color = h ? 1 - order : order;
+            for (int t = C.A.lb[l] + C.gslot; t < C.A.ab[l]; t += C.nslot) tile_gs(C.g, t, C.tid, C.A.X, C.A.RHS, color, C.A.sm, *C.S, C.sync);
+            if (!grid_sync(C.A)) return false;
+        }
+    return true;
+}
+__device__ bool p_restrict_and_save(PersistCtx& C, int l) {
+    for (int t = C.A.lb[l] + C.gslot; t < C.A.ab[l]; t += C.nslot)
+        tile_restrict(C.g, t, C.tid, C.A.X, C.A.RHS, C.A.sm.coeff_ch, C.A.Rr, *C.S, C.res, C.sync);
+    if (!grid_sync(C.A)) return false;
+    for (int t = C.A.nlb[l - 1] + C.gslot; t < C.A.ab[l - 1]; t += C.nslot)
+        tile_fas_save(C.g, t, C.tid, C.A.X, C.A.RHS, C.A.X0, C.A.sm.coeff_ch, *C.S, C.sync);
+    return grid_sync(C.A);
+}
+__device__ bool p_prolong(PersistCtx& C, int l) {
+    for (int t = C.A.lb[l] + C.gslot; t < C.A.le[l]; t += C.nslot) tile_prolong(C.g, t, C.tid, C.A.X, C.A.X0, C.A.P);
+    return grid_sync(C.A);
+}
+__device__ bool p_step1(PersistCtx& C) {
+    if (blockIdx.x == 0) coarse_dense(C.g, C.A.co, C.A.X, C.A.RHS, C.A.X0, C.coarse_smem);
+    return grid_sync(C.A);
+}
+__device__ bool p_step2(PersistCtx& C) {
+    if (!p_gs(C, 2, C.A.level_iters, 0) || !p_restrict_and_save(C, 2)) return false;
+    for (int r = 0; r < C.A.mu; ++r)
+        if (!p_step1(C)) return false;
+    return p_prolong(C, 2) && p_gs(C, 2, C.A.level_iters, 1);
+}
+__device__ bool p_step3(PersistCtx& C) {
+    if (!p_gs(C, 3, C.A.level_iters, 0) || !p_restrict_and_save(C, 3)) return false;
+    for (int r = 0; r < C.A.mu; ++r)
+        if (!p_step2(C)) return false;
+    return p_prolong(C, 3) && p_gs(C, 3, C.A.level_iters, 1);
+}
+
+__global__ void __launch_bounds__(512) k_persist(DevGrid g, PersistArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    PersistCtx C;
+    C.g = g;
+    C.A = A;
+    C.slot = threadIdx.x >> 7;
+    C.tid = threadIdx.x & 127;
+    C.gslot = blockIdx.x * kSlots + C.slot;
+    C.nslot = gridDim.x * kSlots;
+    C.coarse_smem = smraw;
+    C.S = reinterpret_cast<Snap*>(smraw + kCoarseSmem) + C.slot;
+    C.res = reinterpret_cast<float*>(smraw + kCoarseSmem + kSlots * sizeof(Snap)) + C.slot * kCells;
+    C.sync = SlotSync{1 + C.slot};
+    if (A.top == 3) p_step3(C);
+    else p_step2(C);
 }
 
 // ---------------------------------------------------------------------------
@@ -372,7 +516,7 @@ __global__ void __launch_bounds__(128) k_leaf_apply(DevGrid g, const int* leaf, 
     const Quad Q(t, threadIdx.x);
     float4 xr, dg;
     uchar4 ty;
-    load_snap(g, t, P, coeff_ch, LeafHalo{P, g.ctype}, S, Q, xr, ty, dg);
+    load_snap(g, t, P, coeff_ch, LeafHalo{P, g.ctype}, S, Q, xr, ty, dg, BlockSync{});
     float4 ap;
 #pragma unroll
     for (int u = 0; u < 4; ++u)
@@ -889,9 +1033,12 @@ long long kernel_launch_count() { return g_launches.load(std::memory_order_relax
 
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st) {
     if (nt <= 0) return;
-    const float om = (float)omega;
-    if ((double)om == omega) count_launch(), k_gs<true><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
-    else count_launch(), k_gs<false><<<nt, 128, 0, st>>>(g, t0, X, B, coeff_ch, color, om, omega);
+    SmoothArgs A;
+    A.coeff_ch = coeff_ch;
+    A.om = (float)omega;
+    A.exact = ((double)A.om == omega);
+    A.omega = omega;
+    count_launch(), k_gs<<<nt, 128, 0, st>>>(g, t0, X, B, color, A);
 }
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st) {
     if (nt > 0) count_launch(), k_restrict<<<nt, 128, 0, st>>>(g, t0, X, RHS, coeff_ch, Rr);
@@ -951,7 +1098,64 @@ void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, Red
 void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, bool use_handle, cudaStream_t st) {
     count_launch(), k_loop_gate<<<1, 1, 0, st>>>(rs, loop_h, use_handle ? 1 : 0);
 }
-void init_kernel_attributes() { cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmem); }
+void init_kernel_attributes() {
+    cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmem);
+    cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPersistSmem);
+}
+int persist_blocks() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist, 512, kPersistSmem);
+    return per_sm > 0 ? sms * per_sm : 0;
+}
+cudaError_t launch_persist_step(const DevGrid& g, int top, const int* lb, const int* ab, const int* le, const int* nlb, float* X, float* RHS,
+                                float* X0, int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float Rr, float P,
+                                unsigned int* bar, int nblocks, cudaStream_t st) {
+    PersistArgs A;
+    A.top = top;
+    for (int l = 0; l < 4; ++l) {
+        A.lb[l] = lb[l];
+        A.ab[l] = ab[l];
+        A.le[l] = le[l];
+        A.nlb[l] = nlb[l];
+    }
+    A.mu = mu;
+    A.level_iters = level_iters;
+    A.coarsest_iters = coarsest_iters;
+    A.sm.coeff_ch = coeff_ch;
+    A.sm.om = (float)omega;
+    A.sm.exact = ((double)A.sm.om == omega);
+    A.sm.omega = omega;
+    A.co.top = 1;
+    A.co.coeff_ch = coeff_ch;
+    A.co.mu = mu;
+    A.co.level_iters = level_iters;
+    A.co.coarsest_iters = coarsest_iters;
+    A.co.om = A.sm.om;
+    A.co.exact = A.sm.exact;
+    A.co.omega = omega;
+    A.co.Rr = Rr;
+    A.co.P = P;
+    A.Rr = Rr;
+    A.P = P;
+    A.X = X;
+    A.RHS = RHS;
+    A.X0 = X0;
+    A.bar = bar;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = kPersistSmem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    count_launch();
+    return cudaLaunchKernelEx(&cfg, k_persist, g, A);
+}
 
 void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st) {
     if (nt > 0) count_launch(), k_ghost_types<<<nt, 128, 0, st>>>(g, t0);

@@ -33,6 +33,13 @@ void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0,
 void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters,
                         int coarsest_iters, double omega, float R_restrict, float P, cudaStream_t st);
 size_t coarse_step_smem_bytes();
+// FASMuCycleStep of level `top` (2 or 3) with all its recursions in one
+// cooperative launch of `nblocks` co-resident blocks; bar = 3 zeroed words
+// (barrier count, generation, error flag).  Level ranges indexed by level 0..3.
+cudaError_t launch_persist_step(const DevGrid& g, int top, const int* lb, const int* ab, const int* le, const int* nlb, float* X, float* RHS,
+                                float* X0, int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float R_restrict,
+                                float P, unsigned int* bar, int nblocks, cudaStream_t st);
+int persist_blocks();  // co-resident blocks of the persistent kernel on the current device
 
 // --- PCG on LEAF tiles (tile list) ---
 enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3 };

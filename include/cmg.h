@@ -129,11 +129,16 @@ int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float 
 int cmg_amg_solver_destroy(cmg_amg_solver* s);
 /* public fields omega / mu_cycle_repeat_times (src/AMGSolver.h:306-307) */
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
-/* 1 (default): the solve runs as one CUDA graph with a device-side loop;
- * 0: the same kernels launched one by one with the loop test on the host,
- * for profilers that do not enter conditional graph nodes.  No counterpart
- * in the reference, which always launches from the host. */
-int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int use_graph);
+/* Launch flags (default CMG_LAUNCH_GRAPH).
+ * GRAPH: the solve runs as one CUDA graph with a device-side while loop;
+ * without it the same kernels are launched one by one with the loop test on
+ * the host (for profilers that do not enter conditional graph nodes).
+ * PERSISTENT: each visit of multigrid level 2 or 3 runs as one cooperative
+ * kernel with grid barriers; without it, one kernel per phase.  No
+ * counterpart in the reference, which launches every phase from the host. */
+#define CMG_LAUNCH_GRAPH 1
+#define CMG_LAUNCH_PERSISTENT 2
+int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
 /* AMGSolver::solve (src/AMGSolver.cu:1399): solves -lap x = b, b read from
  * channel 1 and overwritten by the residual, x written to channel 0.
  * iters/rel_res are the reference's (num_iters, relative_residual), with

@@ -188,3 +188,22 @@ def test_graph_and_stream_launch_modes_agree():
     x2 = G.download(0)
     assert it1 == it2 and rel1 == rel2
     assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("shell", [False, True])
+def test_persistent_levels_match_per_phase_launches(shell):
+    """Levels 2-3 in one cooperative kernel give bit-identical results to one launch per phase."""
+    if shell:
+        G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5), with_oracle=False)
+        b = G.download(1)
+    else:
+        G, g, solver, b = setup_uniform(3, with_oracle=False)
+    solver.set_launch_mode(use_graph=True, persistent=False)
+    it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x1 = G.download(0)
+    G.upload(1, b)
+    solver.set_launch_mode(use_graph=True, persistent=True)
+    it2, rel2 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x2 = G.download(0)
+    assert (it1, rel1) == (it2, rel2)
+    assert np.array_equal(x1, x2)
