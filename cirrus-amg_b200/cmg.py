@@ -38,7 +38,8 @@ EXPORTS = [
     "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_copy_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
-    "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_full_neg_lap", "cmg_amg_dot",
+    "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_add_gradient_to_face", "cmg_amg_full_neg_lap",
+    "cmg_amg_dot",
     "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solver_set_launch_mode",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
@@ -91,6 +92,7 @@ def lib():
             "cmg_amg_cutcell_sphere_coeffs": (I, [P, I, F, I, P]),
             "cmg_amg_face_velocity_fourier": (I, [P, I, I, P, P, P]),
             "cmg_amg_divergence": (I, [P, I, I, I]),
+            "cmg_amg_add_gradient_to_face": (I, [P, I, I, I]),
             "cmg_amg_full_neg_lap": (I, [P, I, I, I]),
             "cmg_amg_dot": (I, [P, I, I, P]),
             "cmg_amg_solver_create": (I, [I, F, F, F, PP]),
@@ -249,6 +251,9 @@ class HADeviceGrid:
 
     def divergence(self, u_ch, coeff_ch, out_ch):
         _check(self.L.cmg_amg_divergence(self.h, u_ch, coeff_ch, out_ch), "divergence")
+
+    def add_gradient_to_face(self, x_ch, coeff_ch, u_ch):
+        _check(self.L.cmg_amg_add_gradient_to_face(self.h, x_ch, coeff_ch, u_ch), "add_gradient_to_face")
 
     def full_neg_lap(self, x_ch, coeff_ch, ax_ch):
         _check(self.L.cmg_amg_full_neg_lap(self.h, x_ch, coeff_ch, ax_ch), "full_neg_lap")

@@ -271,6 +271,15 @@ int cmg_amg_divergence(cmg_grid* g, int u_ch, int coeff_ch, int out_ch) {
     cmg::launch_divergence(d, G.leaf, G.nleaf, u_ch, coeff_ch, out_ch, G.stream);
     return cmg::check_cuda(cudaGetLastError(), "divergence");
 }
+int cmg_amg_add_gradient_to_face(cmg_grid* g, int x_ch, int coeff_ch, int u_ch) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (!chan_ok(g, x_ch) || u_ch < 0 || u_ch + 3 > g->g.nch || coeff_ch < 0 || coeff_ch + 4 > g->g.nch)
+        return fail(CMG_ERR_INVALID, "cmg_amg_add_gradient_to_face: channel out of range");
+    cmg::Grid& G = g->g;
+    cmg::launch_propagate_ghost(G.dev(), 0, G.n, x_ch, G.stream);
+    cmg::launch_gradient(G.dev(), G.plane(x_ch), coeff_ch, u_ch, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "add_gradient_to_face");
+}
 int cmg_amg_full_neg_lap(cmg_grid* g, int x_ch, int coeff_ch, int ax_ch) {
     if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
     if (!chan_ok(g, x_ch) || !chan_ok(g, ax_ch) || coeff_ch < 0 || coeff_ch + 4 > g->g.nch)

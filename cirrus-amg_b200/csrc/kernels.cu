@@ -1000,6 +1000,33 @@ __global__ void k_divergence(DevGrid g, const int* leaf, int u_ch, int coeff_ch,
     }
 }
 
+// AMGAddGradientToFace128Kernel (src/AMGSolver.cu:634-678) on LEAF and GHOST
+// tiles; GHOST values must already hold their parents' (k_propagate_ghost).
+__global__ void __launch_bounds__(128) k_gradient(DevGrid g, const float* X, int coeff_ch, int u_ch) {
+    __shared__ Snap S;
+    const int t = blockIdx.x;
+    if (!(tile_type(g, t) & (dLeaf | dGhost))) return;
+    const Quad Q(t, threadIdx.x);
+    float4 xr, dg;
+    uchar4 ty;
+    load_snap(g, t, X, coeff_ch, LeafHalo{X, g.ctype}, S, Q, xr, ty, dg, BlockSync{});
+    const float h = voxel_size(g.h0, tile_level(g, t));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float* U = g.plane(u_ch + a);
+        float4 u = ld4(U + Q.base);
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const int i = Q.i, j = Q.j, k = Q.k0 + w;
+            const float pu = S.x[sx(i, j, k)];
+            const float pd = S.x[sx(i - (a == 0), j - (a == 1), k - (a == 2))];
+            const float c = a == 0 ? S.c0[i * 64 + j * 8 + k] : a == 1 ? S.c1[i * 72 + j * 8 + k] : S.c2[i * 72 + j * 9 + k];
+            if (__fdiv_rn(-c, h) > 0.0f) f4set(u, w, __fadd_rn(f4get(u, w), __fdiv_rn(__fsub_rn(pu, pd), h)));
+        }
+        st4(U + Q.base, u);
+    }
+}
+
 __global__ void k_remap(const float* src, float* dst, const int* old_of_new, int n_new, int n_old) {
     const int t = blockIdx.x, c = blockIdx.y;
     const int o = old_of_new[t];
@@ -1183,6 +1210,9 @@ void launch_accumulate_faces(const DevGrid& g, const int* leaf, int nleaf, int u
 }
 void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int coeff_ch, int out_ch, cudaStream_t st) {
     if (nleaf > 0) count_launch(), k_divergence<<<nleaf, 128, 0, st>>>(g, leaf, u_ch, coeff_ch, out_ch);
+}
+void launch_gradient(const DevGrid& g, const float* X, int coeff_ch, int u_ch, cudaStream_t st) {
+    if (g.n > 0) count_launch(), k_gradient<<<g.n, 128, 0, st>>>(g, X, coeff_ch, u_ch);
 }
 void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st) {
     if (n_new > 0 && nch > 0) count_launch(), k_remap<<<dim3(n_new, nch), 128, 0, st>>>(src, dst, old_of_new, n_new, n_old);

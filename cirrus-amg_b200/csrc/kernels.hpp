@@ -68,6 +68,7 @@ void launch_face_velocity(const DevGrid& g, const int* leaf, int nleaf, int u_ch
 void launch_propagate_ghost(const DevGrid& g, int t0, int nt, int ch, cudaStream_t st);
 void launch_accumulate_faces(const DevGrid& g, const int* leaf, int nleaf, int u_ch, cudaStream_t st);
 void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int coeff_ch, int out_ch, cudaStream_t st);
+void launch_gradient(const DevGrid& g, const float* X, int coeff_ch, int u_ch, cudaStream_t st);
 void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st);
 void launch_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new, int n_new, cudaStream_t st);
 void launch_fill(float* p, size_t n, float v, cudaStream_t st);

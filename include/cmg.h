@@ -117,6 +117,9 @@ int cmg_amg_cutcell_sphere_coeffs(cmg_grid* g, int coeff_ch, float R_matrix, int
 int cmg_amg_face_velocity_fourier(cmg_grid* g, int u_ch, int nmodes, const double* k, const double* amp, const double* phase);
 /* AMGVolumeWeightedDivergenceOnLeafs (src/AMGSolver.cu:790) */
 int cmg_amg_divergence(cmg_grid* g, int u_ch, int coeff_ch, int out_ch);
+/* AMGAddGradientToFace (src/AMGSolver.cu:680): u += grad x on faces with a
+ * positive fluid ratio, LEAF and GHOST tiles (GHOST x is first set from the parents) */
+int cmg_amg_add_gradient_to_face(cmg_grid* g, int x_ch, int coeff_ch, int u_ch);
 /* AMGFullNegativeLaplacianOnLeafs (src/AMGSolver.cu:589): Ax on LEAF tiles */
 int cmg_amg_full_neg_lap(cmg_grid* g, int x_ch, int coeff_ch, int ax_ch);
 /* Dot over LEAF tiles (src/PoissonGrid.cu:203) */

@@ -740,7 +740,7 @@ static int is_active_at(const og_grid* g, int t, int level) { /* subtreeType(lev
 
 /* PropagateToChildren + AccumulateToParentsOneStep + NegativeLaplacianSameLevelAMG128
  * on LEAF tiles (AMGFullNegativeLaplacianOnLeafs, AMGSolver.cu:589-632). */
-void og_full_neg_lap_leafs(og_grid* g, int x_ch, int coeff_ch, int ax_ch) {
+static void propagate_and_accumulate(og_grid* g, int x_ch) {
     /* ghost <- parent value (PoissonGrid.cu:377-405), coarse levels first */
     for (int L = 1; L <= g->max_level; L++)
         for (int t = 0; t < g->n; t++) {
@@ -773,6 +773,9 @@ void og_full_neg_lap_leafs(og_grid* g, int x_ch, int coeff_ch, int ax_ch) {
             CH(g, x_ch, p)[parent_cell(g, t, CELL(fl[0], fl[1], fl[2]))] = sum * 0.125f;
         }
     }
+}
+void og_full_neg_lap_leafs(og_grid* g, int x_ch, int coeff_ch, int ax_ch) {
+    propagate_and_accumulate(g, x_ch);
 #pragma omp parallel
     {
         og_snap* S = (og_snap*)malloc(sizeof(og_snap));
@@ -1111,6 +1114,34 @@ void og_divergence(og_grid* g, int u_ch, int coeff_ch, int out_ch) {
             }
             CH(g, out_ch, t)[v] = (CT(g, t)[v] & OG_INTERIOR) ? sum : 0.0f;
         }
+    }
+}
+
+/* AMGAddGradientToFace (src/AMGSolver.cu:634-688): GHOST <- parent and NONLEAF
+ * <- mean of LEAF children for x, then on LEAF and GHOST tiles
+ * u_axis += (x - x_minus) / h on every face whose fluid ratio -c_axis/h > 0. */
+void og_add_gradient_to_face(og_grid* g, int x_ch, int coeff_ch, int u_ch) {
+    propagate_and_accumulate(g, x_ch);
+#pragma omp parallel
+    {
+        og_snap* S = (og_snap*)malloc(sizeof(og_snap));
+#pragma omp for schedule(dynamic, 8)
+        for (int t = 0; t < g->n; t++) {
+            if (!(g->t[t].type & (OG_LEAF | OG_GHOST))) continue;
+            load_snap(g, t, x_ch, coeff_ch, S);
+            float h = voxel_size(g, g->t[t].level);
+            for (int v = 0; v < NC; v++) {
+                int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+                for (int axis = 0; axis < 3; axis++) {
+                    int d[3] = {0, 0, 0};
+                    d[axis] = 1;
+                    float pu = S->x[SX(i, j, k)], pd = S->x[SX(i - d[0], j - d[1], k - d[2])];
+                    float ratio = -S->c[axis][SX(i, j, k)] / h;
+                    if (ratio > 0) CH(g, u_ch + axis, t)[v] += (pu - pd) / h;
+                }
+            }
+        }
+        free(S);
     }
 }
 

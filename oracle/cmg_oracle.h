@@ -13,10 +13,11 @@
  * Parity pin: the reference ships no golden vectors for this path
  * (tests/SolverTests.cu prints, it does not store).  The oracle is pinned by
  * (1) the reference's own known-answer tests restated in tests/ (analytic
- * Laplacian truncation error, -lap == div grad, Neumann/Dirichlet recovery),
- * (2) committed fixtures produced by running the reference's CUDA solver
- * through oracle/ref_harness.cu on a B200, when that harness has been run
- * (tests/golden/), and (3) the FP64 CSR assembly of the same operator.
+ * Laplacian truncation error, -lap == div grad, Neumann/Dirichlet recovery,
+ * divergence-free velocity after projection), and (2) the FP64 CSR assembly
+ * of the same operator solved independently.  The reference's CUDA solver
+ * cannot be run against it: on the adaptive sphere grid it stops on its own
+ * device assertion (src/AMGSolver.cu:873), so it is not run at all.
  */
 #ifndef CMG_ORACLE_H
 #define CMG_ORACLE_H
@@ -76,6 +77,7 @@ int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float R_restric
 
 void og_face_velocity_fourier(og_grid* g, int u_ch, int nmodes, const double* k, const double* amp, const double* phase);
 void og_divergence(og_grid* g, int u_ch, int coeff_ch, int out_ch);
+void og_add_gradient_to_face(og_grid* g, int x_ch, int coeff_ch, int u_ch);
 
 /* FP64 CSR assembly of the leaf operator (unknowns = INTERIOR cells of LEAF tiles) */
 int og_assemble_count(og_grid* g, int coeff_ch, int* n_rows, long long* nnz);

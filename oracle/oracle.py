@@ -60,6 +60,7 @@ def lib():
             "og_amg_solve": (I, [P, I, D, I, F, F, I, D, I, I, I, I, P]),
             "og_face_velocity_fourier": (None, [P, I, I, P, P, P]),
             "og_divergence": (None, [P, I, I, I]),
+            "og_add_gradient_to_face": (None, [P, I, I, I]),
             "og_assemble_count": (I, [P, I, P, P]),
             "og_assemble": (I, [P, I, P, P, P, P, P]),
             "og_csr_solve": (I, [I, P, P, P, P, P, D, I, I, P, P]),
@@ -179,6 +180,9 @@ class Grid:
 
     def divergence(self, u_ch, coeff_ch, out_ch):
         self.L.og_divergence(self.g, u_ch, coeff_ch, out_ch)
+
+    def add_gradient_to_face(self, x_ch, coeff_ch, u_ch):
+        self.L.og_add_gradient_to_face(self.g, x_ch, coeff_ch, u_ch)
 
     def assemble(self, coeff_ch):
         """FP64 CSR of the leaf operator; rows/cols are INTERIOR cells of LEAF tiles."""

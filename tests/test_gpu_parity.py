@@ -207,3 +207,78 @@ def test_persistent_levels_match_per_phase_launches(shell):
     x2 = G.download(0)
     assert (it1, rel1) == (it2, rel2)
     assert np.array_equal(x1, x2)
+
+
+def _kat_product_and_oracle(case_id, prm):
+    from workloads import boundary_rule_types
+
+    G = build_product(case_id, prm)
+    g = build_oracle(case_id, prm)
+    lv, ijk, ty = G.tiles()
+    nb, ch = G.tables()
+    ct = np.zeros((G.num_tiles, 512), np.uint8)
+    leaf = ty == cmg.LEAF
+    ct[leaf] = boundary_rule_types(lv, ijk, ty, nb)[leaf]
+    G.upload_cell_types(ct)
+    g.cell_types()[:] = ct
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    solver.prepareTypesAndCoeffs(G)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    assert np.array_equal(G.download_cell_types(), g.cell_types())
+    return G, g, solver
+
+
+@pytest.mark.parametrize("case_id,prm", [(cmg.CASE_UNIFORM, [2, 2]), (cmg.CASE_CENTER_POINT, [2, 4])])
+def test_kat_recovery_on_gpu(case_id, prm):
+    """TestNeumannDirichletRecovery (tests/SolverTests.cu:363-512) through the C ABI."""
+    from workloads import recovery_fields
+
+    G, g, solver = _kat_product_and_oracle(case_id, prm)
+    lv, ijk, ty = G.tiles()
+    ct = G.download_cell_types()
+    xt = recovery_fields(lv, ijk, ty, ct)
+    G.upload(5, xt)
+    G.full_neg_lap(5, COEFF, 1)
+    it, rel = solver.solve(G, False, 1000, 1e-6, 2, 10, 1, False)
+    m = (ty[:, None] == cmg.LEAF) & (ct == cmg.INTERIOR)
+    err = np.abs(G.download(0)[m] - xt[m]).max()
+    assert rel < 1e-6 and err < 1e-4, (it, rel, err)
+
+
+def test_kat_flux_consistency_on_gpu():
+    """TestAMGLaplacianAndFluxConsistency (tests/SolverTests.cu:242-361) through the C ABI, and equal to the oracle."""
+    from workloads import flux_fields
+
+    G, g, solver = _kat_product_and_oracle(cmg.CASE_UNIFORM, [2, 2])
+    lv, ijk, ty = G.tiles()
+    ct = G.download_cell_types()
+    x = flux_fields(lv, ijk, ty, ct)
+    G.upload(0, x)
+    for a in range(3):
+        G.fill(10 + a, 0.0)
+    G.full_neg_lap(0, COEFF, 1)
+    G.add_gradient_to_face(0, COEFF, 10)
+    G.divergence(10, COEFF, 2)
+    m = (ty[:, None] == cmg.LEAF) & (ct == cmg.INTERIOR)
+    assert np.abs(G.download(2)[m] + G.download(1)[m]).max() < 1e-5
+    g.channel(0)[:] = x
+    g.add_gradient_to_face(0, COEFF, 10)
+    for a in range(3):
+        ud, uo = G.download(10 + a), g.channel(10 + a)
+        assert np.max(np.abs(ud[ty == cmg.LEAF] - uo[ty == cmg.LEAF])) <= 1e-6 * max(1.0, np.max(np.abs(uo)))
+
+
+@pytest.mark.parametrize("prm", [shell_params(3, 4, 5), shell_params(4, 5, 6)])
+def test_kat_projection_on_gpu(prm):
+    """Projection (tests/SolverTests.cu:1846-2158) on the cut-cell sphere octree: after
+    u += grad p the divergence vanishes to the solve tolerance."""
+    from workloads import projected_divergence
+
+    G, _, solver = setup_shell(prm, with_oracle=False)
+    lv, ijk, ty = G.tiles()
+    b0 = G.download(1)
+    it, rel = solver.solve(G, False, 200, 1e-6, 2, 10, 1, False)
+    G.add_gradient_to_face(0, COEFF, U)
+    G.divergence(U, COEFF, 13)
+    ratio = projected_divergence(G.download, lv, ijk, ty, G.download_cell_types(), b0, 13)
+    assert rel < 1e-6 and ratio < 1e-5, (it, rel, ratio)

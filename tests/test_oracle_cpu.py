@@ -167,3 +167,79 @@ def test_cutcell_face_fraction_rules():
         assert np.all(ratio[cut] >= 0.1 - 1e-7)
     assert np.any(ct[leaf] == O.NEUMANN)
     assert np.all(g.channel(COEFF + 3)[leaf][ct[leaf] == O.NEUMANN] == 0)
+
+
+def _kat_grid(case_id, prm):
+    from workloads import boundary_rule_types
+
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(case_id, prm)
+    g.alloc(16)
+    lv, ijk, ty = g.tiles()
+    nbr, par, ch = g.tables()
+    ct = boundary_rule_types(lv, ijk, ty, nbr)
+    types = g.cell_types()
+    types[ty == O.LEAF] = ct[ty == O.LEAF]
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    return g
+
+
+@pytest.mark.parametrize("case_id,prm", [(O.CASE_UNIFORM, [2, 2]), (O.CASE_CENTER_POINT, [2, 4])])
+def test_kat_neumann_dirichlet_recovery(case_id, prm):
+    """TestNeumannDirichletRecovery (tests/SolverTests.cu:363-512): b = A x_true, solve, |x - x_true|_inf < 1e-4."""
+    from workloads import recovery_fields
+
+    g = _kat_grid(case_id, prm)
+    lv, ijk, ty = g.tiles()
+    ct = g.cell_types()
+    xt = recovery_fields(lv, ijk, ty, ct)
+    g.channel(5)[:] = xt
+    g.full_neg_lap_leafs(5, COEFF, 1)
+    it, rel = g.amg_solve(COEFF, max_iters=1000, tol=1e-6, level_iters=2, coarsest_iters=10)
+    m = (ty[:, None] == O.LEAF) & (ct == O.INTERIOR)
+    err = np.abs(g.channel(0)[m] - xt[m]).max()
+    assert rel < 1e-6 and err < 1e-4, (it, rel, err)
+
+
+def test_kat_laplacian_flux_consistency():
+    """TestAMGLaplacianAndFluxConsistency (tests/SolverTests.cu:242-361): -lap x + div(grad x) = 0, L_inf < 1e-5."""
+    from workloads import flux_fields
+
+    g = _kat_grid(O.CASE_UNIFORM, [2, 2])
+    lv, ijk, ty = g.tiles()
+    ct = g.cell_types()
+    g.channel(0)[:] = flux_fields(lv, ijk, ty, ct)
+    for a in range(3):
+        g.channel(10 + a)[:] = 0
+    g.full_neg_lap_leafs(0, COEFF, 1)
+    g.add_gradient_to_face(0, COEFF, 10)
+    g.divergence(10, COEFF, 2)
+    m = (ty[:, None] == O.LEAF) & (ct == O.INTERIOR)
+    diff = np.abs(g.channel(2)[m] + g.channel(1)[m]).max()
+    assert diff < 1e-5, diff
+
+
+def test_kat_projection_divergence_free():
+    """Projection on the cut-cell sphere octree (tests/SolverTests.cu:1846-2158): solve
+    -lap p = div u, u += grad p, then div u vanishes to the solve tolerance."""
+    from workloads import U, fourier_modes, projected_divergence, shell_params
+
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(O.CASE_SHELL, shell_params(2, 3, 4))
+    g.alloc(16)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.cutcell_sphere_coeffs(COEFF, [(0.5, 0.5, 0.5, 0.1)], 0.5)
+    k, amp, ph = fourier_modes(1)
+    g.face_velocity_fourier(U, k, amp, ph)
+    g.divergence(U, COEFF, 1)
+    b0 = g.channel(1).copy()
+    it, rel = g.amg_solve(COEFF, max_iters=200, tol=1e-6)
+    g.add_gradient_to_face(0, COEFF, U)
+    g.divergence(U, COEFF, 13)
+    lv, ijk, ty = g.tiles()
+    ratio = projected_divergence(g.channel, lv, ijk, ty, g.cell_types(), b0, 13)
+    assert rel < 1e-6 and ratio < 1e-5, (it, rel, ratio)

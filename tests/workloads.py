@@ -91,3 +91,71 @@ def setup_shell(params, seed=1, spheres=((0.5, 0.5, 0.5, 0.1),), with_oracle=Tru
         g.face_velocity_fourier(U, k, amp, ph)
         g.divergence(U, COEFF, 1)
     return G, g, solver
+
+
+def boundary_rule_types(lv, ijk, ty, nb):
+    """Cell types of the reference's recovery and flux tests (tests/SolverTests.cu:283-303, 387-411):
+    a LEAF cell with an empty same-level neighbour on the -x side is NEUMANN, on any other
+    side DIRICHLET, otherwise INTERIOR.  nb: [n][>=6] face neighbours (-x,-y,-z,+x,+y,+z)."""
+    v = np.arange(512)
+    l = np.stack([v >> 6, (v >> 3) & 7, v & 7], axis=1)
+    n = len(lv)
+    neu = np.zeros((n, 512), bool)
+    dir_ = np.zeros((n, 512), bool)
+    for axis in range(3):
+        lo = (l[:, axis] == 0)[None, :] & (nb[:, axis] < 0)[:, None]
+        hi = (l[:, axis] == 7)[None, :] & (nb[:, 3 + axis] < 0)[:, None]
+        if axis == 0:
+            neu |= lo
+        else:
+            dir_ |= lo
+        dir_ |= hi
+    ct = np.full((n, 512), 2, np.uint8)
+    ct[dir_] = 1
+    ct[neu] = 4
+    return ct
+
+
+def cell_centres(lv, ijk, h0=0.125):
+    v = np.arange(512)
+    l = np.stack([v >> 6, (v >> 3) & 7, v & 7], axis=1)
+    h = (h0 / (2.0 ** lv)).astype(np.float32)
+    gc = ijk[:, None, :] * 8 + l[None, :, :]
+    return ((gc + 0.5) * h[:, None, None]).astype(np.float32)
+
+
+def recovery_fields(lv, ijk, ty, ct):
+    """x_true = exp(x) sin(y) on INTERIOR cells of LEAF tiles (tests/SolverTests.cu:412-415)."""
+    xc = cell_centres(lv, ijk)
+    f = (np.exp(xc[..., 0]) * np.sin(xc[..., 1])).astype(np.float32)
+    f[(ty != 1)] = 0
+    f[ct != 2] = 0
+    return f
+
+
+def flux_fields(lv, ijk, ty, ct):
+    """x = sin(-2.5 x + y + 7 z) on INTERIOR cells (tests/SolverTests.cu:292-295)."""
+    xc = cell_centres(lv, ijk)
+    f = np.sin(-2.5 * xc[..., 0] + xc[..., 1] + 7 * xc[..., 2]).astype(np.float32)
+    f[(ty != 1)] = 0
+    f[ct != 2] = 0
+    return f
+
+
+def away_from_walls(lv, ijk):
+    """Cells whose 6 neighbours lie inside the domain.  The divergence treats the outer
+    wall as closed (empty neighbour: u = 0, src/AMGSolver.cu:813-816) while the Laplacian
+    treats it as a Dirichlet wall, so the projection is exact only away from it."""
+    v = np.arange(512)
+    l = np.stack([v >> 6, (v >> 3) & 7, v & 7], axis=1)
+    gc = ijk[:, None, :] * 8 + l[None]
+    nmax = (8 << lv.astype(np.int64))[:, None, None] - 1
+    return ~((gc == 0) | (gc == nmax)).any(-1)
+
+
+def projected_divergence(download, lv, ijk, ty, ct, b0, div_ch):
+    """|div u_projected|_2 / |div u|_2 over INTERIOR leaf cells away from the outer walls."""
+    m = (ty[:, None] == 1) & (ct == 2) & away_from_walls(lv, ijk)
+    d0 = np.linalg.norm(b0[m].astype(np.float64))
+    d1 = np.linalg.norm(download(div_ch)[m].astype(np.float64))
+    return d1 / d0
