@@ -222,7 +222,9 @@ def run_ours(args, rank, world, local_rank):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
+        torch.cuda.nvtx.range_push("solve")
         it, rel = one_solve()
+        torch.cuda.nvtx.range_pop()
         iters.append(it)
         rels.append(rel)
         per_ms.append(S.last_solve_ms())

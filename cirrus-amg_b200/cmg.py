@@ -286,10 +286,11 @@ class AMGSolver:
         except Exception:
             pass
 
-    def set_launch_mode(self, use_graph=True, persistent=False):
+    def set_launch_mode(self, use_graph=True, persistent=False, cluster=True):
         """use_graph: one CUDA graph per solve (default) or kernel-by-kernel launches;
-        persistent: levels 2-3 of each cycle in one cooperative kernel (off by default)."""
-        flags = (1 if use_graph else 0) | (2 if persistent else 0)
+        persistent: levels 2-3 of each cycle in one cooperative kernel (off by default);
+        cluster: each visit of level 2 in one 8-CTA cluster launch when levels 0-2 are complete."""
+        flags = (1 if use_graph else 0) | (2 if persistent else 0) | (0 if cluster else 4)
         _check(self.L.cmg_amg_solver_set_launch_mode(self.h, flags), "set_launch_mode")
 
     def _sync_params(self):

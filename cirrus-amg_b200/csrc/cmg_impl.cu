@@ -205,6 +205,7 @@ int Solver::init() {
     init_kernel_attributes();
     persist_nblocks = persist_blocks();
     if (persist_nblocks <= 0) use_persist = false;
+    cluster_ok = cluster_step_supported();
     return check_cuda(cudaGetLastError(), "kernel attributes");
 }
 
@@ -246,10 +247,25 @@ void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, cons
     }
 }
 
-// AMGSolver::FASMuCycleStep (src/AMGSolver.cu:1257-1277).  Levels 0 and 1 run
-// as a single coarse-kernel launch.
+// Levels 0-2 are complete 8^3, 16^3 and 32^3 grids: a NONLEAF root, eight
+// NONLEAF children and 64 grandchildren, none of them GHOST.
+static bool coarse_levels_complete(const Grid& G) {
+    if (G.max_level() < 2) return false;
+    for (int l = 0; l <= 1; ++l)
+        if (G.level_end(l) - G.level_begin(l) != (l ? 8 : 1) || G.nonleaf_begin(l) != G.level_begin(l) || G.ghost_begin(l) != G.level_end(l))
+            return false;
+    return G.ghost_begin(2) - G.level_begin(2) == 64 && G.level_end(2) == G.ghost_begin(2);
+}
+
+// AMGSolver::FASMuCycleStep (src/AMGSolver.cu:1257-1277).  A visit of level 2
+// runs as one cluster launch when levels 0-2 are complete; otherwise levels 0
+// and 1 run as a single coarse-kernel launch.
 void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) const {
     const DevGrid d = G.dev();
+    if (l == 2 && use_cluster && cluster_ok && coarse_levels_complete(G)) {
+        launch_cluster_step(d, A.X, A.RHS, A.X0, A.coeff_ch, A.mu, A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P, st);
+        return;
+    }
     if (l <= 1) {
         launch_coarse_step(d, l, A.X, A.RHS, A.X0, A.coeff_ch, A.mu,
                            A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P, st);
@@ -394,7 +410,7 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     }
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
-    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0), omega};
+    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0), omega};
     Plan plan{};
     if (use_graph) {
         auto it = graphs.find(k);

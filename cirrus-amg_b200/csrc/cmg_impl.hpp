@@ -119,6 +119,8 @@ struct Solver {
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
     bool use_graph = true;    // false: launch kernel by kernel from the host (profiling)
     bool use_persist = false;  // levels 2-3 in one cooperative kernel per visit
+    bool use_cluster = true;   // levels 0-2 in one cluster launch per visit of level 2
+    bool cluster_ok = false;   // the device can run that cluster
     int persist_nblocks = 0;
     unsigned int* bar = nullptr;  // grid-barrier words of the persistent kernel
     unsigned int* h_bar = nullptr;

@@ -1057,6 +1057,7 @@ __global__ void k_count_bad_diag(DevGrid g, int t0, int coeff_ch, int* out) {
 static std::atomic<long long> g_launches{0};
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void note_kernel_launch() { count_launch(); }
 
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st) {
     if (nt <= 0) return;

@@ -33,6 +33,12 @@ void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0,
 void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters,
                         int coarsest_iters, double omega, float R_restrict, float P, cudaStream_t st);
 size_t coarse_step_smem_bytes();
+// FASMuCycleStep of level 2 with its recursion through levels 1 and 0 in one
+// launch of an 8-CTA cluster (coarse_cluster.cu).  Requires levels 0-2 to be
+// complete grids: the root, its 8 children and their 64 children, no GHOST tile.
+void launch_cluster_step(const DevGrid& g, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters, int coarsest_iters,
+                         double omega, float R_restrict, float P, cudaStream_t st);
+bool cluster_step_supported();  // the current device can co-schedule the 8-CTA cluster
 // FASMuCycleStep of level `top` (2 or 3) with all its recursions in one
 // cooperative launch of `nblocks` co-resident blocks; bar = 3 zeroed words
 // (barrier count, generation, error flag).  Level ranges indexed by level 0..3.
@@ -56,6 +62,7 @@ void launch_leaf_copy(const DevGrid& g, const int* leaf, int nleaf, float* dst, 
 void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, ReduceScratch rs, cudaStream_t st);
 void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, bool use_handle, cudaStream_t st);
 void init_kernel_attributes();
+void note_kernel_launch();        // counts one launch made outside kernels.cu
 long long kernel_launch_count();  // kernels enqueued (or captured) by this library so far
 
 // --- operator set-up and right-hand side ---

@@ -137,10 +137,15 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
  * without it the same kernels are launched one by one with the loop test on
  * the host (for profilers that do not enter conditional graph nodes).
  * PERSISTENT: each visit of multigrid level 2 or 3 runs as one cooperative
- * kernel with grid barriers; without it, one kernel per phase.  No
- * counterpart in the reference, which launches every phase from the host. */
+ * kernel with grid barriers; without it, one kernel per phase.
+ * NO_CLUSTER: when levels 0-2 are complete grids, each visit of level 2 (with
+ * its recursion through levels 1 and 0) normally runs as one launch of an
+ * 8-CTA thread-block cluster; this flag launches those phases separately.
+ * None has a counterpart in the reference, which launches every phase from
+ * the host. */
 #define CMG_LAUNCH_GRAPH 1
 #define CMG_LAUNCH_PERSISTENT 2
+#define CMG_LAUNCH_NO_CLUSTER 4
 int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
 /* AMGSolver::solve (src/AMGSolver.cu:1399): solves -lap x = b, b read from
  * channel 1 and overwritten by the residual, x written to channel 0.

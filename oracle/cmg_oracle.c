@@ -173,9 +173,9 @@ static void finalize(og_grid* g) {
     map_rebuild(g);
     compute_max_level(g);
     int n = g->n;
-    g->nbr = (int*)malloc(sizeof(int) * 6 * (n ? n : 1));
-    g->parent = (int*)malloc(sizeof(int) * (n ? n : 1));
-    g->child = (int*)malloc(sizeof(int) * 8 * (n ? n : 1));
+    g->nbr = (int*)malloc(sizeof(int) * 6 * (size_t)(n > 0 ? n : 1));
+    g->parent = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    g->child = (int*)malloc(sizeof(int) * 8 * (size_t)(n > 0 ? n : 1));
     for (int t = 0; t < n; t++) {
         og_tile* T = &g->t[t];
         for (int a = 0; a < 3; a++) {

@@ -198,11 +198,11 @@ def test_persistent_levels_match_per_phase_launches(shell):
         b = G.download(1)
     else:
         G, g, solver, b = setup_uniform(3, with_oracle=False)
-    solver.set_launch_mode(use_graph=True, persistent=False)
+    solver.set_launch_mode(use_graph=True, persistent=False, cluster=False)
     it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
     x1 = G.download(0)
     G.upload(1, b)
-    solver.set_launch_mode(use_graph=True, persistent=True)
+    solver.set_launch_mode(use_graph=True, persistent=True, cluster=False)
     it2, rel2 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
     x2 = G.download(0)
     assert (it1, rel1) == (it2, rel2)
@@ -282,3 +282,44 @@ def test_kat_projection_on_gpu(prm):
     G.divergence(U, COEFF, 13)
     ratio = projected_divergence(G.download, lv, ijk, ty, G.download_cell_types(), b0, 13)
     assert rel < 1e-6 and ratio < 1e-5, (it, rel, ratio)
+
+
+def _mu_cycle_planes(G, solver, cluster, seed, mu, omega):
+    rng = np.random.default_rng(seed)
+    n = G.num_tiles
+    solver.mu_cycle_repeat_times = mu
+    solver.omega = omega
+    G.upload(1, rng.standard_normal((n, 512)).astype(np.float32))
+    G.upload(3, rng.standard_normal((n, 512)).astype(np.float32))
+    G.upload(4, rng.standard_normal((n, 512)).astype(np.float32))
+    solver.set_launch_mode(use_graph=False, cluster=cluster)
+    solver.fas_mu_cycle(G, 4, 1, 3, 2, 10)
+    return G.download(4), G.download(1), G.download(3)
+
+
+@pytest.mark.parametrize("grid", ["uniform32", "uniform64", "shell345"])
+@pytest.mark.parametrize("mu,omega", [(2, 1.5), (1, 1.5), (2, 1.3)])
+def test_cluster_mu_step_matches_per_level_launches(grid, mu, omega):
+    """Levels 0-2 in one 8-CTA cluster launch give the same x, rhs and saved x on
+    every tile as the per-level launches (levels 2 and 1-0 separately)."""
+    if grid == "shell345":
+        G, _, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5), with_oracle=False)
+    else:
+        G, _, solver, _ = setup_uniform(2 if grid == "uniform32" else 3, with_oracle=False)
+    a = _mu_cycle_planes(G, solver, True, 11, mu, omega)
+    b = _mu_cycle_planes(G, solver, False, 11, mu, omega)
+    for pa, pb in zip(a, b):
+        assert np.array_equal(pa, pb)
+
+
+def test_cluster_solve_matches_per_level_launches():
+    G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5), with_oracle=False)
+    b = G.download(1)
+    solver.set_launch_mode(use_graph=True, cluster=False)
+    it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x1 = G.download(0)
+    G.upload(1, b)
+    solver.set_launch_mode(use_graph=True, cluster=True)
+    it2, rel2 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    assert (it1, rel1) == (it2, rel2)
+    assert np.array_equal(x1, G.download(0))
