@@ -31,7 +31,7 @@ CASE_STAR_EMPTY, CASE_STAR_SOLID, CASE_SHELL, CASE_MULTI_SPHERE = 4, 5, 6, 7
 
 # names of every entry point include/cmg.h declares
 EXPORTS = [
-    "cmg_last_error", "cmg_version",
+    "cmg_last_error", "cmg_version", "cmg_check_division",
     "cmg_grid_create", "cmg_grid_destroy", "cmg_grid_set_tile", "cmg_grid_rebuild", "cmg_grid_iterative_refine",
     "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
     "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
@@ -67,6 +67,7 @@ def lib():
         sig = {
             "cmg_last_error": (ctypes.c_char_p, []),
             "cmg_version": (I, []),
+            "cmg_check_division": (I, [ctypes.c_longlong, ctypes.c_ulonglong, P, P]),
             "cmg_grid_create": (I, [F, I, I, PP]),
             "cmg_grid_destroy": (I, [P]),
             "cmg_grid_set_tile": (I, [P, I, I, I, I, I]),
@@ -116,6 +117,15 @@ def lib():
 
 class CmgError(RuntimeError):
     pass
+
+
+def check_division(n, seed=0):
+    """Count of pairs on which the coarse-level division differs from IEEE division,
+    and the first differing (a, d) as float bit patterns."""
+    m = ctypes.c_longlong(0)
+    first = (ctypes.c_uint * 2)()
+    _check(lib().cmg_check_division(int(n), int(seed), ctypes.byref(m), first), "check_division")
+    return m.value, (first[0], first[1])
 
 
 def _check(rc, what):
@@ -289,7 +299,7 @@ class AMGSolver:
     def set_launch_mode(self, use_graph=True, persistent=False, cluster=True):
         """use_graph: one CUDA graph per solve (default) or kernel-by-kernel launches;
         persistent: levels 2-3 of each cycle in one cooperative kernel (off by default);
-        cluster: each visit of level 2 in one 8-CTA cluster launch when levels 0-2 are complete."""
+        cluster: each visit of level 2 in one 9-CTA cluster launch when levels 0-2 are complete."""
         flags = (1 if use_graph else 0) | (2 if persistent else 0) | (0 if cluster else 4)
         _check(self.L.cmg_amg_solver_set_launch_mode(self.h, flags), "set_launch_mode")
 

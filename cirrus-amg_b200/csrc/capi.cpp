@@ -67,6 +67,11 @@ extern "C" {
 
 const char* cmg_last_error(void) { return cmg::last_error(); }
 int cmg_version(void) { return 1; }
+int cmg_check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair) {
+    if (n < 0 || !mismatches) return fail(CMG_ERR_INVALID, "cmg_check_division: bad argument");
+    if (cmg::check_division(n, seed, mismatches, first_pair)) return cmg::check_cuda(cudaGetLastError(), "check_division");
+    return CMG_OK;
+}
 
 int cmg_grid_create(float h0, int num_levels, int num_channels, cmg_grid** out) {
     GUARD_BEGIN
@@ -374,6 +379,7 @@ int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, i
     if (!chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || !chan_ok(g, x0_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_fas_mu_cycle: channel out of range");
     if (int rc = cmg::validate_solver_topology(g->g)) return rc;
     const cmg::MuArgs A = s->s.mu_args(g->g, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters);
+    s->s.enqueue_cluster_pack(g->g, g->g.stream);
     s->s.enqueue_mu_cycle(g->g, A, g->g.stream);
     return cmg::check_cuda(cudaGetLastError(), "fas_mu_cycle");
 }

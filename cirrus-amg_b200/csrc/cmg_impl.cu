@@ -183,6 +183,7 @@ Solver::~Solver() {
     dfree(partial);
     dfree(partial2);
     dfree(s);
+    if (cluster_pack) cudaFree(cluster_pack);
     if (h_s) cudaFreeHost(h_s);
     if (h_bar) cudaFreeHost(h_bar);
     dfree(bar);
@@ -206,6 +207,7 @@ int Solver::init() {
     persist_nblocks = persist_blocks();
     if (persist_nblocks <= 0) use_persist = false;
     cluster_ok = cluster_step_supported();
+    if (cluster_ok) CK(cudaMalloc(&cluster_pack, cluster_pack_bytes()));
     return check_cuda(cudaGetLastError(), "kernel attributes");
 }
 
@@ -257,13 +259,37 @@ static bool coarse_levels_complete(const Grid& G) {
     return G.ghost_begin(2) - G.level_begin(2) == 64 && G.level_end(2) == G.ghost_begin(2);
 }
 
+// the 8 level-1 tiles (root child order) and the 64 level-2 tiles by 4x4x4 tile position
+static void coarse_tiles(const Grid& G, int* tile1, int* tile2) {
+    const std::vector<int>& ch = G.topo.child;
+    for (int c = 0; c < 8; ++c) tile1[c] = ch[c];  // the root is tile 0
+    for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b)
+            for (int c = 0; c < 4; ++c)
+                tile2[a * 16 + b * 4 + c] = ch[8 * tile1[((a >> 1) << 2) | ((b >> 1) << 1) | (c >> 1)] + (((a & 1) << 2) | ((b & 1) << 1) | (c & 1))];
+}
+
+bool Solver::cluster_active(const Grid& G) const { return use_cluster && cluster_ok && coarse_levels_complete(G); }
+
+// pack the static operands of levels 0-2 for the cluster step (coefficients and
+// cell types are fixed for the duration of a solve)
+void Solver::enqueue_cluster_pack(Grid& G, cudaStream_t st) const {
+    if (!cluster_active(G)) return;
+    int tile1[8], tile2[64];
+    coarse_tiles(G, tile1, tile2);
+    launch_cluster_pack(G.dev(), tile1, tile2, coeff_ch, cluster_pack, st);
+}
+
 // AMGSolver::FASMuCycleStep (src/AMGSolver.cu:1257-1277).  A visit of level 2
 // runs as one cluster launch when levels 0-2 are complete; otherwise levels 0
 // and 1 run as a single coarse-kernel launch.
 void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) const {
     const DevGrid d = G.dev();
-    if (l == 2 && use_cluster && cluster_ok && coarse_levels_complete(G)) {
-        launch_cluster_step(d, A.X, A.RHS, A.X0, A.coeff_ch, A.mu, A.level_iters, A.coarsest_iters, A.omega, A.Rr, A.P, st);
+    if (l == 2 && cluster_active(G)) {
+        int tile1[8], tile2[64];
+        coarse_tiles(G, tile1, tile2);
+        launch_cluster_step(d, tile1, tile2, cluster_pack, A.X, A.RHS, A.X0, A.coeff_ch, A.mu, A.level_iters, A.coarsest_iters, A.omega, A.Rr,
+                            A.P, st);
         return;
     }
     if (l <= 1) {
@@ -315,6 +341,7 @@ static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
 void Solver::enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_h, bool graph, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
+    enqueue_cluster_pack(G, st);
     launch_leaf_fill(d, G.leaf, G.nleaf, G.plane(0), 0.0f, st);
     if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(1), kDotRR0, nullptr, rs, st);
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);

@@ -121,6 +121,9 @@ struct Solver {
     bool use_persist = false;  // levels 2-3 in one cooperative kernel per visit
     bool use_cluster = true;   // levels 0-2 in one cluster launch per visit of level 2
     bool cluster_ok = false;   // the device can run that cluster
+    void* cluster_pack = nullptr;  // packed static operands of levels 0-2 (launch_cluster_pack)
+    bool cluster_active(const Grid& G) const;
+    void enqueue_cluster_pack(Grid& G, cudaStream_t st) const;
     int persist_nblocks = 0;
     unsigned int* bar = nullptr;  // grid-barrier words of the persistent kernel
     unsigned int* h_bar = nullptr;

@@ -260,4 +260,24 @@ __device__ __forceinline__ double block_sum128(double v, double* red) {
     return r;
 }
 
+// a / d rounded to the nearest float -- bit-identical to IEEE division -- given
+// yd = 1/d rounded to the nearest double (1.0 / (double)d), for a divisor that is
+// reused many times.  q = RN_double(a * yd) differs from a/d by less than 2^-51.9
+// relative (two double roundings).  A quotient of two 24-bit floats is never a
+// midpoint of adjacent normal floats and stays more than 2^-49 (relative) away
+// from every midpoint: writing the midpoint as M*2^m (M odd, 25 bits), d = D*2^e,
+// a - d*M*2^m is a nonzero multiple of 2^(e+m), so |a/d - M*2^m| >= 2^m / D.
+// Hence q and a/d round to the same float.  This is the argument behind the
+// double-rounding bound for division (S. A. Figueroa, "When is double rounding
+// innocuous?", ACM SIGNUM Newsletter 30(3), 1995), applied to the product with a
+// correctly rounded reciprocal.  Zero, subnormal, huge and non-finite cases take
+// the IEEE division itself.
+__device__ __forceinline__ float div_by_recip(float a, float d, double yd) {
+    const float q = __double2float_rn(__dmul_rn((double)a, yd));
+    const float m = fabsf(q);
+    if (m >= 0x1p-125f && m <= 0x1p127f) return q;
+    if (a == 0.0f && d != 0.0f) return q;
+    return __fdiv_rn(a, d);
+}
+
 }  // namespace cmg

@@ -1057,6 +1057,90 @@ __global__ void k_count_bad_diag(DevGrid g, int t0, int coeff_ch, int* out) {
 static std::atomic<long long> g_launches{0};
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {  // splitmix64 finaliser
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ float make_float(unsigned long long r, int emin, int emax) {
+    const unsigned sign = (unsigned)(r >> 63) << 31;
+    const int e = emin + (int)((r >> 32) % (unsigned long long)(emax - emin + 1));
+    return __uint_as_float(sign | ((unsigned)(e + 127) << 23) | ((unsigned)r & 0x7fffffu));
+}
+// Compares div_by_recip with the IEEE division on pseudo-random pairs: a quarter
+// uniform in sign, exponent and significand; a quarter built to fall within a few
+// ulps of a midpoint between two floats (a = RN(d * m) for a midpoint m); a quarter
+// shaped like Gauss-Seidel updates; a quarter of zeros, subnormals, huge values,
+// infinities and NaNs.
+__global__ void k_check_division(long long n, unsigned long long seed, unsigned long long* mism, unsigned int* first) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long r0 = mix64(seed ^ (unsigned long long)i), r1 = mix64(r0), r2 = mix64(r1);
+        float a, d;
+        switch ((int)(i & 3)) {
+            case 0:
+                a = make_float(r0, -60, 60);
+                d = make_float(r1, -60, 60);
+                break;
+            case 1: {
+                d = make_float(r0, -20, 20);
+                const float q = make_float(r1, -20, 20);
+                const double m = (double)q + 0.5 * ((double)nextafterf(fabsf(q), INFINITY) - (double)fabsf(q)) * (q < 0 ? -1.0 : 1.0);
+                a = __double2float_rn((double)d * m);
+                const int off = (int)(r2 % 5ull) - 2;  // a few ulps either side
+                for (int s = 0; s < (off < 0 ? -off : off); ++s) a = nextafterf(a, off < 0 ? -INFINITY : INFINITY);
+                break;
+            }
+            case 2:
+                a = make_float(r0, -40, 2);
+                d = -make_float(r1 & ~(1ull << 63), -14, 0);
+                break;
+            default: {
+                const float pool[10] = {0.0f, -0.0f, 1e-45f, -3e-39f, 1.17549435e-38f, 3.0e38f, INFINITY, -INFINITY, NAN, 1.0f};
+                a = (r2 & 1) ? pool[r0 % 10] : make_float(r0, -126, 127);
+                d = (r2 & 2) ? pool[r1 % 10] : make_float(r1, -126, 127);
+            }
+        }
+        const float want = __fdiv_rn(a, d);
+        const float got = div_by_recip(a, d, 1.0 / (double)d);
+        const bool same = (__float_as_uint(want) == __float_as_uint(got)) || (isnan(want) && isnan(got));
+        if (!same) {
+            if (atomicAdd(mism, 1ull) == 0ull) {
+                first[0] = __float_as_uint(a);
+                first[1] = __float_as_uint(d);
+            }
+        }
+    }
+}
+}  // namespace
+
+int check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair) {
+    unsigned long long* dm = nullptr;
+    unsigned int* df = nullptr;
+    if (cudaMalloc(&dm, sizeof(unsigned long long)) != cudaSuccess) return 2;
+    if (cudaMalloc(&df, 2 * sizeof(unsigned int)) != cudaSuccess) {
+        cudaFree(dm);
+        return 2;
+    }
+    cudaMemset(dm, 0, sizeof(unsigned long long));
+    cudaMemset(df, 0, 2 * sizeof(unsigned int));
+    count_launch(), k_check_division<<<148 * 8, 256>>>(n, seed, dm, df);
+    unsigned long long hm = 0;
+    unsigned int hf[2] = {0, 0};
+    cudaError_t e = cudaMemcpy(&hm, dm, sizeof(hm), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hf, df, sizeof(hf), cudaMemcpyDeviceToHost);
+    cudaFree(dm);
+    cudaFree(df);
+    if (e != cudaSuccess) return 2;
+    *mismatches = (long long)hm;
+    if (first_pair) {
+        first_pair[0] = hf[0];
+        first_pair[1] = hf[1];
+    }
+    return 0;
+}
 void note_kernel_launch() { count_launch(); }
 
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st) {

@@ -34,11 +34,18 @@ void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* 
                         int coarsest_iters, double omega, float R_restrict, float P, cudaStream_t st);
 size_t coarse_step_smem_bytes();
 // FASMuCycleStep of level 2 with its recursion through levels 1 and 0 in one
-// launch of an 8-CTA cluster (coarse_cluster.cu).  Requires levels 0-2 to be
+// launch of a 9-CTA cluster (coarse_cluster.cu).  Requires levels 0-2 to be
 // complete grids: the root, its 8 children and their 64 children, no GHOST tile.
-void launch_cluster_step(const DevGrid& g, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters, int coarsest_iters,
-                         double omega, float R_restrict, float P, cudaStream_t st);
-bool cluster_step_supported();  // the current device can co-schedule the 8-CTA cluster
+// tile1: the 8 level-1 tiles in root child order; tile2: the 64 level-2 tiles
+// indexed by (i >> 3) * 16 + (j >> 3) * 4 + (k >> 3) of their cells in the 32^3
+// grid.  pack: cluster_pack_bytes() of device memory filled by launch_cluster_pack
+// from the current coefficients and cell types (once per solve).
+cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* tile2, const void* pack, float* X, float* RHS, float* X0,
+                                int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float R_restrict, float P,
+                                cudaStream_t st);
+void launch_cluster_pack(const DevGrid& g, const int* tile1, const int* tile2, int coeff_ch, void* pack, cudaStream_t st);
+size_t cluster_pack_bytes();
+bool cluster_step_supported();  // the current device can co-schedule the 9-CTA cluster
 // FASMuCycleStep of level `top` (2 or 3) with all its recursions in one
 // cooperative launch of `nblocks` co-resident blocks; bar = 3 zeroed words
 // (barrier count, generation, error flag).  Level ranges indexed by level 0..3.
@@ -63,7 +70,9 @@ void launch_recenter(const DevGrid& g, const int* leaf, int nleaf, float* R, Red
 void launch_loop_gate(ReduceScratch rs, cudaGraphConditionalHandle loop_h, bool use_handle, cudaStream_t st);
 void init_kernel_attributes();
 void note_kernel_launch();        // counts one launch made outside kernels.cu
-long long kernel_launch_count();  // kernels enqueued (or captured) by this library so far
+long long kernel_launch_count();
+// div_by_recip against the IEEE division on n pseudo-random pairs; 0 or 2 (CUDA error)
+int check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair);  // kernels enqueued (or captured) by this library so far
 
 // --- operator set-up and right-hand side ---
 void launch_ghost_types(const DevGrid& g, int t0, int nt, cudaStream_t st);

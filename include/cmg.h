@@ -66,6 +66,13 @@ typedef int (*cmg_level_target_fn)(void* user, int level, int i, int j, int k);
 
 const char* cmg_last_error(void);
 int cmg_version(void);
+/* Self-check of the division the Gauss-Seidel sweeps of the coarse levels use
+ * (one double multiply by a precomputed reciprocal, rounded to float) against
+ * the IEEE float division, on n pseudo-random pairs from `seed`.  mismatches
+ * receives the number of results that differ in any bit; first_pair (may be
+ * NULL) the bit patterns of the first differing (a, d).  No counterpart in the
+ * reference, which divides directly (src/AMGSolver.cu:868-875). */
+int cmg_check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair);
 
 /* ---- grid: HADeviceGrid ------------------------------------------------ */
 /* HADeviceGrid(h0, levels_log2_hash) (src/HAGrid.h:416); num_levels = number
@@ -140,7 +147,7 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
  * kernel with grid barriers; without it, one kernel per phase.
  * NO_CLUSTER: when levels 0-2 are complete grids, each visit of level 2 (with
  * its recursion through levels 1 and 0) normally runs as one launch of an
- * 8-CTA thread-block cluster; this flag launches those phases separately.
+ * 9-CTA thread-block cluster; this flag launches those phases separately.
  * None has a counterpart in the reference, which launches every phase from
  * the host. */
 #define CMG_LAUNCH_GRAPH 1

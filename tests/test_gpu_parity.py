@@ -317,9 +317,20 @@ def test_cluster_solve_matches_per_level_launches():
     b = G.download(1)
     solver.set_launch_mode(use_graph=True, cluster=False)
     it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    n1 = solver.last_solve_launches()
     x1 = G.download(0)
     G.upload(1, b)
     solver.set_launch_mode(use_graph=True, cluster=True)
     it2, rel2 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    n2 = solver.last_solve_launches()
+    assert n2 < n1  # the cluster path ran
     assert (it1, rel1) == (it2, rel2)
     assert np.array_equal(x1, G.download(0))
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_division_by_reciprocal_is_ieee_exact(seed):
+    """The coarse-level Gauss-Seidel divides by multiplying with a double reciprocal;
+    on 2^26 adversarial pairs it must equal the IEEE division bit for bit."""
+    m, first = cmg.check_division(1 << 26, seed)
+    assert m == 0, (m, [hex(v) for v in first])
