@@ -152,82 +152,83 @@ struct SlotSync {
     __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 };
 
-// Load the snapshot of tile t (128 threads).  Returns the thread's raw x,
-// cell types and diagonal for its four cells.  LoadAMGLaplacianTileData,
+// What a thread of a 128-thread tile block holds for its four cells after the
+// snapshot load: raw x, x masked to INTERIOR cells (as the snapshot holds it),
+// cell types, diagonal, and the negative-face coefficients c0, c1, c2.
+struct Own {
+    float4 xr, xm, dg, a0, a1, a2;
+    uchar4 ty;
+};
+
+// Load the snapshot of tile t (128 threads).  LoadAMGLaplacianTileData,
 // src/AMGSolver.cu:419-543.  Latency: the neighbour descriptors are the only
 // loads the halo values depend on, so the tile's own loads and the halo loads
 // are all in flight before the first barrier; only the GHOST extrapolation,
 // which needs the tile's own values, waits for it.
+// Halo cells: thread q handles, for r = 0, 1, 2, cell q & 63 of the face of
+// axis r on side q >> 6 (the 384 halo cells of the six faces).
 template <class Halo, class Sync>
 __device__ __forceinline__ void load_snap(const DevGrid& g, int t, const float* X, int coeff_ch, const Halo& halo, Snap& S,
-                                          const Quad& Q, float4& xr, uchar4& ty, float4& dg, const Sync& sync) {
+                                          const Quad& Q, Own& o, const Sync& sync) {
     const float* C0 = g.plane(coeff_ch);
     const float* C1 = g.plane(coeff_ch + 1);
     const float* C2 = g.plane(coeff_ch + 2);
     const float* C3 = g.plane(coeff_ch + 3);
-    // halo cell r of this thread: face f = hh / 64 (axis f/2, side f%2), cell (a, b) on the face
+    const int side = Q.q >> 6, fa = (Q.q >> 3) & 7, fb = Q.q & 7;
     int desc[3];
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const int f = (Q.q + 128 * r) >> 6;
-        desc[r] = g.nbx[8 * t + (f >> 1) + 3 * (f & 1)];
-    }
-    xr = ldcg4(X + Q.base);
-    ty = ldt4(g.ctype + Q.base);
-    const float4 a0 = ld4(C0 + Q.base), a1 = ld4(C1 + Q.base), a2 = ld4(C2 + Q.base);
-    dg = ld4(C3 + Q.base);
+    for (int r = 0; r < 3; ++r) desc[r] = g.nbx[8 * t + r + 3 * side];
+    o.xr = ldcg4(X + Q.base);
+    o.ty = ldt4(g.ctype + Q.base);
+    o.a0 = ld4(C0 + Q.base);
+    o.a1 = ld4(C1 + Q.base);
+    o.a2 = ld4(C2 + Q.base);
+    o.dg = ld4(C3 + Q.base);
     const float h = voxel_size(g.h0, tile_level(g, t));
+    // the neighbour's cell across face (r, side) at face position (fa, fb)
+    const int nl0 = cell_index(side ? 0 : 7, fa, fb), nl1 = cell_index(fa, side ? 0 : 7, fb), nl2 = cell_index(fa, fb, side ? 0 : 7);
     float hv[3], hc[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-        const int hh = Q.q + 128 * r;
-        const int f = hh >> 6, fi = hh & 63;
-        const int axis = f >> 1, s = f & 1;
-        const int a = fi >> 3, b = fi & 7;
-        int nlc[3];
-        nlc[axis] = s ? 0 : 7;
-        if (axis == 0) { nlc[1] = a; nlc[2] = b; }
-        else if (axis == 1) { nlc[0] = a; nlc[2] = b; }
-        else { nlc[0] = a; nlc[1] = b; }
-        const int nl = cell_index(nlc[0], nlc[1], nlc[2]);
+        const int nl = r == 0 ? nl0 : r == 1 ? nl1 : nl2;
         hv[r] = 0.0f;
         hc[r] = h;
         if (desc[r] != 0) {
             const int qn = (desc[r] >> 3) - 1, ntype = desc[r] & 7;
             hv[r] = (ntype & dGhost) ? halo.ghost(g, qn, nl) : halo.active(g, qn, nl, ntype);
-            if (s) hc[r] = g.plane(coeff_ch + axis)[(size_t)qn * kCells + nl];
+            if (side) hc[r] = g.plane(coeff_ch + r)[(size_t)qn * kCells + nl];
         }
     }
+    o.xm.x = o.ty.x == dInterior ? o.xr.x : 0.0f;
+    o.xm.y = o.ty.y == dInterior ? o.xr.y : 0.0f;
+    o.xm.z = o.ty.z == dInterior ? o.xr.z : 0.0f;
+    o.xm.w = o.ty.w == dInterior ? o.xr.w : 0.0f;
     const int s0 = sx(Q.i, Q.j, Q.k0);
-    S.x[s0 + 0] = ty.x == dInterior ? xr.x : 0.0f;
-    S.x[s0 + 1] = ty.y == dInterior ? xr.y : 0.0f;
-    S.x[s0 + 2] = ty.z == dInterior ? xr.z : 0.0f;
-    S.x[s0 + 3] = ty.w == dInterior ? xr.w : 0.0f;
-    *reinterpret_cast<float4*>(&S.c0[Q.i * 64 + Q.j * 8 + Q.k0]) = a0;
-    *reinterpret_cast<float4*>(&S.c1[Q.i * 72 + Q.j * 8 + Q.k0]) = a1;
+    S.x[s0 + 0] = o.xm.x;
+    S.x[s0 + 1] = o.xm.y;
+    S.x[s0 + 2] = o.xm.z;
+    S.x[s0 + 3] = o.xm.w;
+    *reinterpret_cast<float4*>(&S.c0[Q.i * 64 + Q.j * 8 + Q.k0]) = o.a0;
+    *reinterpret_cast<float4*>(&S.c1[Q.i * 72 + Q.j * 8 + Q.k0]) = o.a1;
     const int c2o = Q.i * 72 + Q.j * 9 + Q.k0;
-    S.c2[c2o + 0] = a2.x;
-    S.c2[c2o + 1] = a2.y;
-    S.c2[c2o + 2] = a2.z;
-    S.c2[c2o + 3] = a2.w;
+    S.c2[c2o + 0] = o.a2.x;
+    S.c2[c2o + 1] = o.a2.y;
+    S.c2[c2o + 2] = o.a2.z;
+    S.c2[c2o + 3] = o.a2.w;
     sync();
 
+    const int e = side ? 7 : 0;     // own boundary layer next to the face
+    const int hx = side ? 8 : -1;   // halo layer
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-        const int hh = Q.q + 128 * r;
-        const int f = hh >> 6, fi = hh & 63;
-        const int axis = f >> 1, s = f & 1;
-        const int a = fi >> 3, b = fi & 7;
-        const int axk = s ? 8 : -1;
-        int fl[3], cl[3];
-        if (axis == 0) { fl[0] = axk; fl[1] = a; fl[2] = b; }
-        else if (axis == 1) { fl[0] = a; fl[1] = axk; fl[2] = b; }
-        else { fl[0] = a; fl[1] = b; fl[2] = axk; }
-        cl[0] = fl[0]; cl[1] = fl[1]; cl[2] = fl[2];
-        cl[axis] = s ? 7 : 0;
-        const int fx = sx(fl[0], fl[1], fl[2]);
+        int cl[3];
+        cl[0] = r == 0 ? e : fa;
+        cl[1] = r == 0 ? fa : r == 1 ? e : fb;
+        cl[2] = r == 2 ? e : fb;
+        const int fx = r == 0 ? sx(hx, fa, fb) : r == 1 ? sx(fa, hx, fb) : sx(fa, fb, hx);
         float v = hv[r];
         if (desc[r] != 0 && (desc[r] & dGhost)) {
+            // T-junction: x_in + 0.5 * (x_ghost - mean of the 2x2x2 block of own cells at the face)
             float avg = 0.0f;
 #pragma unroll
             for (int di = 0; di < 2; ++di)
@@ -235,16 +236,38 @@ __device__ __forceinline__ void load_snap(const DevGrid& g, int t, const float* 
                 for (int dj = 0; dj < 2; ++dj)
 #pragma unroll
                     for (int dk = 0; dk < 2; ++dk) avg = __fadd_rn(avg, S.x[sx(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)]);
-            avg = __fdiv_rn(avg, 8.0f);
+            avg = __fmul_rn(avg, 0.125f);  // equals avg / 8 (scaling by a power of two)
             v = __fmaf_rn(0.5f, __fsub_rn(hv[r], avg), S.x[sx(cl[0], cl[1], cl[2])]);
         }
         S.x[fx] = v;
-        if (s) {
-            float* cslot = axis == 0 ? &S.c0[8 * 64 + a * 8 + b] : axis == 1 ? &S.c1[a * 72 + 64 + b] : &S.c2[a * 72 + b * 9 + 8];
+        if (side) {
+            float* cslot = r == 0 ? &S.c0[8 * 64 + fa * 8 + fb] : r == 1 ? &S.c1[fa * 72 + 64 + fb] : &S.c2[fa * 72 + fb * 9 + 8];
             *cslot = hc[r];
         }
     }
     sync();
+}
+
+// negativeLap of own cell u (0..3) of the thread: the snapshot's stencil with the
+// thread's own x and negative-face coefficients taken from registers; same
+// operands in the same order as snap_neg_lap.
+template <int U>
+__device__ __forceinline__ float own_neg_lap(const Snap& S, const Quad& Q, const Own& o) {
+    const float d = f4get(o.dg, U);
+    if (d == 0.0f) return 0.0f;
+    const int k = Q.k0 + U;
+    const int c = sx(Q.i, Q.j, k);
+    float s = __fmul_rn(f4get(o.xm, U), d);
+    s = __fmaf_rn(f4get(o.a0, U), S.x[c - 100], s);
+    s = __fmaf_rn(S.c0[(Q.i + 1) * 64 + Q.j * 8 + k], S.x[c + 100], s);
+    s = __fmaf_rn(f4get(o.a1, U), S.x[c - 10], s);
+    s = __fmaf_rn(S.c1[Q.i * 72 + (Q.j + 1) * 8 + k], S.x[c + 10], s);
+    s = __fmaf_rn(f4get(o.a2, U), U > 0 ? f4get(o.xm, U - 1) : S.x[c - 1], s);
+    s = __fmaf_rn(U < 3 ? f4get(o.a2, U + 1) : S.c2[Q.i * 72 + Q.j * 9 + k + 1], U < 3 ? f4get(o.xm, U + 1) : S.x[c + 1], s);
+    return s;
+}
+__device__ __forceinline__ float own_neg_lap(const Snap& S, const Quad& Q, const Own& o, int u) {
+    return u == 0 ? own_neg_lap<0>(S, Q, o) : u == 1 ? own_neg_lap<1>(S, Q, o) : u == 2 ? own_neg_lap<2>(S, Q, o) : own_neg_lap<3>(S, Q, o);
 }
 
 // Block-wide deterministic double reduction for 128 threads; result valid in thread 0.
@@ -272,12 +295,32 @@ __device__ __forceinline__ double block_sum128(double v, double* red) {
 // innocuous?", ACM SIGNUM Newsletter 30(3), 1995), applied to the product with a
 // correctly rounded reciprocal.  Zero, subnormal, huge and non-finite cases take
 // the IEEE division itself.
+// The argument holds for any yd within 2^-52 (relative) of 1/d, not only for the
+// correctly rounded one.
 __device__ __forceinline__ float div_by_recip(float a, float d, double yd) {
     const float q = __double2float_rn(__dmul_rn((double)a, yd));
     const float m = fabsf(q);
     if (m >= 0x1p-125f && m <= 0x1p127f) return q;
-    if (a == 0.0f && d != 0.0f) return q;
+    // 0 / d for nonzero, non-NaN d: zero with the sign of a * d
+    if (a == 0.0f && d != 0.0f && !isnan(d)) return __int_as_float((__float_as_int(a) ^ __float_as_int(d)) & 0x80000000);
     return __fdiv_rn(a, d);
 }
+// 1/d in double within 2^-52 (relative) for normal d: the single-precision
+// hardware reciprocal (relative error below 2^-22) refined by two Newton-Raphson
+// steps y <- y + y*(1 - d*y) in double (the error squares at each step, then one
+// double rounding remains).  Zero, subnormal, infinite and huge d give inf, NaN or
+// 0 here, which div_by_recip sends to the IEEE division.
+__device__ __forceinline__ double recip_f64(float d) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+    const double dd = (double)d;
+    double y = (double)r;
+    y = __fma_rn(y, __fma_rn(-dd, y, 1.0), y);
+    y = __fma_rn(y, __fma_rn(-dd, y, 1.0), y);
+    return y;
+}
+// a / d, bit-identical to the IEEE division, without the long latency of the
+// division routine on the dependent chain of a Gauss-Seidel update
+__device__ __forceinline__ float div_exact(float a, float d) { return div_by_recip(a, d, recip_f64(d)); }
 
 }  // namespace cmg

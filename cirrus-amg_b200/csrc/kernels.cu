@@ -56,19 +56,19 @@ template <class Sync>
 __device__ __forceinline__ void tile_gs(const DevGrid& g, int t, int tid, float* X, const float* B, int color, const SmoothArgs& A,
                                         Snap& S, const Sync& sync) {
     const Quad Q(t, tid);
-    float4 xr, dg;
-    uchar4 ty;
-    load_snap(g, t, X, A.coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg, sync);
+    Own o;
+    load_snap(g, t, X, A.coeff_ch, MgHalo{X, g.ctype}, S, Q, o, sync);
     const float4 b = ldcg4(B + Q.base);
-    float4 out = xr;
+    float4 out = o.xr;
+    // cells of this colour: u = p and u = p + 2
+    const int p = (Q.i + Q.j + Q.k0 + color) & 1;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int k = Q.k0 + u;
-        if (((Q.i + Q.j + k) & 1) != color) continue;
-        const float d = f4get(dg, u);
-        const float ax = snap_neg_lap(S, Q.i, Q.j, k, d);
-        const float delta = (t4get(ty, u) & dInterior) ? __fdiv_rn(__fsub_rn(f4get(b, u), ax), d) : 0.0f;
-        const float xs = S.x[sx(Q.i, Q.j, k)];
+    for (int h = 0; h < 2; ++h) {
+        const int u = p + 2 * h;
+        const float d = f4get(o.dg, u);
+        const float ax = own_neg_lap(S, Q, o, u);
+        const float delta = (t4get(o.ty, u) & dInterior) ? div_exact(__fsub_rn(f4get(b, u), ax), d) : 0.0f;
+        const float xs = f4get(o.xm, u);
         f4set(out, u, A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega));
     }
     st4(X + Q.base, out);
@@ -80,12 +80,13 @@ template <class Sync>
 __device__ __forceinline__ void tile_restrict(const DevGrid& g, int t, int tid, float* X, float* RHS, int coeff_ch, float Rr, Snap& S,
                                               float* res, const Sync& sync) {
     const Quad Q(t, tid);
-    float4 xr, dg;
-    uchar4 ty;
-    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg, sync);
+    Own o;
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, o, sync);
     const float4 rh = ldcg4(RHS + Q.base);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) res[4 * Q.q + u] = __fsub_rn(f4get(rh, u), snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u)));
+    res[4 * Q.q + 0] = __fsub_rn(rh.x, own_neg_lap<0>(S, Q, o));
+    res[4 * Q.q + 1] = __fsub_rn(rh.y, own_neg_lap<1>(S, Q, o));
+    res[4 * Q.q + 2] = __fsub_rn(rh.z, own_neg_lap<2>(S, Q, o));
+    res[4 * Q.q + 3] = __fsub_rn(rh.w, own_neg_lap<3>(S, Q, o));
     sync();
     if (tid < 64) {
         const int b = tid;
@@ -105,7 +106,7 @@ __device__ __forceinline__ void tile_restrict(const DevGrid& g, int t, int tid, 
             const int4 m = g.meta[t];
             const size_t o = (size_t)p * kCells + cell_index(parent_local(m.y, f0), parent_local(m.z, f1), parent_local(m.w, f2));
             RHS[o] = __fmul_rn(rs, Rr);
-            X[o] = __fdiv_rn(xs, 8.0f);
+            X[o] = __fmul_rn(xs, 0.125f);  // equals xs / 8
         }
     }
     sync();
@@ -116,15 +117,14 @@ template <class Sync>
 __device__ __forceinline__ void tile_fas_save(const DevGrid& g, int t, int tid, const float* X, float* RHS, float* X0, int coeff_ch,
                                               Snap& S, const Sync& sync) {
     const Quad Q(t, tid);
-    float4 xr, dg;
-    uchar4 ty;
-    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, xr, ty, dg, sync);
+    Own o;
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, o, sync);
     float4 rh = ldcg4(RHS + Q.base);
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-        if (t4get(ty, u) & dInterior) {
-            f4set(rh, u, __fadd_rn(f4get(rh, u), snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u))));
-            X0[Q.base + u] = f4get(xr, u);
+        if (t4get(o.ty, u) & dInterior) {
+            f4set(rh, u, __fadd_rn(f4get(rh, u), own_neg_lap(S, Q, o, u)));
+            X0[Q.base + u] = f4get(o.xr, u);
         } else {
             f4set(rh, u, 0.0f);
         }
@@ -225,7 +225,7 @@ struct DenseLevel {
             const int k = 2 * kh + ((i + j + color) & 1);
             const int c = ci(i, j, k);
             const float ax = neg_lap(i, j, k);
-            const float delta = (ty[c] & dInterior) ? __fdiv_rn(__fsub_rn(rhs[c], ax), d[c]) : 0.0f;
+            const float delta = (ty[c] & dInterior) ? div_exact(__fsub_rn(rhs[c], ax), d[c]) : 0.0f;
             const float xs = x[xi(i, j, k)];
             x[xi(i, j, k)] = A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega);
         }
@@ -339,7 +339,7 @@ __device__ void coarse_dense(const DevGrid& g, const CoarseArgs& A, float* X, fl
                         xs = __fadd_rn(xs, L1.x[DenseLevel<16>::xi(2 * i + ii, 2 * j + jj, 2 * k + kk)]);
                     }
             L0.rhs[v] = __fmul_rn(rs, A.Rr);
-            L0.x[DenseLevel<8>::xi(i, j, k)] = L0.ty[v] == dInterior ? __fdiv_rn(xs, 8.0f) : 0.0f;
+            L0.x[DenseLevel<8>::xi(i, j, k)] = L0.ty[v] == dInterior ? __fmul_rn(xs, 0.125f) : 0.0f;
         }
         __syncthreads();
         // FASSaveSolutionAndUpdateSource on the root
@@ -514,16 +514,16 @@ __global__ void __launch_bounds__(128) k_leaf_apply(DevGrid g, const int* leaf, 
     __shared__ double red[4];
     const int t = leaf[blockIdx.x];
     const Quad Q(t, threadIdx.x);
-    float4 xr, dg;
-    uchar4 ty;
-    load_snap(g, t, P, coeff_ch, LeafHalo{P, g.ctype}, S, Q, xr, ty, dg, BlockSync{});
+    Own o;
+    load_snap(g, t, P, coeff_ch, LeafHalo{P, g.ctype}, S, Q, o, BlockSync{});
     float4 ap;
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-        f4set(ap, u, t4get(ty, u) == dInterior ? snap_neg_lap(S, Q.i, Q.j, Q.k0 + u, f4get(dg, u)) : 0.0f);
+    ap.x = o.ty.x == dInterior ? own_neg_lap<0>(S, Q, o) : 0.0f;
+    ap.y = o.ty.y == dInterior ? own_neg_lap<1>(S, Q, o) : 0.0f;
+    ap.z = o.ty.z == dInterior ? own_neg_lap<2>(S, Q, o) : 0.0f;
+    ap.w = o.ty.w == dInterior ? own_neg_lap<3>(S, Q, o) : 0.0f;
     st4(AP + Q.base, ap);
     if (!fuse) return;
-    const double bs = block_sum128(dot4(xr, ap), red);
+    const double bs = block_sum128(dot4(o.xr, ap), red);
     if (threadIdx.x == 0) rs.partial[blockIdx.x] = bs;
     if (last_block(&rs.s->counter[0])) {
         const double tot = sum_partials(rs.partial, gridDim.x, red);
@@ -1007,9 +1007,8 @@ __global__ void __launch_bounds__(128) k_gradient(DevGrid g, const float* X, int
     const int t = blockIdx.x;
     if (!(tile_type(g, t) & (dLeaf | dGhost))) return;
     const Quad Q(t, threadIdx.x);
-    float4 xr, dg;
-    uchar4 ty;
-    load_snap(g, t, X, coeff_ch, LeafHalo{X, g.ctype}, S, Q, xr, ty, dg, BlockSync{});
+    Own o;
+    load_snap(g, t, X, coeff_ch, LeafHalo{X, g.ctype}, S, Q, o, BlockSync{});
     const float h = voxel_size(g.h0, tile_level(g, t));
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -1070,7 +1069,8 @@ __device__ __forceinline__ float make_float(unsigned long long r, int emin, int 
     const int e = emin + (int)((r >> 32) % (unsigned long long)(emax - emin + 1));
     return __uint_as_float(sign | ((unsigned)(e + 127) << 23) | ((unsigned)r & 0x7fffffu));
 }
-// Compares div_by_recip with the IEEE division on pseudo-random pairs: a quarter
+// Compares div_by_recip (with the correctly rounded reciprocal) and div_exact
+// (with the Newton-refined one) with the IEEE division on pseudo-random pairs: a quarter
 // uniform in sign, exponent and significand; a quarter built to fall within a few
 // ulps of a midpoint between two floats (a = RN(d * m) for a midpoint m); a quarter
 // shaped like Gauss-Seidel updates; a quarter of zeros, subnormals, huge values,
@@ -1105,7 +1105,9 @@ __global__ void k_check_division(long long n, unsigned long long seed, unsigned 
         }
         const float want = __fdiv_rn(a, d);
         const float got = div_by_recip(a, d, 1.0 / (double)d);
-        const bool same = (__float_as_uint(want) == __float_as_uint(got)) || (isnan(want) && isnan(got));
+        const float got2 = div_exact(a, d);
+        const bool same = ((__float_as_uint(want) == __float_as_uint(got)) || (isnan(want) && isnan(got))) &&
+                          ((__float_as_uint(want) == __float_as_uint(got2)) || (isnan(want) && isnan(got2)));
         if (!same) {
             if (atomicAdd(mism, 1ull) == 0ull) {
                 first[0] = __float_as_uint(a);

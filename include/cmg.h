@@ -66,9 +66,10 @@ typedef int (*cmg_level_target_fn)(void* user, int level, int i, int j, int k);
 
 const char* cmg_last_error(void);
 int cmg_version(void);
-/* Self-check of the division the Gauss-Seidel sweeps of the coarse levels use
- * (one double multiply by a precomputed reciprocal, rounded to float) against
- * the IEEE float division, on n pseudo-random pairs from `seed`.  mismatches
+/* Self-check of the division the Gauss-Seidel sweeps use (one double multiply
+ * by a double reciprocal of the divisor, rounded to float; the reciprocal either
+ * correctly rounded or refined by Newton steps) against the IEEE float
+ * division, on n pseudo-random pairs from `seed`.  mismatches
  * receives the number of results that differ in any bit; first_pair (may be
  * NULL) the bit patterns of the first differing (a, d).  No counterpart in the
  * reference, which divides directly (src/AMGSolver.cu:868-875). */
