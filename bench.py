@@ -131,6 +131,24 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def replica_time(total_ms, world, device=None):
+    """Whole-job time of N independent replicas: the slowest rank's device time
+    (all_reduce MAX over the default process group; identity for one rank)."""
+    if world <= 1:
+        return total_ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def per_solve_ms(total_ms, steps, world):
+    """ms per solve of the whole job: N replicas each ran `steps` solves in `total_ms`."""
+    return total_ms / (steps * world)
+
+
 def build_workload(cmg):
     G = cmg.HADeviceGrid(0.125, 10, 16)
     G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
@@ -232,11 +250,8 @@ def run_ours(args, rank, world, local_rank):
     e1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    total_ms = e0.elapsed_time(e1)
+    total_ms = replica_time(e0.elapsed_time(e1), world, dev)
     if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
 
     # true residual of the last solution, FP32 operator apply on the device
@@ -293,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
 
     result = None
     if rank == 0:
-        per_solve = total_ms / (args.steps * world)
+        per_solve = per_solve_ms(total_ms, args.steps, world)
         result = {
             "metric": METRIC,
             "value": round(per_solve, 4),
