@@ -39,7 +39,7 @@ EXPORTS = [
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
     "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_add_gradient_to_face", "cmg_amg_full_neg_lap",
-    "cmg_amg_dot",
+    "cmg_amg_dot", "cmg_amg_dot_noalloc",
     "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solver_set_launch_mode",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
@@ -96,6 +96,7 @@ def lib():
             "cmg_amg_add_gradient_to_face": (I, [P, I, I, I]),
             "cmg_amg_full_neg_lap": (I, [P, I, I, I]),
             "cmg_amg_dot": (I, [P, I, I, P]),
+            "cmg_amg_dot_noalloc": (I, [P, I, I, P]),
             "cmg_amg_solver_create": (I, [I, F, F, F, PP]),
             "cmg_amg_solver_destroy": (I, [P]),
             "cmg_amg_solver_set_smoother": (I, [P, D, I]),

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <exception>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "cmg_impl.hpp"
@@ -314,6 +315,20 @@ int cmg_amg_dot(cmg_grid* g, int a_ch, int b_ch, double* out) {
     CKC(cudaMemcpyAsync(out, G.dot_out, sizeof(double), cudaMemcpyDeviceToHost, G.stream));
     CKC(cudaStreamSynchronize(G.stream));
     return CMG_OK;
+}
+
+int cmg_amg_dot_noalloc(cmg_grid* g, int a_ch, int b_ch, double* out) {
+    if (!host_ready(g) || !out) return fail(CMG_ERR_STATE, "cmg_amg_dot_noalloc: grid not built or null result pointer");
+    if (!chan_ok(g, a_ch) || !chan_ok(g, b_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_dot_noalloc: channel out of range");
+    cmg::Grid& G = g->g;
+    const int nleaf = (int)G.topo.leaf_list.size();
+    if (nleaf > cmg::dot_noalloc_max_leaf_tiles()) {
+        return fail(CMG_ERR_INVALID, ("cmg_amg_dot_noalloc: " + std::to_string(nleaf) + " LEAF tiles exceed its fixed scratch of " +
+                                      std::to_string(cmg::dot_noalloc_max_leaf_tiles()) + " tiles").c_str());
+    }
+    // uploading the topology would allocate: the device copy must already be current
+    if (G.dev_version != G.host_version || G.n <= 0) return fail(CMG_ERR_STATE, "cmg_amg_dot_noalloc: the grid has no current device copy");
+    return cmg::check_cuda(cmg::dot_noalloc(G.leaf, G.nleaf, G.plane(a_ch), G.plane(b_ch), out, G.stream), "cmg_amg_dot_noalloc");
 }
 
 int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float P, cmg_amg_solver** out) {

@@ -132,6 +132,14 @@ int cmg_amg_add_gradient_to_face(cmg_grid* g, int x_ch, int coeff_ch, int u_ch);
 int cmg_amg_full_neg_lap(cmg_grid* g, int x_ch, int coeff_ch, int ax_ch);
 /* Dot over LEAF tiles (src/PoissonGrid.cu:203) */
 int cmg_amg_dot(cmg_grid* g, int a_ch, int b_ch, double* out);
+/* The same dot product as cmg_amg_dot (equal bit for bit), for callers that may not
+ * allocate at the call: it allocates no memory.  Its scratch is a fixed 128 KB array in
+ * the library's static device memory, so it serves grids of at most 16384 LEAF tiles
+ * (larger grids: CMG_ERR_INVALID) and needs the grid's device copy to be current
+ * already (CMG_ERR_STATE otherwise).  Calls that overlap in time share that scratch and
+ * race.  The first call on a device looks up the scratch address.  No counterpart in
+ * the reference. */
+int cmg_amg_dot_noalloc(cmg_grid* g, int a_ch, int b_ch, double* out);
 
 /* ---- solver: AMGSolver ------------------------------------------------- */
 /* AMGSolver(coeff_channel, R_matrix, R_restrict, P) (src/AMGSolver.h:309);
