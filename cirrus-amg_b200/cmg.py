@@ -297,11 +297,12 @@ class AMGSolver:
         except Exception:
             pass
 
-    def set_launch_mode(self, use_graph=True, persistent=False, cluster=True):
+    def set_launch_mode(self, use_graph=True, persistent=False, cluster=True, pipeline=True):
         """use_graph: one CUDA graph per solve (default) or kernel-by-kernel launches;
         persistent: levels 2-3 of each cycle in one cooperative kernel (off by default);
-        cluster: each visit of level 2 in one 9-CTA cluster launch when levels 0-2 are complete."""
-        flags = (1 if use_graph else 0) | (2 if persistent else 0) | (0 if cluster else 4)
+        cluster: each visit of level 2 in one 9-CTA cluster launch when levels 0-2 are complete;
+        pipeline: the cycle's smoothing sweeps as a persistent kernel that prefetches the next tile."""
+        flags = (1 if use_graph else 0) | (2 if persistent else 0) | (0 if cluster else 4) | (0 if pipeline else 8)
         _check(self.L.cmg_amg_solver_set_launch_mode(self.h, flags), "set_launch_mode")
 
     def _sync_params(self):

@@ -355,9 +355,10 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu) {
     return CMG_OK;
 }
 int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags) {
-    if (!s || (flags & ~7)) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_launch_mode: bad argument");
+    if (!s || (flags & ~15)) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_launch_mode: bad argument");
     s->s.use_graph = (flags & CMG_LAUNCH_GRAPH) != 0;
     s->s.use_cluster = (flags & CMG_LAUNCH_NO_CLUSTER) == 0;
+    s->s.use_pipe = (flags & CMG_LAUNCH_NO_PIPELINE) == 0;
     s->s.use_persist = (flags & CMG_LAUNCH_PERSISTENT) != 0 && s->s.persist_nblocks > 0;
     return CMG_OK;
 }

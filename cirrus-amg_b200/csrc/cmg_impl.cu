@@ -207,6 +207,7 @@ int Solver::init() {
     persist_nblocks = persist_blocks();
     if (persist_nblocks <= 0) use_persist = false;
     cluster_ok = cluster_step_supported();
+    pipe_ok = gs_pipe_init() > 0;
     if (cluster_ok) CK(cudaMalloc(&cluster_pack, cluster_pack_bytes()));
     return check_cuda(cudaGetLastError(), "kernel attributes");
 }
@@ -240,13 +241,16 @@ MuArgs Solver::mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters
 }
 
 // GaussSeidelAMG (src/AMGSolver.cu:887-894) on the LEAF and NONLEAF tiles of one level
-void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const {
+void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined) const {
     const DevGrid d = G.dev();
     const int t0 = G.level_begin(level), nt = G.ghost_begin(level) - t0;
-    for (int it = 0; it < iters; ++it) {
-        launch_gs(d, t0, nt, X, RHS, coeff_ch, order, omega, st);
-        launch_gs(d, t0, nt, X, RHS, coeff_ch, 1 - order, omega, st);
-    }
+    const bool pipe = pipelined && use_pipe && pipe_ok;
+    for (int it = 0; it < iters; ++it)
+        for (int h = 0; h < 2; ++h) {
+            const int color = h ? 1 - order : order;
+            if (pipe) launch_gs_pipe(d, t0, nt, X, RHS, coeff_ch, color, omega, st);
+            else launch_gs(d, t0, nt, X, RHS, coeff_ch, color, omega, st);
+        }
 }
 
 // Levels 0-2 are complete 8^3, 16^3 and 32^3 grids: a NONLEAF root, eight
@@ -310,12 +314,12 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) c
                             bar, persist_nblocks, st);
         return;
     }
-    enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st);
+    enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st, true);
     launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
     launch_fas_save(d, G.nonleaf_begin(l - 1), G.ghost_begin(l - 1) - G.nonleaf_begin(l - 1), A.X, A.RHS, A.X0, A.coeff_ch, st);
     for (int r = 0; r < A.mu; ++r) enqueue_mu_step(G, l - 1, A, st);
     launch_prolong(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), A.X, A.X0, A.P, st);
-    enqueue_gs(G, l, A.level_iters, 1, A.X, A.RHS, st);
+    enqueue_gs(G, l, A.level_iters, 1, A.X, A.RHS, st, true);
 }
 
 // AMGSolver::FASMuCycle (src/AMGSolver.cu:1279-1292): zero x everywhere, then the top step
@@ -437,7 +441,7 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     }
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
-    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0), omega};
+    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0), omega};
     Plan plan{};
     if (use_graph) {
         auto it = graphs.find(k);

@@ -114,13 +114,16 @@ struct Solver {
     int ensure_scratch(int nleaf);
     ReduceScratch scratch() const { return ReduceScratch{partial, partial2, s}; }
     MuArgs mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) const;
-    void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
+    // pipelined: the x plane is known to be masked to INTERIOR cells (inside the cycle)
+    void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined = false) const;
     void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
     bool use_graph = true;    // false: launch kernel by kernel from the host (profiling)
     bool use_persist = false;  // levels 2-3 in one cooperative kernel per visit
     bool use_cluster = true;   // levels 0-2 in one cluster launch per visit of level 2
     bool cluster_ok = false;   // the device can run that cluster
+    bool use_pipe = true;      // pipelined smoothing kernel inside the cycle
+    bool pipe_ok = false;      // the device can run it
     void* cluster_pack = nullptr;  // packed static operands of levels 0-2 (launch_cluster_pack)
     bool cluster_active(const Grid& G) const;
     void enqueue_cluster_pack(Grid& G, cudaStream_t st) const;

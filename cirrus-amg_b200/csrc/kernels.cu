@@ -106,7 +106,10 @@ __device__ __forceinline__ void tile_restrict(const DevGrid& g, int t, int tid, 
             const int4 m = g.meta[t];
             const size_t o = (size_t)p * kCells + cell_index(parent_local(m.y, f0), parent_local(m.z, f1), parent_local(m.w, f2));
             RHS[o] = __fmul_rn(rs, Rr);
-            X[o] = __fmul_rn(xs, 0.125f);  // equals xs / 8
+            // mean of the 8 children (xs / 8), stored as 0 on cells that are not INTERIOR: every read
+            // of a multigrid x masks it that way, and keeping the plane masked lets the pipelined
+            // smoother read neighbour values without their cell types
+            X[o] = (g.ctype[o] & dInterior) ? __fmul_rn(xs, 0.125f) : 0.0f;
         }
     }
     sync();

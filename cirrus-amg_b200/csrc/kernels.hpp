@@ -24,6 +24,10 @@ struct ReduceScratch {
 };
 
 // --- multigrid ---
+// persistent, software-pipelined colour pass for the multigrid cycle (gs_pipe.cu); needs the
+// x plane masked to INTERIOR cells.  gs_pipe_init: resident blocks on the device (0: unusable).
+int gs_pipe_init();
+void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float R_restrict, cudaStream_t st);
 void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st);

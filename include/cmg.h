@@ -157,11 +157,15 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
  * NO_CLUSTER: when levels 0-2 are complete grids, each visit of level 2 (with
  * its recursion through levels 1 and 0) normally runs as one launch of an
  * 9-CTA thread-block cluster; this flag launches those phases separately.
+ * NO_PIPELINE: the smoothing sweeps of the cycle normally run as a persistent
+ * kernel that loads the next tile while it computes one; this flag uses one
+ * block per tile instead.
  * None has a counterpart in the reference, which launches every phase from
  * the host. */
 #define CMG_LAUNCH_GRAPH 1
 #define CMG_LAUNCH_PERSISTENT 2
 #define CMG_LAUNCH_NO_CLUSTER 4
+#define CMG_LAUNCH_NO_PIPELINE 8
 int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
 /* AMGSolver::solve (src/AMGSolver.cu:1399): solves -lap x = b, b read from
  * channel 1 and overwritten by the residual, x written to channel 0.

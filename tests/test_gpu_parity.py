@@ -284,7 +284,7 @@ def test_kat_projection_on_gpu(prm):
     assert rel < 1e-6 and ratio < 1e-5, (it, rel, ratio)
 
 
-def _mu_cycle_planes(G, solver, cluster, seed, mu, omega):
+def _mu_cycle_planes(G, solver, cluster, seed, mu, omega, pipeline=True):
     rng = np.random.default_rng(seed)
     n = G.num_tiles
     solver.mu_cycle_repeat_times = mu
@@ -292,7 +292,7 @@ def _mu_cycle_planes(G, solver, cluster, seed, mu, omega):
     G.upload(1, rng.standard_normal((n, 512)).astype(np.float32))
     G.upload(3, rng.standard_normal((n, 512)).astype(np.float32))
     G.upload(4, rng.standard_normal((n, 512)).astype(np.float32))
-    solver.set_launch_mode(use_graph=False, cluster=cluster)
+    solver.set_launch_mode(use_graph=False, cluster=cluster, pipeline=pipeline)
     solver.fas_mu_cycle(G, 4, 1, 3, 2, 10)
     return G.download(4), G.download(1), G.download(3)
 
@@ -334,3 +334,27 @@ def test_division_by_reciprocal_is_ieee_exact(seed):
     on 2^26 adversarial pairs it must equal the IEEE division bit for bit."""
     m, first = cmg.check_division(1 << 26, seed)
     assert m == 0, (m, [hex(v) for v in first])
+
+
+@pytest.mark.parametrize("grid", ["uniform64", "shell345", "shell456"])
+def test_pipelined_smoother_matches_per_tile_launches(grid):
+    """The persistent, prefetching smoothing kernel gives the same x, rhs and saved x on
+    every tile as one block per tile, through a whole mu-cycle and a whole solve."""
+    if grid == "uniform64":
+        G, _, solver, _ = setup_uniform(3, with_oracle=False)
+    else:
+        prm = shell_params(coarse=3, mid=4, fine=5) if grid == "shell345" else shell_params(coarse=4, mid=5, fine=6)
+        G, _, solver = setup_shell(prm, with_oracle=False)
+    b = G.download(1)
+    a = _mu_cycle_planes(G, solver, True, 17, 2, 1.5, pipeline=True)
+    c = _mu_cycle_planes(G, solver, True, 17, 2, 1.5, pipeline=False)
+    for pa, pc in zip(a, c):
+        assert np.array_equal(pa, pc)
+    res = []
+    for pipeline in (False, True):
+        G.upload(1, b)
+        solver.set_launch_mode(use_graph=True, pipeline=pipeline)
+        it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+        res.append((it, rel, G.download(0)))
+    assert res[0][:2] == res[1][:2]
+    assert np.array_equal(res[0][2], res[1][2])
