@@ -36,11 +36,13 @@ EXPORTS = [
     "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
     "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
     "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_copy_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
+    "cmg_grid_calc_cell_types_from_leafs",
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
     "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_add_gradient_to_face", "cmg_amg_full_neg_lap",
     "cmg_amg_dot", "cmg_amg_dot_noalloc",
     "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solver_set_launch_mode",
+    "cmg_gmg_solver_create", "cmg_cmg_solver_create", "cmg_mg_vcycle", "cmg_mg_gauss_seidel", "cmg_mg_full_neg_lap",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
     "cmg_amg_last_solve_launches",
@@ -87,6 +89,7 @@ def lib():
             "cmg_grid_copy_channel": (I, [P, I, I]),
             "cmg_grid_set_leaf_cell_types_case": (I, [P, I, P, I]),
             "cmg_grid_set_stream": (I, [P, P]),
+            "cmg_grid_calc_cell_types_from_leafs": (I, [P]),
             "cmg_grid_synchronize": (I, [P]),
             "cmg_amg_prepare_types_and_coeffs": (I, [P, I, F]),
             "cmg_amg_prepare_system": (I, [P, I, F]),
@@ -101,6 +104,11 @@ def lib():
             "cmg_amg_solver_destroy": (I, [P]),
             "cmg_amg_solver_set_smoother": (I, [P, D, I]),
             "cmg_amg_solver_set_launch_mode": (I, [P, I]),
+            "cmg_gmg_solver_create": (I, [F, F, PP]),
+            "cmg_cmg_solver_create": (I, [F, F, PP]),
+            "cmg_mg_vcycle": (I, [P, P, I, I, I, I, I]),
+            "cmg_mg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
+            "cmg_mg_full_neg_lap": (I, [P, P, I, I]),
             "cmg_amg_solve": (I, [P, P, I, I, D, I, I, I, I, P, P]),
             "cmg_amg_solve_host": (I, [P, P, P, P, S, I, D, I, I, I, I, P, P]),
             "cmg_amg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
@@ -236,6 +244,10 @@ class HADeviceGrid:
     def copy(self, src_ch, dst_ch):
         _check(self.L.cmg_grid_copy_channel(self.h, src_ch, dst_ch), "copy_channel")
 
+    def calc_cell_types_from_leafs(self):
+        """CalcCellTypesFromLeafs (src/PoissonGrid.cu:923): NONLEAF and GHOST cell types from the LEAF ones."""
+        _check(self.L.cmg_grid_calc_cell_types_from_leafs(self.h), "calc_cell_types_from_leafs")
+
     def set_leaf_cell_types_case(self, case_id, params=(0, 0)):
         prm = np.asarray(params, dtype=np.float64)
         _check(self.L.cmg_grid_set_leaf_cell_types_case(self.h, case_id, _p(prm), len(prm)), "set_leaf_cell_types")
@@ -345,3 +357,47 @@ class AMGSolver:
         n = ctypes.c_longlong(0)
         _check(self.L.cmg_amg_last_solve_launches(self.h, ctypes.byref(n)), "last_solve_launches")
         return n.value
+
+
+class _GeometricSolver(AMGSolver):
+    """Common part of GMGSolver and CMGSolver: PCG preconditioned by one V-cycle."""
+
+    _create = None
+
+    def __init__(self, one_over_alpha=1.0, prolong_coeff=1.0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        _check(getattr(self.L, self._create)(one_over_alpha, prolong_coeff, ctypes.byref(h)), self._create)
+        self.h = h
+        self.one_over_alpha = one_over_alpha
+        self.prolong_coeff = prolong_coeff
+        self.omega = 1.5  # unused by the V-cycle smoother; kept for the shared launch plumbing
+        self.mu_cycle_repeat_times = 1
+
+    def prepareTypesAndCoeffs(self, grid):
+        raise CmgError("geometric solvers derive their operator from tile and cell types: set the LEAF cell types, "
+                       "then HADeviceGrid.calc_cell_types_from_leafs()")
+
+    def VCycle(self, grid, x_channel, f_channel, rhs_channel, level_iters, coarsest_iters):
+        _check(self.L.cmg_mg_vcycle(self.h, grid.h, x_channel, f_channel, rhs_channel, level_iters, coarsest_iters), "VCycle")
+
+    def gauss_seidel(self, grid, iters, order, level, x_ch, rhs_ch):
+        _check(self.L.cmg_mg_gauss_seidel(self.h, grid.h, iters, order, level, x_ch, rhs_ch), "gauss_seidel")
+
+    def full_neg_lap(self, grid, x_channel, ax_channel):
+        _check(self.L.cmg_mg_full_neg_lap(self.h, grid.h, x_channel, ax_channel), "full_neg_lap")
+
+    def fas_mu_cycle(self, *args, **kwargs):
+        raise CmgError("fas_mu_cycle belongs to AMGSolver; geometric solvers use VCycle")
+
+
+class GMGSolver(_GeometricSolver):
+    """GMGSolver(one_over_alpha, prolong_coeff) (src/GMGSolver.h:17-52)."""
+
+    _create = "cmg_gmg_solver_create"
+
+
+class CMGSolver(_GeometricSolver):
+    """CMGSolver(one_over_alpha, prolong_coeff) (src/CMGSolver.h:17-50)."""
+
+    _create = "cmg_cmg_solver_create"

@@ -16,6 +16,7 @@ struct cmg_grid {
 struct cmg_amg_solver {
     cmg::Solver s;
     cmg_amg_solver(int c, float rm, float rr, float p) : s(c, rm, rr, p) {}
+    cmg_amg_solver(int kind, float one_over_alpha, float prolong) : s(kind, one_over_alpha, prolong) {}
 };
 
 namespace {
@@ -195,6 +196,15 @@ int cmg_grid_copy_channel(cmg_grid* g, int src_ch, int dst_ch) {
     CKC(cudaMemcpyAsync(g->g.plane(dst_ch), g->g.plane(src_ch), sizeof(float) * (size_t)g->g.n * 512, cudaMemcpyDeviceToDevice,
                         g->g.stream));
     return CMG_OK;
+}
+int cmg_grid_calc_cell_types_from_leafs(cmg_grid* g) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_calc_cell_types_from_leafs: grid not built");
+    cmg::Grid& G = g->g;
+    const cmg::DevGrid d = G.dev();
+    for (int L = G.max_level() - 1; L >= 0; --L)
+        cmg::launch_types_from_children(d, G.nonleaf_begin(L), G.ghost_begin(L) - G.nonleaf_begin(L), G.stream);
+    for (int L = 1; L <= G.max_level(); ++L) cmg::launch_ghost_types(d, G.ghost_begin(L), G.level_end(L) - G.ghost_begin(L), G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "calc_cell_types_from_leafs");
 }
 int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams) {
     GUARD_BEGIN
@@ -383,8 +393,55 @@ int cmg_amg_solve_host(cmg_amg_solver* s, cmg_grid* g, const float* b_host, floa
     return CMG_OK;
     GUARD_END
 }
+static int geo_create(int kind, float one_over_alpha, float prolong, cmg_amg_solver** out) {
+    if (!out) return fail(CMG_ERR_INVALID, "solver create: null output");
+    cmg_amg_solver* s = new cmg_amg_solver(kind, one_over_alpha, prolong);
+    int rc = s->s.init();
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return CMG_OK;
+}
+int cmg_gmg_solver_create(float one_over_alpha, float prolong_coeff, cmg_amg_solver** out) {
+    GUARD_BEGIN
+    return geo_create(cmg::kGMG, one_over_alpha, prolong_coeff, out);
+    GUARD_END
+}
+int cmg_cmg_solver_create(float one_over_alpha, float prolong_coeff, cmg_amg_solver** out) {
+    GUARD_BEGIN
+    return geo_create(cmg::kCMG, one_over_alpha, prolong_coeff, out);
+    GUARD_END
+}
+int cmg_mg_vcycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind == cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_mg_vcycle: the solver is an AMG solver (use cmg_amg_fas_mu_cycle)");
+    if (!chan_ok(g, x_ch) || !chan_ok(g, f_ch) || !chan_ok(g, rhs_ch) || level_iters < 0 || coarsest_iters < 0)
+        return fail(CMG_ERR_INVALID, "cmg_mg_vcycle: bad argument");
+    if (int rc = cmg::validate_solver_topology(g->g)) return rc;
+    s->s.enqueue_geo_vcycle(g->g, g->g.plane(x_ch), g->g.plane(f_ch), g->g.plane(rhs_ch), level_iters, coarsest_iters, g->g.stream);
+    return cmg::check_cuda(cudaGetLastError(), "mg_vcycle");
+}
+int cmg_mg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind == cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_mg_gauss_seidel: the solver is an AMG solver (use cmg_amg_gauss_seidel)");
+    if (level < 0 || level > g->g.max_level() || !chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || (order != 0 && order != 1) || iters < 0)
+        return fail(CMG_ERR_INVALID, "cmg_mg_gauss_seidel: bad argument");
+    s->s.enqueue_geo_gs(g->g, level, iters, order, g->g.plane(x_ch), g->g.plane(rhs_ch), g->g.stream);
+    return cmg::check_cuda(cudaGetLastError(), "mg_gauss_seidel");
+}
+int cmg_mg_full_neg_lap(cmg_amg_solver* s, cmg_grid* g, int x_ch, int ax_ch) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind == cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_mg_full_neg_lap: the solver is an AMG solver (use cmg_amg_full_neg_lap)");
+    if (!chan_ok(g, x_ch) || !chan_ok(g, ax_ch) || x_ch == ax_ch) return fail(CMG_ERR_INVALID, "cmg_mg_full_neg_lap: bad channels");
+    s->s.enqueue_geo_full_neg_lap(g->g, g->g.plane(x_ch), g->g.plane(ax_ch), g->g.stream);
+    return cmg::check_cuda(cudaGetLastError(), "mg_full_neg_lap");
+}
+
 int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch) {
     if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_gauss_seidel: not an AMG solver (use cmg_mg_gauss_seidel)");
     if (level < 0 || level > g->g.max_level() || !chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || (order != 0 && order != 1))
         return fail(CMG_ERR_INVALID, "cmg_amg_gauss_seidel: bad argument");
     s->s.enqueue_gs(g->g, level, iters, order, g->g.plane(x_ch), g->g.plane(rhs_ch), g->g.stream);
@@ -392,6 +449,7 @@ int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, i
 }
 int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) {
     if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_fas_mu_cycle: not an AMG solver (use cmg_mg_vcycle)");
     if (!chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || !chan_ok(g, x0_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_fas_mu_cycle: channel out of range");
     if (int rc = cmg::validate_solver_topology(g->g)) return rc;
     const cmg::MuArgs A = s->s.mu_args(g->g, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters);

@@ -322,6 +322,54 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) c
     enqueue_gs(G, l, A.level_iters, 1, A.X, A.RHS, st, true);
 }
 
+// GaussSeidelGMG / GaussSeidelCMG (src/GMGSolver.cu:217-223, src/CMGSolver.cu:271-276)
+void Solver::enqueue_geo_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    const int t0 = G.level_begin(level), nt = G.ghost_begin(level) - t0;
+    for (int it = 0; it < iters; ++it) {
+        launch_geo_gs(kind, d, t0, nt, X, RHS, order, st);
+        launch_geo_gs(kind, d, t0, nt, X, RHS, 1 - order, st);
+    }
+}
+
+// GMGSolver::VCycle (src/GMGSolver.cu:324-388), CMGSolver::VCycle (src/CMGSolver.cu:377-416).
+// GMG restricts from and prolongs into the GHOST tiles of a level as well; CMG does not.
+void Solver::enqueue_geo_vcycle(Grid& G, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    launch_geo_vinit(d, X, RHS, F, st);
+    const int top = G.max_level();
+    for (int i = top; i > 0; --i) {
+        enqueue_geo_gs(G, i, level_iters, 0, X, RHS, st);
+        const int t0 = G.level_begin(i), t1 = kind == kGMG ? G.level_end(i) : G.ghost_begin(i);
+        launch_geo_restrict(kind, d, t0, t1 - t0, X, RHS, R_restrict, st);
+    }
+    enqueue_geo_gs(G, 0, coarsest_iters / 2, 0, X, RHS, st);
+    enqueue_geo_gs(G, 0, coarsest_iters / 2, 1, X, RHS, st);
+    for (int i = 1; i <= top; ++i) {
+        const int t0 = G.level_begin(i), t1 = kind == kGMG ? G.level_end(i) : G.ghost_begin(i);
+        launch_geo_prolong(d, t0, t1 - t0, X, P, st);
+        enqueue_geo_gs(G, i, level_iters, 1, X, RHS, st);
+    }
+}
+
+// FullNegativeLaplacian (src/GMGSolver.cu:167-171): GHOST x from the parents, the operator
+// on LEAF and GHOST tiles, GHOST results added into their LEAF parents.
+// ConservativeFullNegativeLaplacian (src/CMGSolver.cu:210-222): GHOST x from the parents,
+// NONLEAF x as the mean of the LEAF children, the operator on LEAF tiles.
+void Solver::enqueue_geo_full_neg_lap(Grid& G, float* X, float* AX, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    const int ch = (int)((X - G.chan) / ((size_t)G.n * kCells));
+    launch_propagate_ghost(d, 0, G.n, ch, st);
+    if (kind == kCMG) launch_accumulate_cells(d, 0, G.n, dLeaf, X, X, 0.125f, false, st);
+    launch_geo_lap(kind, d, 0, G.n, X, AX, false, kind == kGMG ? (dLeaf | dGhost) : dLeaf, st);
+    if (kind == kGMG) launch_accumulate_cells(d, 0, G.n, dGhost, AX, AX, 1.0f, true, st);
+}
+
+void Solver::enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const {
+    if (kind == kAMG) enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
+    else enqueue_geo_vcycle(G, G.plane(4), G.plane(1), G.plane(3), k.level_iters, k.coarsest_iters, st);
+}
+
 // AMGSolver::FASMuCycle (src/AMGSolver.cu:1279-1292): zero x everywhere, then the top step
 void Solver::enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const {
     launch_fill(A.X, (size_t)G.n * kCells, 0.0f, st);
@@ -345,11 +393,11 @@ static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
 void Solver::enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_h, bool graph, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
-    enqueue_cluster_pack(G, st);
+    if (kind == kAMG) enqueue_cluster_pack(G, st);
     launch_leaf_fill(d, G.leaf, G.nleaf, G.plane(0), 0.0f, st);
     if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(1), kDotRR0, nullptr, rs, st);
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
-    enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
+    enqueue_precond(G, k, st);
     launch_leaf_copy(d, G.leaf, G.nleaf, G.plane(2), G.plane(4), st);
     launch_dot(d, G.leaf, G.nleaf, G.plane(4), G.plane(1), kDotGammaInit, nullptr, rs, st);
     launch_loop_gate(rs, loop_h, graph, st);
@@ -358,7 +406,12 @@ void Solver::enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_
 void Solver::enqueue_body(Grid& G, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool graph, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
-    launch_leaf_apply(d, G.leaf, G.nleaf, G.plane(2), G.plane(3), coeff_ch, true, rs, st);
+    if (kind == kAMG) {
+        launch_leaf_apply(d, G.leaf, G.nleaf, G.plane(2), G.plane(3), coeff_ch, true, rs, st);
+    } else {
+        enqueue_geo_full_neg_lap(G, G.plane(2), G.plane(3), st);
+        launch_dot(d, G.leaf, G.nleaf, G.plane(2), G.plane(3), kDotAlpha, nullptr, rs, st);
+    }
     launch_xr_update(d, G.leaf, G.nleaf, G.plane(0), G.plane(1), G.plane(2), G.plane(3), rs, loop_h, body_h, graph, st);
 }
 // [recenter]; z = M r; gamma_old, gamma, beta; p = z + beta p (src/AMGSolver.cu:1500-1536)
@@ -366,7 +419,7 @@ void Solver::enqueue_tail(Grid& G, const Key& k, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
-    enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
+    enqueue_precond(G, k, st);
     launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(4), kDotBeta, nullptr, rs, st);
     launch_p_update(d, G.leaf, G.nleaf, G.plane(2), G.plane(4), rs, st);
 }
@@ -431,8 +484,9 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
         set_error("solve: grid has no LEAF tiles (rebuild first)");
         return 3;
     }
-    if (G.nch < 5 || coeff_ch < 5 || coeff_ch + 4 > G.nch) {
-        set_error("solve: needs channels 0..4 and coefficient channels coeff..coeff+3 (coeff >= 5)");
+    if (G.nch < 5 || (kind == kAMG && (coeff_ch < 5 || coeff_ch + 4 > G.nch))) {
+        set_error(kind == kAMG ? "solve: needs channels 0..4 and coefficient channels coeff..coeff+3 (coeff >= 5)"
+                               : "solve: needs channels 0..4");
         return 1;
     }
     if (max_iters < 0 || level_iters < 0 || coarsest_iters < 0 || mu < 0) {

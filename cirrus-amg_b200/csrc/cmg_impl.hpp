@@ -109,6 +109,14 @@ struct Solver {
     long long last_launches = 0;
 
     Solver(int c, float rm, float rr, float p) : coeff_ch(c), R_matrix(rm), R_restrict(rr), P(p) {}
+    // GMGSolver(one_over_alpha, prolong_coeff) / CMGSolver(...) (src/GMGSolver.h:21, src/CMGSolver.h:21)
+    Solver(int kind_, float one_over_alpha, float prolong) : coeff_ch(0), R_matrix(1), R_restrict(one_over_alpha), P(prolong), kind(kind_) {}
+    int kind = kAMG;
+    void enqueue_geo_full_neg_lap(Grid& G, float* X, float* AX, cudaStream_t st) const;
+    void enqueue_geo_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
+    void enqueue_geo_vcycle(Grid& G, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, cudaStream_t st) const;
+    // z = M r with the solver's preconditioner (AMG: FAS mu-cycle; GMG/CMG: V-cycle), channel 3 as scratch
+    void enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const;
     ~Solver();
     int init();
     int ensure_scratch(int nleaf);

@@ -596,7 +596,10 @@ __global__ void __launch_bounds__(128) k_dot(const int* leaf, const float* A, co
             if (mode == kDotStore) *out = d;
             else if (mode == kDotRR0) s->rr0 = d;
             else if (mode == kDotGammaInit) s->gamma = d;
-            else {  // src/AMGSolver.cu:1513-1520
+            else if (mode == kDotAlpha) {  // p.Ap and alpha = gamma / p.Ap (src/GMGSolver.cu:518-521)
+                s->pAp = d;
+                s->alpha = s->gamma / d;
+            } else {  // src/AMGSolver.cu:1513-1520
                 s->gamma_old = s->gamma;
                 s->gamma = d;
                 s->beta = d / s->gamma_old;

@@ -23,6 +23,19 @@ struct ReduceScratch {
     PcgScalars* s;
 };
 
+// --- geometric multigrid (geo_mg.cu): GMGSolver / CMGSolver ---
+enum SolverKind : int { kAMG = 0, kGMG = 1, kCMG = 2 };
+// operator on tiles t0..t0+nt whose type (NONLEAF counted as LEAF when sl_is_level) is in `types`
+void launch_geo_lap(int kind, const DevGrid& g, int t0, int nt, const float* X, float* AX, bool sl_is_level, int types, cudaStream_t st);
+void launch_geo_gs(int kind, const DevGrid& g, int t0, int nt, float* X, const float* B, int color, cudaStream_t st);
+void launch_geo_restrict(int kind, const DevGrid& g, int t0, int nt, const float* X, float* RHS, float one_over_alpha, cudaStream_t st);
+void launch_geo_prolong(const DevGrid& g, int t0, int nt, float* X, float P, cudaStream_t st);
+void launch_geo_vinit(const DevGrid& g, float* X, float* RHS, const float* F, cudaStream_t st);
+// CalcCellTypesFromLeafs step 1 on the NONLEAF tiles in t0..t0+nt (one level per launch, finest first)
+void launch_types_from_children(const DevGrid& g, int t0, int nt, cudaStream_t st);
+void launch_accumulate_cells(const DevGrid& g, int t0, int nt, int types, const float* SRC, float* DST, float coeff, bool additive,
+                             cudaStream_t st);
+
 // --- multigrid ---
 // persistent, software-pipelined colour pass for the multigrid cycle (gs_pipe.cu); needs the
 // x plane masked to INTERIOR cells.  gs_pipe_init: resident blocks on the device (0: unusable).
@@ -59,7 +72,7 @@ cudaError_t launch_persist_step(const DevGrid& g, int top, const int* lb, const 
 int persist_blocks();  // co-resident blocks of the persistent kernel on the current device
 
 // --- PCG on LEAF tiles (tile list) ---
-enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3 };
+enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3, kDotAlpha = 4 };
 void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
                        ReduceScratch rs, cudaStream_t st);
 void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,

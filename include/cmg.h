@@ -107,6 +107,11 @@ int cmg_grid_fill_channel(cmg_grid* g, int ch, float value);
  * cells, src/PoissonGrid.cu:87, without the cell-type mask) */
 int cmg_grid_copy_channel(cmg_grid* g, int src_ch, int dst_ch);
 /* CreateTestGrid cell types of LEAF tiles (tests/TestGrids.cuh:161-167) */
+/* CalcCellTypesFromLeafs (src/PoissonGrid.cu:923-977): NONLEAF cell types from their
+ * LEAF/NONLEAF children, finest level first (DIRICHLET before INTERIOR before
+ * NEUMANN), then GHOST cell types from their parents.  Needed before a GMG or CMG
+ * solve; AMG sets its own types in cmg_amg_prepare_types_and_coeffs. */
+int cmg_grid_calc_cell_types_from_leafs(cmg_grid* g);
 int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams);
 /* stream used by every later call on this grid (NULL = legacy default) */
 int cmg_grid_set_stream(cmg_grid* g, void* cuda_stream);
@@ -167,6 +172,25 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
 #define CMG_LAUNCH_NO_CLUSTER 4
 #define CMG_LAUNCH_NO_PIPELINE 8
 int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
+
+/* ---- geometric multigrid preconditioners ---------------------------------
+ * GMGSolver(one_over_alpha, prolong_coeff) (src/GMGSolver.h:21) and
+ * CMGSolver(one_over_alpha, prolong_coeff) (src/CMGSolver.h:21): the same
+ * solver handle type, solved with cmg_amg_solve (GMGSolver::solve,
+ * src/GMGSolver.cu:472-607; CMGSolver::solve, src/CMGSolver.cu:466-601: PCG
+ * preconditioned by one V-cycle, channels as for AMG).  They use no coefficient
+ * channels: the operator comes from tile and cell types.  The reference's tests
+ * construct both with (1, 1) (tests/SolverTests.cu:1055,1077). */
+int cmg_gmg_solver_create(float one_over_alpha, float prolong_coeff, cmg_amg_solver** out);
+int cmg_cmg_solver_create(float one_over_alpha, float prolong_coeff, cmg_amg_solver** out);
+/* GMGSolver::VCycle / CMGSolver::VCycle (src/GMGSolver.cu:324, src/CMGSolver.cu:377):
+ * x_ch <- V-cycle applied to f_ch, rhs_ch used as the cycle's right-hand-side scratch */
+int cmg_mg_vcycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters);
+/* GaussSeidelGMG / GaussSeidelCMG (src/GMGSolver.cu:217, src/CMGSolver.cu:271) */
+int cmg_mg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
+/* FullNegativeLaplacian / ConservativeFullNegativeLaplacian (src/GMGSolver.cu:167,
+ * src/CMGSolver.cu:210); writes GHOST (and, for CMG, NONLEAF) values of x_ch */
+int cmg_mg_full_neg_lap(cmg_amg_solver* s, cmg_grid* g, int x_ch, int ax_ch);
 /* AMGSolver::solve (src/AMGSolver.cu:1399): solves -lap x = b, b read from
  * channel 1 and overwritten by the residual, x written to channel 0.
  * iters/rel_res are the reference's (num_iters, relative_residual), with

@@ -740,7 +740,7 @@ static int is_active_at(const og_grid* g, int t, int level) { /* subtreeType(lev
 
 /* PropagateToChildren + AccumulateToParentsOneStep + NegativeLaplacianSameLevelAMG128
  * on LEAF tiles (AMGFullNegativeLaplacianOnLeafs, AMGSolver.cu:589-632). */
-static void propagate_and_accumulate(og_grid* g, int x_ch) {
+static void propagate_ghosts(og_grid* g, int x_ch) {
     /* ghost <- parent value (PoissonGrid.cu:377-405), coarse levels first */
     for (int L = 1; L <= g->max_level; L++)
         for (int t = 0; t < g->n; t++) {
@@ -756,7 +756,9 @@ static void propagate_and_accumulate(og_grid* g, int x_ch) {
                 CH(g, x_ch, t)[v] = val;
             }
         }
-    /* NONLEAF parent <- 1/8 sum of LEAF children, one step (PoissonGrid.cu:408-465) */
+}
+/* NONLEAF parent <- 1/8 sum of LEAF children, one step (PoissonGrid.cu:408-465) */
+static void accumulate_leafs_to_parents(og_grid* g, int x_ch) {
     for (int t = 0; t < g->n; t++) {
         if (!(g->t[t].type & OG_LEAF)) continue;
         int p = g->parent[t];
@@ -773,6 +775,10 @@ static void propagate_and_accumulate(og_grid* g, int x_ch) {
             CH(g, x_ch, p)[parent_cell(g, t, CELL(fl[0], fl[1], fl[2]))] = sum * 0.125f;
         }
     }
+}
+static void propagate_and_accumulate(og_grid* g, int x_ch) {
+    propagate_ghosts(g, x_ch);
+    accumulate_leafs_to_parents(g, x_ch);
 }
 void og_full_neg_lap_leafs(og_grid* g, int x_ch, int coeff_ch, int ax_ch) {
     propagate_and_accumulate(g, x_ch);
@@ -977,9 +983,14 @@ static void recenter(og_grid* g, int ch) {
     }
 }
 
-/* AMGSolver::solve (AMGSolver.cu:1399-1549).  Channels: x 0, b/r 1, p 2, Ap 3
- * (also the FAS x0), z 4 (PoissonTile.h:13-18).  Returns the iteration count. */
-int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float Rr, float P, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, double* rel_res) {
+/* The PCG of AMGSolver::solve (AMGSolver.cu:1399-1549), GMGSolver::solve and
+ * CMGSolver::solve, with the operator and the preconditioner passed in.
+ * Channels: x 0, b/r 1, p 2, Ap 3 (also the preconditioner's scratch), z 4
+ * (PoissonTile.h:13-18).  Returns the iteration count. */
+typedef void (*apply_fn)(og_grid* g, const void* ctx, int p_ch, int ap_ch);
+typedef void (*precond_fn)(og_grid* g, const void* ctx, int z_ch, int r_ch, int tmp_ch);
+static int pcg(og_grid* g, apply_fn apply, precond_fn precond, const void* ctx, int max_iters, double tol, int sync_stride, int pure_neumann,
+               double* rel_res) {
     const int X = 0, R = 1, PP = 2, AP = 3, Z = 4;
     double rr0 = 0, thr = 0;
     for (int t = 0; t < g->n; t++) if (g->t[t].type & OG_LEAF) memset(CH(g, X, t), 0, sizeof(float) * NC);
@@ -990,12 +1001,12 @@ int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float Rr, float
         if (thr < DBL_MIN) thr = DBL_MIN;
     }
     if (pure_neumann) recenter(g, R);
-    og_fas_mu_cycle(g, mu, Z, R, AP, coeff_ch, level_iters, coarsest_iters, omega, Rr, P);
+    precond(g, ctx, Z, R, AP);
     for (int t = 0; t < g->n; t++) if (g->t[t].type & OG_LEAF) memcpy(CH(g, PP, t), CH(g, Z, t), sizeof(float) * NC);
     double gamma = og_dot(g, Z, R);
     int i;
     for (i = 0; i < max_iters; i++) {
-        og_full_neg_lap_leafs(g, PP, coeff_ch, AP);
+        apply(g, ctx, PP, AP);
         double fp = og_dot(g, PP, AP);
         double alpha = gamma / fp;
         float af = (float)alpha;
@@ -1012,7 +1023,7 @@ int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float Rr, float
             if (rr < thr) { if (rel_res) *rel_res = sqrt(rr / rr0); return i + 1; }
         }
         if (pure_neumann) recenter(g, R);
-        og_fas_mu_cycle(g, mu, Z, R, AP, coeff_ch, level_iters, coarsest_iters, omega, Rr, P);
+        precond(g, ctx, Z, R, AP);
         double gamma_old = gamma;
         gamma = og_dot(g, R, Z);
         double beta = gamma / gamma_old;
@@ -1028,6 +1039,23 @@ int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float Rr, float
         if (rel_res) *rel_res = sqrt(rr / rr0);
     } else if (rel_res) *rel_res = -1;
     return i;
+}
+
+typedef struct {
+    int coeff_ch, mu, level_iters, coarsest_iters;
+    double omega;
+    float Rr, P;
+} amg_ctx;
+static void amg_apply(og_grid* g, const void* ctx, int p_ch, int ap_ch) {
+    og_full_neg_lap_leafs(g, p_ch, ((const amg_ctx*)ctx)->coeff_ch, ap_ch);
+}
+static void amg_precond(og_grid* g, const void* ctx, int z_ch, int r_ch, int tmp_ch) {
+    const amg_ctx* c = (const amg_ctx*)ctx;
+    og_fas_mu_cycle(g, c->mu, z_ch, r_ch, tmp_ch, c->coeff_ch, c->level_iters, c->coarsest_iters, c->omega, c->Rr, c->P);
+}
+int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float Rr, float P, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, double* rel_res) {
+    amg_ctx c = {coeff_ch, mu, level_iters, coarsest_iters, omega, Rr, P};
+    return pcg(g, amg_apply, amg_precond, &c, max_iters, tol, sync_stride, pure_neumann, rel_res);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1332,4 +1360,300 @@ done:
     if (iters_out) *iters_out = it;
     free(dinv); free(r); free(z); free(p); free(q); free(s); free(tv); free(rh);
     return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* geometric multigrid preconditioners: GMGSolver (src/GMGSolver.cu)    */
+/* and CMGSolver (src/CMGSolver.cu), kind OG_GMG / OG_CMG               */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    float x[1000];
+    uint8_t ct[1000];
+    int tt_own;     /* subtree type of the tile */
+    int tt_face[6]; /* subtree type seen across each face (GMG: the tile's own type when empty) */
+} og_gsnap;
+
+/* HATileInfo::subtreeType (HATileInfo.h:79-84) */
+static int subtree_type(const og_grid* g, int t, int sl) {
+    int ty = g->t[t].type;
+    return (g->t[t].level == sl && ty == OG_NONLEAF) ? OG_LEAF : ty;
+}
+
+/* LoadGMGLaplacianTileData (GMGSolver.cu:81-134) and LoadCMGLaplacianTileData
+ * (CMGSolver.cu:59-170): raw x and cell types of the tile and its face halo;
+ * an empty neighbour reads x = 0, DIRICHLET; CMG extrapolates across a GHOST
+ * neighbour as the AMG loader does. */
+static void load_gsnap(const og_grid* g, int kind, int t, int sl, int x_ch, og_gsnap* S) {
+    const float* X = CH(g, x_ch, t);
+    const uint8_t* ty = CT(g, t);
+    S->tt_own = subtree_type(g, t, sl);
+    for (int v = 0; v < NC; v++) {
+        int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+        S->x[SX(i, j, k)] = X[v];
+        S->ct[SX(i, j, k)] = ty[v];
+    }
+    for (int axis = 0; axis < 3; axis++) {
+        for (int s = 0; s < 2; s++) {
+            int sgn = s ? 1 : -1;
+            int q = g->nbr[t * 6 + axis + (s ? 3 : 0)];
+            S->tt_face[axis + 3 * s] = q < 0 ? S->tt_own : subtree_type(g, q, sl);
+            for (int fi = 0; fi < 64; fi++) {
+                int a = fi >> 3, b = fi & 7;
+                int fl[3], cl[3], nl[3];
+                int axk = s ? 8 : -1;
+                if (axis == 0) { fl[0] = axk; fl[1] = a; fl[2] = b; }
+                else if (axis == 1) { fl[0] = a; fl[1] = axk; fl[2] = b; }
+                else { fl[0] = a; fl[1] = b; fl[2] = axk; }
+                for (int d = 0; d < 3; d++) { cl[d] = fl[d]; nl[d] = fl[d]; }
+                cl[axis] -= sgn;
+                nl[axis] = s ? 0 : 7;
+                int fx = SX(fl[0], fl[1], fl[2]);
+                int nv = CELL(nl[0], nl[1], nl[2]);
+                if (q < 0) {
+                    S->x[fx] = 0.0f;
+                    S->ct[fx] = OG_DIRICHLET;
+                } else if (kind == OG_CMG && subtree_type(g, q, sl) == OG_GHOST) {
+                    float avg = 0;
+                    for (int di = 0; di < 2; di++)
+                        for (int dj = 0; dj < 2; dj++)
+                            for (int dk = 0; dk < 2; dk++) avg += S->x[SX(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)];
+                    avg /= 8;
+                    float V1 = CH(g, x_ch, q)[nv];
+                    S->x[fx] = (float)((double)S->x[SX(cl[0], cl[1], cl[2])] + 0.5 * (double)(V1 - avg));
+                    S->ct[fx] = CT(g, q)[nv];
+                } else {
+                    S->x[fx] = CH(g, x_ch, q)[nv];
+                    S->ct[fx] = CT(g, q)[nv];
+                }
+            }
+        }
+    }
+}
+
+/* NegativeLaplacianCoeff: GMG from the tile types of both sides (GMGSolver.cu:3-31),
+ * CMG h unless a side is NEUMANN (CMGSolver.cu:3-7) */
+static float geo_coeff(int kind, float h, int tt0, int tt1, int c0, int c1) {
+    if ((c0 | c1) & OG_NEUMANN) return 0.0f;
+    if (kind == OG_CMG) return h;
+    float ooh = 1.0f / h;
+    int both = (tt0 & OG_LEAF) && (tt1 & OG_LEAF);
+    int lg = ((tt0 & OG_LEAF) && (tt1 & OG_GHOST)) || ((tt0 & OG_GHOST) && (tt1 & OG_LEAF));
+    float oodh = both ? ooh : (lg ? (2.0f * ooh) / 3.0f : 0.0f);
+    return oodh * ooh;
+}
+/* GMGLaplacianTileData::negativeLap (GMGSolver.cu:46-66), CMG's (CMGSolver.cu:22-45):
+ * sum over -x,+x,-y,+y,-z,+z of coeff * (x0 - x1) (or of coeff for the diagonal);
+ * GMG scales by h^3; 0 on cells that are not INTERIOR */
+static float gsnap_neg_lap(int kind, const og_gsnap* S, float h, int v, int diag) {
+    int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+    int c = SX(l[0], l[1], l[2]);
+    int ct0 = S->ct[c];
+    float x0 = S->x[c];
+    float sum = 0;
+    for (int axis = 0; axis < 3; axis++)
+        for (int s = 0; s < 2; s++) {
+            int sgn = s ? 1 : -1;
+            int n[3] = {l[0], l[1], l[2]};
+            n[axis] += sgn;
+            int inside = n[axis] >= 0 && n[axis] < 8;
+            int nc = SX(n[0], n[1], n[2]);
+            int tt1 = inside ? S->tt_own : S->tt_face[axis + 3 * s];
+            float coeff = geo_coeff(kind, h, S->tt_own, tt1, ct0, S->ct[nc]);
+            sum = diag ? sum + coeff : fmaf(coeff, x0 - S->x[nc], sum);
+        }
+    if (!(ct0 & OG_INTERIOR)) return 0.0f;
+    return kind == OG_CMG ? sum : sum * h * h * h;
+}
+
+static int geo_level_member(const og_grid* g, int kind, int t, int level, int with_ghosts) {
+    if (g->t[t].level != level) return 0;
+    int ty = g->t[t].type;
+    return (ty & (OG_LEAF | OG_NONLEAF)) || (with_ghosts && kind == OG_GMG && (ty & OG_GHOST));
+}
+
+/* GaussSeidelGMG / GaussSeidelCMG (GMGSolver.cu:217-223, CMGSolver.cu:271-276) and their
+ * kernels (GMGSolver.cu:173-210, CMGSolver.cu:226-262): x += (b - Ax) / D on INTERIOR cells
+ * of one colour, no relaxation factor */
+static void geo_gs_pass(og_grid* g, int kind, int level, int color, int x_ch, int rhs_ch) {
+    float h = voxel_size(g, level);
+#pragma omp parallel
+    {
+        og_gsnap* S = (og_gsnap*)malloc(sizeof(og_gsnap));
+#pragma omp for schedule(dynamic, 16)
+        for (int t = 0; t < g->n; t++) {
+            if (!geo_level_member(g, kind, t, level, 0)) continue;
+            load_gsnap(g, kind, t, level, x_ch, S);
+            float* X = CH(g, x_ch, t);
+            const float* B = CH(g, rhs_ch, t);
+            for (int v = 0; v < NC; v++) {
+                int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+                if (((i + j + k) & 1) != color) continue;
+                int ct = CT(g, t)[v];
+                float Ax = gsnap_neg_lap(kind, S, h, v, 0);
+                float D = gsnap_neg_lap(kind, S, h, v, 1);
+                float delta = (ct & OG_INTERIOR) ? (B[v] - Ax) / D : 0.0f;
+                X[v] = S->x[SX(i, j, k)] + delta;
+            }
+        }
+        free(S);
+    }
+}
+static void geo_gs(og_grid* g, int kind, int iters, int order, int level, int x_ch, int rhs_ch) {
+    for (int it = 0; it < iters; it++) {
+        geo_gs_pass(g, kind, level, order, x_ch, rhs_ch);
+        geo_gs_pass(g, kind, level, 1 - order, x_ch, rhs_ch);
+    }
+}
+void og_geo_gauss_seidel(og_grid* g, int kind, int iters, int order, int level, int x_ch, int rhs_ch) {
+    geo_gs(g, kind, iters, order, level, x_ch, rhs_ch);
+}
+
+/* ResidualAndRestrict128Kernel (GMGSolver.cu:225-284), ConservativeResidualAndRestrict128Kernel
+ * (CMGSolver.cu:278-331): coarse rhs = one_over_alpha * sum of 8 residuals; a GMG GHOST tile
+ * adds its sum to its LEAF parent's rhs instead */
+static void geo_restrict(og_grid* g, int kind, int level, int x_ch, int rhs_ch, float ooa) {
+    float h = voxel_size(g, level);
+    og_gsnap* S = (og_gsnap*)malloc(sizeof(og_gsnap));
+    float res[NC];
+    for (int t = 0; t < g->n; t++) {
+        if (!geo_level_member(g, kind, t, level, 1)) continue;
+        int p = g->parent[t];
+        if (p < 0) continue;
+        load_gsnap(g, kind, t, level, x_ch, S);
+        for (int v = 0; v < NC; v++) res[v] = CH(g, rhs_ch, t)[v] - gsnap_neg_lap(kind, S, h, v, 0);
+        int ghost = g->t[t].type & OG_GHOST;
+        for (int b = 0; b < 64; b++) {
+            int fl[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
+            float sum = 0;
+            for (int ii = 0; ii < 2; ii++)
+                for (int jj = 0; jj < 2; jj++)
+                    for (int kk = 0; kk < 2; kk++) sum += res[CELL(fl[0] + ii, fl[1] + jj, fl[2] + kk)];
+            float* c = &CH(g, rhs_ch, p)[parent_cell(g, t, CELL(fl[0], fl[1], fl[2]))];
+            if (ghost) *c = *c + sum;
+            else *c = sum * ooa;
+        }
+    }
+    free(S);
+}
+/* ProlongateAndUpdate128Kernel (GMGSolver.cu:286-316), CMG's (CMGSolver.cu:339-370):
+ * x += P * coarse x on INTERIOR cells, GHOST cells take the coarse x, others 0 */
+static void geo_prolong(og_grid* g, int kind, int level, int x_ch, float P) {
+    for (int t = 0; t < g->n; t++) {
+        if (!geo_level_member(g, kind, t, level, 1)) continue;
+        int p = g->parent[t];
+        int ghost = g->t[t].type & OG_GHOST;
+        float* X = CH(g, x_ch, t);
+        for (int v = 0; v < NC; v++) {
+            float cx = p >= 0 ? CH(g, x_ch, p)[parent_cell(g, t, v)] : 0.0f;
+            int in = CT(g, t)[v] & OG_INTERIOR;
+            X[v] = ghost ? (in ? cx : 0.0f) : (in ? fmaf(P, cx, X[v]) : 0.0f);
+        }
+    }
+}
+/* GMGSolver::VCycle (GMGSolver.cu:324-388), CMGSolver::VCycle (CMGSolver.cu:377-416) */
+void og_geo_vcycle(og_grid* g, int kind, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters, float ooa, float P) {
+    for (int t = 0; t < g->n; t++) {
+        memset(CH(g, x_ch, t), 0, sizeof(float) * NC);
+        if (g->t[t].type & OG_GHOST) memset(CH(g, rhs_ch, t), 0, sizeof(float) * NC);
+        else memcpy(CH(g, rhs_ch, t), CH(g, f_ch, t), sizeof(float) * NC);
+    }
+    for (int i = g->max_level; i > 0; i--) {
+        geo_gs(g, kind, level_iters, 0, i, x_ch, rhs_ch);
+        geo_restrict(g, kind, i, x_ch, rhs_ch, ooa);
+    }
+    geo_gs(g, kind, coarsest_iters / 2, 0, 0, x_ch, rhs_ch);
+    geo_gs(g, kind, coarsest_iters / 2, 1, 0, x_ch, rhs_ch);
+    for (int i = 1; i <= g->max_level; i++) {
+        geo_prolong(g, kind, i, x_ch, P);
+        geo_gs(g, kind, level_iters, 1, i, x_ch, rhs_ch);
+    }
+}
+
+/* FullNegativeLaplacian (GMGSolver.cu:167-171): GHOST x from the parents, the operator on
+ * LEAF and GHOST tiles, GHOST results added into their LEAF parents.
+ * ConservativeFullNegativeLaplacian (CMGSolver.cu:210-222): GHOST x from the parents,
+ * NONLEAF x as the mean of LEAF children, the operator on LEAF tiles. */
+void og_geo_full_neg_lap(og_grid* g, int kind, int x_ch, int ax_ch) {
+    propagate_ghosts(g, x_ch);
+    if (kind == OG_CMG) accumulate_leafs_to_parents(g, x_ch);
+#pragma omp parallel
+    {
+        og_gsnap* S = (og_gsnap*)malloc(sizeof(og_gsnap));
+#pragma omp for schedule(dynamic, 16)
+        for (int t = 0; t < g->n; t++) {
+            int ty = g->t[t].type;
+            if (!((ty & OG_LEAF) || (kind == OG_GMG && (ty & OG_GHOST)))) continue;
+            float h = voxel_size(g, g->t[t].level);
+            load_gsnap(g, kind, t, -1, x_ch, S);
+            for (int v = 0; v < NC; v++) CH(g, ax_ch, t)[v] = gsnap_neg_lap(kind, S, h, v, 0);
+        }
+        free(S);
+    }
+    if (kind == OG_GMG) {
+        for (int t = 0; t < g->n; t++) {
+            if (!(g->t[t].type & OG_GHOST)) continue;
+            int p = g->parent[t];
+            if (p < 0) continue;
+            for (int b = 0; b < 64; b++) {
+                int fl[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
+                float sum = 0;
+                for (int ii = 0; ii < 2; ii++)
+                    for (int jj = 0; jj < 2; jj++)
+                        for (int kk = 0; kk < 2; kk++) {
+                            int v = CELL(fl[0] + ii, fl[1] + jj, fl[2] + kk);
+                            sum += (CT(g, t)[v] & (OG_INTERIOR | OG_DIRICHLET | OG_NEUMANN)) ? CH(g, ax_ch, t)[v] : 0.0f;
+                        }
+                float* c = &CH(g, ax_ch, p)[parent_cell(g, t, CELL(fl[0], fl[1], fl[2]))];
+                *c = fmaf(sum, 1.0f, *c);
+            }
+        }
+    }
+}
+
+static void geo_apply(og_grid* g, const void* ctx, int p_ch, int ap_ch) {
+    const int* c = (const int*)ctx;
+    og_geo_full_neg_lap(g, c[0], p_ch, ap_ch);
+}
+static void geo_precond(og_grid* g, const void* ctx, int z_ch, int r_ch, int tmp_ch) {
+    const int* c = (const int*)ctx;
+    const float* f = (const float*)(c + 3);
+    og_geo_vcycle(g, c[0], z_ch, r_ch, tmp_ch, c[1], c[2], f[0], f[1]);
+}
+/* GMGSolver::solve (GMGSolver.cu:472-607), CMGSolver::solve (CMGSolver.cu:466-601) */
+int og_geo_solve(og_grid* g, int kind, float ooa, float P, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, double* rel_res) {
+    int ctx[5] = {kind, level_iters, coarsest_iters, 0, 0};
+    memcpy(&ctx[3], &ooa, sizeof(float));
+    memcpy(&ctx[4], &P, sizeof(float));
+    return pcg(g, geo_apply, geo_precond, ctx, max_iters, tol, sync_stride, pure_neumann, rel_res);
+}
+
+/* CalcCellTypesFromLeafs (PoissonGrid.cu:923-977): NONLEAF cells from their active
+ * children, finest level first (DIRICHLET before INTERIOR before NEUMANN), then GHOST
+ * cells from their parents */
+void og_calc_cell_types_from_leafs(og_grid* g) {
+    for (int L = g->max_level - 1; L >= 0; L--)
+        for (int t = 0; t < g->n; t++) {
+            if (g->t[t].level != L || g->t[t].type != OG_NONLEAF) continue;
+            for (int v = 0; v < NC; v++) {
+                int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+                int c = g->child[t * 8 + ((i >> 2) << 2) + ((j >> 2) << 1) + (k >> 2)];
+                int nd = 0, ni = 0;
+                if (c >= 0 && (g->t[c].type & (OG_LEAF | OG_NONLEAF))) {
+                    int b0 = (i & 3) << 1, b1 = (j & 3) << 1, b2 = (k & 3) << 1;
+                    for (int ii = 0; ii < 2; ii++)
+                        for (int jj = 0; jj < 2; jj++)
+                            for (int kk = 0; kk < 2; kk++) {
+                                int ty = CT(g, c)[CELL(b0 + ii, b1 + jj, b2 + kk)];
+                                if (ty & OG_DIRICHLET) nd++;
+                                else if (ty & OG_INTERIOR) ni++;
+                            }
+                }
+                CT(g, t)[v] = nd > 0 ? OG_DIRICHLET : ni > 0 ? OG_INTERIOR : OG_NEUMANN;
+            }
+        }
+    for (int t = 0; t < g->n; t++) {
+        if (g->t[t].type != OG_GHOST) continue;
+        int p = g->parent[t];
+        for (int v = 0; v < NC; v++) CT(g, t)[v] = p >= 0 ? CT(g, p)[parent_cell(g, t, v)] : OG_DIRICHLET;
+    }
 }

@@ -79,6 +79,15 @@ void og_face_velocity_fourier(og_grid* g, int u_ch, int nmodes, const double* k,
 void og_divergence(og_grid* g, int u_ch, int coeff_ch, int out_ch);
 void og_add_gradient_to_face(og_grid* g, int x_ch, int coeff_ch, int u_ch);
 
+/* geometric multigrid preconditioners (GMGSolver.cu, CMGSolver.cu) */
+#define OG_GMG 1
+#define OG_CMG 2
+void og_calc_cell_types_from_leafs(og_grid* g);
+void og_geo_full_neg_lap(og_grid* g, int kind, int x_ch, int ax_ch);
+void og_geo_gauss_seidel(og_grid* g, int kind, int iters, int order, int level, int x_ch, int rhs_ch);
+void og_geo_vcycle(og_grid* g, int kind, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters, float one_over_alpha, float P);
+int og_geo_solve(og_grid* g, int kind, float one_over_alpha, float P, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, double* rel_res);
+
 /* FP64 CSR assembly of the leaf operator (unknowns = INTERIOR cells of LEAF tiles) */
 int og_assemble_count(og_grid* g, int coeff_ch, int* n_rows, long long* nnz);
 int og_assemble(og_grid* g, int coeff_ch, long long* rowptr, int* col, double* val, int* row_tile, int* row_cell);

@@ -17,6 +17,7 @@ LEAF, NONLEAF, GHOST = 1, 2, 4
 DIRICHLET, INTERIOR, NEUMANN = 1, 2, 4
 CASE_UNIFORM, CASE_CENTER_POINT, CASE_SPHERE_EMPTY, CASE_SPHERE_SOLID = 0, 1, 2, 3
 CASE_STAR_EMPTY, CASE_STAR_SOLID, CASE_SHELL, CASE_MULTI_SPHERE = 4, 5, 6, 7
+GMG, CMG = 1, 2
 
 _lib = None
 
@@ -61,6 +62,11 @@ def lib():
             "og_face_velocity_fourier": (None, [P, I, I, P, P, P]),
             "og_divergence": (None, [P, I, I, I]),
             "og_add_gradient_to_face": (None, [P, I, I, I]),
+            "og_calc_cell_types_from_leafs": (None, [P]),
+            "og_geo_full_neg_lap": (None, [P, I, I, I]),
+            "og_geo_gauss_seidel": (None, [P, I, I, I, I, I, I]),
+            "og_geo_vcycle": (None, [P, I, I, I, I, I, I, F, F]),
+            "og_geo_solve": (I, [P, I, F, F, I, D, I, I, I, I, P]),
             "og_assemble_count": (I, [P, I, P, P]),
             "og_assemble": (I, [P, I, P, P, P, P, P]),
             "og_csr_solve": (I, [I, P, P, P, P, P, D, I, I, P, P]),
@@ -170,6 +176,26 @@ class Grid:
         rel = ctypes.c_double(0)
         it = self.L.og_amg_solve(self.g, coeff_ch, omega, mu, R_restrict, P, max_iters, tol, level_iters,
                                  coarsest_iters, sync_stride, int(pure_neumann), ctypes.byref(rel))
+        return it, rel.value
+
+    def calc_cell_types_from_leafs(self):
+        self.L.og_calc_cell_types_from_leafs(self.g)
+
+    def geo_full_neg_lap(self, kind, x_ch, ax_ch):
+        self.L.og_geo_full_neg_lap(self.g, kind, x_ch, ax_ch)
+
+    def geo_gauss_seidel(self, kind, iters, order, level, x_ch, rhs_ch):
+        self.L.og_geo_gauss_seidel(self.g, kind, iters, order, level, x_ch, rhs_ch)
+
+    def geo_vcycle(self, kind, x_ch, f_ch, rhs_ch, level_iters, coarsest_iters, one_over_alpha=1.0, P=1.0):
+        self.L.og_geo_vcycle(self.g, kind, x_ch, f_ch, rhs_ch, level_iters, coarsest_iters, one_over_alpha, P)
+
+    def geo_solve(self, kind, one_over_alpha=1.0, P=1.0, max_iters=100, tol=1e-6, level_iters=2, coarsest_iters=10,
+                  sync_stride=1, pure_neumann=False):
+        """GMGSolver / CMGSolver::solve: PCG preconditioned by one V-cycle."""
+        rel = ctypes.c_double(0)
+        it = self.L.og_geo_solve(self.g, kind, one_over_alpha, P, max_iters, tol, level_iters, coarsest_iters, sync_stride,
+                                 int(pure_neumann), ctypes.byref(rel))
         return it, rel.value
 
     def face_velocity_fourier(self, u_ch, k, amp, phase):

@@ -358,3 +358,63 @@ def test_pipelined_smoother_matches_per_tile_launches(grid):
         res.append((it, rel, G.download(0)))
     assert res[0][:2] == res[1][:2]
     assert np.array_equal(res[0][2], res[1][2])
+
+
+def _geo_pair(case_id, prm, kind, seed=3):
+    from workloads import uniform_rhs
+
+    G = build_product(case_id, prm)
+    g = build_oracle(case_id, prm)
+    G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    G.calc_cell_types_from_leafs()
+    g.calc_cell_types_from_leafs()
+    assert np.array_equal(G.download_cell_types(), g.cell_types())
+    lv, ijk, ty = G.tiles()
+    b = uniform_rhs(ty == cmg.LEAF, seed)
+    G.upload(1, b)
+    g.channel(1)[:] = b
+    solver = (cmg.GMGSolver if kind == O.GMG else cmg.CMGSolver)(1.0, 1.0)
+    return G, g, solver, b
+
+
+GEO_GRIDS = [(cmg.CASE_UNIFORM, [2, 2]), (cmg.CASE_CENTER_POINT, [2, 4]), (cmg.CASE_SHELL, shell_params(coarse=3, mid=4, fine=5))]
+
+
+@pytest.mark.parametrize("kind", [O.GMG, O.CMG])
+@pytest.mark.parametrize("case_id,prm", GEO_GRIDS)
+def test_geometric_operator_smoother_and_vcycle_match_oracle(kind, case_id, prm):
+    G, g, solver, b = _geo_pair(case_id, prm, kind)
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal((G.num_tiles, 512)).astype(np.float32)
+    G.upload(5, x)
+    g.channel(5)[:] = x
+    solver.full_neg_lap(G, 5, 6)
+    g.geo_full_neg_lap(kind, 5, 6)
+    lv, ijk, ty = G.tiles()
+    leaf = ty == cmg.LEAF
+    assert np.array_equal(G.download(6)[leaf], g.channel(6)[leaf])
+    # one smoothing call per level, then a V-cycle
+    for level in range(G.info()[1] + 1):
+        G.upload(7, x)
+        g.channel(7)[:] = x
+        solver.gauss_seidel(G, 1, 0, level, 7, 1)
+        g.geo_gauss_seidel(kind, 1, 0, level, 7, 1)
+        assert np.array_equal(G.download(7), g.channel(7))
+    solver.VCycle(G, 4, 1, 3, 2, 10)
+    g.geo_vcycle(kind, 4, 1, 3, 2, 10)
+    assert np.array_equal(G.download(4), g.channel(4))
+
+
+@pytest.mark.parametrize("kind", [O.GMG, O.CMG])
+@pytest.mark.parametrize("case_id,prm", GEO_GRIDS)
+def test_geometric_solve_matches_oracle(kind, case_id, prm):
+    G, g, solver, b = _geo_pair(case_id, prm, kind)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    ito, relo = g.geo_solve(kind, 1.0, 1.0, max_iters=100, tol=1e-6, level_iters=2, coarsest_iters=10)
+    assert rel <= 1e-6 and relo <= 1e-6
+    assert abs(it - ito) <= 1
+    lv, ijk, ty = G.tiles()
+    m = ty == cmg.LEAF
+    x = G.download(0)[m]
+    assert np.linalg.norm(x - g.channel(0)[m]) <= 1e-5 * np.linalg.norm(g.channel(0)[m])

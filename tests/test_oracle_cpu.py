@@ -243,3 +243,67 @@ def test_kat_projection_divergence_free():
     lv, ijk, ty = g.tiles()
     ratio = projected_divergence(g.channel, lv, ijk, ty, g.cell_types(), b0, 13)
     assert rel < 1e-6 and ratio < 1e-5, (it, rel, ratio)
+
+
+def _geo_grid(case_id, prm, seed=0):
+    from workloads import uniform_rhs
+
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(case_id, prm)
+    g.alloc(16)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.calc_cell_types_from_leafs()
+    lv, ijk, ty = g.tiles()
+    g.channel(1)[:] = uniform_rhs(ty == O.LEAF, seed)
+    return g
+
+
+@pytest.mark.parametrize("kind", [O.GMG, O.CMG])
+@pytest.mark.parametrize("case_id,prm", [(O.CASE_UNIFORM, [2, 2]), (O.CASE_CENTER_POINT, [2, 4])])
+def test_geometric_solvers_converge(kind, case_id, prm):
+    """GMGSolver / CMGSolver::solve (src/GMGSolver.cu:472, src/CMGSolver.cu:466) with the
+    reference test harness's settings (1, 1) (tests/SolverTests.cu:1055,1077)."""
+    g = _geo_grid(case_id, prm)
+    it, rel = g.geo_solve(kind, 1.0, 1.0, max_iters=100, tol=1e-6, level_iters=2, coarsest_iters=10)
+    assert rel < 1e-6 and it < 30, (it, rel)
+
+
+def test_cmg_operator_equals_amg_finest_operator_on_uniform_grid():
+    """On a single-level grid both are h * (6 x - sum of neighbours): equal solutions."""
+    g = _geo_grid(O.CASE_UNIFORM, [2, 2])
+    b = g.channel(1).copy()
+    g.geo_solve(O.CMG, max_iters=100, tol=1e-7)
+    xc = g.channel(0).copy()
+    g.channel(1)[:] = b
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    g.amg_solve(COEFF, max_iters=100, tol=1e-7)
+    lv, ijk, ty = g.tiles()
+    m = ty == O.LEAF
+    assert np.linalg.norm(xc[m] - g.channel(0)[m]) <= 1e-5 * np.linalg.norm(xc[m])
+
+
+@pytest.mark.parametrize("kind", [O.GMG, O.CMG])
+def test_kat_recovery_geometric(kind):
+    """TestNeumannDirichletRecovery (tests/SolverTests.cu:363-512) with the geometric solvers."""
+    from workloads import boundary_rule_types, recovery_fields
+
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(O.CASE_UNIFORM, [2, 2])
+    g.alloc(16)
+    lv, ijk, ty = g.tiles()
+    nbr, par, ch = g.tables()
+    types = g.cell_types()
+    types[ty == O.LEAF] = boundary_rule_types(lv, ijk, ty, nbr)[ty == O.LEAF]
+    g.calc_cell_types_from_leafs()
+    ct = g.cell_types()
+    xt = recovery_fields(lv, ijk, ty, ct)
+    g.channel(5)[:] = xt
+    g.geo_full_neg_lap(kind, 5, 1)
+    it, rel = g.geo_solve(kind, max_iters=1000, tol=1e-6, level_iters=2, coarsest_iters=10)
+    m = (ty[:, None] == O.LEAF) & (ct == O.INTERIOR)
+    err = np.abs(g.channel(0)[m] - xt[m]).max()
+    assert rel < 1e-6 and err < 1e-4, (it, rel, err)
