@@ -43,6 +43,7 @@ EXPORTS = [
     "cmg_amg_dot", "cmg_amg_dot_noalloc",
     "cmg_amg_solver_create", "cmg_amg_solver_destroy", "cmg_amg_solver_set_smoother", "cmg_amg_solver_set_launch_mode",
     "cmg_gmg_solver_create", "cmg_cmg_solver_create", "cmg_mg_vcycle", "cmg_mg_gauss_seidel", "cmg_mg_full_neg_lap",
+    "cmg_amg_fas_mu_cycle_solve", "cmg_gmg_damped_jacobi_solve",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
     "cmg_amg_last_solve_launches",
@@ -109,6 +110,8 @@ def lib():
             "cmg_mg_vcycle": (I, [P, P, I, I, I, I, I]),
             "cmg_mg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
             "cmg_mg_full_neg_lap": (I, [P, P, I, I]),
+            "cmg_amg_fas_mu_cycle_solve": (I, [P, P, I, I, I, D, I, I, P, P]),
+            "cmg_gmg_damped_jacobi_solve": (I, [P, P, I, I, D, F, P, P]),
             "cmg_amg_solve": (I, [P, P, I, I, D, I, I, I, I, P, P]),
             "cmg_amg_solve_host": (I, [P, P, P, P, S, I, D, I, I, I, I, P, P]),
             "cmg_amg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
@@ -348,6 +351,15 @@ class AMGSolver:
         self._sync_params()
         _check(self.L.cmg_amg_fas_mu_cycle(self.h, grid.h, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters), "fas_mu_cycle")
 
+    def FASMuCycleSolve(self, repeat_times, grid, verbose, max_iters, relative_tolerance, level_iters, coarsest_iters):
+        """AMGSolver::FASMuCycleSolve (src/AMGSolver.cu:1311): mu-cycles as a stand-alone iteration."""
+        self._sync_params()
+        it, rel = ctypes.c_int(0), ctypes.c_double(0)
+        _check(self.L.cmg_amg_fas_mu_cycle_solve(self.h, grid.h, repeat_times, int(verbose), max_iters, relative_tolerance,
+                                                 level_iters, coarsest_iters, ctypes.byref(it), ctypes.byref(rel)),
+               "FASMuCycleSolve")
+        return it.value, rel.value
+
     def last_solve_ms(self):
         ms = ctypes.c_float(0)
         _check(self.L.cmg_amg_last_solve_ms(self.h, ctypes.byref(ms)), "last_solve_ms")
@@ -395,6 +407,17 @@ class GMGSolver(_GeometricSolver):
     """GMGSolver(one_over_alpha, prolong_coeff) (src/GMGSolver.h:17-52)."""
 
     _create = "cmg_gmg_solver_create"
+
+
+def _gmg_damped_jacobi(self, grid, verbose, max_iters, relative_tolerance, omega):
+    """GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:390)."""
+    it, rel = ctypes.c_int(0), ctypes.c_double(0)
+    _check(self.L.cmg_gmg_damped_jacobi_solve(self.h, grid.h, int(verbose), max_iters, relative_tolerance, omega,
+                                              ctypes.byref(it), ctypes.byref(rel)), "dampedJacobiSolve")
+    return it.value, rel.value
+
+
+GMGSolver.dampedJacobiSolve = _gmg_damped_jacobi
 
 
 class CMGSolver(_GeometricSolver):

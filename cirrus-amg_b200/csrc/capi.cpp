@@ -439,6 +439,32 @@ int cmg_mg_full_neg_lap(cmg_amg_solver* s, cmg_grid* g, int x_ch, int ax_ch) {
     return cmg::check_cuda(cudaGetLastError(), "mg_full_neg_lap");
 }
 
+int cmg_amg_fas_mu_cycle_solve(cmg_amg_solver* s, cmg_grid* g, int repeat_times, int verbose, int max_iters, double tol, int level_iters,
+                               int coarsest_iters, int* iters, double* rel_res) {
+    GUARD_BEGIN
+    (void)verbose;
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_fas_mu_cycle_solve: not an AMG solver");
+    if (!iters || !rel_res || repeat_times < 0 || max_iters < 0 || level_iters < 0 || coarsest_iters < 0 || g->g.nch < 3 ||
+        s->s.coeff_ch + 4 > g->g.nch)
+        return fail(CMG_ERR_INVALID, "cmg_amg_fas_mu_cycle_solve: bad argument");
+    if (g->g.nleaf == 0) return fail(CMG_ERR_STATE, "cmg_amg_fas_mu_cycle_solve: no LEAF tiles");
+    if (int rc = s->s.fas_mu_cycle_solve(g->g, repeat_times, max_iters, tol, level_iters, coarsest_iters, iters, rel_res)) return rc;
+    return cmg::check_cuda(cudaGetLastError(), "fas_mu_cycle_solve");
+    GUARD_END
+}
+int cmg_gmg_damped_jacobi_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, float omega, int* iters, double* rel_res) {
+    GUARD_BEGIN
+    (void)verbose;
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind != cmg::kGMG) return fail(CMG_ERR_STATE, "cmg_gmg_damped_jacobi_solve: not a GMG solver");
+    if (!iters || !rel_res || max_iters < 0 || g->g.nch < 4) return fail(CMG_ERR_INVALID, "cmg_gmg_damped_jacobi_solve: bad argument");
+    if (g->g.nleaf == 0) return fail(CMG_ERR_STATE, "cmg_gmg_damped_jacobi_solve: no LEAF tiles");
+    if (int rc = s->s.damped_jacobi_solve(g->g, max_iters, tol, omega, iters, rel_res)) return rc;
+    return cmg::check_cuda(cudaGetLastError(), "damped_jacobi_solve");
+    GUARD_END
+}
+
 int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch) {
     if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
     if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_gauss_seidel: not an AMG solver (use cmg_mg_gauss_seidel)");

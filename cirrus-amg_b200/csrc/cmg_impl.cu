@@ -1,6 +1,7 @@
 // Device octree and AMG solver (see cmg_impl.hpp).
 #include "cmg_impl.hpp"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -363,6 +364,96 @@ void Solver::enqueue_geo_full_neg_lap(Grid& G, float* X, float* AX, cudaStream_t
     if (kind == kCMG) launch_accumulate_cells(d, 0, G.n, dLeaf, X, X, 0.125f, false, st);
     launch_geo_lap(kind, d, 0, G.n, X, AX, false, kind == kGMG ? (dLeaf | dGhost) : dLeaf, st);
     if (kind == kGMG) launch_accumulate_cells(d, 0, G.n, dGhost, AX, AX, 1.0f, true, st);
+}
+
+// FullNegativeLaplacian with calc_diag (src/GMGSolver.cu:167-171): the diagonal, GHOST
+// diagonals added into their LEAF parents (x's GHOST values are refreshed as a side effect)
+void Solver::enqueue_geo_full_neg_lap_diag(Grid& G, float* X, float* D, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    const int ch = (int)((X - G.chan) / ((size_t)G.n * kCells));
+    launch_propagate_ghost(d, 0, G.n, ch, st);
+    launch_geo_lap(kind, d, 0, G.n, X, D, false, dLeaf | dGhost, st, true);
+    launch_accumulate_cells(d, 0, G.n, dGhost, D, D, 1.0f, true, st);
+}
+
+// dot product over a device tile list, read back to the host
+int Solver::host_dot(Grid& G, const int* list, int nlist, const float* A, const float* B, double* out) {
+    if (int rc = ensure_scratch(nlist)) return rc;
+    if (!G.dot_out) CK(cudaMalloc(&G.dot_out, sizeof(double)));
+    launch_dot(G.dev(), list, nlist, A, B, kDotStore, G.dot_out, scratch(), G.stream);
+    CK(cudaMemcpyAsync(out, G.dot_out, sizeof(double), cudaMemcpyDeviceToHost, G.stream));
+    CK(cudaStreamSynchronize(G.stream));
+    return 0;
+}
+
+// AMGSolver::FASMuCycleSolve (src/AMGSolver.cu:1311-1356): mu-cycles on x (channel 0) against
+// b (channel 1), channel 2 as the FAS x0 and then r = b - A x; returns the index of the
+// iteration at which |r| < tol |b| (or max_iters) and |r| / |b|
+int Solver::fas_mu_cycle_solve(Grid& G, int repeat_times, int max_iters, double tol, int level_iters, int coarsest_iters, int* iters, double* rel) {
+    if (int rc = validate_solver_topology(G)) return rc;
+    const DevGrid d = G.dev();
+    cudaStream_t st = G.stream;
+    enqueue_cluster_pack(G, st);
+    launch_fill(G.plane(0), (size_t)G.n * kCells, 0.0f, st);
+    double bb = 0;
+    if (int rc = host_dot(G, G.leaf, G.nleaf, G.plane(1), G.plane(1), &bb)) return rc;
+    const double rhs_norm = std::sqrt(bb);
+    const double thr = std::max(tol * rhs_norm, DBL_MIN);
+    MuArgs A = mu_args(G, 0, 1, 2, level_iters, coarsest_iters);
+    A.mu = repeat_times;
+    double res = rhs_norm;
+    int i = 0;
+    for (; i < max_iters; ++i) {
+        enqueue_mu_step(G, G.max_level(), A, st);
+        // AMGFullNegativeLaplacianOnLeafs with its side effects on x: GHOST and NONLEAF values
+        launch_propagate_ghost(d, 0, G.n, 0, st);
+        launch_accumulate_cells(d, 0, G.n, dLeaf, G.plane(0), G.plane(0), 0.125f, false, st);
+        launch_leaf_apply(d, G.leaf, G.nleaf, G.plane(0), G.plane(2), coeff_ch, false, scratch(), st);
+        launch_leaf_residual(d, G.leaf, G.nleaf, G.plane(1), G.plane(2), false, st);
+        double rr = 0;
+        if (int rc = host_dot(G, G.leaf, G.nleaf, G.plane(2), G.plane(2), &rr)) return rc;
+        res = std::sqrt(rr);
+        if (res < thr) break;
+    }
+    *iters = i;
+    *rel = res / rhs_norm;
+    return 0;
+}
+
+// GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:390-470): channels x 0, b 1, r 2, D 3
+int Solver::damped_jacobi_solve(Grid& G, int max_iters, double tol, float omega, int* iters, double* rel) {
+    if (int rc = validate_solver_topology(G)) return rc;
+    const DevGrid d = G.dev();
+    cudaStream_t st = G.stream;
+    launch_fill(G.plane(0), (size_t)G.n * kCells, 0.0f, st);
+    // |b| over every tile (LEAF | NONLEAF | GHOST, src/GMGSolver.cu:407)
+    std::vector<int> all(G.n);
+    for (int t = 0; t < G.n; ++t) all[t] = t;
+    int* dall = nullptr;
+    CK(cudaMalloc(&dall, sizeof(int) * G.n));
+    int rc = 0;
+    double bb = 0, res = 0, rhs_norm = 0, thr = 0;
+    int i = 0;
+    if (cudaMemcpyAsync(dall, all.data(), sizeof(int) * G.n, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = 2;
+    if (!rc) rc = host_dot(G, dall, G.n, G.plane(1), G.plane(1), &bb);
+    cudaFree(dall);
+    if (rc) return rc;
+    rhs_norm = std::sqrt(bb);
+    thr = std::max(tol * rhs_norm, DBL_MIN);
+    res = rhs_norm;
+    for (; i < max_iters; ++i) {
+        enqueue_geo_full_neg_lap(G, G.plane(0), G.plane(2), st);
+        launch_leaf_residual(d, G.leaf, G.nleaf, G.plane(1), G.plane(2), true, st);
+        double rr = 0;
+        if (int e = host_dot(G, G.leaf, G.nleaf, G.plane(2), G.plane(2), &rr)) return e;
+        res = std::sqrt(rr);
+        if (res < thr) break;
+        enqueue_geo_full_neg_lap_diag(G, G.plane(0), G.plane(3), st);
+        launch_jacobi_update(d, G.leaf, G.nleaf, G.plane(0), G.plane(2), G.plane(3), omega, st);
+    }
+    *iters = i;
+    *rel = res / rhs_norm;
+    return 0;
 }
 
 void Solver::enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const {

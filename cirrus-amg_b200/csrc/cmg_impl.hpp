@@ -115,6 +115,11 @@ struct Solver {
     void enqueue_geo_full_neg_lap(Grid& G, float* X, float* AX, cudaStream_t st) const;
     void enqueue_geo_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st) const;
     void enqueue_geo_vcycle(Grid& G, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, cudaStream_t st) const;
+    void enqueue_geo_full_neg_lap_diag(Grid& G, float* X, float* D, cudaStream_t st) const;
+    // AMGSolver::FASMuCycleSolve and GMGSolver::dampedJacobiSolve: host-driven iterations
+    int fas_mu_cycle_solve(Grid& G, int repeat_times, int max_iters, double tol, int level_iters, int coarsest_iters, int* iters, double* rel);
+    int damped_jacobi_solve(Grid& G, int max_iters, double tol, float omega, int* iters, double* rel);
+    int host_dot(Grid& G, const int* list, int nlist, const float* A, const float* B, double* out);
     // z = M r with the solver's preconditioner (AMG: FAS mu-cycle; GMG/CMG: V-cycle), channel 3 as scratch
     void enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const;
     ~Solver();

@@ -125,7 +125,7 @@ __device__ __forceinline__ float geo_neg_lap(const GSnap& S, float h, float ooh,
 // NegativeLaplacianSameLevel128Kernel / ConservativeNegativeLaplacianSameLevel128Kernel
 // on tiles t0.. whose (subtree) type is in `types`
 template <int KIND>
-__global__ void __launch_bounds__(128) k_geo_lap(DevGrid g, int t0, const float* X, float* AX, int sl_is_level, int types) {
+__global__ void __launch_bounds__(128) k_geo_lap(DevGrid g, int t0, const float* X, float* AX, int sl_is_level, int types, int diag) {
     __shared__ GSnap S;
     const int t = t0 + blockIdx.x;
     const int own_tt = subtree_type(tile_type(g, t), sl_is_level);
@@ -136,8 +136,36 @@ __global__ void __launch_bounds__(128) k_geo_lap(DevGrid g, int t0, const float*
     const float ooh = __fdiv_rn(1.0f, h);
     float4 out;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) f4set(out, u, geo_neg_lap<KIND>(S, h, ooh, own_tt, Q.i, Q.j, Q.k0 + u, false));
+    for (int u = 0; u < 4; ++u) f4set(out, u, geo_neg_lap<KIND>(S, h, ooh, own_tt, Q.i, Q.j, Q.k0 + u, diag != 0));
     st4(AX + Q.base, out);
+}
+
+// r = b - r on the cells of LEAF tiles (every cell, or INTERIOR cells only)
+__global__ void __launch_bounds__(128) k_leaf_residual(DevGrid g, const int* leaf, const float* B, float* R, int interior_only) {
+    const int t = leaf[blockIdx.x];
+    const Quad Q(t, threadIdx.x);
+    const float4 b = ldcg4(B + Q.base);
+    float4 r = ldcg4(R + Q.base);
+    const uchar4 ty = ldt4(g.ctype + Q.base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (!interior_only || (t4get(ty, u) & dInterior)) f4set(r, u, __fsub_rn(f4get(b, u), f4get(r, u)));
+    st4(R + Q.base, r);
+}
+// damped Jacobi update (src/GMGSolver.cu:449-465): x += omega r / D on INTERIOR cells, x = 0 where D = 0
+__global__ void __launch_bounds__(128) k_jacobi_update(DevGrid g, const int* leaf, float* X, const float* R, const float* D, float omega) {
+    const int t = leaf[blockIdx.x];
+    const Quad Q(t, threadIdx.x);
+    float4 x = ldcg4(X + Q.base);
+    const float4 r = ldcg4(R + Q.base), d = ldcg4(D + Q.base);
+    const uchar4 ty = ldt4(g.ctype + Q.base);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (!(t4get(ty, u) & dInterior)) continue;
+        const float dd = f4get(d, u);
+        f4set(x, u, dd == 0.0f ? 0.0f : __fadd_rn(f4get(x, u), div_exact(__fmul_rn(omega, f4get(r, u)), dd)));
+    }
+    st4(X + Q.base, x);
 }
 
 // NegativeLaplacianAndGaussSeidelSameLevel128Kernel (src/GMGSolver.cu:173-210, src/CMGSolver.cu:226-262):
@@ -284,11 +312,22 @@ void launch_types_from_children(const DevGrid& g, int t0, int nt, cudaStream_t s
     k_types_from_children<<<nt, 128, 0, st>>>(g, t0);
 }
 
-void launch_geo_lap(int kind, const DevGrid& g, int t0, int nt, const float* X, float* AX, bool sl_is_level, int types, cudaStream_t st) {
+void launch_geo_lap(int kind, const DevGrid& g, int t0, int nt, const float* X, float* AX, bool sl_is_level, int types, cudaStream_t st,
+                    bool diag) {
     if (nt <= 0) return;
     note_kernel_launch();
-    if (kind == kCMG) k_geo_lap<kCMG><<<nt, 128, 0, st>>>(g, t0, X, AX, sl_is_level ? 1 : 0, types);
-    else k_geo_lap<kGMG><<<nt, 128, 0, st>>>(g, t0, X, AX, sl_is_level ? 1 : 0, types);
+    if (kind == kCMG) k_geo_lap<kCMG><<<nt, 128, 0, st>>>(g, t0, X, AX, sl_is_level ? 1 : 0, types, diag ? 1 : 0);
+    else k_geo_lap<kGMG><<<nt, 128, 0, st>>>(g, t0, X, AX, sl_is_level ? 1 : 0, types, diag ? 1 : 0);
+}
+void launch_leaf_residual(const DevGrid& g, const int* leaf, int nleaf, const float* B, float* R, bool interior_only, cudaStream_t st) {
+    if (nleaf <= 0) return;
+    note_kernel_launch();
+    k_leaf_residual<<<nleaf, 128, 0, st>>>(g, leaf, B, R, interior_only ? 1 : 0);
+}
+void launch_jacobi_update(const DevGrid& g, const int* leaf, int nleaf, float* X, const float* R, const float* D, float omega, cudaStream_t st) {
+    if (nleaf <= 0) return;
+    note_kernel_launch();
+    k_jacobi_update<<<nleaf, 128, 0, st>>>(g, leaf, X, R, D, omega);
 }
 void launch_geo_gs(int kind, const DevGrid& g, int t0, int nt, float* X, const float* B, int color, cudaStream_t st) {
     if (nt <= 0) return;

@@ -26,7 +26,10 @@ struct ReduceScratch {
 // --- geometric multigrid (geo_mg.cu): GMGSolver / CMGSolver ---
 enum SolverKind : int { kAMG = 0, kGMG = 1, kCMG = 2 };
 // operator on tiles t0..t0+nt whose type (NONLEAF counted as LEAF when sl_is_level) is in `types`
-void launch_geo_lap(int kind, const DevGrid& g, int t0, int nt, const float* X, float* AX, bool sl_is_level, int types, cudaStream_t st);
+void launch_geo_lap(int kind, const DevGrid& g, int t0, int nt, const float* X, float* AX, bool sl_is_level, int types, cudaStream_t st,
+                    bool diag = false);
+void launch_leaf_residual(const DevGrid& g, const int* leaf, int nleaf, const float* B, float* R, bool interior_only, cudaStream_t st);
+void launch_jacobi_update(const DevGrid& g, const int* leaf, int nleaf, float* X, const float* R, const float* D, float omega, cudaStream_t st);
 void launch_geo_gs(int kind, const DevGrid& g, int t0, int nt, float* X, const float* B, int color, cudaStream_t st);
 void launch_geo_restrict(int kind, const DevGrid& g, int t0, int nt, const float* X, float* RHS, float one_over_alpha, cudaStream_t st);
 void launch_geo_prolong(const DevGrid& g, int t0, int nt, float* X, float P, cudaStream_t st);

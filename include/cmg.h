@@ -191,6 +191,19 @@ int cmg_mg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, in
 /* FullNegativeLaplacian / ConservativeFullNegativeLaplacian (src/GMGSolver.cu:167,
  * src/CMGSolver.cu:210); writes GHOST (and, for CMG, NONLEAF) values of x_ch */
 int cmg_mg_full_neg_lap(cmg_amg_solver* s, cmg_grid* g, int x_ch, int ax_ch);
+
+/* AMGSolver::FASMuCycleSolve (src/AMGSolver.cu:1311-1356): the FAS mu-cycle with
+ * repeat_times recursions as a stand-alone iteration on x (channel 0) against b
+ * (channel 1, kept), channel 2 as scratch.  iters is the index of the iteration at
+ * which |b - A x| < tol |b| (max_iters if never), rel_res = |b - A x| / |b|.  The
+ * reference's test harness uses it as "amg_vcycle" with AMGSolver(coeff, 0.5, 0.5, 1)
+ * (tests/SolverTests.cu:1100-1112).  Synchronises the host once per iteration. */
+int cmg_amg_fas_mu_cycle_solve(cmg_amg_solver* s, cmg_grid* g, int repeat_times, int verbose, int max_iters, double tol, int level_iters,
+                               int coarsest_iters, int* iters, double* rel_res);
+/* GMGSolver::dampedJacobiSolve (src/GMGSolver.cu:390-470), a GMG solver only: x (channel
+ * 0) += omega r / D against b (channel 1), channels 2-3 as scratch; same result
+ * convention as cmg_amg_fas_mu_cycle_solve ("gmg_jacobi", tests/SolverTests.cu:1063). */
+int cmg_gmg_damped_jacobi_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, float omega, int* iters, double* rel_res);
 /* AMGSolver::solve (src/AMGSolver.cu:1399): solves -lap x = b, b read from
  * channel 1 and overwritten by the residual, x written to channel 0.
  * iters/rel_res are the reference's (num_iters, relative_residual), with

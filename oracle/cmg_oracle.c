@@ -1657,3 +1657,118 @@ void og_calc_cell_types_from_leafs(og_grid* g) {
         for (int v = 0; v < NC; v++) CT(g, t)[v] = p >= 0 ? CT(g, p)[parent_cell(g, t, v)] : OG_DIRICHLET;
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* stand-alone iterative solvers of the reference's test harness        */
+/* ------------------------------------------------------------------ */
+/* Dot over the tiles of the given types */
+static double dot_types(og_grid* g, int a_ch, int b_ch, int types) {
+    double s = 0;
+    for (int t = 0; t < g->n; t++) {
+        if (!(g->t[t].type & types)) continue;
+        const float* A = CH(g, a_ch, t);
+        const float* B = CH(g, b_ch, t);
+        double st = 0;
+        for (int q = 0; q < NC; q += 4) {
+            float f = A[q] * B[q];
+            f = fmaf(A[q + 1], B[q + 1], f);
+            f = fmaf(A[q + 2], B[q + 2], f);
+            f = fmaf(A[q + 3], B[q + 3], f);
+            st += (double)f;
+        }
+        s += st;
+    }
+    return s;
+}
+
+/* AMGSolver::FASMuCycleSolve (AMGSolver.cu:1311-1356): mu-cycles on x (channel 0) against
+ * b (channel 1), channel 2 as the FAS x0 and then the residual b - A x; stops when
+ * |r| < tol |b| and returns the iteration index at which it stopped */
+int og_fas_mu_cycle_solve(og_grid* g, int coeff_ch, int repeat_times, double omega, float Rr, float P, int max_iters, double tol, int level_iters,
+                          int coarsest_iters, double* rel_res) {
+    const int X = 0, B = 1, X0 = 2;
+    memset(CH(g, X, 0), 0, sizeof(float) * NC * g->n);
+    double rhs_norm = sqrt(og_dot(g, B, B));
+    double thr = tol * rhs_norm;
+    if (thr < DBL_MIN) thr = DBL_MIN;
+    mu_args A = {repeat_times, X, B, X0, coeff_ch, level_iters, coarsest_iters, omega, Rr, P};
+    double res = rhs_norm;
+    int i;
+    for (i = 0; i < max_iters; i++) {
+        fas_step(g, g->max_level, &A);
+        og_full_neg_lap_leafs(g, X, coeff_ch, X0);
+        for (int t = 0; t < g->n; t++) {
+            if (!(g->t[t].type & OG_LEAF)) continue;
+            for (int v = 0; v < NC; v++) CH(g, X0, t)[v] = CH(g, B, t)[v] - CH(g, X0, t)[v];
+        }
+        res = sqrt(og_dot(g, X0, X0));
+        if (res < thr) break;
+    }
+    if (rel_res) *rel_res = res / rhs_norm;
+    return i;
+}
+
+/* FullNegativeLaplacian with calc_diag (GMGSolver.cu:167-171): the diagonal of the GMG
+ * operator on LEAF and GHOST tiles, GHOST diagonals added into their LEAF parents */
+static void gmg_full_diag(og_grid* g, int x_ch, int d_ch) {
+    propagate_ghosts(g, x_ch);
+    og_gsnap* S = (og_gsnap*)malloc(sizeof(og_gsnap));
+    for (int t = 0; t < g->n; t++) {
+        int ty = g->t[t].type;
+        if (!(ty & (OG_LEAF | OG_GHOST))) continue;
+        float h = voxel_size(g, g->t[t].level);
+        load_gsnap(g, OG_GMG, t, -1, x_ch, S);
+        for (int v = 0; v < NC; v++) CH(g, d_ch, t)[v] = gsnap_neg_lap(OG_GMG, S, h, v, 1);
+    }
+    free(S);
+    for (int t = 0; t < g->n; t++) {
+        if (!(g->t[t].type & OG_GHOST)) continue;
+        int p = g->parent[t];
+        if (p < 0) continue;
+        for (int b = 0; b < 64; b++) {
+            int fl[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
+            float sum = 0;
+            for (int ii = 0; ii < 2; ii++)
+                for (int jj = 0; jj < 2; jj++)
+                    for (int kk = 0; kk < 2; kk++) {
+                        int v = CELL(fl[0] + ii, fl[1] + jj, fl[2] + kk);
+                        sum += (CT(g, t)[v] & (OG_INTERIOR | OG_DIRICHLET | OG_NEUMANN)) ? CH(g, d_ch, t)[v] : 0.0f;
+                    }
+            float* c = &CH(g, d_ch, p)[parent_cell(g, t, CELL(fl[0], fl[1], fl[2]))];
+            *c = fmaf(sum, 1.0f, *c);
+        }
+    }
+}
+/* GMGSolver::dampedJacobiSolve (GMGSolver.cu:390-470): x += omega r / D on INTERIOR cells
+ * of LEAF tiles (x = 0 where D = 0), channels x 0, b 1, r 2, D 3 */
+int og_gmg_damped_jacobi_solve(og_grid* g, int max_iters, double tol, float omega, double* rel_res) {
+    const int X = 0, B = 1, AX = 2, D = 3;
+    memset(CH(g, X, 0), 0, sizeof(float) * NC * g->n);
+    double rhs_norm = sqrt(dot_types(g, B, B, OG_LEAF | OG_NONLEAF | OG_GHOST));
+    double thr = tol * rhs_norm;
+    if (thr < DBL_MIN) thr = DBL_MIN;
+    double res = rhs_norm;
+    int i;
+    for (i = 0; i < max_iters; i++) {
+        og_geo_full_neg_lap(g, OG_GMG, X, AX);
+        for (int t = 0; t < g->n; t++) {
+            if (!(g->t[t].type & OG_LEAF)) continue;
+            for (int v = 0; v < NC; v++)
+                if (CT(g, t)[v] & OG_INTERIOR) CH(g, AX, t)[v] = CH(g, B, t)[v] - CH(g, AX, t)[v];
+        }
+        res = sqrt(og_dot(g, AX, AX));
+        if (res < thr) break;
+        gmg_full_diag(g, X, D);
+        for (int t = 0; t < g->n; t++) {
+            if (!(g->t[t].type & OG_LEAF)) continue;
+            for (int v = 0; v < NC; v++) {
+                if (!(CT(g, t)[v] & OG_INTERIOR)) continue;
+                float d = CH(g, D, t)[v];
+                if (d == 0.0f) CH(g, X, t)[v] = 0.0f;
+                else CH(g, X, t)[v] = CH(g, X, t)[v] + (omega * CH(g, AX, t)[v]) / d;
+            }
+        }
+    }
+    if (rel_res) *rel_res = res / rhs_norm;
+    return i;
+}

@@ -88,6 +88,10 @@ void og_geo_gauss_seidel(og_grid* g, int kind, int iters, int order, int level, 
 void og_geo_vcycle(og_grid* g, int kind, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters, float one_over_alpha, float P);
 int og_geo_solve(og_grid* g, int kind, float one_over_alpha, float P, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, double* rel_res);
 
+/* stand-alone iterative solvers of the reference's test harness */
+int og_fas_mu_cycle_solve(og_grid* g, int coeff_ch, int repeat_times, double omega, float R_restrict, float P, int max_iters, double tol, int level_iters, int coarsest_iters, double* rel_res);
+int og_gmg_damped_jacobi_solve(og_grid* g, int max_iters, double tol, float omega, double* rel_res);
+
 /* FP64 CSR assembly of the leaf operator (unknowns = INTERIOR cells of LEAF tiles) */
 int og_assemble_count(og_grid* g, int coeff_ch, int* n_rows, long long* nnz);
 int og_assemble(og_grid* g, int coeff_ch, long long* rowptr, int* col, double* val, int* row_tile, int* row_cell);

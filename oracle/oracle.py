@@ -67,6 +67,8 @@ def lib():
             "og_geo_gauss_seidel": (None, [P, I, I, I, I, I, I]),
             "og_geo_vcycle": (None, [P, I, I, I, I, I, I, F, F]),
             "og_geo_solve": (I, [P, I, F, F, I, D, I, I, I, I, P]),
+            "og_fas_mu_cycle_solve": (I, [P, I, I, D, F, F, I, D, I, I, P]),
+            "og_gmg_damped_jacobi_solve": (I, [P, I, D, F, P]),
             "og_assemble_count": (I, [P, I, P, P]),
             "og_assemble": (I, [P, I, P, P, P, P, P]),
             "og_csr_solve": (I, [I, P, P, P, P, P, D, I, I, P, P]),
@@ -196,6 +198,18 @@ class Grid:
         rel = ctypes.c_double(0)
         it = self.L.og_geo_solve(self.g, kind, one_over_alpha, P, max_iters, tol, level_iters, coarsest_iters, sync_stride,
                                  int(pure_neumann), ctypes.byref(rel))
+        return it, rel.value
+
+    def fas_mu_cycle_solve(self, coeff_ch, repeat_times=1, omega=1.5, R_restrict=1.0, P=1.0, max_iters=100, tol=1e-6,
+                           level_iters=2, coarsest_iters=10):
+        rel = ctypes.c_double(0)
+        it = self.L.og_fas_mu_cycle_solve(self.g, coeff_ch, repeat_times, omega, R_restrict, P, max_iters, tol, level_iters,
+                                          coarsest_iters, ctypes.byref(rel))
+        return it, rel.value
+
+    def gmg_damped_jacobi_solve(self, max_iters=100, tol=1e-6, omega=1.0):
+        rel = ctypes.c_double(0)
+        it = self.L.og_gmg_damped_jacobi_solve(self.g, max_iters, tol, omega, ctypes.byref(rel))
         return it, rel.value
 
     def face_velocity_fourier(self, u_ch, k, amp, phase):

@@ -418,3 +418,64 @@ def test_geometric_solve_matches_oracle(kind, case_id, prm):
     m = ty == cmg.LEAF
     x = G.download(0)[m]
     assert np.linalg.norm(x - g.channel(0)[m]) <= 1e-5 * np.linalg.norm(g.channel(0)[m])
+
+
+@pytest.mark.parametrize("case_id,prm", [(cmg.CASE_UNIFORM, [2, 2]), (cmg.CASE_CENTER_POINT, [2, 4])])
+def test_pure_neumann_solve_matches_oracle(case_id, prm):
+    from workloads import pure_neumann_setup
+
+    G = build_product(case_id, prm)
+    g = build_oracle(case_id, prm)
+    lv, ijk, ty = G.tiles()
+    ct, b = pure_neumann_setup(lv, ijk, ty)
+    G.upload_cell_types(ct)
+    g.cell_types()[:] = ct
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    solver.prepareTypesAndCoeffs(G)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    G.upload(1, b)
+    g.channel(1)[:] = b
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, True)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6, pure_neumann=True)
+    assert rel <= 1e-6 and relo <= 1e-6 and abs(it - ito) <= 1
+    m = (ty[:, None] == cmg.LEAF) & (G.download_cell_types() == cmg.INTERIOR)
+    x, xo = G.download(0)[m], g.channel(0)[m]
+    assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("case_id,prm", [(cmg.CASE_UNIFORM, [2, 2]), (cmg.CASE_CENTER_POINT, [2, 4])])
+def test_fas_mu_cycle_solve_matches_oracle(case_id, prm):
+    """AMGSolver::FASMuCycleSolve as the reference harness's "amg_vcycle": AMGSolver(coeff, 0.5, 0.5, 1),
+    mu = 1, level_iters = 1 (tests/SolverTests.cu:1100-1112)."""
+    from workloads import uniform_rhs
+
+    G = build_product(case_id, prm)
+    g = build_oracle(case_id, prm)
+    G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    solver = cmg.AMGSolver(COEFF, 0.5, 0.5, 1.0)
+    solver.prepareTypesAndCoeffs(G)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    lv, ijk, ty = G.tiles()
+    b = uniform_rhs(ty == cmg.LEAF, 0)
+    G.upload(1, b)
+    g.channel(1)[:] = b
+    it, rel = solver.FASMuCycleSolve(1, G, False, 60, 1e-6, 1, 10)
+    ito, relo = g.fas_mu_cycle_solve(COEFF, repeat_times=1, R_restrict=0.5, max_iters=60, tol=1e-6, level_iters=1, coarsest_iters=10)
+    assert abs(it - ito) <= 1
+    assert rel == pytest.approx(relo, rel=1e-3)
+    m = ty == cmg.LEAF
+    x, xo = G.download(0)[m], g.channel(0)[m]
+    assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)
+
+
+def test_gmg_damped_jacobi_matches_oracle():
+    G, g, solver, b = _geo_pair(cmg.CASE_CENTER_POINT, [2, 4], O.GMG)
+    it, rel = solver.dampedJacobiSolve(G, False, 40, 1e-12, 1.0)
+    ito, relo = g.gmg_damped_jacobi_solve(max_iters=40, tol=1e-12, omega=1.0)
+    assert it == ito == 40
+    assert rel == pytest.approx(relo, rel=1e-4)
+    lv, ijk, ty = G.tiles()
+    m = ty == cmg.LEAF
+    x, xo = G.download(0)[m], g.channel(0)[m]
+    assert np.linalg.norm(x - xo) <= 1e-5 * np.linalg.norm(xo)

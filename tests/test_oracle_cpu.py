@@ -307,3 +307,21 @@ def test_kat_recovery_geometric(kind):
     m = (ty[:, None] == O.LEAF) & (ct == O.INTERIOR)
     err = np.abs(g.channel(0)[m] - xt[m]).max()
     assert rel < 1e-6 and err < 1e-4, (it, rel, err)
+
+
+def test_pure_neumann_solve_converges():
+    """is_pure_neumann: r recentred to zero mean before every preconditioning (src/AMGSolver.cu:1425,1505)."""
+    from workloads import pure_neumann_setup
+
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(O.CASE_CENTER_POINT, [2, 4])
+    g.alloc(16)
+    lv, ijk, ty = g.tiles()
+    ct, b = pure_neumann_setup(lv, ijk, ty)
+    g.cell_types()[:] = ct
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    g.channel(1)[:] = b
+    it, rel = g.amg_solve(COEFF, max_iters=100, tol=1e-6, pure_neumann=True)
+    assert rel < 1e-6 and it < 30

@@ -159,3 +159,16 @@ def projected_divergence(download, lv, ijk, ty, ct, b0, div_ch):
     d0 = np.linalg.norm(b0[m].astype(np.float64))
     d1 = np.linalg.norm(download(div_ch)[m].astype(np.float64))
     return d1 / d0
+
+
+def pure_neumann_setup(lv, ijk, ty, seed=4):
+    """LEAF cell types with the outer layer of the domain NEUMANN (no Dirichlet cell anywhere:
+    the operator is singular) and a zero-mean rhs on the INTERIOR cells."""
+    ct = np.where(~away_from_walls(lv, ijk), 4, 2).astype(np.uint8)
+    ct[ty != 1] = 0
+    m = (ty[:, None] == 1) & (ct == 2)
+    rng = np.random.default_rng(seed)
+    b = np.zeros((len(lv), 512), np.float32)
+    b[m] = rng.standard_normal(int(m.sum())).astype(np.float32)
+    b[m] -= b[m].mean(dtype=np.float64).astype(np.float32)
+    return ct, b
