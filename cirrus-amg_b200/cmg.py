@@ -36,7 +36,7 @@ EXPORTS = [
     "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
     "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
     "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_copy_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
-    "cmg_grid_calc_cell_types_from_leafs",
+    "cmg_grid_calc_cell_types_from_leafs", "cmg_grid_load_hagr", "cmg_grid_dump_hagr",
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
     "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_add_gradient_to_face", "cmg_amg_full_neg_lap",
@@ -91,6 +91,8 @@ def lib():
             "cmg_grid_set_leaf_cell_types_case": (I, [P, I, P, I]),
             "cmg_grid_set_stream": (I, [P, P]),
             "cmg_grid_calc_cell_types_from_leafs": (I, [P]),
+            "cmg_grid_load_hagr": (I, [P, S, I, PP]),
+            "cmg_grid_dump_hagr": (I, [P, P, S, ctypes.POINTER(ctypes.c_size_t)]),
             "cmg_grid_synchronize": (I, [P]),
             "cmg_amg_prepare_types_and_coeffs": (I, [P, I, F]),
             "cmg_amg_prepare_system": (I, [P, I, F]),
@@ -161,6 +163,13 @@ class HADeviceGrid:
         self.h0 = h0
         self.num_channels = num_channels
         self._cb = None
+
+    def _adopt(self, h, num_channels):
+        self.L = lib()
+        self.h = h
+        self.num_channels = num_channels
+        self._cb = None
+        self.h0 = None  # held by the library
 
     def __del__(self):
         try:
@@ -246,6 +255,25 @@ class HADeviceGrid:
 
     def copy(self, src_ch, dst_ch):
         _check(self.L.cmg_grid_copy_channel(self.h, src_ch, dst_ch), "copy_channel")
+
+    @classmethod
+    def loadBinaryBlob(cls, blob, num_channels=16):
+        """HADeviceGrid::loadBinaryBlob (src/HAGrid.h:788): a grid from an 'HAGR' v1 blob."""
+        L = lib()
+        buf = (ctypes.c_uint8 * len(blob)).from_buffer_copy(bytes(blob))
+        h = ctypes.c_void_p()
+        _check(L.cmg_grid_load_hagr(buf, len(blob), num_channels, ctypes.byref(h)), "loadBinaryBlob")
+        self = cls.__new__(cls)
+        self._adopt(h, num_channels)
+        return self
+
+    def dumpBinaryBlob(self):
+        """HADeviceGrid::dumpBinaryBlob (src/HAGrid.h:687): the grid as an 'HAGR' v1 blob (bytes)."""
+        n = ctypes.c_size_t(0)
+        _check(self.L.cmg_grid_dump_hagr(self.h, None, 0, ctypes.byref(n)), "dumpBinaryBlob")
+        buf = (ctypes.c_uint8 * n.value)()
+        _check(self.L.cmg_grid_dump_hagr(self.h, buf, n.value, ctypes.byref(n)), "dumpBinaryBlob")
+        return bytes(buf)
 
     def calc_cell_types_from_leafs(self):
         """CalcCellTypesFromLeafs (src/PoissonGrid.cu:923): NONLEAF and GHOST cell types from the LEAF ones."""

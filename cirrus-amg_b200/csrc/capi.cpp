@@ -1,6 +1,7 @@
 // extern "C" entry points declared in include/cmg.h.
 #include "cmg.h"
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -492,6 +493,139 @@ int cmg_amg_last_solve_launches(cmg_amg_solver* s, long long* launches) {
     if (!s || !launches) return fail(CMG_ERR_INVALID, "null argument");
     *launches = s->s.last_launches;
     return CMG_OK;
+}
+
+// ---- 'HAGR' v1 grid blobs (HADeviceGrid::dumpBinaryBlob / loadBinaryBlob, src/HAGrid.h:687-853) ----
+// Layout (little endian, the reference's in-memory structs written raw):
+//   header, 40 bytes: u32 magic 0x52474148, u32 version 1, u32 num_levels, i32 max_level,
+//     u32 tile_size (sizeof(PoissonTile<float,15>) = 44880), u32 coord_size (12), f32 h0,
+//     4 bytes of padding, u64 tile_count;
+//   num_levels x u32 log2 hash sizes;
+//   tile_count records: u32 level, u8 type, 3 x i32 tile coordinate, tile_size bytes of tile:
+//     float data[15][736] (cell values in the first 512 of each channel), 6 neighbour
+//     descriptors (192 bytes, pointers: meaningless in a file), u8 cell types[512] at byte
+//     44352, then flags and status words.
+}  // extern "C"
+
+namespace {
+constexpr uint32_t kHagrMagic = 0x52474148u;
+constexpr size_t kHagrHeader = 40, kHagrTile = 44880, kHagrCoord = 12, kHagrTypes = 44352;
+constexpr int kHagrChannels = 15, kHagrChannelStride = 736;
+constexpr size_t kHagrRecord = 4 + 1 + kHagrCoord + kHagrTile;
+template <class T>
+T rd(const uint8_t* p) {
+    T v;
+    std::memcpy(&v, p, sizeof(T));
+    return v;
+}
+template <class T>
+void wr(uint8_t* p, T v) {
+    std::memcpy(p, &v, sizeof(T));
+}
+}  // namespace
+
+extern "C" {
+
+int cmg_grid_load_hagr(const uint8_t* blob, size_t size, int num_channels, cmg_grid** out) {
+    GUARD_BEGIN
+    if (!blob || !out || num_channels < 1) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad argument");
+    if (size < kHagrHeader) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: buffer too small");
+    if (rd<uint32_t>(blob) != kHagrMagic) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad magic");
+    if (rd<uint32_t>(blob + 4) != 1) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: unsupported version");
+    const uint32_t num_levels = rd<uint32_t>(blob + 8);
+    if (rd<uint32_t>(blob + 16) != kHagrTile) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: tile size is not that of PoissonTile<float,15>");
+    if (rd<uint32_t>(blob + 20) != kHagrCoord) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: coordinate size mismatch");
+    const float h0 = rd<float>(blob + 24);
+    const uint64_t count = rd<uint64_t>(blob + 32);
+    if (num_levels < 1 || num_levels > 16 || !(h0 > 0)) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad header");
+    const size_t body = kHagrHeader + 4 * (size_t)num_levels;
+    if (size < body || (size - body) / kHagrRecord < count) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: buffer truncated");
+    cmg_grid* g = new cmg_grid(h0, (int)num_levels, num_channels);
+    auto bail = [&](int code, const char* msg) {
+        delete g;
+        return fail(code, msg);
+    };
+    const uint8_t* rec = blob + body;
+    for (uint64_t r = 0; r < count; ++r) {
+        const uint8_t* p = rec + r * kHagrRecord;
+        const int level = (int)rd<uint32_t>(p), type = p[4];
+        if (type != CMG_LEAF && type != CMG_NONLEAF && type != CMG_GHOST) return bail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad tile type");
+        if (type == CMG_GHOST) continue;  // GHOST tiles are spawned by the rebuild
+        if (g->g.topo.set(level, rd<int32_t>(p + 5), rd<int32_t>(p + 9), rd<int32_t>(p + 13), type) < 0)
+            return bail(CMG_ERR_INVALID, "cmg_grid_load_hagr: tile level out of range");
+    }
+    if (int rc = g->g.rebuild()) return bail(rc, "cmg_grid_load_hagr: rebuild failed");
+    const int n = g->g.topo.size();
+    const int nc = std::min(num_channels, kHagrChannels);
+    std::vector<float> planes((size_t)nc * n * 512, 0.0f);
+    std::vector<uint8_t> types((size_t)n * 512, 0);
+    for (uint64_t r = 0; r < count; ++r) {
+        const uint8_t* p = rec + r * kHagrRecord;
+        const int t = g->g.topo.find((int)rd<uint32_t>(p), rd<int32_t>(p + 5), rd<int32_t>(p + 9), rd<int32_t>(p + 13));
+        if (t < 0 || g->g.topo.tiles()[t].type != p[4]) return bail(CMG_ERR_TOPOLOGY, "cmg_grid_load_hagr: the blob's tiles are not a graded octree with its ghost layer");
+        const uint8_t* tile = p + 17;
+        for (int c = 0; c < nc; ++c) std::memcpy(&planes[((size_t)c * n + t) * 512], tile + (size_t)c * kHagrChannelStride * 4, 512 * 4);
+        std::memcpy(&types[(size_t)t * 512], tile + kHagrTypes, 512);
+    }
+    if (!grid_ready(g)) return bail(CMG_ERR_CUDA, "cmg_grid_load_hagr: device allocation failed");
+    for (int c = 0; c < num_channels; ++c) {
+        cudaError_t e = c < nc ? cudaMemcpyAsync(g->g.plane(c), &planes[(size_t)c * n * 512], sizeof(float) * n * 512, cudaMemcpyHostToDevice, g->g.stream)
+                               : cudaMemsetAsync(g->g.plane(c), 0, sizeof(float) * n * 512, g->g.stream);
+        if (e != cudaSuccess) return bail(CMG_ERR_CUDA, "cmg_grid_load_hagr: upload failed");
+    }
+    if (cudaMemcpyAsync(g->g.ctype, types.data(), types.size(), cudaMemcpyHostToDevice, g->g.stream) != cudaSuccess ||
+        cudaStreamSynchronize(g->g.stream) != cudaSuccess)
+        return bail(CMG_ERR_CUDA, "cmg_grid_load_hagr: upload failed");
+    *out = g;
+    return CMG_OK;
+    GUARD_END
+}
+
+int cmg_grid_dump_hagr(cmg_grid* g, uint8_t* buf, size_t capacity, size_t* size) {
+    GUARD_BEGIN
+    if (!size) return fail(CMG_ERR_INVALID, "cmg_grid_dump_hagr: null size");
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_dump_hagr: grid not built");
+    const cmg::Grid& G = g->g;
+    const int n = G.topo.size(), nl = G.topo.num_levels();
+    const size_t total = kHagrHeader + 4 * (size_t)nl + (size_t)n * kHagrRecord;
+    *size = total;
+    if (!buf) return CMG_OK;
+    if (capacity < total) return fail(CMG_ERR_INVALID, "cmg_grid_dump_hagr: buffer too small");
+    const int nc = std::min(G.nch, kHagrChannels);
+    std::vector<float> planes((size_t)nc * n * 512);
+    std::vector<uint8_t> types((size_t)n * 512);
+    CKC(cudaMemcpyAsync(planes.data(), G.chan, sizeof(float) * planes.size(), cudaMemcpyDeviceToHost, G.stream));
+    CKC(cudaMemcpyAsync(types.data(), G.ctype, types.size(), cudaMemcpyDeviceToHost, G.stream));
+    CKC(cudaStreamSynchronize(G.stream));
+    std::memset(buf, 0, total);
+    wr<uint32_t>(buf, kHagrMagic);
+    wr<uint32_t>(buf + 4, 1);
+    wr<uint32_t>(buf + 8, (uint32_t)nl);
+    wr<int32_t>(buf + 12, G.max_level());
+    wr<uint32_t>(buf + 16, (uint32_t)kHagrTile);
+    wr<uint32_t>(buf + 20, (uint32_t)kHagrCoord);
+    wr<float>(buf + 24, G.topo.h0());
+    wr<uint64_t>(buf + 32, (uint64_t)n);
+    for (int l = 0; l < nl; ++l) {
+        // hash size for the reference's loader: room for twice the level's tiles, at least 2^8
+        const int cnt = l <= G.max_level() ? G.level_end(l) - G.level_begin(l) : 0;
+        uint32_t lg = 8;
+        while ((1u << lg) < 2u * (uint32_t)cnt + 1u && lg < 30) ++lg;
+        wr<uint32_t>(buf + kHagrHeader + 4 * l, lg);
+    }
+    uint8_t* rec = buf + kHagrHeader + 4 * (size_t)nl;
+    const auto& T = G.topo.tiles();
+    for (int t = 0; t < n; ++t) {
+        uint8_t* p = rec + (size_t)t * kHagrRecord;
+        wr<uint32_t>(p, (uint32_t)T[t].level);
+        p[4] = (uint8_t)T[t].type;
+        for (int d = 0; d < 3; ++d) wr<int32_t>(p + 5 + 4 * d, T[t].c[d]);
+        uint8_t* tile = p + 17;
+        for (int c = 0; c < nc; ++c) std::memcpy(tile + (size_t)c * kHagrChannelStride * 4, &planes[((size_t)c * n + t) * 512], 512 * 4);
+        std::memcpy(tile + kHagrTypes, &types[(size_t)t * 512], 512);
+    }
+    return CMG_OK;
+    GUARD_END
 }
 
 }  // extern "C"

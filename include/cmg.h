@@ -112,6 +112,15 @@ int cmg_grid_copy_channel(cmg_grid* g, int src_ch, int dst_ch);
  * NEUMANN), then GHOST cell types from their parents.  Needed before a GMG or CMG
  * solve; AMG sets its own types in cmg_amg_prepare_types_and_coeffs. */
 int cmg_grid_calc_cell_types_from_leafs(cmg_grid* g);
+/* HADeviceGrid::loadBinaryBlob / dumpBinaryBlob (src/HAGrid.h:687-853): the 'HAGR'
+ * version-1 grid blob with raw PoissonTile<float,15> records (44880 bytes each).
+ * Loading rebuilds the octree from the LEAF and NONLEAF records (GHOST tiles are
+ * spawned again and must match the blob's), copies the cell values of the first
+ * min(num_channels, 15) channels and the cell types of every record, and zeroes any
+ * further channels.  Dumping writes every tile with min(num_channels, 15) channels;
+ * with buf == NULL it only reports the size. */
+int cmg_grid_load_hagr(const uint8_t* blob, size_t size, int num_channels, cmg_grid** out);
+int cmg_grid_dump_hagr(cmg_grid* g, uint8_t* buf, size_t capacity, size_t* size);
 int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams);
 /* stream used by every later call on this grid (NULL = legacy default) */
 int cmg_grid_set_stream(cmg_grid* g, void* cuda_stream);
