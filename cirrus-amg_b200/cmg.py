@@ -45,7 +45,7 @@ EXPORTS = [
     "cmg_gmg_solver_create", "cmg_cmg_solver_create", "cmg_mg_vcycle", "cmg_mg_gauss_seidel", "cmg_mg_full_neg_lap",
     "cmg_amg_fas_mu_cycle_solve", "cmg_gmg_damped_jacobi_solve",
     "cmg_amg_solve",
-    "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
+    "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_gauss_seidel_masked", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
     "cmg_amg_last_solve_launches",
 ]
 
@@ -117,6 +117,7 @@ def lib():
             "cmg_amg_solve": (I, [P, P, I, I, D, I, I, I, I, P, P]),
             "cmg_amg_solve_host": (I, [P, P, P, P, S, I, D, I, I, I, I, P, P]),
             "cmg_amg_gauss_seidel": (I, [P, P, I, I, I, I, I]),
+            "cmg_amg_gauss_seidel_masked": (I, [P, P, I, I, I, I, I]),
             "cmg_amg_fas_mu_cycle": (I, [P, P, I, I, I, I, I]),
             "cmg_amg_last_solve_ms": (I, [P, P]),
             "cmg_amg_last_solve_launches": (I, [P, P]),
@@ -374,6 +375,11 @@ class AMGSolver:
     def gauss_seidel(self, grid, iters, order, level, x_ch, rhs_ch):
         self._sync_params()
         _check(self.L.cmg_amg_gauss_seidel(self.h, grid.h, iters, order, level, x_ch, rhs_ch), "gauss_seidel")
+
+    def gauss_seidel_masked(self, grid, iters, order, level, x_ch, rhs_ch):
+        """The sweeps as the cycle runs them; x must be 0 on cells that are not INTERIOR."""
+        self._sync_params()
+        _check(self.L.cmg_amg_gauss_seidel_masked(self.h, grid.h, iters, order, level, x_ch, rhs_ch), "gauss_seidel_masked")
 
     def fas_mu_cycle(self, grid, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters):
         self._sync_params()

@@ -474,6 +474,14 @@ int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, i
     s->s.enqueue_gs(g->g, level, iters, order, g->g.plane(x_ch), g->g.plane(rhs_ch), g->g.stream);
     return cmg::check_cuda(cudaGetLastError(), "gauss_seidel");
 }
+int cmg_amg_gauss_seidel_masked(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_gauss_seidel_masked: not an AMG solver (use cmg_mg_gauss_seidel)");
+    if (level < 0 || level > g->g.max_level() || !chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || (order != 0 && order != 1))
+        return fail(CMG_ERR_INVALID, "cmg_amg_gauss_seidel_masked: bad argument");
+    s->s.enqueue_gs(g->g, level, iters, order, g->g.plane(x_ch), g->g.plane(rhs_ch), g->g.stream, true);
+    return cmg::check_cuda(cudaGetLastError(), "gauss_seidel");
+}
 int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) {
     if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
     if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_fas_mu_cycle: not an AMG solver (use cmg_mg_vcycle)");

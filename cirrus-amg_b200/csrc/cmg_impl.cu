@@ -288,13 +288,13 @@ void Solver::enqueue_cluster_pack(Grid& G, cudaStream_t st) const {
 // AMGSolver::FASMuCycleStep (src/AMGSolver.cu:1257-1277).  A visit of level 2
 // runs as one cluster launch when levels 0-2 are complete; otherwise levels 0
 // and 1 run as a single coarse-kernel launch.
-void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) const {
+void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st, bool fas2) const {
     const DevGrid d = G.dev();
     if (l == 2 && cluster_active(G)) {
         int tile1[8], tile2[64];
         coarse_tiles(G, tile1, tile2);
         launch_cluster_step(d, tile1, tile2, cluster_pack, A.X, A.RHS, A.X0, A.coeff_ch, A.mu, A.level_iters, A.coarsest_iters, A.omega, A.Rr,
-                            A.P, st);
+                            A.P, fas2, st);
         return;
     }
     if (l <= 1) {
@@ -317,8 +317,10 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st) c
     }
     enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st, true);
     launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
-    launch_fas_save(d, G.nonleaf_begin(l - 1), G.ghost_begin(l - 1) - G.nonleaf_begin(l - 1), A.X, A.RHS, A.X0, A.coeff_ch, st);
-    for (int r = 0; r < A.mu; ++r) enqueue_mu_step(G, l - 1, A, st);
+    // the first cluster launch of level 2 does level 2's FAS update itself when every level-2 tile is NONLEAF
+    const bool fold = l - 1 == 2 && A.mu > 0 && cluster_active(G) && G.nonleaf_begin(2) == G.level_begin(2);
+    if (!fold) launch_fas_save(d, G.nonleaf_begin(l - 1), G.ghost_begin(l - 1) - G.nonleaf_begin(l - 1), A.X, A.RHS, A.X0, A.coeff_ch, st);
+    for (int r = 0; r < A.mu; ++r) enqueue_mu_step(G, l - 1, A, st, fold && r == 0);
     launch_prolong(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), A.X, A.X0, A.P, st);
     enqueue_gs(G, l, A.level_iters, 1, A.X, A.RHS, st, true);
 }

@@ -129,7 +129,7 @@ struct Solver {
     MuArgs mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) const;
     // pipelined: the x plane is known to be masked to INTERIOR cells (inside the cycle)
     void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined = false) const;
-    void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st) const;
+    void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st, bool fas2 = false) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
     bool use_graph = true;    // false: launch kernel by kernel from the host (profiling)
     bool use_persist = false;  // levels 2-3 in one cooperative kernel per visit

@@ -83,7 +83,7 @@ struct ClPack {
 };
 
 struct ClusterArgs {
-    int coeff_ch, mu, level_iters, coarsest_iters, exact;
+    int coeff_ch, mu, level_iters, coarsest_iters, exact, fas2;
     float om, Rr, P;
     double omega;
     int tile1[8];   // level-1 tiles by octant (root child order)
@@ -139,25 +139,47 @@ struct Blk {
     int bi, bj, bk;
 };
 
+// the three neighbours of block cell Q outside the block: x side, y side, z side
 template <int Q>
-__device__ __forceinline__ float blk_nlap(const Blk& o, const float* xs) {
+__device__ __forceinline__ void blk_outer(const Blk& o, const float* xs, float v[3]) {
     constexpr int di = Q >> 2, dj = (Q >> 1) & 1, dk = Q & 1;
-    // neighbours outside the block: the cell of opposite parity along the axis, one block over
+    // the cell of opposite parity along the axis, one block over
     const int b = (o.bi + 1) * 240 + (o.bj + 1) * 24 + (o.bk + 1);
-    const float xmx = di ? o.x[Q - 4] : xs[(Q | 4) * kPar + b - 240];
-    const float xpx = di ? xs[(Q & 3) * kPar + b + 240] : o.x[Q + 4];
-    const float xmy = dj ? o.x[Q - 2] : xs[(Q | 2) * kPar + b - 24];
-    const float xpy = dj ? xs[(Q & 5) * kPar + b + 24] : o.x[Q + 2];
-    const float xmz = dk ? o.x[Q - 1] : xs[(Q | 1) * kPar + b - 1];
-    const float xpz = dk ? xs[(Q & 6) * kPar + b + 1] : o.x[Q + 1];
+    v[0] = di ? xs[(Q & 3) * kPar + b + 240] : xs[(Q | 4) * kPar + b - 240];
+    v[1] = dj ? xs[(Q & 5) * kPar + b + 24] : xs[(Q | 2) * kPar + b - 24];
+    v[2] = dk ? xs[(Q & 6) * kPar + b + 1] : xs[(Q | 1) * kPar + b - 1];
+}
+template <int Q>
+__device__ __forceinline__ float blk_nlap_v(const Blk& o, const float v[3]) {
+    constexpr int di = Q >> 2, dj = (Q >> 1) & 1, dk = Q & 1;
+    const float xmx = di ? o.x[Q - 4] : v[0];
+    const float xpx = di ? v[0] : o.x[Q + 4];
+    const float xmy = dj ? o.x[Q - 2] : v[1];
+    const float xpy = dj ? v[1] : o.x[Q + 2];
+    const float xmz = dk ? o.x[Q - 1] : v[2];
+    const float xpz = dk ? v[2] : o.x[Q + 1];
     return nlap(o.d[Q], o.x[Q], o.cx[4 * di + 2 * dj + dk], xmx, o.cx[4 * (di + 1) + 2 * dj + dk], xpx, o.cy[4 * dj + 2 * di + dk], xmy,
                 o.cy[4 * (dj + 1) + 2 * di + dk], xpy, o.cz[4 * dk + 2 * di + dj], xmz, o.cz[4 * (dk + 1) + 2 * di + dj], xpz);
 }
+template <int Q>
+__device__ __forceinline__ float blk_nlap(const Blk& o, const float* xs) {
+    float v[3];
+    blk_outer<Q>(o, xs, v);
+    return blk_nlap_v<Q>(o, v);
+}
+
+// 32-bit shared::cluster address of `p` (this CTA's shared memory) in CTA `rank`
+__device__ __forceinline__ unsigned peer_addr(const void* p, int rank) {
+    unsigned a;
+    asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"((unsigned)__cvta_generic_to_shared(p)), "r"(rank));
+    return a;
+}
+__device__ __forceinline__ void st_peer(unsigned a, float v) { asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
 
 // Neighbouring octants' halos (octant CTAs only).
 struct Peers {
     int oi, oj, ok;
-    float* rx[3];  // x of the neighbouring octant along x, y, z
+    unsigned rx[3];  // x of the neighbouring octant along x, y, z (shared::cluster addresses)
 };
 
 // store cell Q of the block into shared memory and, for an octant CTA on an octant face, into the neighbour's halo
@@ -168,9 +190,9 @@ __device__ __forceinline__ void blk_publish(const Blk& o, float* xs, const Peers
     const float v = o.x[Q];
     xs[Q * kPar + (o.bi + 1) * 240 + (o.bj + 1) * 24 + (o.bk + 1)] = v;
     if (kRemote) {
-        if (I == (pr.oi ? 0 : 15)) pr.rx[0][xo(pr.oi ? 16 : -1, J, K)] = v;
-        if (J == (pr.oj ? 0 : 15)) pr.rx[1][xo(I, pr.oj ? 16 : -1, K)] = v;
-        if (K == (pr.ok ? 0 : 15)) pr.rx[2][xo(I, J, pr.ok ? 16 : -1)] = v;
+        if (I == (pr.oi ? 0 : 15)) st_peer(pr.rx[0] + 4 * xo(pr.oi ? 16 : -1, J, K), v);
+        if (J == (pr.oj ? 0 : 15)) st_peer(pr.rx[1] + 4 * xo(I, pr.oj ? 16 : -1, K), v);
+        if (K == (pr.ok ? 0 : 15)) st_peer(pr.rx[2] + 4 * xo(I, J, pr.ok ? 16 : -1), v);
     }
 }
 template <bool kRemote>
@@ -185,26 +207,35 @@ __device__ __forceinline__ void blk_publish_all(const Blk& o, float* xs, const P
     blk_publish<7, kRemote>(o, xs, pr);
 }
 
-template <int Q, bool kRemote>
-__device__ __forceinline__ void blk_gs_cell(Blk& o, float* xs, const double* yd, const Peers& pr, const ClusterArgs& A) {
-    const float ax = blk_nlap<Q>(o, xs);
-    o.x[Q] = gs_update(o.x[Q], o.b[Q], ax, o.d[Q], yd[Q * kClThreads + threadIdx.x], (o.in >> Q) & 1u, A);
-    blk_publish<Q, kRemote>(o, xs, pr);
+// one colour of the block, cells Q0..Q3 (the colour of cell q is (di + dj + dk) & 1).  The
+// four cells are not neighbours of one another, so every neighbour load comes first, then
+// the four updates, then the stores: the updates overlap instead of each waiting on the
+// previous cell's shared-memory store.
+template <int Q0, int Q1, int Q2, int Q3, bool kRemote>
+__device__ __forceinline__ void blk_gs_colour(Blk& o, float* xs, const double* yd, const Peers& pr, const ClusterArgs& A) {
+    float v0[3], v1[3], v2[3], v3[3];
+    blk_outer<Q0>(o, xs, v0);
+    blk_outer<Q1>(o, xs, v1);
+    blk_outer<Q2>(o, xs, v2);
+    blk_outer<Q3>(o, xs, v3);
+    const double y0 = yd[Q0 * kClThreads + threadIdx.x], y1 = yd[Q1 * kClThreads + threadIdx.x];
+    const double y2 = yd[Q2 * kClThreads + threadIdx.x], y3 = yd[Q3 * kClThreads + threadIdx.x];
+    const float a0 = blk_nlap_v<Q0>(o, v0), a1 = blk_nlap_v<Q1>(o, v1), a2 = blk_nlap_v<Q2>(o, v2), a3 = blk_nlap_v<Q3>(o, v3);
+    o.x[Q0] = gs_update(o.x[Q0], o.b[Q0], a0, o.d[Q0], y0, (o.in >> Q0) & 1u, A);
+    o.x[Q1] = gs_update(o.x[Q1], o.b[Q1], a1, o.d[Q1], y1, (o.in >> Q1) & 1u, A);
+    o.x[Q2] = gs_update(o.x[Q2], o.b[Q2], a2, o.d[Q2], y2, (o.in >> Q2) & 1u, A);
+    o.x[Q3] = gs_update(o.x[Q3], o.b[Q3], a3, o.d[Q3], y3, (o.in >> Q3) & 1u, A);
+    blk_publish<Q0, kRemote>(o, xs, pr);
+    blk_publish<Q1, kRemote>(o, xs, pr);
+    blk_publish<Q2, kRemote>(o, xs, pr);
+    blk_publish<Q3, kRemote>(o, xs, pr);
 }
-// one colour of the block; the colour of cell q is (di + dj + dk) & 1
 template <bool kRemote>
 __device__ __forceinline__ void blk_gs_pass(Blk& o, float* xs, const double* yd, const Peers& pr, int color, const ClusterArgs& A) {
-    if (color == 0) {
-        blk_gs_cell<0, kRemote>(o, xs, yd, pr, A);
-        blk_gs_cell<3, kRemote>(o, xs, yd, pr, A);
-        blk_gs_cell<5, kRemote>(o, xs, yd, pr, A);
-        blk_gs_cell<6, kRemote>(o, xs, yd, pr, A);
-    } else {
-        blk_gs_cell<1, kRemote>(o, xs, yd, pr, A);
-        blk_gs_cell<2, kRemote>(o, xs, yd, pr, A);
-        blk_gs_cell<4, kRemote>(o, xs, yd, pr, A);
-        blk_gs_cell<7, kRemote>(o, xs, yd, pr, A);
-    }
+    if (color == 0)
+        blk_gs_colour<0, 3, 5, 6, kRemote>(o, xs, yd, pr, A);
+    else
+        blk_gs_colour<1, 2, 4, 7, kRemote>(o, xs, yd, pr, A);
 }
 // ResidualAndRestrictAMG128Kernel (src/AMGSolver.cu:896-960) of the block into its parent cell:
 // rhs = R * sum of the 8 residuals, x = mean of the 8 x (0 unless the parent is INTERIOR)
@@ -361,7 +392,7 @@ __global__ void __launch_bounds__(kClThreads, 1)
 
     if (r < kOct) {
         // ============================ octant CTA ============================
-        for (int a = 0; a < 3; ++a) pr.rx[a] = cluster.map_shared_rank(sm.x, r ^ (4 >> a));
+        for (int a = 0; a < 3; ++a) pr.rx[a] = peer_addr(sm.x, r ^ (4 >> a));
         const int Gi = 16 * pr.oi + 2 * o.bi, Gj = 16 * pr.oj + 2 * o.bj, Gk = 16 * pr.ok + 2 * o.bk;
         float xin[8];
 #pragma unroll
@@ -397,6 +428,30 @@ __global__ void __launch_bounds__(kClThreads, 1)
                 if (fj) xs[xo(2 * o.bi + u, 2 * o.bj + sj, 2 * o.bk + v)] = ((m >> (13 + 2 * u + v)) & 1u) ? hv[4 + 2 * u + v] : 0.0f;
                 if (fk) xs[xo(2 * o.bi + u, 2 * o.bj + v, 2 * o.bk + sk)] = ((m >> (17 + 2 * u + v)) & 1u) ? hv[8 + 2 * u + v] : 0.0f;
             }
+        if (A.fas2) {
+            // ---- FASSaveSolutionAndUpdateSource on level 2: rhs += A x, saved x = x on INTERIOR cells ----
+            __syncthreads();
+            float ax[8];
+            ax[0] = blk_nlap<0>(o, xs);
+            ax[1] = blk_nlap<1>(o, xs);
+            ax[2] = blk_nlap<2>(o, xs);
+            ax[3] = blk_nlap<3>(o, xs);
+            ax[4] = blk_nlap<4>(o, xs);
+            ax[5] = blk_nlap<5>(o, xs);
+            ax[6] = blk_nlap<6>(o, xs);
+            ax[7] = blk_nlap<7>(o, xs);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const long long off = l2_off(A, Gi + (q >> 2), Gj + ((q >> 1) & 1), Gk + (q & 1));
+                if ((o.in >> q) & 1u) {
+                    o.b[q] = __fadd_rn(o.b[q], ax[q]);
+                    X0[off] = o.x[q];
+                } else {
+                    o.b[q] = 0.0f;
+                }
+                RHS[off] = o.b[q];
+            }
+        }
         // every CTA has initialised its halos before any peer writes into them
         cluster.sync();
 
@@ -434,7 +489,7 @@ __global__ void __launch_bounds__(kClThreads, 1)
         for (int q = 0; q < 8; ++q) X[l2_off(A, Gi + (q >> 2), Gj + ((q >> 1) & 1), Gk + (q & 1))] = o.x[q];
     } else {
         // ============================ coarse CTA ============================
-        pr.rx[0] = pr.rx[1] = pr.rx[2] = nullptr;
+        pr.rx[0] = pr.rx[1] = pr.rx[2] = 0u;
         const bool in0 = (m >> 8) & 1u;
         const float d0 = pk.f[44][t], c0mx = pk.f[45][t], c0px = pk.f[46][t], c0my = pk.f[47][t], c0py = pk.f[48][t], c0mz = pk.f[49][t],
                     c0pz = pk.f[50][t];
@@ -552,7 +607,7 @@ __global__ void __launch_bounds__(kClThreads, 1)
 size_t cluster_pack_bytes() { return sizeof(ClPack) * kClCtas; }
 
 static void fill_args(ClusterArgs& A, const int* tile1, const int* tile2, int coeff_ch, int mu, int level_iters, int coarsest_iters,
-                      double omega, float Rr, float P) {
+                      double omega, float Rr, float P, bool fas2) {
     for (int i = 0; i < 8; ++i) A.tile1[i] = tile1[i];
     for (int i = 0; i < 64; ++i) A.tile2[i] = tile2[i];
     A.coeff_ch = coeff_ch;
@@ -564,20 +619,21 @@ static void fill_args(ClusterArgs& A, const int* tile1, const int* tile2, int co
     A.omega = omega;
     A.Rr = Rr;
     A.P = P;
+    A.fas2 = fas2 ? 1 : 0;
 }
 
 void launch_cluster_pack(const DevGrid& g, const int* tile1, const int* tile2, int coeff_ch, void* pack, cudaStream_t st) {
     ClusterArgs A;
-    fill_args(A, tile1, tile2, coeff_ch, 0, 0, 0, 1.0, 1.0f, 1.0f);
+    fill_args(A, tile1, tile2, coeff_ch, 0, 0, 0, 1.0, 1.0f, 1.0f, false);
     note_kernel_launch();
     k_cluster_pack<<<kClCtas, kClThreads, 0, st>>>(g, A, reinterpret_cast<ClPack*>(pack));
 }
 
 cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* tile2, const void* pack, float* X, float* RHS, float* X0,
-                                int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float Rr, float P,
+                                int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float Rr, float P, bool fas2,
                                 cudaStream_t st) {
     ClusterArgs A;
-    fill_args(A, tile1, tile2, coeff_ch, mu, level_iters, coarsest_iters, omega, Rr, P);
+    fill_args(A, tile1, tile2, coeff_ch, mu, level_iters, coarsest_iters, omega, Rr, P, fas2);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kClCtas);
     cfg.blockDim = dim3(kClThreads);

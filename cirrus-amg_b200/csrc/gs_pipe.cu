@@ -29,9 +29,18 @@ struct PipeStage {
     float hx[384];   // halo x of the six faces, [axis][side][a][b]
     unsigned ty[128];
 };
+// The snapshot: masked x of the tile with its one-cell halo, split into four planes by
+// k mod 4 (k = 4h + u: u the plane, h = -1..2 the slot), rows j of 4 slots, layers i of
+// 42 floats, planes of 448 floats.  A warp's threads own (i0..i0+1, j 0..7, h 0..1) and
+// touch one plane per lane at a time: the offsets 4j + h and 42 + 4j + h fill the 32
+// banks once each, and the plane stride is a multiple of 32, so the stores of its own
+// cells and the i/j neighbour loads of a colour pass are free of bank conflicts.
+constexpr int kSxI = 42, kSxJ = 4, kSxP = 448;
+__device__ __forceinline__ int sxp(int i, int j, int k) { return ((k + 4) & 3) * kSxP + (i + 1) * kSxI + (j + 1) * kSxJ + ((k + 4) >> 2); }
+
 struct PipeSmem {
     PipeStage st[2];
-    float x[1000];   // the snapshot: masked x with its one-cell halo, index sx()
+    float x[4 * kSxP];
 };
 constexpr size_t kPipeSmem = sizeof(PipeSmem);
 
@@ -101,14 +110,15 @@ __device__ __forceinline__ void process(const PipeStage& S, float* SX, const Dev
     xm.y = ((tyw >> 8) & 0xffu) == dInterior ? xr.y : 0.0f;
     xm.z = ((tyw >> 16) & 0xffu) == dInterior ? xr.z : 0.0f;
     xm.w = ((tyw >> 24) & 0xffu) == dInterior ? xr.w : 0.0f;
-    const int s0 = sx(Q.i, Q.j, Q.k0);
-    SX[s0 + 0] = xm.x;
-    SX[s0 + 1] = xm.y;
-    SX[s0 + 2] = xm.z;
-    SX[s0 + 3] = xm.w;
+    // own cells (i, j, k0 + u): plane u, slot h + 1
+    const int s0 = (Q.i + 1) * kSxI + (Q.j + 1) * kSxJ + (Q.k0 >> 2) + 1;
+    SX[s0] = xm.x;
+    SX[s0 + kSxP] = xm.y;
+    SX[s0 + 2 * kSxP] = xm.z;
+    SX[s0 + 3 * kSxP] = xm.w;
     const int side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
     const int e = side ? 7 : 0, hxl = side ? 8 : -1;
-    const int fx[3] = {sx(hxl, fa, fb), sx(fa, hxl, fb), sx(fa, fb, hxl)};
+    const int fx[3] = {sxp(hxl, fa, fb), sxp(fa, hxl, fb), sxp(fa, fb, hxl)};
 #pragma unroll
     for (int r = 0; r < 3; ++r)
         if (!(d[r] & dGhost)) SX[fx[r]] = S.hx[r * 128 + q];
@@ -127,9 +137,9 @@ __device__ __forceinline__ void process(const PipeStage& S, float* SX, const Dev
 #pragma unroll
                 for (int dj = 0; dj < 2; ++dj)
 #pragma unroll
-                    for (int dk = 0; dk < 2; ++dk) avg = __fadd_rn(avg, SX[sx(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)]);
+                    for (int dk = 0; dk < 2; ++dk) avg = __fadd_rn(avg, SX[sxp(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)]);
             avg = __fmul_rn(avg, 0.125f);
-            SX[fx[r]] = __fmaf_rn(0.5f, __fsub_rn(S.hx[r * 128 + q], avg), SX[sx(cl[0], cl[1], cl[2])]);
+            SX[fx[r]] = __fmaf_rn(0.5f, __fsub_rn(S.hx[r * 128 + q], avg), SX[sxp(cl[0], cl[1], cl[2])]);
         }
     }
     __syncthreads();
@@ -138,26 +148,35 @@ __device__ __forceinline__ void process(const PipeStage& S, float* SX, const Dev
     const float4 a0 = *reinterpret_cast<const float4*>(&S.c0[4 * q]);
     const float4 a1 = *reinterpret_cast<const float4*>(&S.c1[4 * q]);
     const float4 a2 = *reinterpret_cast<const float4*>(&S.c2[4 * q]);
+    // +x faces: the -x faces of the cells at i + 1 (thread q + 16; row i = 7: from the +x
+    // neighbour, stored after the tile's faces in the same order)
+    const float4 px = *reinterpret_cast<const float4*>(&S.c0[4 * (q + 16)]);
+    // +y faces: the -y faces at j + 1 (thread q + 2), or from the +y neighbour on row j = 7
+    const float4 py = Q.j < 7 ? *reinterpret_cast<const float4*>(&S.c1[4 * (q + 2)])
+                              : *reinterpret_cast<const float4*>(&S.c1h[Q.i * 8 + Q.k0]);
+    // +z face of the last cell of the quad: the next quad's first -z face, or the +z neighbour's
+    const float pz3 = Q.k0 == 0 ? S.c2[4 * (q + 1)] : S.c2h[Q.i * 8 + Q.j];
     float4 out = xr;
     const int p = (Q.i + Q.j + Q.k0 + A.color) & 1;  // own cells of this colour: u = p, p + 2
 #pragma unroll
     for (int hh = 0; hh < 2; ++hh) {
         const int u = p + 2 * hh;
-        const int k = Q.k0 + u;
         const float dd = f4get(dg, u);
         float ax = 0.0f;
         if (dd != 0.0f) {
-            // negativeLap (src/AMGSolver.cu:346-382): diag*x, then -x,+x,-y,+y,-z,+z
-            const int c = sx(Q.i, Q.j, k);
-            const float cpy = Q.j < 7 ? S.c1[Q.i * 64 + (Q.j + 1) * 8 + k] : S.c1h[Q.i * 8 + k];
-            const float cpz = k < 7 ? (u < 3 ? f4get(a2, u + 1) : S.c2[Q.i * 64 + Q.j * 8 + k + 1]) : S.c2h[Q.i * 8 + Q.j];
+            // negativeLap (src/AMGSolver.cu:346-382): diag*x, then -x,+x,-y,+y,-z,+z; the k
+            // neighbours inside the quad are the thread's own cells of the other colour
+            const int c = s0 + u * kSxP;
+            const float xmz = u > 0 ? f4get(xm, u - 1) : SX[s0 - 1 + 3 * kSxP];
+            const float xpz = u < 3 ? f4get(xm, u + 1) : SX[s0 + 1];
+            const float cpz = u < 3 ? f4get(a2, u + 1) : pz3;
             ax = __fmul_rn(f4get(xm, u), dd);
-            ax = __fmaf_rn(f4get(a0, u), SX[c - 100], ax);
-            ax = __fmaf_rn(S.c0[(Q.i + 1) * 64 + Q.j * 8 + k], SX[c + 100], ax);
-            ax = __fmaf_rn(f4get(a1, u), SX[c - 10], ax);
-            ax = __fmaf_rn(cpy, SX[c + 10], ax);
-            ax = __fmaf_rn(f4get(a2, u), SX[c - 1], ax);
-            ax = __fmaf_rn(cpz, SX[c + 1], ax);
+            ax = __fmaf_rn(f4get(a0, u), SX[c - kSxI], ax);
+            ax = __fmaf_rn(f4get(px, u), SX[c + kSxI], ax);
+            ax = __fmaf_rn(f4get(a1, u), SX[c - kSxJ], ax);
+            ax = __fmaf_rn(f4get(py, u), SX[c + kSxJ], ax);
+            ax = __fmaf_rn(f4get(a2, u), xmz, ax);
+            ax = __fmaf_rn(cpz, xpz, ax);
         }
         const bool in = ((tyw >> (8 * u)) & 0xffu) & dInterior;
         const float delta = in ? div_exact(__fsub_rn(f4get(b, u), ax), dd) : 0.0f;
@@ -166,7 +185,6 @@ __device__ __forceinline__ void process(const PipeStage& S, float* SX, const Dev
     }
     st4(X + Q.base, out);
 }
-
 __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const float* B, PipeArgs A) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
     PipeSmem& sm = *reinterpret_cast<PipeSmem*>(pipe_smem);

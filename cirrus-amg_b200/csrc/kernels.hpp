@@ -59,10 +59,11 @@ size_t coarse_step_smem_bytes();
 // tile1: the 8 level-1 tiles in root child order; tile2: the 64 level-2 tiles
 // indexed by (i >> 3) * 16 + (j >> 3) * 4 + (k >> 3) of their cells in the 32^3
 // grid.  pack: cluster_pack_bytes() of device memory filled by launch_cluster_pack
-// from the current coefficients and cell types (once per solve).
+// from the current coefficients and cell types (once per solve).  fas2: do
+// FASSaveSolutionAndUpdateSource on level 2 first (all 64 tiles NONLEAF).
 cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* tile2, const void* pack, float* X, float* RHS, float* X0,
                                 int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float R_restrict, float P,
-                                cudaStream_t st);
+                                bool fas2, cudaStream_t st);
 void launch_cluster_pack(const DevGrid& g, const int* tile1, const int* tile2, int coeff_ch, void* pack, cudaStream_t st);
 size_t cluster_pack_bytes();
 bool cluster_step_supported();  // the current device can co-schedule the 9-CTA cluster

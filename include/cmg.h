@@ -228,6 +228,10 @@ int cmg_amg_solve_host(cmg_amg_solver* s, cmg_grid* g, const float* b_host, floa
                        int sync_stride, int is_pure_neumann, int* iters, double* rel_res);
 /* GaussSeidelAMG (src/AMGSolver.cu:887) on one level */
 int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
+/* The same sweeps as the multigrid cycle runs them (the pipelined persistent kernel):
+ * x must hold 0 on every cell that is not INTERIOR, which the cycle keeps true and
+ * GaussSeidelAMG then preserves.  Results equal cmg_amg_gauss_seidel's on such x. */
+int cmg_amg_gauss_seidel_masked(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
 /* AMGSolver::FASMuCycle (src/AMGSolver.cu:1279) */
 int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters);
 /* device time of the last cmg_amg_solve, milliseconds (CUDA events) */

@@ -360,6 +360,25 @@ def test_pipelined_smoother_matches_per_tile_launches(grid):
     assert np.array_equal(res[0][2], res[1][2])
 
 
+def test_masked_gauss_seidel_entry_matches_plain_sweeps():
+    """cmg_amg_gauss_seidel_masked (the cycle's pipelined kernel) gives the same x as
+    cmg_amg_gauss_seidel on every level when x is 0 on the cells that are not INTERIOR."""
+    G, _, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5), with_oracle=False)
+    rng = np.random.default_rng(23)
+    n = G.num_tiles
+    interior = G.download_cell_types() == cmg.INTERIOR
+    x = np.where(interior, rng.standard_normal((n, 512)), 0.0).astype(np.float32)
+    G.upload(3, rng.standard_normal((n, 512)).astype(np.float32))
+    for level in range(G.max_level + 1):
+        for order in (0, 1):
+            out = []
+            for masked in (False, True):
+                G.upload(4, x)
+                (solver.gauss_seidel_masked if masked else solver.gauss_seidel)(G, 2, order, level, 4, 3)
+                out.append(G.download(4))
+            assert np.array_equal(out[0], out[1]), (level, order)
+
+
 def _geo_pair(case_id, prm, kind, seed=3):
     from workloads import uniform_rhs
 
