@@ -19,6 +19,15 @@ overwrites, is inside the timed region); `e2e` is the same solve through the
 C ABI with host buffers (b copied in from pinned memory, x copied out).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload sphere|uniform64|batched64]
+
+--workload uniform64: the uniform 64^3 grid (level 3), all cells INTERIOR,
+Dirichlet walls, rhs N(0,1) per cell (numpy default_rng(0)) minus its mean.
+--workload batched64: 64 independent octrees (seed 2): finest level 4 or 5 within
+0.05 of the surfaces of 1-3 solid spheres (radius U(0.05, 0.15), centres
+U(0.2, 0.8)^3), level 3 elsewhere, 2:1 graded, each with its own Fourier-
+divergence rhs; a step solves all 64 through one cmg_amg_solve_batch call, 16
+streams; the metric is solves per second, with p50/p99 per-solve device time.
 
 N > 1 runs N independent replicas (the path does not shard).
 """
@@ -149,19 +158,93 @@ def per_solve_ms(total_ms, steps, world):
     return total_ms / (steps * world)
 
 
-def build_workload(cmg):
+WORKLOADS = {
+    "sphere": WORKLOAD,
+    "uniform64": "uniform 64^3 grid (h0=1/8, level 3), all cells INTERIOR, Dirichlet walls, rhs N(0,1) seed 0 minus mean",
+    "batched64": "64 adaptive octrees (seed 2): finest level 4 or 5 within 0.05 of 1-3 solid spheres r~U(0.05,0.15), "
+                 "centres U(0.2,0.8)^3, level 3 elsewhere; Fourier-divergence rhs per octree",
+}
+BATCH_STREAMS = 16
+
+
+def instance_specs(name):
+    """The octrees of a workload: refinement case and parameters, cut-cell spheres, rhs."""
+    if name == "sphere":
+        return [dict(case="shell", params=SHELL, spheres=SPHERES, rhs=("fourier", 1))]
+    if name == "uniform64":
+        return [dict(case="uniform", params=[3, 3], spheres=None, rhs=("normal", 0))]
+    rng = np.random.default_rng(2)
+    specs = []
+    for i in range(64):
+        finest = int(rng.integers(4, 6))
+        ns = int(rng.integers(1, 4))
+        sph = [tuple(float(v) for v in rng.uniform(0.2, 0.8, 3)) + (float(rng.uniform(0.05, 0.15)),) for _ in range(ns)]
+        params = [3, finest, 0.05, ns] + [v for sp in sph for v in sp]
+        specs.append(dict(case="multi", params=params, spheres=sph, rhs=("fourier", 100 + i)))
+    return specs
+
+
+def normal_rhs(ty, seed, leaf):
+    """N(0,1) per LEAF cell in tile order, mean removed, 0 elsewhere."""
+    rng = np.random.default_rng(seed)
+    m = ty == leaf
+    n = int(m.sum())
+    v = rng.standard_normal(n * 512).astype(np.float32)
+    v -= v.mean(dtype=np.float64).astype(np.float32)
+    b = np.zeros((ty.size, 512), np.float32)
+    b[m] = v.reshape(n, 512)
+    return b
+
+
+def build_grid(cmg, spec):
+    """One octree on the device with its operator and rhs (b in channel 1 and BSAVE)."""
+    case = {"shell": cmg.CASE_SHELL, "uniform": cmg.CASE_UNIFORM, "multi": cmg.CASE_MULTI_SPHERE}[spec["case"]]
     G = cmg.HADeviceGrid(0.125, 10, 16)
     G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
     G.rebuild()
-    G.refine_case(cmg.CASE_SHELL, SHELL)
+    G.refine_case(case, spec["params"])
     G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
-    G.cutcell_sphere_coeffs(COEFF, SPHERES, 0.5)
-    k, amp, ph = fourier_modes(1)
-    G.face_velocity_fourier(U, k, amp, ph)
-    G.divergence(U, COEFF, 1)
+    if spec["spheres"]:
+        G.cutcell_sphere_coeffs(COEFF, spec["spheres"], 0.5)
+    else:
+        cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0).prepareTypesAndCoeffs(G)
+    kind, seed = spec["rhs"]
+    if kind == "fourier":
+        k, amp, ph = fourier_modes(seed)
+        G.face_velocity_fourier(U, k, amp, ph)
+        G.divergence(U, COEFF, 1)
+    else:
+        G.upload(1, normal_rhs(G.tiles()[2], seed, cmg.LEAF))
     G.copy(1, BSAVE)
     G.synchronize()
     return G
+
+
+def build_oracle_grid(O, spec):
+    """The same octree, operator and rhs (channel 1) in the oracle."""
+    case = {"shell": O.CASE_SHELL, "uniform": O.CASE_UNIFORM, "multi": O.CASE_MULTI_SPHERE}[spec["case"]]
+    g = O.Grid(0.125, 10)
+    g.set_tile(0, 0, 0, 0, O.LEAF)
+    g.rebuild()
+    g.refine_case(case, spec["params"])
+    g.alloc(16)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    if spec["spheres"]:
+        g.cutcell_sphere_coeffs(COEFF, spec["spheres"], 0.5)
+    else:
+        g.coarsen_types_and_coeffs(COEFF, 0.5)
+    kind, seed = spec["rhs"]
+    if kind == "fourier":
+        k, amp, ph = fourier_modes(seed)
+        g.face_velocity_fourier(U, k, amp, ph)
+        g.divergence(U, COEFF, 1)
+    else:
+        g.channel(1)[:] = normal_rhs(g.tiles()[2], seed, O.LEAF)
+    return g
+
+
+def build_workload(cmg, name="sphere"):
+    return build_grid(cmg, instance_specs(name)[0])
 
 
 def make_solver(cmg):
@@ -178,15 +261,16 @@ def solve_args():
     return (False, SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
 
 
-def cpu_baseline_fp64(G, cmg):
+def cpu_baseline_fp64(G, cmg, spec, what="the workload"):
     """FP64 Jacobi-preconditioned CG (the algorithm of Eigen's default
     ConjugateGradient) on the same operator assembled into CSR, all host cores."""
     from oracle import oracle as O
 
+    case = {"shell": O.CASE_SHELL, "uniform": O.CASE_UNIFORM, "multi": O.CASE_MULTI_SPHERE}[spec["case"]]
     g = O.Grid(0.125, 10)
     g.set_tile(0, 0, 0, 0, O.LEAF)
     g.rebuild()
-    g.refine_case(O.CASE_SHELL, SHELL)
+    g.refine_case(case, spec["params"])
     g.alloc(16)
     lv, ijk, ty = G.tiles()
     olv, oijk, oty = g.tiles()
@@ -202,8 +286,55 @@ def cpu_baseline_fp64(G, cmg):
     x, its, rel = O.csr_solve(rp, ci, va, bb, 1e-6, 4000, 0)
     dt = time.perf_counter() - t0
     return {"value": dt * 1e3, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"one full FP64 Jacobi-CG solve of the workload to 1e-6 ({len(bb)} unknowns, {its} iterations, "
+            "sample": f"one full FP64 Jacobi-CG solve of {what} to 1e-6 ({len(bb)} unknowns, {its} iterations, "
                       f"rel {rel:.2e}); OpenMP over all host threads"}
+
+
+def roofline_gs(G, S, cmg, torch, dev):
+    """Roofline of the dominant kernel: the pipelined red-black GS launch (k_gs_pipe) on the
+    finest level, as the cycle runs it (x starts at 0, so it is 0 on cells that are not
+    INTERIOR), CUDA events on the grid's stream (the default stream here); L2 flushed (a
+    256 MB write) before every measured pair of launches."""
+    ntiles, L, nleaf = G.info()
+    lv, ijk, ty = G.tiles()
+    active = int(((lv == L) & ((ty == cmg.LEAF) | (ty == cmg.NONLEAF))).sum())
+    cells = active * 512
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    G.copy(BSAVE, 1)
+    G.fill(4, 0.0)
+    reps, gs_ms = 20, []
+    torch.cuda.nvtx.range_push("roofline")
+    for r in range(reps + 2):
+        flush.fill_(float(r))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        S.gauss_seidel_masked(G, 1, 0, L, 4, 1)
+        a1.record()
+        torch.cuda.synchronize()
+        if r >= 2:
+            gs_ms.append(a0.elapsed_time(a1) / 2.0)
+    torch.cuda.nvtx.range_pop()
+    gs_ms.sort()
+    launch_ms = gs_ms[len(gs_ms) // 2]
+    peak, peak_kind = measured_peaks()
+    alg_bytes = BYTES_PER_CELL_GS * cells
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
+    return launch_ms, achieved, alg_bytes, L, active, cells, peak, peak_kind, profile_traffic_per_cell()
+
+
+def roofline_entry(launch_ms, achieved, alg_bytes, L, active, cells, peak, peak_kind, tpc):
+    return {
+        "kernel": f"k_gs_pipe (pipelined red-black Gauss-Seidel pass, level {L}, {active} tiles)",
+        "bound": "hbm",
+        "achieved": round(achieved, 1),
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 4),
+        "peak_kind": peak_kind,
+        "algorithmic_bytes_per_launch": alg_bytes,
+        "launch_ms": round(launch_ms, 5),
+        "traffic": (round(tpc * cells) if tpc else None),
+    }
 
 
 def run_ours(args, rank, world, local_rank):
@@ -213,7 +344,8 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    G = build_workload(cmg)
+    spec = instance_specs(args.workload)[0]
+    G = build_grid(cmg, spec)
     S = make_solver(cmg)
     ntiles, maxl, nleaf = G.info()
     lv, ijk, ty = G.tiles()
@@ -280,33 +412,7 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = f0.elapsed_time(f1) / args.steps
     e2e_wall_ms = (time.perf_counter() - t_wall) * 1e3 / args.steps
 
-    # roofline of the dominant kernel: the pipelined red-black GS launch (k_gs_pipe) on the
-    # finest level, as the cycle runs it (x starts at 0, so it is 0 on cells that are not
-    # INTERIOR); L2 flushed (a 256 MB write) before every measured pair of launches
-    L = maxl
-    active = int(((lv == L) & ((ty == cmg.LEAF) | (ty == cmg.NONLEAF))).sum())
-    cells = active * 512
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    G.copy(BSAVE, 1)
-    G.fill(4, 0.0)
-    reps, gs_ms = 20, []
-    torch.cuda.nvtx.range_push("roofline")
-    for r in range(reps + 2):
-        flush.fill_(float(r))
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record()
-        S.gauss_seidel_masked(G, 1, 0, L, 4, 1)
-        a1.record()
-        torch.cuda.synchronize()
-        if r >= 2:
-            gs_ms.append(a0.elapsed_time(a1) / 2.0)
-    torch.cuda.nvtx.range_pop()
-    gs_ms.sort()
-    launch_ms = gs_ms[len(gs_ms) // 2]
-    peak, peak_kind = measured_peaks()
-    alg_bytes = BYTES_PER_CELL_GS * cells
-    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
-    tpc = profile_traffic_per_cell()
+    launch_ms, achieved, alg_bytes, L, active, cells, peak, peak_kind, tpc = roofline_gs(G, S, cmg, torch, dev)
 
     result = None
     if rank == 0:
@@ -325,7 +431,7 @@ def run_ours(args, rank, world, local_rank):
             "dtype": "f32",
             "data": "synthetic",
             "config": {
-                "workload": WORKLOAD,
+                "workload": WORKLOADS[args.workload],
                 "method": "plain FP32 FAS mu-cycle (mu=2) MG-PCG, FP64 dots",
                 "tiles": ntiles, "leaf_tiles": nleaf, "leaf_cells": leaf_cells, "interior_cells": interior, "max_level": maxl,
                 "pcg_iters": iters[-1], "rel_residual_recurrence": rels[-1], "rel_residual_true_fp32_apply": true_rel,
@@ -336,63 +442,165 @@ def run_ours(args, rank, world, local_rank):
             },
             "e2e": {"value": round(e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": count * 4, "d2h_bytes_per_step": count * 4},
             "gpu_launches": int(launches),
-            "roofline": {
-                "kernel": f"k_gs_pipe (pipelined red-black Gauss-Seidel pass, level {L}, {active} tiles)",
-                "bound": "hbm",
-                "achieved": round(achieved, 1),
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": round(achieved / peak, 4),
-                "peak_kind": peak_kind,
-                "algorithmic_bytes_per_launch": alg_bytes,
-                "launch_ms": round(launch_ms, 5),
-                "traffic": (round(tpc * cells) if tpc else None),
-            },
+            "roofline": roofline_entry(launch_ms, achieved, alg_bytes, L, active, cells, peak, peak_kind, tpc),
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline_fp64(G, cmg)
+            result["cpu_baseline"] = cpu_baseline_fp64(G, cmg, spec)
+    return result
+
+
+BATCH_METRIC = "Poisson solves per second to 1e-6 rel. residual, 64 batched adaptive octrees, 1×B200"
+BATCH_UNIT = "solves/s"
+
+
+def run_batched(args, rank, world, local_rank):
+    """64 independent octrees per step, all solved through one cmg_amg_solve_batch call,
+    spread over BATCH_STREAMS streams so the latency-bound solves overlap on the GPU."""
+    import torch
+
+    import cmg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    specs = instance_specs("batched64")
+    grids = [build_grid(cmg, sp) for sp in specs]
+    solvers = [make_solver(cmg) for _ in specs]
+    n = len(grids)
+    infos = [G.info() for G in grids]
+    streams = [torch.cuda.Stream(device=dev) for _ in range(BATCH_STREAMS)]
+    for i, G in enumerate(grids):
+        G.set_stream(streams[i % BATCH_STREAMS].cuda_stream)
+    sargs = (SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
+
+    def one_batch(b_host=None, x_host=None):
+        if b_host is None:
+            for G in grids:
+                G.copy(BSAVE, 1)
+        return cmg.solve_batch(solvers, grids, *sargs, b_host=b_host, x_host=x_host)
+
+    def timed(steps, **kw):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for st in streams:
+            st.wait_event(e0)
+        out = []
+        for _ in range(steps):
+            torch.cuda.nvtx.range_push("batch")
+            out.append(one_batch(**kw))
+            torch.cuda.nvtx.range_pop()
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            torch.cuda.current_stream().wait_event(ev)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for _ in range(max(args.warmup, 1)):
+        one_batch()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    t_ms, out = timed(args.steps)
+    launches = sum(S.last_solve_launches() for S in solvers) * args.steps
+    clocks = sampler.stop()
+    total_ms = replica_time(t_ms, world, dev)
+    per = sorted(m for _, _, ms in out for m in ms)
+    its = [i for it, _, _ in out for i in it]
+    rels = [r for _, rel, _ in out for r in rel]
+
+    # e2e: the same batch through the C ABI with pinned host buffers for b and x
+    b_host = [torch.from_numpy(G.download(BSAVE).reshape(-1)).pin_memory() for G in grids]
+    x_host = [torch.empty_like(b).pin_memory() for b in b_host]
+    hb = dict(b_host=[b.data_ptr() for b in b_host], x_host=[x.data_ptr() for x in x_host])
+    one_batch(**hb)
+    e2e_ms, _ = timed(args.steps, **hb)
+    e2e_ms = replica_time(e2e_ms, world, dev)
+    nbytes = sum(b.numel() * 4 for b in b_host)
+
+    # roofline: k_gs_pipe on the finest level of the largest octree, on the default stream
+    big = max(range(n), key=lambda i: infos[i][0])
+    grids[big].set_stream(0)
+    roof = roofline_gs(grids[big], solvers[big], cmg, torch, dev)
+
+    result = None
+    if rank == 0:
+        value = n * args.steps * world / (total_ms / 1e3)
+        result = {
+            "metric": BATCH_METRIC, "value": round(value, 2), "unit": BATCH_UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": WORKLOADS["batched64"], "method": "plain FP32 FAS mu-cycle (mu=2) MG-PCG, FP64 dots, batched",
+                "instances": n, "streams": BATCH_STREAMS, "tiles": int(sum(i[0] for i in infos)),
+                "leaf_cells": int(sum(i[2] for i in infos)) * 512, "finest_levels": sorted({int(i[1]) for i in infos}),
+                "pcg_iters_mean": round(float(np.mean(its)), 2), "pcg_iters_max": int(max(its)), "rel_residual_max": max(rels),
+                "solve_ms_p50": per[len(per) // 2], "solve_ms_p99": per[min(len(per) - 1, int(0.99 * len(per)))],
+                "l2": f"inputs larger than L2: {16 * sum(i[0] for i in infos) * 2048 / 1e9:.1f} GB of channel planes",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "e2e": {"value": round(n * args.steps * world / (e2e_ms / 1e3), 2), "unit": BATCH_UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes},
+            "gpu_launches": int(launches),
+            "roofline": roofline_entry(*roof),
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline_fp64(grids[0], cmg, specs[0], "octree 0 of the batch")
+            if cb["value"]:
+                cb["sample"] += "; solves/s = 1000 / its ms"
+                cb["value"] = 1000.0 / cb["value"]
+            cb["unit"] = BATCH_UNIT
+            result["cpu_baseline"] = cb
+    for G in grids:
+        G.set_stream(0)
     return result
 
 
 def run_reference(args):
     """The reference's algorithm for this path on the host cores: the oracle's
     restatement of AMGSolver::solve (src/AMGSolver.cu:1399), OpenMP over all
-    host threads, on the same workload."""
+    host threads, on the same workload (for the batch: a sample of its octrees)."""
     from oracle import oracle as O
 
-    g = O.Grid(0.125, 10)
-    g.set_tile(0, 0, 0, 0, O.LEAF)
-    g.rebuild()
-    g.refine_case(O.CASE_SHELL, SHELL)
-    g.alloc(16)
-    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
-    g.cutcell_sphere_coeffs(COEFF, SPHERES, 0.5)
-    k, amp, ph = fourier_modes(1)
-    g.face_velocity_fourier(U, k, amp, ph)
-    g.divergence(U, COEFF, 1)
-    b = g.channel(1).copy()
-    steps = max(1, min(args.steps, 5))
+    specs = instance_specs(args.workload)
+    batched = args.workload == "batched64"
+    sample_specs = specs[:2] if batched else specs[:1]
+    steps = max(1, min(args.steps, 2 if batched else 5))
     warm = min(args.warmup, 1)
     times, it, rel = [], 0, 0.0
-    for s in range(warm + steps):
-        g.channel(1)[:] = b
-        t0 = time.perf_counter()
-        it, rel = g.amg_solve(COEFF, omega=SOLVE["omega"], mu=SOLVE["mu"], max_iters=SOLVE["max_iters"], tol=SOLVE["tol"],
-                              level_iters=SOLVE["level_iters"], coarsest_iters=SOLVE["coarsest_iters"], sync_stride=1)
-        dt = (time.perf_counter() - t0) * 1e3
-        if s >= warm:
-            times.append(dt)
-    v = sum(times) / len(times)
-    sample = (f"{steps} full solves of the workload ({it} PCG iterations, rel {rel:.2e}) by the C restatement of "
-              f"AMGSolver::solve, OpenMP; the reference's own solver is CUDA-only")
+    for sp in sample_specs:
+        g = build_oracle_grid(O, sp)
+        b = g.channel(1).copy()
+        for st in range(warm + steps):
+            g.channel(1)[:] = b
+            t0 = time.perf_counter()
+            it, rel = g.amg_solve(COEFF, omega=SOLVE["omega"], mu=SOLVE["mu"], max_iters=SOLVE["max_iters"], tol=SOLVE["tol"],
+                                  level_iters=SOLVE["level_iters"], coarsest_iters=SOLVE["coarsest_iters"], sync_stride=1)
+            dt = (time.perf_counter() - t0) * 1e3
+            if st >= warm:
+                times.append(dt)
+    ms = sum(times) / len(times)
+    if batched:
+        v, unit, metric, hib = 1000.0 / ms, BATCH_UNIT, BATCH_METRIC, True
+        sample = (f"{steps} solves each of octrees 0 and 1 of the batch by the C restatement of AMGSolver::solve, OpenMP; "
+                  f"solves/s = 1000 / mean ms ({ms:.1f} ms); the reference's own solver is CUDA-only")
+    else:
+        v, unit, metric, hib = ms, UNIT, METRIC, False
+        sample = (f"{steps} full solves of the workload ({it} PCG iterations, rel {rel:.2e}) by the C restatement of "
+                  f"AMGSolver::solve, OpenMP; the reference's own solver is CUDA-only")
     return {
         "impl": "reference",
-        "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warm,
-        "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "method": "reference FAS mu-cycle MG-PCG on host cores"},
-        "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample},
-        "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "metric": metric, "value": round(v, 3), "unit": unit, "n_gpus": 1, "steps": steps, "warmup": warm,
+        "ms_per_step": round(ms, 3), "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": WORKLOADS[args.workload], "method": "reference FAS mu-cycle MG-PCG on host cores"},
+        "cpu_baseline": {"value": round(v, 3), "unit": unit, "cores": os.cpu_count(), "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 3), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
@@ -403,6 +611,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="sphere", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -423,7 +632,7 @@ def main():
 
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    res = run_ours(args, rank, world, local_rank)
+    res = (run_batched if args.workload == "batched64" else run_ours)(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
 

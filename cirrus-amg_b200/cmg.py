@@ -46,7 +46,7 @@ EXPORTS = [
     "cmg_amg_fas_mu_cycle_solve", "cmg_gmg_damped_jacobi_solve",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_gauss_seidel_masked", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
-    "cmg_amg_last_solve_launches",
+    "cmg_amg_last_solve_launches", "cmg_amg_solve_batch",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -121,6 +121,7 @@ def lib():
             "cmg_amg_fas_mu_cycle": (I, [P, P, I, I, I, I, I]),
             "cmg_amg_last_solve_ms": (I, [P, P]),
             "cmg_amg_last_solve_launches": (I, [P, P]),
+            "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -141,6 +142,28 @@ def check_division(n, seed=0):
     first = (ctypes.c_uint * 2)()
     _check(lib().cmg_check_division(int(n), int(seed), ctypes.byref(m), first), "check_division")
     return m.value, (first[0], first[1])
+
+
+def solve_batch(solvers, grids, max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride, is_pure_neumann,
+                b_host=None, x_host=None):
+    """n independent solves, each on its own grid's stream, enqueued together (cmg_amg_solve_batch).
+    b_host / x_host: None, or lists of n host buffer addresses (num_tiles*512 floats each).
+    Returns lists (iters, rel_res, ms)."""
+    n = len(solvers)
+    if len(grids) != n or (b_host is None) != (x_host is None):
+        raise CmgError("solve_batch: solvers, grids and host buffers must match")
+    for s_ in solvers:
+        s_._sync_params()
+    sv = (ctypes.c_void_p * max(n, 1))(*[s_.h for s_ in solvers])
+    gv = (ctypes.c_void_p * max(n, 1))(*[g.h for g in grids])
+    bv = (ctypes.c_void_p * max(n, 1))(*b_host) if b_host is not None else None
+    xv = (ctypes.c_void_p * max(n, 1))(*x_host) if x_host is not None else None
+    it = (ctypes.c_int * max(n, 1))()
+    rel = (ctypes.c_double * max(n, 1))()
+    ms = (ctypes.c_float * max(n, 1))()
+    _check(lib().cmg_amg_solve_batch(sv, gv, n, bv, xv, max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride,
+                                     int(is_pure_neumann), it, rel, ms), "solve_batch")
+    return list(it[:n]), list(rel[:n]), list(ms[:n])
 
 
 def _check(rc, what):

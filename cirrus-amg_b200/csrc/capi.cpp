@@ -394,6 +394,57 @@ int cmg_amg_solve_host(cmg_amg_solver* s, cmg_grid* g, const float* b_host, floa
     return CMG_OK;
     GUARD_END
 }
+int cmg_amg_solve_batch(cmg_amg_solver* const* solvers, cmg_grid* const* grids, int n, const float* const* b_host,
+                        float* const* x_host, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
+                        int pure_neumann, int* iters, double* rel_res, float* ms) {
+    GUARD_BEGIN
+    if (n < 0 || (n > 0 && (!solvers || !grids || !iters || !rel_res)) || (!b_host != !x_host))
+        return fail(CMG_ERR_INVALID, "cmg_amg_solve_batch: bad argument");
+    std::vector<const void*> seen_s, seen_g;
+    for (int i = 0; i < n; ++i) {
+        if (!solvers[i] || !grid_ready(grids[i])) return fail(CMG_ERR_STATE, "cmg_amg_solve_batch: solver or grid not ready");
+        if (b_host && (!b_host[i] || !x_host[i])) return fail(CMG_ERR_INVALID, "cmg_amg_solve_batch: null host buffer");
+        seen_s.push_back(solvers[i]);
+        seen_g.push_back(grids[i]);
+    }
+    std::sort(seen_s.begin(), seen_s.end());
+    std::sort(seen_g.begin(), seen_g.end());
+    if (std::adjacent_find(seen_s.begin(), seen_s.end()) != seen_s.end() || std::adjacent_find(seen_g.begin(), seen_g.end()) != seen_g.end())
+        return fail(CMG_ERR_INVALID, "cmg_amg_solve_batch: solvers and grids must be distinct objects");
+    // enqueue every solve; on a failure, still wait for the ones already in flight
+    int rc = CMG_OK, begun = 0;
+    for (int i = 0; i < n && rc == CMG_OK; ++i) {
+        cmg::Grid& G = grids[i]->g;
+        if (b_host) {
+            const cudaError_t e =
+                cudaMemcpyAsync(G.plane(1), b_host[i], sizeof(float) * (size_t)G.n * 512, cudaMemcpyHostToDevice, G.stream);
+            if (e != cudaSuccess) {
+                rc = cmg::check_cuda(e, "solve_batch: copy of b");
+                break;
+            }
+        }
+        rc = solvers[i]->s.solve_begin(G, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0);
+        if (rc != CMG_OK) break;
+        ++begun;
+        if (x_host) {
+            const cudaError_t e =
+                cudaMemcpyAsync(x_host[i], G.plane(0), sizeof(float) * (size_t)G.n * 512, cudaMemcpyDeviceToHost, G.stream);
+            if (e != cudaSuccess) rc = cmg::check_cuda(e, "solve_batch: copy of x");
+        }
+    }
+    std::string first_error = rc != CMG_OK ? cmg::last_error() : "";
+    for (int i = 0; i < begun; ++i) {
+        const int r = solvers[i]->s.solve_finish(false, &iters[i], &rel_res[i]);
+        if (ms) ms[i] = solvers[i]->s.last_ms;
+        if (r != CMG_OK && rc == CMG_OK) {
+            rc = r;
+            first_error = cmg::last_error();
+        }
+    }
+    if (rc != CMG_OK) return fail(rc, first_error.c_str());
+    return CMG_OK;
+    GUARD_END
+}
 static int geo_create(int kind, float one_over_alpha, float prolong, cmg_amg_solver** out) {
     if (!out) return fail(CMG_ERR_INVALID, "solver create: null output");
     cmg_amg_solver* s = new cmg_amg_solver(kind, one_over_alpha, prolong);

@@ -571,8 +571,8 @@ int Solver::build_graph(Grid& G, const Key& k, Plan* out) {
     return 0;
 }
 
-int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann,
-                  int* iters, double* rel) {
+int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann) {
+    pending = Pending{};
     if (G.n == 0 || G.nleaf == 0) {
         set_error("solve: grid has no LEAF tiles (rebuild first)");
         return 3;
@@ -630,10 +630,26 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     CK(cudaEventRecord(ev1, st));
     CK(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(h_bar, bar, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, st));
+    pending.active = true;
+    pending.stream = st;
+    pending.sync_stride = sync_stride;
+    pending.plan = plan;
+    pending.stream_launches = stream_launches;
+    return 0;
+}
+
+int Solver::solve_finish(bool verbose, int* iters, double* rel) {
+    if (!pending.active) {
+        set_error("solve: no solve in flight on this solver");
+        return 3;
+    }
+    pending.active = false;
+    const cudaStream_t st = pending.stream;
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     cudaEventElapsedTime(&last_ms, ev0, ev1);
     const PcgScalars& r = *h_s;
+    const int sync_stride = pending.sync_stride;
     int n_it = r.iter;
     double rel_res;
     if (sync_stride > 0) {
@@ -651,8 +667,9 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     if (iters) *iters = n_it;
     if (rel) *rel = rel_res;
     // the IF body runs on every iteration except the one that ends the loop
+    const Plan& plan = pending.plan;
     last_launches = use_graph ? plan.k_pre + (long long)r.iter * plan.k_body + (long long)(r.iter > 0 ? r.iter - 1 : 0) * plan.k_if
-                              : stream_launches;
+                              : pending.stream_launches;
     if (verbose) std::printf("cmg AMG-PCG: %d iterations, relative residual %.6e, %.3f ms\n", n_it, rel_res, last_ms);
     if (h_bar[2]) {
         cudaMemsetAsync(bar, 0, sizeof(unsigned int) * 4, st);
@@ -664,6 +681,12 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
         return 5;
     }
     return 0;
+}
+
+int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann,
+                  int* iters, double* rel) {
+    if (int rc = solve_begin(G, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann)) return rc;
+    return solve_finish(verbose, iters, rel);
 }
 
 }  // namespace cmg

@@ -149,6 +149,18 @@ struct Solver {
     int build_graph(Grid& G, const Key& k, Plan* out);
     int solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
               bool pure_neumann, int* iters, double* rel);
+    // solve() in two halves, for batches of independent solves: solve_begin enqueues the whole
+    // solve and the read-back of its scalars on the grid's stream and returns; solve_finish
+    // waits for that stream and computes (iters, rel) as solve() does
+    int solve_begin(Grid& G, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann);
+    int solve_finish(bool verbose, int* iters, double* rel);
+    struct Pending {
+        bool active = false;
+        cudaStream_t stream = nullptr;
+        int sync_stride = 0;
+        Plan plan{};
+        long long stream_launches = -1;
+    } pending;
 };
 
 int check_cuda(cudaError_t e, const char* what);

@@ -226,6 +226,19 @@ int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, do
 int cmg_amg_solve_host(cmg_amg_solver* s, cmg_grid* g, const float* b_host, float* x_host, size_t count,
                        int max_iters, double relative_tolerance, int level_iters, int coarsest_iters,
                        int sync_stride, int is_pure_neumann, int* iters, double* rel_res);
+/* A batch of n independent solves, each AMGSolver::solve (src/AMGSolver.h:62) on its own
+ * grid with its own solver object; the reference has no batched call, its callers loop
+ * over solve().  Every solve is enqueued first, on its grid's stream (cmg_grid_set_stream),
+ * so solves on distinct streams run concurrently; then the call waits for all of them.
+ * b_host and x_host are NULL (b and x in channels 1 and 0 on the device) or arrays of n
+ * host pointers (num_tiles*512 floats each, pinned for the copies to overlap): b is copied
+ * in and x copied out as in cmg_amg_solve_host, inside the call.  solvers and grids must
+ * each be n distinct objects.  iters, rel_res and ms (device time of each solve from CUDA
+ * events on its stream; may be NULL) receive n values. */
+int cmg_amg_solve_batch(cmg_amg_solver* const* solvers, cmg_grid* const* grids, int n,
+                        const float* const* b_host, float* const* x_host,
+                        int max_iters, double relative_tolerance, int level_iters, int coarsest_iters,
+                        int sync_stride, int is_pure_neumann, int* iters, double* rel_res, float* ms);
 /* GaussSeidelAMG (src/AMGSolver.cu:887) on one level */
 int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
 /* The same sweeps as the multigrid cycle runs them (the pipelined persistent kernel):
