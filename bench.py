@@ -386,6 +386,31 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
 
+    # the mixed-precision preconditioner (16-bit operator storage in the smoothing sweeps),
+    # timed the same way on the same solve, against the FP32 solution above
+    x32 = G.download(0)
+    mixed = {}
+    for mode in ("bf16", "fp16"):
+        S.set_storage(mode)
+        for _ in range(3):
+            one_solve()
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record()
+        for _ in range(args.steps):
+            it_m, rel_m = one_solve()
+        m1.record()
+        torch.cuda.synchronize()
+        xm = G.download(0)
+        lm = ty == cmg.LEAF
+        mixed[mode] = {"ms": round(replica_time(m0.elapsed_time(m1), world, dev) / args.steps, 4), "pcg_iters": it_m,
+                       "rel_residual_recurrence": rel_m,
+                       "rel_l2_vs_fp32_solution": float(np.linalg.norm((xm - x32)[lm].astype(np.float64)) /
+                                                        np.linalg.norm(x32[lm].astype(np.float64)))}
+    S.set_storage("fp32")
+    one_solve()
+    torch.cuda.synchronize()
+
     # true residual of the last solution, FP32 operator apply on the device
     x = G.download(0)
     G.full_neg_lap(0, COEFF, 3)
@@ -439,6 +464,7 @@ def run_ours(args, rank, world, local_rank):
                 "l2": f"inputs larger than L2: {16 * ntiles * 2048 / 1e6:.0f} MB of channel planes per grid",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "e2e_wall_ms": round(e2e_wall_ms, 4),
+                "mixed_precision_preconditioner": mixed,
             },
             "e2e": {"value": round(e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": count * 4, "d2h_bytes_per_step": count * 4},
             "gpu_launches": int(launches),

@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(HERE, "libcmg.so")
 
 LEAF, NONLEAF, GHOST = 1, 2, 4
 DIRICHLET, INTERIOR, NEUMANN = 1, 2, 4
+STORAGE = {"fp32": 0, "bf16": 1, "fp16": 2}  # operator storage of the smoothing sweeps
 CASE_UNIFORM, CASE_CENTER_POINT, CASE_SPHERE_EMPTY, CASE_SPHERE_SOLID = 0, 1, 2, 3
 CASE_STAR_EMPTY, CASE_STAR_SOLID, CASE_SHELL, CASE_MULTI_SPHERE = 4, 5, 6, 7
 
@@ -46,7 +47,7 @@ EXPORTS = [
     "cmg_amg_fas_mu_cycle_solve", "cmg_gmg_damped_jacobi_solve",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_gauss_seidel_masked", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
-    "cmg_amg_last_solve_launches", "cmg_amg_solve_batch",
+    "cmg_amg_last_solve_launches", "cmg_amg_solve_batch", "cmg_amg_solver_set_storage",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -122,6 +123,7 @@ def lib():
             "cmg_amg_last_solve_ms": (I, [P, P]),
             "cmg_amg_last_solve_launches": (I, [P, P]),
             "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
+            "cmg_amg_solver_set_storage": (I, [P, I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -371,6 +373,11 @@ class AMGSolver:
         pipeline: the cycle's smoothing sweeps as a persistent kernel that prefetches the next tile."""
         flags = (1 if use_graph else 0) | (2 if persistent else 0) | (0 if cluster else 4) | (0 if pipeline else 8)
         _check(self.L.cmg_amg_solver_set_launch_mode(self.h, flags), "set_launch_mode")
+
+    def set_storage(self, storage):
+        """Operator storage of the mu-cycle's smoothing sweeps: "fp32" (default, the
+        reference's arithmetic), "bf16" or "fp16" (mixed precision)."""
+        _check(self.L.cmg_amg_solver_set_storage(self.h, STORAGE[storage]), "set_storage")
 
     def _sync_params(self):
         _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")

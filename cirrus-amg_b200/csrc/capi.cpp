@@ -373,6 +373,14 @@ int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags) {
     s->s.use_persist = (flags & CMG_LAUNCH_PERSISTENT) != 0 && s->s.persist_nblocks > 0;
     return CMG_OK;
 }
+int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage) {
+    if (!s || storage < CMG_STORAGE_FP32 || storage > CMG_STORAGE_FP16) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_storage: bad argument");
+    if (s->s.kind != cmg::kAMG && storage != CMG_STORAGE_FP32)
+        return fail(CMG_ERR_STATE, "cmg_amg_solver_set_storage: 16-bit operator storage is for AMG solvers");
+    static_assert(CMG_STORAGE_BF16 == cmg::kStorageBF16 && CMG_STORAGE_FP16 == cmg::kStorageFP16, "storage codes");
+    s->s.storage = storage;
+    return CMG_OK;
+}
 int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
                   int pure_neumann, int* iters, double* rel_res) {
     GUARD_BEGIN
@@ -530,6 +538,8 @@ int cmg_amg_gauss_seidel_masked(cmg_amg_solver* s, cmg_grid* g, int iters, int o
     if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_gauss_seidel_masked: not an AMG solver (use cmg_mg_gauss_seidel)");
     if (level < 0 || level > g->g.max_level() || !chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || (order != 0 && order != 1))
         return fail(CMG_ERR_INVALID, "cmg_amg_gauss_seidel_masked: bad argument");
+    if (int rc = s->s.ensure_coeff16(g->g)) return rc;
+    if (s->s.storage != cmg::kStorageFP32) cmg::launch_coeff16(g->g.dev(), s->s.coeff_ch, s->s.storage, s->s.coeff16, g->g.stream);
     s->s.enqueue_gs(g->g, level, iters, order, g->g.plane(x_ch), g->g.plane(rhs_ch), g->g.stream, true);
     return cmg::check_cuda(cudaGetLastError(), "gauss_seidel");
 }
@@ -539,7 +549,8 @@ int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, i
     if (!chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || !chan_ok(g, x0_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_fas_mu_cycle: channel out of range");
     if (int rc = cmg::validate_solver_topology(g->g)) return rc;
     const cmg::MuArgs A = s->s.mu_args(g->g, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters);
-    s->s.enqueue_cluster_pack(g->g, g->g.stream);
+    if (int rc = s->s.ensure_coeff16(g->g)) return rc;
+    s->s.enqueue_operand_pack(g->g, g->g.stream);
     s->s.enqueue_mu_cycle(g->g, A, g->g.stream);
     return cmg::check_cuda(cudaGetLastError(), "fas_mu_cycle");
 }

@@ -185,6 +185,7 @@ Solver::~Solver() {
     dfree(partial2);
     dfree(s);
     if (cluster_pack) cudaFree(cluster_pack);
+    dfree(coeff16);
     if (h_s) cudaFreeHost(h_s);
     if (h_bar) cudaFreeHost(h_bar);
     dfree(bar);
@@ -249,7 +250,7 @@ void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, cons
     for (int it = 0; it < iters; ++it)
         for (int h = 0; h < 2; ++h) {
             const int color = h ? 1 - order : order;
-            if (pipe) launch_gs_pipe(d, t0, nt, X, RHS, coeff_ch, color, omega, st);
+            if (pipe) launch_gs_pipe(d, t0, nt, X, RHS, coeff_ch, color, omega, st, kind == kAMG ? storage : kStorageFP32, coeff16);
             else launch_gs(d, t0, nt, X, RHS, coeff_ch, color, omega, st);
         }
 }
@@ -283,6 +284,27 @@ void Solver::enqueue_cluster_pack(Grid& G, cudaStream_t st) const {
     int tile1[8], tile2[64];
     coarse_tiles(G, tile1, tile2);
     launch_cluster_pack(G.dev(), tile1, tile2, coeff_ch, cluster_pack, st);
+}
+
+int Solver::ensure_coeff16(const Grid& G) {
+    if (storage == kStorageFP32 || kind != kAMG) return 0;
+    const size_t need = coeff16_bytes(G.dev());
+    if (need <= coeff16_cap) return 0;
+    dfree(coeff16);
+    coeff16 = nullptr;
+    coeff16_cap = 0;
+    CK(cudaMalloc(&coeff16, need));
+    coeff16_cap = need;
+    // captured graphs hold the old pointer
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    return 0;
+}
+
+void Solver::enqueue_operand_pack(Grid& G, cudaStream_t st) const {
+    if (kind != kAMG) return;
+    enqueue_cluster_pack(G, st);
+    if (storage != kStorageFP32) launch_coeff16(G.dev(), coeff_ch, storage, coeff16, st);
 }
 
 // AMGSolver::FASMuCycleStep (src/AMGSolver.cu:1257-1277).  A visit of level 2
@@ -393,9 +415,10 @@ int Solver::host_dot(Grid& G, const int* list, int nlist, const float* A, const 
 // iteration at which |r| < tol |b| (or max_iters) and |r| / |b|
 int Solver::fas_mu_cycle_solve(Grid& G, int repeat_times, int max_iters, double tol, int level_iters, int coarsest_iters, int* iters, double* rel) {
     if (int rc = validate_solver_topology(G)) return rc;
+    if (int rc = ensure_coeff16(G)) return rc;
     const DevGrid d = G.dev();
     cudaStream_t st = G.stream;
-    enqueue_cluster_pack(G, st);
+    enqueue_operand_pack(G, st);
     launch_fill(G.plane(0), (size_t)G.n * kCells, 0.0f, st);
     double bb = 0;
     if (int rc = host_dot(G, G.leaf, G.nleaf, G.plane(1), G.plane(1), &bb)) return rc;
@@ -486,7 +509,7 @@ static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
 void Solver::enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_h, bool graph, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
-    if (kind == kAMG) enqueue_cluster_pack(G, st);
+    enqueue_operand_pack(G, st);
     launch_leaf_fill(d, G.leaf, G.nleaf, G.plane(0), 0.0f, st);
     if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(1), kDotRR0, nullptr, rs, st);
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
@@ -588,7 +611,9 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     }
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
-    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu, (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0), omega};
+    if (int rc = ensure_coeff16(G)) return rc;
+    Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu,
+          (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0) | (storage << 4), omega};
     Plan plan{};
     if (use_graph) {
         auto it = graphs.find(k);

@@ -138,6 +138,14 @@ struct Solver {
     bool use_pipe = true;      // pipelined smoothing kernel inside the cycle
     bool pipe_ok = false;      // the device can run it
     void* cluster_pack = nullptr;  // packed static operands of levels 0-2 (launch_cluster_pack)
+    // storage of the operator planes the pipelined smoother reads (kStorageFP32/BF16/FP16);
+    // 16-bit modes read coeff16, a copy made once per solve or cycle by enqueue_operand_pack
+    int storage = kStorageFP32;
+    void* coeff16 = nullptr;
+    size_t coeff16_cap = 0;
+    int ensure_coeff16(const Grid& G);
+    // once per solve or cycle: the cluster step's packed operands and the 16-bit operator copy
+    void enqueue_operand_pack(Grid& G, cudaStream_t st) const;
     bool cluster_active(const Grid& G) const;
     void enqueue_cluster_pack(Grid& G, cudaStream_t st) const;
     int persist_nblocks = 0;

@@ -13,20 +13,33 @@
 // true (x starts at 0; restriction, prolongation and the sweeps write masked values),
 // and on GHOST neighbours being read raw, as the reference does.  The public
 // cmg_amg_gauss_seidel, which takes arbitrary x, keeps using k_gs.
+//
+// The operator planes (diagonal and the three face coefficients) are read either as
+// float (the reference's arithmetic) or, in the mixed-precision mode, from BF16 or FP16
+// copies made once per solve: 8 of the 27 bytes a cell costs per pass.  Every value is
+// widened to float on load and all arithmetic stays FP32, so a 16-bit run equals a
+// float run on coefficients rounded to 16 bits beforehand, bit for bit.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "kernels.hpp"
 
 namespace cmg {
 
 namespace {
 
+template <typename CT>
 struct PipeStage {
-    float x[512], b[512], d[512];
-    float c0[576];   // -x faces of the tile, then the +x faces of row i = 7 (from the +x neighbour)
-    float c1[512];   // -y faces
-    float c2[512];   // -z faces
-    float c1h[64];   // +y faces of row j = 7, [i][k]
-    float c2h[64];   // +z faces of row k = 7, [i][j]
-    float hx[384];   // halo x of the six faces, [axis][side][a][b]
+    float x[512], b[512];
+    CT d[512];        // diagonal
+    CT c0[512];       // -x faces
+    CT c1[512];       // -y faces
+    CT c2[512];       // -z faces
+    // faces taken from the neighbours: +x faces of row i = 7 [j][k], +y faces of row j = 7
+    // [i][k], +z faces of row k = 7 [i][j]; a word holds the float, or for 16-bit storage
+    // the 4-byte-aligned pair of plane elements that contains the face
+    unsigned c0h[64], c1h[64], c2h[64];
+    float hx[384];    // halo x of the six faces, [axis][side][a][b]
     unsigned ty[128];
 };
 // The snapshot: masked x of the tile with its one-cell halo, split into four planes by
@@ -38,15 +51,19 @@ struct PipeStage {
 constexpr int kSxI = 42, kSxJ = 4, kSxP = 448;
 __device__ __forceinline__ int sxp(int i, int j, int k) { return ((k + 4) & 3) * kSxP + (i + 1) * kSxI + (j + 1) * kSxJ + ((k + 4) >> 2); }
 
+template <typename CT>
 struct PipeSmem {
-    PipeStage st[2];
+    PipeStage<CT> st[2];
     float x[4 * kSxP];
 };
-constexpr size_t kPipeSmem = sizeof(PipeSmem);
 
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp8(void* dst, const void* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp4(void* dst, const void* src) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
@@ -56,10 +73,53 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 __device__ __forceinline__ void cp_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// Storage of the operator planes: copies into a stage and widening to float.
+template <typename CT>
+struct Coef;
+template <>
+struct Coef<float> {
+    __device__ static void cp_quad(float* dst, const float* src) { cp16(dst, src); }
+    __device__ static void cp_face(unsigned* dst, const float* plane, size_t o) { cp4(dst, plane + o); }
+    __device__ static unsigned word(float v) { return __float_as_uint(v); }
+    __device__ static float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+    __device__ static float at(const float* p) { return *p; }
+    __device__ static float face(unsigned w, int) { return __uint_as_float(w); }
+};
+// 16-bit storage: 4 elements move as 8 bytes; a face element moves inside its aligned pair
+template <typename CT>
+struct Coef16 {
+    __device__ static void cp_quad(CT* dst, const CT* src) { cp8(dst, src); }
+    __device__ static void cp_face(unsigned* dst, const CT* plane, size_t o) { cp4(dst, plane + (o & ~(size_t)1)); }
+    __device__ static float4 ld4(const CT* p) {
+        const uint2 w = *reinterpret_cast<const uint2*>(p);
+        return make_float4(Coef<CT>::wide(w.x & 0xffffu), Coef<CT>::wide(w.x >> 16), Coef<CT>::wide(w.y & 0xffffu), Coef<CT>::wide(w.y >> 16));
+    }
+    __device__ static float at(const CT* p) { return Coef<CT>::wide(*reinterpret_cast<const unsigned short*>(p)); }
+    __device__ static float face(unsigned w, int odd) { return Coef<CT>::wide(odd ? w >> 16 : w & 0xffffu); }
+};
+template <>
+struct Coef<__nv_bfloat16> : Coef16<__nv_bfloat16> {
+    __device__ static float wide(unsigned bits) { return __uint_as_float(bits << 16); }
+    __device__ static unsigned word(float v) {
+        const unsigned b = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+        return b | (b << 16);
+    }
+};
+template <>
+struct Coef<__half> : Coef16<__half> {
+    __device__ static float wide(unsigned bits) { return __half2float(__ushort_as_half((unsigned short)bits)); }
+    __device__ static unsigned word(float v) {
+        const unsigned b = __half_as_ushort(__float2half_rn(v));
+        return b | (b << 16);
+    }
+};
+
 struct PipeArgs {
-    int t0, nt, coeff_ch, color, exact;
+    int t0, nt, color, exact;
     float om;
     double omega;
+    const void* coef;  // first of the four operator planes (-x, -y, -z faces, diagonal)
+    size_t cstride;    // elements from one operator plane to the next
 };
 
 // neighbour descriptors of the thread's three halo cells: face r on side q >> 6
@@ -69,38 +129,40 @@ __device__ __forceinline__ void load_desc(const DevGrid& g, int t, int side, int
 }
 
 // start the copies of tile t into stage S
-__device__ __forceinline__ void issue(PipeStage& S, const DevGrid& g, int t, const float* X, const float* B, const float* C0,
-                                      const float* C1, const float* C2, const float* C3, const int d[3], int q, float h) {
+template <typename CT>
+__device__ __forceinline__ void issue(PipeStage<CT>& S, const DevGrid& g, int t, const float* X, const float* B, const CT* C0,
+                                      const CT* C1, const CT* C2, const CT* C3, const int d[3], int q, float h) {
     const size_t base = (size_t)t * kCells + 4 * q;
     cp16(&S.x[4 * q], X + base);
     cp16(&S.b[4 * q], B + base);
-    cp16(&S.d[4 * q], C3 + base);
-    cp16(&S.c0[4 * q], C0 + base);
-    cp16(&S.c1[4 * q], C1 + base);
-    cp16(&S.c2[4 * q], C2 + base);
+    Coef<CT>::cp_quad(&S.d[4 * q], C3 + base);
+    Coef<CT>::cp_quad(&S.c0[4 * q], C0 + base);
+    Coef<CT>::cp_quad(&S.c1[4 * q], C1 + base);
+    Coef<CT>::cp_quad(&S.c2[4 * q], C2 + base);
     cp4(&S.ty[q], g.ctype + base);
     const int side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
     const int e = side ? 0 : 7;  // the neighbour's cell next to the shared face
     const int nl[3] = {cell_index(e, fa, fb), cell_index(fa, e, fb), cell_index(fa, fb, e)};
-    float* hc[3] = {&S.c0[512 + fa * 8 + fb], &S.c1h[fa * 8 + fb], &S.c2h[fa * 8 + fb]};
-    const float* Cr[3] = {C0, C1, C2};
+    unsigned* hc[3] = {&S.c0h[fa * 8 + fb], &S.c1h[fa * 8 + fb], &S.c2h[fa * 8 + fb]};
+    const CT* Cr[3] = {C0, C1, C2};
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         float* hxd = &S.hx[r * 128 + q];
         if (d[r] != 0) {
             const size_t o = (size_t)((d[r] >> 3) - 1) * kCells + nl[r];
             cp4(hxd, X + o);
-            if (side) cp4(hc[r], Cr[r] + o);
+            if (side) Coef<CT>::cp_face(hc[r], Cr[r], o);
         } else {
             *hxd = 0.0f;
-            if (side) *hc[r] = h;
+            if (side) *hc[r] = Coef<CT>::word(h);
         }
     }
     cp_commit();
 }
 
 // the snapshot of the staged tile and one colour pass over it
-__device__ __forceinline__ void process(const PipeStage& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
+template <typename CT>
+__device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
                                         const PipeArgs& A) {
     const Quad Q(t, q);
     const float4 xr = *reinterpret_cast<const float4*>(&S.x[4 * q]);
@@ -144,18 +206,20 @@ __device__ __forceinline__ void process(const PipeStage& S, float* SX, const Dev
     }
     __syncthreads();
     const float4 b = *reinterpret_cast<const float4*>(&S.b[4 * q]);
-    const float4 dg = *reinterpret_cast<const float4*>(&S.d[4 * q]);
-    const float4 a0 = *reinterpret_cast<const float4*>(&S.c0[4 * q]);
-    const float4 a1 = *reinterpret_cast<const float4*>(&S.c1[4 * q]);
-    const float4 a2 = *reinterpret_cast<const float4*>(&S.c2[4 * q]);
-    // +x faces: the -x faces of the cells at i + 1 (thread q + 16; row i = 7: from the +x
-    // neighbour, stored after the tile's faces in the same order)
-    const float4 px = *reinterpret_cast<const float4*>(&S.c0[4 * (q + 16)]);
+    const float4 dg = Coef<CT>::ld4(&S.d[4 * q]);
+    const float4 a0 = Coef<CT>::ld4(&S.c0[4 * q]);
+    const float4 a1 = Coef<CT>::ld4(&S.c1[4 * q]);
+    const float4 a2 = Coef<CT>::ld4(&S.c2[4 * q]);
+    // +x faces: the -x faces of the cells at i + 1 (thread q + 16), or from the +x neighbour on row i = 7
+    const float4 px = Q.i < 7 ? Coef<CT>::ld4(&S.c0[4 * (q + 16)])
+                              : make_float4(Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0], 0), Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 1], 1),
+                                            Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 2], 0), Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 3], 1));
     // +y faces: the -y faces at j + 1 (thread q + 2), or from the +y neighbour on row j = 7
-    const float4 py = Q.j < 7 ? *reinterpret_cast<const float4*>(&S.c1[4 * (q + 2)])
-                              : *reinterpret_cast<const float4*>(&S.c1h[Q.i * 8 + Q.k0]);
+    const float4 py = Q.j < 7 ? Coef<CT>::ld4(&S.c1[4 * (q + 2)])
+                              : make_float4(Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0], 0), Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 1], 1),
+                                            Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 2], 0), Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 3], 1));
     // +z face of the last cell of the quad: the next quad's first -z face, or the +z neighbour's
-    const float pz3 = Q.k0 == 0 ? S.c2[4 * (q + 1)] : S.c2h[Q.i * 8 + Q.j];
+    const float pz3 = Q.k0 == 0 ? Coef<CT>::at(&S.c2[4 * (q + 1)]) : Coef<CT>::face(S.c2h[Q.i * 8 + Q.j], 0);
     float4 out = xr;
     const int p = (Q.i + Q.j + Q.k0 + A.color) & 1;  // own cells of this colour: u = p, p + 2
 #pragma unroll
@@ -185,17 +249,18 @@ __device__ __forceinline__ void process(const PipeStage& S, float* SX, const Dev
     }
     st4(X + Q.base, out);
 }
+template <typename CT>
 __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const float* B, PipeArgs A) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
-    PipeSmem& sm = *reinterpret_cast<PipeSmem*>(pipe_smem);
+    PipeSmem<CT>& sm = *reinterpret_cast<PipeSmem<CT>*>(pipe_smem);
     const int q = threadIdx.x, side = q >> 6;
     const int stride = gridDim.x, tend = A.t0 + A.nt;
     int tcur = A.t0 + blockIdx.x;
     if (tcur >= tend) return;
-    const float* C0 = g.plane(A.coeff_ch);
-    const float* C1 = g.plane(A.coeff_ch + 1);
-    const float* C2 = g.plane(A.coeff_ch + 2);
-    const float* C3 = g.plane(A.coeff_ch + 3);
+    const CT* C0 = static_cast<const CT*>(A.coef);
+    const CT* C1 = C0 + A.cstride;
+    const CT* C2 = C1 + A.cstride;
+    const CT* C3 = C2 + A.cstride;
     const float h = voxel_size(g.h0, tile_level(g, tcur));  // all tiles of the launch share the level
     int dcur[3], dnext[3] = {0, 0, 0};
     load_desc(g, tcur, side, dcur);
@@ -225,16 +290,29 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const f
     cp_wait_all();
 }
 
+__device__ __forceinline__ void store16(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+__device__ __forceinline__ void store16(__half* p, float v) { *p = __float2half_rn(v); }
+// the operator planes rounded to 16 bits (round to nearest even), plane after plane
+template <typename CT>
+__global__ void k_coeff16(const float* __restrict__ C, CT* __restrict__ out, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) store16(out + i, C[i]);
+}
+
 int g_pipe_blocks = 0;  // resident blocks of k_gs_pipe on the device
+
+template <typename CT>
+bool set_pipe_smem() {
+    return cudaFuncSetAttribute(k_gs_pipe<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess;
+}
 
 }  // namespace
 
 int gs_pipe_init() {
-    if (cudaFuncSetAttribute(k_gs_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPipeSmem) != cudaSuccess) return 0;
+    if (!set_pipe_smem<float>() || !set_pipe_smem<__nv_bfloat16>() || !set_pipe_smem<__half>()) return 0;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe, 128, kPipeSmem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float>, 128, sizeof(PipeSmem<float>)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -242,19 +320,41 @@ int gs_pipe_init() {
     return g_pipe_blocks;
 }
 
-void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st) {
+size_t coeff16_bytes(const DevGrid& g) { return (size_t)4 * g.n * kCells * 2; }
+
+void launch_coeff16(const DevGrid& g, int coeff_ch, int storage, void* out, cudaStream_t st) {
+    const size_t n = (size_t)4 * g.n * kCells;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    note_kernel_launch();
+    if (storage == kStorageBF16)
+        k_coeff16<__nv_bfloat16><<<blocks, 256, 0, st>>>(g.plane(coeff_ch), static_cast<__nv_bfloat16*>(out), n);
+    else
+        k_coeff16<__half><<<blocks, 256, 0, st>>>(g.plane(coeff_ch), static_cast<__half*>(out), n);
+}
+
+void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st,
+                    int storage, const void* coeff16) {
     if (nt <= 0) return;
     PipeArgs A;
     A.t0 = t0;
     A.nt = nt;
-    A.coeff_ch = coeff_ch;
     A.color = color;
     A.om = (float)omega;
     A.exact = ((double)A.om == omega);
     A.omega = omega;
+    A.cstride = (size_t)g.n * kCells;
     const int blocks = nt < g_pipe_blocks ? nt : g_pipe_blocks;
     note_kernel_launch();
-    k_gs_pipe<<<blocks, 128, kPipeSmem, st>>>(g, X, B, A);
+    if (storage == kStorageFP32) {
+        A.coef = g.plane(coeff_ch);
+        k_gs_pipe<float><<<blocks, 128, sizeof(PipeSmem<float>), st>>>(g, X, B, A);
+    } else if (storage == kStorageBF16) {
+        A.coef = coeff16;
+        k_gs_pipe<__nv_bfloat16><<<blocks, 128, sizeof(PipeSmem<__nv_bfloat16>), st>>>(g, X, B, A);
+    } else {
+        A.coef = coeff16;
+        k_gs_pipe<__half><<<blocks, 128, sizeof(PipeSmem<__half>), st>>>(g, X, B, A);
+    }
 }
 
 }  // namespace cmg

@@ -43,7 +43,13 @@ void launch_accumulate_cells(const DevGrid& g, int t0, int nt, int types, const 
 // persistent, software-pipelined colour pass for the multigrid cycle (gs_pipe.cu); needs the
 // x plane masked to INTERIOR cells.  gs_pipe_init: resident blocks on the device (0: unusable).
 int gs_pipe_init();
-void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
+// Storage of the operator planes the pipelined smoother reads: the float channels, or a
+// BF16 / FP16 copy (coeff16: four planes of num_tiles*512 elements, made by launch_coeff16).
+constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;
+void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st,
+                    int storage = kStorageFP32, const void* coeff16 = nullptr);
+size_t coeff16_bytes(const DevGrid& g);
+void launch_coeff16(const DevGrid& g, int coeff_ch, int storage, void* out, cudaStream_t st);
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float R_restrict, cudaStream_t st);
 void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st);

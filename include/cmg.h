@@ -181,6 +181,16 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
 #define CMG_LAUNCH_NO_CLUSTER 4
 #define CMG_LAUNCH_NO_PIPELINE 8
 int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
+/* Mixed-precision preconditioner (no counterpart in the reference, which is FP32
+ * throughout): the smoothing sweeps of the mu-cycle on levels 3 and finer read the
+ * operator planes (diagonal and face coefficients) from a BF16 or FP16 copy made once
+ * per solve, widening every value to float; x, b, residuals, restriction, the coarse
+ * levels and the PCG iteration stay FP32 with FP64 dot products.  Default FP32, which
+ * is the reference's arithmetic. */
+#define CMG_STORAGE_FP32 0
+#define CMG_STORAGE_BF16 1
+#define CMG_STORAGE_FP16 2
+int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage);
 
 /* ---- geometric multigrid preconditioners ---------------------------------
  * GMGSolver(one_over_alpha, prolong_coeff) (src/GMGSolver.h:21) and
