@@ -73,12 +73,36 @@ int Grid::ensure_device() {
     std::unordered_map<unsigned long long, int> old_index;
     old_index.reserve(2 * dev_keys.size() + 1);
     for (int t = 0; t < (int)dev_keys.size(); ++t) old_index.emplace(dev_keys[t], t);
-    std::vector<int> old_of_new(n_new);
+    // where each tile's data comes from (src/HAGrid.h:1140-1160, PoissonTile.h:151-172):
+    // a tile that survives keeps its own (a LEAF that became NONLEAF included); a LEAF or
+    // NONLEAF tile made by refinement -- new, or a GHOST it replaced -- starts from its
+    // nearest surviving LEAF/NONLEAF ancestor, s levels up, each cell taking the value and
+    // type of the ancestor cell that contains it (childTile applied s times); a new GHOST
+    // tile starts at zero
+    std::vector<int2> src_of_new(n_new);
     std::vector<unsigned long long> keys(n_new);
     for (int t = 0; t < n_new; ++t) {
-        keys[t] = tile_key(topo.tiles()[t]);
+        const TileRec& r = topo.tiles()[t];
+        keys[t] = tile_key(r);
         auto it = old_index.find(keys[t]);
-        old_of_new[t] = it == old_index.end() ? -1 : it->second;
+        src_of_new[t] = make_int2(-1, 0);
+        if (it != old_index.end() && (dev_types[it->second] != kGhost || r.type == kGhost)) {
+            src_of_new[t] = make_int2(it->second, 0);
+        } else if (r.type != kGhost) {
+            for (int sh = 1; sh <= r.level; ++sh) {
+                const TileRec a{r.level - sh, {r.c[0] >> sh, r.c[1] >> sh, r.c[2] >> sh}, 0};
+                auto ia = old_index.find(tile_key(a));
+                if (ia != old_index.end() && dev_types[ia->second] != kGhost) {
+                    src_of_new[t] = make_int2(ia->second, sh);
+                    break;
+                }
+            }
+        }
+    }
+    std::vector<int4> hm(n_new);
+    for (int t = 0; t < n_new; ++t) {
+        const TileRec& r = topo.tiles()[t];
+        hm[t] = make_int4(r.level | (r.type << 8), r.c[0], r.c[1], r.c[2]);
     }
 
     float* chan_new = nullptr;
@@ -86,12 +110,15 @@ int Grid::ensure_device() {
     const size_t cells = (size_t)n_new * kCells;
     CK(cudaMalloc(&chan_new, sizeof(float) * cells * nch + 16));
     CK(cudaMalloc(&ct_new, cells + 16));
-    int* d_map = nullptr;
-    CK(cudaMalloc(&d_map, sizeof(int) * (n_new + 1)));
-    CK(cudaMemcpy(d_map, old_of_new.data(), sizeof(int) * n_new, cudaMemcpyHostToDevice));
+    int2* d_map = nullptr;
+    int4* d_meta = nullptr;
+    CK(cudaMalloc(&d_map, sizeof(int2) * (n_new + 1)));
+    CK(cudaMalloc(&d_meta, sizeof(int4) * (n_new + 1)));
+    CK(cudaMemcpy(d_map, src_of_new.data(), sizeof(int2) * n_new, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_meta, hm.data(), sizeof(int4) * n_new, cudaMemcpyHostToDevice));
     if (n_old > 0) {
-        launch_remap(chan, chan_new, d_map, n_new, nch, n_old, stream);
-        launch_remap_types(ctype, ct_new, d_map, n_new, stream);
+        launch_remap(chan, chan_new, d_map, d_meta, n_new, nch, n_old, stream);
+        launch_remap_types(ctype, ct_new, d_map, d_meta, n_new, stream);
     } else {
         CK(cudaMemsetAsync(chan_new, 0, sizeof(float) * cells * nch, stream));
         CK(cudaMemsetAsync(ct_new, 0, cells, stream));
@@ -104,11 +131,6 @@ int Grid::ensure_device() {
     chan = chan_new;
     ctype = ct_new;
 
-    std::vector<int4> hm(n_new);
-    for (int t = 0; t < n_new; ++t) {
-        const TileRec& r = topo.tiles()[t];
-        hm[t] = make_int4(r.level | (r.type << 8), r.c[0], r.c[1], r.c[2]);
-    }
     std::vector<int> hx((size_t)8 * n_new, 0);
     for (int t = 0; t < n_new; ++t)
         for (int f = 0; f < 6; ++f) {
@@ -116,23 +138,24 @@ int Grid::ensure_device() {
             if (q >= 0) hx[8 * t + f] = ((q + 1) << 3) | topo.tiles()[q].type;
         }
     dfree(meta);
+    meta = d_meta;
     dfree(nb);
     dfree(child);
     dfree(nbx);
     dfree(leaf);
     CK(cudaMalloc(&nbx, sizeof(int) * 8 * (n_new + 1)));
     CK(cudaMemcpy(nbx, hx.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&meta, sizeof(int4) * (n_new + 1)));
     CK(cudaMalloc(&nb, sizeof(int) * 8 * (n_new + 1)));
     CK(cudaMalloc(&child, sizeof(int) * 8 * (n_new + 1)));
     CK(cudaMalloc(&leaf, sizeof(int) * (topo.leaf_list.size() + 1)));
-    CK(cudaMemcpy(meta, hm.data(), sizeof(int4) * n_new, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(nb, topo.nb.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(child, topo.child.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(leaf, topo.leaf_list.data(), sizeof(int) * topo.leaf_list.size(), cudaMemcpyHostToDevice));
     n = n_new;
     nleaf = (int)topo.leaf_list.size();
     dev_keys.swap(keys);
+    dev_types.resize(n_new);
+    for (int t = 0; t < n_new; ++t) dev_types[t] = topo.tiles()[t].type;
     dev_version = host_version;
     ++version;
     return 0;

@@ -27,6 +27,7 @@ struct Grid {
     unsigned long long host_version = 0;  // bumps on every rebuild
     unsigned long long dev_version = 0;   // host_version the device copy matches
     std::vector<unsigned long long> dev_keys;
+    std::vector<int> dev_types;  // tile types of the device copy, in its order
     float* chan = nullptr;
     uint8_t* ctype = nullptr;
     int4* meta = nullptr;

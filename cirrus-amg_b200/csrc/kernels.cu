@@ -1032,17 +1032,30 @@ __global__ void __launch_bounds__(128) k_gradient(DevGrid g, const float* X, int
     }
 }
 
-__global__ void k_remap(const float* src, float* dst, const int* old_of_new, int n_new, int n_old) {
+// cell of source tile for cell (i, j, k) of a new tile at meta m taking data from s levels up:
+// the same cell (s = 0), else the ancestor cell that contains it
+__device__ __forceinline__ int remap_cell(const int4& m, int s, int v) {
+    if (s == 0) return v;
+    const int i = v >> 6, j = (v >> 3) & 7, k = v & 7;
+    const int ai = ((m.y * 8 + i) >> s) - (m.y >> s) * 8;
+    const int aj = ((m.z * 8 + j) >> s) - (m.z >> s) * 8;
+    const int ak = ((m.w * 8 + k) >> s) - (m.w >> s) * 8;
+    return cell_index(ai, aj, ak);
+}
+__global__ void k_remap(const float* src, float* dst, const int2* src_of_new, const int4* meta, int n_new, int n_old) {
     const int t = blockIdx.x, c = blockIdx.y;
-    const int o = old_of_new[t];
+    const int2 o = src_of_new[t];
+    const int4 m = meta[t];
     const size_t dbase = ((size_t)c * n_new + t) * kCells;
     for (int v = threadIdx.x; v < kCells; v += blockDim.x)
-        dst[dbase + v] = (o >= 0) ? src[((size_t)c * n_old + o) * kCells + v] : 0.0f;
+        dst[dbase + v] = (o.x >= 0) ? src[((size_t)c * n_old + o.x) * kCells + remap_cell(m, o.y, v)] : 0.0f;
 }
-__global__ void k_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new) {
+__global__ void k_remap_types(const uint8_t* src, uint8_t* dst, const int2* src_of_new, const int4* meta) {
     const int t = blockIdx.x;
-    const int o = old_of_new[t];
-    for (int v = threadIdx.x; v < kCells; v += blockDim.x) dst[(size_t)t * kCells + v] = (o >= 0) ? src[(size_t)o * kCells + v] : 0;
+    const int2 o = src_of_new[t];
+    const int4 m = meta[t];
+    for (int v = threadIdx.x; v < kCells; v += blockDim.x)
+        dst[(size_t)t * kCells + v] = (o.x >= 0) ? src[(size_t)o.x * kCells + remap_cell(m, o.y, v)] : 0;
 }
 __global__ void k_fill(float* p, size_t n, float v) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
@@ -1307,11 +1320,11 @@ void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, i
 void launch_gradient(const DevGrid& g, const float* X, int coeff_ch, int u_ch, cudaStream_t st) {
     if (g.n > 0) count_launch(), k_gradient<<<g.n, 128, 0, st>>>(g, X, coeff_ch, u_ch);
 }
-void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st) {
-    if (n_new > 0 && nch > 0) count_launch(), k_remap<<<dim3(n_new, nch), 128, 0, st>>>(src, dst, old_of_new, n_new, n_old);
+void launch_remap(const float* src, float* dst, const int2* src_of_new, const int4* meta, int n_new, int nch, int n_old, cudaStream_t st) {
+    if (n_new > 0 && nch > 0) count_launch(), k_remap<<<dim3(n_new, nch), 128, 0, st>>>(src, dst, src_of_new, meta, n_new, n_old);
 }
-void launch_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new, int n_new, cudaStream_t st) {
-    if (n_new > 0) count_launch(), k_remap_types<<<n_new, 128, 0, st>>>(src, dst, old_of_new);
+void launch_remap_types(const uint8_t* src, uint8_t* dst, const int2* src_of_new, const int4* meta, int n_new, cudaStream_t st) {
+    if (n_new > 0) count_launch(), k_remap_types<<<n_new, 128, 0, st>>>(src, dst, src_of_new, meta);
 }
 void launch_fill(float* p, size_t n, float v, cudaStream_t st) {
     if (n > 0) count_launch(), k_fill<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p, n, v);

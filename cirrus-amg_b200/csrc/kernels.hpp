@@ -116,8 +116,10 @@ void launch_propagate_ghost(const DevGrid& g, int t0, int nt, int ch, cudaStream
 void launch_accumulate_faces(const DevGrid& g, const int* leaf, int nleaf, int u_ch, cudaStream_t st);
 void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, int coeff_ch, int out_ch, cudaStream_t st);
 void launch_gradient(const DevGrid& g, const float* X, int coeff_ch, int u_ch, cudaStream_t st);
-void launch_remap(const float* src, float* dst, const int* old_of_new, int n_new, int nch, int n_old, cudaStream_t st);
-void launch_remap_types(const uint8_t* src, uint8_t* dst, const int* old_of_new, int n_new, cudaStream_t st);
+// channel data and cell types of a new tile order: from the old tile src_of_new[t].x, s =
+// src_of_new[t].y levels up (0: the same tile; -1 in .x: zero); meta: the new tiles' meta
+void launch_remap(const float* src, float* dst, const int2* src_of_new, const int4* meta, int n_new, int nch, int n_old, cudaStream_t st);
+void launch_remap_types(const uint8_t* src, uint8_t* dst, const int2* src_of_new, const int4* meta, int n_new, cudaStream_t st);
 void launch_fill(float* p, size_t n, float v, cudaStream_t st);
 void launch_count_bad_diag(const DevGrid& g, int t0, int nt, int coeff_ch, int* out, cudaStream_t st);
 

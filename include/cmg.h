@@ -83,7 +83,10 @@ int cmg_grid_destroy(cmg_grid* g);
 /* setTileHost (src/HAGrid.h:526): add a tile or change its type. */
 int cmg_grid_set_tile(cmg_grid* g, int level, int i, int j, int k, int tile_type);
 /* rebuild (src/HAGrid.h:892): spawn GHOST tiles, order tiles, upload tables.
- * Channel data of tiles that survive is kept; new tiles start at zero. */
+ * Channel data and cell types of tiles that survive are kept; a LEAF or NONLEAF tile
+ * made by refinement takes them from its parent, cell by cell (PoissonTile::childTile,
+ * src/PoissonTile.h:151, as refineStep does, src/HAGrid.h:1140-1160); a new GHOST tile
+ * starts at zero.  The copy runs on the device. */
 int cmg_grid_rebuild(cmg_grid* g);
 /* iterativeRefine (src/HAGrid.h:1173) with a host callback or a built-in case. */
 int cmg_grid_iterative_refine(cmg_grid* g, cmg_level_target_fn fn, void* user, int* steps);
