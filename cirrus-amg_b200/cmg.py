@@ -47,7 +47,7 @@ EXPORTS = [
     "cmg_amg_fas_mu_cycle_solve", "cmg_gmg_damped_jacobi_solve",
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_gauss_seidel_masked", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
-    "cmg_amg_last_solve_launches", "cmg_amg_solve_batch", "cmg_amg_solver_set_storage",
+    "cmg_amg_last_solve_launches", "cmg_amg_solve_batch", "cmg_amg_solver_set_storage", "cmg_amg_divergence_without_coeff",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -124,6 +124,7 @@ def lib():
             "cmg_amg_last_solve_launches": (I, [P, P]),
             "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
             "cmg_amg_solver_set_storage": (I, [P, I]),
+            "cmg_amg_divergence_without_coeff": (I, [P, I, I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -331,6 +332,10 @@ class HADeviceGrid:
 
     def divergence(self, u_ch, coeff_ch, out_ch):
         _check(self.L.cmg_amg_divergence(self.h, u_ch, coeff_ch, out_ch), "divergence")
+
+    def divergence_without_coeff(self, u_ch, out_ch):
+        """AMGVolumeWeightedDivergenceWithoutCoeffOnLeafs (src/AMGSolver.cu:750)."""
+        _check(self.L.cmg_amg_divergence_without_coeff(self.h, u_ch, out_ch), "divergence_without_coeff")
 
     def add_gradient_to_face(self, x_ch, coeff_ch, u_ch):
         _check(self.L.cmg_amg_add_gradient_to_face(self.h, x_ch, coeff_ch, u_ch), "add_gradient_to_face")

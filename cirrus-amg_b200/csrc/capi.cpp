@@ -288,6 +288,17 @@ int cmg_amg_divergence(cmg_grid* g, int u_ch, int coeff_ch, int out_ch) {
     cmg::launch_divergence(d, G.leaf, G.nleaf, u_ch, coeff_ch, out_ch, G.stream);
     return cmg::check_cuda(cudaGetLastError(), "divergence");
 }
+int cmg_amg_divergence_without_coeff(cmg_grid* g, int u_ch, int out_ch) {
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (u_ch < 0 || u_ch + 3 > g->g.nch || !chan_ok(g, out_ch))
+        return fail(CMG_ERR_INVALID, "cmg_amg_divergence_without_coeff: channel out of range");
+    cmg::Grid& G = g->g;
+    const cmg::DevGrid d = G.dev();
+    for (int a = 0; a < 3; ++a) cmg::launch_propagate_ghost(d, 0, G.n, u_ch + a, G.stream);
+    cmg::launch_accumulate_faces(d, G.leaf, G.nleaf, u_ch, G.stream);
+    cmg::launch_divergence(d, G.leaf, G.nleaf, u_ch, -1, out_ch, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "divergence_without_coeff");
+}
 int cmg_amg_add_gradient_to_face(cmg_grid* g, int x_ch, int coeff_ch, int u_ch) {
     if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
     if (!chan_ok(g, x_ch) || u_ch < 0 || u_ch + 3 > g->g.nch || coeff_ch < 0 || coeff_ch + 4 > g->g.nch)

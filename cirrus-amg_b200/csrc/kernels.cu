@@ -989,7 +989,9 @@ __global__ void k_divergence(DevGrid g, const int* leaf, int u_ch, int coeff_ch,
         float sum = 0.0f;
         for (int a = 0; a < 3; ++a) {
             const size_t o = (size_t)t * kCells + v;
-            sum = __fmaf_rn(__fmul_rn(g.plane(u_ch + a)[o], g.plane(coeff_ch + a)[o]), h, sum);
+            const float u0 = g.plane(u_ch + a)[o];
+            // coeff_ch < 0: the coefficient-free variant (src/AMGSolver.cu:750-788), -u0 h h and u1 h h
+            sum = coeff_ch < 0 ? __fmaf_rn(__fmul_rn(-u0, h), h, sum) : __fmaf_rn(__fmul_rn(u0, g.plane(coeff_ch + a)[o]), h, sum);
             int q = t, nv = v + stride[a];
             if (l[a] == 7) {
                 q = g.nb[8 * t + 3 + a];
@@ -998,9 +1000,9 @@ __global__ void k_divergence(DevGrid g, const int* leaf, int u_ch, int coeff_ch,
             float u1 = 0.0f, c1 = 0.0f;
             if (q >= 0) {
                 u1 = g.plane(u_ch + a)[(size_t)q * kCells + nv];
-                c1 = g.plane(coeff_ch + a)[(size_t)q * kCells + nv];
+                if (coeff_ch >= 0) c1 = g.plane(coeff_ch + a)[(size_t)q * kCells + nv];
             }
-            sum = __fmaf_rn(__fmul_rn(-u1, c1), h, sum);
+            sum = coeff_ch < 0 ? __fmaf_rn(__fmul_rn(u1, h), h, sum) : __fmaf_rn(__fmul_rn(-u1, c1), h, sum);
         }
         g.plane(out_ch)[(size_t)t * kCells + v] = (g.ctype[(size_t)t * kCells + v] & dInterior) ? sum : 0.0f;
     }

@@ -142,6 +142,10 @@ int cmg_amg_cutcell_sphere_coeffs(cmg_grid* g, int coeff_ch, float R_matrix, int
 int cmg_amg_face_velocity_fourier(cmg_grid* g, int u_ch, int nmodes, const double* k, const double* amp, const double* phase);
 /* AMGVolumeWeightedDivergenceOnLeafs (src/AMGSolver.cu:790) */
 int cmg_amg_divergence(cmg_grid* g, int u_ch, int coeff_ch, int out_ch);
+/* AMGVolumeWeightedDivergenceWithoutCoeffOnLeafs (src/AMGSolver.cu:750), the form the
+ * reference's projection step calls (cirrus_cutcell/FluidEuler.cu:698, 723): faces
+ * weighted by h*h instead of the coefficients. */
+int cmg_amg_divergence_without_coeff(cmg_grid* g, int u_ch, int out_ch);
 /* AMGAddGradientToFace (src/AMGSolver.cu:680): u += grad x on faces with a
  * positive fluid ratio, LEAF and GHOST tiles (GHOST x is first set from the parents) */
 int cmg_amg_add_gradient_to_face(cmg_grid* g, int x_ch, int coeff_ch, int u_ch);

@@ -1084,7 +1084,9 @@ void og_face_velocity_fourier(og_grid* g, int u_ch, int nm, const double* kv, co
     }
 }
 /* AMGVolumeWeightedDivergenceOnLeafs (AMGSolver.cu:790-835) with its
- * PropagateToChildren and AccumulateFacesToParentsOneStep (PoissonGrid.cu:523-586). */
+ * PropagateToChildren and AccumulateFacesToParentsOneStep (PoissonGrid.cu:523-586);
+ * coeff_ch < 0: AMGVolumeWeightedDivergenceWithoutCoeffOnLeafs (AMGSolver.cu:750-788),
+ * the same sum with -u0 h h and u1 h h for the two faces of each axis. */
 void og_divergence(og_grid* g, int u_ch, int coeff_ch, int out_ch) {
     const int ALL = OG_INTERIOR | OG_DIRICHLET | OG_NEUMANN;
     for (int axis = 0; axis < 3; axis++)
@@ -1130,13 +1132,24 @@ void og_divergence(og_grid* g, int u_ch, int coeff_ch, int out_ch) {
             for (int axis = 0; axis < 3; axis++) {
                 for (int s = 0; s < 2; s++) {
                     if (!s) {
-                        float u0 = CH(g, u_ch + axis, t)[v], c0 = CH(g, coeff_ch + axis, t)[v];
-                        sum = fmaf(u0 * c0, h, sum);
+                        float u0 = CH(g, u_ch + axis, t)[v];
+                        if (coeff_ch < 0) {
+                            sum = fmaf(-u0 * h, h, sum); /* AMGSolver.cu:781, sgn = -1 */
+                        } else {
+                            float c0 = CH(g, coeff_ch + axis, t)[v];
+                            sum = fmaf(u0 * c0, h, sum);
+                        }
                     } else {
                         int nv, q = nb_cell(g, t, v, axis, +1, &nv);
                         float u1 = 0, c1 = 0;
-                        if (q >= 0) { u1 = CH(g, u_ch + axis, q)[nv]; c1 = CH(g, coeff_ch + axis, q)[nv]; }
-                        sum = fmaf(-u1 * c1, h, sum);
+                        if (q >= 0) {
+                            u1 = CH(g, u_ch + axis, q)[nv];
+                            if (coeff_ch >= 0) c1 = CH(g, coeff_ch + axis, q)[nv];
+                        }
+                        if (coeff_ch < 0)
+                            sum = fmaf(u1 * h, h, sum); /* AMGSolver.cu:781, sgn = +1 */
+                        else
+                            sum = fmaf(-u1 * c1, h, sum);
                     }
                 }
             }

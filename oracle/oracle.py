@@ -221,6 +221,9 @@ class Grid:
     def divergence(self, u_ch, coeff_ch, out_ch):
         self.L.og_divergence(self.g, u_ch, coeff_ch, out_ch)
 
+    def divergence_without_coeff(self, u_ch, out_ch):
+        self.L.og_divergence(self.g, u_ch, -1, out_ch)
+
     def add_gradient_to_face(self, x_ch, coeff_ch, u_ch):
         self.L.og_add_gradient_to_face(self.g, x_ch, coeff_ch, u_ch)
 

@@ -245,6 +245,21 @@ def test_kat_recovery_on_gpu(case_id, prm):
     assert rel < 1e-6 and err < 1e-4, (it, rel, err)
 
 
+def test_divergence_without_coeff_matches_oracle():
+    """The coefficient-free divergence the reference's projection calls (FluidEuler.cu:698)
+    on the cut-cell shell octree (GHOST and T-junction faces included), bit for bit."""
+    G, g, _ = setup_shell(shell_params(coarse=3, mid=4, fine=5))
+    rng = np.random.default_rng(9)
+    for a in range(3):
+        u = rng.standard_normal((G.num_tiles, 512)).astype(np.float32)
+        G.upload(U + a, u)
+        g.channel(U + a)[:] = u
+    G.divergence_without_coeff(U, 13)
+    g.divergence_without_coeff(U, 13)
+    m = leaf_mask(G)
+    assert np.array_equal(G.download(13)[m], g.channel(13)[m])
+
+
 def test_kat_flux_consistency_on_gpu():
     """TestAMGLaplacianAndFluxConsistency (tests/SolverTests.cu:242-361) through the C ABI, and equal to the oracle."""
     from workloads import flux_fields

@@ -325,3 +325,25 @@ def test_pure_neumann_solve_converges():
     g.channel(1)[:] = b
     it, rel = g.amg_solve(COEFF, max_iters=100, tol=1e-6, pure_neumann=True)
     assert rel < 1e-6 and it < 30
+
+
+def test_divergence_without_coeff_equals_coefficient_form_on_uniform_faces():
+    """AMGVolumeWeightedDivergenceWithoutCoeffOnLeafs (AMGSolver.cu:750-788) weights every face
+    by h*h; where every face coefficient is -h (a uniform grid, no cut cells, Dirichlet walls)
+    it must equal AMGVolumeWeightedDivergenceOnLeafs (AMGSolver.cu:790-835) bit for bit."""
+    from workloads import build_oracle
+
+    g = build_oracle(O.CASE_UNIFORM, [2, 2])
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    rng = np.random.default_rng(3)
+    u = [rng.standard_normal(g.channel(10).shape).astype(np.float32) for _ in range(3)]
+    for a in range(3):
+        g.channel(10 + a)[:] = u[a]
+    g.divergence(10, COEFF, 1)
+    for a in range(3):
+        g.channel(10 + a)[:] = u[a]
+    g.divergence_without_coeff(10, 2)
+    lv, ijk, ty = g.tiles()
+    m = ty == O.LEAF
+    assert np.array_equal(g.channel(1)[m], g.channel(2)[m])
