@@ -361,7 +361,10 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st, b
         return;
     }
     enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st, true);
-    launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
+    if (use_pipe && pipe_ok)
+        launch_restrict_pipe(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
+    else
+        launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
     // the first cluster launch of level 2 does level 2's FAS update itself when every level-2 tile is NONLEAF
     const bool fold = l - 1 == 2 && A.mu > 0 && cluster_active(G) && G.nonleaf_begin(2) == G.level_begin(2);
     if (!fold) launch_fas_save(d, G.nonleaf_begin(l - 1), G.ghost_begin(l - 1) - G.nonleaf_begin(l - 1), A.X, A.RHS, A.X0, A.coeff_ch, st);

@@ -22,6 +22,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "kernels.hpp"
 
 namespace cmg {
@@ -55,6 +57,12 @@ template <typename CT>
 struct PipeSmem {
     PipeStage<CT> st[2];
     float x[4 * kSxP];
+};
+// the restriction pass also keeps the tile's residuals
+struct PipeSmemR {
+    PipeStage<float> st[2];
+    float x[4 * kSxP];
+    float res[512];
 };
 
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
@@ -120,6 +128,8 @@ struct PipeArgs {
     double omega;
     const void* coef;  // first of the four operator planes (-x, -y, -z faces, diagonal)
     size_t cstride;    // elements from one operator plane to the next
+    float* rhs;        // restriction pass: the right-hand side plane, written on the parent tiles
+    float Rr;          // restriction pass: R_restrict
 };
 
 // neighbour descriptors of the thread's three halo cells: face r on side q >> 6
@@ -160,20 +170,20 @@ __device__ __forceinline__ void issue(PipeStage<CT>& S, const DevGrid& g, int t,
     cp_commit();
 }
 
-// the snapshot of the staged tile and one colour pass over it
+// The masked snapshot of the staged tile in SX: own cells (x is 0 on cells that are not
+// INTERIOR) and the one-cell halo, GHOST faces by the T-junction rule.  Returns the
+// thread's masked quad and the plane-0 offset s0 of its first cell.
 template <typename CT>
-__device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
-                                        const PipeArgs& A) {
-    const Quad Q(t, q);
+__device__ __forceinline__ void build_snapshot(const PipeStage<CT>& S, float* SX, const int d[3], int q, const Quad& Q, float4& xm,
+                                               int& s0) {
     const float4 xr = *reinterpret_cast<const float4*>(&S.x[4 * q]);
     const unsigned tyw = S.ty[q];
-    float4 xm;
     xm.x = (tyw & 0xffu) == dInterior ? xr.x : 0.0f;
     xm.y = ((tyw >> 8) & 0xffu) == dInterior ? xr.y : 0.0f;
     xm.z = ((tyw >> 16) & 0xffu) == dInterior ? xr.z : 0.0f;
     xm.w = ((tyw >> 24) & 0xffu) == dInterior ? xr.w : 0.0f;
     // own cells (i, j, k0 + u): plane u, slot h + 1
-    const int s0 = (Q.i + 1) * kSxI + (Q.j + 1) * kSxJ + (Q.k0 >> 2) + 1;
+    s0 = (Q.i + 1) * kSxI + (Q.j + 1) * kSxJ + (Q.k0 >> 2) + 1;
     SX[s0] = xm.x;
     SX[s0 + kSxP] = xm.y;
     SX[s0 + 2 * kSxP] = xm.z;
@@ -205,54 +215,125 @@ __device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const
         }
     }
     __syncthreads();
-    const float4 b = *reinterpret_cast<const float4*>(&S.b[4 * q]);
-    const float4 dg = Coef<CT>::ld4(&S.d[4 * q]);
-    const float4 a0 = Coef<CT>::ld4(&S.c0[4 * q]);
-    const float4 a1 = Coef<CT>::ld4(&S.c1[4 * q]);
-    const float4 a2 = Coef<CT>::ld4(&S.c2[4 * q]);
+}
+
+// The operator of the thread's quad: diagonal, -x/-y/-z faces, and the +x/+y faces and the
+// +z face of the quad's last cell.
+struct QuadOps {
+    float4 dg, a0, a1, a2, px, py;
+    float pz3;
+};
+template <typename CT>
+__device__ __forceinline__ void load_ops(const PipeStage<CT>& S, int q, const Quad& Q, QuadOps& o) {
+    o.dg = Coef<CT>::ld4(&S.d[4 * q]);
+    o.a0 = Coef<CT>::ld4(&S.c0[4 * q]);
+    o.a1 = Coef<CT>::ld4(&S.c1[4 * q]);
+    o.a2 = Coef<CT>::ld4(&S.c2[4 * q]);
     // +x faces: the -x faces of the cells at i + 1 (thread q + 16), or from the +x neighbour on row i = 7
-    const float4 px = Q.i < 7 ? Coef<CT>::ld4(&S.c0[4 * (q + 16)])
-                              : make_float4(Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0], 0), Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 1], 1),
-                                            Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 2], 0), Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 3], 1));
+    o.px = Q.i < 7 ? Coef<CT>::ld4(&S.c0[4 * (q + 16)])
+                   : make_float4(Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0], 0), Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 1], 1),
+                                 Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 2], 0), Coef<CT>::face(S.c0h[Q.j * 8 + Q.k0 + 3], 1));
     // +y faces: the -y faces at j + 1 (thread q + 2), or from the +y neighbour on row j = 7
-    const float4 py = Q.j < 7 ? Coef<CT>::ld4(&S.c1[4 * (q + 2)])
-                              : make_float4(Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0], 0), Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 1], 1),
-                                            Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 2], 0), Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 3], 1));
+    o.py = Q.j < 7 ? Coef<CT>::ld4(&S.c1[4 * (q + 2)])
+                   : make_float4(Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0], 0), Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 1], 1),
+                                 Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 2], 0), Coef<CT>::face(S.c1h[Q.i * 8 + Q.k0 + 3], 1));
     // +z face of the last cell of the quad: the next quad's first -z face, or the +z neighbour's
-    const float pz3 = Q.k0 == 0 ? Coef<CT>::at(&S.c2[4 * (q + 1)]) : Coef<CT>::face(S.c2h[Q.i * 8 + Q.j], 0);
+    o.pz3 = Q.k0 == 0 ? Coef<CT>::at(&S.c2[4 * (q + 1)]) : Coef<CT>::face(S.c2h[Q.i * 8 + Q.j], 0);
+}
+
+// negativeLap (src/AMGSolver.cu:346-382) of own cell u: diag*x, then -x,+x,-y,+y,-z,+z; the
+// k neighbours inside the quad are the thread's own cells
+__device__ __forceinline__ float quad_neg_lap(const float* SX, const QuadOps& o, const float4& xm, int s0, int u) {
+    const float dd = f4get(o.dg, u);
+    if (dd == 0.0f) return 0.0f;
+    const int c = s0 + u * kSxP;
+    const float xmz = u > 0 ? f4get(xm, u - 1) : SX[s0 - 1 + 3 * kSxP];
+    const float xpz = u < 3 ? f4get(xm, u + 1) : SX[s0 + 1];
+    const float cpz = u < 3 ? f4get(o.a2, u + 1) : o.pz3;
+    float ax = __fmul_rn(f4get(xm, u), dd);
+    ax = __fmaf_rn(f4get(o.a0, u), SX[c - kSxI], ax);
+    ax = __fmaf_rn(f4get(o.px, u), SX[c + kSxI], ax);
+    ax = __fmaf_rn(f4get(o.a1, u), SX[c - kSxJ], ax);
+    ax = __fmaf_rn(f4get(o.py, u), SX[c + kSxJ], ax);
+    ax = __fmaf_rn(f4get(o.a2, u), xmz, ax);
+    ax = __fmaf_rn(cpz, xpz, ax);
+    return ax;
+}
+
+// one colour pass over the staged tile
+template <typename CT>
+__device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
+                                        const PipeArgs& A) {
+    const Quad Q(t, q);
+    float4 xm;
+    int s0;
+    build_snapshot(S, SX, d, q, Q, xm, s0);
+    const float4 xr = *reinterpret_cast<const float4*>(&S.x[4 * q]);
+    const unsigned tyw = S.ty[q];
+    const float4 b = *reinterpret_cast<const float4*>(&S.b[4 * q]);
+    QuadOps o;
+    load_ops(S, q, Q, o);
     float4 out = xr;
     const int p = (Q.i + Q.j + Q.k0 + A.color) & 1;  // own cells of this colour: u = p, p + 2
 #pragma unroll
     for (int hh = 0; hh < 2; ++hh) {
         const int u = p + 2 * hh;
-        const float dd = f4get(dg, u);
-        float ax = 0.0f;
-        if (dd != 0.0f) {
-            // negativeLap (src/AMGSolver.cu:346-382): diag*x, then -x,+x,-y,+y,-z,+z; the k
-            // neighbours inside the quad are the thread's own cells of the other colour
-            const int c = s0 + u * kSxP;
-            const float xmz = u > 0 ? f4get(xm, u - 1) : SX[s0 - 1 + 3 * kSxP];
-            const float xpz = u < 3 ? f4get(xm, u + 1) : SX[s0 + 1];
-            const float cpz = u < 3 ? f4get(a2, u + 1) : pz3;
-            ax = __fmul_rn(f4get(xm, u), dd);
-            ax = __fmaf_rn(f4get(a0, u), SX[c - kSxI], ax);
-            ax = __fmaf_rn(f4get(px, u), SX[c + kSxI], ax);
-            ax = __fmaf_rn(f4get(a1, u), SX[c - kSxJ], ax);
-            ax = __fmaf_rn(f4get(py, u), SX[c + kSxJ], ax);
-            ax = __fmaf_rn(f4get(a2, u), xmz, ax);
-            ax = __fmaf_rn(cpz, xpz, ax);
-        }
+        const float ax = quad_neg_lap(SX, o, xm, s0, u);
         const bool in = ((tyw >> (8 * u)) & 0xffu) & dInterior;
-        const float delta = in ? div_exact(__fsub_rn(f4get(b, u), ax), dd) : 0.0f;
+        const float delta = in ? div_exact(__fsub_rn(f4get(b, u), ax), f4get(o.dg, u)) : 0.0f;
         const float xs = f4get(xm, u);
         f4set(out, u, A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega));
     }
     st4(X + Q.base, out);
 }
-template <typename CT>
+
+// ResidualAndRestrictAMG128Kernel (src/AMGSolver.cu:896-960) of the staged tile into its
+// parent: rhs = R * sum of the 8 children's residuals, x = their mean (0 unless the parent
+// cell is INTERIOR), summed in the order of the per-tile kernel (tile_restrict)
+__device__ __forceinline__ void process_restrict(const PipeStage<float>& S, float* SX, float* res, const DevGrid& g, int t, float* X,
+                                                 float* RHS, const int d[3], int q, float Rr) {
+    const Quad Q(t, q);
+    float4 xm;
+    int s0;
+    build_snapshot(S, SX, d, q, Q, xm, s0);
+    const float4 b = *reinterpret_cast<const float4*>(&S.b[4 * q]);
+    QuadOps o;
+    load_ops(S, q, Q, o);
+    float4 r;
+    r.x = __fsub_rn(b.x, quad_neg_lap(SX, o, xm, s0, 0));
+    r.y = __fsub_rn(b.y, quad_neg_lap(SX, o, xm, s0, 1));
+    r.z = __fsub_rn(b.z, quad_neg_lap(SX, o, xm, s0, 2));
+    r.w = __fsub_rn(b.w, quad_neg_lap(SX, o, xm, s0, 3));
+    *reinterpret_cast<float4*>(&res[4 * q]) = r;
+    __syncthreads();
+    if (q < 64) {
+        const int f0 = (q >> 4) * 2, f1 = ((q >> 2) & 3) * 2, f2 = (q & 3) * 2;
+        float rs = 0.0f, xs = 0.0f;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    rs = __fadd_rn(rs, res[cell_index(f0 + ii, f1 + jj, f2 + kk)]);
+                    xs = __fadd_rn(xs, SX[sxp(f0 + ii, f1 + jj, f2 + kk)]);
+                }
+        const int p = __ldg(g.nb + 8 * t + 6);
+        if (p >= 0) {
+            const int4 m = __ldg(g.meta + t);
+            const size_t po = (size_t)p * kCells + cell_index(parent_local(m.y, f0), parent_local(m.z, f1), parent_local(m.w, f2));
+            RHS[po] = __fmul_rn(rs, Rr);
+            X[po] = (g.ctype[po] & dInterior) ? __fmul_rn(xs, 0.125f) : 0.0f;
+        }
+    }
+}
+
+// MODE 0: one red-black colour pass; MODE 1: residual and restriction into the parents
+template <typename CT, int MODE>
 __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const float* B, PipeArgs A) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
-    PipeSmem<CT>& sm = *reinterpret_cast<PipeSmem<CT>*>(pipe_smem);
+    using Smem = typename std::conditional<MODE == 0, PipeSmem<CT>, PipeSmemR>::type;
+    Smem& sm = *reinterpret_cast<Smem*>(pipe_smem);
     const int q = threadIdx.x, side = q >> 6;
     const int stride = gridDim.x, tend = A.t0 + A.nt;
     int tcur = A.t0 + blockIdx.x;
@@ -276,7 +357,10 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const f
         if (tn2 < tend) load_desc(g, tn2, side, dn2);
         cp_wait_prev();
         __syncthreads();
-        process(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
+        if constexpr (MODE == 0)
+            process(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
+        else
+            process_restrict(sm.st[s], sm.x, sm.res, g, tcur, X, A.rhs, dcur, q, A.Rr);
         __syncthreads();
         if (tnext >= tend) break;
         tcur = tnext;
@@ -302,22 +386,26 @@ int g_pipe_blocks = 0;  // resident blocks of k_gs_pipe on the device
 
 template <typename CT>
 bool set_pipe_smem() {
-    return cudaFuncSetAttribute(k_gs_pipe<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess;
+    return cudaFuncSetAttribute(k_gs_pipe<CT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess;
 }
+int g_restrict_blocks = 0;  // resident blocks of the restriction pass
 
 }  // namespace
 
 int gs_pipe_init() {
     if (!set_pipe_smem<float>() || !set_pipe_smem<__nv_bfloat16>() || !set_pipe_smem<__half>()) return 0;
-    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaFuncSetAttribute(k_gs_pipe<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmemR)) != cudaSuccess) return 0;
+    int dev = 0, sms = 0, per_sm = 0, per_sm_r = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float>, 128, sizeof(PipeSmem<float>)) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float, 0>, 128, sizeof(PipeSmem<float>)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_gs_pipe<float, 1>, 128, sizeof(PipeSmemR)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     g_pipe_blocks = sms * per_sm;
-    return g_pipe_blocks;
+    g_restrict_blocks = sms * per_sm_r;
+    return per_sm_r > 0 ? g_pipe_blocks : 0;
 }
 
 size_t coeff16_bytes(const DevGrid& g) { return (size_t)4 * g.n * kCells * 2; }
@@ -343,18 +431,38 @@ void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, 
     A.exact = ((double)A.om == omega);
     A.omega = omega;
     A.cstride = (size_t)g.n * kCells;
+    A.rhs = nullptr;
+    A.Rr = 1.0f;
     const int blocks = nt < g_pipe_blocks ? nt : g_pipe_blocks;
     note_kernel_launch();
     if (storage == kStorageFP32) {
         A.coef = g.plane(coeff_ch);
-        k_gs_pipe<float><<<blocks, 128, sizeof(PipeSmem<float>), st>>>(g, X, B, A);
+        k_gs_pipe<float, 0><<<blocks, 128, sizeof(PipeSmem<float>), st>>>(g, X, B, A);
     } else if (storage == kStorageBF16) {
         A.coef = coeff16;
-        k_gs_pipe<__nv_bfloat16><<<blocks, 128, sizeof(PipeSmem<__nv_bfloat16>), st>>>(g, X, B, A);
+        k_gs_pipe<__nv_bfloat16, 0><<<blocks, 128, sizeof(PipeSmem<__nv_bfloat16>), st>>>(g, X, B, A);
     } else {
         A.coef = coeff16;
-        k_gs_pipe<__half><<<blocks, 128, sizeof(PipeSmem<__half>), st>>>(g, X, B, A);
+        k_gs_pipe<__half, 0><<<blocks, 128, sizeof(PipeSmem<__half>), st>>>(g, X, B, A);
     }
+}
+
+void launch_restrict_pipe(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st) {
+    if (nt <= 0) return;
+    PipeArgs A;
+    A.t0 = t0;
+    A.nt = nt;
+    A.color = 0;
+    A.om = 1.0f;
+    A.exact = 1;
+    A.omega = 1.0;
+    A.coef = g.plane(coeff_ch);
+    A.cstride = (size_t)g.n * kCells;
+    A.rhs = RHS;
+    A.Rr = Rr;
+    const int blocks = nt < g_restrict_blocks ? nt : g_restrict_blocks;
+    note_kernel_launch();
+    k_gs_pipe<float, 1><<<blocks, 128, sizeof(PipeSmemR), st>>>(g, X, RHS, A);
 }
 
 }  // namespace cmg

@@ -49,6 +49,9 @@ constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;
 void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st,
                     int storage = kStorageFP32, const void* coeff16 = nullptr);
 size_t coeff16_bytes(const DevGrid& g);
+// ResidualAndRestrictAMG128Kernel on tiles t0..t0+nt-1 with the same prefetching pipeline
+// (x masked to INTERIOR cells, as inside the cycle); equals launch_restrict bit for bit.
+void launch_restrict_pipe(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st);
 void launch_coeff16(const DevGrid& g, int coeff_ch, int storage, void* out, cudaStream_t st);
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float R_restrict, cudaStream_t st);
