@@ -48,6 +48,7 @@ EXPORTS = [
     "cmg_amg_solve",
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_gauss_seidel_masked", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
     "cmg_amg_last_solve_launches", "cmg_amg_solve_batch", "cmg_amg_solver_set_storage", "cmg_amg_divergence_without_coeff",
+    "cmg_grid_gather_device_tiles", "cmg_grid_scatter_device_tiles",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -125,6 +126,8 @@ def lib():
             "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
             "cmg_amg_solver_set_storage": (I, [P, I]),
             "cmg_amg_divergence_without_coeff": (I, [P, I, I]),
+            "cmg_grid_gather_device_tiles": (I, [P, P, S, I, I, I]),
+            "cmg_grid_scatter_device_tiles": (I, [P, P, S, I, I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -301,6 +304,17 @@ class HADeviceGrid:
         buf = (ctypes.c_uint8 * n.value)()
         _check(self.L.cmg_grid_dump_hagr(self.h, buf, n.value, ctypes.byref(n)), "dumpBinaryBlob")
         return bytes(buf)
+
+    def gather_device_tiles(self, tile_ptrs, first_ch, num_ch, with_types=True):
+        """Channels (and cell types) from the reference's own device tiles (PoissonTile<float,15>),
+        tile_ptrs[t] = device address of the tile that is tile t of this grid."""
+        arr = (ctypes.c_void_p * max(len(tile_ptrs), 1))(*tile_ptrs)
+        _check(self.L.cmg_grid_gather_device_tiles(self.h, arr, 44880, first_ch, num_ch, int(with_types)), "gather_device_tiles")
+
+    def scatter_device_tiles(self, tile_ptrs, first_ch, num_ch):
+        """Channels of this grid written back into the reference's device tiles."""
+        arr = (ctypes.c_void_p * max(len(tile_ptrs), 1))(*tile_ptrs)
+        _check(self.L.cmg_grid_scatter_device_tiles(self.h, arr, 44880, first_ch, num_ch), "scatter_device_tiles")
 
     def calc_cell_types_from_leafs(self):
         """CalcCellTypesFromLeafs (src/PoissonGrid.cu:923): NONLEAF and GHOST cell types from the LEAF ones."""

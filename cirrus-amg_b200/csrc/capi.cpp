@@ -184,6 +184,42 @@ int cmg_grid_download_cell_types(cmg_grid* g, uint8_t* host, size_t count) {
     CKC(cudaStreamSynchronize(g->g.stream));
     return CMG_OK;
 }
+// the caller's tile address list on the device (one upload per call)
+static int upload_tile_ptrs(cmg_grid* g, const void* const* tile_ptrs, size_t tile_bytes, int first_ch, int num_ch, const char* who) {
+    cmg::Grid& G = g->g;
+    if (!tile_ptrs || tile_bytes != cmg::kRefTileBytes || first_ch < 0 || num_ch < 0 || first_ch + num_ch > std::min(G.nch, 15))
+        return fail(CMG_ERR_INVALID, (std::string(who) + ": bad argument (tile_bytes must be 44880, channels within 0..14)").c_str());
+    for (int t = 0; t < G.n; ++t)
+        if (!tile_ptrs[t] || (reinterpret_cast<uintptr_t>(tile_ptrs[t]) & 15))
+            return fail(CMG_ERR_INVALID, (std::string(who) + ": a tile address is null or not 16-byte aligned").c_str());
+    if (G.n > G.tile_ptrs_cap) {
+        if (G.tile_ptrs) cudaFree(G.tile_ptrs);
+        G.tile_ptrs = nullptr;
+        G.tile_ptrs_cap = 0;
+        CKC(cudaMalloc(&G.tile_ptrs, sizeof(void*) * G.n));
+        G.tile_ptrs_cap = G.n;
+    }
+    CKC(cudaMemcpyAsync(G.tile_ptrs, tile_ptrs, sizeof(void*) * G.n, cudaMemcpyHostToDevice, G.stream));
+    return CMG_OK;
+}
+int cmg_grid_gather_device_tiles(cmg_grid* g, const void* const* tile_ptrs, size_t tile_bytes, int first_ch, int num_ch, int with_types) {
+    GUARD_BEGIN
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_gather_device_tiles: grid not built");
+    if (int rc = upload_tile_ptrs(g, tile_ptrs, tile_bytes, first_ch, num_ch, "cmg_grid_gather_device_tiles")) return rc;
+    cmg::launch_gather_tiles(g->g.dev(), g->g.tile_ptrs, first_ch, num_ch, with_types != 0, g->g.stream);
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return cmg::check_cuda(cudaGetLastError(), "gather_device_tiles");
+    GUARD_END
+}
+int cmg_grid_scatter_device_tiles(cmg_grid* g, const void* const* tile_ptrs, size_t tile_bytes, int first_ch, int num_ch) {
+    GUARD_BEGIN
+    if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_scatter_device_tiles: grid not built");
+    if (int rc = upload_tile_ptrs(g, tile_ptrs, tile_bytes, first_ch, num_ch, "cmg_grid_scatter_device_tiles")) return rc;
+    cmg::launch_scatter_tiles(g->g.dev(), g->g.tile_ptrs, first_ch, num_ch, g->g.stream);
+    CKC(cudaStreamSynchronize(g->g.stream));
+    return cmg::check_cuda(cudaGetLastError(), "scatter_device_tiles");
+    GUARD_END
+}
 int cmg_grid_fill_channel(cmg_grid* g, int ch, float value) {
     if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_grid_fill_channel: grid not built");
     if (!chan_ok(g, ch)) return fail(CMG_ERR_INVALID, "channel out of range");

@@ -42,6 +42,7 @@ Grid::~Grid() {
     dfree(spheres);
     dfree(modes);
     dfree(dot_out);
+    dfree(tile_ptrs);
 }
 
 static unsigned long long tile_key(const TileRec& r) {

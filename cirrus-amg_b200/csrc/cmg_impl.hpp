@@ -39,6 +39,8 @@ struct Grid {
     unsigned long long version = 0;
     float* spheres = nullptr;  // device scratch for set-up calls
     double* modes = nullptr;
+    void** tile_ptrs = nullptr;  // device copy of a caller's tile address list (reference tiles)
+    int tile_ptrs_cap = 0;
     double* dot_out = nullptr;
 
     Grid(float h0, int num_levels, int num_channels) : topo(h0, num_levels), nch(num_channels) {}

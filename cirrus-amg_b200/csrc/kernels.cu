@@ -1059,6 +1059,25 @@ __global__ void k_remap_types(const uint8_t* src, uint8_t* dst, const int2* src_
     for (int v = threadIdx.x; v < kCells; v += blockDim.x)
         dst[(size_t)t * kCells + v] = (o.x >= 0) ? src[(size_t)o.x * kCells + remap_cell(m, o.y, v)] : 0;
 }
+// Channels of the reference's device tiles (PoissonTile<float,15>: mData[15][736] floats,
+// mCellType[512] at byte 44352) to and from the channel planes, one block per (tile, channel).
+constexpr int kRefChannelStride = 736;
+constexpr size_t kRefTypesOffset = 44352;
+__global__ void k_gather_tiles(DevGrid g, const unsigned char* const* ptrs, int first) {
+    const int t = blockIdx.x, c = first + (int)blockIdx.y;
+    const float4* src = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(ptrs[t]) + (size_t)c * kRefChannelStride);
+    reinterpret_cast<float4*>(g.plane(c) + (size_t)t * kCells)[threadIdx.x] = src[threadIdx.x];
+}
+__global__ void k_gather_types(DevGrid g, const unsigned char* const* ptrs) {
+    const int t = blockIdx.x;
+    const uint4* src = reinterpret_cast<const uint4*>(ptrs[t] + kRefTypesOffset);
+    reinterpret_cast<uint4*>(g.ctype + (size_t)t * kCells)[threadIdx.x] = src[threadIdx.x];
+}
+__global__ void k_scatter_tiles(DevGrid g, unsigned char* const* ptrs, int first) {
+    const int t = blockIdx.x, c = first + (int)blockIdx.y;
+    float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(ptrs[t]) + (size_t)c * kRefChannelStride);
+    dst[threadIdx.x] = reinterpret_cast<const float4*>(g.plane(c) + (size_t)t * kCells)[threadIdx.x];
+}
 __global__ void k_fill(float* p, size_t n, float v) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -1327,6 +1346,14 @@ void launch_remap(const float* src, float* dst, const int2* src_of_new, const in
 }
 void launch_remap_types(const uint8_t* src, uint8_t* dst, const int2* src_of_new, const int4* meta, int n_new, cudaStream_t st) {
     if (n_new > 0) count_launch(), k_remap_types<<<n_new, 128, 0, st>>>(src, dst, src_of_new, meta);
+}
+void launch_gather_tiles(const DevGrid& g, const void* const* ptrs, int first, int num, bool types, cudaStream_t st) {
+    const auto P = reinterpret_cast<const unsigned char* const*>(ptrs);
+    if (g.n > 0 && num > 0) count_launch(), k_gather_tiles<<<dim3(g.n, num), 128, 0, st>>>(g, P, first);
+    if (g.n > 0 && types) count_launch(), k_gather_types<<<g.n, 32, 0, st>>>(g, P);
+}
+void launch_scatter_tiles(const DevGrid& g, void* const* ptrs, int first, int num, cudaStream_t st) {
+    if (g.n > 0 && num > 0) count_launch(), k_scatter_tiles<<<dim3(g.n, num), 128, 0, st>>>(g, reinterpret_cast<unsigned char* const*>(ptrs), first);
 }
 void launch_fill(float* p, size_t n, float v, cudaStream_t st) {
     if (n > 0) count_launch(), k_fill<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p, n, v);

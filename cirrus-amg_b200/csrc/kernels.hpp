@@ -121,6 +121,11 @@ void launch_divergence(const DevGrid& g, const int* leaf, int nleaf, int u_ch, i
 void launch_gradient(const DevGrid& g, const float* X, int coeff_ch, int u_ch, cudaStream_t st);
 // channel data and cell types of a new tile order: from the old tile src_of_new[t].x, s =
 // src_of_new[t].y levels up (0: the same tile; -1 in .x: zero); meta: the new tiles' meta
+// channels [first, first+num) (and the cell types) of the reference's device tiles
+// (PoissonTile<float,15>) to and from the planes; ptrs: a device array of g.n tile addresses
+constexpr size_t kRefTileBytes = 44880;
+void launch_gather_tiles(const DevGrid& g, const void* const* ptrs, int first, int num, bool types, cudaStream_t st);
+void launch_scatter_tiles(const DevGrid& g, void* const* ptrs, int first, int num, cudaStream_t st);
 void launch_remap(const float* src, float* dst, const int2* src_of_new, const int4* meta, int n_new, int nch, int n_old, cudaStream_t st);
 void launch_remap_types(const uint8_t* src, uint8_t* dst, const int2* src_of_new, const int4* meta, int n_new, cudaStream_t st);
 void launch_fill(float* p, size_t n, float v, cudaStream_t st);

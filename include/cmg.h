@@ -123,6 +123,18 @@ int cmg_grid_calc_cell_types_from_leafs(cmg_grid* g);
  * further channels.  Dumping writes every tile with min(num_channels, 15) channels;
  * with buf == NULL it only reports the size. */
 int cmg_grid_load_hagr(const uint8_t* blob, size_t size, int num_channels, cmg_grid** out);
+/* A view of the reference's own device tiles, for a caller that keeps its HADeviceGrid
+ * (src/HAGrid.h:357-406): every tile is a PoissonTile<float,15> in device memory
+ * (src/PoissonTile.h:34-39: float mData[15][736], cell values in the first 512 of each
+ * channel; uint8 mCellType[512] at byte 44352; 44880 bytes), reached through the device
+ * pointer of its HATileInfo.  tile_ptrs (host array) holds, for each tile of g in the order
+ * of cmg_grid_tiles, the device address of the reference tile with the same level and
+ * coordinate; tile_bytes must be 44880.  Gather copies channels [first_ch, first_ch+num_ch)
+ * (and, with with_types, the cell types) from those tiles into g; scatter writes the
+ * channels of g back into them.  Both run on the device on g's stream and leave every
+ * other byte of the tiles untouched; only the pointer list crosses from the host. */
+int cmg_grid_gather_device_tiles(cmg_grid* g, const void* const* tile_ptrs, size_t tile_bytes, int first_ch, int num_ch, int with_types);
+int cmg_grid_scatter_device_tiles(cmg_grid* g, const void* const* tile_ptrs, size_t tile_bytes, int first_ch, int num_ch);
 int cmg_grid_dump_hagr(cmg_grid* g, uint8_t* buf, size_t capacity, size_t* size);
 int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* params, int nparams);
 /* stream used by every later call on this grid (NULL = legacy default) */
