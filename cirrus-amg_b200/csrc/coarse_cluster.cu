@@ -114,10 +114,16 @@ __device__ __forceinline__ float nlap(float d, float x, float cmx, float xmx, fl
     s = __fmaf_rn(cpz, xpz, s);
     return s;
 }
-// one Gauss-Seidel update (src/AMGSolver.cu:868-875)
+// one Gauss-Seidel update (src/AMGSolver.cu:868-875); kExact: omega is a float, so x + delta * omega
+// in double rounds to the single fused multiply-add (a compile-time choice keeps the other form
+// off every update's dependency chain)
+template <bool kExact>
 __device__ __forceinline__ float gs_update(float xs, float rhs, float ax, float d, double yd, bool interior, const ClusterArgs& A) {
     const float delta = interior ? div_by_recip(__fsub_rn(rhs, ax), d, yd) : 0.0f;
-    return A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega);
+    if constexpr (kExact)
+        return __fmaf_rn(delta, A.om, xs);
+    else
+        return (float)((double)xs + (double)delta * A.omega);
 }
 
 // Shared memory.  Octant CTA: x (the level-2 octant, halo from the neighbouring
@@ -211,7 +217,7 @@ __device__ __forceinline__ void blk_publish_all(const Blk& o, float* xs, const P
 // four cells are not neighbours of one another, so every neighbour load comes first, then
 // the four updates, then the stores: the updates overlap instead of each waiting on the
 // previous cell's shared-memory store.
-template <int Q0, int Q1, int Q2, int Q3, bool kRemote>
+template <int Q0, int Q1, int Q2, int Q3, bool kRemote, bool kExact>
 __device__ __forceinline__ void blk_gs_colour(Blk& o, float* xs, const double* yd, const Peers& pr, const ClusterArgs& A) {
     float v0[3], v1[3], v2[3], v3[3];
     blk_outer<Q0>(o, xs, v0);
@@ -221,21 +227,21 @@ __device__ __forceinline__ void blk_gs_colour(Blk& o, float* xs, const double* y
     const double y0 = yd[Q0 * kClThreads + threadIdx.x], y1 = yd[Q1 * kClThreads + threadIdx.x];
     const double y2 = yd[Q2 * kClThreads + threadIdx.x], y3 = yd[Q3 * kClThreads + threadIdx.x];
     const float a0 = blk_nlap_v<Q0>(o, v0), a1 = blk_nlap_v<Q1>(o, v1), a2 = blk_nlap_v<Q2>(o, v2), a3 = blk_nlap_v<Q3>(o, v3);
-    o.x[Q0] = gs_update(o.x[Q0], o.b[Q0], a0, o.d[Q0], y0, (o.in >> Q0) & 1u, A);
-    o.x[Q1] = gs_update(o.x[Q1], o.b[Q1], a1, o.d[Q1], y1, (o.in >> Q1) & 1u, A);
-    o.x[Q2] = gs_update(o.x[Q2], o.b[Q2], a2, o.d[Q2], y2, (o.in >> Q2) & 1u, A);
-    o.x[Q3] = gs_update(o.x[Q3], o.b[Q3], a3, o.d[Q3], y3, (o.in >> Q3) & 1u, A);
+    o.x[Q0] = gs_update<kExact>(o.x[Q0], o.b[Q0], a0, o.d[Q0], y0, (o.in >> Q0) & 1u, A);
+    o.x[Q1] = gs_update<kExact>(o.x[Q1], o.b[Q1], a1, o.d[Q1], y1, (o.in >> Q1) & 1u, A);
+    o.x[Q2] = gs_update<kExact>(o.x[Q2], o.b[Q2], a2, o.d[Q2], y2, (o.in >> Q2) & 1u, A);
+    o.x[Q3] = gs_update<kExact>(o.x[Q3], o.b[Q3], a3, o.d[Q3], y3, (o.in >> Q3) & 1u, A);
     blk_publish<Q0, kRemote>(o, xs, pr);
     blk_publish<Q1, kRemote>(o, xs, pr);
     blk_publish<Q2, kRemote>(o, xs, pr);
     blk_publish<Q3, kRemote>(o, xs, pr);
 }
-template <bool kRemote>
+template <bool kRemote, bool kExact>
 __device__ __forceinline__ void blk_gs_pass(Blk& o, float* xs, const double* yd, const Peers& pr, int color, const ClusterArgs& A) {
     if (color == 0)
-        blk_gs_colour<0, 3, 5, 6, kRemote>(o, xs, yd, pr, A);
+        blk_gs_colour<0, 3, 5, 6, kRemote, kExact>(o, xs, yd, pr, A);
     else
-        blk_gs_colour<1, 2, 4, 7, kRemote>(o, xs, yd, pr, A);
+        blk_gs_colour<1, 2, 4, 7, kRemote, kExact>(o, xs, yd, pr, A);
 }
 // ResidualAndRestrictAMG128Kernel (src/AMGSolver.cu:896-960) of the block into its parent cell:
 // rhs = R * sum of the 8 residuals, x = mean of the 8 x (0 unless the parent is INTERIOR)
@@ -363,6 +369,7 @@ __global__ void __launch_bounds__(kClThreads) k_cluster_pack(DevGrid g, const __
 // ---------------------------------------------------------------------------
 // The cluster step
 // ---------------------------------------------------------------------------
+template <bool kExact>
 __global__ void __launch_bounds__(kClThreads, 1)
     k_cluster_step(DevGrid g, const __grid_constant__ ClusterArgs A, const ClPack* packs, float* X, float* RHS, float* X0) {
     extern __shared__ __align__(16) unsigned char cl_smem[];
@@ -457,9 +464,9 @@ __global__ void __launch_bounds__(kClThreads, 1)
 
         // ---- level 2: pre-smoothing ----
         for (int it = 0; it < A.level_iters; ++it) {
-            blk_gs_pass<true>(o, xs, yd, pr, 0, A);
+            blk_gs_pass<true, kExact>(o, xs, yd, pr, 0, A);
             cluster.sync();
-            blk_gs_pass<true>(o, xs, yd, pr, 1, A);
+            blk_gs_pass<true, kExact>(o, xs, yd, pr, 1, A);
             cluster.sync();
         }
         // ---- residual, restriction into the coarse CTA's level-1 grid ----
@@ -480,9 +487,9 @@ __global__ void __launch_bounds__(kClThreads, 1)
         cluster.sync();
         // ---- level 2: post-smoothing ----
         for (int it = 0; it < A.level_iters; ++it) {
-            blk_gs_pass<true>(o, xs, yd, pr, 1, A);
+            blk_gs_pass<true, kExact>(o, xs, yd, pr, 1, A);
             cluster.sync();
-            blk_gs_pass<true>(o, xs, yd, pr, 0, A);
+            blk_gs_pass<true, kExact>(o, xs, yd, pr, 0, A);
             cluster.sync();
         }
 #pragma unroll
@@ -531,9 +538,9 @@ __global__ void __launch_bounds__(kClThreads, 1)
         for (int rep = 0; rep < A.mu; ++rep) {
             // ---- FASMuCycleStep of level 1 ----
             for (int it = 0; it < A.level_iters; ++it) {
-                blk_gs_pass<false>(o, xs, yd, pr, 0, A);
+                blk_gs_pass<false, kExact>(o, xs, yd, pr, 0, A);
                 __syncthreads();
-                blk_gs_pass<false>(o, xs, yd, pr, 1, A);
+                blk_gs_pass<false, kExact>(o, xs, yd, pr, 1, A);
                 __syncthreads();
             }
             {
@@ -563,7 +570,7 @@ __global__ void __launch_bounds__(kClThreads, 1)
                             if (par == (h ^ half)) {
                                 const float ax = nlap(d0, x0, c0mx, sm.x0[q0 - 240], c0px, sm.x0[q0 + 240], c0my, sm.x0[q0 - 24], c0py,
                                                       sm.x0[q0 + 24], c0mz, sm.x0[q0 - 1], c0pz, sm.x0[q0 + 1]);
-                                x0 = gs_update(x0, b0, ax, d0, y0, in0, A);
+                                x0 = gs_update<kExact>(x0, b0, ax, d0, y0, in0, A);
                                 sm.x0[q0] = x0;
                             }
                         }
@@ -572,9 +579,9 @@ __global__ void __launch_bounds__(kClThreads, 1)
             blk_publish_all<false>(o, xs, pr);
             __syncthreads();
             for (int it = 0; it < A.level_iters; ++it) {
-                blk_gs_pass<false>(o, xs, yd, pr, 1, A);
+                blk_gs_pass<false, kExact>(o, xs, yd, pr, 1, A);
                 __syncthreads();
-                blk_gs_pass<false>(o, xs, yd, pr, 0, A);
+                blk_gs_pass<false, kExact>(o, xs, yd, pr, 0, A);
                 __syncthreads();
             }
         }
@@ -647,15 +654,18 @@ cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* t
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
     note_kernel_launch();
-    return cudaLaunchKernelEx(&cfg, k_cluster_step, g, A, reinterpret_cast<const ClPack*>(pack), X, RHS, X0);
+    if (A.exact) return cudaLaunchKernelEx(&cfg, k_cluster_step<true>, g, A, reinterpret_cast<const ClPack*>(pack), X, RHS, X0);
+    return cudaLaunchKernelEx(&cfg, k_cluster_step<false>, g, A, reinterpret_cast<const ClPack*>(pack), X, RHS, X0);
 }
 
 bool cluster_step_supported() {
     int dev = 0, cc = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&cc, cudaDevAttrClusterLaunch, dev) != cudaSuccess || !cc) return false;
-    if (cudaFuncSetAttribute(k_cluster_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_cluster_step, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_cluster_step<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
@@ -671,7 +681,7 @@ bool cluster_step_supported() {
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, k_cluster_step, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_cluster_step<true>, &cfg) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }

@@ -260,8 +260,9 @@ __device__ __forceinline__ float quad_neg_lap(const float* SX, const QuadOps& o,
     return ax;
 }
 
-// one colour pass over the staged tile
-template <typename CT>
+// one colour pass over the staged tile; kExact: omega is a float and the update is one fused
+// multiply-add (compile-time, so the double form stays off the dependency chain)
+template <typename CT, bool kExact>
 __device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
                                         const PipeArgs& A) {
     const Quad Q(t, q);
@@ -282,7 +283,10 @@ __device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const
         const bool in = ((tyw >> (8 * u)) & 0xffu) & dInterior;
         const float delta = in ? div_exact(__fsub_rn(f4get(b, u), ax), f4get(o.dg, u)) : 0.0f;
         const float xs = f4get(xm, u);
-        f4set(out, u, A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega));
+        if constexpr (kExact)
+            f4set(out, u, __fmaf_rn(delta, A.om, xs));
+        else
+            f4set(out, u, (float)((double)xs + (double)delta * A.omega));
     }
     st4(X + Q.base, out);
 }
@@ -329,7 +333,7 @@ __device__ __forceinline__ void process_restrict(const PipeStage<float>& S, floa
 }
 
 // MODE 0: one red-black colour pass; MODE 1: residual and restriction into the parents
-template <typename CT, int MODE>
+template <typename CT, int MODE, bool kExact = true>
 __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const float* B, PipeArgs A) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
     using Smem = typename std::conditional<MODE == 0, PipeSmem<CT>, PipeSmemR>::type;
@@ -358,7 +362,7 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const f
         cp_wait_prev();
         __syncthreads();
         if constexpr (MODE == 0)
-            process(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
+            process<CT, kExact>(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
         else
             process_restrict(sm.st[s], sm.x, sm.res, g, tcur, X, A.rhs, dcur, q, A.Rr);
         __syncthreads();
@@ -386,7 +390,15 @@ int g_pipe_blocks = 0;  // resident blocks of k_gs_pipe on the device
 
 template <typename CT>
 bool set_pipe_smem() {
-    return cudaFuncSetAttribute(k_gs_pipe<CT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess;
+    return cudaFuncSetAttribute(k_gs_pipe<CT, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess &&
+           cudaFuncSetAttribute(k_gs_pipe<CT, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess;
+}
+template <typename CT>
+void launch_pass(int blocks, cudaStream_t st, const DevGrid& g, float* X, const float* B, const PipeArgs& A) {
+    if (A.exact)
+        k_gs_pipe<CT, 0, true><<<blocks, 128, sizeof(PipeSmem<CT>), st>>>(g, X, B, A);
+    else
+        k_gs_pipe<CT, 0, false><<<blocks, 128, sizeof(PipeSmem<CT>), st>>>(g, X, B, A);
 }
 int g_restrict_blocks = 0;  // resident blocks of the restriction pass
 
@@ -398,7 +410,7 @@ int gs_pipe_init() {
     int dev = 0, sms = 0, per_sm = 0, per_sm_r = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float, 0>, 128, sizeof(PipeSmem<float>)) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float, 0, true>, 128, sizeof(PipeSmem<float>)) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_gs_pipe<float, 1>, 128, sizeof(PipeSmemR)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -437,13 +449,13 @@ void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, 
     note_kernel_launch();
     if (storage == kStorageFP32) {
         A.coef = g.plane(coeff_ch);
-        k_gs_pipe<float, 0><<<blocks, 128, sizeof(PipeSmem<float>), st>>>(g, X, B, A);
+        launch_pass<float>(blocks, st, g, X, B, A);
     } else if (storage == kStorageBF16) {
         A.coef = coeff16;
-        k_gs_pipe<__nv_bfloat16, 0><<<blocks, 128, sizeof(PipeSmem<__nv_bfloat16>), st>>>(g, X, B, A);
+        launch_pass<__nv_bfloat16>(blocks, st, g, X, B, A);
     } else {
         A.coef = coeff16;
-        k_gs_pipe<__half, 0><<<blocks, 128, sizeof(PipeSmem<__half>), st>>>(g, X, B, A);
+        launch_pass<__half>(blocks, st, g, X, B, A);
     }
 }
 
