@@ -494,9 +494,10 @@ def run_batched(args, rank, world, local_rank):
     solvers = [make_solver(cmg) for _ in specs]
     n = len(grids)
     infos = [G.info() for G in grids]
-    streams = [torch.cuda.Stream(device=dev) for _ in range(BATCH_STREAMS)]
+    nstreams = max(1, args.streams)
+    streams = [torch.cuda.Stream(device=dev) for _ in range(nstreams)]
     for i, G in enumerate(grids):
-        G.set_stream(streams[i % BATCH_STREAMS].cuda_stream)
+        G.set_stream(streams[i % nstreams].cuda_stream)
     sargs = (SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
 
     def one_batch(b_host=None, x_host=None):
@@ -563,7 +564,7 @@ def run_batched(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {
                 "workload": WORKLOADS["batched64"], "method": "plain FP32 FAS mu-cycle (mu=2) MG-PCG, FP64 dots, batched",
-                "instances": n, "streams": BATCH_STREAMS, "tiles": int(sum(i[0] for i in infos)),
+                "instances": n, "streams": nstreams, "tiles": int(sum(i[0] for i in infos)),
                 "leaf_cells": int(sum(i[2] for i in infos)) * 512, "finest_levels": sorted({int(i[1]) for i in infos}),
                 "pcg_iters_mean": round(float(np.mean(its)), 2), "pcg_iters_max": int(max(its)), "rel_residual_max": max(rels),
                 "solve_ms_p50": per[len(per) // 2], "solve_ms_p99": per[min(len(per) - 1, int(0.99 * len(per)))],
@@ -638,6 +639,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="sphere", choices=sorted(WORKLOADS))
+    ap.add_argument("--streams", type=int, default=BATCH_STREAMS, help="streams of the batched workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
