@@ -49,6 +49,9 @@ EXPORTS = [
     "cmg_amg_solve_host", "cmg_amg_gauss_seidel", "cmg_amg_gauss_seidel_masked", "cmg_amg_fas_mu_cycle", "cmg_amg_last_solve_ms",
     "cmg_amg_last_solve_launches", "cmg_amg_solve_batch", "cmg_amg_solver_set_storage", "cmg_amg_divergence_without_coeff",
     "cmg_grid_gather_device_tiles", "cmg_grid_scatter_device_tiles",
+    "cmg_learned_create", "cmg_learned_destroy", "cmg_learned_num_params", "cmg_learned_get_params",
+    "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
+    "cmg_learned_train", "cmg_amg_solver_set_learned", "cmg_amg_solver_learned_status",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -128,6 +131,17 @@ def lib():
             "cmg_amg_divergence_without_coeff": (I, [P, I, I]),
             "cmg_grid_gather_device_tiles": (I, [P, P, S, I, I, I]),
             "cmg_grid_scatter_device_tiles": (I, [P, P, S, I, I]),
+            "cmg_learned_create": (I, [I, ctypes.c_ulonglong, P]),
+            "cmg_learned_destroy": (I, [P]),
+            "cmg_learned_num_params": (I, [P, P]),
+            "cmg_learned_get_params": (I, [P, P, I]),
+            "cmg_learned_set_params": (I, [P, P, I]),
+            "cmg_learned_set_samples": (I, [P, I, P, P, P, P]),
+            "cmg_learned_forward": (I, [P, I, I, P]),
+            "cmg_learned_gradient": (I, [P, I, I, P, P]),
+            "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
+            "cmg_amg_solver_set_learned": (I, [P, P]),
+            "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -398,6 +412,18 @@ class AMGSolver:
         reference's arithmetic), "bf16" or "fp16" (mixed precision)."""
         _check(self.L.cmg_amg_solver_set_storage(self.h, STORAGE[storage]), "set_storage")
 
+    def set_learned(self, net=None):
+        """Use `net` (a LearnedNet, its current parameters) as the finest-level smoother:
+        flexible PCG judged by the true residual, plain fallback.  None: the plain solve."""
+        _check(self.L.cmg_amg_solver_set_learned(self.h, net.h if net is not None else None), "set_learned")
+
+    def learned_status(self):
+        """(true relative residual, fell back to the plain solve, learned iterations) of the last solve."""
+        tr, fb, it = ctypes.c_double(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(self.L.cmg_amg_solver_learned_status(self.h, ctypes.byref(tr), ctypes.byref(fb), ctypes.byref(it)),
+               "learned_status")
+        return tr.value, bool(fb.value), it.value
+
     def _sync_params(self):
         _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")
 
@@ -452,6 +478,67 @@ class AMGSolver:
         n = ctypes.c_longlong(0)
         _check(self.L.cmg_amg_last_solve_launches(self.h, ctypes.byref(n)), "last_solve_launches")
         return n.value
+
+
+class LearnedNet:
+    """The learned finest-level smoother's per-tile network (BF16 tensor cores), its
+    parameters, Adam state and training samples on the device (no reference counterpart)."""
+
+    def __init__(self, hidden=16, seed=0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        _check(self.L.cmg_learned_create(int(hidden), ctypes.c_ulonglong(seed), ctypes.byref(h)), "cmg_learned_create")
+        self.h = h
+        self.hidden = hidden
+        n = ctypes.c_int(0)
+        _check(self.L.cmg_learned_num_params(self.h, ctypes.byref(n)), "num_params")
+        self.num_params = n.value
+        self.num_samples = 0
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.cmg_learned_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def params(self):
+        p = np.zeros(self.num_params, np.float32)
+        _check(self.L.cmg_learned_get_params(self.h, _p(p), p.size), "get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self.L.cmg_learned_set_params(self.h, _p(p), p.size), "set_params")
+
+    def set_samples(self, rho, diag, types, target=None):
+        """Tiles of 512 cells: rho, diag (float32), types (uint8), target (float32 or None)."""
+        rho = np.ascontiguousarray(rho, dtype=np.float32).reshape(-1, 512)
+        diag = np.ascontiguousarray(diag, dtype=np.float32).reshape(-1, 512)
+        types = np.ascontiguousarray(types, dtype=np.uint8).reshape(-1, 512)
+        tg = None if target is None else np.ascontiguousarray(target, dtype=np.float32).reshape(-1, 512)
+        _check(self.L.cmg_learned_set_samples(self.h, rho.shape[0], _p(rho), _p(diag), _p(types),
+                                              _p(tg) if tg is not None else None), "set_samples")
+        self.num_samples = rho.shape[0]
+
+    def forward(self, first=0, n=None):
+        n = self.num_samples - first if n is None else n
+        out = np.zeros((n, 512), np.float32)
+        _check(self.L.cmg_learned_forward(self.h, first, n, _p(out)), "forward")
+        return out
+
+    def gradient(self, first=0, n=None):
+        n = self.num_samples - first if n is None else n
+        loss = ctypes.c_double(0)
+        g = np.zeros(self.num_params, np.float32)
+        _check(self.L.cmg_learned_gradient(self.h, first, n, ctypes.byref(loss), _p(g)), "gradient")
+        return loss.value, g
+
+    def train(self, epochs, batch=256, lr=1e-3, seed=0):
+        losses = np.zeros(max(epochs, 1), np.float32)
+        _check(self.L.cmg_learned_train(self.h, epochs, batch, float(lr), ctypes.c_ulonglong(seed), _p(losses)), "train")
+        return losses[:epochs]
 
 
 class _GeometricSolver(AMGSolver):

@@ -2,6 +2,7 @@
 #include "cmg.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -13,6 +14,9 @@
 struct cmg_grid {
     cmg::Grid g;
     cmg_grid(float h0, int nl, int nc) : g(h0, nl, nc) {}
+};
+struct cmg_learned {
+    cmg::Net n;
 };
 struct cmg_amg_solver {
     cmg::Solver s;
@@ -427,6 +431,75 @@ int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage) {
     static_assert(CMG_STORAGE_BF16 == cmg::kStorageBF16 && CMG_STORAGE_FP16 == cmg::kStorageFP16, "storage codes");
     s->s.storage = storage;
     return CMG_OK;
+}
+int cmg_learned_create(int hidden, unsigned long long seed, cmg_learned** out) {
+    GUARD_BEGIN
+    if (!out || (hidden != 8 && hidden != 16)) return fail(CMG_ERR_INVALID, "cmg_learned_create: hidden must be 8 or 16");
+    *out = nullptr;
+    auto* n = new cmg_learned();
+    if (int rc = n->n.init(hidden, seed)) {
+        delete n;
+        return rc;
+    }
+    *out = n;
+    return 0;
+    GUARD_END
+}
+int cmg_learned_destroy(cmg_learned* net) {
+    delete net;
+    return 0;
+}
+int cmg_learned_num_params(cmg_learned* net, int* n) {
+    if (!net || !n) return fail(CMG_ERR_INVALID, "cmg_learned_num_params: null argument");
+    *n = net->n.np;
+    return 0;
+}
+int cmg_learned_get_params(cmg_learned* net, float* host, int n) {
+    if (!net || !host || n != net->n.np) return fail(CMG_ERR_INVALID, "cmg_learned_get_params: bad argument");
+    return net->n.get_params(host);
+}
+int cmg_learned_set_params(cmg_learned* net, const float* host, int n) {
+    if (!net || !host || n != net->n.np) return fail(CMG_ERR_INVALID, "cmg_learned_set_params: bad argument");
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(host[i])) return fail(CMG_ERR_NONFINITE, "cmg_learned_set_params: non-finite parameter");
+    return net->n.set_params(host);
+}
+int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target) {
+    GUARD_BEGIN
+    if (!net || n < 0 || (n > 0 && (!rho || !diag || !types))) return fail(CMG_ERR_INVALID, "cmg_learned_set_samples: bad argument");
+    return net->n.set_samples(n, rho, diag, types, target);
+    GUARD_END
+}
+int cmg_learned_forward(cmg_learned* net, int first, int n, float* out) {
+    if (!net || !out || first < 0 || n <= 0 || first + n > net->n.ns) return fail(CMG_ERR_INVALID, "cmg_learned_forward: bad sample range");
+    return net->n.forward(first, n, out);
+}
+int cmg_learned_gradient(cmg_learned* net, int first, int n, double* loss, float* grad) {
+    GUARD_BEGIN
+    if (!net || first < 0 || n <= 0 || first + n > net->n.ns) return fail(CMG_ERR_INVALID, "cmg_learned_gradient: bad sample range");
+    return net->n.gradient(first, n, loss, grad);
+    GUARD_END
+}
+int cmg_learned_train(cmg_learned* net, int epochs, int batch, float lr, unsigned long long seed, float* epoch_loss) {
+    GUARD_BEGIN
+    if (!net || epochs < 0 || batch <= 0 || !(lr > 0.0f)) return fail(CMG_ERR_INVALID, "cmg_learned_train: bad argument");
+    if (net->n.ns <= 0) return fail(CMG_ERR_STATE, "cmg_learned_train: no samples");
+    return net->n.train(epochs, batch, lr, seed, epoch_loss);
+    GUARD_END
+}
+int cmg_amg_solver_set_learned(cmg_amg_solver* s, cmg_learned* net) {
+    GUARD_BEGIN
+    if (!s) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_learned: null solver");
+    if (net && s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_solver_set_learned: not an AMG solver");
+    return s->s.set_learned(net ? &net->n : nullptr);
+    GUARD_END
+}
+int cmg_amg_solver_learned_status(cmg_amg_solver* s, double* true_rel, int* fell_back, int* learned_iters) {
+    if (!s) return fail(CMG_ERR_INVALID, "cmg_amg_solver_learned_status: null solver");
+    if (true_rel) *true_rel = s->s.last_true_rel;
+    if (fell_back) *fell_back = s->s.last_fallback;
+    if (learned_iters) *learned_iters = s->s.last_learned_iters;
+    return 0;
 }
 int cmg_amg_solve(cmg_amg_solver* s, cmg_grid* g, int verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
                   int pure_neumann, int* iters, double* rel_res) {

@@ -210,6 +210,10 @@ Solver::~Solver() {
     dfree(s);
     if (cluster_pack) cudaFree(cluster_pack);
     dfree(coeff16);
+    dfree(lnet.pack);
+    dfree(lnet.bias);
+    dfree(aux);
+    dfree(bsave);
     if (h_s) cudaFreeHost(h_s);
     if (h_bar) cudaFreeHost(h_bar);
     dfree(bar);
@@ -308,6 +312,47 @@ void Solver::enqueue_cluster_pack(Grid& G, cudaStream_t st) const {
     int tile1[8], tile2[64];
     coarse_tiles(G, tile1, tile2);
     launch_cluster_pack(G.dev(), tile1, tile2, coeff_ch, cluster_pack, st);
+}
+
+// The solver keeps its own copy of the net's packed operands.  Graphs captured with the
+// learned smoother read that copy, so a later set_learned with the same width only
+// refreshes its contents; a new width reallocates it and drops the captured graphs.
+int Solver::set_learned(const Net* net) {
+    if (!net) {
+        lnet.enabled = false;
+        return 0;
+    }
+    if (!lnet.pack || lnet.H != net->H) {
+        dfree(lnet.pack);
+        dfree(lnet.bias);
+        lnet.H = 0;
+        CK(cudaMalloc(&lnet.pack, sizeof(uint16_t) * (size_t)net_pack_elems(net->H)));
+        CK(cudaMalloc(&lnet.bias, sizeof(float) * 2 * net->H));
+        lnet.H = net->H;
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+        graphs.clear();
+    }
+    CK(cudaStreamSynchronize(net->st));
+    CK(cudaMemcpy(lnet.pack, net->pack, sizeof(uint16_t) * (size_t)net_pack_elems(net->H), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(lnet.bias, net->bias, sizeof(float) * 2 * net->H, cudaMemcpyDeviceToDevice));
+    lnet.enabled = true;
+    return 0;
+}
+
+int Solver::ensure_aux(const Grid& G) {
+    const size_t need = (size_t)G.n * kCells;
+    if (aux_cap >= need) return 0;
+    dfree(aux);
+    dfree(bsave);
+    aux = bsave = nullptr;
+    aux_cap = 0;
+    CK(cudaMalloc(&aux, sizeof(float) * need));
+    CK(cudaMalloc(&bsave, sizeof(float) * need));
+    aux_cap = need;
+    // captured graphs hold the old pointer
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    return 0;
 }
 
 int Solver::ensure_coeff16(const Grid& G) {
@@ -509,8 +554,21 @@ int Solver::damped_jacobi_solve(Grid& G, int max_iters, double tol, float omega,
 }
 
 void Solver::enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const {
-    if (kind == kAMG) enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
-    else enqueue_geo_vcycle(G, G.plane(4), G.plane(1), G.plane(3), k.level_iters, k.coarsest_iters, st);
+    if (kind != kAMG) {
+        enqueue_geo_vcycle(G, G.plane(4), G.plane(1), G.plane(3), k.level_iters, k.coarsest_iters, st);
+    } else if (!learned_active()) {
+        enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
+    } else {
+        // learned: the cycle saves its FAS x0 in aux so that Ap (channel 3) survives for the
+        // flexible beta; then rho = r - A z on the finest LEAF tiles and z += net(rho) there
+        MuArgs A = mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters);
+        A.X0 = aux;
+        enqueue_mu_cycle(G, A, st);
+        const int L = G.max_level(), t0 = G.level_begin(L), nf = G.nonleaf_begin(L) - t0;
+        launch_leaf_apply(G.dev(), G.leaf + (G.nleaf - nf), nf, G.plane(4), aux, coeff_ch, false, scratch(), st);
+        launch_net_forward(lnet.H, G.plane(1), aux, G.plane(coeff_ch + 3), G.ctype, nullptr, t0, nf, lnet.pack, lnet.bias, G.plane(4), false,
+                           st);
+    }
 }
 
 // AMGSolver::FASMuCycle (src/AMGSolver.cu:1279-1292): zero x everywhere, then the top step
@@ -563,7 +621,8 @@ void Solver::enqueue_tail(Grid& G, const Key& k, cudaStream_t st) const {
     const ReduceScratch rs = scratch();
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
     enqueue_precond(G, k, st);
-    launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(4), kDotBeta, nullptr, rs, st);
+    if (learned_active()) launch_dot_flex(d, G.leaf, G.nleaf, G.plane(1), G.plane(4), G.plane(3), rs, st);
+    else launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(4), kDotBeta, nullptr, rs, st);
     launch_p_update(d, G.leaf, G.nleaf, G.plane(2), G.plane(4), rs, st);
 }
 
@@ -639,8 +698,13 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     if (int rc = validate_solver_topology(G)) return rc;
     if (int rc = ensure_scratch(G.nleaf)) return rc;
     if (int rc = ensure_coeff16(G)) return rc;
+    if (learned_active()) {
+        if (int rc = ensure_aux(G)) return rc;
+    }
     Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu,
-          (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0) | (storage << 4), omega};
+          (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0) | (storage << 4) |
+              (learned_active() ? 256 : 0),
+          omega};
     Plan plan{};
     if (use_graph) {
         auto it = graphs.find(k);
@@ -737,8 +801,48 @@ int Solver::solve_finish(bool verbose, int* iters, double* rel) {
 
 int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, bool pure_neumann,
                   int* iters, double* rel) {
+    const bool learned = learned_active() && G.n > 0 && G.nleaf > 0;
+    last_fallback = 0;
+    last_true_rel = -1.0;
+    if (learned) {
+        if (int rc = ensure_aux(G)) return rc;
+        CK(cudaMemcpyAsync(bsave, G.plane(1), sizeof(float) * (size_t)G.n * kCells, cudaMemcpyDeviceToDevice, G.stream));
+    }
     if (int rc = solve_begin(G, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann)) return rc;
-    return solve_finish(verbose, iters, rel);
+    int it = 0;
+    double rr = 0.0;
+    const int rc = solve_finish(verbose, &it, &rr);
+    const bool converged = h_s->converged != 0 || h_s->rr0 == 0.0;
+    if (learned) {
+        // the true residual judges the learned solve: |b - A x| / |b| on LEAF tiles
+        const DevGrid d = G.dev();
+        launch_leaf_apply(d, G.leaf, G.nleaf, G.plane(0), aux, coeff_ch, false, scratch(), G.stream);
+        launch_leaf_residual(d, G.leaf, G.nleaf, bsave, aux, true, G.stream);
+        double res = 0.0, bb = 0.0;
+        if (int e = host_dot(G, G.leaf, G.nleaf, aux, aux, &res)) return e;
+        if (int e = host_dot(G, G.leaf, G.nleaf, bsave, bsave, &bb)) return e;
+        last_true_rel = bb > 0.0 ? std::sqrt(res / bb) : 0.0;
+        last_learned_iters = it;
+        const bool judged_ok = rc == 0 && std::isfinite(last_true_rel) &&
+                               (sync_stride <= 0 || (converged && last_true_rel <= kLearnedJudgeSlack * tol));
+        if (!judged_ok && rc != 2) {
+            // plain fallback from the saved right-hand side
+            const float saved_ms = last_ms;
+            CK(cudaMemcpyAsync(G.plane(1), bsave, sizeof(float) * (size_t)G.n * kCells, cudaMemcpyDeviceToDevice, G.stream));
+            learned_suspended = true;
+            int prc = solve_begin(G, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann);
+            if (prc == 0) prc = solve_finish(verbose, &it, &rr);
+            learned_suspended = false;
+            last_fallback = 1;
+            last_ms += saved_ms;
+            if (iters) *iters = it;
+            if (rel) *rel = rr;
+            return prc;
+        }
+    }
+    if (iters) *iters = it;
+    if (rel) *rel = rr;
+    return rc;
 }
 
 }  // namespace cmg

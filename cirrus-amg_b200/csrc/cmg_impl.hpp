@@ -77,6 +77,8 @@ struct MuArgs {
     float Rr, P;
 };
 
+struct Net;
+
 // AMGSolver (src/AMGSolver.h:19-75)
 struct Solver {
     int coeff_ch;
@@ -144,6 +146,24 @@ struct Solver {
     // storage of the operator planes the pipelined smoother reads (kStorageFP32/BF16/FP16);
     // 16-bit modes read coeff16, a copy made once per solve or cycle by enqueue_operand_pack
     int storage = kStorageFP32;
+    // learned finest-level smoother (a copy of a Net's packed operands); H = 0: none
+    struct LearnedOps {
+        int H = 0;
+        bool enabled = false;
+        void* pack = nullptr;
+        float* bias = nullptr;
+    } lnet;
+    bool learned_suspended = false;  // the plain fallback solve of a learned solve
+    float* aux = nullptr;            // plane-sized scratch of the learned solve
+    float* bsave = nullptr;          // its right-hand side, kept for the true-residual judge
+    size_t aux_cap = 0;
+    double last_true_rel = -1.0;
+    int last_fallback = 0, last_learned_iters = 0;
+    bool learned_active() const { return lnet.enabled && kind == kAMG && !learned_suspended; }
+    int set_learned(const Net* net);
+    // a learned solve passes when its true relative residual is at most this many times tol
+    static constexpr double kLearnedJudgeSlack = 4.0;
+    int ensure_aux(const Grid& G);
     void* coeff16 = nullptr;
     size_t coeff16_cap = 0;
     int ensure_coeff16(const Grid& G);
@@ -172,6 +192,38 @@ struct Solver {
         Plan plan{};
         long long stream_launches = -1;
     } pending;
+};
+
+// The learned finest-level smoother's network (learned.cu) with its parameters, Adam state
+// and training samples on the device.
+struct Net {
+    int H = 0, np = 0;
+    float* p = nullptr;  // fp32 parameters
+    float* m = nullptr;  // Adam moments
+    float* v = nullptr;
+    int adam_step = 0;
+    void* pack = nullptr;  // bf16 operands made from p
+    float* bias = nullptr;
+    int ns = 0;  // training samples: tiles of 512 cells
+    float* rho = nullptr;
+    float* diag = nullptr;
+    uint8_t* types = nullptr;
+    float* target = nullptr;
+    float* grad = nullptr;  // per batch slot
+    float* loss = nullptr;  // per sample
+    float* gsum = nullptr;
+    int* idx = nullptr;
+    int batch_cap = 0;
+    cudaStream_t st = nullptr;
+    ~Net();
+    int init(int hidden, unsigned long long seed);
+    int set_params(const float* host);
+    int get_params(float* host);
+    int set_samples(int n, const float* rho, const float* diag, const uint8_t* types, const float* target);
+    int forward(int first, int n, float* out_host);
+    int gradient(int first, int n, double* loss_out, float* grad_host);
+    int train(int epochs, int batch, float lr, unsigned long long seed, float* epoch_loss);
+    int ensure_batch(int nb);
 };
 
 int check_cuda(cudaError_t e, const char* what);

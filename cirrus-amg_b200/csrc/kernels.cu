@@ -609,6 +609,32 @@ __global__ void __launch_bounds__(128) k_dot(const int* leaf, const float* A, co
     }
 }
 
+// Flexible CG with a non-linear preconditioner (Polak-Ribiere): with r_new = r_old - alpha Ap,
+// beta = z.(r_new - r_old) / gamma_old = -alpha (Ap.z) / gamma_old; gamma = r_new.z.
+__global__ void __launch_bounds__(128) k_dot_flex(const int* leaf, const float* R, const float* Z, const float* AP, ReduceScratch rs) {
+    __shared__ double red[4];
+    const int t = leaf[blockIdx.x];
+    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
+    const float4 z = ld4(Z + base);
+    const double rz = block_sum128(dot4(ld4(R + base), z), red);
+    const double az = block_sum128(dot4(ld4(AP + base), z), red);
+    if (threadIdx.x == 0) {
+        rs.partial[blockIdx.x] = rz;
+        rs.partial2[blockIdx.x] = az;
+    }
+    if (last_block(&rs.s->counter[2])) {
+        const double g = sum_partials(rs.partial, gridDim.x, red);
+        const double a = sum_partials(rs.partial2, gridDim.x, red);
+        if (threadIdx.x == 0) {
+            PcgScalars* s = rs.s;
+            s->gamma_old = s->gamma;
+            s->gamma = g;
+            s->beta = -s->alpha * a / s->gamma_old;
+            s->counter[2] = 0;
+        }
+    }
+}
+
 // p = z + beta p on INTERIOR cells (src/AMGSolver.cu:1525-1536)
 __global__ void __launch_bounds__(128) k_p_update(DevGrid g, const int* leaf, float* P, const float* Z, ReduceScratch rs) {
     const int t = leaf[blockIdx.x];
@@ -1232,6 +1258,11 @@ void launch_dot(const DevGrid& g, const int* leaf, int nleaf, const float* A, co
                 cudaStream_t st) {
     (void)g;
     if (nleaf > 0) count_launch(), k_dot<<<nleaf, 128, 0, st>>>(leaf, A, B, mode, out, rs);
+}
+void launch_dot_flex(const DevGrid& g, const int* leaf, int nleaf, const float* R, const float* Z, const float* AP, ReduceScratch rs,
+                     cudaStream_t st) {
+    (void)g;
+    if (nleaf > 0) count_launch(), k_dot_flex<<<nleaf, 128, 0, st>>>(leaf, R, Z, AP, rs);
 }
 void launch_p_update(const DevGrid& g, const int* leaf, int nleaf, float* P, const float* Z, ReduceScratch rs, cudaStream_t st) {
     if (nleaf > 0) count_launch(), k_p_update<<<nleaf, 128, 0, st>>>(g, leaf, P, Z, rs);

@@ -49,6 +49,22 @@ constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;
 void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st,
                     int storage = kStorageFP32, const void* coeff16 = nullptr);
 size_t coeff16_bytes(const DevGrid& g);
+// learned finest-level smoother: per-tile conv net, hidden width H = 8 or 16 (learned.cu)
+int net_params(int H);      // fp32 parameters
+int net_pack_elems(int H);  // bf16 elements of the packed operands
+bool net_init();
+void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaStream_t st);
+// samples s < ns are tiles (idx ? idx[s] : t0 + s) of the planes; rho = r - az (az may be null);
+// out[t] += (S/D) f (or = with overwrite) on INTERIOR cells
+void launch_net_forward(int H, const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
+                        const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st);
+void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
+                      const void* pack, const float* bias, float* grad, float* loss, cudaStream_t st);
+void launch_net_reduce_adam(const float* grad, int nb, int np, float scale, float* gout, float* p, float* m, float* v, float lr, int step,
+                            bool update, cudaStream_t st);
+// flexible-CG beta (Polak-Ribiere): gamma = r.z, beta = -alpha (Ap.z) / gamma_old
+void launch_dot_flex(const DevGrid& g, const int* leaf, int nleaf, const float* R, const float* Z, const float* AP, ReduceScratch rs,
+                     cudaStream_t st);
 // ResidualAndRestrictAMG128Kernel on tiles t0..t0+nt-1 with the same prefetching pipeline
 // (x masked to INTERIOR cells, as inside the cycle); equals launch_restrict bit for bit.
 void launch_restrict_pipe(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st);

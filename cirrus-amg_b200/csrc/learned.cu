@@ -1,0 +1,619 @@
+// Learned finest-level smoother: a per-tile 3-D convolutional network on BF16 tensor
+// cores (the reference has no counterpart; it is the learned preconditioner of the
+// learned-versus-plain comparison).
+//
+// After the FAS mu-cycle has produced z = M r, the residual it leaves on the LEAF tiles of
+// the finest level, rho = r - A z, is fed tile by tile to a small network whose output is
+// added to z on INTERIOR cells:
+//     z_t += (S_t / D_t) * f(features_t)
+// features (8 input channels, zero padding at the tile border):
+//     0: rho / S_t   (S_t = root mean square of rho over the tile's INTERIOR cells)
+//     1: INTERIOR flag   2: DIRICHLET flag   3: diagonal of A / D_t (D_t = its maximum)
+// network: conv3x3x3 8->H, bias, ReLU; conv3x3x3 H->H, bias, ReLU; conv3x3x3 H->1
+// (H = 8 or 16).  The target of f is the error the cycle leaves, d = A^-1 rho, scaled
+// by D_t / S_t; the network is trained on (rho, d) pairs made by the plain solver.
+// The preconditioner is no longer linear, so the solve runs flexible CG (Polak-Ribiere
+// beta) and judges its result by the true residual, with the plain solve as fallback.
+//
+// Every convolution is an implicit GEMM on mma.sync m16n8k16 (BF16 operands, FP32
+// accumulation): M = the tile's 512 voxels in 16-voxel fragments (two rows of 8 along
+// the innermost axis), N = output channels, K = (tap, input channel).  Activations live
+// in shared memory as a zero-padded 10^3 voxel grid, channels innermost (16 bytes per
+// 8-channel group); ldmatrix gathers the shifted rows of each tap directly, so no
+// im2col buffer exists.  With 16 channels the two 16-byte groups of a voxel swap places
+// on voxels whose bit 2 is set, which makes every 8-row ldmatrix phase conflict-free.
+// Training uses the same routine for the input gradients (a convolution with the
+// flipped, transposed kernel) and a transposed-operand GEMM (ldmatrix .trans) for the
+// weight gradients, reduced over the batch in a fixed order and applied by Adam.
+#include <cuda_bf16.h>
+
+#include <cmath>
+
+#include "kernels.hpp"
+
+namespace cmg {
+
+namespace {
+
+constexpr int kNetThreads = 128;
+constexpr int kPadVox = 1000;  // 10^3 padded voxels per tile
+
+// tap = dx*9 + dy*3 + dz (each 0..2), offset in the padded voxel grid
+__device__ __forceinline__ int tap_off(int tap) { return (tap / 9 - 1) * 100 + ((tap / 3) % 3 - 1) * 10 + (tap % 3 - 1); }
+__device__ __forceinline__ int pad_vox(int i, int j, int k) { return (i + 1) * 100 + (j + 1) * 10 + (k + 1); }
+
+// element offset of (voxel v, first channel of 8-channel group grp) in an activation buffer of CG groups
+template <int CG>
+__device__ __forceinline__ int act_off(int v, int grp) {
+    if constexpr (CG == 2) return v * 16 + ((grp ^ ((v >> 2) & 1)) << 3);
+    else return v * 8;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t a, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n" : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t a, uint32_t& r0, uint32_t& r1) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t a, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n" : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2_t(uint32_t a, uint32_t& r0, uint32_t& r1) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Convolution of one tile: acc[m][nt] += in (*) w for the 8 M-fragments of this warp.
+// in: activations with CGI 8-channel groups; w: packed weights [NTO*8 rows][ks], row = output
+// channel, column k = tap*(8*CGI) + channel (CGI == 1: two taps per 16-wide K step, tap 27
+// zero-weighted).
+template <int CGI, int NTO>
+__device__ __forceinline__ void conv_tile(const __nv_bfloat16* in, const __nv_bfloat16* w, int ks, float (&acc)[8][NTO][4]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = lane >> 3, r = lane & 7;
+    int vb[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int mt = warp * 8 + m;
+        vb[m] = pad_vox(mt >> 2, (mt & 3) * 2 + (q & 1), r);
+#pragma unroll
+        for (int nt = 0; nt < NTO; ++nt) acc[m][nt][0] = acc[m][nt][1] = acc[m][nt][2] = acc[m][nt][3] = 0.0f;
+    }
+    const uint32_t in_s = smem_u32(in);
+    const uint32_t wrow = NTO == 2 ? smem_u32(w + ((q >> 1) * 8 + r) * ks + (q & 1) * 8) : smem_u32(w + r * ks + (q & 1) * 8);
+    constexpr int kSteps = CGI == 2 ? 27 : 14;
+#pragma unroll 1
+    for (int step = 0; step < kSteps; ++step) {
+        uint32_t b[NTO][2];
+        if constexpr (NTO == 2) ldsm_x4(wrow + step * 32, b[0][0], b[0][1], b[1][0], b[1][1]);
+        else ldsm_x2(wrow + step * 32, b[0][0], b[0][1]);
+        int tap, grp;
+        if constexpr (CGI == 2) {
+            tap = step;
+            grp = q >> 1;
+        } else {
+            tap = 2 * step + (q >> 1);
+            if (tap > 26) tap = 13;  // K padding: zero weights, any finite activation
+            grp = 0;
+        }
+        const int off = tap_off(tap);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            uint32_t a[4];
+            ldsm_x4(in_s + 2 * act_off<CGI>(vb[m] + off, grp), a[0], a[1], a[2], a[3]);
+#pragma unroll
+            for (int nt = 0; nt < NTO; ++nt) mma_bf16(acc[m][nt], a, b[nt][0], b[nt][1]);
+        }
+    }
+}
+
+// Hidden-layer epilogue: forward out = relu(acc + bias); backward out = acc * (ref > 0).
+template <int NTO, bool kBwd>
+__device__ __forceinline__ void store_hidden(const float (&acc)[8][NTO][4], __nv_bfloat16* out, const __nv_bfloat16* ref,
+                                             const float* bias) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int mt = warp * 8 + m;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+            const int v = pad_vox(mt >> 2, (mt & 3) * 2 + hh, g);
+#pragma unroll
+            for (int nt = 0; nt < NTO; ++nt) {
+                const int c = nt * 8 + 2 * tq;
+                const int e = act_off<NTO>(v, nt) + 2 * tq;
+                float x0 = acc[m][nt][2 * hh], x1 = acc[m][nt][2 * hh + 1];
+                if constexpr (kBwd) {
+                    const __nv_bfloat162 rf = *reinterpret_cast<const __nv_bfloat162*>(ref + e);
+                    x0 = __bfloat162float(rf.x) > 0.0f ? x0 : 0.0f;
+                    x1 = __bfloat162float(rf.y) > 0.0f ? x1 : 0.0f;
+                } else {
+                    x0 = fmaxf(__fadd_rn(x0, bias[c]), 0.0f);
+                    x1 = fmaxf(__fadd_rn(x1, bias[c + 1]), 0.0f);
+                }
+                *reinterpret_cast<__nv_bfloat162*>(out + e) = __floats2bfloat162_rn(x0, x1);
+            }
+        }
+    }
+}
+
+// Output epilogue (one real output channel): ys[cell] = acc column 0.
+__device__ __forceinline__ void store_output(const float (&acc)[8][1][4], float* ys) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+    if (tq != 0) return;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int mt = warp * 8 + m;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) ys[(mt >> 2) * 64 + ((mt & 3) * 2 + hh) * 8 + g] = acc[m][0][2 * hh];
+    }
+}
+
+// Weight gradient of one tile: gw[n][tap][c] = sum over voxels v of a[v + tap][c] * d[v][n],
+// as a GEMM with M = (tap, c), N = n, K = voxels (ldmatrix .trans on both operands).
+// a: CGA channel groups; d: NTD groups; only the first nout columns are stored.
+template <int CGA, int NTD>
+__device__ __forceinline__ void wgrad_tile(const __nv_bfloat16* a, const __nv_bfloat16* d, float* __restrict__ gw, int nout) {
+    constexpr int kMT = CGA == 2 ? 27 : 14;
+    constexpr int kPerWarp = (kMT + 3) / 4;
+    constexpr int kCin = 8 * CGA;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = lane >> 3, r = lane & 7, g = lane >> 2, tq = lane & 3;
+    float acc[kPerWarp][NTD][4];
+#pragma unroll
+    for (int mi = 0; mi < kPerWarp; ++mi)
+#pragma unroll
+        for (int nt = 0; nt < NTD; ++nt) acc[mi][nt][0] = acc[mi][nt][1] = acc[mi][nt][2] = acc[mi][nt][3] = 0.0f;
+    int aoff[kPerWarp], agrp[kPerWarp];
+#pragma unroll
+    for (int mi = 0; mi < kPerWarp; ++mi) {
+        const int mt = warp + 4 * mi;
+        int tap;
+        if constexpr (CGA == 2) {
+            tap = mt;
+            agrp[mi] = q & 1;
+        } else {
+            tap = 2 * mt + (q & 1);
+            agrp[mi] = 0;
+        }
+        if (tap > 26) tap = 13;  // padding rows (not stored)
+        aoff[mi] = tap_off(tap);
+    }
+    const uint32_t a_s = smem_u32(a), d_s = smem_u32(d);
+#pragma unroll 1
+    for (int ks = 0; ks < 32; ++ks) {
+        const int i = ks >> 2, j0 = (ks & 3) * 2;
+        uint32_t b[NTD][2];
+        if constexpr (NTD == 2) {
+            const int v = pad_vox(i, j0 + (q & 1), r);
+            ldsm_x4_t(d_s + 2 * act_off<2>(v, q >> 1), b[0][0], b[0][1], b[1][0], b[1][1]);
+        } else {
+            const int v = pad_vox(i, j0 + (q & 1), r);
+            ldsm_x2_t(d_s + 2 * act_off<1>(v, 0), b[0][0], b[0][1]);
+        }
+        const int vb = pad_vox(i, j0 + (q >> 1), r);
+#pragma unroll
+        for (int mi = 0; mi < kPerWarp; ++mi) {
+            if (warp + 4 * mi >= kMT) continue;
+            uint32_t af[4];
+            ldsm_x4_t(a_s + 2 * act_off<CGA>(vb + aoff[mi], agrp[mi]), af[0], af[1], af[2], af[3]);
+#pragma unroll
+            for (int nt = 0; nt < NTD; ++nt) mma_bf16(acc[mi][nt], af, b[nt][0], b[nt][1]);
+        }
+    }
+#pragma unroll
+    for (int mi = 0; mi < kPerWarp; ++mi) {
+        const int mt = warp + 4 * mi;
+        if (mt >= kMT) continue;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+            int tap, c;
+            if constexpr (CGA == 2) {
+                tap = mt;
+                c = g + 8 * hh;
+            } else {
+                tap = 2 * mt + hh;
+                c = g;
+            }
+            if (tap > 26) continue;
+#pragma unroll
+            for (int nt = 0; nt < NTD; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int n = nt * 8 + 2 * tq + e;
+                    if (n < nout) gw[(n * 27 + tap) * kCin + c] = acc[mi][nt][2 * hh + e];
+                }
+        }
+    }
+}
+
+// bias gradient: db[c] = sum over the tile's voxels of d[v][c] (fixed order)
+template <int CG>
+__device__ __forceinline__ void bias_grad(const __nv_bfloat16* d, float* red, float* __restrict__ gb) {
+    constexpr int H = 8 * CG, kParts = kNetThreads / H;
+    const int c = threadIdx.x % H, part = threadIdx.x / H;
+    float s = 0.0f;
+    for (int cell = part; cell < kCells; cell += kParts) {
+        const int v = pad_vox(cell >> 6, (cell >> 3) & 7, cell & 7);
+        s += __bfloat162float(d[act_off<CG>(v, c >> 3) + (c & 7)]);
+    }
+    red[part * H + c] = s;
+    __syncthreads();
+    if (threadIdx.x < H) {
+        float t = 0.0f;
+        for (int p = 0; p < kParts; ++p) t += red[p * H + threadIdx.x];
+        gb[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+// fixed-order block reductions over 128 threads
+__device__ __forceinline__ float block_sum_f(float v, float* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    const float r = (red[0] + red[1]) + (red[2] + red[3]);
+    __syncthreads();
+    return r;
+}
+__device__ __forceinline__ float block_max_f(float v, float* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    const float r = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
+    __syncthreads();
+    return r;
+}
+
+// Where one tile's inputs come from: sample s is tile (idx ? idx[s] : t0 + s) of planes of
+// 512 floats; rho = r - az (az may be null: r already holds rho).
+struct NetIn {
+    const float* r;
+    const float* az;
+    const float* diag;
+    const uint8_t* types;
+    const float* target;
+    const int* idx;
+    int t0;
+};
+
+struct Staged {
+    float rho[4];
+    float tgt[4];
+    bool in[4];
+    float S, D;  // S = 0: nothing to do on this tile
+};
+
+// Stage one tile's features into x0 (8-channel layout); thread q owns cells 4q..4q+3.
+__device__ __forceinline__ Staged stage_features(const NetIn& I, int s, __nv_bfloat16* x0, float* red) {
+    Staged o;
+    const int t = I.idx ? I.idx[s] : I.t0 + s;
+    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
+    float4 r4 = ldcg4(I.r + base);
+    if (I.az) {
+        const float4 a4 = ldcg4(I.az + base);
+        r4 = make_float4(__fsub_rn(r4.x, a4.x), __fsub_rn(r4.y, a4.y), __fsub_rn(r4.z, a4.z), __fsub_rn(r4.w, a4.w));
+    }
+    const float4 dg = ldcg4(I.diag + base);
+    const uchar4 ty = ldt4(I.types + base);
+    const float rr[4] = {r4.x, r4.y, r4.z, r4.w}, dd[4] = {dg.x, dg.y, dg.z, dg.w};
+    const uint8_t tt[4] = {ty.x, ty.y, ty.z, ty.w};
+    float ss = 0.0f, dm = 0.0f, cnt = 0.0f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        o.in[u] = (tt[u] & dInterior) != 0;
+        o.rho[u] = o.in[u] ? rr[u] : 0.0f;
+        ss = __fmaf_rn(o.rho[u], o.rho[u], ss);
+        if (o.in[u]) {
+            dm = fmaxf(dm, fabsf(dd[u]));
+            cnt += 1.0f;
+        }
+    }
+    if (I.target) {
+        const float4 tg = ldcg4(I.target + base);
+        o.tgt[0] = tg.x, o.tgt[1] = tg.y, o.tgt[2] = tg.z, o.tgt[3] = tg.w;
+    }
+    const float sum = block_sum_f(ss, red), n = block_sum_f(cnt, red);
+    o.D = block_max_f(dm, red);
+    o.S = (n > 0.0f && sum > 0.0f && o.D > 0.0f) ? sqrtf(sum / n) : 0.0f;
+    if (o.S == 0.0f) return o;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int cell = 4 * threadIdx.x + u;
+        const int v = pad_vox(cell >> 6, (cell >> 3) & 7, cell & 7);
+        __nv_bfloat162 f[4];
+        f[0] = __floats2bfloat162_rn(o.rho[u] / o.S, o.in[u] ? 1.0f : 0.0f);
+        f[1] = __floats2bfloat162_rn((tt[u] & dDirichlet) ? 1.0f : 0.0f, o.in[u] ? dd[u] / o.D : 0.0f);
+        f[2] = f[3] = __floats2bfloat162_rn(0.0f, 0.0f);
+        *reinterpret_cast<uint4*>(x0 + v * 8) = *reinterpret_cast<const uint4*>(f);
+    }
+    return o;
+}
+
+template <int H>
+struct NetDims {
+    static constexpr int CG = H / 8;
+    static constexpr int KS1 = 232;                 // 8 input channels: 28 taps x 8 + 8 (odd number of 16-byte rows)
+    static constexpr int KSH = CG == 2 ? 440 : 232;  // H input channels
+    static constexpr int F1 = 0, F2 = F1 + H * KS1, F3 = F2 + H * KSH, G3 = F3 + 8 * KSH, G2 = G3 + H * KS1;
+    static constexpr int kFwd = G3;      // bf16 elements the forward pass needs
+    static constexpr int kPack = G2 + H * KSH;
+    // fp32 parameters: W1[H][27][8], b1[H], W2[H][27][H], b2[H], W3[27][H]
+    static constexpr int W1 = 0, B1 = W1 + H * 216, W2 = B1 + H, B2 = W2 + H * 27 * H, W3 = B2 + H, kParams = W3 + 27 * H;
+    static constexpr int kAct8 = kPadVox * 8, kActH = kPadVox * H;  // bf16 elements of the activation buffers
+};
+
+template <int H>
+__device__ __forceinline__ void copy_weights(__nv_bfloat16* dst, const __nv_bfloat16* src, int n, float* bias, const float* bsrc) {
+    for (int i = threadIdx.x; i < n / 8; i += kNetThreads) reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+    if (threadIdx.x < 2 * H) bias[threadIdx.x] = bsrc[threadIdx.x];
+}
+__device__ __forceinline__ void zero_smem(void* p, int bytes) {
+    for (int i = threadIdx.x; i < bytes / 16; i += kNetThreads) reinterpret_cast<uint4*>(p)[i] = make_uint4(0, 0, 0, 0);
+}
+
+// Forward pass over samples; out (z) += (S/D) * f on INTERIOR cells, or, with overwrite, out = (S/D) * f.
+template <int H>
+__global__ void __launch_bounds__(kNetThreads) k_net_forward(NetIn I, int ns, const __nv_bfloat16* __restrict__ pack,
+                                                             const float* __restrict__ bias_g, float* __restrict__ out, int overwrite) {
+    using Dm = NetDims<H>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* x0 = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* a1 = x0 + Dm::kAct8;
+    __nv_bfloat16* a2 = a1 + Dm::kActH;
+    __nv_bfloat16* wt = a2 + Dm::kActH;
+    float* bias = reinterpret_cast<float*>(wt + Dm::kFwd);
+    float* ys = bias + 2 * H;
+    float* red = ys + kCells;
+    zero_smem(smem, 2 * (Dm::kAct8 + 2 * Dm::kActH));
+    copy_weights<H>(wt, pack, Dm::kFwd, bias, bias_g);
+    __syncthreads();
+    for (int s = blockIdx.x; s < ns; s += gridDim.x) {
+        const Staged st = stage_features(I, s, x0, red);
+        const int t = I.idx ? I.idx[s] : I.t0 + s;
+        if (st.S == 0.0f) {
+            if (overwrite) st4(out + (size_t)t * kCells + 4 * threadIdx.x, make_float4(0.f, 0.f, 0.f, 0.f));
+            continue;  // uniform over the block
+        }
+        __syncthreads();
+        {
+            float acc[8][Dm::CG][4];
+            conv_tile<1, Dm::CG>(x0, wt + Dm::F1, Dm::KS1, acc);
+            store_hidden<Dm::CG, false>(acc, a1, nullptr, bias);
+        }
+        __syncthreads();
+        {
+            float acc[8][Dm::CG][4];
+            conv_tile<Dm::CG, Dm::CG>(a1, wt + Dm::F2, Dm::KSH, acc);
+            store_hidden<Dm::CG, false>(acc, a2, nullptr, bias + H);
+        }
+        __syncthreads();
+        {
+            float acc[8][1][4];
+            conv_tile<Dm::CG, 1>(a2, wt + Dm::F3, Dm::KSH, acc);
+            store_output(acc, ys);
+        }
+        __syncthreads();
+        const float sc = st.S / st.D;
+        float* o = out + (size_t)t * kCells + 4 * threadIdx.x;
+        float4 z = overwrite ? make_float4(0.f, 0.f, 0.f, 0.f) : ldcg4(o);
+        float zz[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (st.in[u]) zz[u] = __fmaf_rn(sc, ys[4 * threadIdx.x + u], zz[u]);
+        st4(o, make_float4(zz[0], zz[1], zz[2], zz[3]));
+        __syncthreads();  // ys and x0 are rewritten by the next sample
+    }
+}
+
+// Forward and backward pass of one batch: per batch slot b (sample idx[b]) the gradient of
+// sum over INTERIOR cells of (f - target * D/S)^2 goes to grad[b][kParams] and the sum to loss[b].
+template <int H>
+__global__ void __launch_bounds__(kNetThreads) k_net_train(NetIn I, int nb, const __nv_bfloat16* __restrict__ pack,
+                                                           const float* __restrict__ bias_g, float* __restrict__ grad,
+                                                           float* __restrict__ loss) {
+    using Dm = NetDims<H>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* x0 = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* dy = x0 + Dm::kAct8;
+    __nv_bfloat16* a1 = dy + Dm::kAct8;
+    __nv_bfloat16* a2 = a1 + Dm::kActH;  // later dz1
+    __nv_bfloat16* dz2 = a2 + Dm::kActH;
+    __nv_bfloat16* wt = dz2 + Dm::kActH;
+    float* bias = reinterpret_cast<float*>(wt + Dm::kPack);
+    float* ys = bias + 2 * H;
+    float* red = ys + kCells;  // 128 floats
+    zero_smem(smem, 2 * (2 * Dm::kAct8 + 3 * Dm::kActH));
+    copy_weights<H>(wt, pack, Dm::kPack, bias, bias_g);
+    __syncthreads();
+    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+        float* gw = grad + (size_t)b * Dm::kParams;
+        const Staged st = stage_features(I, b, x0, red);
+        if (st.S == 0.0f) {
+            for (int p = threadIdx.x; p < Dm::kParams; p += kNetThreads) gw[p] = 0.0f;
+            if (threadIdx.x == 0) loss[b] = 0.0f;
+            continue;
+        }
+        __syncthreads();
+        {
+            float acc[8][Dm::CG][4];
+            conv_tile<1, Dm::CG>(x0, wt + Dm::F1, Dm::KS1, acc);
+            store_hidden<Dm::CG, false>(acc, a1, nullptr, bias);
+        }
+        __syncthreads();
+        {
+            float acc[8][Dm::CG][4];
+            conv_tile<Dm::CG, Dm::CG>(a1, wt + Dm::F2, Dm::KSH, acc);
+            store_hidden<Dm::CG, false>(acc, a2, nullptr, bias + H);
+        }
+        __syncthreads();
+        {
+            float acc[8][1][4];
+            conv_tile<Dm::CG, 1>(a2, wt + Dm::F3, Dm::KSH, acc);
+            store_output(acc, ys);
+        }
+        __syncthreads();
+        // dL/df = 2 (f - target D/S) on INTERIOR cells, into channel 0 of dy
+        const float sc = st.D / st.S;
+        float l = 0.0f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int cell = 4 * threadIdx.x + u;
+            const float e = st.in[u] ? __fsub_rn(ys[cell], __fmul_rn(st.tgt[u], sc)) : 0.0f;
+            l = __fmaf_rn(e, e, l);
+            dy[pad_vox(cell >> 6, (cell >> 3) & 7, cell & 7) * 8] = __float2bfloat16_rn(2.0f * e);
+        }
+        const float lt = block_sum_f(l, red);  // synchronises: dy is complete
+        if (threadIdx.x == 0) loss[b] = lt;
+        wgrad_tile<Dm::CG, 1>(a2, dy, gw + Dm::W3, 1);  // W3[tap][c] as [n = 0][tap][c]
+        {
+            float acc[8][Dm::CG][4];
+            conv_tile<1, Dm::CG>(dy, wt + Dm::G3, Dm::KS1, acc);
+            store_hidden<Dm::CG, true>(acc, dz2, a2, nullptr);
+        }
+        __syncthreads();
+        wgrad_tile<Dm::CG, Dm::CG>(a1, dz2, gw + Dm::W2, H);
+        bias_grad<Dm::CG>(dz2, red, gw + Dm::B2);
+        {
+            float acc[8][Dm::CG][4];
+            conv_tile<Dm::CG, Dm::CG>(dz2, wt + Dm::G2, Dm::KSH, acc);
+            store_hidden<Dm::CG, true>(acc, a2, a1, nullptr);  // dz1 over a2
+        }
+        __syncthreads();
+        wgrad_tile<1, Dm::CG>(x0, a2, gw + Dm::W1, H);
+        bias_grad<Dm::CG>(a2, red, gw + Dm::B1);
+        // bias_grad ends with a barrier: the buffers may be rewritten by the next sample
+    }
+}
+
+// fp32 parameters -> packed bf16 operands (forward F1..F3, flipped/transposed G3, G2) and biases
+template <int H>
+__global__ void k_net_pack(const float* __restrict__ p, __nv_bfloat16* __restrict__ pack, float* __restrict__ bias) {
+    using Dm = NetDims<H>;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < 2 * H) bias[e] = e < H ? p[Dm::B1 + e] : p[Dm::B2 + e - H];
+    if (e >= Dm::kPack) return;
+    float v = 0.0f;
+    if (e < Dm::F2) {  // F1[n][tap*8 + c]
+        const int n = e / Dm::KS1, k = e % Dm::KS1, tap = k / 8, c = k % 8;
+        if (tap < 27) v = p[Dm::W1 + (n * 27 + tap) * 8 + c];
+    } else if (e < Dm::F3) {  // F2[n][tap*H + c]
+        const int n = (e - Dm::F2) / Dm::KSH, k = (e - Dm::F2) % Dm::KSH, tap = k / H, c = k % H;
+        if (tap < 27) v = p[Dm::W2 + (n * 27 + tap) * H + c];
+    } else if (e < Dm::G3) {  // F3[n][tap*H + c], row 0 only
+        const int n = (e - Dm::F3) / Dm::KSH, k = (e - Dm::F3) % Dm::KSH, tap = k / H, c = k % H;
+        if (n == 0 && tap < 27) v = p[Dm::W3 + tap * H + c];
+    } else if (e < Dm::G2) {  // G3[h][tap'*8 + c] = W3[26 - tap'][h] for c = 0
+        const int h = (e - Dm::G3) / Dm::KS1, k = (e - Dm::G3) % Dm::KS1, tap = k / 8, c = k % 8;
+        if (c == 0 && tap < 27) v = p[Dm::W3 + (26 - tap) * H + h];
+    } else {  // G2[cin][tap'*H + cout] = W2[cout][26 - tap'][cin]
+        const int ci = (e - Dm::G2) / Dm::KSH, k = (e - Dm::G2) % Dm::KSH, tap = k / H, co = k % H;
+        if (tap < 27) v = p[Dm::W2 + (co * 27 + (26 - tap)) * H + ci];
+    }
+    pack[e] = __float2bfloat16_rn(v);
+}
+
+// Sum the batch's gradients in slot order (scaled), optionally store them, then one Adam step.
+__global__ void k_net_reduce_adam(const float* __restrict__ grad, int nb, int np, float scale, float* __restrict__ gout,
+                                  float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2,
+                                  float bc1, float bc2, int update) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= np) return;
+    float g = 0.0f;
+    for (int b = 0; b < nb; ++b) g += grad[(size_t)b * np + e];
+    g *= scale;
+    if (gout) gout[e] = g;
+    if (!update) return;
+    const float mm = b1 * m[e] + (1.0f - b1) * g, vv = b2 * v[e] + (1.0f - b2) * g * g;
+    m[e] = mm;
+    v[e] = vv;
+    p[e] -= lr * (mm / bc1) / (sqrtf(vv / bc2) + 1e-8f);
+}
+
+template <int H>
+size_t forward_smem() {
+    using Dm = NetDims<H>;
+    return 2 * (size_t)(Dm::kAct8 + 2 * Dm::kActH + Dm::kFwd) + sizeof(float) * (2 * H + kCells + 32);
+}
+template <int H>
+size_t train_smem() {
+    using Dm = NetDims<H>;
+    return 2 * (size_t)(2 * Dm::kAct8 + 3 * Dm::kActH + Dm::kPack) + sizeof(float) * (2 * H + kCells + kNetThreads);
+}
+
+int g_fwd_blocks[2] = {0, 0};  // resident forward blocks per SM (H = 8, 16)
+
+}  // namespace
+
+int net_params(int H) { return H == 16 ? NetDims<16>::kParams : NetDims<8>::kParams; }
+int net_pack_elems(int H) { return H == 16 ? NetDims<16>::kPack : NetDims<8>::kPack; }
+
+bool net_init() {
+    bool ok = true;
+    ok = ok && cudaFuncSetAttribute(k_net_forward<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<8>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_net_forward<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<16>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_net_train<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem<8>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_net_train<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem<16>()) == cudaSuccess;
+    if (!ok) return false;
+    ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_blocks[0], k_net_forward<8>, kNetThreads, forward_smem<8>()) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_blocks[1], k_net_forward<16>, kNetThreads, forward_smem<16>()) == cudaSuccess;
+    return ok && g_fwd_blocks[0] > 0 && g_fwd_blocks[1] > 0;
+}
+
+static int num_sms() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaStream_t st) {
+    const int n = net_pack_elems(H);
+    note_kernel_launch();
+    if (H == 16) k_net_pack<16><<<(n + 255) / 256, 256, 0, st>>>(params, (__nv_bfloat16*)pack, bias);
+    else k_net_pack<8><<<(n + 255) / 256, 256, 0, st>>>(params, (__nv_bfloat16*)pack, bias);
+}
+
+void launch_net_forward(int H, const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
+                        const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st) {
+    if (ns <= 0) return;
+    const NetIn I{r, az, diag, types, nullptr, idx, t0};
+    const int cap = num_sms() * g_fwd_blocks[H == 16 ? 1 : 0];
+    const int blocks = ns < cap ? ns : cap;
+    note_kernel_launch();
+    if (H == 16)
+        k_net_forward<16><<<blocks, kNetThreads, forward_smem<16>(), st>>>(I, ns, (const __nv_bfloat16*)pack, bias, out, overwrite);
+    else
+        k_net_forward<8><<<blocks, kNetThreads, forward_smem<8>(), st>>>(I, ns, (const __nv_bfloat16*)pack, bias, out, overwrite);
+}
+
+void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
+                      const void* pack, const float* bias, float* grad, float* loss, cudaStream_t st) {
+    if (nb <= 0) return;
+    const NetIn I{rho, nullptr, diag, types, target, idx, 0};
+    const int sms = num_sms();
+    const int blocks = nb < sms ? nb : sms;
+    note_kernel_launch();
+    if (H == 16)
+        k_net_train<16><<<blocks, kNetThreads, train_smem<16>(), st>>>(I, nb, (const __nv_bfloat16*)pack, bias, grad, loss);
+    else
+        k_net_train<8><<<blocks, kNetThreads, train_smem<8>(), st>>>(I, nb, (const __nv_bfloat16*)pack, bias, grad, loss);
+}
+
+void launch_net_reduce_adam(const float* grad, int nb, int np, float scale, float* gout, float* p, float* m, float* v, float lr, int step,
+                            bool update, cudaStream_t st) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = update ? 1.0f - (float)std::pow(0.9, step) : 1.0f, bc2 = update ? 1.0f - (float)std::pow(0.999, step) : 1.0f;
+    note_kernel_launch();
+    k_net_reduce_adam<<<(np + 255) / 256, 256, 0, st>>>(grad, nb, np, scale, gout, p, m, v, lr, b1, b2, bc1, bc2, update ? 1 : 0);
+}
+
+}  // namespace cmg

@@ -210,6 +210,36 @@ int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
 #define CMG_STORAGE_BF16 1
 #define CMG_STORAGE_FP16 2
 int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage);
+/* Learned finest-level smoother (no counterpart in the reference).  A per-tile 3-D conv
+ * net (conv3x3x3 8->H, ReLU, H->H, ReLU, H->1; H = 8 or 16) on BF16 tensor cores adds
+ * (S/D) f(rho/S, INTERIOR, DIRICHLET, diag/D) to z on the finest level's LEAF tiles after
+ * each mu-cycle, rho = r - A z being the residual the cycle leaves (S: its RMS on the
+ * tile, D: the tile's largest diagonal).  The solve then runs flexible CG (Polak-Ribiere
+ * beta), judges the result by the true residual |b - A x| / |b| and falls back to the
+ * plain solve when that exceeds 4 tol or the solve does not converge.
+ * Samples are tiles of 512 cells (cell i*64 + j*8 + k): rho, the diagonal of A (the
+ * coefficient channel coeff+3), cell types and the target error d = A^-1 rho.
+ * The net keeps its parameters, Adam state and samples on the device; training runs
+ * the forward and backward kernels on the GPU. */
+typedef struct cmg_learned cmg_learned;
+int cmg_learned_create(int hidden, unsigned long long seed, cmg_learned** out);
+int cmg_learned_destroy(cmg_learned* net);
+int cmg_learned_num_params(cmg_learned* net, int* n);
+/* fp32 parameters: W1[H][27][8], b1[H], W2[H][27][H], b2[H], W3[27][H]; tap = dx*9+dy*3+dz */
+int cmg_learned_get_params(cmg_learned* net, float* host, int n);
+int cmg_learned_set_params(cmg_learned* net, const float* host, int n); /* also resets Adam */
+int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target);
+/* correction (S/D) f on INTERIOR cells (0 elsewhere) of samples first..first+n-1 */
+int cmg_learned_forward(cmg_learned* net, int first, int n, float* out);
+/* mean loss sum (f - target D/S)^2 / (n 512) over samples first..first+n-1 and its gradient */
+int cmg_learned_gradient(cmg_learned* net, int first, int n, double* loss, float* grad);
+/* Adam (beta 0.9/0.999) over shuffled batches; epoch_loss[e] (may be NULL) */
+int cmg_learned_train(cmg_learned* net, int epochs, int batch, float lr, unsigned long long seed, float* epoch_loss);
+/* use the net's current parameters as the solver's finest-level smoother (NULL: plain) */
+int cmg_amg_solver_set_learned(cmg_amg_solver* s, cmg_learned* net);
+/* of the last cmg_amg_solve with a learned smoother: true relative residual, whether it
+ * fell back to the plain solve, and the learned attempt's iterations */
+int cmg_amg_solver_learned_status(cmg_amg_solver* s, double* true_rel, int* fell_back, int* learned_iters);
 
 /* ---- geometric multigrid preconditioners ---------------------------------
  * GMGSolver(one_over_alpha, prolong_coeff) (src/GMGSolver.h:21) and

@@ -1,0 +1,146 @@
+"""FP64 CPU restatement of the learned finest-level smoother's network (test infrastructure only).
+
+Imported by tests/ -- never by the product.  The reference has no learned preconditioner;
+this module restates the network that cirrus-amg_b200/csrc/learned.cu runs on BF16 tensor
+cores, so that its forward pass, loss and gradients can be checked:
+
+  features per 8^3 tile (channels-last, zero padding outside the tile):
+      0: rho / S (S = RMS of rho over INTERIOR cells)   1: INTERIOR   2: DIRICHLET
+      3: diag / D on INTERIOR cells (D = max |diag| over INTERIOR cells)   4-7: 0
+  a1 = relu(conv(x, W1) + b1); a2 = relu(conv(a1, W2) + b2); f = conv(a2, W3)
+  correction = (S / D) f on INTERIOR cells
+  loss = sum over tiles and INTERIOR cells of (f - target D / S)^2 / (n 512)
+
+Every convolution is 3x3x3 with tap = dx*9 + dy*3 + dz.  The GPU path rounds the
+features, the weights and the activations a1, a2, 2 (f - t), dz2, dz1 to BF16 and
+accumulates in FP32; `emulate_bf16=True` applies the same roundings here (in FP64
+arithmetic otherwise), which is what the gradient check compares against.
+"""
+import numpy as np
+
+DIRICHLET, INTERIOR, NEUMANN = 1, 2, 4
+
+
+def bf16(x):
+    """Round to the nearest BF16 (ties to even) via FP32, as __float2bfloat16_rn does."""
+    f = np.ascontiguousarray(np.asarray(x, dtype=np.float64).astype(np.float32))
+    u = f.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
+def layout(H):
+    W1 = 0
+    B1 = W1 + H * 216
+    W2 = B1 + H
+    B2 = W2 + H * 27 * H
+    W3 = B2 + H
+    return dict(W1=W1, B1=B1, W2=W2, B2=B2, W3=W3, n=W3 + 27 * H)
+
+
+def unpack(p, H):
+    L = layout(H)
+    p = np.asarray(p, dtype=np.float64)
+    return (p[L["W1"]:L["B1"]].reshape(H, 27, 8), p[L["B1"]:L["W2"]], p[L["W2"]:L["B2"]].reshape(H, 27, H),
+            p[L["B2"]:L["W3"]], p[L["W3"]:L["n"]].reshape(1, 27, H))
+
+
+def _taps():
+    return [(t // 9, (t // 3) % 3, t % 3) for t in range(27)]
+
+
+def conv(x, W):
+    """x [n, 8, 8, 8, Cin], W [Cout, 27, Cin] -> [n, 8, 8, 8, Cout]; out[v] = sum_t x[v + off(t)] W[:, t]."""
+    n = x.shape[0]
+    xp = np.zeros((n, 10, 10, 10, x.shape[4]))
+    xp[:, 1:9, 1:9, 1:9] = x
+    out = np.zeros((n, 8, 8, 8, W.shape[0]))
+    for t, (dx, dy, dz) in enumerate(_taps()):
+        out += np.einsum("sijkc,nc->sijkn", xp[:, dx:dx + 8, dy:dy + 8, dz:dz + 8], W[:, t, :])
+    return out
+
+
+def conv_input_grad(d, W):
+    """Gradient of conv's input: da[u] = sum_t W[:, t]^T d[u - off(t)] (zero outside the tile)."""
+    n = d.shape[0]
+    dp = np.zeros((n, 10, 10, 10, d.shape[4]))
+    dp[:, 1:9, 1:9, 1:9] = d
+    out = np.zeros((n, 8, 8, 8, W.shape[2]))
+    for t, (dx, dy, dz) in enumerate(_taps()):
+        out += np.einsum("sijkn,nc->sijkc", dp[:, 2 - dx:10 - dx, 2 - dy:10 - dy, 2 - dz:10 - dz], W[:, t, :])
+    return out
+
+
+def conv_weight_grad(x, d):
+    """Gradient of conv's weights: gW[n, t, c] = sum_v x[v + off(t), c] d[v, n]."""
+    xp = np.zeros((x.shape[0], 10, 10, 10, x.shape[4]))
+    xp[:, 1:9, 1:9, 1:9] = x
+    g = np.zeros((d.shape[4], 27, x.shape[4]))
+    for t, (dx, dy, dz) in enumerate(_taps()):
+        g[:, t, :] = np.einsum("sijkc,sijkn->nc", xp[:, dx:dx + 8, dy:dy + 8, dz:dz + 8], d)
+    return g
+
+
+def features(rho, diag, types, emulate_bf16=True):
+    """Per-tile features; rho, diag [n, 512] float32, types [n, 512] uint8 (cell i*64 + j*8 + k)."""
+    rho = np.asarray(rho, dtype=np.float32).reshape(-1, 512)
+    diag = np.asarray(diag, dtype=np.float32).reshape(-1, 512)
+    types = np.asarray(types, dtype=np.uint8).reshape(-1, 512)
+    inter = (types & INTERIOR) != 0
+    r = np.where(inter, rho, 0.0).astype(np.float64)
+    cnt = inter.sum(1)
+    D = np.where(inter, np.abs(diag), 0.0).max(1).astype(np.float64)
+    ss = (r * r).sum(1)
+    ok = (cnt > 0) & (ss > 0) & (D > 0)
+    S = np.where(ok, np.sqrt(ss / np.maximum(cnt, 1)), 0.0)
+    x = np.zeros((rho.shape[0], 512, 8))
+    Ssafe = np.where(ok, S, 1.0)[:, None]
+    Dsafe = np.where(ok, D, 1.0)[:, None]
+    x[:, :, 0] = r / Ssafe
+    x[:, :, 1] = inter
+    x[:, :, 2] = (types & DIRICHLET) != 0
+    x[:, :, 3] = np.where(inter, diag / Dsafe, 0.0)
+    if emulate_bf16:
+        x = bf16(x)
+    return x.reshape(-1, 8, 8, 8, 8), S, D, inter, ok
+
+
+def forward(p, H, rho, diag, types, emulate_bf16=True):
+    """Correction (S/D) f on INTERIOR cells, [n, 512]."""
+    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16)
+    f, _ = _forward_net(p, H, x, emulate_bf16)
+    sc = np.where(ok, S / np.where(ok, D, 1.0), 0.0)[:, None]
+    return np.where(inter & ok[:, None], sc * f.reshape(-1, 512), 0.0)
+
+
+def _forward_net(p, H, x, emulate_bf16):
+    W1, b1, W2, b2, W3 = unpack(p, H)
+    r = bf16 if emulate_bf16 else (lambda a: a)
+    W1, W2, W3 = r(W1), r(W2), r(W3)
+    a1 = r(np.maximum(conv(x, W1) + b1, 0.0))
+    a2 = r(np.maximum(conv(a1, W2) + b2, 0.0))
+    f = conv(a2, W3)[..., 0]
+    return f, (x, a1, a2, W1, W2, W3)
+
+
+def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True):
+    """Mean loss and its gradient (layout of `layout(H)`)."""
+    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16)
+    n = x.shape[0]
+    f, (x, a1, a2, W1, W2, W3) = _forward_net(p, H, x, emulate_bf16)
+    r = bf16 if emulate_bf16 else (lambda a: a)
+    tgt = np.asarray(target, dtype=np.float64).reshape(-1, 512) * np.where(ok, D / np.where(ok, S, 1.0), 0.0)[:, None]
+    m = inter & ok[:, None]
+    e = np.where(m, f.reshape(-1, 512) - tgt, 0.0)
+    scale = 1.0 / (n * 512)
+    loss = (e * e).sum() * scale
+    dy = r(2.0 * e).reshape(n, 8, 8, 8, 1)
+    gW3 = conv_weight_grad(a2, dy)
+    dz2 = r(conv_input_grad(dy, W3) * (a2 > 0))
+    gW2 = conv_weight_grad(a1, dz2)
+    gb2 = dz2.sum((0, 1, 2, 3))
+    dz1 = r(conv_input_grad(dz2, W2) * (a1 > 0))
+    gW1 = conv_weight_grad(x, dz1)
+    gb1 = dz1.sum((0, 1, 2, 3))
+    g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel()]) * scale
+    return loss, g

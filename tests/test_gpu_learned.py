@@ -1,0 +1,155 @@
+"""Learned finest-level smoother: the per-tile network's forward pass and gradients
+against the FP64 CPU restatement (oracle/learned_oracle.py), GPU training, and the
+learned solve (flexible PCG, true-residual judge, plain fallback) against the plain one."""
+import numpy as np
+import pytest
+
+import cmg
+import learned
+from oracle import learned_oracle as LO
+from workloads import COEFF, setup_uniform, uniform_rhs
+
+pytestmark = pytest.mark.gpu
+
+
+def random_samples(n, seed):
+    """Tiles with mixed cell types, residual scales over six decades, one all-zero tile and
+    one tile without INTERIOR cells (both give a zero correction)."""
+    rng = np.random.default_rng(seed)
+    types = np.full((n, 512), cmg.INTERIOR, np.uint8)
+    u = rng.uniform(size=(n, 512))
+    types[u < 0.08] = cmg.DIRICHLET
+    types[(u >= 0.08) & (u < 0.15)] = cmg.NEUMANN
+    rho = (rng.standard_normal((n, 512)) * 10.0 ** rng.uniform(-3, 3, (n, 1))).astype(np.float32)
+    diag = (rng.uniform(0.3, 6.0, (n, 512)) / 64.0).astype(np.float32)
+    target = (rng.standard_normal((n, 512)) * 10.0 ** rng.uniform(-2, 2, (n, 1))).astype(np.float32)
+    rho[1] = 0.0
+    types[2] = cmg.NEUMANN
+    return rho, diag, types, target
+
+
+def random_params(H, seed, scale=0.15):
+    rng = np.random.default_rng(seed)
+    L = LO.layout(H)
+    p = (rng.standard_normal(L["n"]) * scale).astype(np.float32)
+    p[L["B1"]:L["W2"]] = rng.uniform(-0.1, 0.1, H)
+    p[L["B2"]:L["W3"]] = rng.uniform(-0.1, 0.1, H)
+    return p
+
+
+@pytest.mark.parametrize("H", [8, 16])
+def test_forward_matches_oracle(H):
+    rho, diag, types, target = random_samples(12, 10 + H)
+    net = cmg.LearnedNet(H, seed=1)
+    p = random_params(H, 20 + H)
+    net.set_params(p)
+    net.set_samples(rho, diag, types, target)
+    out = net.forward()
+    ref = LO.forward(p, H, rho, diag, types)
+    assert np.all(out[1] == 0) and np.all(out[2] == 0)
+    assert np.all(out[(types & cmg.INTERIOR) == 0] == 0)
+    for s in range(out.shape[0]):
+        m = np.abs(ref[s]).max()
+        if m == 0:
+            continue
+        # same BF16 roundings on both sides; FP32 against FP64 accumulation and rare
+        # rounding-boundary flips of a BF16 activation remain
+        assert np.abs(out[s] - ref[s]).max() <= 1e-2 * m, s
+
+
+@pytest.mark.parametrize("H", [8, 16])
+def test_gradient_matches_oracle(H):
+    rho, diag, types, target = random_samples(10, 30 + H)
+    net = cmg.LearnedNet(H, seed=2)
+    p = random_params(H, 40 + H)
+    net.set_params(p)
+    net.set_samples(rho, diag, types, target)
+    loss, g = net.gradient()
+    rl, rg = LO.loss_and_grad(p, H, rho, diag, types, target)
+    assert abs(loss - rl) <= 1e-3 * rl
+    L = LO.layout(H)
+    for a, b in [("W1", "B1"), ("B1", "W2"), ("W2", "B2"), ("B2", "W3"), ("W3", "n")]:
+        gs, rs = g[L[a]:L[b]], rg[L[a]:L[b]]
+        assert np.linalg.norm(gs - rs) <= 2e-2 * np.linalg.norm(rs) + 1e-12, a
+    # padded input channels 4..7 of W1 get exactly zero gradient
+    gw1 = g[L["W1"]:L["B1"]].reshape(H, 27, 8)
+    assert np.all(gw1[:, :, 4:] == 0)
+
+
+def test_gradient_is_deterministic():
+    rho, diag, types, target = random_samples(9, 5)
+    net = cmg.LearnedNet(16, seed=4)
+    net.set_samples(rho, diag, types, target)
+    l1, g1 = net.gradient()
+    l2, g2 = net.gradient()
+    assert l1 == l2 and np.array_equal(g1, g2)
+
+
+def _uniform_pairs(L, seeds, iters=(1, 2, 3)):
+    G, _, solver, _ = setup_uniform(L, seed=seeds[0], with_oracle=False)
+    lv, _, ty = G.tiles()
+    rhs = [uniform_rhs(ty == cmg.LEAF, s) for s in seeds]
+    return G, solver, learned.collect_pairs(G, solver, COEFF, rhs, iters=iters), ty
+
+
+def test_pairs_satisfy_the_error_equation():
+    """d = A^-1 rho: A d reproduces rho on the finest LEAF tiles."""
+    G, solver, pairs, ty = _uniform_pairs(2, [7], iters=(2,))
+    fine = learned.finest_leaf_tiles(G)
+    d = np.zeros((G.num_tiles, 512), np.float32)
+    d[fine] = pairs["d"]
+    G.upload(13, d)
+    G.full_neg_lap(13, COEFF, 14)
+    ad = G.download(14)[fine]
+    assert np.linalg.norm(ad - pairs["rho"]) <= 1e-5 * np.linalg.norm(pairs["rho"])
+
+
+def test_training_reduces_loss():
+    G, solver, pairs, ty = _uniform_pairs(2, [100, 101, 102, 103])
+    net0 = cmg.LearnedNet(16, seed=0)
+    net0.set_samples(pairs["rho"], pairs["diag"], pairs["types"], pairs["d"])
+    l0, _ = net0.gradient()
+    net, losses = learned.train(pairs, hidden=16, epochs=15, batch=64, lr=2e-3, seed=0)
+    l1, _ = net.gradient()
+    assert np.all(np.isfinite(losses))
+    assert l1 < 0.7 * l0, (l0, l1, losses)
+
+
+def test_learned_solve_matches_plain():
+    """An untrained net: flexible PCG still reaches the tolerance (or falls back), the true
+    residual judges it, and x agrees with the plain solve."""
+    G, _, solver, b = setup_uniform(3, seed=0, with_oracle=False)
+    net = cmg.LearnedNet(16, seed=5)
+    rows = learned.compare(G, solver, net, [b])
+    ip, tp, il, tl, tr, fb, dx = rows[0]
+    assert tr <= 4e-6
+    assert dx <= 1e-4, rows
+    assert il <= 100
+
+
+def test_nonfinite_net_falls_back_to_plain():
+    """A net whose output overflows makes the learned solve non-finite; the plain solve takes over."""
+    G, _, solver, b = setup_uniform(2, seed=3, with_oracle=False)
+    ip, _ = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    xp = G.download(0)
+    net = cmg.LearnedNet(8, seed=6)
+    net.set_params(np.full(net.num_params, 3e37, np.float32))
+    solver.set_learned(net)
+    G.upload(1, b)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    tr, fb, _ = solver.learned_status()
+    assert fb and it == ip and rel < 1e-6
+    assert np.array_equal(G.download(0), xp)
+
+
+def test_trained_net_against_plain(capsys):
+    """What the trained network gains: trained on other right-hand sides of the uniform 64^3
+    grid, compared with the plain solve on the benchmark rhs (seed 0)."""
+    G, solver, pairs, ty = _uniform_pairs(3, list(range(100, 106)))
+    net, losses = learned.train(pairs, hidden=16, epochs=20, batch=256, lr=2e-3, seed=0)
+    b = uniform_rhs(ty == cmg.LEAF, 0)
+    rows = learned.compare(G, solver, net, [b, b])
+    with capsys.disabled():
+        print("\nlearned vs plain (uniform 64^3): losses", losses[0], losses[-1], "rows", rows)
+    ip, tp, il, tl, tr, fb, dx = rows[-1]
+    assert not fb and tr <= 4e-6 and dx <= 1e-4

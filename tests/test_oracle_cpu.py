@@ -347,3 +347,45 @@ def test_divergence_without_coeff_equals_coefficient_form_on_uniform_faces():
     lv, ijk, ty = g.tiles()
     m = ty == O.LEAF
     assert np.array_equal(g.channel(1)[m], g.channel(2)[m])
+
+
+def test_learned_oracle_gradient_matches_finite_differences():
+    """The FP64 restatement of the learned smoother's network: its backward pass against
+    central differences of its own loss (no BF16 rounding), on two tiles."""
+    from oracle import learned_oracle as LO
+
+    H = 8
+    rng = np.random.default_rng(0)
+    n = 2
+    types = np.full((n, 512), LO.INTERIOR, np.uint8)
+    types[:, rng.uniform(size=512) < 0.1] = LO.DIRICHLET
+    rho = rng.standard_normal((n, 512)).astype(np.float32)
+    diag = rng.uniform(0.5, 6.0, (n, 512)).astype(np.float32)
+    target = rng.standard_normal((n, 512)).astype(np.float32)
+    L = LO.layout(H)
+    p = rng.standard_normal(L["n"]) * 0.2
+    p[L["B1"]:L["W2"]] = 0.3
+    p[L["B2"]:L["W3"]] = 0.3
+    _, g = LO.loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=False)
+    picks = list(rng.choice(L["n"], 24, replace=False)) + [L["B1"], L["B2"] + 1, L["W3"] + 5]
+    eps = 1e-6
+    for i in picks:
+        if L["W1"] <= i < L["B1"] and (i - L["W1"]) % 8 >= 4:
+            continue  # padded input channels: zero input, zero gradient
+        q = p.copy()
+        q[i] += eps
+        lp, _ = LO.loss_and_grad(q, H, rho, diag, types, target, emulate_bf16=False)
+        q[i] -= 2 * eps
+        lm, _ = LO.loss_and_grad(q, H, rho, diag, types, target, emulate_bf16=False)
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i])) + 1e-7, (i, fd, g[i])
+
+
+def test_learned_oracle_bf16_rounding():
+    from oracle import learned_oracle as LO
+
+    v = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -2.5, 0.0, 3.0e38])
+    r = LO.bf16(v)
+    assert r[0] == 1.0 and r[1] == 1.0  # tie to even
+    assert r[2] == 1.0 + 2.0 ** -6  # tie to even (upwards)
+    assert r[3] == -2.5 and r[4] == 0.0
