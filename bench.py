@@ -337,6 +337,77 @@ def roofline_entry(launch_ms, achieved, alg_bytes, L, active, cells, peak, peak_
     }
 
 
+def training_rhs(cmg, G, spec, n):
+    """Right-hand sides of the learned smoother's training pairs: the workload's rhs kind with
+    other seeds (normal: 100..; Fourier divergence: 200..); never the timed rhs."""
+    kind, _ = spec["rhs"]
+    out = []
+    _, _, ty = G.tiles()
+    for i in range(n):
+        if kind == "fourier":
+            k, amp, ph = fourier_modes(200 + i)
+            G.face_velocity_fourier(U, k, amp, ph)
+            G.divergence(U, COEFF, 1)
+            out.append(G.download(1))
+        else:
+            out.append(normal_rhs(ty, 100 + i, cmg.LEAF))
+    return out
+
+
+LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, iters=(1, 2, 3, 5), rhs=10, max_tiles=1250)
+
+
+def learned_block(cmg, torch, spec, steps, world, dev):
+    """The learned finest-level smoother on one workload: pairs from plain solves of other
+    right-hand sides of the same octree, trained on the GPU, then the timed rhs solved plain
+    and learned, each timed over `steps` solves with CUDA events (the learned solve's
+    true-residual judge included)."""
+    import learned
+
+    G = build_grid(cmg, spec)
+    S = make_solver(cmg)
+    t0 = time.perf_counter()
+    rhs = training_rhs(cmg, G, spec, LEARNED["rhs"])
+    # channels 10-12 (the face velocity, spent once the rhs exist) hold z, the FAS x0 and A z
+    pairs = learned.collect_pairs(G, S, COEFF, rhs, iters=LEARNED["iters"], max_tiles=LEARNED["max_tiles"], z_ch=U, x0_ch=U + 1,
+                                  az_ch=U + 2)
+    t1 = time.perf_counter()
+    net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
+                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"])
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+
+    def timed(use_net):
+        S.set_learned(net if use_net else None)
+        for _ in range(3):
+            G.copy(BSAVE, 1)
+            S.solve(G, *solve_args())
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            G.copy(BSAVE, 1)
+            it, rel = S.solve(G, *solve_args())
+        b.record()
+        torch.cuda.synchronize()
+        return replica_time(a.elapsed_time(b), world, dev) / steps, it, G.download(0)
+
+    plain_ms, plain_it, xp = timed(False)
+    ms, it, xl = timed(True)
+    true_rel, fell_back, learned_it = S.learned_status()
+    S.set_learned(None)
+    _, _, ty = G.tiles()
+    lm = ty == cmg.LEAF
+    return {"hidden": LEARNED["hidden"],
+            "damping": LEARNED["damping"], "train_pairs": int(pairs["rho"].shape[0]), "collect_s": round(t1 - t0, 3),
+            "train_s": round(t2 - t1, 3), "epochs": LEARNED["epochs"], "loss_first_epoch": float(losses[0]),
+            "loss_last_epoch": float(losses[-1]), "plain_ms": round(plain_ms, 4), "plain_pcg_iters": plain_it,
+            "learned_ms": round(ms, 4), "pcg_iters": it, "learned_pcg_iters": learned_it, "fell_back": fell_back,
+            "rel_residual_true": true_rel,
+            "rel_l2_vs_plain_solution": float(np.linalg.norm((xl - xp)[lm].astype(np.float64)) /
+                                              np.linalg.norm(xp[lm].astype(np.float64)))}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -411,6 +482,13 @@ def run_ours(args, rank, world, local_rank):
     one_solve()
     torch.cuda.synchronize()
 
+    # the learned finest-level smoother on the uniform 64^3 grid and on this workload
+    learned_res = []
+    if not args.no_learned:
+        for name in dict.fromkeys(["uniform64", args.workload]):
+            learned_res.append(dict(learned_block(cmg, torch, dict(instance_specs(name)[0], name=name), args.steps, world, dev),
+                                    workload=WORKLOADS[name]))
+
     # true residual of the last solution, FP32 operator apply on the device
     x = G.download(0)
     G.full_neg_lap(0, COEFF, 3)
@@ -465,6 +543,7 @@ def run_ours(args, rank, world, local_rank):
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "e2e_wall_ms": round(e2e_wall_ms, 4),
                 "mixed_precision_preconditioner": mixed,
+                "learned_preconditioner": learned_res,
             },
             "e2e": {"value": round(e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": count * 4, "d2h_bytes_per_step": count * 4},
             "gpu_launches": int(launches),
@@ -638,6 +717,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-smoother comparison")
     ap.add_argument("--workload", default="sphere", choices=sorted(WORKLOADS))
     ap.add_argument("--streams", type=int, default=BATCH_STREAMS, help="streams of the batched workload")
     args = ap.parse_args()

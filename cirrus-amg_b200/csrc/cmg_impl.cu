@@ -818,9 +818,12 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
         const DevGrid d = G.dev();
         launch_leaf_apply(d, G.leaf, G.nleaf, G.plane(0), aux, coeff_ch, false, scratch(), G.stream);
         launch_leaf_residual(d, G.leaf, G.nleaf, bsave, aux, true, G.stream);
-        double res = 0.0, bb = 0.0;
+        double res = 0.0, bb = h_s->rr0;  // rr0 = b.b on LEAF tiles when the solve tracks the residual
+        const bool have_bb = sync_stride > 0 && !pure_neumann;
         if (int e = host_dot(G, G.leaf, G.nleaf, aux, aux, &res)) return e;
-        if (int e = host_dot(G, G.leaf, G.nleaf, bsave, bsave, &bb)) return e;
+        if (!have_bb) {
+            if (int e = host_dot(G, G.leaf, G.nleaf, bsave, bsave, &bb)) return e;
+        }
         last_true_rel = bb > 0.0 ? std::sqrt(res / bb) : 0.0;
         last_learned_iters = it;
         const bool judged_ok = rc == 0 && std::isfinite(last_true_rel) &&

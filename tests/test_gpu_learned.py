@@ -144,12 +144,15 @@ def test_nonfinite_net_falls_back_to_plain():
 
 def test_trained_net_against_plain(capsys):
     """What the trained network gains: trained on other right-hand sides of the uniform 64^3
-    grid, compared with the plain solve on the benchmark rhs (seed 0)."""
-    G, solver, pairs, ty = _uniform_pairs(3, list(range(100, 106)))
-    net, losses = learned.train(pairs, hidden=16, epochs=20, batch=256, lr=2e-3, seed=0)
+    grid (seeds 100-109), compared with the plain solve on the benchmark rhs (seed 0).
+    The damped net (output x 0.5) saves one of the plain solve's 8 PCG iterations."""
+    G, solver, pairs, ty = _uniform_pairs(3, list(range(100, 110)), iters=(1, 2, 3, 5))
+    net, losses = learned.train(pairs, hidden=8, epochs=30, batch=256, lr=2e-3, seed=0, damping=0.5)
     b = uniform_rhs(ty == cmg.LEAF, 0)
     rows = learned.compare(G, solver, net, [b, b])
     with capsys.disabled():
         print("\nlearned vs plain (uniform 64^3): losses", losses[0], losses[-1], "rows", rows)
+    assert losses[-1] < 0.9 * losses[0]
     ip, tp, il, tl, tr, fb, dx = rows[-1]
     assert not fb and tr <= 4e-6 and dx <= 1e-4
+    assert il < ip, rows
