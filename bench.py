@@ -354,7 +354,7 @@ def training_rhs(cmg, G, spec, n):
     return out
 
 
-LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, iters=(1, 2, 3, 5), rhs=10, max_tiles=1250)
+LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, loss="energy", iters=(1, 2, 3, 5), rhs=10, max_tiles=1250)
 
 
 def learned_block(cmg, torch, spec, steps, world, dev):
@@ -373,7 +373,7 @@ def learned_block(cmg, torch, spec, steps, world, dev):
                                   az_ch=U + 2)
     t1 = time.perf_counter()
     net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
-                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"])
+                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
     torch.cuda.synchronize()
     t2 = time.perf_counter()
 
@@ -398,7 +398,7 @@ def learned_block(cmg, torch, spec, steps, world, dev):
     S.set_learned(None)
     _, _, ty = G.tiles()
     lm = ty == cmg.LEAF
-    return {"hidden": LEARNED["hidden"],
+    return {"hidden": LEARNED["hidden"], "loss": LEARNED["loss"],
             "damping": LEARNED["damping"], "train_pairs": int(pairs["rho"].shape[0]), "collect_s": round(t1 - t0, 3),
             "train_s": round(t2 - t1, 3), "epochs": LEARNED["epochs"], "loss_first_epoch": float(losses[0]),
             "loss_last_epoch": float(losses[-1]), "plain_ms": round(plain_ms, 4), "plain_pcg_iters": plain_it,

@@ -51,7 +51,7 @@ EXPORTS = [
     "cmg_grid_gather_device_tiles", "cmg_grid_scatter_device_tiles",
     "cmg_learned_create", "cmg_learned_destroy", "cmg_learned_num_params", "cmg_learned_get_params",
     "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
-    "cmg_learned_train", "cmg_amg_solver_set_learned", "cmg_amg_solver_learned_status",
+    "cmg_learned_train", "cmg_learned_set_loss", "cmg_amg_solver_set_learned", "cmg_amg_solver_learned_status",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -140,6 +140,7 @@ def lib():
             "cmg_learned_forward": (I, [P, I, I, P]),
             "cmg_learned_gradient": (I, [P, I, I, P, P]),
             "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
+            "cmg_learned_set_loss": (I, [P, I]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
         }
@@ -521,6 +522,10 @@ class LearnedNet:
         _check(self.L.cmg_learned_set_samples(self.h, rho.shape[0], _p(rho), _p(diag), _p(types),
                                               _p(tg) if tg is not None else None), "set_samples")
         self.num_samples = rho.shape[0]
+
+    def set_loss(self, kind):
+        """"mse" (squared error, default) or "energy" (tile Laplacian-weighted)."""
+        _check(self.L.cmg_learned_set_loss(self.h, {"mse": 0, "energy": 1}[kind]), "set_loss")
 
     def forward(self, first=0, n=None):
         n = self.num_samples - first if n is None else n

@@ -59,7 +59,7 @@ void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaSt
 void launch_net_forward(int H, const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
                         const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st);
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
-                      const void* pack, const float* bias, float* grad, float* loss, cudaStream_t st);
+                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st);
 void launch_net_reduce_adam(const float* grad, int nb, int np, float scale, float* gout, float* p, float* m, float* v, float lr, int step,
                             bool update, cudaStream_t st);
 // flexible-CG beta (Polak-Ribiere): gamma = r.z, beta = -alpha (Ap.z) / gamma_old

@@ -414,12 +414,13 @@ __global__ void __launch_bounds__(kNetThreads) k_net_forward(NetIn I, int ns, co
     }
 }
 
-// Forward and backward pass of one batch: per batch slot b (sample idx[b]) the gradient of
-// sum over INTERIOR cells of (f - target * D/S)^2 goes to grad[b][kParams] and the sum to loss[b].
+// Forward and backward pass of one batch: per batch slot b (sample idx[b]) the gradient of the
+// tile's loss (sum over INTERIOR cells of (f - target * D/S)^2, or its energy form, see below)
+// goes to grad[b][kParams] and the loss to loss[b].
 template <int H>
 __global__ void __launch_bounds__(kNetThreads) k_net_train(NetIn I, int nb, const __nv_bfloat16* __restrict__ pack,
                                                            const float* __restrict__ bias_g, float* __restrict__ grad,
-                                                           float* __restrict__ loss) {
+                                                           float* __restrict__ loss, int loss_kind) {
     using Dm = NetDims<H>;
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* x0 = reinterpret_cast<__nv_bfloat16*>(smem);
@@ -461,15 +462,36 @@ __global__ void __launch_bounds__(kNetThreads) k_net_train(NetIn I, int nb, cons
             store_output(acc, ys);
         }
         __syncthreads();
-        // dL/df = 2 (f - target D/S) on INTERIOR cells, into channel 0 of dy
+        // e = f - target D/S on INTERIOR cells (0 elsewhere).  Loss kind 0: sum e^2, dL/df = 2 e.
+        // Kind 1 (energy): e^T L e with L the 7-point Laplacian of the tile (6 on the diagonal,
+        // -1 per neighbour inside the tile, zero outside), dL/df = 2 (L e) on INTERIOR cells.
         const float sc = st.D / st.S;
+        float e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = st.in[u] ? __fsub_rn(ys[4 * threadIdx.x + u], __fmul_rn(st.tgt[u], sc)) : 0.0f;
+        if (loss_kind == 1) {
+            __syncthreads();  // every thread has read its f
+#pragma unroll
+            for (int u = 0; u < 4; ++u) ys[4 * threadIdx.x + u] = e[u];
+            __syncthreads();
+        }
         float l = 0.0f;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int cell = 4 * threadIdx.x + u;
-            const float e = st.in[u] ? __fsub_rn(ys[cell], __fmul_rn(st.tgt[u], sc)) : 0.0f;
-            l = __fmaf_rn(e, e, l);
-            dy[pad_vox(cell >> 6, (cell >> 3) & 7, cell & 7) * 8] = __float2bfloat16_rn(2.0f * e);
+            const int cell = 4 * threadIdx.x + u, ci = cell >> 6, cj = (cell >> 3) & 7, ck = cell & 7;
+            float g = e[u];
+            if (loss_kind == 1) {
+                float nbs = 0.0f;
+                if (ci > 0) nbs += ys[cell - 64];
+                if (ci < 7) nbs += ys[cell + 64];
+                if (cj > 0) nbs += ys[cell - 8];
+                if (cj < 7) nbs += ys[cell + 8];
+                if (ck > 0) nbs += ys[cell - 1];
+                if (ck < 7) nbs += ys[cell + 1];
+                g = st.in[u] ? __fsub_rn(6.0f * e[u], nbs) : 0.0f;
+            }
+            l = __fmaf_rn(e[u], g, l);
+            dy[pad_vox(ci, cj, ck) * 8] = __float2bfloat16_rn(2.0f * g);
         }
         const float lt = block_sum_f(l, red);  // synchronises: dy is complete
         if (threadIdx.x == 0) loss[b] = lt;
@@ -596,16 +618,16 @@ void launch_net_forward(int H, const float* r, const float* az, const float* dia
 }
 
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
-                      const void* pack, const float* bias, float* grad, float* loss, cudaStream_t st) {
+                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st) {
     if (nb <= 0) return;
     const NetIn I{rho, nullptr, diag, types, target, idx, 0};
     const int sms = num_sms();
     const int blocks = nb < sms ? nb : sms;
     note_kernel_launch();
     if (H == 16)
-        k_net_train<16><<<blocks, kNetThreads, train_smem<16>(), st>>>(I, nb, (const __nv_bfloat16*)pack, bias, grad, loss);
+        k_net_train<16><<<blocks, kNetThreads, train_smem<16>(), st>>>(I, nb, (const __nv_bfloat16*)pack, bias, grad, loss, loss_kind);
     else
-        k_net_train<8><<<blocks, kNetThreads, train_smem<8>(), st>>>(I, nb, (const __nv_bfloat16*)pack, bias, grad, loss);
+        k_net_train<8><<<blocks, kNetThreads, train_smem<8>(), st>>>(I, nb, (const __nv_bfloat16*)pack, bias, grad, loss, loss_kind);
 }
 
 void launch_net_reduce_adam(const float* grad, int nb, int np, float scale, float* gout, float* p, float* m, float* v, float lr, int step,

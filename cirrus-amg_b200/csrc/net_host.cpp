@@ -149,11 +149,11 @@ int Net::forward(int first, int n, float* out_host) {
     return rc;
 }
 
-// loss = sum over samples and INTERIOR cells of (f - target D/S)^2 / (n * 512) and its gradient
+// loss = sum over samples of the tile loss (loss_kind) / (n * 512) and its gradient
 int Net::gradient(int first, int n, double* loss_out, float* grad_host) {
     if (int rc = ensure_batch(n)) return rc;
     const size_t o = (size_t)first * kCells;
-    launch_net_train(H, rho + o, diag + o, types + o, target + o, nullptr, n, pack, bias, grad, loss, st);
+    launch_net_train(H, rho + o, diag + o, types + o, target + o, nullptr, n, pack, bias, grad, loss, loss_kind, st);
     const float scale = 1.0f / ((float)n * kCells);
     launch_net_reduce_adam(grad, n, np, scale, gsum, p, m, v, 0.0f, 0, false, st);
     std::vector<float> l(n);
@@ -186,7 +186,7 @@ int Net::train(int epochs, int batch, float lr, unsigned long long seed, float* 
         NCK(cudaMemcpyAsync(idx, perm.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
         for (int b0 = 0; b0 < ns; b0 += batch) {
             const int nb = ns - b0 < batch ? ns - b0 : batch;
-            launch_net_train(H, rho, diag, types, target, idx + b0, nb, pack, bias, grad, loss + b0, st);
+            launch_net_train(H, rho, diag, types, target, idx + b0, nb, pack, bias, grad, loss + b0, loss_kind, st);
             launch_net_reduce_adam(grad, nb, np, 1.0f / ((float)nb * kCells), nullptr, p, m, v, lr, ++adam_step, true, st);
             launch_net_pack(H, p, pack, bias, st);
         }

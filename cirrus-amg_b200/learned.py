@@ -60,12 +60,13 @@ def collect_pairs(G, solver, coeff_ch, rhs_list, iters=(1, 2, 3, 5), z_ch=13, x0
     return {k: np.concatenate(v) for k, v in out.items()}
 
 
-def train(pairs, hidden=16, epochs=20, batch=256, lr=2e-3, seed=0, net=None, damping=1.0):
+def train(pairs, hidden=16, epochs=20, batch=256, lr=2e-3, seed=0, net=None, damping=1.0, loss="mse"):
     """A LearnedNet trained on `pairs` (from collect_pairs); returns (net, per-epoch loss).
     damping scales the trained network's output (its last layer is linear): the step length
-    of the learned correction inside the preconditioner."""
+    of the learned correction inside the preconditioner.  loss: "mse" or "energy"."""
     if net is None:
         net = cmg.LearnedNet(hidden, seed)
+    net.set_loss(loss)
     net.set_samples(pairs["rho"], pairs["diag"], pairs["types"], pairs["d"])
     losses = net.train(epochs, batch, lr, seed)
     if damping != 1.0:

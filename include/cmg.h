@@ -216,7 +216,7 @@ int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage);
  * each mu-cycle, rho = r - A z being the residual the cycle leaves (S: its RMS on the
  * tile, D: the tile's largest diagonal).  The solve then runs flexible CG (Polak-Ribiere
  * beta), judges the result by the true residual |b - A x| / |b| and falls back to the
- * plain solve when that exceeds 4 tol or the solve does not converge.
+ * plain solve when that exceeds 10 tol or the solve does not converge.
  * Samples are tiles of 512 cells (cell i*64 + j*8 + k): rho, the diagonal of A (the
  * coefficient channel coeff+3), cell types and the target error d = A^-1 rho.
  * The net keeps its parameters, Adam state and samples on the device; training runs
@@ -231,7 +231,11 @@ int cmg_learned_set_params(cmg_learned* net, const float* host, int n); /* also 
 int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target);
 /* correction (S/D) f on INTERIOR cells (0 elsewhere) of samples first..first+n-1 */
 int cmg_learned_forward(cmg_learned* net, int first, int n, float* out);
-/* mean loss sum (f - target D/S)^2 / (n 512) over samples first..first+n-1 and its gradient */
+/* training loss per tile, e = f - target D/S on INTERIOR cells (0 elsewhere):
+ * kind 0 (default) sum e^2; kind 1 (energy) e^T L e, L the tile's 7-point Laplacian
+ * (6 on the diagonal, -1 per neighbour inside the tile), which weighs rough errors as PCG does */
+int cmg_learned_set_loss(cmg_learned* net, int kind);
+/* mean loss (sum of tile losses) / (n 512) over samples first..first+n-1 and its gradient */
 int cmg_learned_gradient(cmg_learned* net, int first, int n, double* loss, float* grad);
 /* Adam (beta 0.9/0.999) over shuffled batches; epoch_loss[e] (may be NULL) */
 int cmg_learned_train(cmg_learned* net, int epochs, int batch, float lr, unsigned long long seed, float* epoch_loss);

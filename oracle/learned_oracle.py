@@ -9,7 +9,8 @@ cores, so that its forward pass, loss and gradients can be checked:
       3: diag / D on INTERIOR cells (D = max |diag| over INTERIOR cells)   4-7: 0
   a1 = relu(conv(x, W1) + b1); a2 = relu(conv(a1, W2) + b2); f = conv(a2, W3)
   correction = (S / D) f on INTERIOR cells
-  loss = sum over tiles and INTERIOR cells of (f - target D / S)^2 / (n 512)
+  loss = sum over tiles and INTERIOR cells of (f - target D / S)^2 / (n 512), or with the
+         energy loss e^T L e per tile (L: the tile's 7-point Laplacian, zero outside)
 
 Every convolution is 3x3x3 with tap = dx*9 + dy*3 + dz.  The GPU path rounds the
 features, the weights and the activations a1, a2, 2 (f - t), dz2, dz1 to BF16 and
@@ -123,8 +124,19 @@ def _forward_net(p, H, x, emulate_bf16):
     return f, (x, a1, a2, W1, W2, W3)
 
 
-def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True):
-    """Mean loss and its gradient (layout of `layout(H)`)."""
+def tile_laplacian(e):
+    """7-point Laplacian of [n, 512] cell values within each tile: 6 e - (neighbours inside the tile)."""
+    g = np.asarray(e, dtype=np.float64).reshape(-1, 8, 8, 8)
+    p = np.zeros((g.shape[0], 10, 10, 10))
+    p[:, 1:9, 1:9, 1:9] = g
+    nb = (p[:, :-2, 1:-1, 1:-1] + p[:, 2:, 1:-1, 1:-1] + p[:, 1:-1, :-2, 1:-1] + p[:, 1:-1, 2:, 1:-1] +
+          p[:, 1:-1, 1:-1, :-2] + p[:, 1:-1, 1:-1, 2:])
+    return (6.0 * g - nb).reshape(-1, 512)
+
+
+def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True, kind=0):
+    """Mean loss and its gradient (layout of `layout(H)`); kind 0: sum e^2 per tile,
+    kind 1: e^T L e with L = tile_laplacian."""
     x, S, D, inter, ok = features(rho, diag, types, emulate_bf16)
     n = x.shape[0]
     f, (x, a1, a2, W1, W2, W3) = _forward_net(p, H, x, emulate_bf16)
@@ -132,9 +144,10 @@ def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True):
     tgt = np.asarray(target, dtype=np.float64).reshape(-1, 512) * np.where(ok, D / np.where(ok, S, 1.0), 0.0)[:, None]
     m = inter & ok[:, None]
     e = np.where(m, f.reshape(-1, 512) - tgt, 0.0)
+    g = np.where(m, tile_laplacian(e), 0.0) if kind == 1 else e
     scale = 1.0 / (n * 512)
-    loss = (e * e).sum() * scale
-    dy = r(2.0 * e).reshape(n, 8, 8, 8, 1)
+    loss = (e * g).sum() * scale
+    dy = r(2.0 * g).reshape(n, 8, 8, 8, 1)
     gW3 = conv_weight_grad(a2, dy)
     dz2 = r(conv_input_grad(dy, W3) * (a2 > 0))
     gW2 = conv_weight_grad(a1, dz2)

@@ -57,15 +57,16 @@ def test_forward_matches_oracle(H):
         assert np.abs(out[s] - ref[s]).max() <= 1e-2 * m, s
 
 
-@pytest.mark.parametrize("H", [8, 16])
-def test_gradient_matches_oracle(H):
+@pytest.mark.parametrize("H,kind", [(8, 0), (16, 0), (8, 1), (16, 1)])
+def test_gradient_matches_oracle(H, kind):
     rho, diag, types, target = random_samples(10, 30 + H)
     net = cmg.LearnedNet(H, seed=2)
     p = random_params(H, 40 + H)
     net.set_params(p)
+    net.set_loss(["mse", "energy"][kind])
     net.set_samples(rho, diag, types, target)
     loss, g = net.gradient()
-    rl, rg = LO.loss_and_grad(p, H, rho, diag, types, target)
+    rl, rg = LO.loss_and_grad(p, H, rho, diag, types, target, kind=kind)
     assert abs(loss - rl) <= 1e-3 * rl
     L = LO.layout(H)
     for a, b in [("W1", "B1"), ("B1", "W2"), ("W2", "B2"), ("B2", "W3"), ("W3", "n")]:
@@ -145,9 +146,9 @@ def test_nonfinite_net_falls_back_to_plain():
 def test_trained_net_against_plain(capsys):
     """What the trained network gains: trained on other right-hand sides of the uniform 64^3
     grid (seeds 100-109), compared with the plain solve on the benchmark rhs (seed 0).
-    The damped net (output x 0.5) saves one of the plain solve's 8 PCG iterations."""
+    The damped net (output x 0.5, energy loss) saves one of the plain solve's 8 PCG iterations."""
     G, solver, pairs, ty = _uniform_pairs(3, list(range(100, 110)), iters=(1, 2, 3, 5))
-    net, losses = learned.train(pairs, hidden=8, epochs=30, batch=256, lr=2e-3, seed=0, damping=0.5)
+    net, losses = learned.train(pairs, hidden=8, epochs=30, batch=256, lr=2e-3, seed=0, damping=0.5, loss="energy")
     b = uniform_rhs(ty == cmg.LEAF, 0)
     rows = learned.compare(G, solver, net, [b, b])
     with capsys.disabled():

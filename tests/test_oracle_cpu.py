@@ -349,9 +349,11 @@ def test_divergence_without_coeff_equals_coefficient_form_on_uniform_faces():
     assert np.array_equal(g.channel(1)[m], g.channel(2)[m])
 
 
-def test_learned_oracle_gradient_matches_finite_differences():
+@pytest.mark.parametrize("kind", [0, 1])
+def test_learned_oracle_gradient_matches_finite_differences(kind):
     """The FP64 restatement of the learned smoother's network: its backward pass against
-    central differences of its own loss (no BF16 rounding), on two tiles."""
+    central differences of its own loss (no BF16 rounding), on two tiles, for the squared
+    error and the energy loss."""
     from oracle import learned_oracle as LO
 
     H = 8
@@ -366,7 +368,7 @@ def test_learned_oracle_gradient_matches_finite_differences():
     p = rng.standard_normal(L["n"]) * 0.2
     p[L["B1"]:L["W2"]] = 0.3
     p[L["B2"]:L["W3"]] = 0.3
-    _, g = LO.loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=False)
+    _, g = LO.loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=False, kind=kind)
     picks = list(rng.choice(L["n"], 24, replace=False)) + [L["B1"], L["B2"] + 1, L["W3"] + 5]
     eps = 1e-6
     for i in picks:
@@ -374,9 +376,9 @@ def test_learned_oracle_gradient_matches_finite_differences():
             continue  # padded input channels: zero input, zero gradient
         q = p.copy()
         q[i] += eps
-        lp, _ = LO.loss_and_grad(q, H, rho, diag, types, target, emulate_bf16=False)
+        lp, _ = LO.loss_and_grad(q, H, rho, diag, types, target, emulate_bf16=False, kind=kind)
         q[i] -= 2 * eps
-        lm, _ = LO.loss_and_grad(q, H, rho, diag, types, target, emulate_bf16=False)
+        lm, _ = LO.loss_and_grad(q, H, rho, diag, types, target, emulate_bf16=False, kind=kind)
         fd = (lp - lm) / (2 * eps)
         assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i])) + 1e-7, (i, fd, g[i])
 
