@@ -51,7 +51,7 @@ EXPORTS = [
     "cmg_grid_gather_device_tiles", "cmg_grid_scatter_device_tiles",
     "cmg_learned_create", "cmg_learned_destroy", "cmg_learned_num_params", "cmg_learned_get_params",
     "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
-    "cmg_learned_train", "cmg_learned_set_loss", "cmg_amg_solver_set_learned", "cmg_amg_solver_learned_status",
+    "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned", "cmg_amg_solver_learned_status",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -141,6 +141,7 @@ def lib():
             "cmg_learned_gradient": (I, [P, I, I, P, P]),
             "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
             "cmg_learned_set_loss": (I, [P, I]),
+            "cmg_learned_set_inference": (I, [I]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
         }
@@ -479,6 +480,11 @@ class AMGSolver:
         n = ctypes.c_longlong(0)
         _check(self.L.cmg_amg_last_solve_launches(self.h, ctypes.byref(n)), "last_solve_launches")
         return n.value
+
+
+def set_learned_inference(kind):
+    """Inference kernel of the learned smoother: "mma.sync" (default) or "tcgen05"."""
+    _check(lib().cmg_learned_set_inference({"mma.sync": 0, "tcgen05": 1}[kind]), "set_learned_inference")
 
 
 class LearnedNet:

@@ -480,6 +480,11 @@ int cmg_learned_gradient(cmg_learned* net, int first, int n, double* loss, float
     return net->n.gradient(first, n, loss, grad);
     GUARD_END
 }
+int cmg_learned_set_inference(int kind) {
+    if (kind != 0 && kind != 1) return fail(CMG_ERR_INVALID, "cmg_learned_set_inference: kind must be 0 (mma.sync) or 1 (tcgen05)");
+    cmg::net_set_inference_kind(kind);
+    return 0;
+}
 int cmg_learned_set_loss(cmg_learned* net, int kind) {
     if (!net || (kind != 0 && kind != 1)) return fail(CMG_ERR_INVALID, "cmg_learned_set_loss: kind must be 0 or 1");
     net->n.loss_kind = kind;

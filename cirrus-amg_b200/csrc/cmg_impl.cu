@@ -826,7 +826,8 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
         }
         last_true_rel = bb > 0.0 ? std::sqrt(res / bb) : 0.0;
         last_learned_iters = it;
-        const bool judged_ok = rc == 0 && std::isfinite(last_true_rel) &&
+        const bool tc_ok = net_take_tc_error() == 0;
+        const bool judged_ok = rc == 0 && tc_ok && std::isfinite(last_true_rel) &&
                                (sync_stride <= 0 || (converged && last_true_rel <= kLearnedJudgeSlack * tol));
         if (!judged_ok && rc != 2) {
             // plain fallback from the saved right-hand side

@@ -53,6 +53,9 @@ size_t coeff16_bytes(const DevGrid& g);
 int net_params(int H);      // fp32 parameters
 int net_pack_elems(int H);  // bf16 elements of the packed operands
 bool net_init();
+void net_set_inference_kind(int kind);  // 0: mma.sync (default), 1: tcgen05
+int net_inference_kind();
+int net_take_tc_error();  // 1 if a tcgen05 inference launch timed out waiting for its MMAs (then cleared)
 void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaStream_t st);
 // samples s < ns are tiles (idx ? idx[s] : t0 + s) of the planes; rho = r - az (az may be null);
 // out[t] += (S/D) f (or = with overwrite) on INTERIOR cells

@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <type_traits>
 
 #include "kernels.hpp"
 
@@ -414,6 +415,263 @@ __global__ void __launch_bounds__(kNetThreads) k_net_forward(NetIn I, int ns, co
     }
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05.mma, accumulators in TMEM)
+// ---------------------------------------------------------------------------
+// Activations are channel-group-major planes: element (voxel v, channel c) of a buffer with
+// CG groups sits at ((c >> 3) * kTcVox + v) * 8 + (c & 7), 16 bytes per voxel and group.  One
+// MMA computes one i-plane of the tile (M = 64 voxels: 8 rows j of 8 voxels k) against N
+// output channels for one 16-wide K step.  In the no-swizzle K-major operand layout the
+// 8-voxel rows are core matrices (128 contiguous bytes), the 8 rows sit 10 voxels (160 B)
+// apart (the stride-dimension offset) and the two K halves are the two channel groups
+// (kTcVox voxels apart) or, with 8 input channels, the next tap (the leading-dimension
+// offset).  A tap's shifted operand is therefore only a different start address: no im2col.
+// Weights are stored per K step as [K half][n][8] (core matrices of 8 output channels).
+// The accumulator of plane p occupies TMEM columns p*N .. p*N+N-1; row r of an M = 64 MMA
+// lives in TMEM lane (r % 16) + 32 (r / 16), so warp w reads rows 16w .. 16w+15 through
+// its own 32-lane quarter.
+constexpr int kTcVox = 1008;  // padded voxels per group plane (16 beyond the grid: K padding reads there)
+
+__device__ int g_net_tc_error;  // set when an MMA completion wait gives up
+
+template <int H>
+struct TcDims {
+    static constexpr int CG = H / 8;
+    static constexpr int S1 = 14, SH = CG == 2 ? 27 : 14;  // K steps of 16
+    static constexpr int W1 = 0, W2 = W1 + S1 * 2 * H * 8, W3 = W2 + SH * 2 * H * 8, kW = W3 + SH * 2 * 8 * 8;  // bf16 elements
+    static constexpr int kAct = kTcVox * H;
+    static constexpr int kCols = H == 16 ? 128 : 64;  // TMEM columns: 8 planes x N
+    // shared memory: a1 | x0 and a2 in the same place (x0 is dead once layer 1 has run) | weights
+    static constexpr int kActElems = 2 * kAct;
+};
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) |
+           (1ull << 46);  // no swizzle, version 1
+}
+// kind::f16 instruction descriptor: F32 accumulator, BF16 A and B, both K-major, M = 64
+__host__ __device__ constexpr uint32_t umma_idesc(int N) { return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | (4u << 24); }
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(done)
+                 : "r"(mbar), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+// bounded wait for an MMA completion phase
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (int i = 0; i < (1 << 20); ++i)
+        if (mbar_try(mbar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
+          "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Issue one layer (thread 0): for each i-plane p and K step s, D[p] (+)= A(p, s) B(s).
+// CGI: 8-channel groups of the input; N: output columns; steps: K steps of 16.
+template <int CGI, int N>
+__device__ __forceinline__ void tc_issue_layer(uint32_t in_s, uint32_t w_s, int steps, uint32_t taddr) {
+    constexpr uint32_t idesc = umma_idesc(N);
+    const uint32_t b_lbo = N * 16, b_sbo = 128;
+#pragma unroll 1
+    for (int st = 0; st < steps; ++st) {  // K outer, planes inner: 8 independent accumulators in flight
+        int t0, lbo;
+        if constexpr (CGI == 2) {
+            t0 = st;
+            lbo = kTcVox * 16;
+        } else {
+            t0 = 2 * st;
+            lbo = (t0 + 1 <= 26 ? tap_off(t0 + 1) - tap_off(t0) : 1) * 16;  // tap 27: zero weights
+        }
+        const uint64_t b = umma_desc(w_s + (uint32_t)(st * 2 * N * 8 * 2), b_lbo, b_sbo);
+        const uint32_t a0 = in_s + (uint32_t)(pad_vox(0, 0, 0) + tap_off(t0)) * 16u;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            const uint64_t a = umma_desc(a0 + (uint32_t)(p * 100 * 16), (uint32_t)lbo, 160u);
+            umma_f16(taddr + (uint32_t)(p * N), a, b, idesc, st > 0 ? 1u : 0u);
+        }
+    }
+}
+
+// Hidden-layer epilogue from TMEM: all eight planes' accumulators loaded before one wait, then
+// relu(acc + bias) to BF16 into the channel-group-major buffer out (rows 16w..16w+15 of each
+// plane, held by lanes 0-15 of warp w).
+template <int H>
+__device__ __forceinline__ void tc_epilogue_hidden(uint32_t lane_base, int warp, int lane, const float* bias, __nv_bfloat16* out) {
+    constexpr int CG = H / 8;
+    float v[8][H];
+#pragma unroll
+    for (int pl = 0; pl < 8; ++pl) {
+        if constexpr (H == 16) tmem_ld16(lane_base + pl * H, v[pl]);
+        else tmem_ld8(lane_base + pl * H, v[pl]);
+    }
+    tmem_wait_ld();
+    if (lane >= 16) return;
+    const int r = 16 * warp + lane;
+#pragma unroll
+    for (int pl = 0; pl < 8; ++pl) {
+        const int vx = pad_vox(pl, r >> 3, r & 7);
+#pragma unroll
+        for (int g = 0; g < CG; ++g) {
+            __nv_bfloat162 o[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                o[e] = __floats2bfloat162_rn(fmaxf(__fadd_rn(v[pl][8 * g + 2 * e], bias[8 * g + 2 * e]), 0.0f),
+                                             fmaxf(__fadd_rn(v[pl][8 * g + 2 * e + 1], bias[8 * g + 2 * e + 1]), 0.0f));
+            *reinterpret_cast<uint4*>(out + (g * kTcVox + vx) * 8) = *reinterpret_cast<const uint4*>(o);
+        }
+    }
+}
+
+template <int H>
+__global__ void __launch_bounds__(kNetThreads) k_net_forward_tc(NetIn I, int ns, const __nv_bfloat16* __restrict__ pack,
+                                                                const float* __restrict__ bias_g, float* __restrict__ out, int overwrite) {
+    using Dm = NetDims<H>;
+    using Tc = TcDims<H>;
+    constexpr int CG = Tc::CG;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* a1 = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* x0 = a1 + Tc::kAct;
+    __nv_bfloat16* a2 = x0;  // group 0 of a2 covers x0 exactly; both keep zero halos
+    __nv_bfloat16* wt = a2 + Tc::kAct;
+    float* bias = reinterpret_cast<float*>(wt + Tc::kW);
+    float* ys = bias + 2 * H;
+    float* red = ys + kCells;                                          // 32 floats
+    unsigned long long* mbar = reinterpret_cast<unsigned long long*>(red + 32);  // 8-byte aligned
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    zero_smem(smem, 2 * Tc::kActElems);
+    // weights: [step][K half][n][8] from the packed [n][k] rows (k = step*16 + half*8 + c)
+    for (int e = tid; e < Tc::kW; e += kNetThreads) {
+        int base, n_rows, ks, src0, rel = e;
+        if (e < Tc::W2) {
+            base = Tc::W1, n_rows = H, ks = Dm::KS1, src0 = Dm::F1;
+        } else if (e < Tc::W3) {
+            base = Tc::W2, n_rows = H, ks = Dm::KSH, src0 = Dm::F2;
+        } else {
+            base = Tc::W3, n_rows = 8, ks = Dm::KSH, src0 = Dm::F3;
+        }
+        rel = e - base;
+        const int c = rel & 7, n = (rel >> 3) % n_rows, hs = (rel >> 3) / n_rows, half = hs & 1, stp = hs >> 1;
+        wt[e] = pack[src0 + n * ks + stp * 16 + half * 8 + c];
+    }
+    if (tid < 2 * H) bias[tid] = bias_g[tid];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(Tc::kCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = *tslot;
+    const uint32_t mb = smem_u32(mbar);
+    const uint32_t lane_base = taddr + ((uint32_t)(32 * warp) << 16);
+    uint32_t phase = 0;
+    bool ok = true;
+
+    // one layer: issue, wait, read the accumulators of this warp's rows
+    auto run_layer = [&](auto cgi_tag, auto n_tag, uint32_t in_s, uint32_t w_s, int steps) -> bool {
+        constexpr int CGI = decltype(cgi_tag)::value, N = decltype(n_tag)::value;
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            tc_issue_layer<CGI, N>(in_s, w_s, steps, taddr);
+            umma_commit(mb);
+        }
+        const bool done = mbar_wait(mb, phase);
+        phase ^= 1u;
+        tc_fence_after();
+        return __syncthreads_and(done ? 1 : 0) != 0;
+    };
+
+    for (int s = blockIdx.x; s < ns && ok; s += gridDim.x) {
+        const Staged st = stage_features(I, s, x0, red);
+        const int t = I.idx ? I.idx[s] : I.t0 + s;
+        if (st.S == 0.0f) {
+            if (overwrite) st4(out + (size_t)t * kCells + 4 * tid, make_float4(0.f, 0.f, 0.f, 0.f));
+            continue;  // uniform over the block
+        }
+        // layer 1: x0 (8 channels) -> a1
+        ok = run_layer(std::integral_constant<int, 1>{}, std::integral_constant<int, H>{}, smem_u32(x0), smem_u32(wt + Tc::W1), Tc::S1);
+        if (!ok) break;
+        tc_epilogue_hidden<H>(lane_base, warp, lane, bias, a1);
+        // layer 2: a1 -> a2
+        ok = run_layer(std::integral_constant<int, CG>{}, std::integral_constant<int, H>{}, smem_u32(a1), smem_u32(wt + Tc::W2), Tc::SH);
+        if (!ok) break;
+        tc_epilogue_hidden<H>(lane_base, warp, lane, bias + H, a2);
+        // layer 3: a2 -> one channel (N = 8, column 0)
+        ok = run_layer(std::integral_constant<int, CG>{}, std::integral_constant<int, 8>{}, smem_u32(a2), smem_u32(wt + Tc::W3), Tc::SH);
+        if (!ok) break;
+        {
+            float v[8][8];
+#pragma unroll
+            for (int pl = 0; pl < 8; ++pl) tmem_ld8(lane_base + pl * 8, v[pl]);
+            tmem_wait_ld();
+            if (lane < 16) {
+#pragma unroll
+                for (int pl = 0; pl < 8; ++pl) ys[pl * 64 + 16 * warp + lane] = v[pl][0];
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        const float sc = st.S / st.D;
+        float* o = out + (size_t)t * kCells + 4 * tid;
+        float4 z = overwrite ? make_float4(0.f, 0.f, 0.f, 0.f) : ldcg4(o);
+        float zz[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (st.in[u]) zz[u] = __fmaf_rn(sc, ys[4 * tid + u], zz[u]);
+        st4(o, make_float4(zz[0], zz[1], zz[2], zz[3]));
+        __syncthreads();  // ys and x0 are rewritten by the next sample
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(&g_net_tc_error, 1);
+        mbar_wait(mb, phase ^ 1u);  // the outstanding phase, bounded
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(Tc::kCols) : "memory");
+}
+
 // Forward and backward pass of one batch: per batch slot b (sample idx[b]) the gradient of the
 // tile's loss (sum over INTERIOR cells of (f - target * D/S)^2, or its energy form, see below)
 // goes to grad[b][kParams] and the loss to loss[b].
@@ -571,7 +829,15 @@ size_t train_smem() {
     return 2 * (size_t)(2 * Dm::kAct8 + 3 * Dm::kActH + Dm::kPack) + sizeof(float) * (2 * H + kCells + kNetThreads);
 }
 
-int g_fwd_blocks[2] = {0, 0};  // resident forward blocks per SM (H = 8, 16)
+template <int H>
+size_t forward_tc_smem() {
+    using Tc = TcDims<H>;
+    return 2 * (size_t)(Tc::kActElems + Tc::kW) + sizeof(float) * (2 * H + kCells + 32) + 16;
+}
+
+int g_fwd_blocks[2] = {0, 0};     // resident forward blocks per SM (H = 8, 16), mma.sync kernel
+int g_fwd_tc_blocks[2] = {0, 0};  // the same for the tcgen05 kernel
+int g_infer_kind = 0;             // 0: mma.sync inference kernel (measured faster at N = 8), 1: tcgen05
 
 }  // namespace
 
@@ -585,9 +851,19 @@ bool net_init() {
     ok = ok && cudaFuncSetAttribute(k_net_train<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem<8>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_net_train<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem<16>()) == cudaSuccess;
     if (!ok) return false;
+    ok = ok && cudaFuncSetAttribute(k_net_forward_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_tc_smem<8>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_net_forward_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_tc_smem<16>()) == cudaSuccess;
+    if (!ok) return false;
     ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_blocks[0], k_net_forward<8>, kNetThreads, forward_smem<8>()) == cudaSuccess &&
-         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_blocks[1], k_net_forward<16>, kNetThreads, forward_smem<16>()) == cudaSuccess;
-    return ok && g_fwd_blocks[0] > 0 && g_fwd_blocks[1] > 0;
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_blocks[1], k_net_forward<16>, kNetThreads, forward_smem<16>()) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_tc_blocks[0], k_net_forward_tc<8>, kNetThreads, forward_tc_smem<8>()) ==
+             cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_fwd_tc_blocks[1], k_net_forward_tc<16>, kNetThreads, forward_tc_smem<16>()) ==
+             cudaSuccess;
+    // each resident tcgen05 block holds 64 or 128 of the SM's 512 TMEM columns
+    if (g_fwd_tc_blocks[0] > 8) g_fwd_tc_blocks[0] = 8;
+    if (g_fwd_tc_blocks[1] > 4) g_fwd_tc_blocks[1] = 4;
+    return ok && g_fwd_blocks[0] > 0 && g_fwd_blocks[1] > 0 && g_fwd_tc_blocks[0] > 0 && g_fwd_tc_blocks[1] > 0;
 }
 
 static int num_sms() {
@@ -608,6 +884,25 @@ void launch_net_forward(int H, const float* r, const float* az, const float* dia
                         const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st) {
     if (ns <= 0) return;
     const NetIn I{r, az, diag, types, nullptr, idx, t0};
+    if (g_infer_kind == 1) {
+        // resident blocks per SM from shared memory (1 KB reserved per block) and TMEM (512 columns)
+        int dev = 0, smem_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        const size_t per = (H == 16 ? forward_tc_smem<16>() : forward_tc_smem<8>()) + 1024;
+        int per_sm = (int)((size_t)smem_sm / per);
+        const int tmem_cap = 512 / (H == 16 ? TcDims<16>::kCols : TcDims<8>::kCols);
+        if (per_sm > tmem_cap) per_sm = tmem_cap;
+        if (per_sm < 1) per_sm = 1;
+        const int cap = num_sms() * per_sm;
+        const int blocks = ns < cap ? ns : cap;
+        note_kernel_launch();
+        if (H == 16)
+            k_net_forward_tc<16><<<blocks, kNetThreads, forward_tc_smem<16>(), st>>>(I, ns, (const __nv_bfloat16*)pack, bias, out, overwrite);
+        else
+            k_net_forward_tc<8><<<blocks, kNetThreads, forward_tc_smem<8>(), st>>>(I, ns, (const __nv_bfloat16*)pack, bias, out, overwrite);
+        return;
+    }
     const int cap = num_sms() * g_fwd_blocks[H == 16 ? 1 : 0];
     const int blocks = ns < cap ? ns : cap;
     note_kernel_launch();
@@ -615,6 +910,16 @@ void launch_net_forward(int H, const float* r, const float* az, const float* dia
         k_net_forward<16><<<blocks, kNetThreads, forward_smem<16>(), st>>>(I, ns, (const __nv_bfloat16*)pack, bias, out, overwrite);
     else
         k_net_forward<8><<<blocks, kNetThreads, forward_smem<8>(), st>>>(I, ns, (const __nv_bfloat16*)pack, bias, out, overwrite);
+}
+
+void net_set_inference_kind(int kind) { g_infer_kind = kind; }
+int net_inference_kind() { return g_infer_kind; }
+// 1 if a tcgen05 inference launch gave up waiting for its MMAs since the last call (and clears it)
+int net_take_tc_error() {
+    int v = 0, z = 0;
+    if (cudaMemcpyFromSymbol(&v, g_net_tc_error, sizeof(int)) != cudaSuccess) return -1;
+    if (v) cudaMemcpyToSymbol(g_net_tc_error, &z, sizeof(int));
+    return v;
 }
 
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,

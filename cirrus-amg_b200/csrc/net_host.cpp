@@ -146,6 +146,10 @@ int Net::forward(int first, int n, float* out_host) {
     int rc = check_cuda(cudaMemcpyAsync(out_host, out, sizeof(float) * c, cudaMemcpyDeviceToHost, st), "forward: read-back");
     if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "forward");
     cudaFree(out);
+    if (!rc && net_take_tc_error() == 1) {
+        set_error("learned forward: a tensor-core MMA did not complete in time");
+        rc = 2;
+    }
     return rc;
 }
 

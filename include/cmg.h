@@ -231,6 +231,10 @@ int cmg_learned_set_params(cmg_learned* net, const float* host, int n); /* also 
 int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target);
 /* correction (S/D) f on INTERIOR cells (0 elsewhere) of samples first..first+n-1 */
 int cmg_learned_forward(cmg_learned* net, int first, int n, float* out);
+/* inference kernel of every net in the process: 0 (default) mma.sync, 1 tcgen05.mma with
+ * TMEM accumulators; both compute the same network (FP32 accumulation, BF16 operands).  With
+ * 8 output channels the tcgen05 MMAs are M = 64, N = 8 and measured slower than mma.sync. */
+int cmg_learned_set_inference(int kind);
 /* training loss per tile, e = f - target D/S on INTERIOR cells (0 elsewhere):
  * kind 0 (default) sum e^2; kind 1 (energy) e^T L e, L the tile's 7-point Laplacian
  * (6 on the diagonal, -1 per neighbour inside the tile), which weighs rough errors as PCG does */

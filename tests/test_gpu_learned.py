@@ -37,14 +37,19 @@ def random_params(H, seed, scale=0.15):
     return p
 
 
-@pytest.mark.parametrize("H", [8, 16])
-def test_forward_matches_oracle(H):
+@pytest.mark.parametrize("H,kind", [(8, "tcgen05"), (16, "tcgen05"), (8, "mma.sync"), (16, "mma.sync")])
+def test_forward_matches_oracle(H, kind):
+    """Both inference kernels (tcgen05 with TMEM accumulators, and mma.sync) against the oracle."""
     rho, diag, types, target = random_samples(12, 10 + H)
     net = cmg.LearnedNet(H, seed=1)
     p = random_params(H, 20 + H)
     net.set_params(p)
     net.set_samples(rho, diag, types, target)
-    out = net.forward()
+    cmg.set_learned_inference(kind)
+    try:
+        out = net.forward()
+    finally:
+        cmg.set_learned_inference("mma.sync")
     ref = LO.forward(p, H, rho, diag, types)
     assert np.all(out[1] == 0) and np.all(out[2] == 0)
     assert np.all(out[(types & cmg.INTERIOR) == 0] == 0)
@@ -75,6 +80,22 @@ def test_gradient_matches_oracle(H, kind):
     # padded input channels 4..7 of W1 get exactly zero gradient
     gw1 = g[L["W1"]:L["B1"]].reshape(H, 27, 8)
     assert np.all(gw1[:, :, 4:] == 0)
+
+
+def test_inference_kernels_agree():
+    """tcgen05 and mma.sync inference on 300 tiles: the same products, summed in different orders."""
+    rho, diag, types, target = random_samples(300, 77)
+    net = cmg.LearnedNet(16, seed=8)
+    net.set_params(random_params(16, 78))
+    net.set_samples(rho, diag, types, target)
+    out_ms = net.forward()
+    cmg.set_learned_inference("tcgen05")
+    try:
+        out_tc = net.forward()
+    finally:
+        cmg.set_learned_inference("mma.sync")
+    scale = np.abs(out_ms).max(axis=1, keepdims=True) + 1e-30
+    assert np.all(np.abs(out_tc - out_ms) <= 1e-2 * scale)
 
 
 def test_gradient_is_deterministic():
@@ -114,6 +135,23 @@ def test_training_reduces_loss():
     l1, _ = net.gradient()
     assert np.all(np.isfinite(losses))
     assert l1 < 0.7 * l0, (l0, l1, losses)
+
+
+def test_learned_solve_with_tcgen05_inference():
+    """The learned solve with the tcgen05 inference kernel: same iterations as with mma.sync
+    and the same solution to FP32 rounding."""
+    G, solver, pairs, ty = _uniform_pairs(2, [100, 101, 102])
+    net, _ = learned.train(pairs, hidden=8, epochs=10, batch=128, lr=2e-3, seed=0, damping=0.5, loss="energy")
+    b = uniform_rhs(ty == cmg.LEAF, 0)
+    rows_ms = learned.compare(G, solver, net, [b])
+    cmg.set_learned_inference("tcgen05")
+    try:
+        rows_tc = learned.compare(G, solver, net, [b])
+    finally:
+        cmg.set_learned_inference("mma.sync")
+    assert not rows_tc[0][5] and rows_tc[0][4] <= 1e-5
+    assert abs(rows_tc[0][2] - rows_ms[0][2]) <= 1
+    assert rows_tc[0][6] <= 1e-4
 
 
 def test_learned_solve_matches_plain():
