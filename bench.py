@@ -163,14 +163,27 @@ WORKLOADS = {
     "uniform64": "uniform 64^3 grid (h0=1/8, level 3), all cells INTERIOR, Dirichlet walls, rhs N(0,1) seed 0 minus mean",
     "batched64": "64 adaptive octrees (seed 2): finest level 4 or 5 within 0.05 of 1-3 solid spheres r~U(0.05,0.15), "
                  "centres U(0.2,0.8)^3, level 3 elsewhere; Fourier-divergence rhs per octree",
+    "moving_sphere": "sequence of adaptive sphere octrees (levels 4/5/6, r=0.1) with the sphere centre moving on a circle of "
+                     "radius 0.25 around (0.5,0.5,0.5) in the z=0.5 plane at 1 revolution per 400 steps; octree, cut-cell "
+                     "operator and Fourier-divergence rhs (seed 1) rebuilt per step",
 }
 BATCH_STREAMS = 16
+
+
+def moving_sphere_spec(step):
+    """Position `step` of the moving-sphere sequence: centre on a circle of radius 0.25, 400 steps per turn."""
+    th = 2.0 * np.pi * step / 400.0
+    c = (0.5 + 0.25 * np.cos(th), 0.5 + 0.25 * np.sin(th), 0.5)
+    return dict(case="shell", params=[4, 6, 5, c[0], c[1], c[2], 0.1, 0.05, 0.15], spheres=[(c[0], c[1], c[2], 0.1)],
+                rhs=("fourier", 1))
 
 
 def instance_specs(name):
     """The octrees of a workload: refinement case and parameters, cut-cell spheres, rhs."""
     if name == "sphere":
         return [dict(case="shell", params=SHELL, spheres=SPHERES, rhs=("fourier", 1))]
+    if name == "moving_sphere":
+        return [moving_sphere_spec(0)]
     if name == "uniform64":
         return [dict(case="uniform", params=[3, 3], spheres=None, rhs=("normal", 0))]
     rng = np.random.default_rng(2)
@@ -406,6 +419,82 @@ def learned_block(cmg, torch, spec, steps, world, dev):
             "rel_residual_true": true_rel,
             "rel_l2_vs_plain_solution": float(np.linalg.norm((xl - xp)[lm].astype(np.float64)) /
                                               np.linalg.norm(xp[lm].astype(np.float64)))}
+
+
+def run_sequence(args, rank, world, local_rank):
+    """The moving-sphere sequence: --steps positions, each with its own octree, cut-cell
+    operator and rhs; at each position the plain and the learned solve (trained once on the
+    first position, on other right-hand sides) are timed on the device.  value = mean plain ms
+    per solve; the learned figures sit in config."""
+    import torch
+
+    import cmg
+    import learned
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    spec0 = moving_sphere_spec(0)
+    G = build_grid(cmg, spec0)
+    S = make_solver(cmg)
+    t0 = time.perf_counter()
+    rhs = training_rhs(cmg, G, spec0, LEARNED["rhs"])
+    pairs = learned.collect_pairs(G, S, COEFF, rhs, iters=LEARNED["iters"], max_tiles=LEARNED["max_tiles"], z_ch=U, x0_ch=U + 1,
+                                  az_ch=U + 2)
+    net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
+                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
+    train_s = time.perf_counter() - t0
+    del G
+    for _ in range(args.warmup):  # warm both graphs on the first position
+        G = build_grid(cmg, spec0)
+        for use in (None, net):
+            S.set_learned(use)
+            G.copy(BSAVE, 1)
+            S.solve(G, *solve_args())
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    plain_ms, learned_ms, plain_it, learned_it, fallbacks, true_rel, setup_s, launches = [], [], [], [], 0, [], 0.0, 0
+    for k in range(args.steps):
+        t1 = time.perf_counter()
+        G = build_grid(cmg, moving_sphere_spec(k))
+        setup_s += time.perf_counter() - t1
+        S.set_learned(None)
+        G.copy(BSAVE, 1)
+        it, _ = S.solve(G, *solve_args())
+        plain_ms.append(S.last_solve_ms())
+        plain_it.append(it)
+        launches += S.last_solve_launches()
+        S.set_learned(net)
+        G.copy(BSAVE, 1)
+        it, _ = S.solve(G, *solve_args())
+        learned_ms.append(S.last_solve_ms())
+        launches += S.last_solve_launches()
+        tr, fb, lit = S.learned_status()
+        learned_it.append(lit)
+        fallbacks += int(fb)
+        true_rel.append(tr)
+        S.set_learned(None)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    mp, ml = float(np.mean(plain_ms)), float(np.mean(learned_ms))
+    return {
+        "metric": METRIC, "value": round(mp, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(mp, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOADS["moving_sphere"], "method": "plain FP32 FAS mu-cycle (mu=2) MG-PCG, FP64 dots",
+            "timing": "device time of each solve's graph (CUDA events inside the library); octree rebuild per step not timed",
+            "l2": "inputs larger than L2: ~550 MB of channel planes per octree",
+            "plain_pcg_iters": [min(plain_it), max(plain_it)], "octree_setup_s_per_step": round(setup_s / max(args.steps, 1), 3),
+            "learned_preconditioner": {
+                "hidden": LEARNED["hidden"], "loss": LEARNED["loss"], "damping": LEARNED["damping"],
+                "trained_on": "position 0, 10 other right-hand sides", "train_and_collect_s": round(train_s, 3),
+                "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+                "ms_mean": round(ml, 4), "learned_pcg_iters": [min(learned_it), max(learned_it)], "fell_back": fallbacks,
+                "rel_residual_true_max": float(max(true_rel)), "plain_ms_mean": round(mp, 4)},
+        },
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
 
 
 def run_ours(args, rank, world, local_rank):
@@ -740,7 +829,8 @@ def main():
 
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    res = (run_batched if args.workload == "batched64" else run_ours)(args, rank, world, local_rank)
+    runner = {"batched64": run_batched, "moving_sphere": run_sequence}.get(args.workload, run_ours)
+    res = runner(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
 

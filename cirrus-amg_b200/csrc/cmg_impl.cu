@@ -2,6 +2,7 @@
 #include "cmg_impl.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -158,7 +159,10 @@ int Grid::ensure_device() {
     dev_types.resize(n_new);
     for (int t = 0; t < n_new; ++t) dev_types[t] = topo.tiles()[t].type;
     dev_version = host_version;
-    ++version;
+    // process-wide unique: a solver's cached graphs are keyed by (grid address, version), and a
+    // grid created after another was destroyed may reuse its address
+    static std::atomic<unsigned long long> next_version{0};
+    version = ++next_version;
     return 0;
 }
 
@@ -708,6 +712,11 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     Plan plan{};
     if (use_graph) {
         auto it = graphs.find(k);
+        if (it == graphs.end() && graphs.size() >= kMaxCachedGraphs) {
+            // graphs of grids that no longer exist never match again: drop the cache when it grows
+            for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+            graphs.clear();
+        }
         if (it == graphs.end()) {
             if (int rc = build_graph(G, k, &plan)) return rc;
             graphs[k] = plan;

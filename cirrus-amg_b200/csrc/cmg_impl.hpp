@@ -111,6 +111,7 @@ struct Solver {
         int k_pre, k_body, k_if;  // kernel nodes before the loop, per iteration, in the per-iteration IF body
     };
     std::map<Key, Plan> graphs;
+    static constexpr size_t kMaxCachedGraphs = 64;
     long long last_launches = 0;
 
     Solver(int c, float rm, float rr, float p) : coeff_ch(c), R_matrix(rm), R_restrict(rr), P(p) {}

@@ -60,3 +60,24 @@ def test_batch_rejects_a_repeated_solver():
     S = inst[0][1]
     with pytest.raises(cmg.CmgError):
         cmg.solve_batch([S, S], [G for G, _ in inst], 100, 1e-6, 2, 10, 1, False)
+
+
+def test_solver_reused_across_destroyed_and_recreated_grids():
+    """One solver, grids destroyed and created in turn (a new grid may take a destroyed one's
+    address): every solve equals a solve by a fresh solver on the same grid."""
+    import gc
+
+    from workloads import COEFF
+
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    for c in [(0.5, 0.5, 0.5), (0.55, 0.5, 0.5), (0.5, 0.5, 0.5)]:
+        G, _, _ = setup_shell(shell_params(3, 4, 5, c, 0.1), spheres=[c + (0.1,)], with_oracle=False)
+        b = G.download(1)
+        it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+        x = G.download(0)
+        G.upload(1, b)
+        fresh = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+        it2, rel2 = fresh.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+        assert it == it2 and rel == rel2 and np.array_equal(x, G.download(0))
+        del G, fresh
+        gc.collect()
