@@ -367,6 +367,7 @@ def training_rhs(cmg, G, spec, n):
     return out
 
 
+LEARNED_INFERENCE = ["mma.sync"]  # set from --learned-inference
 LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, loss="energy", iters=(1, 2, 3, 5), rhs=10, max_tiles=1250)
 
 
@@ -411,7 +412,7 @@ def learned_block(cmg, torch, spec, steps, world, dev):
     S.set_learned(None)
     _, _, ty = G.tiles()
     lm = ty == cmg.LEAF
-    return {"hidden": LEARNED["hidden"], "loss": LEARNED["loss"],
+    return {"hidden": LEARNED["hidden"], "loss": LEARNED["loss"], "inference_kernel": LEARNED_INFERENCE[0],
             "damping": LEARNED["damping"], "train_pairs": int(pairs["rho"].shape[0]), "collect_s": round(t1 - t0, 3),
             "train_s": round(t2 - t1, 3), "epochs": LEARNED["epochs"], "loss_first_epoch": float(losses[0]),
             "loss_last_epoch": float(losses[-1]), "plain_ms": round(plain_ms, 4), "plain_pcg_iters": plain_it,
@@ -487,7 +488,7 @@ def run_sequence(args, rank, world, local_rank):
             "plain_pcg_iters": [min(plain_it), max(plain_it)], "octree_setup_s_per_step": round(setup_s / max(args.steps, 1), 3),
             "learned_preconditioner": {
                 "hidden": LEARNED["hidden"], "loss": LEARNED["loss"], "damping": LEARNED["damping"],
-                "trained_on": "position 0, 10 other right-hand sides", "train_and_collect_s": round(train_s, 3),
+                "inference_kernel": LEARNED_INFERENCE[0], "trained_on": "position 0, 10 other right-hand sides", "train_and_collect_s": round(train_s, 3),
                 "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
                 "ms_mean": round(ml, 4), "learned_pcg_iters": [min(learned_it), max(learned_it)], "fell_back": fallbacks,
                 "rel_residual_true_max": float(max(true_rel)), "plain_ms_mean": round(mp, 4)},
@@ -807,6 +808,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-smoother comparison")
+    ap.add_argument("--learned-inference", default="mma.sync", choices=["mma.sync", "tcgen05"],
+                    help="inference kernel of the learned smoother")
     ap.add_argument("--workload", default="sphere", choices=sorted(WORKLOADS))
     ap.add_argument("--streams", type=int, default=BATCH_STREAMS, help="streams of the batched workload")
     args = ap.parse_args()
@@ -815,6 +818,12 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl != "reference":
+        import cmg
+
+        LEARNED_INFERENCE[0] = args.learned_inference
+        cmg.set_learned_inference(args.learned_inference)
 
     if args.impl == "reference":
         if rank == 0:
