@@ -274,9 +274,12 @@ def solve_args():
     return (False, SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
 
 
-def cpu_baseline_fp64(G, cmg, spec, what="the workload"):
+def cpu_baseline_fp64(G, cmg, spec, what="the workload", solutions=None):
     """FP64 Jacobi-preconditioned CG (the algorithm of Eigen's default
-    ConjugateGradient) on the same operator assembled into CSR, all host cores."""
+    ConjugateGradient) on the same operator assembled into CSR, all host cores.
+    With `solutions` ({name: [tiles, 512] array}), the FP64 solution is refined after the
+    timed solve (one residual-correction solve, to ~1e-10) and each solution's relative L2
+    error against it over the unknowns is reported."""
     from oracle import oracle as O
 
     case = {"shell": O.CASE_SHELL, "uniform": O.CASE_UNIFORM, "multi": O.CASE_MULTI_SPHERE}[spec["case"]]
@@ -298,9 +301,19 @@ def cpu_baseline_fp64(G, cmg, spec, what="the workload"):
     t0 = time.perf_counter()
     x, its, rel = O.csr_solve(rp, ci, va, bb, 1e-6, 4000, 0)
     dt = time.perf_counter() - t0
-    return {"value": dt * 1e3, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"one full FP64 Jacobi-CG solve of {what} to 1e-6 ({len(bb)} unknowns, {its} iterations, "
-                      f"rel {rel:.2e}); OpenMP over all host threads"}
+    out = {"value": dt * 1e3, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+           "sample": f"one full FP64 Jacobi-CG solve of {what} to 1e-6 ({len(bb)} unknowns, {its} iterations, "
+                     f"rel {rel:.2e}); OpenMP over all host threads"}
+    if solutions:
+        r = bb - O.csr_matvec(rp, ci, va, x)
+        dx, its2, rel2 = O.csr_solve(rp, ci, va, r, 1e-4, 4000, 0)
+        xr = x + dx
+        res = np.linalg.norm(bb - O.csr_matvec(rp, ci, va, xr)) / np.linalg.norm(bb)
+        nx = np.linalg.norm(xr)
+        out["error_vs_fp64"] = {name: float(np.linalg.norm(sol[rt, rc].astype(np.float64) - xr) / nx)
+                                for name, sol in solutions.items()}
+        out["error_vs_fp64"]["fp64_reference_rel_residual"] = float(res)
+    return out
 
 
 def roofline_gs(G, S, cmg, torch, dev):
@@ -550,7 +563,7 @@ def run_ours(args, rank, world, local_rank):
     # the mixed-precision preconditioner (16-bit operator storage in the smoothing sweeps),
     # timed the same way on the same solve, against the FP32 solution above
     x32 = G.download(0)
-    mixed = {}
+    mixed, mixed_x = {}, {"fp32": x32}
     for mode in ("bf16", "fp16"):
         S.set_storage(mode)
         for _ in range(3):
@@ -563,6 +576,7 @@ def run_ours(args, rank, world, local_rank):
         m1.record()
         torch.cuda.synchronize()
         xm = G.download(0)
+        mixed_x[mode] = xm
         lm = ty == cmg.LEAF
         mixed[mode] = {"ms": round(replica_time(m0.elapsed_time(m1), world, dev) / args.steps, 4), "pcg_iters": it_m,
                        "rel_residual_recurrence": rel_m,
@@ -641,7 +655,11 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline_fp64(G, cmg, spec)
+            cb = cpu_baseline_fp64(G, cmg, spec, solutions=mixed_x)
+            err = cb.pop("error_vs_fp64", None)
+            result["cpu_baseline"] = cb
+            if err:
+                result["config"]["solution_error_vs_fp64"] = err
     return result
 
 
