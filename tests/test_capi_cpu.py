@@ -93,3 +93,33 @@ def test_bad_arguments_return_status_codes():
     prm = np.array([3.0, 3.0])
     assert L.cmg_grid_refine_case(G.h, 99, prm.ctypes.data_as(ctypes.c_void_p), 2, None) == 1
     assert b"not built" in L.cmg_last_error() or b"bad argument" in L.cmg_last_error()
+
+
+def test_learned_entry_points_reject_bad_arguments():
+    """The learned smoother's entry points validate their arguments before touching the GPU."""
+    L = cmg.lib()
+    out = ctypes.c_void_p()
+    assert L.cmg_learned_create(12, 0, ctypes.byref(out)) == 1  # hidden must be 8 or 16
+    assert L.cmg_learned_create(8, 0, None) == 1
+    assert L.cmg_learned_set_inference(2) == 1
+    assert L.cmg_learned_set_loss(None, 0) == 1
+    n = ctypes.c_int(0)
+    assert L.cmg_learned_num_params(None, ctypes.byref(n)) == 1
+    assert L.cmg_learned_forward(None, 0, 1, None) == 1
+    assert L.cmg_learned_gradient(None, 0, 1, None, None) == 1
+    assert L.cmg_learned_train(None, 1, 1, ctypes.c_float(1e-3), 0, None) == 1
+    assert L.cmg_amg_solver_set_learned(None, None) == 1
+    assert L.cmg_amg_solver_learned_status(None, None, None, None) == 1
+    assert L.cmg_learned_destroy(None) == 0
+    assert L.cmg_learned_create(12, 0, ctypes.byref(out)) == 1
+    assert b"hidden" in L.cmg_last_error()
+
+
+def test_learned_oracle_parameter_layout_matches_header():
+    """The parameter layout of the FP64 restatement: W1[H][27][8], b1[H], W2[H][27][H], b2[H], W3[27][H]."""
+    from oracle import learned_oracle as LO
+
+    for H in (8, 16):
+        L = LO.layout(H)
+        assert L["B1"] == H * 216 and L["W2"] == L["B1"] + H
+        assert L["B2"] == L["W2"] + 27 * H * H and L["W3"] == L["B2"] + H and L["n"] == L["W3"] + 27 * H
