@@ -51,7 +51,8 @@ EXPORTS = [
     "cmg_grid_gather_device_tiles", "cmg_grid_scatter_device_tiles",
     "cmg_learned_create", "cmg_learned_destroy", "cmg_learned_num_params", "cmg_learned_get_params",
     "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
-    "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned", "cmg_amg_solver_learned_status",
+    "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned",
+    "cmg_amg_solver_autotune", "cmg_amg_solver_learned_status",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -142,6 +143,7 @@ def lib():
             "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
             "cmg_learned_set_loss": (I, [P, I]),
             "cmg_learned_set_inference": (I, [I]),
+            "cmg_amg_solver_autotune": (I, [P, P, I, P, P, P, P, I, D, I, P, P, P]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
         }
@@ -426,6 +428,31 @@ class AMGSolver:
                "learned_status")
         return tr.value, bool(fb.value), it.value
 
+    def autotune(self, grid, candidates=None, max_iters=100, relative_tolerance=1e-6, repeats=2):
+        """Time solves of the grid's current rhs (channel 1) under each candidate
+        (omega, mu, level_iters, coarsest_iters) and keep the fastest that converges.  Sets
+        self.omega and self.mu_cycle_repeat_times; returns (best candidate or None, table of
+        (candidate, ms or None, iters))."""
+        if candidates is None:
+            candidates = default_tune_candidates()
+        n = len(candidates)
+        om = np.array([c[0] for c in candidates], np.float64)
+        mu = np.array([c[1] for c in candidates], np.int32)
+        li = np.array([c[2] for c in candidates], np.int32)
+        ci = np.array([c[3] for c in candidates], np.int32)
+        ms = np.zeros(n, np.float32)
+        its = np.zeros(n, np.int32)
+        best = ctypes.c_int(-1)
+        self._sync_params()
+        _check(self.L.cmg_amg_solver_autotune(self.h, grid.h, n, _p(om), _p(mu), _p(li), _p(ci), max_iters, relative_tolerance,
+                                               repeats, _p(ms), _p(its), ctypes.byref(best)), "autotune")
+        table = [(tuple(candidates[i]), float(ms[i]) if ms[i] >= 0 else None, int(its[i])) for i in range(n)]
+        if best.value < 0:
+            return None, table
+        b = tuple(candidates[best.value])
+        self.omega, self.mu_cycle_repeat_times = float(b[0]), int(b[1])
+        return b, table
+
     def _sync_params(self):
         _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")
 
@@ -480,6 +507,11 @@ class AMGSolver:
         n = ctypes.c_longlong(0)
         _check(self.L.cmg_amg_last_solve_launches(self.h, ctypes.byref(n)), "last_solve_launches")
         return n.value
+
+
+def default_tune_candidates():
+    """The autotuner's default search: omega x mu x level_iters x coarsest_iters."""
+    return [(om, mu, li, ci) for om in (0.8, 0.9, 1.0, 1.1, 1.2, 1.5) for mu in (1, 2) for li in (1, 2, 3) for ci in (2, 5, 10)]
 
 
 def set_learned_inference(kind):

@@ -858,4 +858,54 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     return rc;
 }
 
+int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, const int* li_c, const int* ci_c, int max_iters, double tol,
+                     int repeats, float* ms, int* iters, int* best) {
+    *best = -1;
+    if (int rc = ensure_aux(G)) return rc;  // bsave keeps the rhs between the timed solves
+    const size_t bytes = sizeof(float) * (size_t)G.n * kCells;
+    CK(cudaMemcpyAsync(bsave, G.plane(1), bytes, cudaMemcpyDeviceToDevice, G.stream));
+    const double omega0 = omega;
+    const int mu0 = mu;
+    float best_ms = 0.0f;
+    for (int i = 0; i < n; ++i) {
+        omega = omega_c[i];
+        mu = mu_c[i];
+        float tmin = -1.0f;
+        bool ok = true;
+        int it = 0;
+        for (int r = 0; r <= repeats; ++r) {  // the first solve builds the graph and is not counted
+            CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
+            if (int rc = solve_begin(G, max_iters, tol, li_c[i], ci_c[i], 1, false)) {
+                omega = omega0, mu = mu0;
+                return rc;
+            }
+            double rel = 0.0;
+            const int rc = solve_finish(false, &it, &rel);
+            if (rc == 5) ok = false;  // non-finite: this setting diverges
+            else if (rc) {
+                omega = omega0, mu = mu0;
+                return rc;
+            }
+            if (!(h_s->converged || h_s->rr0 == 0.0)) ok = false;
+            if (r > 0 && (tmin < 0.0f || last_ms < tmin)) tmin = last_ms;
+        }
+        ms[i] = ok ? tmin : -1.0f;
+        iters[i] = it;
+        if (ok && (*best < 0 || tmin < best_ms)) {
+            *best = i;
+            best_ms = tmin;
+        }
+    }
+    CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
+    CK(cudaStreamSynchronize(G.stream));
+    if (*best >= 0) {
+        omega = omega_c[*best];
+        mu = mu_c[*best];
+    } else {
+        omega = omega0;
+        mu = mu0;
+    }
+    return 0;
+}
+
 }  // namespace cmg

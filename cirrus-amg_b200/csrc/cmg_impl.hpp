@@ -183,6 +183,11 @@ struct Solver {
     int build_graph(Grid& G, const Key& k, Plan* out);
     int solve(Grid& G, bool verbose, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride,
               bool pure_neumann, int* iters, double* rel);
+    // Autotuner: times solves of the grid's current rhs (channel 1) under each candidate
+    // (omega, mu, level_iters, coarsest_iters), keeps the fastest that converges and sets its
+    // omega and mu on the solver.  ms[i] = best of `repeats` timed solves (-1: not converged).
+    int autotune(Grid& G, int n, const double* omega, const int* mu, const int* level_iters, const int* coarsest_iters, int max_iters,
+                 double tol, int repeats, float* ms, int* iters, int* best);
     // solve() in two halves, for batches of independent solves: solve_begin enqueues the whole
     // solve and the read-back of its scalars on the grid's stream and returns; solve_finish
     // waits for that stream and computes (iters, rel) as solve() does

@@ -181,6 +181,15 @@ int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float 
 int cmg_amg_solver_destroy(cmg_amg_solver* s);
 /* public fields omega / mu_cycle_repeat_times (src/AMGSolver.h:306-307) */
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
+/* Autotuner (no counterpart in the reference): solves the grid's current rhs (channel 1)
+ * under each of n candidate smoother settings (omega[i], mu[i], level_iters[i],
+ * coarsest_iters[i]) to tol, `repeats` timed solves each after one untimed solve, and keeps
+ * the fastest setting that converges: ms[i] (-1: did not converge), iters[i], *best (-1:
+ * none).  The solver's omega and mu become the best candidate's; pass its level_iters and
+ * coarsest_iters to cmg_amg_solve.  Channel 1 is restored, channel 0 holds the last solution.
+ * Tune on a right-hand side other than the ones to be timed. */
+int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const double* omega, const int* mu, const int* level_iters,
+                            const int* coarsest_iters, int max_iters, double tol, int repeats, float* ms, int* iters, int* best);
 /* Launch flags (default CMG_LAUNCH_GRAPH).
  * GRAPH: the solve runs as one CUDA graph with a device-side while loop;
  * without it the same kernels are launched one by one with the loop test on

@@ -1,0 +1,47 @@
+"""The smoother-parameter autotuner (cmg_amg_solver_autotune): it keeps the fastest setting
+that converges, restores the right-hand side, and the tuned solve agrees with the plain one."""
+import numpy as np
+import pytest
+
+import cmg
+from workloads import setup_uniform, uniform_rhs
+
+pytestmark = pytest.mark.gpu
+
+
+def test_autotune_keeps_fastest_converging_setting():
+    G, _, solver, b0 = setup_uniform(3, seed=0, with_oracle=False)
+    _, _, ty = G.tiles()
+    b_train = uniform_rhs(ty == cmg.LEAF, 100)
+    G.upload(1, b_train)
+    cands = [(1.5, 2, 2, 10), (1.0, 2, 2, 5), (1.0, 1, 1, 2), (1.2, 2, 1, 5)]
+    best, table = solver.autotune(G, cands, max_iters=7, relative_tolerance=1e-6, repeats=2)
+    assert best is not None
+    conv = [t for t in table if t[1] is not None]
+    assert best == min(conv, key=lambda t: t[1])[0]
+    for cand, ms, it in table:
+        if ms is None:
+            assert it == 7  # ran out of iterations
+    assert (solver.omega, solver.mu_cycle_repeat_times) == best[:2]
+    assert np.array_equal(G.download(1), b_train)
+
+    # the tuned setting on the timed rhs, against the plain (reference) setting
+    G.upload(1, b0)
+    it_t, rel_t = solver.solve(G, False, 100, 1e-6, best[2], best[3], 1, False)
+    x_t = G.download(0)
+    plain = cmg.AMGSolver(6, 0.5, 1.0, 1.0)
+    G.upload(1, b0)
+    it_p, rel_p = plain.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x_p = G.download(0)
+    assert rel_t < 1e-6 and rel_p < 1e-6
+    assert it_t <= it_p
+    assert np.linalg.norm(x_t - x_p) <= 1e-5 * np.linalg.norm(x_p)
+
+
+def test_autotune_reports_no_setting_when_none_converges():
+    G, _, solver, b0 = setup_uniform(2, seed=1, with_oracle=False)
+    om0 = solver.omega
+    best, table = solver.autotune(G, [(1.5, 2, 2, 10)], max_iters=1, relative_tolerance=1e-12, repeats=1)
+    assert best is None and table[0][1] is None
+    assert solver.omega == om0
+    assert np.array_equal(G.download(1), b0)
