@@ -457,6 +457,11 @@ def run_sequence(args, rank, world, local_rank):
     net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
                                 lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
     train_s = time.perf_counter() - t0
+    # the autotuned smoother, tuned once at position 0 on a training rhs
+    St = make_solver(cmg)
+    G.upload(1, rhs[0])
+    best, _ = St.autotune(G, max_iters=SOLVE["max_iters"], relative_tolerance=SOLVE["tol"], repeats=1)
+    targs = (False, SOLVE["max_iters"], SOLVE["tol"], best[2], best[3], SOLVE["sync_stride"], False) if best else None
     del G
     for _ in range(args.warmup):  # warm both graphs on the first position
         G = build_grid(cmg, spec0)
@@ -467,6 +472,7 @@ def run_sequence(args, rank, world, local_rank):
     sampler = ClockSampler(local_rank)
     sampler.start()
     plain_ms, learned_ms, plain_it, learned_it, fallbacks, true_rel, setup_s, launches = [], [], [], [], 0, [], 0.0, 0
+    tuned_ms, tuned_it = [], []
     for k in range(args.steps):
         t1 = time.perf_counter()
         G = build_grid(cmg, moving_sphere_spec(k))
@@ -487,6 +493,11 @@ def run_sequence(args, rank, world, local_rank):
         fallbacks += int(fb)
         true_rel.append(tr)
         S.set_learned(None)
+        if targs:
+            G.copy(BSAVE, 1)
+            it, _ = St.solve(G, *targs)
+            tuned_ms.append(St.last_solve_ms())
+            tuned_it.append(it)
     torch.cuda.synchronize()
     clocks = sampler.stop()
     mp, ml = float(np.mean(plain_ms)), float(np.mean(learned_ms))
@@ -505,6 +516,10 @@ def run_sequence(args, rank, world, local_rank):
                 "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
                 "ms_mean": round(ml, 4), "learned_pcg_iters": [min(learned_it), max(learned_it)], "fell_back": fallbacks,
                 "rel_residual_true_max": float(max(true_rel)), "plain_ms_mean": round(mp, 4)},
+            "autotuned_smoother": None if not targs else {
+                "tuned_on": "position 0, one training rhs", "omega": best[0], "mu": best[1], "level_iters": best[2],
+                "coarsest_iters": best[3], "ms_mean": round(float(np.mean(tuned_ms)), 4),
+                "pcg_iters": [min(tuned_it), max(tuned_it)], "speedup_vs_plain": round(mp / float(np.mean(tuned_ms)), 3)},
         },
         "gpu_launches": int(launches),
         "clocks": clocks,
@@ -728,11 +743,11 @@ def run_batched(args, rank, world, local_rank):
         G.set_stream(streams[i % nstreams].cuda_stream)
     sargs = (SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
 
-    def one_batch(b_host=None, x_host=None):
+    def one_batch(b_host=None, x_host=None, solve_args=None):
         if b_host is None:
             for G in grids:
                 G.copy(BSAVE, 1)
-        return cmg.solve_batch(solvers, grids, *sargs, b_host=b_host, x_host=x_host)
+        return cmg.solve_batch(solvers, grids, *(solve_args or sargs), b_host=b_host, x_host=x_host)
 
     def timed(steps, **kw):
         torch.cuda.synchronize()
@@ -782,6 +797,32 @@ def run_batched(args, rank, world, local_rank):
     big = max(range(n), key=lambda i: infos[i][0])
     grids[big].set_stream(0)
     roof = roofline_gs(grids[big], solvers[big], cmg, torch, dev)
+    grids[big].set_stream(streams[big % nstreams].cuda_stream)
+
+    # the autotuned smoother: tuned once on octree 0 with a training rhs, applied to all 64
+    tuned = None
+    if not args.no_learned:
+        G0 = grids[0]
+        G0.upload(1, training_rhs(cmg, G0, specs[0], 1)[0])
+        t0 = time.perf_counter()
+        best, table = solvers[0].autotune(G0, max_iters=SOLVE["max_iters"], relative_tolerance=SOLVE["tol"], repeats=2)
+        tune_s = time.perf_counter() - t0
+        if best is not None:
+            for S in solvers:
+                S.omega, S.mu_cycle_repeat_times = best[0], best[1]
+            targs = (SOLVE["max_iters"], SOLVE["tol"], best[2], best[3], SOLVE["sync_stride"], False)
+            one_batch(solve_args=targs)
+            t_t, out_t = timed(args.steps, solve_args=targs)
+            per_t = sorted(m for _, _, ms in out_t for m in ms)
+            its_t = [i for it, _, _ in out_t for i in it]
+            tuned = {"tuned_on": "octree 0, one training rhs (Fourier seed 200)", "tune_s": round(tune_s, 3),
+                     "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3],
+                     "solves_per_s": round(n * args.steps * world / (replica_time(t_t, world, dev) / 1e3), 2),
+                     "pcg_iters_mean": round(float(np.mean(its_t)), 2), "pcg_iters_max": int(max(its_t)),
+                     "rel_residual_max": max(r for _, rel, _ in out_t for r in rel),
+                     "solve_ms_p50": per_t[len(per_t) // 2], "solve_ms_p99": per_t[min(len(per_t) - 1, int(0.99 * len(per_t)))]}
+            for S in solvers:
+                S.omega, S.mu_cycle_repeat_times = SOLVE["omega"], SOLVE["mu"]
 
     result = None
     if rank == 0:
@@ -798,6 +839,7 @@ def run_batched(args, rank, world, local_rank):
                 "solve_ms_p50": per[len(per) // 2], "solve_ms_p99": per[min(len(per) - 1, int(0.99 * len(per)))],
                 "l2": f"inputs larger than L2: {16 * sum(i[0] for i in infos) * 2048 / 1e9:.1f} GB of channel planes",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "autotuned_smoother": tuned,
             },
             "e2e": {"value": round(n * args.steps * world / (e2e_ms / 1e3), 2), "unit": BATCH_UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
