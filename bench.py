@@ -658,7 +658,9 @@ def run_ours(args, rank, world, local_rank):
                 a.record()
                 for _ in range(args.steps):
                     G.copy(BSAVE, 1)
+                    torch.cuda.nvtx.range_push("tuned_solve")
                     it_t, _ = S2.solve(G, *args_t)
+                    torch.cuda.nvtx.range_pop()
                 b_.record()
                 torch.cuda.synchronize()
                 return replica_time(a.elapsed_time(b_), world, dev) / args.steps, it_t, G.download(0)
