@@ -511,7 +511,7 @@ class AMGSolver:
 
 def default_tune_candidates():
     """The autotuner's default search: omega x mu x level_iters x coarsest_iters."""
-    return [(om, mu, li, ci) for om in (0.8, 0.9, 1.0, 1.1, 1.2, 1.5) for mu in (1, 2) for li in (1, 2, 3) for ci in (2, 5, 10)]
+    return [(om, mu, li, ci) for om in (0.8, 0.9, 1.0, 1.1, 1.2, 1.3, 1.5) for mu in (1, 2) for li in (1, 2, 3) for ci in (2, 5, 10)]
 
 
 def set_learned_inference(kind):
