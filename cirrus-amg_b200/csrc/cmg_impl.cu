@@ -888,6 +888,11 @@ int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, con
             }
             if (!(h_s->converged || h_s->rr0 == 0.0)) ok = false;
             if (r > 0 && (tmin < 0.0f || last_ms < tmin)) tmin = last_ms;
+            // a candidate whose first solve is already far slower than the best is not timed further
+            if (r == 0 && (!ok || (*best >= 0 && last_ms > 1.5f * best_ms))) {
+                if (ok) tmin = last_ms;
+                break;
+            }
         }
         ms[i] = ok ? tmin : -1.0f;
         iters[i] = it;

@@ -183,7 +183,9 @@ int cmg_amg_solver_destroy(cmg_amg_solver* s);
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
 /* Autotuner (no counterpart in the reference): solves the grid's current rhs (channel 1)
  * under each of n candidate smoother settings (omega[i], mu[i], level_iters[i],
- * coarsest_iters[i]) to tol, `repeats` timed solves each after one untimed solve, and keeps
+ * coarsest_iters[i]) to tol, `repeats` timed solves each after one untimed solve (a candidate
+ * whose first solve is slower than 1.5x the best so far, or does not converge, is not timed
+ * further; its ms[i] is that first solve's), and keeps
  * the fastest setting that converges: ms[i] (-1: did not converge), iters[i], *best (-1:
  * none).  The solver's omega and mu become the best candidate's; pass its level_iters and
  * coarsest_iters to cmg_amg_solve.  Channel 1 is restored, channel 0 holds the last solution.
