@@ -123,3 +123,21 @@ def test_learned_oracle_parameter_layout_matches_header():
         L = LO.layout(H)
         assert L["B1"] == H * 216 and L["W2"] == L["B1"] + H
         assert L["B2"] == L["W2"] + 27 * H * H and L["W3"] == L["B2"] + H and L["n"] == L["W3"] + 27 * H
+
+
+def test_autotune_rejects_bad_arguments():
+    """cmg_amg_solver_autotune checks its arguments before touching the GPU (a solver needs a
+    GPU to exist, so only the null-object and empty-candidate cases run here)."""
+    L = cmg.lib()
+    om = np.array([1.0], np.float64)
+    mu = np.array([1], np.int32)
+    li = np.array([2], np.int32)
+    ci = np.array([5], np.int32)
+    ms = np.zeros(1, np.float32)
+    its = np.zeros(1, np.int32)
+    best = ctypes.c_int(7)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    for n, tol in [(1, 1e-6), (0, 1e-6), (1, 0.0)]:
+        assert L.cmg_amg_solver_autotune(None, None, n, P(om), P(mu), P(li), P(ci), 10, ctypes.c_double(tol), 1, P(ms), P(its),
+                                         ctypes.byref(best)) == 1
+    assert b"autotune" in L.cmg_last_error()
