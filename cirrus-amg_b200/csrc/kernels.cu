@@ -25,9 +25,19 @@ __device__ __forceinline__ bool last_block(unsigned int* counter) {
     __syncthreads();
     return is_last;
 }
+// Thread t sums partials t, t+128, t+256, ... in that order; the loads are issued eight at a
+// time before the adds, which keeps the order (and the result) and overlaps the L2 latency.
 __device__ __forceinline__ double sum_partials(const double* part, int n, double* red) {
     double s = 0;
-    for (int i = threadIdx.x; i < n; i += 128) s += __ldcg(part + i);
+    int i = threadIdx.x;
+    for (; i + 7 * 128 < n; i += 8 * 128) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldcg(part + i + u * 128);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += v[u];
+    }
+    for (; i < n; i += 128) s += __ldcg(part + i);
     return block_sum128(s, red);
 }
 // products of four cells summed in float, the reference's Dot128Kernel (src/PoissonGrid.cu:168-172)
