@@ -518,7 +518,7 @@ def run_sequence(args, rank, world, local_rank):
                 "rel_residual_true_max": float(max(true_rel)), "plain_ms_mean": round(mp, 4)},
             "autotuned_smoother": None if not targs else {
                 "tuned_on": "position 0, one training rhs", "omega": best[0], "mu": best[1], "level_iters": best[2],
-                "coarsest_iters": best[3], "ms_mean": round(float(np.mean(tuned_ms)), 4),
+                "coarsest_iters": best[3], "finest_iters": best[4], "ms_mean": round(float(np.mean(tuned_ms)), 4),
                 "pcg_iters": [min(tuned_it), max(tuned_it)], "speedup_vs_plain": round(mp / float(np.mean(tuned_ms)), 3)},
         },
         "gpu_launches": int(launches),
@@ -670,7 +670,7 @@ def run_ours(args, rank, world, local_rank):
             S2.set_storage("fp32")
             tuned = {"tuned_on": "one training rhs of the same octree (seed 100 / Fourier seed 200), never the timed one",
                      "tune_s": round(tune_s, 3), "candidates": len(table),
-                     "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3],
+                     "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3], "finest_iters": best[4],
                      "ms": round(ms_t, 4), "pcg_iters": it_t, "ms_bf16_storage": round(ms_tb, 4), "pcg_iters_bf16_storage": it_tb,
                      "plain_setting": {"omega": SOLVE["omega"], "mu": SOLVE["mu"], "level_iters": SOLVE["level_iters"],
                                        "coarsest_iters": SOLVE["coarsest_iters"]}}
@@ -811,20 +811,20 @@ def run_batched(args, rank, world, local_rank):
         tune_s = time.perf_counter() - t0
         if best is not None:
             for S in solvers:
-                S.omega, S.mu_cycle_repeat_times = best[0], best[1]
+                S.omega, S.mu_cycle_repeat_times, S.finest_iters = best[0], best[1], best[4]
             targs = (SOLVE["max_iters"], SOLVE["tol"], best[2], best[3], SOLVE["sync_stride"], False)
             one_batch(solve_args=targs)
             t_t, out_t = timed(args.steps, solve_args=targs)
             per_t = sorted(m for _, _, ms in out_t for m in ms)
             its_t = [i for it, _, _ in out_t for i in it]
             tuned = {"tuned_on": "octree 0, one training rhs (Fourier seed 200)", "tune_s": round(tune_s, 3),
-                     "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3],
+                     "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3], "finest_iters": best[4],
                      "solves_per_s": round(n * args.steps * world / (replica_time(t_t, world, dev) / 1e3), 2),
                      "pcg_iters_mean": round(float(np.mean(its_t)), 2), "pcg_iters_max": int(max(its_t)),
                      "rel_residual_max": max(r for _, rel, _ in out_t for r in rel),
                      "solve_ms_p50": per_t[len(per_t) // 2], "solve_ms_p99": per_t[min(len(per_t) - 1, int(0.99 * len(per_t)))]}
             for S in solvers:
-                S.omega, S.mu_cycle_repeat_times = SOLVE["omega"], SOLVE["mu"]
+                S.omega, S.mu_cycle_repeat_times, S.finest_iters = SOLVE["omega"], SOLVE["mu"], -1
 
     result = None
     if rank == 0:

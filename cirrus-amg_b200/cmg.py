@@ -52,7 +52,7 @@ EXPORTS = [
     "cmg_learned_create", "cmg_learned_destroy", "cmg_learned_num_params", "cmg_learned_get_params",
     "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
     "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned",
-    "cmg_amg_solver_autotune", "cmg_amg_solver_learned_status",
+    "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -143,7 +143,8 @@ def lib():
             "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
             "cmg_learned_set_loss": (I, [P, I]),
             "cmg_learned_set_inference": (I, [I]),
-            "cmg_amg_solver_autotune": (I, [P, P, I, P, P, P, P, I, D, I, P, P, P]),
+            "cmg_amg_solver_autotune": (I, [P, P, I, P, P, P, P, P, I, D, I, P, P, P]),
+            "cmg_amg_solver_set_finest_iters": (I, [P, I]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
         }
@@ -394,6 +395,7 @@ class AMGSolver:
         self.R_matrix_coeff = R_matrix_coeff
         self.omega = 1.5
         self.mu_cycle_repeat_times = 2
+        self.finest_iters = -1  # sweeps on the finest level; -1: level_iters (the reference)
 
     def __del__(self):
         try:
@@ -430,12 +432,14 @@ class AMGSolver:
 
     def autotune(self, grid, candidates=None, max_iters=100, relative_tolerance=1e-6, repeats=2):
         """Time solves of the grid's current rhs (channel 1) under each candidate
-        (omega, mu, level_iters, coarsest_iters) and keep the fastest that converges.  Sets
-        self.omega and self.mu_cycle_repeat_times; returns (best candidate or None, table of
-        (candidate, ms or None, iters))."""
+        (omega, mu, level_iters, coarsest_iters[, finest_iters]) and keep the fastest that
+        converges.  Sets self.omega, self.mu_cycle_repeat_times and self.finest_iters; returns
+        (best candidate as a 5-tuple or None, table of (candidate, ms or None, iters))."""
         if candidates is None:
             candidates = default_tune_candidates()
+        candidates = [tuple(c) + (-1,) * (5 - len(c)) for c in candidates]
         n = len(candidates)
+        fi = np.array([c[4] for c in candidates], np.int32)
         om = np.array([c[0] for c in candidates], np.float64)
         mu = np.array([c[1] for c in candidates], np.int32)
         li = np.array([c[2] for c in candidates], np.int32)
@@ -444,17 +448,19 @@ class AMGSolver:
         its = np.zeros(n, np.int32)
         best = ctypes.c_int(-1)
         self._sync_params()
-        _check(self.L.cmg_amg_solver_autotune(self.h, grid.h, n, _p(om), _p(mu), _p(li), _p(ci), max_iters, relative_tolerance,
-                                               repeats, _p(ms), _p(its), ctypes.byref(best)), "autotune")
+        _check(self.L.cmg_amg_solver_autotune(self.h, grid.h, n, _p(om), _p(mu), _p(li), _p(ci), _p(fi), max_iters,
+                                               relative_tolerance, repeats, _p(ms), _p(its), ctypes.byref(best)), "autotune")
         table = [(tuple(candidates[i]), float(ms[i]) if ms[i] >= 0 else None, int(its[i])) for i in range(n)]
         if best.value < 0:
             return None, table
         b = tuple(candidates[best.value])
-        self.omega, self.mu_cycle_repeat_times = float(b[0]), int(b[1])
+        self.omega, self.mu_cycle_repeat_times, self.finest_iters = float(b[0]), int(b[1]), int(b[4])
         return b, table
 
     def _sync_params(self):
         _check(self.L.cmg_amg_solver_set_smoother(self.h, float(self.omega), int(self.mu_cycle_repeat_times)), "set_smoother")
+        if hasattr(self, "finest_iters"):
+            _check(self.L.cmg_amg_solver_set_finest_iters(self.h, int(self.finest_iters)), "set_finest_iters")
 
     def prepareTypesAndCoeffs(self, grid):
         _check(self.L.cmg_amg_prepare_types_and_coeffs(grid.h, self.coeff_channel, self.R_matrix_coeff), "prepareTypesAndCoeffs")
@@ -510,8 +516,12 @@ class AMGSolver:
 
 
 def default_tune_candidates():
-    """The autotuner's default search: omega x mu x level_iters x coarsest_iters."""
-    return [(om, mu, li, ci) for om in (0.8, 0.9, 1.0, 1.1, 1.2, 1.3, 1.5) for mu in (1, 2) for li in (1, 2, 3) for ci in (2, 5, 10)]
+    """The autotuner's default search: omega x mu x level_iters x coarsest_iters (finest level
+    as the others), and for V-cycles a finest level with fewer sweeps than the others."""
+    grid = [(om, mu, li, ci, -1) for om in (0.8, 0.9, 1.0, 1.1, 1.2, 1.3, 1.5) for mu in (1, 2) for li in (1, 2, 3)
+            for ci in (2, 5, 10)]
+    grid += [(om, 1, li, ci, fi) for om in (1.0, 1.2, 1.3) for li in (2, 3, 4) for ci in (5, 10) for fi in (1, 2) if fi < li]
+    return grid
 
 
 def set_learned_inference(kind):

@@ -268,6 +268,8 @@ MuArgs Solver::mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters
     A.mu = mu;
     A.level_iters = level_iters;
     A.coarsest_iters = coarsest_iters;
+    A.finest_level = G.max_level();
+    A.finest_iters = finest_iters;
     A.omega = omega;
     A.Rr = R_restrict;
     A.P = P;
@@ -410,7 +412,8 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st, b
                             bar, persist_nblocks, st);
         return;
     }
-    enqueue_gs(G, l, A.level_iters, 0, A.X, A.RHS, st, true);
+    const int li = (l == A.finest_level && A.finest_iters >= 0) ? A.finest_iters : A.level_iters;
+    enqueue_gs(G, l, li, 0, A.X, A.RHS, st, true);
     if (use_pipe && pipe_ok)
         launch_restrict_pipe(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
     else
@@ -420,7 +423,7 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st, b
     if (!fold) launch_fas_save(d, G.nonleaf_begin(l - 1), G.ghost_begin(l - 1) - G.nonleaf_begin(l - 1), A.X, A.RHS, A.X0, A.coeff_ch, st);
     for (int r = 0; r < A.mu; ++r) enqueue_mu_step(G, l - 1, A, st, fold && r == 0);
     launch_prolong(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), A.X, A.X0, A.P, st);
-    enqueue_gs(G, l, A.level_iters, 1, A.X, A.RHS, st, true);
+    enqueue_gs(G, l, li, 1, A.X, A.RHS, st, true);
 }
 
 // GaussSeidelGMG / GaussSeidelCMG (src/GMGSolver.cu:217-223, src/CMGSolver.cu:271-276)
@@ -707,7 +710,7 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     }
     Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu,
           (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0) | (storage << 4) |
-              (learned_active() ? 256 : 0),
+              (learned_active() ? 256 : 0) | ((finest_iters + 1) << 10),
           omega};
     Plan plan{};
     if (use_graph) {
@@ -858,32 +861,33 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     return rc;
 }
 
-int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, const int* li_c, const int* ci_c, int max_iters, double tol,
-                     int repeats, float* ms, int* iters, int* best) {
+int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, const int* li_c, const int* ci_c, const int* fi_c,
+                     int max_iters, double tol, int repeats, float* ms, int* iters, int* best) {
     *best = -1;
     if (int rc = ensure_aux(G)) return rc;  // bsave keeps the rhs between the timed solves
     const size_t bytes = sizeof(float) * (size_t)G.n * kCells;
     CK(cudaMemcpyAsync(bsave, G.plane(1), bytes, cudaMemcpyDeviceToDevice, G.stream));
     const double omega0 = omega;
-    const int mu0 = mu;
+    const int mu0 = mu, fi0 = finest_iters;
     float best_ms = 0.0f;
     for (int i = 0; i < n; ++i) {
         omega = omega_c[i];
         mu = mu_c[i];
+        finest_iters = fi_c ? fi_c[i] : -1;
         float tmin = -1.0f;
         bool ok = true;
         int it = 0;
         for (int r = 0; r <= repeats; ++r) {  // the first solve builds the graph and is not counted
             CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
             if (int rc = solve_begin(G, max_iters, tol, li_c[i], ci_c[i], 1, false)) {
-                omega = omega0, mu = mu0;
+                omega = omega0, mu = mu0, finest_iters = fi0;
                 return rc;
             }
             double rel = 0.0;
             const int rc = solve_finish(false, &it, &rel);
             if (rc == 5) ok = false;  // non-finite: this setting diverges
             else if (rc) {
-                omega = omega0, mu = mu0;
+                omega = omega0, mu = mu0, finest_iters = fi0;
                 return rc;
             }
             if (!(h_s->converged || h_s->rr0 == 0.0)) ok = false;
@@ -906,9 +910,11 @@ int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, con
     if (*best >= 0) {
         omega = omega_c[*best];
         mu = mu_c[*best];
+        finest_iters = fi_c ? fi_c[*best] : -1;
     } else {
         omega = omega0;
         mu = mu0;
+        finest_iters = fi0;
     }
     return 0;
 }

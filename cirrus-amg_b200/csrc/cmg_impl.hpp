@@ -73,6 +73,7 @@ struct MuArgs {
     float* RHS;
     float* X0;
     int coeff_ch, mu, level_iters, coarsest_iters;
+    int finest_level = -1, finest_iters = -1;  // sweeps on the finest level when >= 0 (levels >= 3)
     double omega;
     float Rr, P;
 };
@@ -85,6 +86,7 @@ struct Solver {
     float R_matrix, R_restrict, P;
     double omega = 1.5;
     int mu = 2;
+    int finest_iters = -1;  // sweeps on the finest level (-1: level_iters, as the reference)
 
     double* partial = nullptr;
     double* partial2 = nullptr;
@@ -186,8 +188,8 @@ struct Solver {
     // Autotuner: times solves of the grid's current rhs (channel 1) under each candidate
     // (omega, mu, level_iters, coarsest_iters), keeps the fastest that converges and sets its
     // omega and mu on the solver.  ms[i] = best of `repeats` timed solves (-1: not converged).
-    int autotune(Grid& G, int n, const double* omega, const int* mu, const int* level_iters, const int* coarsest_iters, int max_iters,
-                 double tol, int repeats, float* ms, int* iters, int* best);
+    int autotune(Grid& G, int n, const double* omega, const int* mu, const int* level_iters, const int* coarsest_iters,
+                 const int* finest_iters, int max_iters, double tol, int repeats, float* ms, int* iters, int* best);
     // solve() in two halves, for batches of independent solves: solve_begin enqueues the whole
     // solve and the read-back of its scalars on the grid's stream and returns; solve_finish
     // waits for that stream and computes (iters, rel) as solve() does

@@ -183,7 +183,7 @@ int cmg_amg_solver_destroy(cmg_amg_solver* s);
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
 /* Autotuner (no counterpart in the reference): solves the grid's current rhs (channel 1)
  * under each of n candidate smoother settings (omega[i], mu[i], level_iters[i],
- * coarsest_iters[i]) to tol, `repeats` timed solves each after one untimed solve (a candidate
+ * coarsest_iters[i], finest_iters[i]) to tol, `repeats` timed solves each after one untimed solve (a candidate
  * whose first solve is slower than 1.5x the best so far, or does not converge, is not timed
  * further; its ms[i] is that first solve's), and keeps
  * the fastest setting that converges: ms[i] (-1: did not converge), iters[i], *best (-1:
@@ -191,7 +191,12 @@ int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
  * coarsest_iters to cmg_amg_solve.  Channel 1 is restored, channel 0 holds the last solution.
  * Tune on a right-hand side other than the ones to be timed. */
 int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const double* omega, const int* mu, const int* level_iters,
-                            const int* coarsest_iters, int max_iters, double tol, int repeats, float* ms, int* iters, int* best);
+                            const int* coarsest_iters, const int* finest_iters, int max_iters, double tol, int repeats, float* ms,
+                            int* iters, int* best);
+/* Sweeps per visit on the finest level (levels >= 3), -1 (default): level_iters, as the
+ * reference does on every level.  No counterpart in the reference.  finest_iters of the
+ * autotuner (may be NULL) are candidates for it; the best one is set on the solver. */
+int cmg_amg_solver_set_finest_iters(cmg_amg_solver* s, int finest_iters);
 /* Launch flags (default CMG_LAUNCH_GRAPH).
  * GRAPH: the solve runs as one CUDA graph with a device-side while loop;
  * without it the same kernels are launched one by one with the loop test on

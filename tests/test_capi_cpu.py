@@ -138,6 +138,6 @@ def test_autotune_rejects_bad_arguments():
     best = ctypes.c_int(7)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     for n, tol in [(1, 1e-6), (0, 1e-6), (1, 0.0)]:
-        assert L.cmg_amg_solver_autotune(None, None, n, P(om), P(mu), P(li), P(ci), 10, ctypes.c_double(tol), 1, P(ms), P(its),
-                                         ctypes.byref(best)) == 1
+        assert L.cmg_amg_solver_autotune(None, None, n, P(om), P(mu), P(li), P(ci), None, 10, ctypes.c_double(tol), 1, P(ms),
+                                         P(its), ctypes.byref(best)) == 1
     assert b"autotune" in L.cmg_last_error()

@@ -45,3 +45,19 @@ def test_autotune_reports_no_setting_when_none_converges():
     assert best is None and table[0][1] is None
     assert solver.omega == om0
     assert np.array_equal(G.download(1), b0)
+
+
+def test_finest_iters_override():
+    """finest_iters equal to level_iters is the reference's cycle bit for bit; fewer sweeps on
+    the finest level give another cycle that still converges."""
+    G, _, solver, b = setup_uniform(3, seed=2, with_oracle=False)
+    it0, rel0 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x0 = G.download(0)
+    solver.finest_iters = 2
+    G.upload(1, b)
+    it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    assert it0 == it1 and rel0 == rel1 and np.array_equal(G.download(0), x0)
+    solver.finest_iters = 1
+    G.upload(1, b)
+    it2, rel2 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    assert rel2 < 1e-6 and not np.array_equal(G.download(0), x0)
