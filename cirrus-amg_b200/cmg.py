@@ -143,7 +143,7 @@ def lib():
             "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
             "cmg_learned_set_loss": (I, [P, I]),
             "cmg_learned_set_inference": (I, [I]),
-            "cmg_amg_solver_autotune": (I, [P, P, I, P, P, P, P, P, I, D, I, P, P, P]),
+            "cmg_amg_solver_autotune": (I, [P, P, I, P, I, D, I, P, P, P]),
             "cmg_amg_solver_set_finest_iters": (I, [P, I]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
@@ -433,28 +433,25 @@ class AMGSolver:
     def autotune(self, grid, candidates=None, max_iters=100, relative_tolerance=1e-6, repeats=2):
         """Time solves of the grid's current rhs (channel 1) under each candidate
         (omega, mu, level_iters, coarsest_iters[, finest_iters]) and keep the fastest that
-        converges.  Sets self.omega, self.mu_cycle_repeat_times and self.finest_iters; returns
-        (best candidate as a 5-tuple or None, table of (candidate, ms or None, iters))."""
+        converges.  Sets omega, mu_cycle_repeat_times and finest_iters; returns (best candidate
+        as a 5-tuple or None, table of (candidate, ms or None, iters))."""
         if candidates is None:
             candidates = default_tune_candidates()
         candidates = [tuple(c) + (-1,) * (5 - len(c)) for c in candidates]
         n = len(candidates)
-        fi = np.array([c[4] for c in candidates], np.int32)
-        om = np.array([c[0] for c in candidates], np.float64)
-        mu = np.array([c[1] for c in candidates], np.int32)
-        li = np.array([c[2] for c in candidates], np.int32)
-        ci = np.array([c[3] for c in candidates], np.int32)
+        arr = (TuneCandidate * n)(*[TuneCandidate(float(c[0]), int(c[1]), int(c[2]), int(c[3]), int(c[4])) for c in candidates])
         ms = np.zeros(n, np.float32)
         its = np.zeros(n, np.int32)
         best = ctypes.c_int(-1)
         self._sync_params()
-        _check(self.L.cmg_amg_solver_autotune(self.h, grid.h, n, _p(om), _p(mu), _p(li), _p(ci), _p(fi), max_iters,
-                                               relative_tolerance, repeats, _p(ms), _p(its), ctypes.byref(best)), "autotune")
-        table = [(tuple(candidates[i]), float(ms[i]) if ms[i] >= 0 else None, int(its[i])) for i in range(n)]
+        _check(self.L.cmg_amg_solver_autotune(self.h, grid.h, n, ctypes.cast(arr, ctypes.c_void_p), max_iters, relative_tolerance,
+                                               repeats, _p(ms), _p(its), ctypes.byref(best)), "autotune")
+        table = [(candidates[i], float(ms[i]) if ms[i] >= 0 else None, int(its[i])) for i in range(n)]
         if best.value < 0:
             return None, table
-        b = tuple(candidates[best.value])
-        self.omega, self.mu_cycle_repeat_times, self.finest_iters = float(b[0]), int(b[1]), int(b[4])
+        b = candidates[best.value]
+        self.omega, self.mu_cycle_repeat_times = float(b[0]), int(b[1])
+        self.finest_iters = int(b[4])
         return b, table
 
     def _sync_params(self):
@@ -513,6 +510,12 @@ class AMGSolver:
         n = ctypes.c_longlong(0)
         _check(self.L.cmg_amg_last_solve_launches(self.h, ctypes.byref(n)), "last_solve_launches")
         return n.value
+
+
+class TuneCandidate(ctypes.Structure):
+    """cmg_tune_candidate of include/cmg.h."""
+    _fields_ = [("omega", ctypes.c_double), ("mu", ctypes.c_int), ("level_iters", ctypes.c_int),
+                ("coarsest_iters", ctypes.c_int), ("finest_iters", ctypes.c_int)]
 
 
 def default_tune_candidates():

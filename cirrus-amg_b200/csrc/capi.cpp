@@ -421,19 +421,20 @@ int cmg_amg_solver_set_finest_iters(cmg_amg_solver* s, int finest_iters) {
     s->s.finest_iters = finest_iters;
     return CMG_OK;
 }
-int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const double* omega, const int* mu, const int* level_iters,
-                            const int* coarsest_iters, const int* finest_iters, int max_iters, double tol, int repeats, float* ms,
-                            int* iters, int* best) {
+int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const cmg_tune_candidate* c, int max_iters, double tol, int repeats,
+                            float* ms, int* iters, int* best) {
     GUARD_BEGIN
-    if (!s || !g || n <= 0 || !omega || !mu || !level_iters || !coarsest_iters || !ms || !iters || !best || max_iters <= 0 ||
-        !(tol > 0.0) || repeats < 1)
+    if (!s || !g || n <= 0 || !c || !ms || !iters || !best || max_iters <= 0 || !(tol > 0.0) || repeats < 1)
         return fail(CMG_ERR_INVALID, "cmg_amg_solver_autotune: bad argument");
-    for (int i = 0; i < n; ++i)
-        if (!(omega[i] > 0.0) || mu[i] < 0 || level_iters[i] < 0 || coarsest_iters[i] < 0 || (finest_iters && finest_iters[i] < -1))
+    std::vector<cmg::TuneCandidate> v(n);
+    for (int i = 0; i < n; ++i) {
+        if (!(c[i].omega > 0.0) || c[i].mu < 0 || c[i].level_iters < 0 || c[i].coarsest_iters < 0 || c[i].finest_iters < -1)
             return fail(CMG_ERR_INVALID, "cmg_amg_solver_autotune: bad candidate");
+        v[i] = cmg::TuneCandidate{c[i].omega, c[i].mu, c[i].level_iters, c[i].coarsest_iters, c[i].finest_iters};
+    }
     if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_solver_autotune: not an AMG solver");
     if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_amg_solver_autotune: grid not built");
-    return s->s.autotune(g->g, n, omega, mu, level_iters, coarsest_iters, finest_iters, max_iters, tol, repeats, ms, iters, best);
+    return s->s.autotune(g->g, n, v.data(), max_iters, tol, repeats, ms, iters, best);
     GUARD_END
 }
 int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags) {

@@ -861,33 +861,33 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     return rc;
 }
 
-int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, const int* li_c, const int* ci_c, const int* fi_c,
-                     int max_iters, double tol, int repeats, float* ms, int* iters, int* best) {
+int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, double tol, int repeats, float* ms, int* iters, int* best) {
     *best = -1;
     if (int rc = ensure_aux(G)) return rc;  // bsave keeps the rhs between the timed solves
     const size_t bytes = sizeof(float) * (size_t)G.n * kCells;
     CK(cudaMemcpyAsync(bsave, G.plane(1), bytes, cudaMemcpyDeviceToDevice, G.stream));
     const double omega0 = omega;
     const int mu0 = mu, fi0 = finest_iters;
+    auto restore = [&]() { omega = omega0, mu = mu0, finest_iters = fi0; };
     float best_ms = 0.0f;
     for (int i = 0; i < n; ++i) {
-        omega = omega_c[i];
-        mu = mu_c[i];
-        finest_iters = fi_c ? fi_c[i] : -1;
+        omega = c[i].omega;
+        mu = c[i].mu;
+        finest_iters = c[i].finest_iters;
         float tmin = -1.0f;
         bool ok = true;
         int it = 0;
         for (int r = 0; r <= repeats; ++r) {  // the first solve builds the graph and is not counted
             CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
-            if (int rc = solve_begin(G, max_iters, tol, li_c[i], ci_c[i], 1, false)) {
-                omega = omega0, mu = mu0, finest_iters = fi0;
+            if (int rc = solve_begin(G, max_iters, tol, c[i].level_iters, c[i].coarsest_iters, 1, false)) {
+                restore();
                 return rc;
             }
             double rel = 0.0;
             const int rc = solve_finish(false, &it, &rel);
             if (rc == 5) ok = false;  // non-finite: this setting diverges
             else if (rc) {
-                omega = omega0, mu = mu0, finest_iters = fi0;
+                restore();
                 return rc;
             }
             if (!(h_s->converged || h_s->rr0 == 0.0)) ok = false;
@@ -907,14 +907,11 @@ int Solver::autotune(Grid& G, int n, const double* omega_c, const int* mu_c, con
     }
     CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
     CK(cudaStreamSynchronize(G.stream));
+    restore();
     if (*best >= 0) {
-        omega = omega_c[*best];
-        mu = mu_c[*best];
-        finest_iters = fi_c ? fi_c[*best] : -1;
-    } else {
-        omega = omega0;
-        mu = mu0;
-        finest_iters = fi0;
+        omega = c[*best].omega;
+        mu = c[*best].mu;
+        finest_iters = c[*best].finest_iters;
     }
     return 0;
 }

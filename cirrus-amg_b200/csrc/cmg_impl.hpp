@@ -80,6 +80,11 @@ struct MuArgs {
 
 struct Net;
 
+struct TuneCandidate {
+    double omega;
+    int mu, level_iters, coarsest_iters, finest_iters;
+};
+
 // AMGSolver (src/AMGSolver.h:19-75)
 struct Solver {
     int coeff_ch;
@@ -188,8 +193,7 @@ struct Solver {
     // Autotuner: times solves of the grid's current rhs (channel 1) under each candidate
     // (omega, mu, level_iters, coarsest_iters), keeps the fastest that converges and sets its
     // omega and mu on the solver.  ms[i] = best of `repeats` timed solves (-1: not converged).
-    int autotune(Grid& G, int n, const double* omega, const int* mu, const int* level_iters, const int* coarsest_iters,
-                 const int* finest_iters, int max_iters, double tol, int repeats, float* ms, int* iters, int* best);
+    int autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, double tol, int repeats, float* ms, int* iters, int* best);
     // solve() in two halves, for batches of independent solves: solve_begin enqueues the whole
     // solve and the read-back of its scalars on the grid's stream and returns; solve_finish
     // waits for that stream and computes (iters, rel) as solve() does

@@ -181,21 +181,26 @@ int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float 
 int cmg_amg_solver_destroy(cmg_amg_solver* s);
 /* public fields omega / mu_cycle_repeat_times (src/AMGSolver.h:306-307) */
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
+/* One smoother setting for the autotuner.  finest_iters: sweeps per visit (before and after
+ * the coarse correction alike) on the finest level, levels >= 3; -1: level_iters, which is
+ * the reference's cycle. */
+typedef struct cmg_tune_candidate {
+    double omega;
+    int mu, level_iters, coarsest_iters, finest_iters;
+} cmg_tune_candidate;
 /* Autotuner (no counterpart in the reference): solves the grid's current rhs (channel 1)
- * under each of n candidate smoother settings (omega[i], mu[i], level_iters[i],
- * coarsest_iters[i], finest_iters[i]) to tol, `repeats` timed solves each after one untimed solve (a candidate
- * whose first solve is slower than 1.5x the best so far, or does not converge, is not timed
- * further; its ms[i] is that first solve's), and keeps
- * the fastest setting that converges: ms[i] (-1: did not converge), iters[i], *best (-1:
- * none).  The solver's omega and mu become the best candidate's; pass its level_iters and
- * coarsest_iters to cmg_amg_solve.  Channel 1 is restored, channel 0 holds the last solution.
- * Tune on a right-hand side other than the ones to be timed. */
-int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const double* omega, const int* mu, const int* level_iters,
-                            const int* coarsest_iters, const int* finest_iters, int max_iters, double tol, int repeats, float* ms,
-                            int* iters, int* best);
-/* Sweeps per visit on the finest level (levels >= 3), -1 (default): level_iters, as the
- * reference does on every level.  No counterpart in the reference.  finest_iters of the
- * autotuner (may be NULL) are candidates for it; the best one is set on the solver. */
+ * under each of n candidate settings to tol, `repeats` timed solves each after one untimed
+ * solve (a candidate whose first solve is slower than 1.5x the best so far, or does not
+ * converge, is not timed further; its ms[i] is that first solve's), and keeps the fastest
+ * setting that converges: ms[i] (-1: did not converge), iters[i], *best (-1: none).  The
+ * solver takes the best candidate's omega, mu and finest_iters; pass its
+ * level_iters and coarsest_iters to cmg_amg_solve.  Channel 1 is restored, channel 0 holds
+ * the last solution.  Tune on a right-hand side other than the ones to be timed. */
+int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const cmg_tune_candidate* candidates, int max_iters, double tol,
+                            int repeats, float* ms, int* iters, int* best);
+/* Sweeps per visit on the finest level (levels >= 3), the same before and after the coarse
+ * correction so that the preconditioner stays symmetric; -1 (default): level_iters, as the
+ * reference does on every level.  No counterpart in the reference. */
 int cmg_amg_solver_set_finest_iters(cmg_amg_solver* s, int finest_iters);
 /* Launch flags (default CMG_LAUNCH_GRAPH).
  * GRAPH: the solve runs as one CUDA graph with a device-side while loop;

@@ -129,15 +129,14 @@ def test_autotune_rejects_bad_arguments():
     """cmg_amg_solver_autotune checks its arguments before touching the GPU (a solver needs a
     GPU to exist, so only the null-object and empty-candidate cases run here)."""
     L = cmg.lib()
-    om = np.array([1.0], np.float64)
-    mu = np.array([1], np.int32)
-    li = np.array([2], np.int32)
-    ci = np.array([5], np.int32)
+    arr = (cmg.TuneCandidate * 1)(cmg.TuneCandidate(1.0, 1, 2, 5, -1))
     ms = np.zeros(1, np.float32)
     its = np.zeros(1, np.int32)
     best = ctypes.c_int(7)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     for n, tol in [(1, 1e-6), (0, 1e-6), (1, 0.0)]:
-        assert L.cmg_amg_solver_autotune(None, None, n, P(om), P(mu), P(li), P(ci), None, 10, ctypes.c_double(tol), 1, P(ms),
+        assert L.cmg_amg_solver_autotune(None, None, n, ctypes.cast(arr, ctypes.c_void_p), 10, ctypes.c_double(tol), 1, P(ms),
                                          P(its), ctypes.byref(best)) == 1
     assert b"autotune" in L.cmg_last_error()
+    assert L.cmg_amg_solver_set_finest_iters(None, 2) == 1
+    assert ctypes.sizeof(cmg.TuneCandidate) == 24
