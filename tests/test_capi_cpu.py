@@ -140,3 +140,29 @@ def test_autotune_rejects_bad_arguments():
     assert b"autotune" in L.cmg_last_error()
     assert L.cmg_amg_solver_set_finest_iters(None, 2) == 1
     assert ctypes.sizeof(cmg.TuneCandidate) == 24
+
+
+def test_default_tune_candidates_are_valid_and_symmetric():
+    """The autotuner's default search: distinct settings, the reference setting among them, and
+    a finest-level sweep count below the level count only (never asymmetric pre/post)."""
+    cands = cmg.default_tune_candidates()
+    assert len(cands) == len(set(cands)) == 156
+    assert (1.5, 2, 2, 10, -1) in cands
+    for om, mu, li, ci, fi in cands:
+        assert om > 0 and mu in (1, 2) and li >= 1 and ci >= 1
+        assert fi == -1 or 1 <= fi < li
+
+
+def test_moving_sphere_positions_stay_inside_the_domain():
+    """The moving-sphere sequence: centre on a circle of radius 0.25 in z = 0.5, 400 steps per
+    turn, sphere (r = 0.1) and its 0.15 refinement band inside [0, 1]^3."""
+    import bench
+
+    for k in (0, 50, 100, 199, 399):
+        sp = bench.moving_sphere_spec(k)
+        cx, cy, cz, r = sp["spheres"][0]
+        assert abs(np.hypot(cx - 0.5, cy - 0.5) - 0.25) < 1e-12 and cz == 0.5 and r == 0.1
+        assert min(cx, cy, cz) - r - 0.15 >= 0.0 - 1e-12 and max(cx, cy, cz) + r + 0.15 <= 1.0 + 1e-12
+        assert sp["params"][3:6] == [cx, cy, cz]
+    c0, c400 = bench.moving_sphere_spec(0)["spheres"][0], bench.moving_sphere_spec(400)["spheres"][0]
+    assert np.allclose(c0, c400)
