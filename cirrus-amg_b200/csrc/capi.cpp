@@ -13,7 +13,15 @@
 
 struct cmg_grid {
     cmg::Grid g;
+    // reduction scratch of the stand-alone dot product, owned by (and freed with) the grid
+    double* dot_partial = nullptr;
+    cmg::PcgScalars* dot_s = nullptr;
+    int dot_cap = 0;
     cmg_grid(float h0, int nl, int nc) : g(h0, nl, nc) {}
+    ~cmg_grid() {
+        if (dot_partial) cudaFree(dot_partial);
+        if (dot_s) cudaFree(dot_s);
+    }
 };
 struct cmg_learned {
     cmg::Net n;
@@ -45,20 +53,6 @@ bool host_ready(cmg_grid* g) { return g && g->g.built && g->g.topo.size() > 0; }
 // topology built and its device copy current (uploads it on first use)
 bool grid_ready(cmg_grid* g) { return host_ready(g) && g->g.ensure_device() == 0; }
 bool chan_ok(cmg_grid* g, int ch) { return ch >= 0 && ch < g->g.nch; }
-
-// per-grid reduction scratch for stand-alone dot products
-struct DotScratch {
-    double* partial = nullptr;
-    cmg::PcgScalars* s = nullptr;
-    int cap = 0;
-};
-DotScratch& dot_scratch(cmg_grid* g) {
-    static thread_local std::vector<std::pair<cmg_grid*, DotScratch>> v;
-    for (auto& p : v)
-        if (p.first == g) return p.second;
-    v.push_back({g, DotScratch{}});
-    return v.back().second;
-}
 
 int prepare_system(cmg::Grid& G, int coeff_ch, float R) {
     const cmg::DevGrid d = G.dev();
@@ -361,19 +355,20 @@ int cmg_amg_dot(cmg_grid* g, int a_ch, int b_ch, double* out) {
     if (!grid_ready(g) || !out) return fail(CMG_ERR_STATE, "grid not built");
     if (!chan_ok(g, a_ch) || !chan_ok(g, b_ch)) return fail(CMG_ERR_INVALID, "cmg_amg_dot: channel out of range");
     cmg::Grid& G = g->g;
-    DotScratch& D = dot_scratch(g);
-    if (D.cap < G.nleaf) {
-        if (D.partial) cudaFree(D.partial);
-        CKC(cudaMalloc(&D.partial, sizeof(double) * (G.nleaf + 1)));
-        D.cap = G.nleaf;
+    if (g->dot_cap < G.nleaf) {
+        if (g->dot_partial) cudaFree(g->dot_partial);
+        g->dot_partial = nullptr;
+        g->dot_cap = 0;
+        CKC(cudaMalloc(&g->dot_partial, sizeof(double) * (G.nleaf + 1)));
+        g->dot_cap = G.nleaf;
     }
-    if (!D.s) {
-        CKC(cudaMalloc(&D.s, sizeof(cmg::PcgScalars)));
-        CKC(cudaMemset(D.s, 0, sizeof(cmg::PcgScalars)));
+    if (!g->dot_s) {
+        CKC(cudaMalloc(&g->dot_s, sizeof(cmg::PcgScalars)));
+        CKC(cudaMemset(g->dot_s, 0, sizeof(cmg::PcgScalars)));
     }
     if (!G.dot_out) CKC(cudaMalloc(&G.dot_out, sizeof(double)));
     cmg::launch_dot(G.dev(), G.leaf, G.nleaf, G.plane(a_ch), G.plane(b_ch), cmg::kDotStore, G.dot_out,
-                    cmg::ReduceScratch{D.partial, nullptr, D.s}, G.stream);
+                    cmg::ReduceScratch{g->dot_partial, nullptr, g->dot_s}, G.stream);
     CKC(cudaMemcpyAsync(out, G.dot_out, sizeof(double), cudaMemcpyDeviceToHost, G.stream));
     CKC(cudaStreamSynchronize(G.stream));
     return CMG_OK;
