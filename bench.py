@@ -29,7 +29,8 @@ U(0.2, 0.8)^3), level 3 elsewhere, 2:1 graded, each with its own Fourier-
 divergence rhs; a step solves all 64 through one cmg_amg_solve_batch call, 16
 streams; the metric is solves per second, with p50/p99 per-solve device time.
 
-N > 1 runs N independent replicas (the path does not shard).
+N > 1 runs N independent replicas: one solve works on one octree in one GPU's memory,
+and the path has no partition that avoids an exchange per sweep.
 """
 import argparse
 import json

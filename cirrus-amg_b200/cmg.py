@@ -37,7 +37,7 @@ EXPORTS = [
     "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
     "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
     "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_copy_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
-    "cmg_grid_calc_cell_types_from_leafs", "cmg_grid_load_hagr", "cmg_grid_dump_hagr",
+    "cmg_grid_calc_cell_types_from_leafs", "cmg_grid_load_hagr", "cmg_grid_dump_hagr", "cmg_ref_record_layout",
     "cmg_grid_synchronize",
     "cmg_amg_prepare_types_and_coeffs", "cmg_amg_prepare_system", "cmg_amg_cutcell_sphere_coeffs",
     "cmg_amg_face_velocity_fourier", "cmg_amg_divergence", "cmg_amg_add_gradient_to_face", "cmg_amg_full_neg_lap",
@@ -98,6 +98,7 @@ def lib():
             "cmg_grid_set_stream": (I, [P, P]),
             "cmg_grid_calc_cell_types_from_leafs": (I, [P]),
             "cmg_grid_load_hagr": (I, [P, S, I, PP]),
+            "cmg_ref_record_layout": (I, [P, I]),
             "cmg_grid_dump_hagr": (I, [P, P, S, ctypes.POINTER(ctypes.c_size_t)]),
             "cmg_grid_synchronize": (I, [P]),
             "cmg_amg_prepare_types_and_coeffs": (I, [P, I, F]),
@@ -158,6 +159,19 @@ def lib():
 
 class CmgError(RuntimeError):
     pass
+
+
+def ref_record_layout():
+    """The 'HAGR' header and PoissonTile<float,15> record layout the library assumes
+    (see cmg_ref_record_layout in include/cmg.h), as a dict."""
+    L = lib()
+    m = L.cmg_ref_record_layout(None, 0)
+    out = (ctypes.c_longlong * m)()
+    L.cmg_ref_record_layout(out, m)
+    keys = ["header_bytes", "off_magic", "off_version", "off_num_levels", "off_max_level", "off_tile_size",
+            "off_coord_size", "off_h0", "off_tile_count", "coord_bytes", "tile_bytes", "types_offset",
+            "channels", "channel_stride"]
+    return dict(zip(keys, list(out)))
 
 
 def check_division(n, seed=0):

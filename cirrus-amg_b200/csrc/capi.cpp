@@ -385,7 +385,7 @@ int cmg_amg_dot_noalloc(cmg_grid* g, int a_ch, int b_ch, double* out) {
     }
     // uploading the topology would allocate: the device copy must already be current
     if (G.dev_version != G.host_version || G.n <= 0) return fail(CMG_ERR_STATE, "cmg_amg_dot_noalloc: the grid has no current device copy");
-    return cmg::check_cuda(cmg::dot_noalloc(G.leaf, G.nleaf, G.plane(a_ch), G.plane(b_ch), out, G.stream), "cmg_amg_dot_noalloc");
+    return cmg::check_cuda(cmg::dot_noalloc(G.device, G.leaf, G.nleaf, G.plane(a_ch), G.plane(b_ch), out, G.stream), "cmg_amg_dot_noalloc");
 }
 
 int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float P, cmg_amg_solver** out) {
@@ -407,7 +407,7 @@ int cmg_amg_solver_destroy(cmg_amg_solver* s) {
 }
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu) {
     if (!s || mu < 0 || !(omega > 0)) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_smoother: bad argument");
-    s->s.omega = omega;
+    s->s.omega = (double)(float)omega;  // AMGSolver::omega is a float (src/AMGSolver.h:29)
     s->s.mu = mu;
     return CMG_OK;
 }
@@ -425,7 +425,7 @@ int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const cmg_tun
     for (int i = 0; i < n; ++i) {
         if (!(c[i].omega > 0.0) || c[i].mu < 0 || c[i].level_iters < 0 || c[i].coarsest_iters < 0 || c[i].finest_iters < -1)
             return fail(CMG_ERR_INVALID, "cmg_amg_solver_autotune: bad candidate");
-        v[i] = cmg::TuneCandidate{c[i].omega, c[i].mu, c[i].level_iters, c[i].coarsest_iters, c[i].finest_iters};
+        v[i] = cmg::TuneCandidate{(double)(float)c[i].omega, c[i].mu, c[i].level_iters, c[i].coarsest_iters, c[i].finest_iters};
     }
     if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, "cmg_amg_solver_autotune: not an AMG solver");
     if (!grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_amg_solver_autotune: grid not built");
@@ -727,6 +727,9 @@ namespace {
 constexpr uint32_t kHagrMagic = 0x52474148u;
 constexpr size_t kHagrHeader = 40, kHagrTile = 44880, kHagrCoord = 12, kHagrTypes = 44352;
 constexpr int kHagrChannels = 15, kHagrChannelStride = 736;
+// byte offsets of the header fields: magic, version, num_levels, max_level, tile_size,
+// coord_size, h0, tile_count
+constexpr size_t kHagrOff[8] = {0, 4, 8, 12, 16, 20, 24, 32};
 constexpr size_t kHagrRecord = 4 + 1 + kHagrCoord + kHagrTile;
 template <class T>
 T rd(const uint8_t* p) {
@@ -742,17 +745,29 @@ void wr(uint8_t* p, T v) {
 
 extern "C" {
 
+int cmg_ref_record_layout(long long* out, int n) {
+    static_assert(kHagrTile == cmg::kRefTileBytes, "one tile layout for blobs and device views");
+    const long long v[] = {(long long)kHagrHeader, (long long)kHagrOff[0], (long long)kHagrOff[1], (long long)kHagrOff[2],
+                           (long long)kHagrOff[3], (long long)kHagrOff[4], (long long)kHagrOff[5], (long long)kHagrOff[6],
+                           (long long)kHagrOff[7], (long long)kHagrCoord, (long long)kHagrTile, (long long)kHagrTypes,
+                           (long long)kHagrChannels, (long long)kHagrChannelStride};
+    const int m = (int)(sizeof(v) / sizeof(v[0]));
+    if (!out) return m;
+    for (int i = 0; i < m && i < n; ++i) out[i] = v[i];
+    return m;
+}
+
 int cmg_grid_load_hagr(const uint8_t* blob, size_t size, int num_channels, cmg_grid** out) {
     GUARD_BEGIN
     if (!blob || !out || num_channels < 1) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad argument");
     if (size < kHagrHeader) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: buffer too small");
-    if (rd<uint32_t>(blob) != kHagrMagic) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad magic");
-    if (rd<uint32_t>(blob + 4) != 1) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: unsupported version");
-    const uint32_t num_levels = rd<uint32_t>(blob + 8);
-    if (rd<uint32_t>(blob + 16) != kHagrTile) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: tile size is not that of PoissonTile<float,15>");
-    if (rd<uint32_t>(blob + 20) != kHagrCoord) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: coordinate size mismatch");
-    const float h0 = rd<float>(blob + 24);
-    const uint64_t count = rd<uint64_t>(blob + 32);
+    if (rd<uint32_t>(blob + kHagrOff[0]) != kHagrMagic) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad magic");
+    if (rd<uint32_t>(blob + kHagrOff[1]) != 1) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: unsupported version");
+    const uint32_t num_levels = rd<uint32_t>(blob + kHagrOff[2]);
+    if (rd<uint32_t>(blob + kHagrOff[4]) != kHagrTile) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: tile size is not that of PoissonTile<float,15>");
+    if (rd<uint32_t>(blob + kHagrOff[5]) != kHagrCoord) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: coordinate size mismatch");
+    const float h0 = rd<float>(blob + kHagrOff[6]);
+    const uint64_t count = rd<uint64_t>(blob + kHagrOff[7]);
     if (num_levels < 1 || num_levels > 16 || !(h0 > 0)) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: bad header");
     const size_t body = kHagrHeader + 4 * (size_t)num_levels;
     if (size < body || (size - body) / kHagrRecord < count) return fail(CMG_ERR_INVALID, "cmg_grid_load_hagr: buffer truncated");
@@ -814,14 +829,14 @@ int cmg_grid_dump_hagr(cmg_grid* g, uint8_t* buf, size_t capacity, size_t* size)
     CKC(cudaMemcpyAsync(types.data(), G.ctype, types.size(), cudaMemcpyDeviceToHost, G.stream));
     CKC(cudaStreamSynchronize(G.stream));
     std::memset(buf, 0, total);
-    wr<uint32_t>(buf, kHagrMagic);
-    wr<uint32_t>(buf + 4, 1);
-    wr<uint32_t>(buf + 8, (uint32_t)nl);
-    wr<int32_t>(buf + 12, G.max_level());
-    wr<uint32_t>(buf + 16, (uint32_t)kHagrTile);
-    wr<uint32_t>(buf + 20, (uint32_t)kHagrCoord);
-    wr<float>(buf + 24, G.topo.h0());
-    wr<uint64_t>(buf + 32, (uint64_t)n);
+    wr<uint32_t>(buf + kHagrOff[0], kHagrMagic);
+    wr<uint32_t>(buf + kHagrOff[1], 1);
+    wr<uint32_t>(buf + kHagrOff[2], (uint32_t)nl);
+    wr<int32_t>(buf + kHagrOff[3], G.max_level());
+    wr<uint32_t>(buf + kHagrOff[4], (uint32_t)kHagrTile);
+    wr<uint32_t>(buf + kHagrOff[5], (uint32_t)kHagrCoord);
+    wr<float>(buf + kHagrOff[6], G.topo.h0());
+    wr<uint64_t>(buf + kHagrOff[7], (uint64_t)n);
     for (int l = 0; l < nl; ++l) {
         // hash size for the reference's loader: room for twice the level's tiles, at least 2^8
         const int cnt = l <= G.max_level() ? G.level_end(l) - G.level_begin(l) : 0;

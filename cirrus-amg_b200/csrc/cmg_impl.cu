@@ -110,6 +110,7 @@ int Grid::ensure_device() {
     float* chan_new = nullptr;
     uint8_t* ct_new = nullptr;
     const size_t cells = (size_t)n_new * kCells;
+    if (device < 0) CK(cudaGetDevice(&device));
     CK(cudaMalloc(&chan_new, sizeof(float) * cells * nch + 16));
     CK(cudaMalloc(&ct_new, cells + 16));
     int2* d_map = nullptr;

@@ -42,6 +42,7 @@ struct Grid {
     void** tile_ptrs = nullptr;  // device copy of a caller's tile address list (reference tiles)
     int tile_ptrs_cap = 0;
     double* dot_out = nullptr;
+    int device = -1;  // the CUDA device the device copy lives on (current at its first allocation)
 
     Grid(float h0, int num_levels, int num_channels) : topo(h0, num_levels), nch(num_channels) {}
     ~Grid();

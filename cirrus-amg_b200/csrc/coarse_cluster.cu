@@ -114,14 +114,13 @@ __device__ __forceinline__ float nlap(float d, float x, float cmx, float xmx, fl
     s = __fmaf_rn(cpz, xpz, s);
     return s;
 }
-// one Gauss-Seidel update (src/AMGSolver.cu:868-875); kExact: omega is a float, so x + delta * omega
-// in double rounds to the single fused multiply-add (a compile-time choice keeps the other form
-// off every update's dependency chain)
+// one Gauss-Seidel update (src/AMGSolver.cu:868-875); kExact: omega is a float (as the
+// reference's AMGSolver::omega always is), so the product delta * omega is exact in double
 template <bool kExact>
 __device__ __forceinline__ float gs_update(float xs, float rhs, float ax, float d, double yd, bool interior, const ClusterArgs& A) {
     const float delta = interior ? div_by_recip(__fsub_rn(rhs, ax), d, yd) : 0.0f;
     if constexpr (kExact)
-        return __fmaf_rn(delta, A.om, xs);
+        return relax_ref(xs, delta, A.om);
     else
         return (float)((double)xs + (double)delta * A.omega);
 }

@@ -323,4 +323,13 @@ __device__ __forceinline__ double recip_f64(float d) {
 // division routine on the dependent chain of a Gauss-Seidel update
 __device__ __forceinline__ float div_exact(float a, float d) { return div_by_recip(a, d, recip_f64(d)); }
 
+// The Gauss-Seidel relaxation x + delta * omega as the reference evaluates it
+// (src/AMGSolver.cu:874): delta and x are floats, omega a float held in a double, so the
+// product is exact in double, the sum is rounded once to double and then once to float.
+// A single-precision fused multiply-add rounds once to float and can differ from that in
+// the last bit (a sum within half a double ulp of a float midpoint), so it is not used.
+__device__ __forceinline__ float relax_ref(float xs, float delta, float om) {
+    return __double2float_rn(__fma_rn((double)delta, (double)om, (double)xs));
+}
+
 }  // namespace cmg

@@ -11,17 +11,23 @@
 // Limits and rules:
 //  * at most kNoAllocMaxLeafTiles LEAF tiles (one partial sum per tile); larger grids
 //    are rejected with CMG_ERR_INVALID before anything is launched;
-//  * the arrival counter (the last scratch word) must start at zero.  Static device
-//    memory is zero when the module loads, and the block that finishes last resets it
-//    to zero, so every call leaves it ready for the next;
+//  * each call clears the arrival counter (a scratch word) on its stream before its
+//    launch (cudaMemsetAsync, which allocates nothing) and poisons the result word with a
+//    NaN, so a call never depends on what an earlier call left in the array;
 //  * the scratch is shared by all calls on a device, so calls that overlap in time
-//    (other streams, other host threads) race on it and give wrong results.  Calls
-//    must be ordered, e.g. on one stream;
+//    (other streams, other host threads) race on it and give wrong results -- the
+//    overlapping calls only, since the next ordered call starts clean.  A call whose
+//    result word still holds the NaN after its launch reports CMG_ERR_CUDA.  Calls must
+//    be ordered, e.g. on one stream;
+//  * the call runs on the grid's device (the one current when its device copy was
+//    first allocated), switching to it and back if another device is current;
 //  * the first call on each device looks up the array's device address for that device
 //    (cudaGetSymbolAddress, with the device current); later calls reuse it.  Make one
-//    call on each device before the time-critical part starts.
+//    call on each device before the time-critical part starts.  The cached address is
+//    not refreshed after cudaDeviceReset, so do not use this entry point across one.
 // The arithmetic and summation order are those of k_dot, so the result equals
 // cmg_amg_dot's bit for bit.
+#include <cstring>
 #include <mutex>
 
 #include "kernels.hpp"
@@ -69,16 +75,14 @@ constexpr int kMaxDevices = 64;
 std::mutex g_addr_mutex;
 unsigned long long* g_addr[kMaxDevices] = {};
 
-// device address of the scratch array on the current device (looked up once per device)
-cudaError_t scratch_address(unsigned long long** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
+// device address of the scratch array on device dev, which must be current (looked up
+// once per device)
+cudaError_t scratch_address(int dev, unsigned long long** out) {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_addr_mutex);
     if (!g_addr[dev]) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_dot_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_dot_scratch);
         if (e != cudaSuccess) return e;
         g_addr[dev] = static_cast<unsigned long long*>(p);
     }
@@ -90,22 +94,49 @@ cudaError_t scratch_address(unsigned long long** out) {
 
 int dot_noalloc_max_leaf_tiles() { return kNoAllocMaxLeafTiles; }
 
-cudaError_t dot_noalloc(const int* leaf, int nleaf, const float* A, const float* B, double* out_host, cudaStream_t st) {
-    if (nleaf <= 0) {
-        *out_host = 0.0;
-        return cudaSuccess;
-    }
-    if (nleaf > kNoAllocMaxLeafTiles) return cudaErrorInvalidValue;
+namespace {
+// the call proper, with the grid's device current
+cudaError_t dot_noalloc_on(int device, const int* leaf, int nleaf, const float* A, const float* B, double* out_host,
+                           cudaStream_t st) {
     unsigned long long* scratch = nullptr;
-    cudaError_t e = scratch_address(&scratch);
+    cudaError_t e = scratch_address(device, &scratch);
+    if (e != cudaSuccess) return e;
+    // counter to zero, result word to a NaN (all bits set): neither allocates
+    e = cudaMemsetAsync(scratch + kNoAllocMaxLeafTiles + 1, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch + kNoAllocMaxLeafTiles, 0xff, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     note_kernel_launch();
     k_dot_noalloc<<<nleaf, 128, 0, st>>>(leaf, A, B, scratch);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    e = cudaMemcpyAsync(out_host, scratch + kNoAllocMaxLeafTiles, sizeof(double), cudaMemcpyDeviceToHost, st);
+    unsigned long long bits = 0;
+    e = cudaMemcpyAsync(&bits, scratch + kNoAllocMaxLeafTiles, sizeof(bits), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
-    return cudaStreamSynchronize(st);
+    if (bits == ~0ull) return cudaErrorLaunchFailure;  // no block finished last: an overlapping call
+    std::memcpy(out_host, &bits, sizeof(double));
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t dot_noalloc(int device, const int* leaf, int nleaf, const float* A, const float* B, double* out_host,
+                        cudaStream_t st) {
+    if (nleaf <= 0) {
+        *out_host = 0.0;
+        return cudaSuccess;
+    }
+    if (nleaf > kNoAllocMaxLeafTiles) return cudaErrorInvalidValue;
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    if (device < 0) device = cur;
+    if (device != cur && (e = cudaSetDevice(device)) != cudaSuccess) return e;
+    e = dot_noalloc_on(device, leaf, nleaf, A, B, out_host, st);
+    if (device != cur) {
+        const cudaError_t e2 = cudaSetDevice(cur);
+        if (e == cudaSuccess) e = e2;
+    }
+    return e;
 }
 
 }  // namespace cmg

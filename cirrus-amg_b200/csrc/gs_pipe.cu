@@ -260,8 +260,8 @@ __device__ __forceinline__ float quad_neg_lap(const float* SX, const QuadOps& o,
     return ax;
 }
 
-// one colour pass over the staged tile; kExact: omega is a float and the update is one fused
-// multiply-add (compile-time, so the double form stays off the dependency chain)
+// one colour pass over the staged tile; kExact: omega is a float (the reference's form with an
+// exact double product, relax_ref)
 template <typename CT, bool kExact>
 __device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
                                         const PipeArgs& A) {
@@ -284,7 +284,7 @@ __device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const
         const float delta = in ? div_exact(__fsub_rn(f4get(b, u), ax), f4get(o.dg, u)) : 0.0f;
         const float xs = f4get(xm, u);
         if constexpr (kExact)
-            f4set(out, u, __fmaf_rn(delta, A.om, xs));
+            f4set(out, u, relax_ref(xs, delta, A.om));
         else
             f4set(out, u, (float)((double)xs + (double)delta * A.omega));
     }

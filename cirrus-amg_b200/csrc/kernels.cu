@@ -79,7 +79,7 @@ __device__ __forceinline__ void tile_gs(const DevGrid& g, int t, int tid, float*
         const float ax = own_neg_lap(S, Q, o, u);
         const float delta = (t4get(o.ty, u) & dInterior) ? div_exact(__fsub_rn(f4get(b, u), ax), d) : 0.0f;
         const float xs = f4get(o.xm, u);
-        f4set(out, u, A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega));
+        f4set(out, u, A.exact ? relax_ref(xs, delta, A.om) : (float)((double)xs + (double)delta * A.omega));
     }
     st4(X + Q.base, out);
     sync();
@@ -240,7 +240,7 @@ struct DenseLevel {
             const float ax = neg_lap(i, j, k);
             const float delta = (ty[c] & dInterior) ? div_exact(__fsub_rn(rhs[c], ax), d[c]) : 0.0f;
             const float xs = x[xi(i, j, k)];
-            x[xi(i, j, k)] = A.exact ? __fmaf_rn(delta, A.om, xs) : (float)((double)xs + (double)delta * A.omega);
+            x[xi(i, j, k)] = A.exact ? relax_ref(xs, delta, A.om) : (float)((double)xs + (double)delta * A.omega);
         }
         __syncthreads();
     }
@@ -782,13 +782,16 @@ __device__ float face_fluid_ratio(const float phi[4]) {
         const double t1 = 0.5 * (double)frac_inside(phi[f1], phi[(f1 + 3) & 3]) * (double)frac_inside(phi[f1], phi[(f1 + 1) & 3]);
         ret = (float)(t0 + t1);
     } else {
-        double s = 0;
+        // the two crossing edges of a trapezoid, summed in float (the sign of a zero
+        // result follows that sum)
+        float e[2] = {0.0f, 0.0f};
+        int ne = 0;
         for (int i = 0; i < 4; ++i) {
             if (in[i]) continue;
             const int nbc = in[(i + 1) & 3] ? ((i + 1) & 3) : ((i + 3) & 3);
-            s += (double)frac_inside(phi[i], phi[nbc]);
+            e[ne++] = frac_inside(phi[i], phi[nbc]);
         }
-        ret = (float)(0.5 * s);
+        ret = (float)(0.5 * (double)__fadd_rn(e[0], e[1]));
     }
     if (ret < 0.1f && ret != 0.0f) ret = 0.1f;
     return ret;

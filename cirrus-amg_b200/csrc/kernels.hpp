@@ -122,7 +122,7 @@ void note_kernel_launch();        // counts one launch made outside kernels.cu
 long long kernel_launch_count();
 // dot product over the LEAF tiles with scratch in a fixed static device array
 // (dot_noalloc.cu); cudaErrorInvalidValue if nleaf exceeds dot_noalloc_max_leaf_tiles()
-cudaError_t dot_noalloc(const int* leaf, int nleaf, const float* A, const float* B, double* out_host, cudaStream_t st);
+cudaError_t dot_noalloc(int device, const int* leaf, int nleaf, const float* A, const float* B, double* out_host, cudaStream_t st);
 int dot_noalloc_max_leaf_tiles();
 // div_by_recip against the IEEE division on n pseudo-random pairs; 0 or 2 (CUDA error)
 int check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair);  // kernels enqueued (or captured) by this library so far

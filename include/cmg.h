@@ -123,6 +123,14 @@ int cmg_grid_calc_cell_types_from_leafs(cmg_grid* g);
  * further channels.  Dumping writes every tile with min(num_channels, 15) channels;
  * with buf == NULL it only reports the size. */
 int cmg_grid_load_hagr(const uint8_t* blob, size_t size, int num_channels, cmg_grid** out);
+/* The record layout this library reads and writes, for a binding that checks it against
+ * its own build of the reference structs: out[0..13] = header bytes (sizeof of the local
+ * Header struct of HADeviceGrid::dumpBinaryBlob, src/HAGrid.h:699-708), the offsets of its
+ * eight fields (magic, version, num_levels, max_level, tile_size, coord_size, h0,
+ * tile_count), sizeof(Coord), sizeof(PoissonTile<float,15>), offsetof its mCellType,
+ * its channel count and channel stride in floats (src/PoissonTile.h:28-39).  Returns the
+ * number of entries (14); with out == NULL only that. */
+int cmg_ref_record_layout(long long* out, int n);
 /* A view of the reference's own device tiles, for a caller that keeps its HADeviceGrid
  * (src/HAGrid.h:357-406): every tile is a PoissonTile<float,15> in device memory
  * (src/PoissonTile.h:34-39: float mData[15][736], cell values in the first 512 of each
@@ -169,17 +177,21 @@ int cmg_amg_dot(cmg_grid* g, int a_ch, int b_ch, double* out);
  * allocate at the call: it allocates no memory.  Its scratch is a fixed 128 KB array in
  * the library's static device memory, so it serves grids of at most 16384 LEAF tiles
  * (larger grids: CMG_ERR_INVALID) and needs the grid's device copy to be current
- * already (CMG_ERR_STATE otherwise).  Calls that overlap in time share that scratch and
- * race.  The first call on a device looks up the scratch address.  No counterpart in
- * the reference. */
+ * already (CMG_ERR_STATE otherwise).  It runs on the grid's device.  Calls that overlap
+ * in time share that scratch and race; each call clears it first, so only the
+ * overlapping calls are affected, and one that finds no result reports CMG_ERR_CUDA.
+ * The first call on a device looks up the scratch address (not refreshed after a
+ * cudaDeviceReset).  No counterpart in the reference. */
 int cmg_amg_dot_noalloc(cmg_grid* g, int a_ch, int b_ch, double* out);
 
 /* ---- solver: AMGSolver ------------------------------------------------- */
-/* AMGSolver(coeff_channel, R_matrix, R_restrict, P) (src/AMGSolver.h:309);
- * omega = 1.5, mu = 2 as there (src/AMGSolver.h:306-307). */
+/* AMGSolver(coeff_channel, R_matrix, R_restrict, P) (src/AMGSolver.h:31);
+ * omega = 1.5, mu = 2 as there (src/AMGSolver.h:28-29). */
 int cmg_amg_solver_create(int coeff_ch, float R_matrix, float R_restrict, float P, cmg_amg_solver** out);
 int cmg_amg_solver_destroy(cmg_amg_solver* s);
-/* public fields omega / mu_cycle_repeat_times (src/AMGSolver.h:306-307) */
+/* public fields omega / mu_cycle_repeat_times (src/AMGSolver.h:28-29); omega is held as a
+ * float, as the reference's field is (T omega), so the Gauss-Seidel update
+ * x + delta * omega rounds exactly as the reference's does */
 int cmg_amg_solver_set_smoother(cmg_amg_solver* s, double omega, int mu);
 /* One smoother setting for the autotuner.  finest_iters: sweeps per visit (before and after
  * the coarse correction alike) on the finest level, levels >= 3; -1: level_iters, which is

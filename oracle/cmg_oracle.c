@@ -47,6 +47,7 @@ struct og_grid {
     int nch;
     float* data;
     uint8_t* ctype;
+    int ref_mask; /* apply CoarsenOffDiagCoefficientsOneStepKernel's cell-type mask to the stored types */
 };
 
 /* ------------------------------------------------------------------ */
@@ -240,13 +241,12 @@ static double box_sphere_surface_dist(const double mn[3], const double mx[3], co
     if (r < dn) return dn - r;
     return r - df;
 }
-static int case_target(const og_grid* g, const og_tile* T, int case_id, const double* prm, int nprm) {
+static int case_target_at(float h, const int tc[3], int case_id, const double* prm, int nprm) {
     int min_level = (int)prm[0], max_level = (int)prm[1];
-    float h = voxel_size(g, T->level);
     float mn[3], mx[3];
     for (int d = 0; d < 3; d++) { /* HAAccessor.h:123-128 */
-        mn[d] = ((float)T->c[d] * 8.0f) * h;
-        mx[d] = ((float)(T->c[d] + 1) * 8.0f) * h;
+        mn[d] = ((float)tc[d] * 8.0f) * h;
+        mx[d] = ((float)(tc[d] + 1) * 8.0f) * h;
     }
     switch (case_id) {
     case OG_CASE_UNIFORM: return max_level;
@@ -277,7 +277,7 @@ static int case_target(const og_grid* g, const og_tile* T, int case_id, const do
         int mid_level = (int)prm[2];
         double c[3] = {prm[3], prm[4], prm[5]}, r = prm[6], bf = prm[7], bm = prm[8];
         double dmn[3], dmx[3], hd = (double)h;
-        for (int d = 0; d < 3; d++) { dmn[d] = T->c[d] * 8.0 * hd; dmx[d] = (T->c[d] + 1) * 8.0 * hd; }
+        for (int d = 0; d < 3; d++) { dmn[d] = tc[d] * 8.0 * hd; dmx[d] = (tc[d] + 1) * 8.0 * hd; }
         double dist = box_sphere_surface_dist(dmn, dmx, c, r);
         return dist <= bf ? max_level : (dist <= bm ? mid_level : min_level);
     }
@@ -286,7 +286,7 @@ static int case_target(const og_grid* g, const og_tile* T, int case_id, const do
         double band = prm[2];
         int ns = (int)prm[3];
         double dmn[3], dmx[3], hd = (double)h;
-        for (int d = 0; d < 3; d++) { dmn[d] = T->c[d] * 8.0 * hd; dmx[d] = (T->c[d] + 1) * 8.0 * hd; }
+        for (int d = 0; d < 3; d++) { dmn[d] = tc[d] * 8.0 * hd; dmx[d] = (tc[d] + 1) * 8.0 * hd; }
         for (int s = 0; s < ns && 4 + 4 * s + 3 < nprm; s++) {
             double c[3] = {prm[4 + 4 * s], prm[5 + 4 * s], prm[6 + 4 * s]};
             if (box_sphere_surface_dist(dmn, dmx, c, prm[7 + 4 * s]) <= band) return max_level;
@@ -296,10 +296,28 @@ static int case_target(const og_grid* g, const og_tile* T, int case_id, const do
     }
     return min_level;
 }
+static int case_target(const og_grid* g, const og_tile* T, int case_id, const double* prm, int nprm) {
+    return case_target_at(voxel_size(g, T->level), T->c, case_id, prm, nprm);
+}
+/* exported for the reference pin: the target of the tile (level, i, j, k) */
+int og_case_target_at(float h0, int case_id, const double* prm, int nprm, int level, int i, int j, int k) {
+    int tc[3] = {i, j, k};
+    return case_target_at(h0 / (float)(1 << level), tc, case_id, prm, nprm);
+}
 
 /* HADeviceGrid::refineStep (HAGrid.h:1088-1170).  Reads see the grid as it
  * was at the start of the step, as the device-side flag kernels do. */
-static int refine_step(og_grid* g, int case_id, const double* prm, int nprm) {
+typedef struct {
+    int case_id, nprm;
+    const double* prm;
+    og_target_fn fn;
+    void* user;
+} target_src;
+static int target_of(const og_grid* g, const og_tile* T, const target_src* src) {
+    if (src->fn) return src->fn(src->user, T->level, T->c[0], T->c[1], T->c[2]);
+    return case_target(g, T, src->case_id, src->prm, src->nprm);
+}
+static int refine_step(og_grid* g, const target_src* src) {
     int nsnap = g->n, total = 0;
     int* type0 = (int*)malloc(sizeof(int) * (nsnap ? nsnap : 1));
     for (int t = 0; t < nsnap; t++) { type0[t] = g->t[t].type; g->t[t].flag = 0; }
@@ -308,7 +326,7 @@ static int refine_step(og_grid* g, int case_id, const double* prm, int nprm) {
         for (int t = 0; t < nsnap; t++) {
             og_tile* T = &g->t[t];
             if (T->level != L || !(type0[t] & OG_LEAF)) continue;
-            int refine = case_target(g, T, case_id, prm, nprm) > L;
+            int refine = target_of(g, T, src) > L;
             if (L < maxl) {
                 for (int ci = 0; ci < 8; ci++) {
                     int c = map_find(g, L + 1, 2 * T->c[0] + (ci & 1), 2 * T->c[1] + ((ci >> 1) & 1), 2 * T->c[2] + ((ci >> 2) & 1));
@@ -344,18 +362,28 @@ static int refine_step(og_grid* g, int case_id, const double* prm, int nprm) {
     return total;
 }
 
-/* HADeviceGrid::iterativeRefine (HAGrid.h:1173-1182) with a built-in target. */
-int og_refine_case(og_grid* g, int case_id, const double* prm, int nprm) {
+/* HADeviceGrid::iterativeRefine (HAGrid.h:1173-1182) */
+static int refine_loop(og_grid* g, const target_src* src) {
     compute_max_level(g);
     int steps = 0;
     while (1) {
-        int cnt = refine_step(g, case_id, prm, nprm);
+        int cnt = refine_step(g, src);
         spawn_ghosts(g);
         steps++;
         if (cnt == 0 || steps > 64) break;
     }
     finalize(g);
     return steps;
+}
+/* with a built-in target */
+int og_refine_case(og_grid* g, int case_id, const double* prm, int nprm) {
+    target_src src = {case_id, nprm, prm, NULL, NULL};
+    return refine_loop(g, &src);
+}
+/* with a caller's target function of (level, tile coordinate) */
+int og_refine_fn(og_grid* g, og_target_fn fn, void* user) {
+    target_src src = {0, 0, NULL, fn, user};
+    return refine_loop(g, &src);
 }
 
 int og_num_tiles(const og_grid* g) { return g->n; }
@@ -386,26 +414,33 @@ uint8_t* og_cell_types(og_grid* g) { return g->ctype; }
 #define CT(g, t) (g->ctype + (size_t)(t) * NC)
 
 /* CreateTestGrid cell types (TestGrids.cuh:161-167) for LEAF tiles. */
+static void leaf_cell_types_at(float h, const int tc[3], int case_id, uint8_t* out) {
+    for (int v = 0; v < NC; v++) {
+        int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+        uint8_t ty = OG_INTERIOR;
+        if (case_id == OG_CASE_SPHERE_SOLID || case_id == OG_CASE_STAR_SOLID) {
+            float mn[3], mx[3];
+            for (int d = 0; d < 3; d++) { /* HAAccessor.h:132-138 */
+                int gc = tc[d] * 8 + l[d];
+                mn[d] = (float)gc * h; mx[d] = (float)(gc + 1) * h;
+            }
+            int c = corner_count(case_id == OG_CASE_SPHERE_SOLID ? phi_sphere_quarter : phi_star, mn, mx, 0.0f);
+            ty = (c == 8) ? OG_NEUMANN : OG_INTERIOR;
+        }
+        out[v] = ty;
+    }
+}
 void og_set_leaf_cell_types_case(og_grid* g, int case_id, const double* prm, int nprm) {
     (void)prm; (void)nprm;
     for (int t = 0; t < g->n; t++) {
         if (!(g->t[t].type & OG_LEAF)) continue;
-        float h = voxel_size(g, g->t[t].level);
-        for (int v = 0; v < NC; v++) {
-            int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
-            uint8_t ty = OG_INTERIOR;
-            if (case_id == OG_CASE_SPHERE_SOLID || case_id == OG_CASE_STAR_SOLID) {
-                float mn[3], mx[3];
-                for (int d = 0; d < 3; d++) { /* HAAccessor.h:132-138 */
-                    int gc = g->t[t].c[d] * 8 + l[d];
-                    mn[d] = (float)gc * h; mx[d] = (float)(gc + 1) * h;
-                }
-                int c = corner_count(case_id == OG_CASE_SPHERE_SOLID ? phi_sphere_quarter : phi_star, mn, mx, 0.0f);
-                ty = (c == 8) ? OG_NEUMANN : OG_INTERIOR;
-            }
-            CT(g, t)[v] = ty;
-        }
+        leaf_cell_types_at(voxel_size(g, g->t[t].level), g->t[t].c, case_id, CT(g, t));
     }
+}
+/* exported for the reference pin: leaf cell types of the tile (level, i, j, k) */
+void og_case_types_at(float h0, int case_id, int level, int i, int j, int k, uint8_t* out512) {
+    int tc[3] = {i, j, k};
+    leaf_cell_types_at(h0 / (float)(1 << level), tc, case_id, out512);
 }
 
 /* ------------------------------------------------------------------ */
@@ -443,6 +478,8 @@ static void ghost_types_from_parents(og_grid* g) { /* AMGSolver.cu:265-274, Mesh
     }
 }
 
+void og_set_reference_mask(og_grid* g, int on) { g->ref_mask = on; }
+
 /* PrepareLaplacianSystemFromLeafAndGhostCellTypesAndFaceCoeffs (AMGSolver.cu:89-254) */
 void og_prepare_system(og_grid* g, int coeff_ch, float R) {
     /* 1. coarse face coefficient += R * sum of the 4 fine faces, fine levels first
@@ -450,7 +487,9 @@ void og_prepare_system(og_grid* g, int coeff_ch, float R) {
      *    of the fine level takes part (a NONLEAF tile counts as a LEAF of the
      *    subtree cut at its level).  The cell-type mask the reference applies
      *    admits every valid type; NONLEAF cell types are only computed in step 2,
-     *    so the mask is taken as open here. */
+     *    so the mask is taken as open here.  og_set_reference_mask(g, 1) applies
+     *    the mask to whatever types the grid holds at this point instead (the
+     *    reference reads NONLEAF types there before any write). */
     for (int L = g->max_level; L > 0; L--) {
         for (int t = 0; t < g->n; t++) {
             if (g->t[t].level != L) continue;
@@ -465,7 +504,13 @@ void og_prepare_system(og_grid* g, int coeff_ch, float R) {
                         for (int kk = 0; kk < 2; kk++) {
                             int o[3];
                             o[axis] = 0; o[(axis + 1) % 3] = jj; o[(axis + 2) % 3] = kk; /* rotateCoord, HAAccessor.h:25 */
-                            sum += CH(g, coeff_ch + axis, t)[CELL(fl[0] + o[0], fl[1] + o[1], fl[2] + o[2])];
+                            int fv = CELL(fl[0] + o[0], fl[1] + o[1], fl[2] + o[2]);
+                            /* the reference masks by the fine cell's stored type
+                             * (INTERIOR | DIRICHLET | NEUMANN); with ref_mask off the
+                             * mask is open, see the comment above */
+                            float fc = CH(g, coeff_ch + axis, t)[fv];
+                            if (g->ref_mask && !(CT(g, t)[fv] & (OG_INTERIOR | OG_DIRICHLET | OG_NEUMANN))) fc = 0.0f;
+                            sum += fc;
                         }
                     float* cc = &CH(g, coeff_ch + axis, p)[cv];
                     *cc = fmaf(sum, R, *cc);
@@ -592,14 +637,16 @@ static float face_fluid_ratio(const float phi[4]) {
         double t0 = 0.5 * (double)frac_inside(phi[f0], phi[(f0 + 3) & 3]) * (double)frac_inside(phi[f0], phi[(f0 + 1) & 3]);
         double t1 = 0.5 * (double)frac_inside(phi[f1], phi[(f1 + 3) & 3]) * (double)frac_inside(phi[f1], phi[(f1 + 1) & 3]);
         ret = (float)(t0 + t1);
-    } else { /* two adjacent solid corners: a trapezoid from the two crossing edges */
-        double s = 0;
+    } else { /* two adjacent solid corners: a trapezoid from the two crossing edges,
+              * summed in float as the reference does (the sign of a zero result follows) */
+        float e[2] = {0.0f, 0.0f};
+        int ne = 0;
         for (int i = 0; i < 4; i++) {
             if (in[i]) continue;
             int nb = in[(i + 1) & 3] ? ((i + 1) & 3) : ((i + 3) & 3);
-            s += (double)frac_inside(phi[i], phi[nb]);
+            e[ne++] = frac_inside(phi[i], phi[nb]);
         }
-        ret = (float)(0.5 * s);
+        ret = (float)(0.5 * (double)(e[0] + e[1]));
     }
     if (ret < 0.1f && ret != 0.0f) ret = 0.1f;
     return ret;
@@ -618,23 +665,44 @@ static float node_sdf(const og_grid* g, int t, int li, int lj, int lk, int ns, c
     float h = voxel_size(g, T->level);
     return sdf_spheres((float)(T->c[0] * 8 + li) * h, (float)(T->c[1] * 8 + lj) * h, (float)(T->c[2] * 8 + lk) * h, ns, s);
 }
+/* node SDF of a tile: 9^3 nodes, node (i, j, k) at i*81 + j*9 + k (PoissonTile.h:72) */
+static void tile_node_sdf(const og_grid* g, int t, int ns, const float* s, float* nodes) {
+    for (int i = 0; i < 9; i++)
+        for (int j = 0; j < 9; j++)
+            for (int k = 0; k < 9; k++) nodes[i * 81 + j * 9 + k] = node_sdf(g, t, i, j, k, ns, s);
+}
+/* CellCornerSDFInsideCount (MeshCutCell.cu:239-260): corners of cell (li, lj, lk) below iso */
+static int cell_corner_inside_count(const float* nodes, int li, int lj, int lk, float iso) {
+    int cnt = 0;
+    for (int d = 0; d < 8; d++)
+        if (nodes[(li + (d >> 2)) * 81 + (lj + ((d >> 1) & 1)) * 9 + (lk + (d & 1))] - iso < 0) cnt++;
+    return cnt;
+}
+/* exported for the reference pin */
+float og_frac_inside(float a, float b) { return frac_inside(a, b); }
+void og_face_fluid_ratio(const float* phi4, int n, float* out) {
+    for (int i = 0; i < n; i++) out[i] = face_fluid_ratio(phi4 + 4 * i);
+}
+void og_cell_corner_inside_count(const float* nodes729, float iso, int* out512) {
+    for (int v = 0; v < NC; v++) out512[v] = cell_corner_inside_count(nodes729, v >> 6, (v >> 3) & 7, v & 7, iso);
+}
 /* CreateAMGLaplacianSystemWithSolidCutOnNodeSDF (MeshCutCell.cu:416-543) with
  * the node SDF of a union of spheres evaluated analytically at tile nodes. */
 void og_cutcell_sphere_coeffs(og_grid* g, int coeff_ch, float R, int ns, const float* s) {
     for (int t = 0; t < g->n; t++) {
         if (!(g->t[t].type & OG_LEAF)) continue;
         float eps = voxel_size(g, g->t[t].level) * 1e-3f; /* SDF_REL_EPS, MeshCutCell.h:8 */
-        for (int v = 0; v < NC; v++) {
-            int l[3] = {v >> 6, (v >> 3) & 7, v & 7}, cnt = 0;
-            for (int d = 0; d < 8; d++)
-                if (node_sdf(g, t, l[0] + (d >> 2), l[1] + ((d >> 1) & 1), l[2] + (d & 1), ns, s) - eps < 0) cnt++;
-            if (cnt == 8) CT(g, t)[v] = OG_NEUMANN;
-        }
+        float nodes[729];
+        tile_node_sdf(g, t, ns, s, nodes);
+        for (int v = 0; v < NC; v++)
+            if (cell_corner_inside_count(nodes, v >> 6, (v >> 3) & 7, v & 7, eps) == 8) CT(g, t)[v] = OG_NEUMANN;
     }
     ghost_types_from_parents(g);
     for (int t = 0; t < g->n; t++) {
         int tt0 = g->t[t].type;
         float h = voxel_size(g, g->t[t].level);
+        float nodes[729];
+        if (tt0 != OG_NONLEAF) tile_node_sdf(g, t, ns, s, nodes);
         for (int v = 0; v < NC; v++) {
             int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
             for (int axis = 0; axis < 3; axis++) {
@@ -651,7 +719,7 @@ void og_cutcell_sphere_coeffs(og_grid* g, int coeff_ch, float R, int ns, const f
                             {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0}}};
                         float phi[4];
                         for (int q4 = 0; q4 < 4; q4++)
-                            phi[q4] = node_sdf(g, t, l[0] + cyc[axis][q4][0], l[1] + cyc[axis][q4][1], l[2] + cyc[axis][q4][2], ns, s);
+                            phi[q4] = nodes[(l[0] + cyc[axis][q4][0]) * 81 + (l[1] + cyc[axis][q4][1]) * 9 + (l[2] + cyc[axis][q4][2])];
                         c = -(h * face_fluid_ratio(phi));
                     }
                 }
@@ -819,7 +887,9 @@ static void gs_pass(og_grid* g, int level, int color, int x_ch, int coeff_ch, in
                 float D = S->d[v];
                 float delta = (ct & OG_INTERIOR) ? (B[v] - Ax) / D : 0.0f;
                 float xs = S->x[SX(i, j, k)];
-                X[v] = exact ? fmaf(delta, om, xs) : (float)((double)xs + (double)delta * omega);
+                /* AMGSolver.cu:874: x + delta * omega with omega a double holding a float: the
+                 * product is exact in double, the sum rounds to double, then to float */
+                X[v] = exact ? (float)fma((double)delta, (double)om, (double)xs) : (float)((double)xs + (double)delta * omega);
             }
         }
         free(S);

@@ -52,6 +52,8 @@ void og_grid_free(og_grid* g);
 int og_set_tile(og_grid* g, int level, int i, int j, int k, int type);
 int og_rebuild(og_grid* g);
 int og_refine_case(og_grid* g, int case_id, const double* params, int nparams);
+typedef int (*og_target_fn)(void* user, int level, int i, int j, int k);
+int og_refine_fn(og_grid* g, og_target_fn fn, void* user);
 int og_num_tiles(const og_grid* g);
 int og_max_level(const og_grid* g);
 void og_get_tiles(const og_grid* g, int* level, int* ijk, uint8_t* type);
@@ -97,6 +99,18 @@ int og_assemble_count(og_grid* g, int coeff_ch, int* n_rows, long long* nnz);
 int og_assemble(og_grid* g, int coeff_ch, long long* rowptr, int* col, double* val, int* row_tile, int* row_cell);
 int og_csr_solve(int n, const long long* rowptr, const int* col, const double* val, const double* b, double* x, double tol, int max_iters, int method, int* iters_out, double* rel_out);
 int og_csr_matvec(int n, const long long* rowptr, const int* col, const double* val, const double* x, double* y);
+
+/* pieces exported so that tests can compare them with the reference's own
+ * host-compiled functions (oracle/_ref, built by oracle/build_ref.py) */
+float og_frac_inside(float a, float b);
+void og_face_fluid_ratio(const float* phi4, int n, float* out);
+void og_cell_corner_inside_count(const float* nodes729, float iso, int* out512);
+int og_case_target_at(float h0, int case_id, const double* params, int nparams, int level, int i, int j, int k);
+void og_case_types_at(float h0, int case_id, int level, int i, int j, int k, uint8_t* out512);
+/* 1: coarsen off-diagonals under the reference's cell-type mask applied to the
+ * types the grid holds at that point (NONLEAF types included); 0 (default):
+ * the mask is open */
+void og_set_reference_mask(og_grid* g, int on);
 
 #ifdef __cplusplus
 }

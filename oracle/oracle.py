@@ -19,6 +19,8 @@ CASE_UNIFORM, CASE_CENTER_POINT, CASE_SPHERE_EMPTY, CASE_SPHERE_SOLID = 0, 1, 2,
 CASE_STAR_EMPTY, CASE_STAR_SOLID, CASE_SHELL, CASE_MULTI_SPHERE = 4, 5, 6, 7
 GMG, CMG = 1, 2
 
+TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
+
 _lib = None
 
 
@@ -73,6 +75,13 @@ def lib():
             "og_assemble": (I, [P, I, P, P, P, P, P]),
             "og_csr_solve": (I, [I, P, P, P, P, P, D, I, I, P, P]),
             "og_csr_matvec": (I, [I, P, P, P, P, P]),
+            "og_frac_inside": (F, [F, F]),
+            "og_face_fluid_ratio": (None, [P, I, P]),
+            "og_cell_corner_inside_count": (None, [P, F, P]),
+            "og_case_target_at": (I, [F, I, P, I, I, I, I, I]),
+            "og_case_types_at": (None, [F, I, I, I, I, I, P]),
+            "og_set_reference_mask": (None, [P, I]),
+            "og_refine_fn": (I, [P, TARGET_FN, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -110,6 +119,14 @@ class Grid:
     def refine_case(self, case_id, params):
         prm = np.asarray(params, dtype=np.float64)
         return self.L.og_refine_case(self.g, case_id, _p(prm), len(prm))
+
+    def iterative_refine(self, level_target):
+        """level_target(level, i, j, k) -> target level of that tile (HADeviceGrid::iterativeRefine)."""
+        cb = TARGET_FN(lambda user, level, i, j, k: int(level_target(level, i, j, k)))
+        return self.L.og_refine_fn(self.g, cb, None)
+
+    def set_reference_mask(self, on):
+        self.L.og_set_reference_mask(self.g, int(bool(on)))
 
     @property
     def n(self):
@@ -259,3 +276,32 @@ def csr_matvec(rp, ci, va, x):
     y = np.zeros(n, np.float64)
     lib().og_csr_matvec(n, _p(rp), _p(ci), _p(va), _p(x), _p(y))
     return y
+
+
+def frac_inside(a, b):
+    return lib().og_frac_inside(a, b)
+
+
+def face_fluid_ratio(phi4):
+    phi4 = np.ascontiguousarray(phi4, np.float32).reshape(-1, 4)
+    out = np.zeros(len(phi4), np.float32)
+    lib().og_face_fluid_ratio(_p(phi4), len(phi4), _p(out))
+    return out
+
+
+def cell_corner_inside_count(nodes729, iso):
+    nodes = np.ascontiguousarray(nodes729, np.float32).reshape(729)
+    out = np.zeros(512, np.int32)
+    lib().og_cell_corner_inside_count(_p(nodes), iso, _p(out))
+    return out
+
+
+def case_target_at(h0, case_id, params, level, ijk):
+    prm = np.asarray(params, dtype=np.float64)
+    return lib().og_case_target_at(h0, case_id, _p(prm), len(prm), level, int(ijk[0]), int(ijk[1]), int(ijk[2]))
+
+
+def case_types_at(h0, case_id, level, ijk):
+    out = np.zeros(512, np.uint8)
+    lib().og_case_types_at(h0, case_id, level, int(ijk[0]), int(ijk[1]), int(ijk[2]), _p(out))
+    return out

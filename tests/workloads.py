@@ -17,6 +17,13 @@ COEFF = 6  # coefficient channels 6..9 (the reference tests use 6, SolverTests.c
 U = 10     # face-velocity channels 10..12
 
 
+def same_bits(a, b):
+    """Bitwise equality of float arrays (np.array_equal treats -0.0 and 0.0 as equal)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def fourier_modes(seed, n=16):
     rng = np.random.default_rng(seed)
     k = rng.integers(1, 9, size=(n, 3)).astype(np.float64)
