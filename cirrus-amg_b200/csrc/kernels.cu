@@ -820,8 +820,9 @@ __global__ void k_face_coeffs(DevGrid g, int t0, int coeff_ch, int ns, const flo
         const int stride[3] = {64, 8, 1};
         const int c0 = g.ctype[(size_t)t * kCells + v];
         for (int a = 0; a < 3; ++a) {
-            float c = 0.0f;
+            float c = 0.0f;  // NONLEAF: 0 (src/AMGSolver.cu:287, MeshCutCell.cu:463)
             if (tt0 != dNonLeaf) {
+                c = -0.0f;  // LEAF/GHOST: -coeff with coeff = 0 unless the face is valid (:312)
                 int q = t, nv = v - stride[a];
                 if (l[a] == 0) {
                     q = g.nb[8 * t + a];

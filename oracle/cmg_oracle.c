@@ -706,8 +706,9 @@ void og_cutcell_sphere_coeffs(og_grid* g, int coeff_ch, float R, int ns, const f
         for (int v = 0; v < NC; v++) {
             int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
             for (int axis = 0; axis < 3; axis++) {
-                float c = 0;
+                float c = 0; /* NONLEAF: 0 (MeshCutCell.cu:463) */
                 if (tt0 != OG_NONLEAF) {
+                    c = -0.0f; /* LEAF/GHOST: -coeff, coeff = 0 on an invalid face (MeshCutCell.cu:535) */
                     int nv, q = nb_cell(g, t, v, axis, -1, &nv);
                     int tt1 = (q < 0) ? tt0 : g->t[q].type;
                     int ct1 = (q < 0) ? OG_DIRICHLET : CT(g, q)[nv];
