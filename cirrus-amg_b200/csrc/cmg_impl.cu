@@ -805,6 +805,10 @@ int Solver::solve_finish(bool verbose, int* iters, double* rel) {
         set_error("solve: grid barrier of the persistent multigrid kernel timed out");
         return 2;
     }
+    if (gs_pipe_take_error()) {
+        set_error("solve: a smoothing sweep timed out waiting for its tile copies");
+        return 2;
+    }
     if (r.nonfinite) {
         set_error("solve: non-finite value in a PCG reduction");
         return 5;

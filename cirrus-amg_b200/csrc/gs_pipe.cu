@@ -4,9 +4,14 @@
 //
 // k_gs spends most of a tile's life waiting: the neighbour descriptors arrive, then
 // the halo loads go out, then the block computes.  Here each 128-thread block walks a
-// strided list of tiles and keeps the next tile's planes and halo in flight (cp.async
-// into a second shared-memory stage) while it computes the current one.  No register
-// holds data in flight and nothing spins: cp.async.wait_group is the only wait.
+// strided list of tiles and keeps the next tile's planes and halo in flight (into a
+// second shared-memory stage) while it computes the current one.  A tile's own data are
+// seven contiguous blocks (x, rhs, the four operator planes, the cell types: 2 KB, or
+// 1 KB for a 16-bit plane, and 512 B): one thread moves them with 1-D bulk copies
+// (cp.async.bulk, the TMA engine) that complete on the stage's mbarrier; the halo words
+// are scattered and keep per-thread cp.async.  No register holds data in flight.  The
+// mbarrier waits are bounded: a wait that gives up sets an error flag that the solve
+// reports, and the block stops.
 //
 // Halo values are read without the neighbour's cell types.  That relies on the
 // multigrid x plane holding 0 on every cell that is not INTERIOR, which the cycle keeps
@@ -22,6 +27,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <cstddef>
 #include <type_traits>
 
 #include "kernels.hpp"
@@ -31,7 +37,7 @@ namespace cmg {
 namespace {
 
 template <typename CT>
-struct PipeStage {
+struct alignas(16) PipeStage {
     float x[512], b[512];
     CT d[512];        // diagonal
     CT c0[512];       // -x faces
@@ -44,6 +50,14 @@ struct PipeStage {
     float hx[384];    // halo x of the six faces, [axis][side][a][b]
     unsigned ty[128];
 };
+// bulk-copy destinations: 16-byte aligned offsets
+template <typename CT>
+constexpr bool stage_aligned() {
+    return offsetof(PipeStage<CT>, b) % 16 == 0 && offsetof(PipeStage<CT>, d) % 16 == 0 && offsetof(PipeStage<CT>, c0) % 16 == 0 &&
+           offsetof(PipeStage<CT>, c1) % 16 == 0 && offsetof(PipeStage<CT>, c2) % 16 == 0 && offsetof(PipeStage<CT>, ty) % 16 == 0 &&
+           sizeof(PipeStage<CT>) % 16 == 0;
+}
+static_assert(stage_aligned<float>() && stage_aligned<__nv_bfloat16>() && stage_aligned<__half>(), "stage layout");
 // The snapshot: masked x of the tile with its one-cell halo, split into four planes by
 // k mod 4 (k = 4h + u: u the plane, h = -1..2 the slot), rows j of 4 slots, layers i of
 // 42 floats, planes of 448 floats.  A warp's threads own (i0..i0+1, j 0..7, h 0..1) and
@@ -65,19 +79,38 @@ struct PipeSmemR {
     float res[512];
 };
 
-__device__ __forceinline__ void cp16(void* dst, const void* src) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp8(void* dst, const void* src) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
-}
 __device__ __forceinline__ void cp4(void* dst, const void* src) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// 1-D bulk copies onto an mbarrier (both addresses 16-byte aligned, sizes multiples of 16)
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned mb) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned mb, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned mb) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(mb) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned mb, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(ok) : "r"(mb), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait for phase `parity` of an mbarrier (each try_wait suspends for a while)
+constexpr int kMbarTries = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned parity) {
+    for (int i = 0; i < kMbarTries; ++i)
+        if (mbar_try(mb, parity)) return true;
+    return false;
+}
+__device__ int g_pipe_error;  // set when a stage's bulk copies did not arrive in time
 __device__ __forceinline__ void cp_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
@@ -86,7 +119,6 @@ template <typename CT>
 struct Coef;
 template <>
 struct Coef<float> {
-    __device__ static void cp_quad(float* dst, const float* src) { cp16(dst, src); }
     __device__ static void cp_face(unsigned* dst, const float* plane, size_t o) { cp4(dst, plane + o); }
     __device__ static unsigned word(float v) { return __float_as_uint(v); }
     __device__ static float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -96,7 +128,6 @@ struct Coef<float> {
 // 16-bit storage: 4 elements move as 8 bytes; a face element moves inside its aligned pair
 template <typename CT>
 struct Coef16 {
-    __device__ static void cp_quad(CT* dst, const CT* src) { cp8(dst, src); }
     __device__ static void cp_face(unsigned* dst, const CT* plane, size_t o) { cp4(dst, plane + (o & ~(size_t)1)); }
     __device__ static float4 ld4(const CT* p) {
         const uint2 w = *reinterpret_cast<const uint2*>(p);
@@ -138,18 +169,24 @@ __device__ __forceinline__ void load_desc(const DevGrid& g, int t, int side, int
     for (int r = 0; r < 3; ++r) d[r] = __ldg(g.nbx + 8 * t + r + 3 * side);
 }
 
-// start the copies of tile t into stage S
+// start the copies of tile t into stage S (mbarrier mb takes the bulk part)
 template <typename CT>
-__device__ __forceinline__ void issue(PipeStage<CT>& S, const DevGrid& g, int t, const float* X, const float* B, const CT* C0,
-                                      const CT* C1, const CT* C2, const CT* C3, const int d[3], int q, float h) {
-    const size_t base = (size_t)t * kCells + 4 * q;
-    cp16(&S.x[4 * q], X + base);
-    cp16(&S.b[4 * q], B + base);
-    Coef<CT>::cp_quad(&S.d[4 * q], C3 + base);
-    Coef<CT>::cp_quad(&S.c0[4 * q], C0 + base);
-    Coef<CT>::cp_quad(&S.c1[4 * q], C1 + base);
-    Coef<CT>::cp_quad(&S.c2[4 * q], C2 + base);
-    cp4(&S.ty[q], g.ctype + base);
+__device__ __forceinline__ void issue(PipeStage<CT>& S, unsigned mb, const DevGrid& g, int t, const float* X, const float* B,
+                                      const CT* C0, const CT* C1, const CT* C2, const CT* C3, const int d[3], int q, float h) {
+    const size_t tb = (size_t)t * kCells;
+    if (q == 0) {
+        constexpr unsigned kF = kCells * sizeof(float), kC = kCells * sizeof(CT), kT = kCells;
+        // the stage was last read through ordinary loads; order them before the async writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect(mb, 2 * kF + 4 * kC + kT);
+        bulk_g2s(S.x, X + tb, kF, mb);
+        bulk_g2s(S.b, B + tb, kF, mb);
+        bulk_g2s(S.d, C3 + tb, kC, mb);
+        bulk_g2s(S.c0, C0 + tb, kC, mb);
+        bulk_g2s(S.c1, C1 + tb, kC, mb);
+        bulk_g2s(S.c2, C2 + tb, kC, mb);
+        bulk_g2s(S.ty, g.ctype + tb, kT, mb);
+    }
     const int side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
     const int e = side ? 0 : 7;  // the neighbour's cell next to the shared face
     const int nl[3] = {cell_index(e, fa, fb), cell_index(fa, e, fb), cell_index(fa, fb, e)};
@@ -335,13 +372,21 @@ __device__ __forceinline__ void process_restrict(const PipeStage<float>& S, floa
 // MODE 0: one red-black colour pass; MODE 1: residual and restriction into the parents
 template <typename CT, int MODE, bool kExact = true>
 __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const float* B, PipeArgs A) {
-    extern __shared__ __align__(16) unsigned char pipe_smem[];
+    extern __shared__ __align__(128) unsigned char pipe_smem[];
+    __shared__ __align__(8) unsigned long long mbar[2];
     using Smem = typename std::conditional<MODE == 0, PipeSmem<CT>, PipeSmemR>::type;
     Smem& sm = *reinterpret_cast<Smem*>(pipe_smem);
     const int q = threadIdx.x, side = q >> 6;
     const int stride = gridDim.x, tend = A.t0 + A.nt;
     int tcur = A.t0 + blockIdx.x;
     if (tcur >= tend) return;
+    const unsigned mb0 = smem_addr(&mbar[0]);  // stage s: mb0 + 8 s
+    if (q == 0) {
+        mbar_init(mb0);
+        mbar_init(mb0 + 8);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
     const CT* C0 = static_cast<const CT*>(A.coef);
     const CT* C1 = C0 + A.cstride;
     const CT* C2 = C1 + A.cstride;
@@ -351,16 +396,24 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const f
     load_desc(g, tcur, side, dcur);
     int tnext = tcur + stride;
     if (tnext < tend) load_desc(g, tnext, side, dnext);
-    issue(sm.st[0], g, tcur, X, B, C0, C1, C2, C3, dcur, q, h);
+    issue(sm.st[0], mb0, g, tcur, X, B, C0, C1, C2, C3, dcur, q, h);
+    bool pending_other = false;  // bulk copies in flight into the other stage
     for (int k = 0;; ++k) {
         const int s = k & 1;
-        if (tnext < tend) issue(sm.st[s ^ 1], g, tnext, X, B, C0, C1, C2, C3, dnext, q, h);
+        pending_other = tnext < tend;
+        if (pending_other) issue(sm.st[s ^ 1], mb0 + 8 * (s ^ 1), g, tnext, X, B, C0, C1, C2, C3, dnext, q, h);
         else cp_commit();
         const int tn2 = tnext + stride;
         int dn2[3] = {0, 0, 0};
         if (tn2 < tend) load_desc(g, tn2, side, dn2);
         cp_wait_prev();
-        __syncthreads();
+        // stage s is the (k >> 1)-th use of its mbarrier
+        const bool ok = mbar_wait(mb0 + 8 * s, (unsigned)(k >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (q == 0) atomicExch(&g_pipe_error, 1);
+            if (pending_other) mbar_wait(mb0 + 8 * (s ^ 1), (unsigned)((k + 1) >> 1) & 1u);
+            break;
+        }
         if constexpr (MODE == 0)
             process<CT, kExact>(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
         else
@@ -403,6 +456,13 @@ void launch_pass(int blocks, cudaStream_t st, const DevGrid& g, float* X, const 
 int g_restrict_blocks = 0;  // resident blocks of the restriction pass
 
 }  // namespace
+
+int gs_pipe_take_error() {
+    int v = 0, z = 0;
+    if (cudaMemcpyFromSymbol(&v, g_pipe_error, sizeof(int)) != cudaSuccess) return -1;
+    if (v) cudaMemcpyToSymbol(g_pipe_error, &z, sizeof(int));
+    return v;
+}
 
 int gs_pipe_init() {
     if (!set_pipe_smem<float>() || !set_pipe_smem<__nv_bfloat16>() || !set_pipe_smem<__half>()) return 0;

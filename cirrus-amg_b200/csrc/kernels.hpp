@@ -43,6 +43,8 @@ void launch_accumulate_cells(const DevGrid& g, int t0, int nt, int types, const 
 // persistent, software-pipelined colour pass for the multigrid cycle (gs_pipe.cu); needs the
 // x plane masked to INTERIOR cells.  gs_pipe_init: resident blocks on the device (0: unusable).
 int gs_pipe_init();
+// 1 if a pipelined sweep gave up waiting for its bulk copies since the last call (then cleared)
+int gs_pipe_take_error();
 // Storage of the operator planes the pipelined smoother reads: the float channels, or a
 // BF16 / FP16 copy (coeff16: four planes of num_tiles*512 elements, made by launch_coeff16).
 constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;
