@@ -576,12 +576,18 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
 
-    # the mixed-precision preconditioner (16-bit operator storage in the smoothing sweeps),
-    # timed the same way on the same solve, against the FP32 solution above
+    # the mixed-precision preconditioner, timed the same way on the same solve, against the
+    # FP32 solution above: 16-bit operator storage in the smoothing sweeps; the FP64 direct
+    # coarsest solve alone (timed against the reference's coarsest sweeps); and the whole
+    # mixed mode (BF16 storage, FP64 true residual every 10 iterations, direct coarsest)
     x32 = G.download(0)
     mixed, mixed_x = {}, {"fp32": x32}
-    for mode in ("bf16", "fp16"):
-        S.set_storage(mode)
+    mixed_modes = {"bf16": ("bf16", 0, False), "fp16": ("fp16", 0, False), "fp32_direct_coarsest": ("fp32", 0, True),
+                   "bf16_replace10_direct_coarsest": ("bf16", 10, True)}
+    for mode, (storage, every, direct) in mixed_modes.items():
+        S.set_storage(storage)
+        S.set_residual_replacement(every)
+        S.set_coarsest_direct(direct)
         for _ in range(3):
             one_solve()
         torch.cuda.synchronize()
@@ -595,10 +601,12 @@ def run_ours(args, rank, world, local_rank):
         mixed_x[mode] = xm
         lm = ty == cmg.LEAF
         mixed[mode] = {"ms": round(replica_time(m0.elapsed_time(m1), world, dev) / args.steps, 4), "pcg_iters": it_m,
-                       "rel_residual_recurrence": rel_m,
+                       "rel_residual_recurrence": rel_m, "residual_replacements": S.last_replacements(),
                        "rel_l2_vs_fp32_solution": float(np.linalg.norm((xm - x32)[lm].astype(np.float64)) /
                                                         np.linalg.norm(x32[lm].astype(np.float64)))}
     S.set_storage("fp32")
+    S.set_residual_replacement(0)
+    S.set_coarsest_direct(False)
     one_solve()
     torch.cuda.synchronize()
 

@@ -53,6 +53,7 @@ EXPORTS = [
     "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
     "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned",
     "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
+    "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -146,6 +147,9 @@ def lib():
             "cmg_learned_set_inference": (I, [I]),
             "cmg_amg_solver_autotune": (I, [P, P, I, P, I, D, I, P, P, P]),
             "cmg_amg_solver_set_finest_iters": (I, [P, I]),
+            "cmg_amg_solver_set_residual_replacement": (I, [P, I]),
+            "cmg_amg_solver_set_coarsest_direct": (I, [P, I]),
+            "cmg_amg_solver_residual_replacements": (I, [P, ctypes.POINTER(I)]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
         }
@@ -426,6 +430,21 @@ class AMGSolver:
         pipeline: the cycle's smoothing sweeps as a persistent kernel that prefetches the next tile."""
         flags = (1 if use_graph else 0) | (2 if persistent else 0) | (0 if cluster else 4) | (0 if pipeline else 8)
         _check(self.L.cmg_amg_solver_set_launch_mode(self.h, flags), "set_launch_mode")
+
+    def set_residual_replacement(self, every):
+        """Replace the recurrence residual by b - A x (stencil in FP64) every `every` PCG
+        iterations; 0 (default) never, as the reference."""
+        _check(self.L.cmg_amg_solver_set_residual_replacement(self.h, int(every)), "set_residual_replacement")
+
+    def set_coarsest_direct(self, on=True):
+        """Level 0 solved exactly (FP64 Cholesky-based inverse) when the cluster step runs
+        levels 0-2, instead of the reference's coarsest sweeps."""
+        _check(self.L.cmg_amg_solver_set_coarsest_direct(self.h, int(bool(on))), "set_coarsest_direct")
+
+    def last_replacements(self):
+        n = ctypes.c_int(0)
+        _check(self.L.cmg_amg_solver_residual_replacements(self.h, ctypes.byref(n)), "residual_replacements")
+        return n.value
 
     def set_storage(self, storage):
         """Operator storage of the mu-cycle's smoothing sweeps: "fp32" (default, the

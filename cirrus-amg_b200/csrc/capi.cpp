@@ -416,6 +416,21 @@ int cmg_amg_solver_set_finest_iters(cmg_amg_solver* s, int finest_iters) {
     s->s.finest_iters = finest_iters;
     return CMG_OK;
 }
+int cmg_amg_solver_set_residual_replacement(cmg_amg_solver* s, int every) {
+    if (!s || every < 0 || every > 1000) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_residual_replacement: bad argument (0..1000)");
+    s->s.replace_every = every;
+    return CMG_OK;
+}
+int cmg_amg_solver_set_coarsest_direct(cmg_amg_solver* s, int on) {
+    if (!s) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_coarsest_direct: null solver");
+    s->s.coarsest_direct = on != 0;
+    return CMG_OK;
+}
+int cmg_amg_solver_residual_replacements(cmg_amg_solver* s, int* count) {
+    if (!s || !count) return fail(CMG_ERR_INVALID, "cmg_amg_solver_residual_replacements: bad argument");
+    *count = s->s.last_replaced;
+    return CMG_OK;
+}
 int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const cmg_tune_candidate* c, int max_iters, double tol, int repeats,
                             float* ms, int* iters, int* best) {
     GUARD_BEGIN

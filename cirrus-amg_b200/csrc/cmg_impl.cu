@@ -219,6 +219,8 @@ Solver::~Solver() {
     dfree(lnet.bias);
     dfree(aux);
     dfree(bsave);
+    dfree(bkeep);
+    dfree(root_inv);
     if (h_s) cudaFreeHost(h_s);
     if (h_bar) cudaFreeHost(h_bar);
     dfree(bar);
@@ -362,6 +364,101 @@ int Solver::ensure_aux(const Grid& G) {
     return 0;
 }
 
+int Solver::ensure_bkeep(const Grid& G) {
+    const size_t need = (size_t)G.n * kCells;
+    if (bkeep_cap >= need) return 0;
+    dfree(bkeep);
+    bkeep = nullptr;
+    bkeep_cap = 0;
+    CK(cudaMalloc(&bkeep, sizeof(float) * need));
+    bkeep_cap = need;
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);  // captured graphs hold the old pointer
+    graphs.clear();
+    return 0;
+}
+
+// The coarsest operator (the root tile, level 0: no neighbours, so every face outside it
+// is a Dirichlet face with x = 0) on its INTERIOR cells, A[v][v] = diagonal and A[v][u] =
+// the face coefficient between u and v, factorised A = L L^T in double and inverted as
+// L^-T L^-1; the inverse goes to the device in the coarse CTA's thread order.  Rebuilt only
+// when the root's operator changed since the last solve.
+int Solver::prepare_root_inverse(Grid& G) {
+    std::vector<float> ops((size_t)5 * kCells);
+    for (int a = 0; a < 4; ++a)
+        CK(cudaMemcpyAsync(&ops[(size_t)a * kCells], G.plane(coeff_ch + a), sizeof(float) * kCells, cudaMemcpyDeviceToHost, G.stream));
+    std::vector<uint8_t> ty(kCells);
+    CK(cudaMemcpyAsync(ty.data(), G.ctype, kCells, cudaMemcpyDeviceToHost, G.stream));
+    CK(cudaStreamSynchronize(G.stream));
+    for (int v = 0; v < kCells; ++v) ops[(size_t)4 * kCells + v] = (float)ty[v];
+    if (root_inv && ops == root_ops) return 0;
+    std::vector<int> idx(kCells, -1), cell;
+    for (int v = 0; v < kCells; ++v)
+        if (ty[v] == kInterior) {
+            idx[v] = (int)cell.size();
+            cell.push_back(v);
+        }
+    const int m = (int)cell.size();
+    std::vector<double> A((size_t)m * m, 0.0);
+    for (int r = 0; r < m; ++r) {
+        const int v = cell[r];
+        A[(size_t)r * m + r] = ops[(size_t)3 * kCells + v];
+        const int l[3] = {v >> 6, (v >> 3) & 7, v & 7};
+        for (int a = 0; a < 3; ++a) {
+            const int stride = a == 0 ? 64 : a == 1 ? 8 : 1;
+            if (l[a] > 0 && idx[v - stride] >= 0) A[(size_t)r * m + idx[v - stride]] = ops[(size_t)a * kCells + v];               // -face of v
+            if (l[a] < 7 && idx[v + stride] >= 0) A[(size_t)r * m + idx[v + stride]] = ops[(size_t)a * kCells + v + stride];  // -face of the upper cell
+        }
+    }
+    // A = L L^T (lower triangle of A, in place)
+    for (int j = 0; j < m; ++j) {
+        double d = A[(size_t)j * m + j];
+        for (int k = 0; k < j; ++k) d -= A[(size_t)j * m + k] * A[(size_t)j * m + k];
+        if (!(d > 0.0)) {
+            set_error("coarsest direct solve: the root operator is not positive definite");
+            return 5;
+        }
+        const double ljj = std::sqrt(d);
+        A[(size_t)j * m + j] = ljj;
+        for (int i = j + 1; i < m; ++i) {
+            double sum = A[(size_t)i * m + j];
+            for (int k = 0; k < j; ++k) sum -= A[(size_t)i * m + k] * A[(size_t)j * m + k];
+            A[(size_t)i * m + j] = sum / ljj;
+        }
+    }
+    // W = L^-1 (lower triangular), then A^-1 = W^T W
+    std::vector<double> W((size_t)m * m, 0.0);
+    for (int c = 0; c < m; ++c)
+        for (int i = c; i < m; ++i) {
+            double sum = i == c ? 1.0 : 0.0;
+            for (int k = c; k < i; ++k) sum -= A[(size_t)i * m + k] * W[(size_t)k * m + c];
+            W[(size_t)i * m + c] = sum / A[(size_t)i * m + i];
+        }
+    std::vector<double> inv((size_t)m * m, 0.0);
+    for (int r = 0; r < m; ++r)
+        for (int c = 0; c <= r; ++c) {
+            double sum = 0.0;
+            for (int k = r; k < m; ++k) sum += W[(size_t)k * m + r] * W[(size_t)k * m + c];
+            inv[(size_t)r * m + c] = inv[(size_t)c * m + r] = sum;
+        }
+    std::vector<double> M((size_t)kCells * kCells, 0.0);
+    for (int j = 0; j < kCells; ++j) {
+        const int rj = idx[cluster_thread_cell(j)];
+        if (rj < 0) continue;
+        for (int t = 0; t < kCells; ++t) {
+            const int rt = idx[cluster_thread_cell(t)];
+            if (rt >= 0) M[(size_t)j * kCells + t] = inv[(size_t)rj * m + rt];
+        }
+    }
+    if (!root_inv) {
+        CK(cudaMalloc(&root_inv, sizeof(double) * M.size()));
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);  // captured graphs hold the old pointer
+        graphs.clear();
+    }
+    CK(cudaMemcpy(root_inv, M.data(), sizeof(double) * M.size(), cudaMemcpyHostToDevice));
+    root_ops.swap(ops);
+    return 0;
+}
+
 int Solver::ensure_coeff16(const Grid& G) {
     if (storage == kStorageFP32 || kind != kAMG) return 0;
     const size_t need = coeff16_bytes(G.dev());
@@ -392,7 +489,7 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st, b
         int tile1[8], tile2[64];
         coarse_tiles(G, tile1, tile2);
         launch_cluster_step(d, tile1, tile2, cluster_pack, A.X, A.RHS, A.X0, A.coeff_ch, A.mu, A.level_iters, A.coarsest_iters, A.omega, A.Rr,
-                            A.P, fas2, st);
+                            A.P, fas2, st, coarsest_direct ? root_inv : nullptr);
         return;
     }
     if (l <= 1) {
@@ -604,6 +701,7 @@ void Solver::enqueue_pre(Grid& G, const Key& k, cudaGraphConditionalHandle loop_
     const ReduceScratch rs = scratch();
     enqueue_operand_pack(G, st);
     launch_leaf_fill(d, G.leaf, G.nleaf, G.plane(0), 0.0f, st);
+    if (replacing()) launch_leaf_copy(d, G.leaf, G.nleaf, bkeep, G.plane(1), st);
     if (k.sync > 0) launch_dot(d, G.leaf, G.nleaf, G.plane(1), G.plane(1), kDotRR0, nullptr, rs, st);
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
     enqueue_precond(G, k, st);
@@ -627,6 +725,7 @@ void Solver::enqueue_body(Grid& G, cudaGraphConditionalHandle loop_h, cudaGraphC
 void Solver::enqueue_tail(Grid& G, const Key& k, cudaStream_t st) const {
     const DevGrid d = G.dev();
     const ReduceScratch rs = scratch();
+    if (replacing()) launch_true_residual(d, G.leaf, G.nleaf, G.plane(0), bkeep, G.plane(1), coeff_ch, s, replace_every, st);
     if (k.pure_neumann) launch_recenter(d, G.leaf, G.nleaf, G.plane(1), rs, st);
     enqueue_precond(G, k, st);
     if (learned_active()) launch_dot_flex(d, G.leaf, G.nleaf, G.plane(1), G.plane(4), G.plane(3), rs, st);
@@ -709,9 +808,16 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     if (learned_active()) {
         if (int rc = ensure_aux(G)) return rc;
     }
+    if (replacing()) {
+        if (int rc = ensure_bkeep(G)) return rc;
+    }
+    if (coarsest_direct && kind == kAMG && cluster_active(G)) {
+        if (int rc = prepare_root_inverse(G)) return rc;
+    }
     Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu,
           (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0) | (storage << 4) |
-              (learned_active() ? 256 : 0) | ((finest_iters + 1) << 10),
+              (learned_active() ? 256 : 0) | ((finest_iters + 1) << 10) | ((replacing() ? replace_every : 0) << 20) |
+              (coarsest_direct ? (1 << 30) : 0),
           omega};
     Plan plan{};
     if (use_graph) {
@@ -778,6 +884,7 @@ int Solver::solve_finish(bool verbose, int* iters, double* rel) {
     CK(cudaGetLastError());
     cudaEventElapsedTime(&last_ms, ev0, ev1);
     const PcgScalars& r = *h_s;
+    last_replaced = r.replaced;
     const int sync_stride = pending.sync_stride;
     int n_it = r.iter;
     double rel_res;

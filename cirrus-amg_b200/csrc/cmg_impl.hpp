@@ -175,6 +175,21 @@ struct Solver {
     // 3.5 tol, so a tighter bound would reject sound solves
     static constexpr double kLearnedJudgeSlack = 10.0;
     int ensure_aux(const Grid& G);
+    // FP64 true-residual replacement every `replace_every` PCG iterations (0: off, the
+    // reference's recurrence); bkeep holds the solve's right-hand side for it
+    int replace_every = 0;
+    float* bkeep = nullptr;
+    size_t bkeep_cap = 0;
+    int last_replaced = 0;
+    int ensure_bkeep(const Grid& G);
+    bool replacing() const { return replace_every > 0 && kind == kAMG; }
+    // direct coarsest solve inside the cluster step (mixed-precision mode): the inverse of
+    // the 8^3 root operator in double, from an FP64 Cholesky factor formed on the host
+    // whenever the root's operator changes; null or off: the reference's sweeps
+    bool coarsest_direct = false;
+    double* root_inv = nullptr;
+    std::vector<float> root_ops;  // the root operator the inverse was formed from
+    int prepare_root_inverse(Grid& G);
     void* coeff16 = nullptr;
     size_t coeff16_cap = 0;
     int ensure_coeff16(const Grid& G);

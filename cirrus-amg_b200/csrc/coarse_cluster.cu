@@ -86,6 +86,9 @@ struct ClusterArgs {
     int coeff_ch, mu, level_iters, coarsest_iters, exact, fas2;
     float om, Rr, P;
     double omega;
+    // direct coarsest solve (mixed-precision mode): the inverse of the root operator in
+    // double, [j][t] = (A0^-1)[cell of thread j][cell of thread t]; null: Gauss-Seidel
+    const double* root_inv;
     int tile1[8];   // level-1 tiles by octant (root child order)
     int tile2[64];  // level-2 tiles by (I>>3)*16 + (J>>3)*4 + (K>>3) over the 32^3 grid
 };
@@ -133,6 +136,7 @@ struct ClSmem {
     float b1[8][kClThreads];   // coarse: restricted level-1 rhs, written by the octant CTAs
     float s1[8][kClThreads];   // coarse: saved level-1 x, read back by the octant CTAs
     float x0[kPar];            // coarse: root x, zero halo, layout ro()
+    float b0[kClThreads];      // coarse: root rhs by owning thread (direct coarsest solve)
 };
 constexpr size_t kClSmem = sizeof(ClSmem);
 
@@ -558,9 +562,27 @@ __global__ void __launch_bounds__(kClThreads, 1)
             } else {
                 b0 = 0.0f;
             }
-            // mu coarsest solves: coarsest_iters/2 sweeps in order 0, then in order 1
+            // mu coarsest solves: coarsest_iters/2 sweeps in order 0, then in order 1; or, in
+            // the mixed-precision mode, one exact solve x0 = A0^-1 b0 in double (the later mu
+            // visits of the same right-hand side would leave it unchanged)
             const int par = (o.bi + o.bj + o.bk) & 1;
             const double y0 = sm.yd[8][t];
+            if (A.root_inv) {
+                sm.b0[t] = b0;
+                __syncthreads();
+                if (in0) {
+                    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                    const double* M = A.root_inv + t;
+                    for (int j = 0; j < kClThreads; j += 4) {
+                        a0 = fma(__ldg(M + (size_t)j * kClThreads), (double)sm.b0[j], a0);
+                        a1 = fma(__ldg(M + (size_t)(j + 1) * kClThreads), (double)sm.b0[j + 1], a1);
+                        a2 = fma(__ldg(M + (size_t)(j + 2) * kClThreads), (double)sm.b0[j + 2], a2);
+                        a3 = fma(__ldg(M + (size_t)(j + 3) * kClThreads), (double)sm.b0[j + 3], a3);
+                    }
+                    x0 = __double2float_rn((a0 + a1) + (a2 + a3));
+                }
+                sm.x0[q0] = x0;
+            } else
             for (int rr = 0; rr < A.mu; ++rr)
                 for (int half = 0; half < 2; ++half)
                     for (int it = 0; it < A.coarsest_iters / 2; ++it)
@@ -613,7 +635,8 @@ __global__ void __launch_bounds__(kClThreads, 1)
 size_t cluster_pack_bytes() { return sizeof(ClPack) * kClCtas; }
 
 static void fill_args(ClusterArgs& A, const int* tile1, const int* tile2, int coeff_ch, int mu, int level_iters, int coarsest_iters,
-                      double omega, float Rr, float P, bool fas2) {
+                      double omega, float Rr, float P, bool fas2, const double* root_inv = nullptr) {
+    A.root_inv = root_inv;
     for (int i = 0; i < 8; ++i) A.tile1[i] = tile1[i];
     for (int i = 0; i < 64; ++i) A.tile2[i] = tile2[i];
     A.coeff_ch = coeff_ch;
@@ -635,11 +658,17 @@ void launch_cluster_pack(const DevGrid& g, const int* tile1, const int* tile2, i
     k_cluster_pack<<<kClCtas, kClThreads, 0, st>>>(g, A, reinterpret_cast<ClPack*>(pack));
 }
 
+int cluster_thread_cell(int t) {
+    const int w = t >> 5, lane = t & 31;
+    const int bk = lane & 7, bj = ((w & 3) << 1) | ((lane >> 3) & 1), bi = ((w >> 2) << 1) | (lane >> 4);
+    return (bi << 6) | (bj << 3) | bk;
+}
+
 cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* tile2, const void* pack, float* X, float* RHS, float* X0,
                                 int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float Rr, float P, bool fas2,
-                                cudaStream_t st) {
+                                cudaStream_t st, const double* root_inv) {
     ClusterArgs A;
-    fill_args(A, tile1, tile2, coeff_ch, mu, level_iters, coarsest_iters, omega, Rr, P, fas2);
+    fill_args(A, tile1, tile2, coeff_ch, mu, level_iters, coarsest_iters, omega, Rr, P, fas2, root_inv);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kClCtas);
     cfg.blockDim = dim3(kClThreads);

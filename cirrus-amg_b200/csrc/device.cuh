@@ -266,6 +266,22 @@ __device__ __forceinline__ float own_neg_lap(const Snap& S, const Quad& Q, const
     s = __fmaf_rn(U < 3 ? f4get(o.a2, U + 1) : S.c2[Q.i * 72 + Q.j * 9 + k + 1], U < 3 ? f4get(o.xm, U + 1) : S.x[c + 1], s);
     return s;
 }
+// the same stencil accumulated in double (the FP64 true residual of residual replacement)
+template <int U>
+__device__ __forceinline__ double own_neg_lap64(const Snap& S, const Quad& Q, const Own& o) {
+    const float d = f4get(o.dg, U);
+    if (d == 0.0f) return 0.0;
+    const int k = Q.k0 + U;
+    const int c = sx(Q.i, Q.j, k);
+    double s = (double)f4get(o.xm, U) * (double)d;
+    s = fma((double)f4get(o.a0, U), (double)S.x[c - 100], s);
+    s = fma((double)S.c0[(Q.i + 1) * 64 + Q.j * 8 + k], (double)S.x[c + 100], s);
+    s = fma((double)f4get(o.a1, U), (double)S.x[c - 10], s);
+    s = fma((double)S.c1[Q.i * 72 + (Q.j + 1) * 8 + k], (double)S.x[c + 10], s);
+    s = fma((double)f4get(o.a2, U), (double)(U > 0 ? f4get(o.xm, U - 1) : S.x[c - 1]), s);
+    s = fma((double)(U < 3 ? f4get(o.a2, U + 1) : S.c2[Q.i * 72 + Q.j * 9 + k + 1]), (double)(U < 3 ? f4get(o.xm, U + 1) : S.x[c + 1]), s);
+    return s;
+}
 __device__ __forceinline__ float own_neg_lap(const Snap& S, const Quad& Q, const Own& o, int u) {
     return u == 0 ? own_neg_lap<0>(S, Q, o) : u == 1 ? own_neg_lap<1>(S, Q, o) : u == 2 ? own_neg_lap<2>(S, Q, o) : own_neg_lap<3>(S, Q, o);
 }

@@ -551,6 +551,30 @@ __global__ void __launch_bounds__(128) k_leaf_apply(DevGrid g, const int* leaf, 
 
 // x += alpha p, r -= alpha Ap on INTERIOR cells (src/AMGSolver.cu:1462-1485),
 // r.r (src/AMGSolver.cu:1488) and the convergence test (src/AMGSolver.cu:1487-1496)
+// True-residual replacement (no counterpart in the reference; the mixed-precision solve):
+// on iterations that are a multiple of `every`, r = b - A x on the LEAF tiles, the stencil
+// summed in double and the difference rounded once to float.  Cells that are not INTERIOR
+// keep b, which the recurrence never changes there.  The iteration count is read on the
+// device, so every other iteration returns at once.
+__global__ void __launch_bounds__(128) k_true_residual(DevGrid g, const int* leaf, const float* X, const float* B, float* R,
+                                                       int coeff_ch, PcgScalars* s, int every) {
+    const int it = s->iter;
+    if (it == 0 || it % every != 0) return;
+    __shared__ Snap S;
+    const int t = leaf[blockIdx.x];
+    const Quad Q(t, threadIdx.x);
+    Own o;
+    load_snap(g, t, X, coeff_ch, LeafHalo{X, g.ctype}, S, Q, o, BlockSync{});
+    const float4 b = ld4(B + Q.base);
+    float4 r = b;
+    if (o.ty.x == dInterior) r.x = (float)((double)b.x - own_neg_lap64<0>(S, Q, o));
+    if (o.ty.y == dInterior) r.y = (float)((double)b.y - own_neg_lap64<1>(S, Q, o));
+    if (o.ty.z == dInterior) r.z = (float)((double)b.z - own_neg_lap64<2>(S, Q, o));
+    if (o.ty.w == dInterior) r.w = (float)((double)b.w - own_neg_lap64<3>(S, Q, o));
+    st4(R + Q.base, r);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ++s->replaced;
+}
+
 __global__ void __launch_bounds__(128) k_xr_update(DevGrid g, const int* leaf, float* X, float* R, const float* P, const float* AP,
                                                    ReduceScratch rs, cudaGraphConditionalHandle loop_h,
                                                    cudaGraphConditionalHandle body_h, int use_handles) {
@@ -1262,6 +1286,10 @@ void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* 
 void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
                        ReduceScratch rs, cudaStream_t st) {
     if (nleaf > 0) count_launch(), k_leaf_apply<<<nleaf, 128, 0, st>>>(g, leaf, P, AP, coeff_ch, fuse_alpha ? 1 : 0, rs);
+}
+void launch_true_residual(const DevGrid& g, const int* leaf, int nleaf, const float* X, const float* B, float* R, int coeff_ch,
+                          PcgScalars* s, int every, cudaStream_t st) {
+    if (nleaf > 0 && every > 0) count_launch(), k_true_residual<<<nleaf, 128, 0, st>>>(g, leaf, X, B, R, coeff_ch, s, every);
 }
 void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,
                       ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool use_handles,

@@ -13,6 +13,7 @@ struct PcgScalars {
     double gamma, gamma_old, beta, alpha, pAp, rr, rr0, thr, tol;
     double mean, count;
     int iter, done, converged, nonfinite;
+    int replaced;  // true-residual replacements made by the solve
     int max_iters, sync_stride;
     unsigned int counter[8];
 };
@@ -93,7 +94,11 @@ size_t coarse_step_smem_bytes();
 // FASSaveSolutionAndUpdateSource on level 2 first (all 64 tiles NONLEAF).
 cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* tile2, const void* pack, float* X, float* RHS, float* X0,
                                 int coeff_ch, int mu, int level_iters, int coarsest_iters, double omega, float R_restrict, float P,
-                                bool fas2, cudaStream_t st);
+                                bool fas2, cudaStream_t st, const double* root_inv = nullptr);
+// root_inv (optional): the coarsest level solved exactly as x0 = A0^-1 b0 in double instead of
+// by Gauss-Seidel sweeps; [j][t] = (A0^-1)[cluster_thread_cell(j)][cluster_thread_cell(t)],
+// 512 x 512 doubles, zero rows and columns for cells that are not INTERIOR
+int cluster_thread_cell(int t);  // root cell owned by thread t of the coarse CTA
 void launch_cluster_pack(const DevGrid& g, const int* tile1, const int* tile2, int coeff_ch, void* pack, cudaStream_t st);
 size_t cluster_pack_bytes();
 bool cluster_step_supported();  // the current device can co-schedule the 9-CTA cluster
@@ -109,6 +114,10 @@ int persist_blocks();  // co-resident blocks of the persistent kernel on the cur
 enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3, kDotAlpha = 4 };
 void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,
                        ReduceScratch rs, cudaStream_t st);
+// r = b - A x (stencil in double) on the LEAF tiles when the solve's iteration count is a
+// positive multiple of `every`; a no-op launch on the other iterations
+void launch_true_residual(const DevGrid& g, const int* leaf, int nleaf, const float* X, const float* B, float* R, int coeff_ch,
+                          PcgScalars* s, int every, cudaStream_t st);
 void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,
                       ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool use_handles,
                       cudaStream_t st);

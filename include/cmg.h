@@ -214,6 +214,21 @@ int cmg_amg_solver_autotune(cmg_amg_solver* s, cmg_grid* g, int n, const cmg_tun
  * correction so that the preconditioner stays symmetric; -1 (default): level_iters, as the
  * reference does on every level.  No counterpart in the reference. */
 int cmg_amg_solver_set_finest_iters(cmg_amg_solver* s, int finest_iters);
+/* True-residual replacement, the mixed-precision solve's safeguard: every `every` PCG
+ * iterations (0, the default: never) the recurrence residual is replaced by b - A x computed
+ * on the device with the stencil summed in double, from a copy of b the solve keeps.  The
+ * reference has no counterpart: its residual is the recurrence's, and its only other
+ * residual is the FP64 dot of it (src/AMGSolver.cu:1487-1499).  `count` receives the
+ * replacements the last solve made. */
+int cmg_amg_solver_set_residual_replacement(cmg_amg_solver* s, int every);
+int cmg_amg_solver_residual_replacements(cmg_amg_solver* s, int* count);
+/* Direct coarsest solve (mixed-precision mode; no counterpart in the reference, which runs
+ * coarsest_iters Gauss-Seidel sweeps on level 0, src/AMGSolver.cu:1260-1264): with on != 0,
+ * whenever levels 0-2 are complete (the cluster step runs them), level 0 is solved exactly,
+ * x0 = A0^-1 b0 in double.  A0 is the 8^3 root operator on its INTERIOR cells; its inverse
+ * is formed from an FP64 Cholesky factor on the host when the operator changes, and applied
+ * on the device.  Other octrees keep the sweeps. */
+int cmg_amg_solver_set_coarsest_direct(cmg_amg_solver* s, int on);
 /* Launch flags (default CMG_LAUNCH_GRAPH).
  * GRAPH: the solve runs as one CUDA graph with a device-side while loop;
  * without it the same kernels are launched one by one with the loop test on

@@ -93,3 +93,86 @@ def test_mixed_solve_converges_to_the_fp64_solution(storage, grid):
     assert it <= it32 + 2, (it, it32)
     xs, rt, rc = fp64_solution(g, b, 0 if grid == "uniform64" else 1)
     assert _rel_l2(G.download(0)[rt, rc], xs) <= 1e-5
+
+
+def test_true_residual_replacement():
+    """Every `every` iterations the recurrence residual is replaced by b - A x (stencil in
+    FP64).  A weak preconditioner (one sweep per level, two on the coarsest) makes the solve
+    long enough for several replacements; it must still converge to the FP64 solution with
+    about the iteration count of the plain recurrence.  With `every` beyond the iteration
+    count the solve is the plain one, bit for bit."""
+    from test_gpu_parity import fp64_solution
+
+    G, g, solver, b = setup_uniform(3)
+    solver.omega = 1.0
+    solver.mu_cycle_repeat_times = 1
+    it0, rel0 = solver.solve(G, False, 100, 1e-6, 1, 2, 1, False)
+    x0 = G.download(0)
+    assert solver.last_replacements() == 0
+    G.upload(1, b)
+    solver.set_residual_replacement(3)
+    it1, rel1 = solver.solve(G, False, 100, 1e-6, 1, 2, 1, False)
+    n = solver.last_replacements()
+    assert it0 >= 7, it0
+    assert n == (it1 - 1) // 3 and n >= 2, (n, it1)
+    assert rel1 <= 1e-6 and abs(it1 - it0) <= 1, (it0, it1)
+    xs, rt, rc = fp64_solution(g, b, 0)
+    x1 = G.download(0)
+    assert _rel_l2(x1[rt, rc], xs) <= 1e-5
+    # the replaced residual is the true one: |b - A x| / |b| from the FP64 operator
+    rp, ci, va, rt2, rc2 = g.assemble(COEFF)
+    from oracle import oracle as O
+
+    ax = O.csr_matvec(rp, ci, va, x1[rt2, rc2].astype(np.float64))
+    bb = b[rt2, rc2].astype(np.float64)
+    true_rel = np.linalg.norm(bb - ax) / np.linalg.norm(bb)
+    assert true_rel <= 2e-6, true_rel
+    G.upload(1, b)
+    solver.set_residual_replacement(1000)
+    it2, rel2 = solver.solve(G, False, 100, 1e-6, 1, 2, 1, False)
+    assert solver.last_replacements() == 0
+    assert (it2, rel2) == (it0, rel0) and np.array_equal(G.download(0), x0)
+
+
+@pytest.mark.parametrize("grid", ["uniform32", "uniform64", "shell345"])
+def test_direct_coarsest_solve(grid):
+    """Level 0 solved exactly in double (FP64 Cholesky-based inverse of the root operator)
+    inside the cluster step: the solve converges to the FP64 solution in no more PCG
+    iterations than with the reference's coarsest sweeps."""
+    from test_gpu_parity import fp64_solution
+
+    if grid.startswith("uniform"):
+        G, g, solver, b = setup_uniform(2 if grid == "uniform32" else 3)
+    else:
+        G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5))
+        b = G.download(1)
+        g.channel(1)[:] = b
+    it0, rel0 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    solver.set_coarsest_direct(True)
+    G.upload(1, b)
+    it1, rel1 = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    assert rel1 <= 1e-6 and it1 <= it0, (it0, it1)
+    xs, rt, rc = fp64_solution(g, b, 0 if grid.startswith("uniform") else 1)
+    assert _rel_l2(G.download(0)[rt, rc], xs) <= 1e-5
+    # fewer coarsest sweeps than the reference's ten cannot beat the exact solve
+    solver.set_coarsest_direct(False)
+    G.upload(1, b)
+    it2, _ = solver.solve(G, False, 100, 1e-6, 2, 2, 1, False)
+    assert it1 <= it2
+
+
+def test_mixed_mode_on_the_sphere_octree():
+    """Config 3's whole mixed mode on the 3/4/5 sphere octree: BF16 operator storage, true
+    residual every 10 iterations and the direct coarsest solve, against the FP64 solution."""
+    from test_gpu_parity import fp64_solution
+
+    G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5))
+    b = G.download(1)
+    g.channel(1)[:] = b
+    solver.set_storage("bf16")
+    solver.set_residual_replacement(10)
+    solver.set_coarsest_direct(True)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    assert rel <= 1e-6
+    xs, rt, rc = fp64_solution(g, b, 1)
+    assert _rel_l2(G.download(0)[rt, rc], xs) <= 1e-5
