@@ -216,7 +216,7 @@ def build_grid(cmg, spec):
     G = cmg.HADeviceGrid(0.125, 10, 16)
     G.set_tile_host(0, (0, 0, 0), cmg.LEAF)
     G.rebuild()
-    G.refine_case(case, spec["params"])
+    G.refine_case(case, spec["params"], on_device=True)  # the octree built in device memory
     G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
     if spec["spheres"]:
         G.cutcell_sphere_coeffs(COEFF, spec["spheres"], 0.5)
@@ -582,10 +582,15 @@ def run_ours(args, rank, world, local_rank):
     # mixed mode (BF16 storage, FP64 true residual every 10 iterations, direct coarsest)
     x32 = G.download(0)
     mixed, mixed_x = {}, {"fp32": x32}
-    mixed_modes = {"bf16": ("bf16", 0, False), "fp16": ("fp16", 0, False), "fp32_direct_coarsest": ("fp32", 0, True),
-                   "bf16_replace10_direct_coarsest": ("bf16", 10, True)}
-    for mode, (storage, every, direct) in mixed_modes.items():
+    # (operator storage, x/rhs of levels >= 3 in BF16, true residual every N, direct coarsest)
+    mixed_modes = {"bf16": ("bf16", False, 0, False), "fp16": ("fp16", False, 0, False),
+                   "bf16_operator_x_rhs": ("bf16", True, 0, False),
+                   "bf16_operator_x_rhs_replace10": ("bf16", True, 10, False),
+                   "fp32_direct_coarsest": ("fp32", False, 0, True),
+                   "bf16_operator_x_rhs_replace10_direct_coarsest": ("bf16", True, 10, True)}
+    for mode, (storage, cycle16, every, direct) in mixed_modes.items():
         S.set_storage(storage)
+        S.set_cycle_bf16(cycle16)
         S.set_residual_replacement(every)
         S.set_coarsest_direct(direct)
         for _ in range(3):
@@ -605,6 +610,7 @@ def run_ours(args, rank, world, local_rank):
                        "rel_l2_vs_fp32_solution": float(np.linalg.norm((xm - x32)[lm].astype(np.float64)) /
                                                         np.linalg.norm(x32[lm].astype(np.float64)))}
     S.set_storage("fp32")
+    S.set_cycle_bf16(False)
     S.set_residual_replacement(0)
     S.set_coarsest_direct(False)
     one_solve()

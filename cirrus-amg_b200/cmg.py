@@ -34,7 +34,7 @@ CASE_STAR_EMPTY, CASE_STAR_SOLID, CASE_SHELL, CASE_MULTI_SPHERE = 4, 5, 6, 7
 EXPORTS = [
     "cmg_last_error", "cmg_version", "cmg_check_division",
     "cmg_grid_create", "cmg_grid_destroy", "cmg_grid_set_tile", "cmg_grid_rebuild", "cmg_grid_iterative_refine",
-    "cmg_grid_refine_case", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
+    "cmg_grid_refine_case", "cmg_grid_refine_case_device", "cmg_grid_info", "cmg_grid_tiles", "cmg_grid_tables", "cmg_grid_channel_ptr",
     "cmg_grid_cell_type_ptr", "cmg_grid_upload_channel", "cmg_grid_download_channel", "cmg_grid_upload_cell_types",
     "cmg_grid_download_cell_types", "cmg_grid_fill_channel", "cmg_grid_copy_channel", "cmg_grid_set_leaf_cell_types_case", "cmg_grid_set_stream",
     "cmg_grid_calc_cell_types_from_leafs", "cmg_grid_load_hagr", "cmg_grid_dump_hagr", "cmg_ref_record_layout",
@@ -53,7 +53,7 @@ EXPORTS = [
     "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
     "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned",
     "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
-    "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct",
+    "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct", "cmg_amg_solver_set_cycle_bf16",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -84,6 +84,7 @@ def lib():
             "cmg_grid_rebuild": (I, [P]),
             "cmg_grid_iterative_refine": (I, [P, TARGET_FN, P, P]),
             "cmg_grid_refine_case": (I, [P, I, P, I, P]),
+            "cmg_grid_refine_case_device": (I, [P, I, P, I, P]),
             "cmg_grid_info": (I, [P, P, P, P]),
             "cmg_grid_tiles": (I, [P, P, P, P]),
             "cmg_grid_tables": (I, [P, P, P]),
@@ -149,6 +150,7 @@ def lib():
             "cmg_amg_solver_set_finest_iters": (I, [P, I]),
             "cmg_amg_solver_set_residual_replacement": (I, [P, I]),
             "cmg_amg_solver_set_coarsest_direct": (I, [P, I]),
+            "cmg_amg_solver_set_cycle_bf16": (I, [P, I]),
             "cmg_amg_solver_residual_replacements": (I, [P, ctypes.POINTER(I)]),
             "cmg_amg_solver_set_learned": (I, [P, P]),
             "cmg_amg_solver_learned_status": (I, [P, P, P, P]),
@@ -260,10 +262,13 @@ class HADeviceGrid:
         _check(self.L.cmg_grid_iterative_refine(self.h, cb, None, ctypes.byref(steps)), "iterative_refine")
         return steps.value
 
-    def refine_case(self, case_id, params):
+    def refine_case(self, case_id, params, on_device=False):
+        """iterativeRefine with a built-in target; on_device: the whole build (refinement,
+        ghost layer, canonical order, tables) in device memory (cmg_grid_refine_case_device)."""
         prm = np.asarray(params, dtype=np.float64)
         steps = ctypes.c_int(0)
-        _check(self.L.cmg_grid_refine_case(self.h, case_id, _p(prm), len(prm), ctypes.byref(steps)), "refine_case")
+        fn = self.L.cmg_grid_refine_case_device if on_device else self.L.cmg_grid_refine_case
+        _check(fn(self.h, case_id, _p(prm), len(prm), ctypes.byref(steps)), "refine_case")
         return steps.value
 
     def info(self):
@@ -440,6 +445,10 @@ class AMGSolver:
         """Level 0 solved exactly (FP64 Cholesky-based inverse) when the cluster step runs
         levels 0-2, instead of the reference's coarsest sweeps."""
         _check(self.L.cmg_amg_solver_set_coarsest_direct(self.h, int(bool(on))), "set_coarsest_direct")
+
+    def set_cycle_bf16(self, on=True):
+        """x, rhs and saved x of the cycle's levels >= 3 stored in BF16 (FP32 arithmetic)."""
+        _check(self.L.cmg_amg_solver_set_cycle_bf16(self.h, int(bool(on))), "set_cycle_bf16")
 
     def last_replacements(self):
         n = ctypes.c_int(0)

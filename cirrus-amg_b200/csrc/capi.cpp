@@ -119,6 +119,13 @@ int cmg_grid_refine_case(cmg_grid* g, int case_id, const double* params, int npa
     return g->g.rebuild();
     GUARD_END
 }
+int cmg_grid_refine_case_device(cmg_grid* g, int case_id, const double* params, int nparams, int* steps) {
+    GUARD_BEGIN
+    if (!g || !params || nparams < 2 || nparams > cmg::kDevTopoMaxParams || case_id < 0 || case_id > 7)
+        return fail(CMG_ERR_INVALID, "cmg_grid_refine_case_device: bad argument");
+    return g->g.refine_case_device(case_id, params, nparams, steps);
+    GUARD_END
+}
 int cmg_grid_info(cmg_grid* g, int* num_tiles, int* max_level, int* num_leaf_tiles) {
     if (!g) return fail(CMG_ERR_INVALID, "null grid");
     if (num_tiles) *num_tiles = g->g.built ? g->g.topo.size() : 0;
@@ -419,6 +426,11 @@ int cmg_amg_solver_set_finest_iters(cmg_amg_solver* s, int finest_iters) {
 int cmg_amg_solver_set_residual_replacement(cmg_amg_solver* s, int every) {
     if (!s || every < 0 || every > 1000) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_residual_replacement: bad argument (0..1000)");
     s->s.replace_every = every;
+    return CMG_OK;
+}
+int cmg_amg_solver_set_cycle_bf16(cmg_amg_solver* s, int on) {
+    if (!s) return fail(CMG_ERR_INVALID, "cmg_amg_solver_set_cycle_bf16: null solver");
+    s->s.cycle_bf16 = on != 0;
     return CMG_OK;
 }
 int cmg_amg_solver_set_coarsest_direct(cmg_amg_solver* s, int on) {

@@ -44,6 +44,7 @@ Grid::~Grid() {
     dfree(modes);
     dfree(dot_out);
     dfree(tile_ptrs);
+    delete topo_builder;
 }
 
 static unsigned long long tile_key(const TileRec& r) {
@@ -56,6 +57,32 @@ static unsigned long long tile_key(const TileRec& r) {
 int Grid::rebuild() {
     topo.spawn_ghosts();
     topo.canonicalize();
+    built = true;
+    ++host_version;
+    return 0;
+}
+
+int Grid::refine_case_device(int case_id, const double* params, int nparams, int* steps) {
+    if (!device_case_supported(case_id)) {
+        const float h0 = topo.h0();
+        std::vector<double> prm(params, params + nparams);
+        const int st = topo.iterative_refine([&](int level, int i, int j, int k) {
+            const int c[3] = {i, j, k};
+            return case_target(case_id, prm.data(), (int)prm.size(), h0, level, c);
+        });
+        if (steps) *steps = st;
+        return rebuild();
+    }
+    if (!topo_builder) topo_builder = new DeviceTopoBuilder();
+    const int rc = device_refine_case(*topo_builder, topo, case_id, params, nparams, stream, steps);
+    if (rc == 1) {
+        set_error("refine_case_device: bad parameters");
+        return 1;
+    }
+    if (rc) {
+        set_error("refine_case_device: CUDA error in the device octree builder");
+        return 2;
+    }
     built = true;
     ++host_version;
     return 0;
@@ -221,6 +248,7 @@ Solver::~Solver() {
     dfree(bsave);
     dfree(bkeep);
     dfree(root_inv);
+    dfree(x16);
     if (h_s) cudaFreeHost(h_s);
     if (h_bar) cudaFreeHost(h_bar);
     dfree(bar);
@@ -280,14 +308,17 @@ MuArgs Solver::mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters
 }
 
 // GaussSeidelAMG (src/AMGSolver.cu:887-894) on the LEAF and NONLEAF tiles of one level
-void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined) const {
+void Solver::enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined,
+                        void* X16, const void* RHS16) const {
     const DevGrid d = G.dev();
     const int t0 = G.level_begin(level), nt = G.ghost_begin(level) - t0;
     const bool pipe = pipelined && use_pipe && pipe_ok;
     for (int it = 0; it < iters; ++it)
         for (int h = 0; h < 2; ++h) {
             const int color = h ? 1 - order : order;
-            if (pipe) launch_gs_pipe(d, t0, nt, X, RHS, coeff_ch, color, omega, st, kind == kAMG ? storage : kStorageFP32, coeff16);
+            const int stg = kind == kAMG ? storage : kStorageFP32;
+            if (X16) launch_gs_pipe(d, t0, nt, X16, RHS16, true, coeff_ch, color, omega, st, stg, coeff16);
+            else if (pipe) launch_gs_pipe(d, t0, nt, X, RHS, false, coeff_ch, color, omega, st, stg, coeff16);
             else launch_gs(d, t0, nt, X, RHS, coeff_ch, color, omega, st);
         }
 }
@@ -362,6 +393,22 @@ int Solver::ensure_aux(const Grid& G) {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
     graphs.clear();
     return 0;
+}
+
+int Solver::ensure_x16(const Grid& G) {
+    const size_t need = (size_t)G.n * kCells;
+    if (x16_cap >= need) return 0;
+    dfree(x16);
+    x16 = nullptr;
+    x16_cap = 0;
+    CK(cudaMalloc(&x16, 3 * 2 * need));
+    x16_cap = need;
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);  // captured graphs hold the old pointer
+    graphs.clear();
+    return 0;
+}
+bool Solver::cycle16_active(const Grid& G) const {
+    return cycle_bf16 && kind == kAMG && use_pipe && pipe_ok && !use_persist && !learned_active() && G.max_level() >= 3;
 }
 
 int Solver::ensure_bkeep(const Grid& G) {
@@ -511,9 +558,28 @@ void Solver::enqueue_mu_step(Grid& G, int l, const MuArgs& A, cudaStream_t st, b
         return;
     }
     const int li = (l == A.finest_level && A.finest_iters >= 0) ? A.finest_iters : A.level_iters;
+    if (A.X16 && l >= 3) {
+        // the mixed-precision cycle's BF16 levels; level 2 and below stay float
+        const bool p16 = l - 1 >= 3;
+        void* Xp = p16 ? A.X16 : (void*)A.X;
+        void* Rp = p16 ? A.RHS16 : (void*)A.RHS;
+        void* X0p = p16 ? A.X016 : (void*)A.X0;
+        enqueue_gs(G, l, li, 0, A.X, A.RHS, st, true, A.X16, A.RHS16);
+        launch_restrict_pipe(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X16, A.RHS16, true, Xp, Rp, p16, A.coeff_ch, A.Rr,
+                             st);
+        const bool fold = l - 1 == 2 && A.mu > 0 && cluster_active(G) && G.nonleaf_begin(2) == G.level_begin(2);
+        const int nb0 = G.nonleaf_begin(l - 1), nbn = G.ghost_begin(l - 1) - nb0;
+        if (p16) launch_fas_pipe_x16(d, nb0, nbn, A.X16, A.RHS16, A.X016, A.coeff_ch, st);
+        else if (!fold) launch_fas_save(d, nb0, nbn, A.X, A.RHS, A.X0, A.coeff_ch, st);
+        for (int r = 0; r < A.mu; ++r) enqueue_mu_step(G, l - 1, A, st, fold && r == 0);
+        launch_prolong_x16(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), A.X16, Xp, X0p, p16, A.P, st);
+        enqueue_gs(G, l, li, 1, A.X, A.RHS, st, true, A.X16, A.RHS16);
+        return;
+    }
     enqueue_gs(G, l, li, 0, A.X, A.RHS, st, true);
     if (use_pipe && pipe_ok)
-        launch_restrict_pipe(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
+        launch_restrict_pipe(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, false, A.X, A.RHS, false, A.coeff_ch,
+                             A.Rr, st);
     else
         launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), A.X, A.RHS, A.coeff_ch, A.Rr, st);
     // the first cluster launch of level 2 does level 2's FAS update itself when every level-2 tile is NONLEAF
@@ -661,6 +727,21 @@ int Solver::damped_jacobi_solve(Grid& G, int max_iters, double tol, float omega,
 void Solver::enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const {
     if (kind != kAMG) {
         enqueue_geo_vcycle(G, G.plane(4), G.plane(1), G.plane(3), k.level_iters, k.coarsest_iters, st);
+    } else if (cycle16_active(G)) {
+        // x, rhs and saved x of levels >= 3 in BF16: the right-hand side goes in on the LEAF
+        // tiles of those levels, the cycle runs, z comes back out there
+        MuArgs A = mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters);
+        const size_t plane = (size_t)G.n * kCells;
+        A.X16 = x16;
+        A.RHS16 = static_cast<unsigned short*>(x16) + plane;
+        A.X016 = static_cast<unsigned short*>(x16) + 2 * plane;
+        int first = 0;  // LEAF tiles of levels 0-2 lead the leaf list
+        for (int l = 0; l < 3; ++l) first += G.nonleaf_begin(l) - G.level_begin(l);
+        launch_fill(A.X, plane, 0.0f, st);
+        cudaMemsetAsync(A.X16, 0, 2 * plane, st);
+        launch_leaf_to_bf16(G.leaf + first, G.nleaf - first, A.RHS, A.RHS16, st);
+        enqueue_mu_step(G, G.max_level(), A, st);
+        launch_leaf_from_bf16(G.leaf + first, G.nleaf - first, A.X16, A.X, st);
     } else if (!learned_active()) {
         enqueue_mu_cycle(G, mu_args(G, 4, 1, 3, k.level_iters, k.coarsest_iters), st);
     } else {
@@ -811,13 +892,16 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     if (replacing()) {
         if (int rc = ensure_bkeep(G)) return rc;
     }
+    if (cycle16_active(G)) {
+        if (int rc = ensure_x16(G)) return rc;
+    }
     if (coarsest_direct && kind == kAMG && cluster_active(G)) {
         if (int rc = prepare_root_inverse(G)) return rc;
     }
     Key k{&G, G.version, level_iters, coarsest_iters, pure_neumann ? 1 : 0, mu,
           (sync_stride > 0 ? 1 : 0) | (use_persist ? 2 : 0) | (use_cluster ? 4 : 0) | (use_pipe ? 8 : 0) | (storage << 4) |
               (learned_active() ? 256 : 0) | ((finest_iters + 1) << 10) | ((replacing() ? replace_every : 0) << 20) |
-              (coarsest_direct ? (1 << 30) : 0),
+              (coarsest_direct ? (1 << 30) : 0) | (cycle16_active(G) ? (1 << 9) : 0),
           omega};
     Plan plan{};
     if (use_graph) {

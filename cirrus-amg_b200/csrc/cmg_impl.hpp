@@ -10,6 +10,7 @@
 
 #include "kernels.hpp"
 #include "topology.hpp"
+#include "topo_device.hpp"
 
 namespace cmg {
 
@@ -42,11 +43,14 @@ struct Grid {
     void** tile_ptrs = nullptr;  // device copy of a caller's tile address list (reference tiles)
     int tile_ptrs_cap = 0;
     double* dot_out = nullptr;
+    DeviceTopoBuilder* topo_builder = nullptr;  // device octree builder (refine_case_device)
     int device = -1;  // the CUDA device the device copy lives on (current at its first allocation)
 
     Grid(float h0, int num_levels, int num_channels) : topo(h0, num_levels), nch(num_channels) {}
     ~Grid();
     int rebuild();        // host: ghosts, order, tables
+    // the built-in refinement case built on the device (cases 0-3, 6, 7; the others on the host)
+    int refine_case_device(int case_id, const double* params, int nparams, int* steps);
     int ensure_device();  // device: storage and tables of the current topology
     DevGrid dev() const {
         DevGrid d;
@@ -73,6 +77,10 @@ struct MuArgs {
     float* X;
     float* RHS;
     float* X0;
+    // the mixed-precision cycle: x, rhs and saved x of levels >= 3 in BF16 planes (null: float)
+    void* X16 = nullptr;
+    void* RHS16 = nullptr;
+    void* X016 = nullptr;
     int coeff_ch, mu, level_iters, coarsest_iters;
     int finest_level = -1, finest_iters = -1;  // sweeps on the finest level when >= 0 (levels >= 3)
     double omega;
@@ -142,7 +150,8 @@ struct Solver {
     ReduceScratch scratch() const { return ReduceScratch{partial, partial2, s}; }
     MuArgs mu_args(Grid& G, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) const;
     // pipelined: the x plane is known to be masked to INTERIOR cells (inside the cycle)
-    void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined = false) const;
+    void enqueue_gs(Grid& G, int level, int iters, int order, float* X, const float* RHS, cudaStream_t st, bool pipelined = false,
+                    void* X16 = nullptr, const void* RHS16 = nullptr) const;
     void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st, bool fas2 = false) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
     bool use_graph = true;    // false: launch kernel by kernel from the host (profiling)
@@ -183,6 +192,13 @@ struct Solver {
     int last_replaced = 0;
     int ensure_bkeep(const Grid& G);
     bool replacing() const { return replace_every > 0 && kind == kAMG; }
+    // BF16 storage of the cycle's x and rhs on levels >= 3 (mixed-precision mode); three
+    // BF16 planes (x, rhs, saved x) of the grid's size
+    bool cycle_bf16 = false;
+    void* x16 = nullptr;
+    size_t x16_cap = 0;
+    int ensure_x16(const Grid& G);
+    bool cycle16_active(const Grid& G) const;
     // direct coarsest solve inside the cluster step (mixed-precision mode): the inverse of
     // the 8^3 root operator in double, from an FP64 Cholesky factor formed on the host
     // whenever the root's operator changes; null or off: the reference's sweeps

@@ -117,15 +117,11 @@ __device__ __forceinline__ float nlap(float d, float x, float cmx, float xmx, fl
     s = __fmaf_rn(cpz, xpz, s);
     return s;
 }
-// one Gauss-Seidel update (src/AMGSolver.cu:868-875); kExact: omega is a float (as the
-// reference's AMGSolver::omega always is), so the product delta * omega is exact in double
-template <bool kExact>
+// one Gauss-Seidel update (src/AMGSolver.cu:868-875); kRelax: how omega is applied (relax<>)
+template <int kRelax>
 __device__ __forceinline__ float gs_update(float xs, float rhs, float ax, float d, double yd, bool interior, const ClusterArgs& A) {
     const float delta = interior ? div_by_recip(__fsub_rn(rhs, ax), d, yd) : 0.0f;
-    if constexpr (kExact)
-        return relax_ref(xs, delta, A.om);
-    else
-        return (float)((double)xs + (double)delta * A.omega);
+    return relax<kRelax>(xs, delta, A.om, A.omega);
 }
 
 // Shared memory.  Octant CTA: x (the level-2 octant, halo from the neighbouring
@@ -220,7 +216,7 @@ __device__ __forceinline__ void blk_publish_all(const Blk& o, float* xs, const P
 // four cells are not neighbours of one another, so every neighbour load comes first, then
 // the four updates, then the stores: the updates overlap instead of each waiting on the
 // previous cell's shared-memory store.
-template <int Q0, int Q1, int Q2, int Q3, bool kRemote, bool kExact>
+template <int Q0, int Q1, int Q2, int Q3, bool kRemote, int kExact>
 __device__ __forceinline__ void blk_gs_colour(Blk& o, float* xs, const double* yd, const Peers& pr, const ClusterArgs& A) {
     float v0[3], v1[3], v2[3], v3[3];
     blk_outer<Q0>(o, xs, v0);
@@ -239,7 +235,7 @@ __device__ __forceinline__ void blk_gs_colour(Blk& o, float* xs, const double* y
     blk_publish<Q2, kRemote>(o, xs, pr);
     blk_publish<Q3, kRemote>(o, xs, pr);
 }
-template <bool kRemote, bool kExact>
+template <bool kRemote, int kExact>
 __device__ __forceinline__ void blk_gs_pass(Blk& o, float* xs, const double* yd, const Peers& pr, int color, const ClusterArgs& A) {
     if (color == 0)
         blk_gs_colour<0, 3, 5, 6, kRemote, kExact>(o, xs, yd, pr, A);
@@ -372,7 +368,7 @@ __global__ void __launch_bounds__(kClThreads) k_cluster_pack(DevGrid g, const __
 // ---------------------------------------------------------------------------
 // The cluster step
 // ---------------------------------------------------------------------------
-template <bool kExact>
+template <int kExact>
 __global__ void __launch_bounds__(kClThreads, 1)
     k_cluster_step(DevGrid g, const __grid_constant__ ClusterArgs A, const ClPack* packs, float* X, float* RHS, float* X0) {
     extern __shared__ __align__(16) unsigned char cl_smem[];
@@ -644,7 +640,7 @@ static void fill_args(ClusterArgs& A, const int* tile1, const int* tile2, int co
     A.level_iters = level_iters;
     A.coarsest_iters = coarsest_iters;
     A.om = (float)omega;
-    A.exact = ((double)A.om == omega);
+    A.exact = relax_mode(omega);
     A.omega = omega;
     A.Rr = Rr;
     A.P = P;
@@ -682,18 +678,22 @@ cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* t
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
     note_kernel_launch();
-    if (A.exact) return cudaLaunchKernelEx(&cfg, k_cluster_step<true>, g, A, reinterpret_cast<const ClPack*>(pack), X, RHS, X0);
-    return cudaLaunchKernelEx(&cfg, k_cluster_step<false>, g, A, reinterpret_cast<const ClPack*>(pack), X, RHS, X0);
+    const ClPack* pk = reinterpret_cast<const ClPack*>(pack);
+    if (A.exact == kRelaxShort) return cudaLaunchKernelEx(&cfg, k_cluster_step<kRelaxShort>, g, A, pk, X, RHS, X0);
+    if (A.exact == kRelaxRef) return cudaLaunchKernelEx(&cfg, k_cluster_step<kRelaxRef>, g, A, pk, X, RHS, X0);
+    return cudaLaunchKernelEx(&cfg, k_cluster_step<kRelaxDouble>, g, A, pk, X, RHS, X0);
 }
 
 bool cluster_step_supported() {
     int dev = 0, cc = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&cc, cudaDevAttrClusterLaunch, dev) != cudaSuccess || !cc) return false;
-    if (cudaFuncSetAttribute(k_cluster_step<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_cluster_step<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-        cudaFuncSetAttribute(k_cluster_step<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_cluster_step<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_cluster_step<kRelaxShort>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<kRelaxShort>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<kRelaxRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<kRelaxRef>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<kRelaxDouble>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cluster_step<kRelaxDouble>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
@@ -709,7 +709,7 @@ bool cluster_step_supported() {
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, k_cluster_step<true>, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_cluster_step<kRelaxRef>, &cfg) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }

@@ -36,9 +36,9 @@ namespace cmg {
 
 namespace {
 
-template <typename CT>
+template <typename CT, typename XT = float>
 struct alignas(16) PipeStage {
-    float x[512], b[512];
+    XT x[512], b[512];
     CT d[512];        // diagonal
     CT c0[512];       // -x faces
     CT c1[512];       // -y faces
@@ -47,17 +47,20 @@ struct alignas(16) PipeStage {
     // [i][k], +z faces of row k = 7 [i][j]; a word holds the float, or for 16-bit storage
     // the 4-byte-aligned pair of plane elements that contains the face
     unsigned c0h[64], c1h[64], c2h[64];
-    float hx[384];    // halo x of the six faces, [axis][side][a][b]
+    unsigned hx[384];  // halo x of the six faces, [axis][side][a][b]: the float, or the BF16 pair
     unsigned ty[128];
 };
 // bulk-copy destinations: 16-byte aligned offsets
-template <typename CT>
+template <typename CT, typename XT>
 constexpr bool stage_aligned() {
-    return offsetof(PipeStage<CT>, b) % 16 == 0 && offsetof(PipeStage<CT>, d) % 16 == 0 && offsetof(PipeStage<CT>, c0) % 16 == 0 &&
-           offsetof(PipeStage<CT>, c1) % 16 == 0 && offsetof(PipeStage<CT>, c2) % 16 == 0 && offsetof(PipeStage<CT>, ty) % 16 == 0 &&
-           sizeof(PipeStage<CT>) % 16 == 0;
+    using S = PipeStage<CT, XT>;
+    return offsetof(S, b) % 16 == 0 && offsetof(S, d) % 16 == 0 && offsetof(S, c0) % 16 == 0 && offsetof(S, c1) % 16 == 0 &&
+           offsetof(S, c2) % 16 == 0 && offsetof(S, ty) % 16 == 0 && sizeof(S) % 16 == 0;
 }
-static_assert(stage_aligned<float>() && stage_aligned<__nv_bfloat16>() && stage_aligned<__half>(), "stage layout");
+static_assert(stage_aligned<float, float>() && stage_aligned<__nv_bfloat16, float>() && stage_aligned<__half, float>() &&
+                  stage_aligned<float, __nv_bfloat16>() && stage_aligned<__nv_bfloat16, __nv_bfloat16>() &&
+                  stage_aligned<__half, __nv_bfloat16>(),
+              "stage layout");
 // The snapshot: masked x of the tile with its one-cell halo, split into four planes by
 // k mod 4 (k = 4h + u: u the plane, h = -1..2 the slot), rows j of 4 slots, layers i of
 // 42 floats, planes of 448 floats.  A warp's threads own (i0..i0+1, j 0..7, h 0..1) and
@@ -67,14 +70,15 @@ static_assert(stage_aligned<float>() && stage_aligned<__nv_bfloat16>() && stage_
 constexpr int kSxI = 42, kSxJ = 4, kSxP = 448;
 __device__ __forceinline__ int sxp(int i, int j, int k) { return ((k + 4) & 3) * kSxP + (i + 1) * kSxI + (j + 1) * kSxJ + ((k + 4) >> 2); }
 
-template <typename CT>
+template <typename CT, typename XT>
 struct PipeSmem {
-    PipeStage<CT> st[2];
+    PipeStage<CT, XT> st[2];
     float x[4 * kSxP];
 };
-// the restriction pass also keeps the tile's residuals
+// the restriction pass also keeps the tile's residuals (operator in float)
+template <typename XT>
 struct PipeSmemR {
-    PipeStage<float> st[2];
+    PipeStage<float, XT> st[2];
     float x[4 * kSxP];
     float res[512];
 };
@@ -153,13 +157,43 @@ struct Coef<__half> : Coef16<__half> {
     }
 };
 
+// Storage of x and rhs (the mixed-precision cycle keeps them in BF16 on levels >= 3).
+template <typename XT>
+struct XStore;
+template <>
+struct XStore<float> {
+    __device__ static void cp_halo(unsigned* dst, const float* X, size_t o) { cp4(dst, X + o); }
+    __device__ static float halo(unsigned w, int) { return __uint_as_float(w); }
+    __device__ static float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+    __device__ static void st4g(float* p, float4 v) { st4(p, v); }
+    __device__ static void st1(float* p, float v) { *p = v; }
+};
+template <>
+struct XStore<__nv_bfloat16> {
+    // a halo element moves inside its 4-byte-aligned pair
+    __device__ static void cp_halo(unsigned* dst, const __nv_bfloat16* X, size_t o) { cp4(dst, X + (o & ~(size_t)1)); }
+    __device__ static float wide(unsigned bits) { return __uint_as_float(bits << 16); }
+    __device__ static float halo(unsigned w, int odd) { return wide(odd ? w >> 16 : w & 0xffffu); }
+    __device__ static float4 ld4(const __nv_bfloat16* p) {
+        const uint2 w = *reinterpret_cast<const uint2*>(p);
+        return make_float4(wide(w.x & 0xffffu), wide(w.x >> 16), wide(w.y & 0xffffu), wide(w.y >> 16));
+    }
+    __device__ static unsigned bits(float v) { return (unsigned)__bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+    __device__ static void st4g(__nv_bfloat16* p, float4 v) {
+        *reinterpret_cast<uint2*>(p) = make_uint2(bits(v.x) | (bits(v.y) << 16), bits(v.z) | (bits(v.w) << 16));
+    }
+    __device__ static void st1(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
 struct PipeArgs {
-    int t0, nt, color, exact;
+    int t0, nt, color, exact;  // exact: the relaxation mode (kRelax*)
     float om;
     double omega;
     const void* coef;  // first of the four operator planes (-x, -y, -z faces, diagonal)
     size_t cstride;    // elements from one operator plane to the next
-    float* rhs;        // restriction pass: the right-hand side plane, written on the parent tiles
+    void* xp;          // restriction pass: the x plane of the parent tiles
+    void* rhsp;        // restriction pass: the rhs plane of the parent tiles; FAS pass: the tiles' own rhs
+    void* x0p;         // FAS pass: the saved-x plane
     float Rr;          // restriction pass: R_restrict
 };
 
@@ -170,17 +204,17 @@ __device__ __forceinline__ void load_desc(const DevGrid& g, int t, int side, int
 }
 
 // start the copies of tile t into stage S (mbarrier mb takes the bulk part)
-template <typename CT>
-__device__ __forceinline__ void issue(PipeStage<CT>& S, unsigned mb, const DevGrid& g, int t, const float* X, const float* B,
+template <typename CT, typename XT>
+__device__ __forceinline__ void issue(PipeStage<CT, XT>& S, unsigned mb, const DevGrid& g, int t, const XT* X, const XT* B,
                                       const CT* C0, const CT* C1, const CT* C2, const CT* C3, const int d[3], int q, float h) {
     const size_t tb = (size_t)t * kCells;
     if (q == 0) {
-        constexpr unsigned kF = kCells * sizeof(float), kC = kCells * sizeof(CT), kT = kCells;
+        constexpr unsigned kX = kCells * sizeof(XT), kC = kCells * sizeof(CT), kT = kCells;
         // the stage was last read through ordinary loads; order them before the async writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect(mb, 2 * kF + 4 * kC + kT);
-        bulk_g2s(S.x, X + tb, kF, mb);
-        bulk_g2s(S.b, B + tb, kF, mb);
+        mbar_expect(mb, 2 * kX + 4 * kC + kT);
+        bulk_g2s(S.x, X + tb, kX, mb);
+        bulk_g2s(S.b, B + tb, kX, mb);
         bulk_g2s(S.d, C3 + tb, kC, mb);
         bulk_g2s(S.c0, C0 + tb, kC, mb);
         bulk_g2s(S.c1, C1 + tb, kC, mb);
@@ -194,13 +228,13 @@ __device__ __forceinline__ void issue(PipeStage<CT>& S, unsigned mb, const DevGr
     const CT* Cr[3] = {C0, C1, C2};
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-        float* hxd = &S.hx[r * 128 + q];
+        unsigned* hxd = &S.hx[r * 128 + q];
         if (d[r] != 0) {
             const size_t o = (size_t)((d[r] >> 3) - 1) * kCells + nl[r];
-            cp4(hxd, X + o);
+            XStore<XT>::cp_halo(hxd, X, o);
             if (side) Coef<CT>::cp_face(hc[r], Cr[r], o);
         } else {
-            *hxd = 0.0f;
+            *hxd = 0u;
             if (side) *hc[r] = Coef<CT>::word(h);
         }
     }
@@ -210,10 +244,10 @@ __device__ __forceinline__ void issue(PipeStage<CT>& S, unsigned mb, const DevGr
 // The masked snapshot of the staged tile in SX: own cells (x is 0 on cells that are not
 // INTERIOR) and the one-cell halo, GHOST faces by the T-junction rule.  Returns the
 // thread's masked quad and the plane-0 offset s0 of its first cell.
-template <typename CT>
-__device__ __forceinline__ void build_snapshot(const PipeStage<CT>& S, float* SX, const int d[3], int q, const Quad& Q, float4& xm,
+template <typename CT, typename XT>
+__device__ __forceinline__ void build_snapshot(const PipeStage<CT, XT>& S, float* SX, const int d[3], int q, const Quad& Q, float4& xm,
                                                int& s0) {
-    const float4 xr = *reinterpret_cast<const float4*>(&S.x[4 * q]);
+    const float4 xr = XStore<XT>::ld4(&S.x[4 * q]);
     const unsigned tyw = S.ty[q];
     xm.x = (tyw & 0xffu) == dInterior ? xr.x : 0.0f;
     xm.y = ((tyw >> 8) & 0xffu) == dInterior ? xr.y : 0.0f;
@@ -228,9 +262,14 @@ __device__ __forceinline__ void build_snapshot(const PipeStage<CT>& S, float* SX
     const int side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
     const int e = side ? 7 : 0, hxl = side ? 8 : -1;
     const int fx[3] = {sxp(hxl, fa, fb), sxp(fa, hxl, fb), sxp(fa, fb, hxl)};
+    // the halo cell's position in its 4-byte pair (16-bit storage): the parity of its last index
+    const int odd[3] = {fb & 1, fb & 1, side ? 0 : 1};
+    float hxv[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) hxv[r] = XStore<XT>::halo(S.hx[r * 128 + q], odd[r]);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
-        if (!(d[r] & dGhost)) SX[fx[r]] = S.hx[r * 128 + q];
+        if (!(d[r] & dGhost)) SX[fx[r]] = hxv[r];
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
@@ -248,7 +287,7 @@ __device__ __forceinline__ void build_snapshot(const PipeStage<CT>& S, float* SX
 #pragma unroll
                     for (int dk = 0; dk < 2; ++dk) avg = __fadd_rn(avg, SX[sxp(cl[0] ^ di, cl[1] ^ dj, cl[2] ^ dk)]);
             avg = __fmul_rn(avg, 0.125f);
-            SX[fx[r]] = __fmaf_rn(0.5f, __fsub_rn(S.hx[r * 128 + q], avg), SX[sxp(cl[0], cl[1], cl[2])]);
+            SX[fx[r]] = __fmaf_rn(0.5f, __fsub_rn(hxv[r], avg), SX[sxp(cl[0], cl[1], cl[2])]);
         }
     }
     __syncthreads();
@@ -260,8 +299,8 @@ struct QuadOps {
     float4 dg, a0, a1, a2, px, py;
     float pz3;
 };
-template <typename CT>
-__device__ __forceinline__ void load_ops(const PipeStage<CT>& S, int q, const Quad& Q, QuadOps& o) {
+template <typename CT, typename XT>
+__device__ __forceinline__ void load_ops(const PipeStage<CT, XT>& S, int q, const Quad& Q, QuadOps& o) {
     o.dg = Coef<CT>::ld4(&S.d[4 * q]);
     o.a0 = Coef<CT>::ld4(&S.c0[4 * q]);
     o.a1 = Coef<CT>::ld4(&S.c1[4 * q]);
@@ -297,18 +336,17 @@ __device__ __forceinline__ float quad_neg_lap(const float* SX, const QuadOps& o,
     return ax;
 }
 
-// one colour pass over the staged tile; kExact: omega is a float (the reference's form with an
-// exact double product, relax_ref)
-template <typename CT, bool kExact>
-__device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const DevGrid& g, int t, float* X, const int d[3], int q,
+// one colour pass over the staged tile; kRelax: how omega is applied (relax<>)
+template <typename CT, typename XT, int kRelax>
+__device__ __forceinline__ void process(const PipeStage<CT, XT>& S, float* SX, const DevGrid& g, int t, XT* X, const int d[3], int q,
                                         const PipeArgs& A) {
     const Quad Q(t, q);
     float4 xm;
     int s0;
     build_snapshot(S, SX, d, q, Q, xm, s0);
-    const float4 xr = *reinterpret_cast<const float4*>(&S.x[4 * q]);
+    const float4 xr = XStore<XT>::ld4(&S.x[4 * q]);
     const unsigned tyw = S.ty[q];
-    const float4 b = *reinterpret_cast<const float4*>(&S.b[4 * q]);
+    const float4 b = XStore<XT>::ld4(&S.b[4 * q]);
     QuadOps o;
     load_ops(S, q, Q, o);
     float4 out = xr;
@@ -320,24 +358,22 @@ __device__ __forceinline__ void process(const PipeStage<CT>& S, float* SX, const
         const bool in = ((tyw >> (8 * u)) & 0xffu) & dInterior;
         const float delta = in ? div_exact(__fsub_rn(f4get(b, u), ax), f4get(o.dg, u)) : 0.0f;
         const float xs = f4get(xm, u);
-        if constexpr (kExact)
-            f4set(out, u, relax_ref(xs, delta, A.om));
-        else
-            f4set(out, u, (float)((double)xs + (double)delta * A.omega));
+        f4set(out, u, relax<kRelax>(xs, delta, A.om, A.omega));
     }
-    st4(X + Q.base, out);
+    XStore<XT>::st4g(X + Q.base, out);
 }
 
 // ResidualAndRestrictAMG128Kernel (src/AMGSolver.cu:896-960) of the staged tile into its
 // parent: rhs = R * sum of the 8 children's residuals, x = their mean (0 unless the parent
 // cell is INTERIOR), summed in the order of the per-tile kernel (tile_restrict)
-__device__ __forceinline__ void process_restrict(const PipeStage<float>& S, float* SX, float* res, const DevGrid& g, int t, float* X,
-                                                 float* RHS, const int d[3], int q, float Rr) {
+template <typename XT, typename PT>
+__device__ __forceinline__ void process_restrict(const PipeStage<float, XT>& S, float* SX, float* res, const DevGrid& g, int t, PT* X,
+                                                 PT* RHS, const int d[3], int q, float Rr) {
     const Quad Q(t, q);
     float4 xm;
     int s0;
     build_snapshot(S, SX, d, q, Q, xm, s0);
-    const float4 b = *reinterpret_cast<const float4*>(&S.b[4 * q]);
+    const float4 b = XStore<XT>::ld4(&S.b[4 * q]);
     QuadOps o;
     load_ops(S, q, Q, o);
     float4 r;
@@ -363,18 +399,44 @@ __device__ __forceinline__ void process_restrict(const PipeStage<float>& S, floa
         if (p >= 0) {
             const int4 m = __ldg(g.meta + t);
             const size_t po = (size_t)p * kCells + cell_index(parent_local(m.y, f0), parent_local(m.z, f1), parent_local(m.w, f2));
-            RHS[po] = __fmul_rn(rs, Rr);
-            X[po] = (g.ctype[po] & dInterior) ? __fmul_rn(xs, 0.125f) : 0.0f;
+            XStore<PT>::st1(RHS + po, __fmul_rn(rs, Rr));
+            XStore<PT>::st1(X + po, (g.ctype[po] & dInterior) ? __fmul_rn(xs, 0.125f) : 0.0f);
         }
     }
 }
 
-// MODE 0: one red-black colour pass; MODE 1: residual and restriction into the parents
-template <typename CT, int MODE, bool kExact = true>
-__global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const float* B, PipeArgs A) {
+// FASSaveSolutionAndUpdateSource128Kernel (src/AMGSolver.cu:1176-1206) of the staged NONLEAF
+// tile: rhs += A x and x0 = x on INTERIOR cells, rhs = 0 elsewhere (the cycle's 16-bit levels)
+template <typename XT>
+__device__ __forceinline__ void process_fas(const PipeStage<float, XT>& S, float* SX, const DevGrid& g, int t, XT* RHS, XT* X0,
+                                            const int d[3], int q) {
+    const Quad Q(t, q);
+    float4 xm;
+    int s0;
+    build_snapshot(S, SX, d, q, Q, xm, s0);
+    const float4 b = XStore<XT>::ld4(&S.b[4 * q]);
+    const float4 xr = XStore<XT>::ld4(&S.x[4 * q]);
+    const unsigned tyw = S.ty[q];
+    QuadOps o;
+    load_ops(S, q, Q, o);
+    float4 rh;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const bool in = ((tyw >> (8 * u)) & 0xffu) & dInterior;
+        f4set(rh, u, in ? __fadd_rn(f4get(b, u), quad_neg_lap(SX, o, xm, s0, u)) : 0.0f);
+        if (in) XStore<XT>::st1(X0 + Q.base + u, f4get(xr, u));
+    }
+    XStore<XT>::st4g(RHS + Q.base, rh);
+}
+
+// MODE 0: one red-black colour pass; MODE 1: residual and restriction into the parents (PT:
+// the parents' x/rhs storage); MODE 2: the FAS update of NONLEAF tiles.  XT: x/rhs storage.
+template <typename CT, int MODE, int kRelax = kRelaxRef, typename XT = float, typename PT = float>
+__global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, XT* X, const XT* B, PipeArgs A) {
     extern __shared__ __align__(128) unsigned char pipe_smem[];
     __shared__ __align__(8) unsigned long long mbar[2];
-    using Smem = typename std::conditional<MODE == 0, PipeSmem<CT>, PipeSmemR>::type;
+    using Smem = typename std::conditional<MODE == 0, PipeSmem<CT, XT>, PipeSmemR<XT>>::type;
+    static_assert(MODE == 0 || std::is_same<CT, float>::value, "restriction and FAS read the float operator");
     Smem& sm = *reinterpret_cast<Smem*>(pipe_smem);
     const int q = threadIdx.x, side = q >> 6;
     const int stride = gridDim.x, tend = A.t0 + A.nt;
@@ -415,9 +477,11 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, float* X, const f
             break;
         }
         if constexpr (MODE == 0)
-            process<CT, kExact>(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
+            process<CT, XT, kRelax>(sm.st[s], sm.x, g, tcur, X, dcur, q, A);
+        else if constexpr (MODE == 1)
+            process_restrict<XT, PT>(sm.st[s], sm.x, sm.res, g, tcur, static_cast<PT*>(A.xp), static_cast<PT*>(A.rhsp), dcur, q, A.Rr);
         else
-            process_restrict(sm.st[s], sm.x, sm.res, g, tcur, X, A.rhs, dcur, q, A.Rr);
+            process_fas<XT>(sm.st[s], sm.x, g, tcur, static_cast<XT*>(A.rhsp), static_cast<XT*>(A.x0p), dcur, q);
         __syncthreads();
         if (tnext >= tend) break;
         tcur = tnext;
@@ -441,17 +505,27 @@ __global__ void k_coeff16(const float* __restrict__ C, CT* __restrict__ out, siz
 
 int g_pipe_blocks = 0;  // resident blocks of k_gs_pipe on the device
 
-template <typename CT>
-bool set_pipe_smem() {
-    return cudaFuncSetAttribute(k_gs_pipe<CT, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess &&
-           cudaFuncSetAttribute(k_gs_pipe<CT, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmem<CT>)) == cudaSuccess;
+using bf16 = __nv_bfloat16;
+
+template <typename K>
+bool set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
 }
-template <typename CT>
-void launch_pass(int blocks, cudaStream_t st, const DevGrid& g, float* X, const float* B, const PipeArgs& A) {
-    if (A.exact)
-        k_gs_pipe<CT, 0, true><<<blocks, 128, sizeof(PipeSmem<CT>), st>>>(g, X, B, A);
+template <typename CT, typename XT>
+bool set_pipe_smem() {
+    const size_t b = sizeof(PipeSmem<CT, XT>);
+    return set_smem(k_gs_pipe<CT, 0, kRelaxShort, XT>, b) && set_smem(k_gs_pipe<CT, 0, kRelaxRef, XT>, b) &&
+           set_smem(k_gs_pipe<CT, 0, kRelaxDouble, XT>, b);
+}
+template <typename CT, typename XT>
+void launch_pass(int blocks, cudaStream_t st, const DevGrid& g, XT* X, const XT* B, const PipeArgs& A) {
+    const size_t sm = sizeof(PipeSmem<CT, XT>);
+    if (A.exact == kRelaxShort)
+        k_gs_pipe<CT, 0, kRelaxShort, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
+    else if (A.exact == kRelaxRef)
+        k_gs_pipe<CT, 0, kRelaxRef, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
     else
-        k_gs_pipe<CT, 0, false><<<blocks, 128, sizeof(PipeSmem<CT>), st>>>(g, X, B, A);
+        k_gs_pipe<CT, 0, kRelaxDouble, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
 }
 int g_restrict_blocks = 0;  // resident blocks of the restriction pass
 
@@ -465,13 +539,18 @@ int gs_pipe_take_error() {
 }
 
 int gs_pipe_init() {
-    if (!set_pipe_smem<float>() || !set_pipe_smem<__nv_bfloat16>() || !set_pipe_smem<__half>()) return 0;
-    if (cudaFuncSetAttribute(k_gs_pipe<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PipeSmemR)) != cudaSuccess) return 0;
+    if (!set_pipe_smem<float, float>() || !set_pipe_smem<bf16, float>() || !set_pipe_smem<__half, float>() ||
+        !set_pipe_smem<float, bf16>() || !set_pipe_smem<bf16, bf16>() || !set_pipe_smem<__half, bf16>())
+        return 0;
+    if (!set_smem(k_gs_pipe<float, 1>, sizeof(PipeSmemR<float>)) || !set_smem(k_gs_pipe<float, 1, kRelaxRef, bf16, bf16>, sizeof(PipeSmemR<bf16>)) ||
+        !set_smem(k_gs_pipe<float, 1, kRelaxRef, bf16, float>, sizeof(PipeSmemR<bf16>)) ||
+        !set_smem(k_gs_pipe<float, 2, kRelaxRef, bf16>, sizeof(PipeSmemR<bf16>)))
+        return 0;
     int dev = 0, sms = 0, per_sm = 0, per_sm_r = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float, 0, true>, 128, sizeof(PipeSmem<float>)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_gs_pipe<float, 1>, 128, sizeof(PipeSmemR)) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_pipe<float, 0, kRelaxRef>, 128, sizeof(PipeSmem<float, float>)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, k_gs_pipe<float, 1>, 128, sizeof(PipeSmemR<float>)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -492,49 +571,133 @@ void launch_coeff16(const DevGrid& g, int coeff_ch, int storage, void* out, cuda
         k_coeff16<__half><<<blocks, 256, 0, st>>>(g.plane(coeff_ch), static_cast<__half*>(out), n);
 }
 
-void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st,
-                    int storage, const void* coeff16) {
+void launch_gs_pipe(const DevGrid& g, int t0, int nt, void* X, const void* B, bool x16, int coeff_ch, int color, double omega,
+                    cudaStream_t st, int storage, const void* coeff16) {
     if (nt <= 0) return;
-    PipeArgs A;
+    PipeArgs A = {};
     A.t0 = t0;
     A.nt = nt;
     A.color = color;
     A.om = (float)omega;
-    A.exact = ((double)A.om == omega);
+    A.exact = relax_mode(omega);
     A.omega = omega;
     A.cstride = (size_t)g.n * kCells;
-    A.rhs = nullptr;
     A.Rr = 1.0f;
+    A.coef = storage == kStorageFP32 ? (const void*)g.plane(coeff_ch) : coeff16;
     const int blocks = nt < g_pipe_blocks ? nt : g_pipe_blocks;
     note_kernel_launch();
-    if (storage == kStorageFP32) {
-        A.coef = g.plane(coeff_ch);
-        launch_pass<float>(blocks, st, g, X, B, A);
-    } else if (storage == kStorageBF16) {
-        A.coef = coeff16;
-        launch_pass<__nv_bfloat16>(blocks, st, g, X, B, A);
+    if (!x16) {
+        float* Xf = static_cast<float*>(X);
+        const float* Bf = static_cast<const float*>(B);
+        if (storage == kStorageFP32) launch_pass<float>(blocks, st, g, Xf, Bf, A);
+        else if (storage == kStorageBF16) launch_pass<bf16>(blocks, st, g, Xf, Bf, A);
+        else launch_pass<__half>(blocks, st, g, Xf, Bf, A);
     } else {
-        A.coef = coeff16;
-        launch_pass<__half>(blocks, st, g, X, B, A);
+        bf16* Xh = static_cast<bf16*>(X);
+        const bf16* Bh = static_cast<const bf16*>(B);
+        if (storage == kStorageFP32) launch_pass<float>(blocks, st, g, Xh, Bh, A);
+        else if (storage == kStorageBF16) launch_pass<bf16>(blocks, st, g, Xh, Bh, A);
+        else launch_pass<__half>(blocks, st, g, Xh, Bh, A);
     }
 }
 
-void launch_restrict_pipe(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st) {
+void launch_restrict_pipe(const DevGrid& g, int t0, int nt, const void* X, const void* B, bool x16, void* Xp, void* RHSp, bool p16,
+                          int coeff_ch, float Rr, cudaStream_t st) {
     if (nt <= 0) return;
-    PipeArgs A;
+    PipeArgs A = {};
     A.t0 = t0;
     A.nt = nt;
-    A.color = 0;
+    A.exact = kRelaxRef;
     A.om = 1.0f;
-    A.exact = 1;
     A.omega = 1.0;
     A.coef = g.plane(coeff_ch);
     A.cstride = (size_t)g.n * kCells;
-    A.rhs = RHS;
+    A.xp = Xp;
+    A.rhsp = RHSp;
     A.Rr = Rr;
     const int blocks = nt < g_restrict_blocks ? nt : g_restrict_blocks;
     note_kernel_launch();
-    k_gs_pipe<float, 1><<<blocks, 128, sizeof(PipeSmemR), st>>>(g, X, RHS, A);
+    if (!x16) {
+        k_gs_pipe<float, 1><<<blocks, 128, sizeof(PipeSmemR<float>), st>>>(g, (float*)X, (const float*)B, A);
+    } else if (p16) {
+        k_gs_pipe<float, 1, kRelaxRef, bf16, bf16><<<blocks, 128, sizeof(PipeSmemR<bf16>), st>>>(g, (bf16*)X, (const bf16*)B, A);
+    } else {
+        k_gs_pipe<float, 1, kRelaxRef, bf16, float><<<blocks, 128, sizeof(PipeSmemR<bf16>), st>>>(g, (bf16*)X, (const bf16*)B, A);
+    }
+}
+
+namespace {
+__device__ __forceinline__ float ldx(const float* p) { return *p; }
+__device__ __forceinline__ float ldx(const bf16* p) { return __bfloat162float(*p); }
+// FASProlongateAndUpdateAMG128Kernel (src/AMGSolver.cu:1216-1248) on a level whose x is BF16;
+// the parent level's x and saved x are BF16 or float (PT)
+template <typename PT>
+__global__ void __launch_bounds__(128) k_prolong_x16(DevGrid g, int t0, bf16* X, const PT* Xc, const PT* X0c, float P) {
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    const int4 m = g.meta[t];
+    const bool ghost = (m.x >> 8) & dGhost;
+    const int p = g.nb[8 * t + 6];
+    const float4 xr = XStore<bf16>::ld4(X + Q.base);
+    const uchar4 ty = ldt4(g.ctype + Q.base);
+    const int pi = parent_local(m.y, Q.i), pj = parent_local(m.z, Q.j);
+    float4 out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        float cx = 0.0f, cx0 = 0.0f;
+        if (p >= 0) {
+            const size_t o = (size_t)p * kCells + cell_index(pi, pj, parent_local(m.w, Q.k0 + u));
+            cx = ldx(Xc + o);
+            cx0 = ldx(X0c + o);
+        }
+        const bool in = t4get(ty, u) & dInterior;
+        f4set(out, u, ghost ? (in ? cx : 0.0f) : (in ? __fmaf_rn(P, __fsub_rn(cx, cx0), f4get(xr, u)) : 0.0f));
+    }
+    XStore<bf16>::st4g(X + Q.base, out);
+}
+// the cycle's right-hand side in BF16 on the given LEAF tiles, and the cycle's result back
+__global__ void __launch_bounds__(128) k_leaf_to_bf16(const int* leaf, const float* R, bf16* R16) {
+    const size_t base = (size_t)leaf[blockIdx.x] * kCells + 4 * threadIdx.x;
+    XStore<bf16>::st4g(R16 + base, *reinterpret_cast<const float4*>(R + base));
+}
+__global__ void __launch_bounds__(128) k_leaf_from_bf16(const int* leaf, const bf16* X16, float* Z) {
+    const size_t base = (size_t)leaf[blockIdx.x] * kCells + 4 * threadIdx.x;
+    st4(Z + base, XStore<bf16>::ld4(X16 + base));
+}
+}  // namespace
+
+void launch_prolong_x16(const DevGrid& g, int t0, int nt, void* X, const void* Xc, const void* X0c, bool p16, float P, cudaStream_t st) {
+    if (nt <= 0) return;
+    note_kernel_launch();
+    if (p16) k_prolong_x16<bf16><<<nt, 128, 0, st>>>(g, t0, (bf16*)X, (const bf16*)Xc, (const bf16*)X0c, P);
+    else k_prolong_x16<float><<<nt, 128, 0, st>>>(g, t0, (bf16*)X, (const float*)Xc, (const float*)X0c, P);
+}
+void launch_leaf_to_bf16(const int* leaf, int nleaf, const float* R, void* R16, cudaStream_t st) {
+    if (nleaf <= 0) return;
+    note_kernel_launch();
+    k_leaf_to_bf16<<<nleaf, 128, 0, st>>>(leaf, R, (bf16*)R16);
+}
+void launch_leaf_from_bf16(const int* leaf, int nleaf, const void* X16, float* Z, cudaStream_t st) {
+    if (nleaf <= 0) return;
+    note_kernel_launch();
+    k_leaf_from_bf16<<<nleaf, 128, 0, st>>>(leaf, (const bf16*)X16, Z);
+}
+
+void launch_fas_pipe_x16(const DevGrid& g, int t0, int nt, const void* X, void* RHS, void* X0, int coeff_ch, cudaStream_t st) {
+    if (nt <= 0) return;
+    PipeArgs A = {};
+    A.t0 = t0;
+    A.nt = nt;
+    A.exact = kRelaxRef;
+    A.om = 1.0f;
+    A.omega = 1.0;
+    A.coef = g.plane(coeff_ch);
+    A.cstride = (size_t)g.n * kCells;
+    A.rhsp = RHS;
+    A.x0p = X0;
+    const int blocks = nt < g_restrict_blocks ? nt : g_restrict_blocks;
+    note_kernel_launch();
+    k_gs_pipe<float, 2, kRelaxRef, bf16><<<blocks, 128, sizeof(PipeSmemR<bf16>), st>>>(g, (bf16*)X, (const bf16*)RHS, A);
 }
 
 }  // namespace cmg

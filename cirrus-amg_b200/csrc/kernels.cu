@@ -79,7 +79,7 @@ __device__ __forceinline__ void tile_gs(const DevGrid& g, int t, int tid, float*
         const float ax = own_neg_lap(S, Q, o, u);
         const float delta = (t4get(o.ty, u) & dInterior) ? div_exact(__fsub_rn(f4get(b, u), ax), d) : 0.0f;
         const float xs = f4get(o.xm, u);
-        f4set(out, u, A.exact ? relax_ref(xs, delta, A.om) : (float)((double)xs + (double)delta * A.omega));
+        f4set(out, u, relax_rt(A.exact, xs, delta, A.om, A.omega));
     }
     st4(X + Q.base, out);
     sync();
@@ -240,7 +240,7 @@ struct DenseLevel {
             const float ax = neg_lap(i, j, k);
             const float delta = (ty[c] & dInterior) ? div_exact(__fsub_rn(rhs[c], ax), d[c]) : 0.0f;
             const float xs = x[xi(i, j, k)];
-            x[xi(i, j, k)] = A.exact ? relax_ref(xs, delta, A.om) : (float)((double)xs + (double)delta * A.omega);
+            x[xi(i, j, k)] = relax_rt(A.exact, xs, delta, A.om, A.omega);
         }
         __syncthreads();
     }
@@ -1174,7 +1174,8 @@ __device__ __forceinline__ float make_float(unsigned long long r, int emin, int 
     return __uint_as_float(sign | ((unsigned)(e + 127) << 23) | ((unsigned)r & 0x7fffffu));
 }
 // Compares div_by_recip (with the correctly rounded reciprocal) and div_exact
-// (with the Newton-refined one) with the IEEE division on pseudo-random pairs: a quarter
+// (with the Newton-refined one) with the IEEE division, and relax_short with relax_ref,
+// on pseudo-random pairs.  Division pairs: a quarter
 // uniform in sign, exponent and significand; a quarter built to fall within a few
 // ulps of a midpoint between two floats (a = RN(d * m) for a midpoint m); a quarter
 // shaped like Gauss-Seidel updates; a quarter of zeros, subnormals, huge values,
@@ -1218,6 +1219,49 @@ __global__ void k_check_division(long long n, unsigned long long seed, unsigned 
                 first[1] = __float_as_uint(d);
             }
         }
+        // the relaxation: relax_short against relax_ref for omegas of at most three significant
+        // bits, on pairs (x, delta): uniform; delta * omega within a few ulps of k half-ulps of
+        // x (sums near a float midpoint); delta * omega an exact midpoint with x tiny (where the
+        // double rounding matters); zeros, subnormals and non-finite values
+        {
+            const float oms[6] = {1.5f, 1.0f, 1.25f, 1.75f, 0.75f, 3.0f};
+            const unsigned long long r3 = mix64(r2), r4 = mix64(r3);
+            const float om = oms[r4 % 6ull];
+            float x, dl;
+            switch ((int)((i >> 2) & 3)) {
+                case 0:
+                    x = make_float(r3, -40, 40);
+                    dl = make_float(r4, -40, 40);
+                    break;
+                case 1: {
+                    x = make_float(r3, -20, 20);
+                    const double ulp = (double)nextafterf(fabsf(x), INFINITY) - (double)fabsf(x);
+                    const double k = 0.5 * (double)((r4 >> 8) % 7ull + 1ull) * (((r4 >> 16) & 1ull) ? 1.0 : -1.0);
+                    dl = __double2float_rn(k * ulp / (double)om);
+                    const int off = (int)((r4 >> 20) % 5ull) - 2;
+                    for (int q = 0; q < (off < 0 ? -off : off); ++q) dl = nextafterf(dl, off < 0 ? -INFINITY : INFINITY);
+                    break;
+                }
+                case 2: {
+                    dl = __uint_as_float(__float_as_uint(make_float(r3, -10, 10)) | 1u);  // odd significand
+                    const int ed = (int)((__float_as_uint(dl) >> 23) & 0xffu) - 127;
+                    x = make_float(r4, ed - 80, ed - 20);
+                    break;
+                }
+                default: {
+                    const float pool[10] = {0.0f, -0.0f, 1e-45f, -3e-39f, 1.17549435e-38f, 3.0e38f, INFINITY, -INFINITY, NAN, 1.0f};
+                    x = (r4 & 1) ? pool[r3 % 10] : make_float(r3, -126, 127);
+                    dl = (r4 & 2) ? pool[(r3 >> 8) % 10] : make_float(r4, -126, 127);
+                }
+            }
+            const float rw = relax_ref(x, dl, om), rg = relax_short(x, dl, om);
+            if (!((__float_as_uint(rw) == __float_as_uint(rg)) || (isnan(rw) && isnan(rg)))) {
+                if (atomicAdd(mism, 1ull) == 0ull) {
+                    first[0] = __float_as_uint(x);
+                    first[1] = __float_as_uint(dl);
+                }
+            }
+        }
     }
 }
 }  // namespace
@@ -1254,7 +1298,7 @@ void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int c
     SmoothArgs A;
     A.coeff_ch = coeff_ch;
     A.om = (float)omega;
-    A.exact = ((double)A.om == omega);
+    A.exact = relax_mode(omega);
     A.omega = omega;
     count_launch(), k_gs<<<nt, 128, 0, st>>>(g, t0, X, B, color, A);
 }
@@ -1277,7 +1321,7 @@ void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* 
     A.level_iters = level_iters;
     A.coarsest_iters = coarsest_iters;
     A.om = (float)omega;
-    A.exact = ((double)A.om == omega);
+    A.exact = relax_mode(omega);
     A.omega = omega;
     A.Rr = Rr;
     A.P = P;
@@ -1352,7 +1396,7 @@ cudaError_t launch_persist_step(const DevGrid& g, int top, const int* lb, const 
     A.coarsest_iters = coarsest_iters;
     A.sm.coeff_ch = coeff_ch;
     A.sm.om = (float)omega;
-    A.sm.exact = ((double)A.sm.om == omega);
+    A.sm.exact = relax_mode(omega);
     A.sm.omega = omega;
     A.co.top = 1;
     A.co.coeff_ch = coeff_ch;

@@ -49,8 +49,8 @@ int gs_pipe_take_error();
 // Storage of the operator planes the pipelined smoother reads: the float channels, or a
 // BF16 / FP16 copy (coeff16: four planes of num_tiles*512 elements, made by launch_coeff16).
 constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;
-void launch_gs_pipe(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st,
-                    int storage = kStorageFP32, const void* coeff16 = nullptr);
+void launch_gs_pipe(const DevGrid& g, int t0, int nt, void* X, const void* B, bool x16, int coeff_ch, int color, double omega,
+                    cudaStream_t st, int storage, const void* coeff16);
 size_t coeff16_bytes(const DevGrid& g);
 // learned finest-level smoother: per-tile conv net, hidden width H = 8 or 16 (learned.cu)
 int net_params(int H);      // fp32 parameters
@@ -73,7 +73,17 @@ void launch_dot_flex(const DevGrid& g, const int* leaf, int nleaf, const float* 
                      cudaStream_t st);
 // ResidualAndRestrictAMG128Kernel on tiles t0..t0+nt-1 with the same prefetching pipeline
 // (x masked to INTERIOR cells, as inside the cycle); equals launch_restrict bit for bit.
-void launch_restrict_pipe(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float Rr, cudaStream_t st);
+// residual and restriction of the tiles t0..t0+nt into their parents: x and b of the tiles in
+// float or BF16 (x16), the parents' x and rhs planes Xp/RHSp in float or BF16 (p16)
+void launch_restrict_pipe(const DevGrid& g, int t0, int nt, const void* X, const void* B, bool x16, void* Xp, void* RHSp, bool p16,
+                          int coeff_ch, float Rr, cudaStream_t st);
+// the mixed-precision cycle's BF16 levels: FAS update of NONLEAF tiles (rhs += A x, x0 = x),
+// prolongation from a parent level in BF16 (p16) or float, and the conversions of the
+// finest right-hand side and result on the given LEAF tiles
+void launch_fas_pipe_x16(const DevGrid& g, int t0, int nt, const void* X, void* RHS, void* X0, int coeff_ch, cudaStream_t st);
+void launch_prolong_x16(const DevGrid& g, int t0, int nt, void* X, const void* Xc, const void* X0c, bool p16, float P, cudaStream_t st);
+void launch_leaf_to_bf16(const int* leaf, int nleaf, const float* R, void* R16, cudaStream_t st);
+void launch_leaf_from_bf16(const int* leaf, int nleaf, const void* X16, float* Z, cudaStream_t st);
 void launch_coeff16(const DevGrid& g, int coeff_ch, int storage, void* out, cudaStream_t st);
 void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int coeff_ch, int color, double omega, cudaStream_t st);
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float R_restrict, cudaStream_t st);

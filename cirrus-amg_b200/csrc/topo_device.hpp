@@ -1,0 +1,35 @@
+// Octree refinement, ghost spawning and the canonical tables built on the device
+// (topo_device.cu) for the built-in refinement targets.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "topology.hpp"
+
+namespace cmg {
+
+constexpr int kDevTopoMaxParams = 64;
+
+// Device work space of the builder: tile pool, hash table, sort buffers (grow-only).
+struct DeviceTopoBuilder {
+    int cap = 0;         // tile records
+    unsigned hcap = 0;   // hash slots (power of two, at least twice cap)
+    unsigned long long *hk = nullptr, *keys = nullptr, *keys2 = nullptr;
+    int *hv = nullptr, *type0 = nullptr, *flag = nullptr, *idx = nullptr, *idx2 = nullptr, *nb = nullptr, *child = nullptr;
+    int* scal = nullptr;
+    int4 *rec = nullptr, *rec2 = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    cudaError_t reserve(int tiles);
+    void release();
+    ~DeviceTopoBuilder();
+};
+
+// Cases the device builder computes exactly as the host (case_target): 0-3, 6, 7.
+bool device_case_supported(int case_id);
+// Topology::iterative_refine with case_target, then the ghost layer and the canonical
+// order and tables, on the device; the result is adopted by `topo`.  0 on success, 1 for
+// an unsupported case or bad parameters, 2 for a CUDA error.
+int device_refine_case(DeviceTopoBuilder& B, Topology& topo, int case_id, const double* params, int nparams, cudaStream_t st,
+                       int* steps);
+
+}  // namespace cmg

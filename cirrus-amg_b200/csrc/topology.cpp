@@ -14,14 +14,24 @@ uint64_t Topology::key(int level, int i, int j, int k) {
            ((uint64_t)((j + 4) & 0x3ffff) << 18) | (uint64_t)((k + 4) & 0x3ffff);
 }
 
+void Topology::ensure_index() const {
+    if (!index_stale_) return;
+    index_.clear();
+    index_.reserve(2 * tiles_.size() + 16);
+    for (int t = 0; t < (int)tiles_.size(); ++t) index_.emplace(key(tiles_[t].level, tiles_[t].c[0], tiles_[t].c[1], tiles_[t].c[2]), t);
+    index_stale_ = false;
+}
+
 int Topology::find(int level, int i, int j, int k) const {
     if (level < 0 || level >= num_levels_) return -1;
+    ensure_index();
     auto it = index_.find(key(level, i, j, k));
     return it == index_.end() ? -1 : it->second;
 }
 
 int Topology::set(int level, int i, int j, int k, int type) {
     if (level < 0 || level >= num_levels_) return -1;
+    ensure_index();
     uint64_t kk = key(level, i, j, k);
     auto it = index_.find(kk);
     if (it != index_.end()) {
@@ -176,6 +186,22 @@ std::vector<int> Topology::canonicalize() {
         for (int ci = 0; ci < 8; ++ci)
             child[8 * t + ci] = find(tr.level + 1, 2 * tr.c[0] + (ci >> 2), 2 * tr.c[1] + ((ci >> 1) & 1), 2 * tr.c[2] + (ci & 1));
     }
+    set_ranges();
+    return order;
+}
+
+void Topology::adopt(std::vector<TileRec>&& sorted, std::vector<int>&& nb_table, std::vector<int>&& child_table) {
+    tiles_ = std::move(sorted);
+    nb = std::move(nb_table);
+    child = std::move(child_table);
+    index_.clear();
+    index_stale_ = true;
+    update_max_level();
+    set_ranges();
+}
+
+void Topology::set_ranges() {
+    const int n = (int)tiles_.size();
     level_begin.assign(num_levels_, n);
     level_end.assign(num_levels_, n);
     nonleaf_begin.assign(num_levels_, n);
@@ -196,7 +222,6 @@ std::vector<int> Topology::canonicalize() {
         nonleaf_begin[L] = nlb;
         ghost_begin[L] = gb;
     }
-    return order;
 }
 
 // ---------------------------------------------------------------------------

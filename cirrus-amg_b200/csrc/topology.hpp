@@ -39,6 +39,9 @@ public:
     // Sort tiles by (level, type, Morton) and build the device tables.
     // Returns, for every tile in the new order, the tile's old index.
     std::vector<int> canonicalize();
+    // Take a tile list already in canonical order with its nb / child tables (built
+    // elsewhere, e.g. on the device) and derive the level ranges and the LEAF list.
+    void adopt(std::vector<TileRec>&& sorted, std::vector<int>&& nb_table, std::vector<int>&& child_table);
 
     // tables (valid after canonicalize)
     std::vector<int> nb;     // [n][8]: -x,-y,-z,+x,+y,+z, parent, -1
@@ -56,8 +59,12 @@ private:
     float h0_;
     int num_levels_;
     int max_level_ = -1;
+    void ensure_index() const;
+    void set_ranges();
+
     std::vector<TileRec> tiles_;
-    std::unordered_map<uint64_t, int> index_;
+    mutable std::unordered_map<uint64_t, int> index_;
+    mutable bool index_stale_ = false;  // adopt() leaves the key index to be rebuilt on first use
 };
 
 // Built-in refinement targets and LEAF cell types (tests/TestGrids.cuh).

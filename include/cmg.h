@@ -66,13 +66,15 @@ typedef int (*cmg_level_target_fn)(void* user, int level, int i, int j, int k);
 
 const char* cmg_last_error(void);
 int cmg_version(void);
-/* Self-check of the division the Gauss-Seidel sweeps use (one double multiply
- * by a double reciprocal of the divisor, rounded to float; the reciprocal either
- * correctly rounded or refined by Newton steps) against the IEEE float
- * division, on n pseudo-random pairs from `seed`.  mismatches
- * receives the number of results that differ in any bit; first_pair (may be
- * NULL) the bit patterns of the first differing (a, d).  No counterpart in the
- * reference, which divides directly (src/AMGSolver.cu:868-875). */
+/* Self-check of the arithmetic the Gauss-Seidel sweeps use in place of the reference's
+ * expressions (src/AMGSolver.cu:868-875): the division (one double multiply by a double
+ * reciprocal of the divisor, rounded to float; the reciprocal either correctly rounded or
+ * refined by Newton steps) against the IEEE float division, and the relaxation
+ * x + delta * omega by one float fused multiply-add where that is provably the same
+ * against the reference's double evaluation, for omegas of at most three significant
+ * bits; on n pseudo-random pairs of each from `seed`.  mismatches receives the number of
+ * results that differ in any bit; first_pair (may be NULL) the bit patterns of the first
+ * differing pair.  No counterpart in the reference. */
 int cmg_check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair);
 
 /* ---- grid: HADeviceGrid ------------------------------------------------ */
@@ -91,6 +93,14 @@ int cmg_grid_rebuild(cmg_grid* g);
 /* iterativeRefine (src/HAGrid.h:1173) with a host callback or a built-in case. */
 int cmg_grid_iterative_refine(cmg_grid* g, cmg_level_target_fn fn, void* user, int* steps);
 int cmg_grid_refine_case(cmg_grid* g, int case_id, const double* params, int nparams, int* steps);
+/* The same refinement as cmg_grid_refine_case, then the ghost layer, the canonical tile
+ * order and the index tables, all built in device memory on the grid's stream: a tile pool
+ * with an atomic counter, an open-addressing hash of tile keys, two kernels per level for
+ * refineStep's flags and the new tiles (src/HAGrid.h:1088-1170; the reference does that
+ * part on the host), one for spawnGhostTiles (:856-889) and a radix sort for the order.
+ * The result equals cmg_grid_refine_case's tile for tile.  Cases 0-3, 6 and 7; the star
+ * cases (4, 5), whose targets use transcendental functions, are refined on the host. */
+int cmg_grid_refine_case_device(cmg_grid* g, int case_id, const double* params, int nparams, int* steps);
 /* numTotalTiles / mMaxLevel (src/HAGrid.h:504, 366) */
 int cmg_grid_info(cmg_grid* g, int* num_tiles, int* max_level, int* num_leaf_tiles);
 /* tile list in device order: level[n], ijk[3n], type[n] (host buffers) */
@@ -229,6 +239,13 @@ int cmg_amg_solver_residual_replacements(cmg_amg_solver* s, int* count);
  * is formed from an FP64 Cholesky factor on the host when the operator changes, and applied
  * on the device.  Other octrees keep the sweeps. */
 int cmg_amg_solver_set_coarsest_direct(cmg_amg_solver* s, int on);
+/* BF16 storage of the preconditioner's grids (mixed-precision mode; no counterpart in the
+ * reference): with on != 0, x, rhs and the saved FAS x of levels >= 3 live in BF16 planes
+ * and every sweep, restriction, FAS update and prolongation there reads and writes BF16,
+ * computing in FP32; levels 0-2 and the outer PCG stay FP32.  The right-hand side enters
+ * rounded to BF16 and z leaves widened from it.  Needs the pipelined smoother (the default
+ * launch mode) and is ignored by the learned solve. */
+int cmg_amg_solver_set_cycle_bf16(cmg_amg_solver* s, int on);
 /* Launch flags (default CMG_LAUNCH_GRAPH).
  * GRAPH: the solve runs as one CUDA graph with a device-side while loop;
  * without it the same kernels are launched one by one with the loop test on

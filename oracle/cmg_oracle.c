@@ -24,6 +24,16 @@
 #endif
 
 #define NC 512
+/* nearest BF16 (ties to even), as a float: the storage of the mixed-precision cycle's x and
+ * rhs on levels >= 3 (finite values) */
+static float bf16_round(float v) {
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    memcpy(&v, &u, 4);
+    return v;
+}
+#define XS(g, level, v) (((g)->x_bf16 && (level) >= 3) ? bf16_round(v) : (v))
 #define CELL(i, j, k) (((i) << 6) | ((j) << 3) | (k))
 #define SX(i, j, k) (((i) + 1) * 100 + ((j) + 1) * 10 + ((k) + 1))
 
@@ -48,6 +58,7 @@ struct og_grid {
     float* data;
     uint8_t* ctype;
     int ref_mask; /* apply CoarsenOffDiagCoefficientsOneStepKernel's cell-type mask to the stored types */
+    int x_bf16;   /* the mixed-precision cycle: x and rhs of levels >= 3 stored in BF16 */
 };
 
 /* ------------------------------------------------------------------ */
@@ -479,6 +490,7 @@ static void ghost_types_from_parents(og_grid* g) { /* AMGSolver.cu:265-274, Mesh
 }
 
 void og_set_reference_mask(og_grid* g, int on) { g->ref_mask = on; }
+void og_set_x_bf16(og_grid* g, int on) { g->x_bf16 = on; }
 
 /* PrepareLaplacianSystemFromLeafAndGhostCellTypesAndFaceCoeffs (AMGSolver.cu:89-254) */
 void og_prepare_system(og_grid* g, int coeff_ch, float R) {
@@ -886,11 +898,11 @@ static void gs_pass(og_grid* g, int level, int color, int x_ch, int coeff_ch, in
                 uint8_t ct = CT(g, t)[v];
                 float Ax = snap_neg_lap(S, v);
                 float D = S->d[v];
-                float delta = (ct & OG_INTERIOR) ? (B[v] - Ax) / D : 0.0f;
+                float delta = (ct & OG_INTERIOR) ? (XS(g, level, B[v]) - Ax) / D : 0.0f;
                 float xs = S->x[SX(i, j, k)];
                 /* AMGSolver.cu:874: x + delta * omega with omega a double holding a float: the
                  * product is exact in double, the sum rounds to double, then to float */
-                X[v] = exact ? (float)fma((double)delta, (double)om, (double)xs) : (float)((double)xs + (double)delta * omega);
+                X[v] = XS(g, level, exact ? (float)fma((double)delta, (double)om, (double)xs) : (float)((double)xs + (double)delta * omega));
             }
         }
         free(S);
@@ -914,7 +926,7 @@ void og_residual_restrict(og_grid* g, int level, int x_ch, int coeff_ch, int rhs
             if (!is_active_at(g, t, level)) continue;
             int p = g->parent[t];
             load_snap(g, t, x_ch, coeff_ch, S);
-            for (int v = 0; v < NC; v++) res[v] = CH(g, rhs_ch, t)[v] - snap_neg_lap(S, v);
+            for (int v = 0; v < NC; v++) res[v] = XS(g, level, CH(g, rhs_ch, t)[v]) - snap_neg_lap(S, v);
             if (p < 0) continue;
             for (int b = 0; b < 64; b++) {
                 int fl[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
@@ -926,8 +938,8 @@ void og_residual_restrict(og_grid* g, int level, int x_ch, int coeff_ch, int rhs
                             xs += S->x[SX(fl[0] + ii, fl[1] + jj, fl[2] + kk)];
                         }
                 int cv = parent_cell(g, t, CELL(fl[0], fl[1], fl[2]));
-                CH(g, rhs_ch, p)[cv] = rs * R_restrict;
-                CH(g, x_ch, p)[cv] = xs / 8;
+                CH(g, rhs_ch, p)[cv] = XS(g, level - 1, rs * R_restrict);
+                CH(g, x_ch, p)[cv] = XS(g, level - 1, xs / 8);
             }
         }
         free(S);
@@ -947,7 +959,7 @@ void og_fas_save(og_grid* g, int level, int x_ch, int coeff_ch, int rhs_ch, int 
             for (int v = 0; v < NC; v++) lap[v] = snap_neg_lap(S, v);
             for (int v = 0; v < NC; v++) {
                 if (CT(g, t)[v] & OG_INTERIOR) {
-                    CH(g, rhs_ch, t)[v] = CH(g, rhs_ch, t)[v] + lap[v];
+                    CH(g, rhs_ch, t)[v] = XS(g, level, XS(g, level, CH(g, rhs_ch, t)[v]) + lap[v]);
                     CH(g, x0_ch, t)[v] = CH(g, x_ch, t)[v];
                 } else CH(g, rhs_ch, t)[v] = 0.0f;
             }
@@ -972,8 +984,8 @@ void og_fas_prolong(og_grid* g, int level, int x_ch, int x0_ch, float P) {
                 cx0 = CH(g, x0_ch, p)[pv];
             }
             int in = CT(g, t)[v] & OG_INTERIOR;
-            if (ghost) X[v] = in ? cx : 0.0f;
-            else X[v] = in ? fmaf(P, cx - cx0, X[v]) : 0.0f;
+            if (ghost) X[v] = in ? XS(g, level, cx) : 0.0f;
+            else X[v] = in ? XS(g, level, fmaf(P, cx - cx0, X[v])) : 0.0f;
         }
     }
 }

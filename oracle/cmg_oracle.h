@@ -111,6 +111,9 @@ void og_case_types_at(float h0, int case_id, int level, int i, int j, int k, uin
  * types the grid holds at that point (NONLEAF types included); 0 (default):
  * the mask is open */
 void og_set_reference_mask(og_grid* g, int on);
+/* 1: the mixed-precision cycle -- x and rhs of levels >= 3 held in BF16 (every write there
+ * rounded to BF16; the finest right-hand side read through its BF16 copy) */
+void og_set_x_bf16(og_grid* g, int on);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,7 @@ def lib():
             "og_case_target_at": (I, [F, I, P, I, I, I, I, I]),
             "og_case_types_at": (None, [F, I, I, I, I, I, P]),
             "og_set_reference_mask": (None, [P, I]),
+            "og_set_x_bf16": (None, [P, I]),
             "og_refine_fn": (I, [P, TARGET_FN, P]),
         }
         for name, (res, args) in sig.items():
@@ -127,6 +128,9 @@ class Grid:
 
     def set_reference_mask(self, on):
         self.L.og_set_reference_mask(self.g, int(bool(on)))
+
+    def set_x_bf16(self, on):
+        self.L.og_set_x_bf16(self.g, int(bool(on)))
 
     @property
     def n(self):

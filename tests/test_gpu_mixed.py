@@ -162,17 +162,45 @@ def test_direct_coarsest_solve(grid):
 
 
 def test_mixed_mode_on_the_sphere_octree():
-    """Config 3's whole mixed mode on the 3/4/5 sphere octree: BF16 operator storage, true
-    residual every 10 iterations and the direct coarsest solve, against the FP64 solution."""
+    """Config 3's whole mixed mode on the 3/4/5 sphere octree: BF16 operator, x and rhs storage,
+    true residual every 10 iterations and the direct coarsest solve, against the FP64 solution."""
     from test_gpu_parity import fp64_solution
 
     G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5))
     b = G.download(1)
     g.channel(1)[:] = b
     solver.set_storage("bf16")
+    solver.set_cycle_bf16(True)
     solver.set_residual_replacement(10)
     solver.set_coarsest_direct(True)
     it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
     assert rel <= 1e-6
     xs, rt, rc = fp64_solution(g, b, 1)
     assert _rel_l2(G.download(0)[rt, rc], xs) <= 1e-5
+
+
+@pytest.mark.parametrize("grid", ["uniform64", "shell345"])
+def test_bf16_cycle_storage_matches_the_oracle(grid):
+    """x, rhs and saved x of levels >= 3 in BF16 planes (FP32 arithmetic): the solve follows the
+    oracle run with the same roundings (og_set_x_bf16) to +-1 iteration and 1e-5, and the FP64
+    solution to 1e-5, in the iteration count of the FP32 cycle within one."""
+    from test_gpu_parity import fp64_solution
+
+    if grid == "uniform64":
+        G, g, solver, b = setup_uniform(3)
+    else:
+        G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5))
+        b = G.download(1)
+        g.channel(1)[:] = b
+    it32, _ = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    G.upload(1, b)
+    solver.set_cycle_bf16(True)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    x = G.download(0)
+    g.set_x_bf16(True)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    assert rel <= 1e-6 and abs(it - ito) <= 1 and abs(it - it32) <= 1, (it, ito, it32)
+    m = G.tiles()[2] == cmg.LEAF
+    assert _rel_l2(x[m], g.channel(0)[m]) <= 1e-5
+    xs, rt, rc = fp64_solution(g, b, 0 if grid == "uniform64" else 1)
+    assert _rel_l2(x[rt, rc], xs) <= 1e-5

@@ -428,3 +428,23 @@ def test_learned_oracle_reproduces_golden():
     assert np.allclose(fwd, d["forward"], rtol=1e-5, atol=1e-6 * np.abs(d["forward"]).max())
     assert abs(loss - float(d["loss"])) <= 1e-9 * abs(float(d["loss"]))
     assert np.allclose(grad, d["grad"], rtol=1e-5, atol=1e-6 * np.abs(d["grad"]).max())
+
+
+def test_oracle_bf16_cycle_storage_converges_like_fp32():
+    """The mixed-precision cycle of the oracle (x and rhs of levels >= 3 rounded to BF16 at
+    every write) on uniform 64^3: the iterations of the FP32 cycle within one, the FP32
+    solution within 1e-5."""
+    from workloads import build_oracle, uniform_rhs
+
+    g = build_oracle(O.CASE_UNIFORM, [3, 3])
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    b = uniform_rhs(g.tiles()[2] == O.LEAF, 0)
+    g.channel(1)[:] = b
+    it0, rel0 = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    x0 = g.channel(0).copy()
+    g.channel(1)[:] = b
+    g.set_x_bf16(True)
+    it1, rel1 = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    assert rel1 <= 1e-6 and abs(it1 - it0) <= 1
+    assert np.linalg.norm((g.channel(0) - x0).astype(np.float64)) <= 1e-5 * np.linalg.norm(x0.astype(np.float64))
