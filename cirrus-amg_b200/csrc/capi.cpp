@@ -253,6 +253,11 @@ int cmg_grid_set_leaf_cell_types_case(cmg_grid* g, int case_id, const double* pa
     (void)params;
     (void)nparams;
     if (!grid_ready(g)) return fail(CMG_ERR_STATE, "grid not built");
+    if (cmg::device_cell_types_supported(case_id)) {
+        cmg::Grid& G = g->g;
+        return cmg::check_cuda(cmg::device_leaf_cell_types(G.meta, G.ctype, G.leaf, G.nleaf, case_id, G.topo.h0(), G.stream),
+                               "cmg_grid_set_leaf_cell_types_case");
+    }
     const int n = g->g.n;
     std::vector<uint8_t> ty((size_t)n * 512);
     CKC(cudaMemcpy(ty.data(), g->g.ctype, ty.size(), cudaMemcpyDeviceToHost));

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <unordered_map>
 
 namespace cmg {
@@ -32,9 +33,53 @@ static void dfree(T*& p) {
     p = nullptr;
 }
 
+// The channel planes and cell types of grids come from a stream-ordered pool per device
+// that keeps freed memory: an octree rebuilt for every position of a moving obstacle (a
+// new grid or a new topology each time) reuses the same few hundred MB instead of
+// mapping fresh memory each time.
+static cudaError_t plane_pool(int dev, cudaMemPool_t* out) {
+    static std::mutex m;
+    static std::unordered_map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(m);
+    auto it = pools.find(dev);
+    if (it != pools.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    unsigned long long keep = ~0ull;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    pools.emplace(dev, pool);
+    *out = pool;
+    return cudaSuccess;
+}
+template <class T>
+static cudaError_t pool_alloc(T** p, size_t bytes, int dev, cudaStream_t st) {
+    cudaMemPool_t pool;
+    cudaError_t e = plane_pool(dev, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync((void**)p, bytes, pool, st);
+}
+template <class T>
+static void pool_free(T*& p, cudaStream_t st) {
+    if (p) cudaFreeAsync((void*)p, st);
+    p = nullptr;
+}
+
 Grid::~Grid() {
-    dfree(chan);
-    dfree(ctype);
+    // cudaFree synchronised the device here before the planes came from a pool; keep that,
+    // so that no work of the grid's stream still reads them, then free on the legacy stream
+    // (the caller's stream may be gone by now)
+    if (chan || ctype) cudaDeviceSynchronize();
+    pool_free(chan, nullptr);
+    pool_free(ctype, nullptr);
     dfree(meta);
     dfree(nb);
     dfree(child);
@@ -138,8 +183,8 @@ int Grid::ensure_device() {
     uint8_t* ct_new = nullptr;
     const size_t cells = (size_t)n_new * kCells;
     if (device < 0) CK(cudaGetDevice(&device));
-    CK(cudaMalloc(&chan_new, sizeof(float) * cells * nch + 16));
-    CK(cudaMalloc(&ct_new, cells + 16));
+    CK(pool_alloc(&chan_new, sizeof(float) * cells * nch + 16, device, stream));
+    CK(pool_alloc(&ct_new, cells + 16, device, stream));
     int2* d_map = nullptr;
     int4* d_meta = nullptr;
     CK(cudaMalloc(&d_map, sizeof(int2) * (n_new + 1)));
@@ -156,8 +201,8 @@ int Grid::ensure_device() {
     CK(cudaStreamSynchronize(stream));
     CK(cudaGetLastError());
     cudaFree(d_map);
-    dfree(chan);
-    dfree(ctype);
+    pool_free(chan, stream);
+    pool_free(ctype, stream);
     chan = chan_new;
     ctype = ct_new;
 

@@ -679,7 +679,6 @@ cudaError_t launch_cluster_step(const DevGrid& g, const int* tile1, const int* t
     cfg.numAttrs = 1;
     note_kernel_launch();
     const ClPack* pk = reinterpret_cast<const ClPack*>(pack);
-    if (A.exact == kRelaxShort) return cudaLaunchKernelEx(&cfg, k_cluster_step<kRelaxShort>, g, A, pk, X, RHS, X0);
     if (A.exact == kRelaxRef) return cudaLaunchKernelEx(&cfg, k_cluster_step<kRelaxRef>, g, A, pk, X, RHS, X0);
     return cudaLaunchKernelEx(&cfg, k_cluster_step<kRelaxDouble>, g, A, pk, X, RHS, X0);
 }
@@ -688,9 +687,7 @@ bool cluster_step_supported() {
     int dev = 0, cc = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&cc, cudaDevAttrClusterLaunch, dev) != cudaSuccess || !cc) return false;
-    if (cudaFuncSetAttribute(k_cluster_step<kRelaxShort>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_cluster_step<kRelaxShort>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-        cudaFuncSetAttribute(k_cluster_step<kRelaxRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
+    if (cudaFuncSetAttribute(k_cluster_step<kRelaxRef>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
         cudaFuncSetAttribute(k_cluster_step<kRelaxRef>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
         cudaFuncSetAttribute(k_cluster_step<kRelaxDouble>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem) != cudaSuccess ||
         cudaFuncSetAttribute(k_cluster_step<kRelaxDouble>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {

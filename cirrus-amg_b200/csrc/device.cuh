@@ -9,7 +9,6 @@
 // These tables replace the reference's per-voxel hash probes
 // (HATileAccessor::findVoxel, src/HAAccessor.h:278).
 #pragma once
-#include <cstring>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -349,47 +348,17 @@ __device__ __forceinline__ float relax_ref(float xs, float delta, float om) {
     return __double2float_rn(__fma_rn((double)delta, (double)om, (double)xs));
 }
 
-// relax_ref's value from one single-precision fused multiply-add, for an omega whose
-// significand has at most three significant bits (1, 1.25, 1.5, 1.75 times a power of two;
-// the reference's default 1.5 among them).  Then p = delta * omega has at most 27
-// significant bits, and the two roundings of relax_ref can only differ from the single one
-// when the double sum lands exactly on a midpoint m between two floats while x + p does not.
-// Writing L for the lowest bit position of x, p and m, x + p - m is a multiple of 2^L and
-// must be below half a double ulp of m, so L <= e(m) - 53.  If x supplies that low bit, x is
-// below 2^-29 of the sum and p must itself be the midpoint -- possible only when |x| is below
-// 2^-51 |p|.  If p supplies it (|p| below 2^-26 |x|), then x - m is a non-zero multiple of
-// 2^(e(m)-24) (x is a float, m is not), far larger than |p|.  A sum that cancels keeps at
-// most 28 significant bits and is exact in double.  So the single FMA is used whenever x is
-// zero, delta is zero, or both are normal and |x| >= 2^-27 |delta * omega| (by exponents);
-// otherwise the double form.  cmg_check_division compares the two on adversarial pairs.
-__device__ __forceinline__ float relax_short(float xs, float delta, float om) {
-    const unsigned ux = __float_as_uint(xs), ud = __float_as_uint(delta);
-    const int ex = (int)((ux >> 23) & 0xffu), ed = (int)((ud >> 23) & 0xffu);
-    const int ew = (int)((__float_as_uint(om) >> 23) & 0xffu) - 127;
-    const bool normal = (unsigned)(ex - 1) < 254u && (unsigned)(ed - 1) < 254u;
-    const bool fast = (normal && ex - ed >= ew - 27) || (ux << 1) == 0u || (ud << 1) == 0u;
-    return fast ? __fmaf_rn(delta, om, xs) : relax_ref(xs, delta, om);
-}
-// how a smoother applies omega: not a float (x + delta * omega in double), a float
-// (relax_ref), or a float with at most three significant bits (relax_short)
-enum : int { kRelaxDouble = 0, kRelaxRef = 1, kRelaxShort = 2 };
-inline int relax_mode(double omega) {
-    const float om = (float)omega;
-    if ((double)om != omega) return kRelaxDouble;
-    unsigned u;
-    memcpy(&u, &om, sizeof(u));
-    const unsigned e = (u >> 23) & 0xffu;
-    return (e != 0u && e != 255u && (u & 0x1FFFFFu) == 0u) ? kRelaxShort : kRelaxRef;
-}
+// how a smoother applies omega: a float (relax_ref, as the reference's AMGSolver::omega
+// always is), or not a float (x + delta * omega in double, the product rounded too)
+enum : int { kRelaxDouble = 0, kRelaxRef = 1 };
+inline int relax_mode(double omega) { return (double)(float)omega == omega ? kRelaxRef : kRelaxDouble; }
 template <int M>
 __device__ __forceinline__ float relax(float xs, float delta, float om, double omega) {
-    if constexpr (M == kRelaxShort) return relax_short(xs, delta, om);
-    else if constexpr (M == kRelaxRef) return relax_ref(xs, delta, om);
+    if constexpr (M == kRelaxRef) return relax_ref(xs, delta, om);
     else return (float)((double)xs + (double)delta * omega);
 }
 __device__ __forceinline__ float relax_rt(int mode, float xs, float delta, float om, double omega) {
-    return mode == kRelaxShort ? relax_short(xs, delta, om) : mode == kRelaxRef ? relax_ref(xs, delta, om)
-                                                                                 : (float)((double)xs + (double)delta * omega);
+    return mode == kRelaxRef ? relax_ref(xs, delta, om) : (float)((double)xs + (double)delta * omega);
 }
 
 }  // namespace cmg

@@ -514,15 +514,12 @@ bool set_smem(K kernel, size_t bytes) {
 template <typename CT, typename XT>
 bool set_pipe_smem() {
     const size_t b = sizeof(PipeSmem<CT, XT>);
-    return set_smem(k_gs_pipe<CT, 0, kRelaxShort, XT>, b) && set_smem(k_gs_pipe<CT, 0, kRelaxRef, XT>, b) &&
-           set_smem(k_gs_pipe<CT, 0, kRelaxDouble, XT>, b);
+    return set_smem(k_gs_pipe<CT, 0, kRelaxRef, XT>, b) && set_smem(k_gs_pipe<CT, 0, kRelaxDouble, XT>, b);
 }
 template <typename CT, typename XT>
 void launch_pass(int blocks, cudaStream_t st, const DevGrid& g, XT* X, const XT* B, const PipeArgs& A) {
     const size_t sm = sizeof(PipeSmem<CT, XT>);
-    if (A.exact == kRelaxShort)
-        k_gs_pipe<CT, 0, kRelaxShort, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
-    else if (A.exact == kRelaxRef)
+    if (A.exact == kRelaxRef)
         k_gs_pipe<CT, 0, kRelaxRef, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
     else
         k_gs_pipe<CT, 0, kRelaxDouble, XT><<<blocks, 128, sm, st>>>(g, X, B, A);

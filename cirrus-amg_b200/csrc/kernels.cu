@@ -1174,8 +1174,7 @@ __device__ __forceinline__ float make_float(unsigned long long r, int emin, int 
     return __uint_as_float(sign | ((unsigned)(e + 127) << 23) | ((unsigned)r & 0x7fffffu));
 }
 // Compares div_by_recip (with the correctly rounded reciprocal) and div_exact
-// (with the Newton-refined one) with the IEEE division, and relax_short with relax_ref,
-// on pseudo-random pairs.  Division pairs: a quarter
+// (with the Newton-refined one) with the IEEE division on pseudo-random pairs: a quarter
 // uniform in sign, exponent and significand; a quarter built to fall within a few
 // ulps of a midpoint between two floats (a = RN(d * m) for a midpoint m); a quarter
 // shaped like Gauss-Seidel updates; a quarter of zeros, subnormals, huge values,
@@ -1217,49 +1216,6 @@ __global__ void k_check_division(long long n, unsigned long long seed, unsigned 
             if (atomicAdd(mism, 1ull) == 0ull) {
                 first[0] = __float_as_uint(a);
                 first[1] = __float_as_uint(d);
-            }
-        }
-        // the relaxation: relax_short against relax_ref for omegas of at most three significant
-        // bits, on pairs (x, delta): uniform; delta * omega within a few ulps of k half-ulps of
-        // x (sums near a float midpoint); delta * omega an exact midpoint with x tiny (where the
-        // double rounding matters); zeros, subnormals and non-finite values
-        {
-            const float oms[6] = {1.5f, 1.0f, 1.25f, 1.75f, 0.75f, 3.0f};
-            const unsigned long long r3 = mix64(r2), r4 = mix64(r3);
-            const float om = oms[r4 % 6ull];
-            float x, dl;
-            switch ((int)((i >> 2) & 3)) {
-                case 0:
-                    x = make_float(r3, -40, 40);
-                    dl = make_float(r4, -40, 40);
-                    break;
-                case 1: {
-                    x = make_float(r3, -20, 20);
-                    const double ulp = (double)nextafterf(fabsf(x), INFINITY) - (double)fabsf(x);
-                    const double k = 0.5 * (double)((r4 >> 8) % 7ull + 1ull) * (((r4 >> 16) & 1ull) ? 1.0 : -1.0);
-                    dl = __double2float_rn(k * ulp / (double)om);
-                    const int off = (int)((r4 >> 20) % 5ull) - 2;
-                    for (int q = 0; q < (off < 0 ? -off : off); ++q) dl = nextafterf(dl, off < 0 ? -INFINITY : INFINITY);
-                    break;
-                }
-                case 2: {
-                    dl = __uint_as_float(__float_as_uint(make_float(r3, -10, 10)) | 1u);  // odd significand
-                    const int ed = (int)((__float_as_uint(dl) >> 23) & 0xffu) - 127;
-                    x = make_float(r4, ed - 80, ed - 20);
-                    break;
-                }
-                default: {
-                    const float pool[10] = {0.0f, -0.0f, 1e-45f, -3e-39f, 1.17549435e-38f, 3.0e38f, INFINITY, -INFINITY, NAN, 1.0f};
-                    x = (r4 & 1) ? pool[r3 % 10] : make_float(r3, -126, 127);
-                    dl = (r4 & 2) ? pool[(r3 >> 8) % 10] : make_float(r4, -126, 127);
-                }
-            }
-            const float rw = relax_ref(x, dl, om), rg = relax_short(x, dl, om);
-            if (!((__float_as_uint(rw) == __float_as_uint(rg)) || (isnan(rw) && isnan(rg)))) {
-                if (atomicAdd(mism, 1ull) == 0ull) {
-                    first[0] = __float_as_uint(x);
-                    first[1] = __float_as_uint(dl);
-                }
             }
         }
     }

@@ -308,7 +308,39 @@ __global__ void k_tables(Tab T, int n, int* nb, int* child) {
     for (int ci = 0; ci < 8; ++ci) child[8 * t + ci] = T.find(L + 1, 2 * c[0] + (ci >> 2), 2 * c[1] + ((ci >> 1) & 1), 2 * c[2] + (ci & 1));
 }
 
+// CreateTestGrid's LEAF cell types (tests/TestGrids.cuh:161-167, topology.cpp case_cell_type):
+// NEUMANN where all 8 corners of the cell are inside the solid sphere (case 3), else INTERIOR
+__global__ void __launch_bounds__(128) k_leaf_case_types(const int4* meta, uint8_t* ctype, const int* leaf, int case_id, float h0) {
+    const int t = leaf[blockIdx.x];
+    const int4 m = meta[t];
+    const int level = m.x & 0xff;
+    const float h = __fdiv_rn(h0, (float)(1 << level));
+    uint8_t* out = ctype + (size_t)t * 512;
+    for (int v = threadIdx.x; v < 512; v += 128) {
+        uint8_t ty = kInterior;
+        if (case_id == 3) {
+            const int l[3] = {v >> 6, (v >> 3) & 7, v & 7}, tc[3] = {m.y, m.z, m.w};
+            float mn[3], mx[3];
+            for (int d = 0; d < 3; ++d) {
+                const int gc = tc[d] * 8 + l[d];
+                mn[d] = __fmul_rn((float)gc, h);
+                mx[d] = __fmul_rn((float)(gc + 1), h);
+            }
+            ty = corners_in_quarter(mn, mx, 0.0f) == 8 ? kNeumann : kInterior;
+        }
+        out[v] = ty;
+    }
+}
+
 }  // namespace
+
+bool device_cell_types_supported(int case_id) { return case_id >= 0 && case_id <= 7 && case_id != 5; }
+
+cudaError_t device_leaf_cell_types(const int4* meta, uint8_t* ctype, const int* leaf, int nleaf, int case_id, float h0, cudaStream_t st) {
+    if (nleaf <= 0) return cudaSuccess;
+    k_leaf_case_types<<<nleaf, 128, 0, st>>>(meta, ctype, leaf, case_id, h0);
+    return cudaGetLastError();
+}
 
 DeviceTopoBuilder::~DeviceTopoBuilder() { release(); }
 

@@ -32,4 +32,10 @@ bool device_case_supported(int case_id);
 int device_refine_case(DeviceTopoBuilder& B, Topology& topo, int case_id, const double* params, int nparams, cudaStream_t st,
                        int* steps);
 
+// CreateTestGrid's LEAF cell types of the built-in cases on the device (all but the star
+// case 5, whose corner test uses transcendental functions): the same values as the host's
+// case_cell_type, written into the cell-type plane of the given LEAF tiles
+bool device_cell_types_supported(int case_id);
+cudaError_t device_leaf_cell_types(const int4* meta, uint8_t* ctype, const int* leaf, int nleaf, int case_id, float h0, cudaStream_t st);
+
 }  // namespace cmg

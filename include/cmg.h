@@ -66,15 +66,13 @@ typedef int (*cmg_level_target_fn)(void* user, int level, int i, int j, int k);
 
 const char* cmg_last_error(void);
 int cmg_version(void);
-/* Self-check of the arithmetic the Gauss-Seidel sweeps use in place of the reference's
- * expressions (src/AMGSolver.cu:868-875): the division (one double multiply by a double
- * reciprocal of the divisor, rounded to float; the reciprocal either correctly rounded or
- * refined by Newton steps) against the IEEE float division, and the relaxation
- * x + delta * omega by one float fused multiply-add where that is provably the same
- * against the reference's double evaluation, for omegas of at most three significant
- * bits; on n pseudo-random pairs of each from `seed`.  mismatches receives the number of
- * results that differ in any bit; first_pair (may be NULL) the bit patterns of the first
- * differing pair.  No counterpart in the reference. */
+/* Self-check of the division the Gauss-Seidel sweeps use (one double multiply
+ * by a double reciprocal of the divisor, rounded to float; the reciprocal either
+ * correctly rounded or refined by Newton steps) against the IEEE float
+ * division, on n pseudo-random pairs from `seed`.  mismatches
+ * receives the number of results that differ in any bit; first_pair (may be
+ * NULL) the bit patterns of the first differing (a, d).  No counterpart in the
+ * reference, which divides directly (src/AMGSolver.cu:868-875). */
 int cmg_check_division(long long n, unsigned long long seed, long long* mismatches, unsigned int* first_pair);
 
 /* ---- grid: HADeviceGrid ------------------------------------------------ */
