@@ -436,6 +436,47 @@ def learned_block(cmg, torch, spec, steps, world, dev):
                                               np.linalg.norm(xp[lm].astype(np.float64)))}
 
 
+def learned_on_tuned(cmg, torch, G, S2, best, spec, steps, world, dev):
+    """The learned finest-level smoother on top of the autotuned cycle: training pairs from the
+    residual the tuned cycle leaves (other right-hand sides of the same octree), the net trained
+    on the GPU, then the timed rhs solved by the tuned cycle without and with it."""
+    import learned
+
+    t0 = time.perf_counter()
+    rhs = training_rhs(cmg, G, spec, LEARNED["rhs"])
+    pairs = learned.collect_pairs(G, S2, COEFF, rhs, iters=LEARNED["iters"], max_tiles=LEARNED["max_tiles"], z_ch=U, x0_ch=U + 1,
+                                  az_ch=U + 2, level_iters=best[2], coarsest_iters=best[3])
+    net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
+                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    args_t = (False, SOLVE["max_iters"], SOLVE["tol"], best[2], best[3], SOLVE["sync_stride"], False)
+
+    def timed(use_net):
+        S2.set_learned(net if use_net else None)
+        for _ in range(3):
+            G.copy(BSAVE, 1)
+            S2.solve(G, *args_t)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            G.copy(BSAVE, 1)
+            it, _ = S2.solve(G, *args_t)
+        b.record()
+        torch.cuda.synchronize()
+        return replica_time(a.elapsed_time(b), world, dev) / steps, it
+
+    tuned_ms, tuned_it = timed(False)
+    ms, it = timed(True)
+    true_rel, fell_back, learned_it = S2.learned_status()
+    S2.set_learned(None)
+    return {"trained_on": "residuals the tuned cycle leaves on other right-hand sides of the same octree",
+            "train_and_collect_s": round(train_s, 3), "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "tuned_ms": round(tuned_ms, 4), "tuned_pcg_iters": tuned_it, "learned_on_tuned_ms": round(ms, 4),
+            "learned_pcg_iters": learned_it, "fell_back": fell_back, "rel_residual_true": true_rel}
+
+
 def run_sequence(args, rank, world, local_rank):
     """The moving-sphere sequence: --steps positions, each with its own octree, cut-cell
     operator and rhs; at each position the plain and the learned solve (trained once on the
@@ -683,12 +724,14 @@ def run_ours(args, rank, world, local_rank):
             ms_t, it_t, mixed_x["tuned"] = timed_tuned("fp32")
             ms_tb, it_tb, mixed_x["tuned_bf16"] = timed_tuned("bf16")
             S2.set_storage("fp32")
+            on_top = learned_on_tuned(cmg, torch, G, S2, best, spec, args.steps, world, dev)
             tuned = {"tuned_on": "one training rhs of the same octree (seed 100 / Fourier seed 200), never the timed one",
                      "tune_s": round(tune_s, 3), "candidates": len(table),
                      "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3], "finest_iters": best[4],
                      "ms": round(ms_t, 4), "pcg_iters": it_t, "ms_bf16_storage": round(ms_tb, 4), "pcg_iters_bf16_storage": it_tb,
                      "plain_setting": {"omega": SOLVE["omega"], "mu": SOLVE["mu"], "level_iters": SOLVE["level_iters"],
-                                       "coarsest_iters": SOLVE["coarsest_iters"]}}
+                                       "coarsest_iters": SOLVE["coarsest_iters"]},
+                     "learned_smoother_on_top": on_top}
 
     result = None
     if rank == 0:
