@@ -54,6 +54,41 @@ SPHERES = [(0.5, 0.5, 0.5, 0.1)]
 WORKLOAD = "adaptive sphere octree 128^3/256^3/512^3 (h0=1/8, levels 4/5/6), Neumann cut-cell sphere r=0.1, Fourier-divergence rhs seed 1"
 SOLVE = dict(max_iters=100, tol=1e-6, level_iters=2, coarsest_iters=10, sync_stride=1, omega=1.5, mu=2)
 BYTES_PER_CELL_GS = 27  # x 4 + rhs 4 + 4 coefficients 16 + type 1 + half of x written 2
+# algorithmic bytes per cell of the other tile steps of a solve (float planes, 1-byte types)
+BYTES_PER_CELL = dict(
+    restrict=26,  # x 4 + rhs 4 + coefficients 16 + type 1 read, the parent's x and rhs (8 B per 8 cells) written
+    fas=33,       # x 4 + rhs 4 + coefficients 16 + type 1 read, rhs 4 + saved x 4 written
+    prolong=10,   # x 4 + type 1 read, the parent's x and saved x (8 B per 8 cells) read, x 4 written
+    apply=25,     # p 4 + coefficients 16 + type 1 read, Ap 4 written
+    xr=25,        # x, r, p, Ap 16 + type 1 read, x and r 8 written
+    dot=8,        # two planes read
+    pupdate=13,   # p, z 8 + type 1 read, p 4 written
+    fill=4,       # z = 0 on every tile
+    coarse=29,    # levels 0-1 (9 tiles): x, rhs, saved x, coefficients, type read, x written once per visit
+)
+
+
+def solve_algorithmic_bytes(G, mu, level_iters, iters):
+    """Algorithmic DRAM bytes of one plain solve of octree G that took `iters` PCG iterations:
+    every tile step of the FAS mu-cycle (a level-l step runs mu^(top-l) times per cycle) and
+    of the PCG vector updates, each plane read or written once per step."""
+    lv, _, ty = G.tiles()
+    import cmg
+
+    top = int(lv.max())
+    act = [int(((lv == l) & (ty != cmg.GHOST)).sum()) for l in range(top + 1)]
+    alll = [int((lv == l).sum()) for l in range(top + 1)]
+    nonleaf = [int(((lv == l) & (ty == cmg.NONLEAF)).sum()) for l in range(top + 1)]
+    nleaf = int((ty == cmg.LEAF).sum())
+    B, c = BYTES_PER_CELL, 512
+    cycle = 0.0
+    for l in range(2, top + 1):
+        v = mu ** (top - l)
+        step = 2 * level_iters * act[l] * BYTES_PER_CELL_GS + act[l] * B["restrict"] + nonleaf[l - 1] * B["fas"] + alll[l] * B["prolong"]
+        cycle += v * step * c
+    cycle += (mu ** max(top - 1, 0)) * 9 * c * B["coarse"] + len(lv) * c * B["fill"]
+    leaf_iter = nleaf * c * (B["apply"] + B["xr"] + B["dot"] + B["pupdate"])
+    return iters * cycle + iters * leaf_iter + nleaf * c * (B["dot"] + B["fill"])
 
 
 def fourier_modes(seed=1, n=16):

@@ -54,6 +54,7 @@ EXPORTS = [
     "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned",
     "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
     "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct", "cmg_amg_solver_set_cycle_bf16",
+    "cmg_batch_create", "cmg_batch_destroy", "cmg_batch_set_schedule", "cmg_batch_schedule", "cmg_batch_solve", "cmg_batch_autotune",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -131,6 +132,12 @@ def lib():
             "cmg_amg_last_solve_ms": (I, [P, P]),
             "cmg_amg_last_solve_launches": (I, [P, P]),
             "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
+            "cmg_batch_create": (I, [P, P, I, P]),
+            "cmg_batch_destroy": (I, [P]),
+            "cmg_batch_set_schedule": (I, [P, I, I, D]),
+            "cmg_batch_schedule": (I, [P, P, P, P, P, P]),
+            "cmg_batch_solve": (I, [P, P, P, I, D, I, I, I, I, P, P, P, P]),
+            "cmg_batch_autotune": (I, [P, P, P, P, I, I, D, I, I, I, P, P]),
             "cmg_amg_solver_set_storage": (I, [P, I]),
             "cmg_amg_divergence_without_coeff": (I, [P, I, I]),
             "cmg_grid_gather_device_tiles": (I, [P, P, S, I, I, I]),
@@ -209,6 +216,86 @@ def solve_batch(solvers, grids, max_iters, relative_tolerance, level_iters, coar
     _check(lib().cmg_amg_solve_batch(sv, gv, n, bv, xv, max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride,
                                      int(is_pure_neumann), it, rel, ms), "solve_batch")
     return list(it[:n]), list(rel[:n]), list(ms[:n])
+
+
+class PersistentBatch:
+    """n octrees solved by ONE persistent launch inside a CUDA graph (cmg_batch_*): groups of
+    resident blocks take the octrees largest first from a device queue and run each one's
+    whole solve.  solvers[i] gives grid i its settings (one solver may serve several grids);
+    results equal solver.solve(grid, ...) bit for bit.  Solvers and grids must outlive it."""
+
+    def __init__(self, solvers, grids):
+        if len(solvers) != len(grids):
+            raise CmgError("PersistentBatch: one solver per grid")
+        self.L = lib()
+        self.solvers, self.grids = list(solvers), list(grids)
+        self.n = len(grids)
+        sv = (ctypes.c_void_p * max(self.n, 1))(*[s_.h for s_ in self.solvers])
+        gv = (ctypes.c_void_p * max(self.n, 1))(*[g.h for g in self.grids])
+        h = ctypes.c_void_p()
+        _check(self.L.cmg_batch_create(sv, gv, self.n, ctypes.byref(h)), "cmg_batch_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.cmg_batch_destroy(self.h)
+            self.h = None
+
+    def set_schedule(self, group_blocks=0, split=0.0, slots=4):
+        """blocks of `slots` 128-thread slots (4, 6, 8); groups of `group_blocks` blocks on the
+        shared queue (0: the resident blocks spread over the octrees); split > 0: octrees too
+        large for such a group within split x (total work / resident blocks) get a group of
+        their own"""
+        _check(self.L.cmg_batch_set_schedule(self.h, int(slots), int(group_blocks), float(split)), "set_schedule")
+
+    def set_group_blocks(self, group_blocks):
+        self.set_schedule(group_blocks, 0.0, self.schedule()[0])
+
+    def schedule(self):
+        """(slots, small groups' blocks, groups, dedicated groups, resident blocks) of the next solve"""
+        v = [ctypes.c_int(0) for _ in range(5)]
+        _check(self.L.cmg_batch_schedule(self.h, *[ctypes.byref(x) for x in v]), "schedule")
+        return tuple(x.value for x in v)
+
+    def _sync(self):
+        for s_ in {id(s_): s_ for s_ in self.solvers}.values():
+            s_._sync_params()
+
+    def solve(self, max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride, is_pure_neumann, b_host=None, x_host=None):
+        """Returns (iters, rel_res, per-octree ms inside the launch, launch ms).  b_host / x_host:
+        None (b, x in channels 1, 0) or lists of n host buffer addresses."""
+        if (b_host is None) != (x_host is None):
+            raise CmgError("PersistentBatch.solve: b_host and x_host go together")
+        self._sync()
+        n = max(self.n, 1)
+        bv = (ctypes.c_void_p * n)(*b_host) if b_host is not None else None
+        xv = (ctypes.c_void_p * n)(*x_host) if x_host is not None else None
+        it, rel, ims = (ctypes.c_int * n)(), (ctypes.c_double * n)(), (ctypes.c_float * n)()
+        bms = ctypes.c_float(0)
+        _check(self.L.cmg_batch_solve(self.h, bv, xv, max_iters, relative_tolerance, level_iters, coarsest_iters, sync_stride,
+                                      int(is_pure_neumann), it, rel, ims, ctypes.byref(bms)), "batch solve")
+        return list(it[:self.n]), list(rel[:self.n]), list(ims[:self.n]), bms.value
+
+    def autotune(self, candidates, max_iters, relative_tolerance, level_iters, coarsest_iters, repeats=2):
+        """candidates: (group_blocks, split, slots) tuples (shorter tuples or a bare int: split 0,
+        4 slots).  Times each schedule after one calibration run; keeps and returns the fastest
+        (None if none converged) with the list of times (-1: not converged)."""
+        self._sync()
+
+        def norm(c):
+            c = (c,) if isinstance(c, int) else tuple(c)
+            return (int(c[0]), float(c[1]) if len(c) > 1 else 0.0, int(c[2]) if len(c) > 2 else 4)
+
+        cand = [norm(c) for c in candidates]
+        m = len(cand)
+        gv = (ctypes.c_int * m)(*[c[0] for c in cand])
+        sv = (ctypes.c_double * m)(*[c[1] for c in cand])
+        nv = (ctypes.c_int * m)(*[c[2] for c in cand])
+        ms = (ctypes.c_float * m)()
+        best = ctypes.c_int(-1)
+        _check(self.L.cmg_batch_autotune(self.h, nv, gv, sv, m, max_iters, relative_tolerance, level_iters, coarsest_iters, repeats, ms,
+                                         ctypes.byref(best)), "batch autotune")
+        return (candidates[best.value] if best.value >= 0 else None), list(ms[:m])
 
 
 def _check(rc, what):

@@ -631,6 +631,81 @@ int cmg_amg_solve_batch(cmg_amg_solver* const* solvers, cmg_grid* const* grids, 
     return CMG_OK;
     GUARD_END
 }
+struct cmg_batch {
+    cmg::Batch b;
+};
+int cmg_batch_create(cmg_amg_solver* const* solvers, cmg_grid* const* grids, int n, cmg_batch** out) {
+    GUARD_BEGIN
+    if (!out || n < 0 || (n > 0 && (!solvers || !grids))) return fail(CMG_ERR_INVALID, "cmg_batch_create: bad argument");
+    std::vector<cmg::Solver*> sv(n);
+    std::vector<cmg::Grid*> gv(n);
+    std::vector<const void*> seen;
+    for (int i = 0; i < n; ++i) {
+        if (!solvers[i] || !grid_ready(grids[i])) return fail(CMG_ERR_STATE, "cmg_batch_create: solver or grid not ready");
+        sv[i] = &solvers[i]->s;
+        gv[i] = &grids[i]->g;
+        seen.push_back(grids[i]);
+    }
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+        return fail(CMG_ERR_INVALID, "cmg_batch_create: grids must be distinct objects");
+    cmg_batch* b = new cmg_batch();
+    if (int rc = b->b.init(sv.data(), gv.data(), n)) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return CMG_OK;
+    GUARD_END
+}
+int cmg_batch_destroy(cmg_batch* b) {
+    delete b;
+    return CMG_OK;
+}
+int cmg_batch_schedule(cmg_batch* b, int* slots, int* group_blocks, int* groups, int* dedicated, int* resident_blocks) {
+    if (!b || !slots || !group_blocks || !groups || !dedicated || !resident_blocks)
+        return fail(CMG_ERR_INVALID, "cmg_batch_schedule: bad argument");
+    GUARD_BEGIN
+    return b->b.schedule(slots, group_blocks, groups, dedicated, resident_blocks);
+    GUARD_END
+}
+int cmg_batch_solve(cmg_batch* b, const float* const* b_host, float* const* x_host, int max_iters, double tol, int level_iters,
+                    int coarsest_iters, int sync_stride, int pure_neumann, int* iters, double* rel_res, float* instance_ms, float* batch_ms) {
+    GUARD_BEGIN
+    const int n = b ? (int)b->b.grids.size() : 0;
+    if (!b || (!b_host != !x_host) || (n > 0 && (!iters || !rel_res))) return fail(CMG_ERR_INVALID, "cmg_batch_solve: bad argument");
+    if (b_host)
+        for (int i = 0; i < n; ++i)
+            if (!b_host[i] || !x_host[i]) return fail(CMG_ERR_INVALID, "cmg_batch_solve: null host buffer");
+    for (cmg::Grid* g : b->b.grids)
+        if (!g->built || g->ensure_device() != 0) return fail(CMG_ERR_STATE, "cmg_batch_solve: grid not built");
+    const int rc = b->b.run(b_host, x_host, max_iters, tol, level_iters, coarsest_iters, sync_stride, pure_neumann != 0, iters, rel_res,
+                            instance_ms);
+    if (batch_ms) *batch_ms = b->b.last_ms;
+    return rc;
+    GUARD_END
+}
+int cmg_batch_set_schedule(cmg_batch* b, int slots, int group_blocks, double split) {
+    if (!b || !cmg::batch_slots_supported(slots) || group_blocks < 0 || !(split >= 0.0))
+        return fail(CMG_ERR_INVALID, "cmg_batch_set_schedule: bad argument");
+    b->b.slots = slots;
+    b->b.group_blocks = group_blocks;
+    b->b.split = split;
+    return CMG_OK;
+}
+int cmg_batch_autotune(cmg_batch* b, const int* slots, const int* group_blocks, const double* split, int ncand, int max_iters, double tol,
+                       int level_iters, int coarsest_iters, int repeats, float* ms, int* best) {
+    GUARD_BEGIN
+    if (!b || !group_blocks || ncand <= 0 || !ms || !best || max_iters <= 0 || !(tol > 0.0) || repeats < 1)
+        return fail(CMG_ERR_INVALID, "cmg_batch_autotune: bad argument");
+    for (int i = 0; i < ncand; ++i)
+        if (group_blocks[i] <= 0 || (split && !(split[i] >= 0.0)) || (slots && !cmg::batch_slots_supported(slots[i])))
+            return fail(CMG_ERR_INVALID, "cmg_batch_autotune: bad candidate");
+    for (cmg::Grid* g : b->b.grids)
+        if (!g->built || g->ensure_device() != 0) return fail(CMG_ERR_STATE, "cmg_batch_autotune: grid not built");
+    return b->b.autotune(slots, group_blocks, split, ncand, max_iters, tol, level_iters, coarsest_iters, 1, repeats, ms, best);
+    GUARD_END
+}
 static int geo_create(int kind, float one_over_alpha, float prolong, cmg_amg_solver** out) {
     if (!out) return fail(CMG_ERR_INVALID, "solver create: null output");
     cmg_amg_solver* s = new cmg_amg_solver(kind, one_over_alpha, prolong);

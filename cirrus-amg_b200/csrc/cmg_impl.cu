@@ -1002,19 +1002,9 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     return 0;
 }
 
-int Solver::solve_finish(bool verbose, int* iters, double* rel) {
-    if (!pending.active) {
-        set_error("solve: no solve in flight on this solver");
-        return 3;
-    }
-    pending.active = false;
-    const cudaStream_t st = pending.stream;
-    CK(cudaStreamSynchronize(st));
-    CK(cudaGetLastError());
-    cudaEventElapsedTime(&last_ms, ev0, ev1);
-    const PcgScalars& r = *h_s;
-    last_replaced = r.replaced;
-    const int sync_stride = pending.sync_stride;
+// iterations and relative residual of a finished solve, from its final scalars: with no
+// convergence test (sync_stride 0) the residual is unknown (-1); b = 0 ends at once
+static void pcg_outcome(const PcgScalars& r, int sync_stride, int* iters, double* rel) {
     int n_it = r.iter;
     double rel_res;
     if (sync_stride > 0) {
@@ -1029,6 +1019,25 @@ int Solver::solve_finish(bool verbose, int* iters, double* rel) {
     } else {
         rel_res = -1.0;
     }
+    *iters = n_it;
+    *rel = rel_res;
+}
+
+int Solver::solve_finish(bool verbose, int* iters, double* rel) {
+    if (!pending.active) {
+        set_error("solve: no solve in flight on this solver");
+        return 3;
+    }
+    pending.active = false;
+    const cudaStream_t st = pending.stream;
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    cudaEventElapsedTime(&last_ms, ev0, ev1);
+    const PcgScalars& r = *h_s;
+    last_replaced = r.replaced;
+    int n_it = 0;
+    double rel_res = 0.0;
+    pcg_outcome(r, pending.sync_stride, &n_it, &rel_res);
     if (iters) *iters = n_it;
     if (rel) *rel = rel_res;
     // the IF body runs on every iteration except the one that ends the loop
@@ -1155,6 +1164,383 @@ int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, doub
         finest_iters = c[*best].finest_iters;
     }
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Batch: many octrees in one persistent launch inside a CUDA graph
+// ---------------------------------------------------------------------------
+Batch::~Batch() {
+    if (st) cudaStreamSynchronize(st);
+    if (exec) cudaGraphExecDestroy(exec);
+    dfree(d_inst);
+    dfree(d_order);
+    dfree(d_groups);
+    dfree(d_block_group);
+    dfree(d_ctl);
+    dfree(d_part);
+    dfree(d_s);
+    dfree(d_clock);
+    for (void* p : {(void*)h_inst, (void*)h_order, (void*)h_groups, (void*)h_block_group, (void*)h_ctl, (void*)h_s, (void*)h_clock})
+        if (p) cudaFreeHost(p);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (st) cudaStreamDestroy(st);
+}
+
+int Batch::init(Solver* const* s, Grid* const* g, int n) {
+    solvers.assign(s, s + n);
+    grids.assign(g, g + n);
+    CK(cudaGetDevice(&device));
+    int resident = 0;
+    for (int ns : {4, 6, 8}) resident = std::max(resident, batch_resident_blocks(ns));
+    if (resident <= 0) {
+        set_error("batch: the persistent batched kernel cannot be resident on this device");
+        return 2;
+    }
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    const size_t m = (size_t)std::max(n, 1);
+    CK(cudaMalloc(&d_inst, sizeof(BatchInst) * m));
+    CK(cudaMallocHost(&h_inst, sizeof(BatchInst) * m));
+    CK(cudaMalloc(&d_order, sizeof(int) * m));
+    CK(cudaMallocHost(&h_order, sizeof(int) * m));
+    CK(cudaMalloc(&d_groups, sizeof(BatchGroup) * resident));
+    CK(cudaMallocHost(&h_groups, sizeof(BatchGroup) * resident));
+    CK(cudaMalloc(&d_block_group, sizeof(int) * resident));
+    CK(cudaMallocHost(&h_block_group, sizeof(int) * resident));
+    CK(cudaMalloc(&d_s, sizeof(PcgScalars) * m));
+    CK(cudaMallocHost(&h_s, sizeof(PcgScalars) * m));
+    CK(cudaMalloc(&d_clock, sizeof(unsigned long long) * 4 * m));
+    CK(cudaMallocHost(&h_clock, sizeof(unsigned long long) * 4 * m));
+    ctl_words = batch_ctl_words(resident);
+    CK(cudaMalloc(&d_ctl, sizeof(unsigned int) * ctl_words));
+    CK(cudaMemset(d_ctl, 0, sizeof(unsigned int) * ctl_words));
+    CK(cudaMallocHost(&h_ctl, sizeof(unsigned int) * 2));
+    return 0;
+}
+
+// estimated work of one cycle per instance: each level's tiles (plus a fixed cost per step)
+// times its visits per cycle, mu^(top - l)
+static std::vector<double> batch_work_estimate(const Batch& B) {
+    std::vector<double> w(B.grids.size());
+    for (size_t i = 0; i < w.size(); ++i) {
+        const Grid& G = *B.grids[i];
+        const int mu = std::max(B.solvers[i]->mu, 1);
+        double wk = 0.0, visits = 1.0;
+        for (int l = G.max_level(); l >= 0; --l, visits *= mu) wk += visits * (G.level_end(l) - G.level_begin(l) + 16);
+        w[i] = wk;
+    }
+    return w;
+}
+
+int Batch::schedule(int* ns, int* G, int* groups, int* dedicated, int* resident) {
+    const int n = (int)grids.size();
+    int ng = 0, dyn = 0, ded = 0;
+    const int nb = plan(weight.size() == (size_t)n ? weight : batch_work_estimate(*this), &ng, &dyn, &ded);
+    *ns = slots;
+    *G = last_plan_gs;
+    *groups = ng;
+    *dedicated = ded;
+    *resident = batch_resident_blocks(slots);
+    if (nb <= 0) {
+        set_error("batch: no resident blocks for the persistent batched kernel");
+        return 2;
+    }
+    return 0;
+}
+
+int Batch::plan(const std::vector<double>& w, int* ngroups, int* dyn_begin, int* dedicated) {
+    const int R = batch_resident_blocks(slots);
+    const int n = (int)grids.size();
+    *ngroups = *dyn_begin = *dedicated = 0;
+    if (R <= 0 || n == 0) return 0;
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return w[a] > w[b]; });
+    const int gs = std::min(R, group_blocks > 0 ? group_blocks : std::max(1, R / n));
+    last_plan_gs = gs;
+    int used = 0, ng = 0, nbig = 0;
+    if (split > 0.0) {
+        // octrees that would not end within the budget in a small group get a group of their own
+        double total = 0.0;
+        for (double v : w) total += v;
+        const double T = split * total / R;
+        for (int k = 0; k < n; ++k) {
+            const int i = idx[k];
+            const int need = std::min((int)std::ceil(w[i] / T), R - used - gs);  // keep one small group
+            if (need <= gs) break;
+            h_groups[ng] = BatchGroup{used, need, nbig, nbig + 1};
+            h_order[nbig] = i;
+            for (int b = used; b < used + need; ++b) h_block_group[b] = ng;
+            used += need;
+            ++ng;
+            ++nbig;
+        }
+    }
+    for (int k = nbig; k < n; ++k) h_order[k] = idx[k];
+    // the remaining blocks as small groups on the shared queue (never more groups than octrees)
+    const int small = std::min((R - used) / gs, std::max(n - nbig, 0));
+    for (int q = 0; q < small; ++q) {
+        h_groups[ng] = BatchGroup{used, gs, 0, 0};
+        for (int b = used; b < used + gs; ++b) h_block_group[b] = ng;
+        used += gs;
+        ++ng;
+    }
+    *ngroups = ng;
+    *dyn_begin = nbig;
+    *dedicated = nbig;
+    return used;
+}
+
+int Batch::run(const float* const* b_host, float* const* x_host, int max_iters, double tol, int level_iters, int coarsest_iters,
+               int sync_stride, bool pure_neumann, int* iters, double* rel, float* instance_ms) {
+    const int n = (int)grids.size();
+    if (n == 0) return 0;
+    if (max_iters < 0 || level_iters < 0 || coarsest_iters < 0) {
+        set_error("batch: negative iteration count");
+        return 1;
+    }
+    int cur = 0;
+    CK(cudaGetDevice(&cur));
+    if (cur != device) {
+        set_error("batch: the current device is not the one the batch was created on");
+        return 3;
+    }
+    // every instance: an AMG solver in the reference's FP32 form, a built grid on this device
+    size_t need = 0;
+    for (int i = 0; i < n; ++i) {
+        const Solver& S = *solvers[i];
+        Grid& G = *grids[i];
+        if (S.kind != kAMG || S.storage != kStorageFP32 || S.lnet.enabled || S.replace_every > 0 || S.cycle_bf16 || S.coarsest_direct ||
+            S.mu < 0) {
+            set_error("batch: every solver must be an AMG solver with FP32 storage and no learned, replacement, BF16-cycle or "
+                      "direct-coarsest option");
+            return 1;
+        }
+        if (G.n == 0 || G.nleaf == 0) {
+            set_error("batch: a grid has no LEAF tiles (rebuild first)");
+            return 3;
+        }
+        if (G.nch < 5 || S.coeff_ch < 5 || S.coeff_ch + 4 > G.nch) {
+            set_error("batch: needs channels 0..4 and coefficient channels coeff..coeff+3 (coeff >= 5)");
+            return 1;
+        }
+        if (G.device != device) {
+            set_error("batch: a grid lives on another device");
+            return 3;
+        }
+        if (G.max_level() >= kBatchMaxLevels) {
+            set_error("batch: octree deeper than the batched kernel supports");
+            return 1;
+        }
+        if (int rc = validate_solver_topology(G)) return rc;
+        need += 4 * (size_t)G.nleaf;
+    }
+    if (need > part_cap) {
+        CK(cudaStreamSynchronize(st));
+        dfree(d_part);
+        CK(cudaMalloc(&d_part, sizeof(double) * need));
+        part_cap = need;
+    }
+    int ngroups = 0, dyn_begin = 0, dedicated = 0;
+    const int nblocks = plan(weight.size() == (size_t)n ? weight : batch_work_estimate(*this), &ngroups, &dyn_begin, &dedicated);
+    if (nblocks <= 0) {
+        set_error("batch: no resident blocks for the persistent batched kernel");
+        return 2;
+    }
+    // instance table
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        const Solver& S = *solvers[i];
+        Grid& G = *grids[i];
+        BatchInst& I = h_inst[i];
+        std::memset(&I, 0, sizeof(I));
+        I.g = G.dev();
+        I.leaf = G.leaf;
+        I.nleaf = G.nleaf;
+        I.top = G.max_level();
+        for (int l = 0; l <= I.top; ++l) {
+            I.lb[l] = G.level_begin(l);
+            I.ab[l] = G.ghost_begin(l);
+            I.le[l] = G.level_end(l);
+            I.nlb[l] = G.nonleaf_begin(l);
+        }
+        I.coeff_ch = S.coeff_ch;
+        I.mu = S.mu;
+        I.finest_iters = S.finest_iters;
+        I.exact = relax_mode(S.omega);
+        I.om = (float)S.omega;
+        I.omega = S.omega;
+        I.Rr = S.R_restrict;
+        I.P = S.P;
+        I.partial = d_part + off;
+        off += 4 * (size_t)G.nleaf;
+        I.s = d_s + i;
+        I.clock = d_clock + 4 * i;
+    }
+    // the grids' own streams may still carry uploads
+    std::vector<cudaStream_t> seen;
+    for (Grid* g : grids)
+        if (std::find(seen.begin(), seen.end(), g->stream) == seen.end()) {
+            seen.push_back(g->stream);
+            CK(cudaStreamSynchronize(g->stream));
+        }
+    CK(cudaMemcpyAsync(d_inst, h_inst, sizeof(BatchInst) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_order, h_order, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_groups, h_groups, sizeof(BatchGroup) * ngroups, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_block_group, h_block_group, sizeof(int) * nblocks, cudaMemcpyHostToDevice, st));
+    if (b_host)
+        for (int i = 0; i < n; ++i)
+            CK(cudaMemcpyAsync(grids[i]->plane(1), b_host[i], sizeof(float) * (size_t)grids[i]->n * kCells, cudaMemcpyHostToDevice, st));
+    const GraphKey k{slots, nblocks, ngroups, dyn_begin, max_iters, sync_stride, pure_neumann ? 1 : 0, level_iters, coarsest_iters, tol};
+    if (!exec || !(k == key)) {
+        if (exec) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        BatchArgs A;
+        A.inst = d_inst;
+        A.order = d_order;
+        A.groups = d_groups;
+        A.block_group = d_block_group;
+        A.n = n;
+        A.ngroups = ngroups;
+        A.dyn_begin = dyn_begin;
+        A.max_iters = max_iters;
+        A.sync_stride = sync_stride;
+        A.pure_neumann = pure_neumann ? 1 : 0;
+        A.level_iters = level_iters;
+        A.coarsest_iters = coarsest_iters;
+        A.tol = tol;
+        A.ctl = d_ctl;
+        cudaStream_t cs = nullptr;
+        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaMemsetAsync(d_ctl, 0, sizeof(unsigned int) * ctl_words, cs);
+            const cudaError_t le = launch_batch_solve(A, nblocks, slots, cs);
+            e = cudaStreamEndCapture(cs, &graph);
+            if (le != cudaSuccess) e = le;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) {
+            exec = nullptr;
+            return check_cuda(e, "batch: capture of the persistent launch");
+        }
+        key = k;
+    }
+    CK(cudaEventRecord(ev0, st));
+    CK(cudaGraphLaunch(exec, st));
+    CK(cudaEventRecord(ev1, st));
+    if (x_host)
+        for (int i = 0; i < n; ++i)
+            CK(cudaMemcpyAsync(x_host[i], grids[i]->plane(0), sizeof(float) * (size_t)grids[i]->n * kCells, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_s, d_s, sizeof(PcgScalars) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_clock, d_clock, sizeof(unsigned long long) * 4 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    cudaEventElapsedTime(&last_ms, ev0, ev1);
+    last_nblocks = nblocks;
+    last_groups = ngroups;
+    last_dedicated = dedicated;
+    if (h_ctl[1]) {
+        set_error("batch: a group barrier of the persistent batched kernel timed out");
+        return 2;
+    }
+    int rc = 0;
+    for (int i = 0; i < n; ++i) {
+        int it = 0;
+        double rr = 0.0;
+        pcg_outcome(h_s[i], sync_stride, &it, &rr);
+        if (iters) iters[i] = it;
+        if (rel) rel[i] = rr;
+        if (instance_ms) instance_ms[i] = (float)((double)(h_clock[4 * i + 1] - h_clock[4 * i]) * 1e-6);
+        if (h_s[i].nonfinite && rc == 0) {
+            set_error("batch: non-finite value in a PCG reduction of instance " + std::to_string(i));
+            rc = 5;
+        }
+    }
+    return rc;
+}
+
+int Batch::autotune(const int* slots_c, const int* cand, const double* split_c, int ncand, int max_iters, double tol, int level_iters,
+                    int coarsest_iters, int sync_stride, int repeats, float* ms, int* best) {
+    *best = -1;
+    const int n = (int)grids.size();
+    if (n == 0) return 0;
+    // the right-hand sides the grids hold now, restored before every run and at the end
+    size_t total = 0;
+    for (Grid* g : grids) total += (size_t)g->n * kCells;
+    float* keep = nullptr;
+    CK(cudaMalloc(&keep, sizeof(float) * total));
+    auto copy_all = [&](bool save) -> int {
+        size_t o = 0;
+        for (Grid* g : grids) {
+            const size_t c = (size_t)g->n * kCells;
+            CK(cudaMemcpyAsync(save ? keep + o : g->plane(1), save ? g->plane(1) : keep + o, sizeof(float) * c, cudaMemcpyDeviceToDevice,
+                               st));
+            o += c;
+        }
+        return 0;
+    };
+    for (Grid* g : grids) CK(cudaStreamSynchronize(g->stream));
+    int rc = copy_all(true);
+    const int g0 = group_blocks, ns0 = slots;
+    const double s0 = split;
+    std::vector<int> it(n);
+    std::vector<double> rr(n);
+    std::vector<float> ims(n);
+    // calibration: every octree's block-time (solve time x blocks of its group)
+    if (rc == 0) rc = copy_all(false);
+    if (rc == 0) {
+        const int e = run(nullptr, nullptr, max_iters, tol, level_iters, coarsest_iters, sync_stride, false, it.data(), rr.data(), ims.data());
+        if (e && e != 5) rc = e;
+        if (rc == 0) {
+            std::vector<double> w(n);
+            for (int i = 0; i < n; ++i) w[i] = (double)ims[i] * (double)h_clock[4 * i + 2];
+            weight = w;
+        }
+    }
+    float best_ms = 0.0f;
+    for (int c = 0; c < ncand && rc == 0; ++c) {
+        group_blocks = cand[c];
+        split = split_c ? split_c[c] : 0.0;
+        slots = slots_c ? slots_c[c] : ns0;
+        float tmin = -1.0f;
+        bool ok = true;
+        for (int r = 0; r <= repeats && rc == 0; ++r) {  // the first run builds the graph and is not counted
+            if ((rc = copy_all(false))) break;
+            const int e = run(nullptr, nullptr, max_iters, tol, level_iters, coarsest_iters, sync_stride, false, it.data(), rr.data(), nullptr);
+            if (e == 5) ok = false;
+            else if (e) rc = e;
+            for (int i = 0; i < n && sync_stride > 0; ++i)
+                if (!(h_s[i].converged || h_s[i].rr0 == 0.0)) ok = false;
+            if (r > 0 && (tmin < 0.0f || last_ms < tmin)) tmin = last_ms;
+        }
+        ms[c] = ok ? tmin : -1.0f;
+        if (rc == 0 && ok && (*best < 0 || tmin < best_ms)) {
+            *best = c;
+            best_ms = tmin;
+        }
+    }
+    if (rc == 0) rc = copy_all(false);
+    cudaStreamSynchronize(st);
+    cudaFree(keep);
+    if (*best >= 0) {
+        group_blocks = cand[*best];
+        split = split_c ? split_c[*best] : 0.0;
+        slots = slots_c ? slots_c[*best] : ns0;
+    } else {
+        group_blocks = g0;
+        split = s0;
+        slots = ns0;
+    }
+    return rc;
 }
 
 }  // namespace cmg

@@ -273,6 +273,72 @@ struct Net {
     int ensure_batch(int nb);
 };
 
+// Many octrees solved by one persistent cooperative launch inside a CUDA graph
+// (batch_persist.cu).  Each instance is a grid with the AMG solver whose settings (omega,
+// mu, coefficient channel, finest-level sweeps) it is solved with; the solver objects only
+// carry settings here, the batch owns all scratch.
+// The schedule: groups of `group_blocks` blocks take octrees from a shared queue, largest
+// first.  With split > 0 the octrees too large for such a group get a group of their own,
+// sized so that it ends in about split x (total work / resident blocks); the work of each
+// octree is its measured block-time from the last autotune, else a cycle-work estimate.
+struct Batch {
+    std::vector<Solver*> solvers;
+    std::vector<Grid*> grids;
+    int device = 0;
+    int slots = 4;         // 128-thread slots per block: 4, 6 or 8
+    int group_blocks = 0;  // 0: automatic (the resident blocks spread over the instances)
+    double split = 0.0;
+    int last_plan_gs = 0;
+    std::vector<double> weight;  // block-ms per instance, measured by autotune (empty: estimate)
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    BatchInst* d_inst = nullptr;
+    BatchInst* h_inst = nullptr;  // pinned
+    int* d_order = nullptr;
+    int* h_order = nullptr;  // pinned
+    BatchGroup* d_groups = nullptr;
+    BatchGroup* h_groups = nullptr;  // pinned
+    int* d_block_group = nullptr;
+    int* h_block_group = nullptr;  // pinned
+    unsigned int* d_ctl = nullptr;
+    unsigned int* h_ctl = nullptr;  // pinned: the error word read back
+    size_t ctl_words = 0;
+    double* d_part = nullptr;
+    size_t part_cap = 0;  // doubles
+    PcgScalars* d_s = nullptr;
+    PcgScalars* h_s = nullptr;  // pinned
+    unsigned long long* d_clock = nullptr;
+    unsigned long long* h_clock = nullptr;  // pinned, 4 per instance
+    cudaGraphExec_t exec = nullptr;
+    struct GraphKey {
+        int slots, nblocks, ngroups, dyn_begin, max_iters, sync_stride, pure_neumann, level_iters, coarsest_iters;
+        double tol;
+        bool operator==(const GraphKey& o) const {
+            return std::tie(slots, nblocks, ngroups, dyn_begin, max_iters, sync_stride, pure_neumann, level_iters, coarsest_iters, tol) ==
+                   std::tie(o.slots, o.nblocks, o.ngroups, o.dyn_begin, o.max_iters, o.sync_stride, o.pure_neumann, o.level_iters,
+                            o.coarsest_iters, o.tol);
+        }
+    } key{};
+    float last_ms = 0.0f;
+    int last_nblocks = 0, last_groups = 0, last_dedicated = 0;
+    ~Batch();
+    int init(Solver* const* s, Grid* const* g, int n);
+    // the plan a run uses: groups (h_groups, h_block_group), queue order (h_order), the first
+    // shared-queue position; returns the blocks launched (0: none resident)
+    int plan(const std::vector<double>& w, int* ngroups, int* dyn_begin, int* dedicated);
+    // the plan a run would use: slots per block, small groups' size, groups, dedicated groups,
+    // resident blocks
+    int schedule(int* ns, int* G, int* groups, int* dedicated, int* resident);
+    int run(const float* const* b_host, float* const* x_host, int max_iters, double tol, int level_iters, int coarsest_iters,
+            int sync_stride, bool pure_neumann, int* iters, double* rel, float* instance_ms);
+    // One calibration run measures each octree's block-time; then the batch is timed under
+    // each candidate schedule (slots[i], group_blocks[i], split[i]), best of `repeats` runs after one
+    // untimed run, every run from the right-hand sides the grids held on entry (restored
+    // afterwards); the fastest whose solves all converge is kept.
+    int autotune(const int* slots_c, const int* cand, const double* split_c, int ncand, int max_iters, double tol, int level_iters,
+                 int coarsest_iters, int sync_stride, int repeats, float* ms, int* best);
+};
+
 int check_cuda(cudaError_t e, const char* what);
 int validate_solver_topology(const Grid& G);
 

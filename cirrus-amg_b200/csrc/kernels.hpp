@@ -120,6 +120,45 @@ cudaError_t launch_persist_step(const DevGrid& g, int top, const int* lb, const 
                                 float P, unsigned int* bar, int nblocks, cudaStream_t st);
 int persist_blocks();  // co-resident blocks of the persistent kernel on the current device
 
+// --- many octrees solved by one persistent launch (batch_persist.cu) ---
+// One instance: its octree, level ranges, the mu-cycle settings of its solver, and its
+// own scratch.  Planes of the solve: x 0, r 1, p 2, Ap 3, z 4 (the cycle's x); the cycle's
+// rhs and saved x live in planes 1 and 3 on NONLEAF tiles, as in the single solve.
+constexpr int kBatchMaxLevels = 16;
+struct BatchInst {
+    DevGrid g;
+    const int* leaf;
+    int nleaf, top;  // LEAF tile list; finest level
+    int lb[kBatchMaxLevels], ab[kBatchMaxLevels], le[kBatchMaxLevels], nlb[kBatchMaxLevels];
+    int coeff_ch, mu, finest_iters, exact;  // exact: relaxation form (relax_mode of omega)
+    float om, Rr, P;
+    double omega;
+    double* partial;  // 4 * nleaf doubles: two buffers of (per-tile sums, per-tile counts), used in turn
+    PcgScalars* s;     // final scalars, read by the host
+    unsigned long long* clock;  // [4]: start and end of this instance's solve (globaltimer, ns), blocks and group that ran it
+};
+// A group of blocks: blocks [first, first + size) solve the instances order[sbegin..send)
+// first, one after another, then take instances from the shared queue order[dyn_begin..n)
+struct BatchGroup {
+    int first, size, sbegin, send;
+};
+struct BatchArgs {
+    const BatchInst* inst;
+    const int* order;              // queue position -> instance
+    const BatchGroup* groups;      // ngroups entries
+    const int* block_group;        // block -> its group
+    int n, ngroups, dyn_begin;
+    int max_iters, sync_stride, pure_neumann, level_iters, coarsest_iters;
+    double tol;
+    unsigned int* ctl;  // batch_ctl_words(groups) zeroed words: queue head, error flag, per-group barrier
+};
+size_t batch_ctl_words(int groups);
+// blocks of `slots` 128-thread slots (4, 6 or 8): co-resident blocks on the current device
+bool batch_slots_supported(int slots);
+int batch_resident_blocks(int slots);
+size_t batch_smem_bytes(int slots);
+cudaError_t launch_batch_solve(const BatchArgs& A, int nblocks, int slots, cudaStream_t st);
+
 // --- PCG on LEAF tiles (tile list) ---
 enum DotMode : int { kDotStore = 0, kDotRR0 = 1, kDotGammaInit = 2, kDotBeta = 3, kDotAlpha = 4 };
 void launch_leaf_apply(const DevGrid& g, const int* leaf, int nleaf, const float* P, float* AP, int coeff_ch, bool fuse_alpha,

@@ -369,6 +369,49 @@ int cmg_amg_solve_batch(cmg_amg_solver* const* solvers, cmg_grid* const* grids, 
                         const float* const* b_host, float* const* x_host,
                         int max_iters, double relative_tolerance, int level_iters, int coarsest_iters,
                         int sync_stride, int is_pure_neumann, int* iters, double* rel_res, float* ms);
+/* ---- many octrees in ONE persistent launch ----
+ * n independent solves, each AMGSolver::solve (src/AMGSolver.h:62) of grid i with the
+ * settings of solver i (omega, mu, coefficient channel, finest-level sweeps), run by one
+ * cooperative kernel launch captured in a CUDA graph.  The resident blocks form groups of
+ * `group_blocks` blocks; each group takes the next octree from a device work queue (the
+ * largest mu-cycle work first), runs its whole PCG solve, and takes the next.  Results are
+ * cmg_amg_solve's bit for bit.  The reference has no batched call: its callers loop over
+ * solve() (cirrus_cutcell/FluidEuler.cu:702-707).
+ * Grids must be n distinct built grids on the current device; a solver may serve several
+ * grids.  Solvers must be AMG solvers with FP32 storage and none of the learned,
+ * residual-replacement, BF16-cycle or direct-coarsest options (CMG_ERR_INVALID otherwise).
+ * The batch keeps the pointers: solvers and grids must outlive it, and a grid rebuilt
+ * since the last call is picked up by the next call. */
+typedef struct cmg_batch cmg_batch;
+int cmg_batch_create(cmg_amg_solver* const* solvers, cmg_grid* const* grids, int n, cmg_batch** out);
+int cmg_batch_destroy(cmg_batch* b);
+/* The schedule: blocks of `slots` 128-thread slots (4, the default, 6 or 8; more slots hide
+ * more memory latency, fewer leave each thread more registers), groups of `group_blocks`
+ * blocks (0, the default: the resident blocks spread over the octrees) that take octrees
+ * from the shared queue, largest first.  split > 0: each
+ * octree that would not end within split x (total work / resident blocks) in such a group
+ * gets a group of its own sized for that budget (work: each octree's block-time measured by
+ * the last cmg_batch_autotune, else an estimate from its tiles per level); 0: no such groups. */
+int cmg_batch_set_schedule(cmg_batch* b, int slots, int group_blocks, double split);
+/* the plan the next solve uses: slots, small groups' blocks, groups, dedicated groups, resident blocks */
+int cmg_batch_schedule(cmg_batch* b, int* slots, int* group_blocks, int* groups, int* dedicated, int* resident_blocks);
+/* b_host / x_host: NULL (b and x in channels 1 and 0 on the device) or n host pointers
+ * (num_tiles*512 floats each, pinned for full-speed copies), copied in and out inside the
+ * call.  iters, rel_res (n values, required) as cmg_amg_solve gives them; instance_ms
+ * (n values, may be NULL): each octree's solve time inside the launch (device clock);
+ * batch_ms (may be NULL): the launch's time (CUDA events). */
+int cmg_batch_solve(cmg_batch* b, const float* const* b_host, float* const* x_host, int max_iters, double relative_tolerance,
+                    int level_iters, int coarsest_iters, int sync_stride, int is_pure_neumann, int* iters, double* rel_res,
+                    float* instance_ms, float* batch_ms);
+/* The schedule autotuner: one calibration run measures each octree's block-time; then the
+ * batch (convergence test every iteration) is timed under each candidate schedule
+ * (slots[i], group_blocks[i], split[i]; slots may be NULL: the current, split may be NULL:
+ * all 0), best of `repeats` runs after one
+ * untimed run, each run from the right-hand sides the grids hold on entry (restored at the
+ * end); keeps the fastest candidate whose solves all converge.  ms[i] = its time (-1: did
+ * not converge), *best = its index (-1: none). */
+int cmg_batch_autotune(cmg_batch* b, const int* slots, const int* group_blocks, const double* split, int ncand, int max_iters,
+                       double relative_tolerance, int level_iters, int coarsest_iters, int repeats, float* ms, int* best);
 /* GaussSeidelAMG (src/AMGSolver.cu:887) on one level */
 int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
 /* The same sweeps as the multigrid cycle runs them (the pipelined persistent kernel):
