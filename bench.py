@@ -26,8 +26,10 @@ Dirichlet walls, rhs N(0,1) per cell (numpy default_rng(0)) minus its mean.
 --workload batched64: 64 independent octrees (seed 2): finest level 4 or 5 within
 0.05 of the surfaces of 1-3 solid spheres (radius U(0.05, 0.15), centres
 U(0.2, 0.8)^3), level 3 elsewhere, 2:1 graded, each with its own Fourier-
-divergence rhs; a step solves all 64 through one cmg_amg_solve_batch call, 16
-streams; the metric is solves per second, with p50/p99 per-solve device time.
+divergence rhs; a step solves all 64 in one persistent kernel launch inside a CUDA
+graph (cmg_batch_solve, schedule picked by its autotuner); the metric is solves per
+second, with p50/p99 of each octree's solve time inside the launch.  The same batch
+as 64 graph launches on 16 streams (cmg_amg_solve_batch) is reported beside it.
 
 N > 1 runs N independent replicas: one solve works on one octree in one GPU's memory,
 and the path has no partition that avoids an exchange per sweep.
@@ -816,11 +818,16 @@ def run_ours(args, rank, world, local_rank):
 
 BATCH_METRIC = "Poisson solves per second to 1e-6 rel. residual, 64 batched adaptive octrees, 1×B200"
 BATCH_UNIT = "solves/s"
+# candidate schedules of the persistent batch: (blocks per small group, split, slots per block)
+BATCH_SCHEDULES = [(g, sp, ns) for ns in (6, 8) for g, sp in ((4, 0.0), (6, 0.0), (8, 0.0), (2, 1.0), (4, 1.0), (4, 1.2))] + [(4, 1.0, 4)]
 
 
 def run_batched(args, rank, world, local_rank):
-    """64 independent octrees per step, all solved through one cmg_amg_solve_batch call,
-    spread over BATCH_STREAMS streams so the latency-bound solves overlap on the GPU."""
+    """64 independent octrees per step, all solved by ONE persistent cooperative kernel launch
+    inside a CUDA graph (cmg_batch_solve): groups of blocks take the octrees from a device
+    queue, largest first; the schedule (slots per block, group sizes, groups of their own for
+    the largest octrees) is picked by the batch autotuner.  The same batch as 64 graph
+    launches on BATCH_STREAMS streams (cmg_amg_solve_batch) is timed beside it."""
     import torch
 
     import cmg
@@ -832,36 +839,37 @@ def run_batched(args, rank, world, local_rank):
     solvers = [make_solver(cmg) for _ in specs]
     n = len(grids)
     infos = [G.info() for G in grids]
-    nstreams = max(1, args.streams)
-    streams = [torch.cuda.Stream(device=dev) for _ in range(nstreams)]
-    for i, G in enumerate(grids):
-        G.set_stream(streams[i % nstreams].cuda_stream)
     sargs = (SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
+    batch = cmg.PersistentBatch(solvers, grids)
+
+    def restore():
+        for G in grids:
+            G.copy(BSAVE, 1)
 
     def one_batch(b_host=None, x_host=None, solve_args=None):
         if b_host is None:
-            for G in grids:
-                G.copy(BSAVE, 1)
-        return cmg.solve_batch(solvers, grids, *(solve_args or sargs), b_host=b_host, x_host=x_host)
+            restore()
+        return batch.solve(*(solve_args or sargs), b_host=b_host, x_host=x_host)
 
-    def timed(steps, **kw):
+    def timed(steps, fn, **kw):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for st in streams:
-            st.wait_event(e0)
         out = []
         for _ in range(steps):
             torch.cuda.nvtx.range_push("batch")
-            out.append(one_batch(**kw))
+            out.append(fn(**kw))
             torch.cuda.nvtx.range_pop()
-        for st in streams:
-            ev = torch.cuda.Event()
-            ev.record(st)
-            torch.cuda.current_stream().wait_event(ev)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), out
+
+    # the schedule: the autotuner times the candidates (the schedule never changes a result)
+    restore()
+    t0 = time.perf_counter()
+    sched, sched_table = batch.autotune(BATCH_SCHEDULES, *sargs[:4], repeats=2)
+    sched_s = time.perf_counter() - t0
+    slots, gblocks, ngroups, dedicated, resident = batch.schedule()
 
     for _ in range(max(args.warmup, 1)):
         one_batch()
@@ -871,28 +879,64 @@ def run_batched(args, rank, world, local_rank):
         dist.barrier()
     sampler = ClockSampler(local_rank)
     sampler.start()
-    t_ms, out = timed(args.steps)
-    launches = sum(S.last_solve_launches() for S in solvers) * args.steps
+    t_ms, out = timed(args.steps, one_batch)
     clocks = sampler.stop()
     total_ms = replica_time(t_ms, world, dev)
-    per = sorted(m for _, _, ms in out for m in ms)
-    its = [i for it, _, _ in out for i in it]
-    rels = [r for _, rel, _ in out for r in rel]
+    per = sorted(m for _, _, ms, _ in out for m in ms)
+    launch_ms = sorted(bms for _, _, _, bms in out)
+    its = [i for it, _, _, _ in out for i in it]
+    rels = [r for _, rel, _, _ in out for r in rel]
 
     # e2e: the same batch through the C ABI with pinned host buffers for b and x
     b_host = [torch.from_numpy(G.download(BSAVE).reshape(-1)).pin_memory() for G in grids]
     x_host = [torch.empty_like(b).pin_memory() for b in b_host]
     hb = dict(b_host=[b.data_ptr() for b in b_host], x_host=[x.data_ptr() for x in x_host])
     one_batch(**hb)
-    e2e_ms, _ = timed(args.steps, **hb)
+    e2e_ms, _ = timed(args.steps, one_batch, **hb)
     e2e_ms = replica_time(e2e_ms, world, dev)
     nbytes = sum(b.numel() * 4 for b in b_host)
 
-    # roofline: k_gs_pipe on the finest level of the largest octree, on the default stream
-    big = max(range(n), key=lambda i: infos[i][0])
-    grids[big].set_stream(0)
-    roof = roofline_gs(grids[big], solvers[big], cmg, torch, dev)
-    grids[big].set_stream(streams[big % nstreams].cuda_stream)
+    # roofline of the one kernel: algorithmic bytes of all 64 solves / its CUDA-event time
+    alg = sum(solve_algorithmic_bytes(G, SOLVE["mu"], SOLVE["level_iters"], it) for G, it in zip(grids, out[0][0]))
+    lms = launch_ms[len(launch_ms) // 2]
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (lms * 1e-3) / 1e9
+    roof = {"kernel": f"k_batch_solve (persistent batch: {slots} slots per block, {ngroups} groups, {dedicated} of them for one octree each)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": int(alg), "launch_ms": round(lms, 4), "traffic": None}
+
+    # the same batch as separate graph launches on BATCH_STREAMS streams
+    nstreams = max(1, args.streams)
+    streams = [torch.cuda.Stream(device=dev) for _ in range(nstreams)]
+    for i, G in enumerate(grids):
+        G.set_stream(streams[i % nstreams].cuda_stream)
+
+    def ms_batch(solve_args=None):
+        restore()
+        return cmg.solve_batch(solvers, grids, *(solve_args or sargs))
+
+    def timed_streams(steps, solve_args=None):
+        ms_batch(solve_args)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for st in streams:
+            st.wait_event(e0)
+        res = [ms_batch(solve_args) for _ in range(steps)]
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            torch.cuda.current_stream().wait_event(ev)
+        e1.record()
+        torch.cuda.synchronize()
+        return replica_time(e0.elapsed_time(e1), world, dev), res
+
+    ms_t, ms_out = timed_streams(args.steps)
+    ms_per = sorted(m for _, _, ms in ms_out for m in ms)
+    multistream = {"streams": nstreams, "solves_per_s": round(n * args.steps * world / (ms_t / 1e3), 2),
+                   "solve_ms_p50": ms_per[len(ms_per) // 2], "solve_ms_p99": ms_per[min(len(ms_per) - 1, int(0.99 * len(ms_per)))]}
+    for G in grids:
+        G.set_stream(0)
 
     # the autotuned smoother: tuned once on octree 0 with a training rhs, applied to all 64
     tuned = None
@@ -906,15 +950,24 @@ def run_batched(args, rank, world, local_rank):
             for S in solvers:
                 S.omega, S.mu_cycle_repeat_times, S.finest_iters = best[0], best[1], best[4]
             targs = (SOLVE["max_iters"], SOLVE["tol"], best[2], best[3], SOLVE["sync_stride"], False)
+            restore()
+            tsched, _ = batch.autotune(BATCH_SCHEDULES, *targs[:4], repeats=1)
             one_batch(solve_args=targs)
-            t_t, out_t = timed(args.steps, solve_args=targs)
-            per_t = sorted(m for _, _, ms in out_t for m in ms)
-            its_t = [i for it, _, _ in out_t for i in it]
+            t_t, out_t = timed(args.steps, one_batch, solve_args=targs)
+            per_t = sorted(m for _, _, ms, _ in out_t for m in ms)
+            its_t = [i for it, _, _, _ in out_t for i in it]
+            for i, G in enumerate(grids):
+                G.set_stream(streams[i % nstreams].cuda_stream)
+            ms_tt, _ = timed_streams(args.steps, targs)
+            for G in grids:
+                G.set_stream(0)
             tuned = {"tuned_on": "octree 0, one training rhs (Fourier seed 200)", "tune_s": round(tune_s, 3),
                      "omega": best[0], "mu": best[1], "level_iters": best[2], "coarsest_iters": best[3], "finest_iters": best[4],
+                     "schedule": list(tsched) if tsched is not None else None,
                      "solves_per_s": round(n * args.steps * world / (replica_time(t_t, world, dev) / 1e3), 2),
+                     "multistream_solves_per_s": round(n * args.steps * world / (ms_tt / 1e3), 2),
                      "pcg_iters_mean": round(float(np.mean(its_t)), 2), "pcg_iters_max": int(max(its_t)),
-                     "rel_residual_max": max(r for _, rel, _ in out_t for r in rel),
+                     "rel_residual_max": max(r for _, rel, _, _ in out_t for r in rel),
                      "solve_ms_p50": per_t[len(per_t) // 2], "solve_ms_p99": per_t[min(len(per_t) - 1, int(0.99 * len(per_t)))]}
             for S in solvers:
                 S.omega, S.mu_cycle_repeat_times, S.finest_iters = SOLVE["omega"], SOLVE["mu"], -1
@@ -928,18 +981,26 @@ def run_batched(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {
                 "workload": WORKLOADS["batched64"], "method": "plain FP32 FAS mu-cycle (mu=2) MG-PCG, FP64 dots, batched",
-                "instances": n, "streams": nstreams, "tiles": int(sum(i[0] for i in infos)),
+                "execution": "one persistent cooperative kernel launch per batch, inside a CUDA graph",
+                "schedule": {"slots_per_block": slots, "small_group_blocks": gblocks, "groups": ngroups, "dedicated_groups": dedicated,
+                             "resident_blocks": resident, "split": (sched[1] if sched is not None and not isinstance(sched, int) else 0.0),
+                             "tune_s": round(sched_s, 3),
+                             "candidates_ms": {str(tuple(c) if not isinstance(c, int) else c): round(m, 2) for c, m in zip(BATCH_SCHEDULES, sched_table)}},
+                "instances": n, "tiles": int(sum(i[0] for i in infos)),
                 "leaf_cells": int(sum(i[2] for i in infos)) * 512, "finest_levels": sorted({int(i[1]) for i in infos}),
                 "pcg_iters_mean": round(float(np.mean(its)), 2), "pcg_iters_max": int(max(its)), "rel_residual_max": max(rels),
                 "solve_ms_p50": per[len(per) // 2], "solve_ms_p99": per[min(len(per) - 1, int(0.99 * len(per)))],
+                "per_solve_ms_is": "each octree's solve time inside the launch (device clock)",
+                "launch_ms_median": round(lms, 4),
+                "multistream": multistream,
                 "l2": f"inputs larger than L2: {16 * sum(i[0] for i in infos) * 2048 / 1e9:.1f} GB of channel planes",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "autotuned_smoother": tuned,
             },
             "e2e": {"value": round(n * args.steps * world / (e2e_ms / 1e3), 2), "unit": BATCH_UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
-            "gpu_launches": int(launches),
-            "roofline": roofline_entry(*roof),
+            "gpu_launches": int(args.steps),
+            "roofline": roof,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
@@ -949,8 +1010,6 @@ def run_batched(args, rank, world, local_rank):
                 cb["value"] = 1000.0 / cb["value"]
             cb["unit"] = BATCH_UNIT
             result["cpu_baseline"] = cb
-    for G in grids:
-        G.set_stream(0)
     return result
 
 
