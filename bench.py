@@ -834,13 +834,17 @@ def run_batched(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    specs = instance_specs("batched64")
+    specs = instance_specs("batched64")[:max(1, args.batch_instances)]
     grids = [build_grid(cmg, sp) for sp in specs]
     solvers = [make_solver(cmg) for _ in specs]
     n = len(grids)
     infos = [G.info() for G in grids]
     sargs = (SOLVE["max_iters"], SOLVE["tol"], SOLVE["level_iters"], SOLVE["coarsest_iters"], SOLVE["sync_stride"], False)
     batch = cmg.PersistentBatch(solvers, grids)
+    fixed = None
+    if args.batch_schedule:
+        g_, sp_, ns_ = args.batch_schedule.split(",")
+        fixed = (int(g_), float(sp_), int(ns_))
 
     def restore():
         for G in grids:
@@ -867,7 +871,12 @@ def run_batched(args, rank, world, local_rank):
     # the schedule: the autotuner times the candidates (the schedule never changes a result)
     restore()
     t0 = time.perf_counter()
-    sched, sched_table = batch.autotune(BATCH_SCHEDULES, *sargs[:4], repeats=2)
+    if fixed is None:
+        cands = BATCH_SCHEDULES
+        sched, sched_table = batch.autotune(cands, *sargs[:4], repeats=2)
+    else:
+        cands, sched, sched_table = [], fixed, []
+        batch.set_schedule(*fixed)
     sched_s = time.perf_counter() - t0
     slots, gblocks, ngroups, dedicated, resident = batch.schedule()
 
@@ -951,7 +960,9 @@ def run_batched(args, rank, world, local_rank):
                 S.omega, S.mu_cycle_repeat_times, S.finest_iters = best[0], best[1], best[4]
             targs = (SOLVE["max_iters"], SOLVE["tol"], best[2], best[3], SOLVE["sync_stride"], False)
             restore()
-            tsched, _ = batch.autotune(BATCH_SCHEDULES, *targs[:4], repeats=1)
+            tsched = fixed
+            if fixed is None:
+                tsched, _ = batch.autotune(BATCH_SCHEDULES, *targs[:4], repeats=1)
             one_batch(solve_args=targs)
             t_t, out_t = timed(args.steps, one_batch, solve_args=targs)
             per_t = sorted(m for _, _, ms, _ in out_t for m in ms)
@@ -985,7 +996,7 @@ def run_batched(args, rank, world, local_rank):
                 "schedule": {"slots_per_block": slots, "small_group_blocks": gblocks, "groups": ngroups, "dedicated_groups": dedicated,
                              "resident_blocks": resident, "split": (sched[1] if sched is not None and not isinstance(sched, int) else 0.0),
                              "tune_s": round(sched_s, 3),
-                             "candidates_ms": {str(tuple(c) if not isinstance(c, int) else c): round(m, 2) for c, m in zip(BATCH_SCHEDULES, sched_table)}},
+                             "candidates_ms": {str(tuple(c) if not isinstance(c, int) else c): round(m, 2) for c, m in zip(cands, sched_table)}},
                 "instances": n, "tiles": int(sum(i[0] for i in infos)),
                 "leaf_cells": int(sum(i[2] for i in infos)) * 512, "finest_levels": sorted({int(i[1]) for i in infos}),
                 "pcg_iters_mean": round(float(np.mean(its)), 2), "pcg_iters_max": int(max(its)), "rel_residual_max": max(rels),
@@ -1067,6 +1078,9 @@ def main():
                     help="inference kernel of the learned smoother")
     ap.add_argument("--workload", default="sphere", choices=sorted(WORKLOADS))
     ap.add_argument("--streams", type=int, default=BATCH_STREAMS, help="streams of the batched workload")
+    ap.add_argument("--batch-instances", type=int, default=64, help="batched workload: solve only its first N octrees (profiling)")
+    ap.add_argument("--batch-schedule", default=None,
+                    help="batched workload: a fixed schedule 'group_blocks,split,slots' instead of the autotuned one (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
