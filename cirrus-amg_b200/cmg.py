@@ -55,6 +55,7 @@ EXPORTS = [
     "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
     "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct", "cmg_amg_solver_set_cycle_bf16",
     "cmg_batch_create", "cmg_batch_destroy", "cmg_batch_set_schedule", "cmg_batch_schedule", "cmg_batch_solve", "cmg_batch_autotune",
+    "cmg_amg_vcycle", "cmg_amg_mu_cycle", "cmg_amg_fas_f_cycle",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -132,6 +133,9 @@ def lib():
             "cmg_amg_last_solve_ms": (I, [P, P]),
             "cmg_amg_last_solve_launches": (I, [P, P]),
             "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
+            "cmg_amg_vcycle": (I, [P, P, I, I, I, I, I]),
+            "cmg_amg_mu_cycle": (I, [P, P, I, I, I, I, I, I]),
+            "cmg_amg_fas_f_cycle": (I, [P, P, I, I, I, I, I]),
             "cmg_batch_create": (I, [P, P, I, P]),
             "cmg_batch_destroy": (I, [P]),
             "cmg_batch_set_schedule": (I, [P, I, I, D]),
@@ -620,6 +624,21 @@ class AMGSolver:
     def fas_mu_cycle(self, grid, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters):
         self._sync_params()
         _check(self.L.cmg_amg_fas_mu_cycle(self.h, grid.h, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters), "fas_mu_cycle")
+
+    def VCycle(self, grid, x_ch, f_ch, rhs_ch, level_iters, coarsest_iters):
+        """AMGSolver::VCycle (src/AMGSolver.cu:1060): correction-scheme V-cycle from x = 0 for rhs f."""
+        self._sync_params()
+        _check(self.L.cmg_amg_vcycle(self.h, grid.h, x_ch, f_ch, rhs_ch, level_iters, coarsest_iters), "VCycle")
+
+    def muCycle(self, repeat_times, grid, x_ch, f_ch, rhs_ch, level_iters, coarsest_iters):
+        """AMGSolver::muCycle (src/AMGSolver.cu:1151): correction-scheme mu-cycle from x = 0 for rhs f."""
+        self._sync_params()
+        _check(self.L.cmg_amg_mu_cycle(self.h, grid.h, repeat_times, x_ch, f_ch, rhs_ch, level_iters, coarsest_iters), "muCycle")
+
+    def FASFCycle(self, grid, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters):
+        """AMGSolver::FASFCycle (src/AMGSolver.cu:1358): the FAS full-multigrid cycle."""
+        self._sync_params()
+        _check(self.L.cmg_amg_fas_f_cycle(self.h, grid.h, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters), "FASFCycle")
 
     def FASMuCycleSolve(self, repeat_times, grid, verbose, max_iters, relative_tolerance, level_iters, coarsest_iters):
         """AMGSolver::FASMuCycleSolve (src/AMGSolver.cu:1311): mu-cycles as a stand-alone iteration."""

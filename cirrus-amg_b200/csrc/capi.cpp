@@ -807,6 +807,47 @@ int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, i
     s->s.enqueue_mu_cycle(g->g, A, g->g.stream);
     return cmg::check_cuda(cudaGetLastError(), "fas_mu_cycle");
 }
+static int cycle_args_ok(cmg_amg_solver* s, cmg_grid* g, const char* what) {
+    if (!s || !grid_ready(g)) return fail(CMG_ERR_STATE, "solver or grid not ready");
+    if (s->s.kind != cmg::kAMG) return fail(CMG_ERR_STATE, (std::string(what) + ": not an AMG solver").c_str());
+    return cmg::validate_solver_topology(g->g);
+}
+int cmg_amg_vcycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters) {
+    GUARD_BEGIN
+    if (int rc = cycle_args_ok(s, g, "cmg_amg_vcycle")) return rc;
+    if (!chan_ok(g, x_ch) || !chan_ok(g, f_ch) || !chan_ok(g, rhs_ch) || x_ch == f_ch || x_ch == rhs_ch || f_ch == rhs_ch ||
+        level_iters < 0 || coarsest_iters < 0)
+        return fail(CMG_ERR_INVALID, "cmg_amg_vcycle: bad argument");
+    cmg::Grid& G = g->g;
+    s->s.enqueue_vcycle_cs(G, G.plane(x_ch), G.plane(f_ch), G.plane(rhs_ch), level_iters, coarsest_iters, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "vcycle");
+    GUARD_END
+}
+int cmg_amg_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int repeat_times, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters) {
+    GUARD_BEGIN
+    if (int rc = cycle_args_ok(s, g, "cmg_amg_mu_cycle")) return rc;
+    if (!chan_ok(g, x_ch) || !chan_ok(g, f_ch) || !chan_ok(g, rhs_ch) || x_ch == f_ch || x_ch == rhs_ch || f_ch == rhs_ch ||
+        repeat_times < 0 || level_iters < 0 || coarsest_iters < 0)
+        return fail(CMG_ERR_INVALID, "cmg_amg_mu_cycle: bad argument");
+    cmg::Grid& G = g->g;
+    s->s.enqueue_mu_cycle_cs(G, repeat_times, G.plane(x_ch), G.plane(f_ch), G.plane(rhs_ch), level_iters, coarsest_iters, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "mu_cycle");
+    GUARD_END
+}
+int cmg_amg_fas_f_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters) {
+    GUARD_BEGIN
+    if (int rc = cycle_args_ok(s, g, "cmg_amg_fas_f_cycle")) return rc;
+    if (!chan_ok(g, x_ch) || !chan_ok(g, rhs_ch) || !chan_ok(g, x0_ch) || x_ch == rhs_ch || x_ch == x0_ch || rhs_ch == x0_ch ||
+        level_iters < 0 || coarsest_iters < 0)
+        return fail(CMG_ERR_INVALID, "cmg_amg_fas_f_cycle: bad argument");
+    cmg::Grid& G = g->g;
+    const cmg::MuArgs A = s->s.mu_args(G, x_ch, rhs_ch, x0_ch, level_iters, coarsest_iters);
+    if (int rc = s->s.ensure_coeff16(G)) return rc;
+    s->s.enqueue_operand_pack(G, G.stream);
+    s->s.enqueue_fas_f_cycle(G, A, G.stream);
+    return cmg::check_cuda(cudaGetLastError(), "fas_f_cycle");
+    GUARD_END
+}
 int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms) {
     if (!s || !ms) return fail(CMG_ERR_INVALID, "null argument");
     *ms = s->s.last_ms;

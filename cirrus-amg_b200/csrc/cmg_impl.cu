@@ -808,6 +808,65 @@ void Solver::enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const {
     enqueue_mu_step(G, G.max_level(), A, st);
 }
 
+// AMGSolver::VCycle (src/AMGSolver.cu:1060-1128): downstroke of pre-smoothing and
+// restriction (the coarse x becomes the mean of the fine x), the coarsest level, then
+// prolongation x += P x_coarse and post-smoothing, coarse to fine
+void Solver::enqueue_vcycle_cs(Grid& G, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    launch_cycle_init(d, X, RHS, F, st);
+    for (int l = G.max_level(); l > 0; --l) {
+        enqueue_gs(G, l, level_iters, 0, X, RHS, st);
+        launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), X, RHS, coeff_ch, R_restrict, st);
+    }
+    enqueue_gs(G, 0, coarsest_iters / 2, 0, X, RHS, st);
+    enqueue_gs(G, 0, coarsest_iters / 2, 1, X, RHS, st);
+    for (int l = 1; l <= G.max_level(); ++l) {
+        launch_prolong_add(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), X, P, st);
+        enqueue_gs(G, l, level_iters, 1, X, RHS, st);
+    }
+}
+// AMGSolver::muCycleStep (src/AMGSolver.cu:1130-1149): below the pre-smoothing and the
+// restriction, the LEAF tiles of the coarser level take rhs = f minus the flux from their
+// NONLEAF neighbours and the NONLEAF tiles start from x = 0
+void Solver::enqueue_mu_step_cs(Grid& G, int l, int repeat_times, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters,
+                                cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    if (l == 0) {
+        enqueue_gs(G, 0, coarsest_iters / 2, 0, X, RHS, st);
+        enqueue_gs(G, 0, coarsest_iters / 2, 1, X, RHS, st);
+        return;
+    }
+    enqueue_gs(G, l, level_iters, 0, X, RHS, st);
+    launch_restrict(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), X, RHS, coeff_ch, R_restrict, st);
+    launch_deduct_flux(d, G.level_begin(l - 1), G.nonleaf_begin(l - 1) - G.level_begin(l - 1), X, F, RHS, coeff_ch, st);
+    const int nb0 = G.nonleaf_begin(l - 1), nbn = G.ghost_begin(l - 1) - nb0;
+    if (nbn > 0) launch_fill(X + (size_t)nb0 * kCells, (size_t)nbn * kCells, 0.0f, st);
+    for (int r = 0; r < repeat_times; ++r) enqueue_mu_step_cs(G, l - 1, repeat_times, X, F, RHS, level_iters, coarsest_iters, st);
+    launch_prolong_add(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), X, P, st);
+    enqueue_gs(G, l, level_iters, 1, X, RHS, st);
+}
+// AMGSolver::muCycle (src/AMGSolver.cu:1151-1174)
+void Solver::enqueue_mu_cycle_cs(Grid& G, int repeat_times, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters,
+                                 cudaStream_t st) const {
+    launch_cycle_init(G.dev(), X, RHS, F, st);
+    enqueue_mu_step_cs(G, G.max_level(), repeat_times, X, F, RHS, level_iters, coarsest_iters, st);
+}
+// AMGSolver::FASFCycle (src/AMGSolver.cu:1358-1387); the rhs goes down by
+// RestrictSourceToCoarse (:1295-1307): R times the sum of the 8 children's INTERIOR values
+void Solver::enqueue_fas_f_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const {
+    const DevGrid d = G.dev();
+    launch_fill(A.X, (size_t)G.n * kCells, 0.0f, st);
+    for (int l = G.max_level(); l > 0; --l)
+        launch_accumulate_cells(d, G.level_begin(l), G.ghost_begin(l) - G.level_begin(l), dLeaf | dNonLeaf, A.RHS, A.RHS, A.Rr, false, st,
+                                dInterior);
+    enqueue_gs(G, 0, A.coarsest_iters / 2, 0, A.X, A.RHS, st);
+    enqueue_gs(G, 0, A.coarsest_iters / 2, 1, A.X, A.RHS, st);
+    for (int l = 1; l <= G.max_level(); ++l) {
+        launch_prolong_add(d, G.level_begin(l), G.level_end(l) - G.level_begin(l), A.X, A.P, st);
+        enqueue_mu_step(G, l, A, st);
+    }
+}
+
 static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t>& tail) {
     cudaStreamCaptureStatus stt;
     const cudaGraphNode_t* deps = nullptr;

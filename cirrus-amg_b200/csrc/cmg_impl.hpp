@@ -154,6 +154,16 @@ struct Solver {
                     void* X16 = nullptr, const void* RHS16 = nullptr) const;
     void enqueue_mu_step(Grid& G, int level, const MuArgs& A, cudaStream_t st, bool fas2 = false) const;
     void enqueue_mu_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
+    // AMGSolver::VCycle (src/AMGSolver.cu:1060-1128) and muCycle (:1151-1174): correction
+    // schemes from x = 0 with right-hand side f (channel F, read only) and working rhs RHS
+    void enqueue_vcycle_cs(Grid& G, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters, cudaStream_t st) const;
+    void enqueue_mu_cycle_cs(Grid& G, int repeat_times, float* X, const float* F, float* RHS, int level_iters, int coarsest_iters,
+                             cudaStream_t st) const;
+    void enqueue_mu_step_cs(Grid& G, int level, int repeat_times, float* X, const float* F, float* RHS, int level_iters,
+                            int coarsest_iters, cudaStream_t st) const;
+    // AMGSolver::FASFCycle (src/AMGSolver.cu:1358-1387): the rhs restricted to every level, the
+    // coarsest level smoothed, then prolongation and one FASMuCycleStep per level, coarse to fine
+    void enqueue_fas_f_cycle(Grid& G, const MuArgs& A, cudaStream_t st) const;
     bool use_graph = true;    // false: launch kernel by kernel from the host (profiling)
     bool use_persist = false;  // levels 2-3 in one cooperative kernel per visit
     bool use_cluster = true;   // levels 0-2 in one cluster launch per visit of level 2

@@ -262,7 +262,8 @@ __global__ void __launch_bounds__(128) k_geo_vinit(DevGrid g, float* X, float* R
 
 // AccumulateToParentsOneStepKernel (src/PoissonGrid.cu:408-449) from the tiles of type `types`:
 // parent cell = coeff * sum of its 8 children (added to it when `additive`)
-__global__ void __launch_bounds__(64) k_accumulate_cells(DevGrid g, int t0, int types, const float* SRC, float* DST, float coeff, int additive) {
+__global__ void __launch_bounds__(64) k_accumulate_cells(DevGrid g, int t0, int types, const float* SRC, float* DST, float coeff, int additive,
+                                                         int cell_mask) {
     const int t = t0 + blockIdx.x;
     if (!(tile_type(g, t) & types)) return;
     const int p = g.nb[8 * t + 6];
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(64) k_accumulate_cells(DevGrid g, int t0, int 
         for (int jj = 0; jj < 2; ++jj)
             for (int kk = 0; kk < 2; ++kk) {
                 const size_t o = (size_t)t * kCells + cell_index(f0 + ii, f1 + jj, f2 + kk);
-                sum = __fadd_rn(sum, (g.ctype[o] & (dInterior | dDirichlet | dNeumann)) ? ldcg(SRC + o) : 0.0f);
+                sum = __fadd_rn(sum, (g.ctype[o] & cell_mask) ? ldcg(SRC + o) : 0.0f);
             }
     const int4 m = g.meta[t];
     const size_t po = (size_t)p * kCells + cell_index(parent_local(m.y, f0), parent_local(m.z, f1), parent_local(m.w, f2));
@@ -352,10 +353,10 @@ void launch_geo_vinit(const DevGrid& g, float* X, float* RHS, const float* F, cu
     k_geo_vinit<<<g.n, 128, 0, st>>>(g, X, RHS, F);
 }
 void launch_accumulate_cells(const DevGrid& g, int t0, int nt, int types, const float* SRC, float* DST, float coeff, bool additive,
-                             cudaStream_t st) {
+                             cudaStream_t st, int cell_mask) {
     if (nt <= 0) return;
     note_kernel_launch();
-    k_accumulate_cells<<<nt, 64, 0, st>>>(g, t0, types, SRC, DST, coeff, additive ? 1 : 0);
+    k_accumulate_cells<<<nt, 64, 0, st>>>(g, t0, types, SRC, DST, coeff, additive ? 1 : 0, cell_mask);
 }
 
 }  // namespace cmg

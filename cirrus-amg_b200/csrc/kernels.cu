@@ -35,6 +35,80 @@ __global__ void __launch_bounds__(128) k_prolong(DevGrid g, int t0, float* X, co
     tile_prolong(g, t0 + blockIdx.x, threadIdx.x, X, X0, P);
 }
 
+// ---------------------------------------------------------------------------
+// Steps of the cycles nothing in the reference's solve calls: AMGSolver::VCycle and
+// muCycle (src/AMGSolver.cu:1060-1173), correction schemes with a separate right-hand side
+// f, and the prolongation of FASFCycle (src/AMGSolver.cu:1358-1387).
+// ---------------------------------------------------------------------------
+// the cycle's start: x = 0 on every tile, rhs = f on LEAF and NONLEAF tiles, 0 on GHOST
+// tiles (src/AMGSolver.cu:1063-1080)
+__global__ void __launch_bounds__(128) k_cycle_init(DevGrid g, float* X, float* RHS, const float* F) {
+    const int t = blockIdx.x;
+    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    st4(X + base, z);
+    st4(RHS + base, (tile_type(g, t) & dGhost) ? z : ld4(F + base));
+}
+// ProlongateAndUpdateAMG128Kernel (src/AMGSolver.cu:1026-1057) on every tile of a level:
+// GHOST cells take the parent's x, the others add P times it; 0 on cells that are not INTERIOR
+__global__ void __launch_bounds__(128) k_prolong_add(DevGrid g, int t0, float* X, float P) {
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    const int4 m = g.meta[t];
+    const bool ghost = (m.x >> 8) & dGhost;
+    const int p = g.nb[8 * t + 6];
+    const float4 xr = ld4(X + Q.base);
+    const uchar4 ty = ldt4(g.ctype + Q.base);
+    const int pi = parent_local(m.y, Q.i), pj = parent_local(m.z, Q.j);
+    float4 out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const float cx = p >= 0 ? X[(size_t)p * kCells + cell_index(pi, pj, parent_local(m.w, Q.k0 + u))] : 0.0f;
+        const bool in = t4get(ty, u) & dInterior;
+        f4set(out, u, ghost ? (in ? cx : 0.0f) : (in ? __fmaf_rn(P, cx, f4get(xr, u)) : 0.0f));
+    }
+    st4(X + Q.base, out);
+}
+// DeductFluxOnAbsLeafs128Kernel (src/AMGSolver.cu:966-992) on LEAF tiles: rhs = f minus the
+// operator's terms from cells of NONLEAF neighbour tiles (AMGLaplacianTileData::
+// negativeLapOuterNonLeaf, src/AMGSolver.cu:384-405: the tile's own cells count 0, each face
+// term in the order -x,+x,-y,+y,-z,+z) on INTERIOR cells, 0 elsewhere
+__global__ void __launch_bounds__(128) k_deduct_flux(DevGrid g, int t0, const float* X, const float* F, float* RHS, int coeff_ch) {
+    __shared__ Snap S;
+    const int t = t0 + blockIdx.x;
+    const Quad Q(t, threadIdx.x);
+    Own o;
+    load_snap(g, t, X, coeff_ch, MgHalo{X, g.ctype}, S, Q, o, BlockSync{});
+    bool nonleaf[6];  // -x, -y, -z, +x, +y, +z neighbour tile is NONLEAF
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int d = g.nbx[8 * t + f];
+        nonleaf[f] = d != 0 && (d & 7) == dNonLeaf;
+    }
+    const float4 fv = ld4(F + Q.base);
+    float4 out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int i = Q.i, j = Q.j, k = Q.k0 + u;
+        const float d = f4get(o.dg, u);
+        float s = 0.0f;
+        if (d != 0.0f) {
+            s = __fmul_rn(0.0f, d);
+            // -x, +x
+            s = __fmaf_rn(S.c0[i * 64 + j * 8 + k], (i == 0 && nonleaf[0]) ? S.x[sx(i - 1, j, k)] : 0.0f, s);
+            s = __fmaf_rn(S.c0[(i + 1) * 64 + j * 8 + k], (i == 7 && nonleaf[3]) ? S.x[sx(i + 1, j, k)] : 0.0f, s);
+            // -y, +y
+            s = __fmaf_rn(S.c1[i * 72 + j * 8 + k], (j == 0 && nonleaf[1]) ? S.x[sx(i, j - 1, k)] : 0.0f, s);
+            s = __fmaf_rn(S.c1[i * 72 + (j + 1) * 8 + k], (j == 7 && nonleaf[4]) ? S.x[sx(i, j + 1, k)] : 0.0f, s);
+            // -z, +z
+            s = __fmaf_rn(S.c2[i * 72 + j * 9 + k], (k == 0 && nonleaf[2]) ? S.x[sx(i, j, k - 1)] : 0.0f, s);
+            s = __fmaf_rn(S.c2[i * 72 + j * 9 + k + 1], (k == 7 && nonleaf[5]) ? S.x[sx(i, j, k + 1)] : 0.0f, s);
+        }
+        f4set(out, u, (t4get(o.ty, u) & dInterior) ? __fsub_rn(f4get(fv, u), s) : 0.0f);
+    }
+    st4(RHS + Q.base, out);
+}
+
 __global__ void __launch_bounds__(1024) k_coarse(DevGrid g, CoarseArgs A, float* X, float* RHS, float* X0) {
     extern __shared__ __align__(16) unsigned char smraw[];
     coarse_dense(g, A, X, RHS, X0, smraw);
@@ -903,6 +977,15 @@ void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RH
 }
 void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st) {
     if (nt > 0) count_launch(), k_prolong<<<nt, 128, 0, st>>>(g, t0, X, X0, P);
+}
+void launch_cycle_init(const DevGrid& g, float* X, float* RHS, const float* F, cudaStream_t st) {
+    if (g.n > 0) count_launch(), k_cycle_init<<<g.n, 128, 0, st>>>(g, X, RHS, F);
+}
+void launch_prolong_add(const DevGrid& g, int t0, int nt, float* X, float P, cudaStream_t st) {
+    if (nt > 0) count_launch(), k_prolong_add<<<nt, 128, 0, st>>>(g, t0, X, P);
+}
+void launch_deduct_flux(const DevGrid& g, int t0, int nt, const float* X, const float* F, float* RHS, int coeff_ch, cudaStream_t st) {
+    if (nt > 0) count_launch(), k_deduct_flux<<<nt, 128, 0, st>>>(g, t0, X, F, RHS, coeff_ch);
 }
 size_t coarse_step_smem_bytes() { return kCoarseSmem; }
 void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters,

@@ -37,8 +37,9 @@ void launch_geo_prolong(const DevGrid& g, int t0, int nt, float* X, float P, cud
 void launch_geo_vinit(const DevGrid& g, float* X, float* RHS, const float* F, cudaStream_t st);
 // CalcCellTypesFromLeafs step 1 on the NONLEAF tiles in t0..t0+nt (one level per launch, finest first)
 void launch_types_from_children(const DevGrid& g, int t0, int nt, cudaStream_t st);
+// cell_mask: the cell types whose values count (AccumulateToParentsOneStepKernel's cell_types)
 void launch_accumulate_cells(const DevGrid& g, int t0, int nt, int types, const float* SRC, float* DST, float coeff, bool additive,
-                             cudaStream_t st);
+                             cudaStream_t st, int cell_mask = dInterior | dDirichlet | dNeumann);
 
 // --- multigrid ---
 // persistent, software-pipelined colour pass for the multigrid cycle (gs_pipe.cu); needs the
@@ -89,6 +90,12 @@ void launch_gs(const DevGrid& g, int t0, int nt, float* X, const float* B, int c
 void launch_restrict(const DevGrid& g, int t0, int nt, float* X, float* RHS, int coeff_ch, float R_restrict, cudaStream_t st);
 void launch_fas_save(const DevGrid& g, int t0, int nt, const float* X, float* RHS, float* X0, int coeff_ch, cudaStream_t st);
 void launch_prolong(const DevGrid& g, int t0, int nt, float* X, const float* X0, float P, cudaStream_t st);
+// the correction-scheme cycles (AMGSolver::VCycle / muCycle) and FASFCycle: x = 0 and rhs = f
+// (0 on GHOST tiles) on every tile; prolongation x += P x_parent (GHOST: x = x_parent) on the
+// tiles t0..t0+nt of one level; rhs = f - (terms from NONLEAF neighbour tiles) on LEAF tiles
+void launch_cycle_init(const DevGrid& g, float* X, float* RHS, const float* F, cudaStream_t st);
+void launch_prolong_add(const DevGrid& g, int t0, int nt, float* X, float P, cudaStream_t st);
+void launch_deduct_flux(const DevGrid& g, int t0, int nt, const float* X, const float* F, float* RHS, int coeff_ch, cudaStream_t st);
 // Whole FASMuCycleStep of level `top` (0 or 1) in one thread block, the
 // root and its eight children resident in shared memory as dense grids.
 void launch_coarse_step(const DevGrid& g, int top, float* X, float* RHS, float* X0, int coeff_ch, int mu, int level_iters,

@@ -420,6 +420,18 @@ int cmg_amg_gauss_seidel(cmg_amg_solver* s, cmg_grid* g, int iters, int order, i
 int cmg_amg_gauss_seidel_masked(cmg_amg_solver* s, cmg_grid* g, int iters, int order, int level, int x_ch, int rhs_ch);
 /* AMGSolver::FASMuCycle (src/AMGSolver.cu:1279) */
 int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters);
+/* The cycles nothing in the reference's solve calls, on the grid's stream:
+ * AMGSolver::VCycle (src/AMGSolver.cu:1060): a correction-scheme V-cycle from x = 0 (every
+ * tile) with right-hand side f (f_ch, read only) copied into rhs_ch (0 on GHOST tiles);
+ * AMGSolver::muCycle (src/AMGSolver.cu:1151): its mu-cycle, repeat_times visits of each
+ * coarser level, the LEAF tiles of a coarser level solving for f minus the flux from their
+ * NONLEAF neighbours (muCycleStep, :1130); AMGSolver::FASFCycle (src/AMGSolver.cu:1358): the
+ * rhs restricted to every level, the coarsest level smoothed, then prolongation and one
+ * FASMuCycleStep per level from coarse to fine (x0_ch: the saved x).  Channels must be
+ * distinct. */
+int cmg_amg_vcycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters);
+int cmg_amg_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int repeat_times, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters);
+int cmg_amg_fas_f_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters);
 /* device time of the last cmg_amg_solve, milliseconds (CUDA events) */
 int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms);
 /* number of this library's kernels the last cmg_amg_solve executed (counted

@@ -1016,6 +1016,155 @@ void og_fas_mu_cycle(og_grid* g, int mu, int x_ch, int rhs_ch, int x0_ch, int co
     fas_step(g, g->max_level, &A);
 }
 
+/* ------------------------------------------------------------------ */
+/* the cycles nothing in the reference's solve calls                   */
+/* ------------------------------------------------------------------ */
+/* AMGSolver::VCycle / muCycle start (AMGSolver.cu:1063-1080): x = 0 on every tile, rhs = f on
+ * LEAF and NONLEAF tiles, 0 on GHOST tiles */
+static void cycle_init(og_grid* g, int x_ch, int f_ch, int rhs_ch) {
+    for (int t = 0; t < g->n; t++) {
+        int ghost = g->t[t].type & OG_GHOST;
+        for (int v = 0; v < NC; v++) {
+            CH(g, x_ch, t)[v] = 0.0f;
+            CH(g, rhs_ch, t)[v] = ghost ? 0.0f : CH(g, f_ch, t)[v];
+        }
+    }
+}
+/* ProlongateAndUpdateAMG128Kernel (AMGSolver.cu:1026-1057), every tile of `level`: GHOST cells
+ * take the parent's x, the others add P times it; 0 on cells that are not INTERIOR */
+static void prolong_add(og_grid* g, int level, int x_ch, float P) {
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int t = 0; t < g->n; t++) {
+        if (g->t[t].level != level) continue;
+        int p = g->parent[t];
+        int ghost = g->t[t].type & OG_GHOST;
+        float* X = CH(g, x_ch, t);
+        for (int v = 0; v < NC; v++) {
+            float cx = p >= 0 ? CH(g, x_ch, p)[parent_cell(g, t, v)] : 0.0f;
+            int in = CT(g, t)[v] & OG_INTERIOR;
+            if (ghost) X[v] = in ? cx : 0.0f;
+            else X[v] = in ? fmaf(P, cx, X[v]) : 0.0f;
+        }
+    }
+}
+/* DeductFluxOnAbsLeafs128Kernel (AMGSolver.cu:966-992) on the LEAF tiles of `level`: rhs = f
+ * - negativeLapOuterNonLeaf (AMGSolver.cu:384-405) on INTERIOR cells, 0 elsewhere.  Only
+ * cells of NONLEAF neighbour tiles count; the tile's own cells (LEAF) count 0. */
+static void deduct_flux(og_grid* g, int level, int x_ch, int coeff_ch, int f_ch, int rhs_ch) {
+#pragma omp parallel
+    {
+        og_snap* S = (og_snap*)malloc(sizeof(og_snap));
+#pragma omp for schedule(dynamic, 8)
+        for (int t = 0; t < g->n; t++) {
+            if (g->t[t].level != level || !(g->t[t].type & OG_LEAF)) continue;
+            load_snap(g, t, x_ch, coeff_ch, S);
+            for (int v = 0; v < NC; v++) {
+                int c[3] = {v >> 6, (v >> 3) & 7, v & 7};
+                float d = S->d[v], s = 0.0f;
+                if (d != 0.0f) {
+                    s = 0.0f * d;
+                    for (int axis = 0; axis < 3; axis++)
+                        for (int side = 0; side < 2; side++) {
+                            int sgn = side ? 1 : -1;
+                            int n[3] = {c[0], c[1], c[2]}, u[3] = {c[0], c[1], c[2]};
+                            n[axis] += sgn;
+                            u[axis] += side;
+                            float x1 = 0.0f;
+                            if (n[axis] < 0 || n[axis] > 7) {
+                                int q = g->nbr[t * 6 + axis + (side ? 3 : 0)];
+                                if (q >= 0 && g->t[q].type == OG_NONLEAF) x1 = S->x[SX(n[0], n[1], n[2])];
+                            }
+                            s = fmaf(S->c[axis][SX(u[0], u[1], u[2])], x1, s);
+                        }
+                }
+                CH(g, rhs_ch, t)[v] = (CT(g, t)[v] & OG_INTERIOR) ? CH(g, f_ch, t)[v] - s : 0.0f;
+            }
+        }
+        free(S);
+    }
+}
+/* SetLevelZeroAbsTiles128Kernel (AMGSolver.cu:1001-1018): x = 0 on the NONLEAF tiles of `level` */
+static void set_zero_nonleaf(og_grid* g, int level, int x_ch) {
+    for (int t = 0; t < g->n; t++)
+        if (g->t[t].level == level && (g->t[t].type & OG_NONLEAF)) memset(CH(g, x_ch, t), 0, sizeof(float) * NC);
+}
+typedef struct {
+    int rep, x_ch, f_ch, rhs_ch, coeff_ch, level_iters, coarsest_iters;
+    double omega;
+    float Rr, P;
+} cs_args;
+/* AMGSolver::muCycleStep (AMGSolver.cu:1130-1149) */
+static void mu_step_cs(og_grid* g, int l, const cs_args* A) {
+    if (l == 0) {
+        og_gauss_seidel(g, A->coarsest_iters / 2, 0, 0, A->x_ch, A->coeff_ch, A->rhs_ch, A->omega);
+        og_gauss_seidel(g, A->coarsest_iters / 2, 1, 0, A->x_ch, A->coeff_ch, A->rhs_ch, A->omega);
+        return;
+    }
+    og_gauss_seidel(g, A->level_iters, 0, l, A->x_ch, A->coeff_ch, A->rhs_ch, A->omega);
+    og_residual_restrict(g, l, A->x_ch, A->coeff_ch, A->rhs_ch, A->Rr);
+    deduct_flux(g, l - 1, A->x_ch, A->coeff_ch, A->f_ch, A->rhs_ch);
+    set_zero_nonleaf(g, l - 1, A->x_ch);
+    for (int r = 0; r < A->rep; r++) mu_step_cs(g, l - 1, A);
+    prolong_add(g, l, A->x_ch, A->P);
+    og_gauss_seidel(g, A->level_iters, 1, l, A->x_ch, A->coeff_ch, A->rhs_ch, A->omega);
+}
+/* AMGSolver::muCycle (AMGSolver.cu:1151-1174) */
+void og_mu_cycle(og_grid* g, int repeat_times, int x_ch, int f_ch, int rhs_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega,
+                 float R_restrict, float P) {
+    cs_args A = {repeat_times, x_ch, f_ch, rhs_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict, P};
+    cycle_init(g, x_ch, f_ch, rhs_ch);
+    mu_step_cs(g, g->max_level, &A);
+}
+/* AMGSolver::VCycle (AMGSolver.cu:1060-1128) */
+void og_vcycle(og_grid* g, int x_ch, int f_ch, int rhs_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega, float R_restrict,
+               float P) {
+    cycle_init(g, x_ch, f_ch, rhs_ch);
+    for (int l = g->max_level; l > 0; l--) {
+        og_gauss_seidel(g, level_iters, 0, l, x_ch, coeff_ch, rhs_ch, omega);
+        og_residual_restrict(g, l, x_ch, coeff_ch, rhs_ch, R_restrict);
+    }
+    og_gauss_seidel(g, coarsest_iters / 2, 0, 0, x_ch, coeff_ch, rhs_ch, omega);
+    og_gauss_seidel(g, coarsest_iters / 2, 1, 0, x_ch, coeff_ch, rhs_ch, omega);
+    for (int l = 1; l <= g->max_level; l++) {
+        prolong_add(g, l, x_ch, P);
+        og_gauss_seidel(g, level_iters, 1, l, x_ch, coeff_ch, rhs_ch, omega);
+    }
+}
+/* RestrictSourceToCoarse (AMGSolver.cu:1295-1307): AccumulateToParentsOneStepKernel
+ * (PoissonGrid.cu:408-453) on the LEAF and NONLEAF tiles of `level`, INTERIOR cells only,
+ * the parent cell set to R times the sum of its 8 children */
+static void restrict_source(og_grid* g, int level, int ch, float R) {
+    for (int t = 0; t < g->n; t++) {
+        if (!is_active_at(g, t, level)) continue;
+        int p = g->parent[t];
+        if (p < 0) continue;
+        for (int b = 0; b < 64; b++) {
+            int fl[3] = {(b >> 4) * 2, ((b >> 2) & 3) * 2, (b & 3) * 2};
+            float sum = 0;
+            for (int ii = 0; ii < 2; ii++)
+                for (int jj = 0; jj < 2; jj++)
+                    for (int kk = 0; kk < 2; kk++) {
+                        int v = CELL(fl[0] + ii, fl[1] + jj, fl[2] + kk);
+                        sum += (CT(g, t)[v] & OG_INTERIOR) ? CH(g, ch, t)[v] : 0.0f;
+                    }
+            CH(g, ch, p)[parent_cell(g, t, CELL(fl[0], fl[1], fl[2]))] = sum * R;
+        }
+    }
+}
+/* AMGSolver::FASFCycle (AMGSolver.cu:1358-1387) */
+void og_fas_f_cycle(og_grid* g, int mu, int x_ch, int rhs_ch, int x0_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega,
+                    float R_restrict, float P) {
+    memset(CH(g, x_ch, 0), 0, sizeof(float) * NC * g->n);
+    for (int l = g->max_level; l > 0; l--) restrict_source(g, l, rhs_ch, R_restrict);
+    og_gauss_seidel(g, coarsest_iters / 2, 0, 0, x_ch, coeff_ch, rhs_ch, omega);
+    og_gauss_seidel(g, coarsest_iters / 2, 1, 0, x_ch, coeff_ch, rhs_ch, omega);
+    mu_args A = {mu, x_ch, rhs_ch, x0_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict, P};
+    for (int l = 1; l <= g->max_level; l++) {
+        prolong_add(g, l, x_ch, P);
+        fas_step(g, l, &A);
+    }
+}
+
 /* Dot128Kernel + DeviceReduce (PoissonGrid.cu:156-214): all 512 cells of LEAF
  * tiles, products of each group of four cells summed in float, then double. */
 double og_dot(og_grid* g, int a_ch, int b_ch) {

@@ -74,6 +74,12 @@ void og_residual_restrict(og_grid* g, int level, int x_ch, int coeff_ch, int rhs
 void og_fas_save(og_grid* g, int level, int x_ch, int coeff_ch, int rhs_ch, int x0_ch);
 void og_fas_prolong(og_grid* g, int level, int x_ch, int x0_ch, float P);
 void og_fas_mu_cycle(og_grid* g, int mu, int x_ch, int rhs_ch, int x0_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega, float R_restrict, float P);
+/* AMGSolver::VCycle / muCycle (correction schemes for rhs f) and FASFCycle */
+void og_vcycle(og_grid* g, int x_ch, int f_ch, int rhs_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega, float R_restrict, float P);
+void og_mu_cycle(og_grid* g, int repeat_times, int x_ch, int f_ch, int rhs_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega,
+                 float R_restrict, float P);
+void og_fas_f_cycle(og_grid* g, int mu, int x_ch, int rhs_ch, int x0_ch, int coeff_ch, int level_iters, int coarsest_iters, double omega,
+                    float R_restrict, float P);
 double og_dot(og_grid* g, int a_ch, int b_ch);
 int og_amg_solve(og_grid* g, int coeff_ch, double omega, int mu, float R_restrict, float P, int max_iters, double tol, int level_iters, int coarsest_iters, int sync_stride, int pure_neumann, double* rel_res);
 

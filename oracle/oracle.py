@@ -59,6 +59,9 @@ def lib():
             "og_fas_save": (None, [P, I, I, I, I, I]),
             "og_fas_prolong": (None, [P, I, I, I, F]),
             "og_fas_mu_cycle": (None, [P, I, I, I, I, I, I, I, D, F, F]),
+            "og_vcycle": (None, [P, I, I, I, I, I, I, D, F, F]),
+            "og_mu_cycle": (None, [P, I, I, I, I, I, I, I, D, F, F]),
+            "og_fas_f_cycle": (None, [P, I, I, I, I, I, I, I, D, F, F]),
             "og_dot": (D, [P, I, I]),
             "og_amg_solve": (I, [P, I, D, I, F, F, I, D, I, I, I, I, P]),
             "og_face_velocity_fourier": (None, [P, I, I, P, P, P]),
@@ -190,6 +193,18 @@ class Grid:
 
     def fas_mu_cycle(self, mu, x_ch, rhs_ch, x0_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict=1.0, P=1.0):
         self.L.og_fas_mu_cycle(self.g, mu, x_ch, rhs_ch, x0_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict, P)
+
+    def vcycle(self, x_ch, f_ch, rhs_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict=1.0, P=1.0):
+        """AMGSolver::VCycle (src/AMGSolver.cu:1060)"""
+        self.L.og_vcycle(self.g, x_ch, f_ch, rhs_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict, P)
+
+    def mu_cycle(self, repeat_times, x_ch, f_ch, rhs_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict=1.0, P=1.0):
+        """AMGSolver::muCycle (src/AMGSolver.cu:1151)"""
+        self.L.og_mu_cycle(self.g, repeat_times, x_ch, f_ch, rhs_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict, P)
+
+    def fas_f_cycle(self, mu, x_ch, rhs_ch, x0_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict=1.0, P=1.0):
+        """AMGSolver::FASFCycle (src/AMGSolver.cu:1358)"""
+        self.L.og_fas_f_cycle(self.g, mu, x_ch, rhs_ch, x0_ch, coeff_ch, level_iters, coarsest_iters, omega, R_restrict, P)
 
     def dot(self, a, b):
         return self.L.og_dot(self.g, a, b)

@@ -82,6 +82,38 @@ def test_uniform_mu_cycle_matches_oracle():
     assert rel_l2(G.download(4)[m], g.channel(4)[m]) <= 1e-5
 
 
+@pytest.mark.parametrize("cycle", ["vcycle", "mu1", "mu2", "fcycle"])
+@pytest.mark.parametrize("shell", [False, True])
+def test_cycle_variants_match_oracle(cycle, shell):
+    """AMGSolver::VCycle, muCycle (repeat 1 and 2) and FASFCycle (src/AMGSolver.cu:1060-1174,
+    1358-1387), which nothing in the reference's solve calls: x and the working rhs on every
+    tile against the oracle.  The sphere octree has LEAF tiles next to NONLEAF tiles on a
+    coarser level (muCycleStep's flux deduction) and GHOST tiles."""
+    if shell:
+        G, g, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5))
+        f = G.download(1)
+    else:
+        G, g, solver, f = setup_uniform(3)
+    for ch, v in ((11, f), (1, f)):
+        G.upload(ch, v)
+        g.channel(ch)[:] = v
+    if cycle == "vcycle":
+        solver.VCycle(G, 0, 11, 1, 2, 10)
+        g.vcycle(0, 11, 1, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    elif cycle.startswith("mu"):
+        solver.muCycle(int(cycle[2]), G, 0, 11, 1, 2, 10)
+        g.mu_cycle(int(cycle[2]), 0, 11, 1, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    else:
+        solver.FASFCycle(G, 0, 1, 3, 2, 10)
+        g.fas_f_cycle(2, 0, 1, 3, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    x, xo = G.download(0), g.channel(0)
+    assert np.all(np.isfinite(x))
+    assert rel_l2(x, xo) <= 1e-6
+    assert rel_l2(G.download(1), g.channel(1)) <= 1e-6
+    if cycle != "fcycle":
+        assert np.array_equal(G.download(11), f)  # f is read only
+
+
 @pytest.mark.parametrize("mu", [2, 1])
 def test_uniform_solve_matches_oracle_and_fp64(mu):
     G, g, solver, b = setup_uniform(3)

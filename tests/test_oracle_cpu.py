@@ -448,3 +448,37 @@ def test_oracle_bf16_cycle_storage_converges_like_fp32():
     it1, rel1 = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
     assert rel1 <= 1e-6 and abs(it1 - it0) <= 1
     assert np.linalg.norm((g.channel(0) - x0).astype(np.float64)) <= 1e-5 * np.linalg.norm(x0.astype(np.float64))
+
+
+@pytest.mark.parametrize("cycle", ["vcycle", "mu1", "mu2", "fcycle"])
+@pytest.mark.parametrize("case", ["uniform3", "shell345"])
+def test_oracle_cycle_variants_reduce_the_residual(cycle, case):
+    """AMGSolver::VCycle, muCycle and FASFCycle (src/AMGSolver.cu:1060-1174, 1358-1387) as the
+    oracle restates them: one cycle from x = 0 leaves a residual well below |f| on the LEAF
+    tiles' INTERIOR cells, and f itself is left unchanged."""
+    from workloads import build_oracle, shell_params, uniform_rhs
+
+    if case == "uniform3":
+        g = build_oracle(O.CASE_UNIFORM, [3, 3])
+    else:
+        g = build_oracle(O.CASE_SHELL, shell_params(3, 4, 5))
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.coarsen_types_and_coeffs(COEFF, 0.5)
+    lv, ijk, ty = g.tiles()
+    f = uniform_rhs(ty == O.LEAF, 0)
+    g.channel(11)[:] = f
+    g.channel(1)[:] = f
+    if cycle == "vcycle":
+        g.vcycle(0, 11, 1, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    elif cycle.startswith("mu"):
+        g.mu_cycle(int(cycle[2]), 0, 11, 1, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    else:
+        g.fas_f_cycle(2, 0, 1, 3, COEFF, 2, 10, 1.5, 1.0, 1.0)
+    x = g.channel(0)
+    assert np.all(np.isfinite(x))
+    g.full_neg_lap_leafs(0, COEFF, 12)
+    m = (g.cell_types() == O.INTERIOR) & (ty == O.LEAF)[:, None]
+    r = f - g.channel(12)
+    assert np.linalg.norm(r[m]) < 0.2 * np.linalg.norm(f[m])
+    if cycle != "fcycle":
+        assert np.array_equal(g.channel(11), f)
