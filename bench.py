@@ -419,7 +419,44 @@ def training_rhs(cmg, G, spec, n):
 
 
 LEARNED_INFERENCE = ["mma.sync"]  # set from --learned-inference
-LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, loss="energy", iters=(1, 2, 3, 5), rhs=10, max_tiles=1250)
+LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, loss="energy", iters=(1, 2, 3, 5), rhs=10, max_tiles=1250,
+               octrees=3)
+
+
+def random_octree_specs(spec, k, seed=300):
+    """k octrees like `spec` with the sphere moved and resized at random (centre U(0.3, 0.7)^3,
+    radius U(0.07, 0.13), seeded): the training octrees of the learned smoother.  A uniform
+    workload has one octree, so it trains on its own (with other right-hand sides)."""
+    if spec["case"] != "shell":
+        return [spec]
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(k):
+        c = tuple(float(v) for v in rng.uniform(0.3, 0.7, 3))
+        r = float(rng.uniform(0.07, 0.13))
+        p = list(spec["params"])
+        p[3:7] = [c[0], c[1], c[2], r]
+        out.append(dict(case="shell", params=p, spheres=[c + (r,)], rhs=spec["rhs"]))
+    return out
+
+
+def collect_training_pairs(cmg, spec, S):
+    """Training pairs of the learned smoother: plain solves of right-hand sides of the
+    workload's kind (training seeds, never the timed rhs) on random octrees like the
+    workload's (random_octree_specs), LEARNED["rhs"] right-hand sides in all."""
+    import learned
+
+    specs = random_octree_specs(spec, LEARNED["octrees"])
+    per = max(1, LEARNED["rhs"] // len(specs))
+    parts = []
+    for i, sp in enumerate(specs):
+        G = build_grid(cmg, sp)
+        rhs = training_rhs(cmg, G, sp, per)
+        # channels 10-12 (the face velocity, spent once the rhs exist) hold z, the FAS x0 and A z
+        parts.append(learned.collect_pairs(G, S, COEFF, rhs, iters=LEARNED["iters"], max_tiles=LEARNED["max_tiles"], z_ch=U, x0_ch=U + 1,
+                                           az_ch=U + 2, seed=i))
+        del G
+    return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
 
 
 def learned_block(cmg, torch, spec, steps, world, dev):
@@ -429,13 +466,10 @@ def learned_block(cmg, torch, spec, steps, world, dev):
     true-residual judge included)."""
     import learned
 
-    G = build_grid(cmg, spec)
     S = make_solver(cmg)
     t0 = time.perf_counter()
-    rhs = training_rhs(cmg, G, spec, LEARNED["rhs"])
-    # channels 10-12 (the face velocity, spent once the rhs exist) hold z, the FAS x0 and A z
-    pairs = learned.collect_pairs(G, S, COEFF, rhs, iters=LEARNED["iters"], max_tiles=LEARNED["max_tiles"], z_ch=U, x0_ch=U + 1,
-                                  az_ch=U + 2)
+    pairs = collect_training_pairs(cmg, spec, S)
+    G = build_grid(cmg, spec)
     t1 = time.perf_counter()
     net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
                                 lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
@@ -516,8 +550,8 @@ def learned_on_tuned(cmg, torch, G, S2, best, spec, steps, world, dev):
 
 def run_sequence(args, rank, world, local_rank):
     """The moving-sphere sequence: --steps positions, each with its own octree, cut-cell
-    operator and rhs; at each position the plain and the learned solve (trained once on the
-    first position, on other right-hand sides) are timed on the device.  value = mean plain ms
+    operator and rhs; at each position the plain and the learned solve (trained once, on
+    random sphere octrees) are timed on the device.  value = mean plain ms
     per solve; the learned figures sit in config."""
     import torch
 
@@ -527,15 +561,14 @@ def run_sequence(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     spec0 = moving_sphere_spec(0)
-    G = build_grid(cmg, spec0)
     S = make_solver(cmg)
     t0 = time.perf_counter()
-    rhs = training_rhs(cmg, G, spec0, LEARNED["rhs"])
-    pairs = learned.collect_pairs(G, S, COEFF, rhs, iters=LEARNED["iters"], max_tiles=LEARNED["max_tiles"], z_ch=U, x0_ch=U + 1,
-                                  az_ch=U + 2)
+    pairs = collect_training_pairs(cmg, spec0, S)  # random sphere octrees, not the sequence's
     net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
                                 lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
     train_s = time.perf_counter() - t0
+    G = build_grid(cmg, spec0)
+    rhs = training_rhs(cmg, G, spec0, 1)
     # the autotuned smoother, tuned once at position 0 on a training rhs
     St = make_solver(cmg)
     G.upload(1, rhs[0])

@@ -50,7 +50,7 @@ EXPORTS = [
     "cmg_amg_last_solve_launches", "cmg_amg_solve_batch", "cmg_amg_solver_set_storage", "cmg_amg_divergence_without_coeff",
     "cmg_grid_gather_device_tiles", "cmg_grid_scatter_device_tiles",
     "cmg_learned_create", "cmg_learned_destroy", "cmg_learned_num_params", "cmg_learned_get_params",
-    "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient",
+    "cmg_learned_set_params", "cmg_learned_set_samples", "cmg_learned_forward", "cmg_learned_gradient", "cmg_learned_apply_grid",
     "cmg_learned_train", "cmg_learned_set_loss", "cmg_learned_set_inference", "cmg_amg_solver_set_learned",
     "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
     "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct", "cmg_amg_solver_set_cycle_bf16",
@@ -151,7 +151,8 @@ def lib():
             "cmg_learned_num_params": (I, [P, P]),
             "cmg_learned_get_params": (I, [P, P, I]),
             "cmg_learned_set_params": (I, [P, P, I]),
-            "cmg_learned_set_samples": (I, [P, I, P, P, P, P]),
+            "cmg_learned_set_samples": (I, [P, I, P, P, P, P, P, P]),
+            "cmg_learned_apply_grid": (I, [P, P, I, I, I, I, I, I]),
             "cmg_learned_forward": (I, [P, I, I, P]),
             "cmg_learned_gradient": (I, [P, I, I, P, P]),
             "cmg_learned_train": (I, [P, I, I, F, ctypes.c_ulonglong, P]),
@@ -712,15 +713,24 @@ class LearnedNet:
         p = np.ascontiguousarray(p, dtype=np.float32)
         _check(self.L.cmg_learned_set_params(self.h, _p(p), p.size), "set_params")
 
-    def set_samples(self, rho, diag, types, target=None):
-        """Tiles of 512 cells: rho, diag (float32), types (uint8), target (float32 or None)."""
+    def set_samples(self, rho, diag, types, target=None, faces=None, halo=None):
+        """Tiles of 512 cells: rho, diag (float32), types (uint8), target (float32 or None);
+        faces [n, 3, 512] (the -x/-y/-z face coefficients) and halo [n, 768] (the residual
+        across the six faces, then 1/0 flags), each optional."""
         rho = np.ascontiguousarray(rho, dtype=np.float32).reshape(-1, 512)
         diag = np.ascontiguousarray(diag, dtype=np.float32).reshape(-1, 512)
         types = np.ascontiguousarray(types, dtype=np.uint8).reshape(-1, 512)
+        n = rho.shape[0]
         tg = None if target is None else np.ascontiguousarray(target, dtype=np.float32).reshape(-1, 512)
-        _check(self.L.cmg_learned_set_samples(self.h, rho.shape[0], _p(rho), _p(diag), _p(types),
-                                              _p(tg) if tg is not None else None), "set_samples")
+        fc = None if faces is None else np.ascontiguousarray(faces, dtype=np.float32).reshape(n, 3, 512)
+        hl = None if halo is None else np.ascontiguousarray(halo, dtype=np.float32).reshape(n, 768)
+        _check(self.L.cmg_learned_set_samples(self.h, n, _p(rho), _p(diag), _p(types), _p(tg) if tg is not None else None,
+                                              _p(fc) if fc is not None else None, _p(hl) if hl is not None else None), "set_samples")
         self.num_samples = rho.shape[0]
+
+    def apply_grid(self, grid, level, r_ch, az_ch, coeff_ch, out_ch, overwrite=True):
+        """The net on the grid's LEAF tiles of `level` (cmg_learned_apply_grid)."""
+        _check(self.L.cmg_learned_apply_grid(self.h, grid.h, level, r_ch, az_ch, coeff_ch, out_ch, int(overwrite)), "apply_grid")
 
     def set_loss(self, kind):
         """"mse" (squared error, default) or "energy" (tile Laplacian-weighted)."""

@@ -512,15 +512,36 @@ int cmg_learned_set_params(cmg_learned* net, const float* host, int n) {
         if (!std::isfinite(host[i])) return fail(CMG_ERR_NONFINITE, "cmg_learned_set_params: non-finite parameter");
     return net->n.set_params(host);
 }
-int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target) {
+int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target,
+                            const float* faces, const float* halo) {
     GUARD_BEGIN
     if (!net || n < 0 || (n > 0 && (!rho || !diag || !types))) return fail(CMG_ERR_INVALID, "cmg_learned_set_samples: bad argument");
-    return net->n.set_samples(n, rho, diag, types, target);
+    return net->n.set_samples(n, rho, diag, types, target, faces, halo);
     GUARD_END
 }
 int cmg_learned_forward(cmg_learned* net, int first, int n, float* out) {
     if (!net || !out || first < 0 || n <= 0 || first + n > net->n.ns) return fail(CMG_ERR_INVALID, "cmg_learned_forward: bad sample range");
     return net->n.forward(first, n, out);
+}
+int cmg_learned_apply_grid(cmg_learned* net, cmg_grid* g, int level, int r_ch, int az_ch, int coeff_ch, int out_ch, int overwrite) {
+    GUARD_BEGIN
+    if (!net || !grid_ready(g)) return fail(CMG_ERR_STATE, "cmg_learned_apply_grid: net or grid not ready");
+    cmg::Grid& G = g->g;
+    if (level < 0 || level > G.max_level() || !chan_ok(g, r_ch) || (az_ch >= 0 && !chan_ok(g, az_ch)) || !chan_ok(g, out_ch) ||
+        coeff_ch < 0 || coeff_ch + 4 > G.nch || out_ch == r_ch || out_ch == az_ch)
+        return fail(CMG_ERR_INVALID, "cmg_learned_apply_grid: bad argument");
+    const int t0 = G.level_begin(level), nt = G.nonleaf_begin(level) - t0;
+    cmg::NetExtra ex;
+    ex.faces = G.plane(coeff_ch);
+    ex.fstride = (size_t)G.n * 512;
+    ex.ftile = 512;
+    ex.nbx = G.nbx;
+    cmg::launch_net_forward(net->n.H, G.plane(r_ch), az_ch >= 0 ? G.plane(az_ch) : nullptr, G.plane(coeff_ch + 3), G.ctype, nullptr, t0, nt,
+                            net->n.pack, net->n.bias, G.plane(out_ch), overwrite != 0, G.stream, ex);
+    CKC(cudaStreamSynchronize(G.stream));
+    if (cmg::net_take_tc_error() == 1) return fail(CMG_ERR_CUDA, "cmg_learned_apply_grid: a tensor-core MMA did not complete in time");
+    return cmg::check_cuda(cudaGetLastError(), "learned apply");
+    GUARD_END
 }
 int cmg_learned_gradient(cmg_learned* net, int first, int n, double* loss, float* grad) {
     GUARD_BEGIN

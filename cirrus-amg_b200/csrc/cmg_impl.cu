@@ -797,8 +797,14 @@ void Solver::enqueue_precond(Grid& G, const Key& k, cudaStream_t st) const {
         enqueue_mu_cycle(G, A, st);
         const int L = G.max_level(), t0 = G.level_begin(L), nf = G.nonleaf_begin(L) - t0;
         launch_leaf_apply(G.dev(), G.leaf + (G.nleaf - nf), nf, G.plane(4), aux, coeff_ch, false, scratch(), st);
+        // the net also sees each cell's face coefficients and the residual across the tile's faces
+        NetExtra ex;
+        ex.faces = G.plane(coeff_ch);
+        ex.fstride = (size_t)G.n * kCells;
+        ex.ftile = kCells;
+        ex.nbx = G.nbx;
         launch_net_forward(lnet.H, G.plane(1), aux, G.plane(coeff_ch + 3), G.ctype, nullptr, t0, nf, lnet.pack, lnet.bias, G.plane(4), false,
-                           st);
+                           st, ex);
     }
 }
 

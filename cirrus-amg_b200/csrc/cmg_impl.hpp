@@ -276,7 +276,12 @@ struct Net {
     int init(int hidden, unsigned long long seed);
     int set_params(const float* host);
     int get_params(float* host);
-    int set_samples(int n, const float* rho, const float* diag, const uint8_t* types, const float* target);
+    // faces: [n][3][512] -x/-y/-z face coefficients, halo: [n][768] (NetExtra's layout); either may be null
+    float* faces = nullptr;
+    float* halo = nullptr;
+    int set_samples(int n, const float* rho, const float* diag, const uint8_t* types, const float* target, const float* faces_h = nullptr,
+                    const float* halo_h = nullptr);
+    NetExtra extra(int first) const;
     int forward(int first, int n, float* out_host);
     int gradient(int first, int n, double* loss_out, float* grad_host);
     int train(int epochs, int batch, float lr, unsigned long long seed, float* epoch_loss);

@@ -61,12 +61,24 @@ void net_set_inference_kind(int kind);  // 0: mma.sync (default), 1: tcgen05
 int net_inference_kind();
 int net_take_tc_error();  // 1 if a tcgen05 inference launch timed out waiting for its MMAs (then cleared)
 void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaStream_t st);
+// Optional inputs of the net beyond rho, the cell types and the diagonal: the -x/-y/-z face
+// coefficients (face a of tile t at faces + a*fstride + t*ftile), and the residual's 1-cell
+// halo, either stored per sample (halo: [768] per sample, 6 faces x 64 values then 6 x 64
+// flags, face r*128 + side*64 + a*8 + b) or read on the grid from same-level LEAF neighbours
+// through the face-neighbour table (nbx, with rho = r - az there).
+struct NetExtra {
+    const float* faces = nullptr;
+    size_t fstride = 0, ftile = 0;
+    const float* halo = nullptr;
+    const int* nbx = nullptr;
+};
 // samples s < ns are tiles (idx ? idx[s] : t0 + s) of the planes; rho = r - az (az may be null);
 // out[t] += (S/D) f (or = with overwrite) on INTERIOR cells
 void launch_net_forward(int H, const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
-                        const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st);
+                        const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st, const NetExtra& ex = NetExtra{});
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
-                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st);
+                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st,
+                      const NetExtra& ex = NetExtra{});
 void launch_net_reduce_adam(const float* grad, int nb, int np, float scale, float* gout, float* p, float* m, float* v, float lr, int step,
                             bool update, cudaStream_t st);
 // flexible-CG beta (Polak-Ribiere): gamma = r.z, beta = -alpha (Ap.z) / gamma_old

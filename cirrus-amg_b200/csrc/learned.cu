@@ -6,9 +6,14 @@
 // the finest level, rho = r - A z, is fed tile by tile to a small network whose output is
 // added to z on INTERIOR cells:
 //     z_t += (S_t / D_t) * f(features_t)
-// features (8 input channels, zero padding at the tile border):
+// features (8 input channels on the 10^3 grid of the tile and its 1-cell border):
 //     0: rho / S_t   (S_t = root mean square of rho over the tile's INTERIOR cells)
 //     1: INTERIOR flag   2: DIRICHLET flag   3: diagonal of A / D_t (D_t = its maximum)
+//     4-6: the -x/-y/-z face coefficients of A / D_t (on cut cells they carry the face
+//          fractions of the cut-cell operator)   7: 0
+//     border: channel 0 the residual rho / S_t of the neighbour cell across each face and
+//     channel 1 a flag for it (INTERIOR cells of same-level LEAF neighbours), 0 elsewhere;
+//     the hidden layers are zero-padded
 // network: conv3x3x3 8->H, bias, ReLU; conv3x3x3 H->H, bias, ReLU; conv3x3x3 H->1
 // (H = 8 or 16).  The target of f is the error the cycle leaves, d = A^-1 rho, scaled
 // by D_t / S_t; the network is trained on (rho, d) pairs made by the plain solver.
@@ -275,7 +280,8 @@ __device__ __forceinline__ float block_max_f(float v, float* red) {
 }
 
 // Where one tile's inputs come from: sample s is tile (idx ? idx[s] : t0 + s) of planes of
-// 512 floats; rho = r - az (az may be null: r already holds rho).
+// 512 floats; rho = r - az (az may be null: r already holds rho).  ex: the face coefficients
+// and the residual's 1-cell halo (NetExtra), each optional.
 struct NetIn {
     const float* r;
     const float* az;
@@ -284,6 +290,7 @@ struct NetIn {
     const float* target;
     const int* idx;
     int t0;
+    NetExtra ex;
 };
 
 struct Staged {
@@ -326,6 +333,15 @@ __device__ __forceinline__ Staged stage_features(const NetIn& I, int s, __nv_bfl
     o.D = block_max_f(dm, red);
     o.S = (n > 0.0f && sum > 0.0f && o.D > 0.0f) ? sqrtf(sum / n) : 0.0f;
     if (o.S == 0.0f) return o;
+    // the -x, -y, -z face coefficients (cut cells: scaled by their face fractions)
+    float fc[3][4] = {};
+    if (I.ex.faces) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float4 f4 = ldcg4(I.ex.faces + (size_t)a * I.ex.fstride + (size_t)t * I.ex.ftile + 4 * threadIdx.x);
+            fc[a][0] = f4.x, fc[a][1] = f4.y, fc[a][2] = f4.z, fc[a][3] = f4.w;
+        }
+    }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         const int cell = 4 * threadIdx.x + u;
@@ -333,10 +349,52 @@ __device__ __forceinline__ Staged stage_features(const NetIn& I, int s, __nv_bfl
         __nv_bfloat162 f[4];
         f[0] = __floats2bfloat162_rn(o.rho[u] / o.S, o.in[u] ? 1.0f : 0.0f);
         f[1] = __floats2bfloat162_rn((tt[u] & dDirichlet) ? 1.0f : 0.0f, o.in[u] ? dd[u] / o.D : 0.0f);
-        f[2] = f[3] = __floats2bfloat162_rn(0.0f, 0.0f);
+        f[2] = __floats2bfloat162_rn(o.in[u] ? fc[0][u] / o.D : 0.0f, o.in[u] ? fc[1][u] / o.D : 0.0f);
+        f[3] = __floats2bfloat162_rn(o.in[u] ? fc[2][u] / o.D : 0.0f, 0.0f);
         *reinterpret_cast<uint4*>(x0 + v * 8) = *reinterpret_cast<const uint4*>(f);
     }
+    // the residual's 1-cell halo: thread q owns cell (fa, fb) of the face of axis r on side
+    // q >> 6 for r = 0, 1, 2 (channel 0: rho / S of the neighbour cell, channel 1: 1 when it
+    // is an INTERIOR cell of a LEAF neighbour tile, else both 0)
+    if (I.ex.halo || I.ex.nbx) {
+        const int q = threadIdx.x, side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
+        const int e = side ? 0 : 7, hx = side ? 8 : -1;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            float hv = 0.0f, ok = 0.0f;
+            if (I.ex.halo) {
+                const float* hs = I.ex.halo + (size_t)t * 768;
+                hv = __ldcg(hs + r * 128 + q);
+                ok = __ldcg(hs + 384 + r * 128 + q);
+            } else {
+                const int d = I.ex.nbx[8 * t + r + 3 * side];
+                if (d != 0 && (d & 7) == dLeaf) {
+                    const size_t on = (size_t)((d >> 3) - 1) * kCells +
+                                      (r == 0 ? cell_index(e, fa, fb) : r == 1 ? cell_index(fa, e, fb) : cell_index(fa, fb, e));
+                    if (I.types[on] & dInterior) {
+                        hv = __ldcg(I.r + on);
+                        if (I.az) hv = __fsub_rn(hv, __ldcg(I.az + on));
+                        ok = 1.0f;
+                    }
+                }
+            }
+            const int v = r == 0 ? pad_vox(hx, fa, fb) : r == 1 ? pad_vox(fa, hx, fb) : pad_vox(fa, fb, hx);
+            __nv_bfloat162 f[4];
+            f[0] = __floats2bfloat162_rn(ok != 0.0f ? hv / o.S : 0.0f, ok);
+            f[1] = f[2] = f[3] = __floats2bfloat162_rn(0.0f, 0.0f);
+            *reinterpret_cast<uint4*>(x0 + v * 8) = *reinterpret_cast<const uint4*>(f);
+        }
+    }
     return o;
+}
+// zero the face halo voxels of an 8-channel buffer (whose other use needs zero padding)
+__device__ __forceinline__ void clear_face_halo(__nv_bfloat16* x0) {
+    const int q = threadIdx.x, side = q >> 6, fa = (q >> 3) & 7, fb = q & 7, hx = side ? 8 : -1;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int v = r == 0 ? pad_vox(hx, fa, fb) : r == 1 ? pad_vox(fa, hx, fb) : pad_vox(fa, fb, hx);
+        *reinterpret_cast<uint4*>(x0 + v * 8) = make_uint4(0, 0, 0, 0);
+    }
 }
 
 template <int H>
@@ -632,6 +690,8 @@ __global__ void __launch_bounds__(kNetThreads) k_net_forward_tc(NetIn I, int ns,
         // layer 1: x0 (8 channels) -> a1
         ok = run_layer(std::integral_constant<int, 1>{}, std::integral_constant<int, H>{}, smem_u32(x0), smem_u32(wt + Tc::W1), Tc::S1);
         if (!ok) break;
+        // x0 doubles as group 0 of a2, whose halo must be zero for layer 3
+        if (I.ex.halo || I.ex.nbx) clear_face_halo(x0);
         tc_epilogue_hidden<H>(lane_base, warp, lane, bias, a1);
         // layer 2: a1 -> a2
         ok = run_layer(std::integral_constant<int, CG>{}, std::integral_constant<int, H>{}, smem_u32(a1), smem_u32(wt + Tc::W2), Tc::SH);
@@ -881,9 +941,9 @@ void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaSt
 }
 
 void launch_net_forward(int H, const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
-                        const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st) {
+                        const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st, const NetExtra& ex) {
     if (ns <= 0) return;
-    const NetIn I{r, az, diag, types, nullptr, idx, t0};
+    const NetIn I{r, az, diag, types, nullptr, idx, t0, ex};
     if (g_infer_kind == 1) {
         // resident blocks per SM from shared memory (1 KB reserved per block) and TMEM (512 columns)
         int dev = 0, smem_sm = 0;
@@ -923,9 +983,9 @@ int net_take_tc_error() {
 }
 
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
-                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st) {
+                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st, const NetExtra& ex) {
     if (nb <= 0) return;
-    const NetIn I{rho, nullptr, diag, types, target, idx, 0};
+    const NetIn I{rho, nullptr, diag, types, target, idx, 0, ex};
     const int sms = num_sms();
     const int blocks = nb < sms ? nb : sms;
     note_kernel_launch();

@@ -50,6 +50,8 @@ Net::~Net() {
     nfree(diag);
     nfree(types);
     nfree(target);
+    nfree(faces);
+    nfree(halo);
     nfree(grad);
     nfree(loss);
     nfree(gsum);
@@ -103,16 +105,26 @@ int Net::get_params(float* host) {
     return 0;
 }
 
-int Net::set_samples(int n, const float* hr, const float* hd, const uint8_t* ht, const float* htg) {
+int Net::set_samples(int n, const float* hr, const float* hd, const uint8_t* ht, const float* htg, const float* hfaces, const float* hhalo) {
     nfree(rho);
     nfree(diag);
     nfree(types);
     nfree(target);
     nfree(loss);
     nfree(idx);
+    nfree(faces);
+    nfree(halo);
     ns = 0;
     if (n <= 0) return 0;
     const size_t c = (size_t)n * kCells;
+    if (hfaces) {
+        NCK(cudaMalloc(&faces, sizeof(float) * 3 * c));
+        NCK(cudaMemcpyAsync(faces, hfaces, sizeof(float) * 3 * c, cudaMemcpyHostToDevice, st));
+    }
+    if (hhalo) {
+        NCK(cudaMalloc(&halo, sizeof(float) * 768 * (size_t)n));
+        NCK(cudaMemcpyAsync(halo, hhalo, sizeof(float) * 768 * (size_t)n, cudaMemcpyHostToDevice, st));
+    }
     NCK(cudaMalloc(&rho, sizeof(float) * c));
     NCK(cudaMalloc(&diag, sizeof(float) * c));
     NCK(cudaMalloc(&types, c));
@@ -138,11 +150,23 @@ int Net::ensure_batch(int nb) {
     return 0;
 }
 
+// the samples' optional inputs from sample `first` on: faces [sample][3][512], halo [sample][768]
+NetExtra Net::extra(int first) const {
+    NetExtra ex;
+    if (faces) {
+        ex.faces = faces + (size_t)first * 3 * kCells;
+        ex.fstride = kCells;
+        ex.ftile = 3 * kCells;
+    }
+    if (halo) ex.halo = halo + (size_t)first * 768;
+    return ex;
+}
+
 int Net::forward(int first, int n, float* out_host) {
     const size_t o = (size_t)first * kCells, c = (size_t)n * kCells;
     float* out = nullptr;
     NCK(cudaMalloc(&out, sizeof(float) * c));
-    launch_net_forward(H, rho + o, nullptr, diag + o, types + o, nullptr, 0, n, pack, bias, out, true, st);
+    launch_net_forward(H, rho + o, nullptr, diag + o, types + o, nullptr, 0, n, pack, bias, out, true, st, extra(first));
     int rc = check_cuda(cudaMemcpyAsync(out_host, out, sizeof(float) * c, cudaMemcpyDeviceToHost, st), "forward: read-back");
     if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "forward");
     cudaFree(out);
@@ -157,7 +181,7 @@ int Net::forward(int first, int n, float* out_host) {
 int Net::gradient(int first, int n, double* loss_out, float* grad_host) {
     if (int rc = ensure_batch(n)) return rc;
     const size_t o = (size_t)first * kCells;
-    launch_net_train(H, rho + o, diag + o, types + o, target + o, nullptr, n, pack, bias, grad, loss, loss_kind, st);
+    launch_net_train(H, rho + o, diag + o, types + o, target + o, nullptr, n, pack, bias, grad, loss, loss_kind, st, extra(first));
     const float scale = 1.0f / ((float)n * kCells);
     launch_net_reduce_adam(grad, n, np, scale, gsum, p, m, v, 0.0f, 0, false, st);
     std::vector<float> l(n);
@@ -190,7 +214,7 @@ int Net::train(int epochs, int batch, float lr, unsigned long long seed, float* 
         NCK(cudaMemcpyAsync(idx, perm.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
         for (int b0 = 0; b0 < ns; b0 += batch) {
             const int nb = ns - b0 < batch ? ns - b0 : batch;
-            launch_net_train(H, rho, diag, types, target, idx + b0, nb, pack, bias, grad, loss + b0, loss_kind, st);
+            launch_net_train(H, rho, diag, types, target, idx + b0, nb, pack, bias, grad, loss + b0, loss_kind, st, extra(0));
             launch_net_reduce_adam(grad, nb, np, 1.0f / ((float)nb * kCells), nullptr, p, m, v, lr, ++adam_step, true, st);
             launch_net_pack(H, p, pack, bias, st);
         }

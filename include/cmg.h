@@ -291,9 +291,20 @@ int cmg_learned_num_params(cmg_learned* net, int* n);
 /* fp32 parameters: W1[H][27][8], b1[H], W2[H][27][H], b2[H], W3[27][H]; tap = dx*9+dy*3+dz */
 int cmg_learned_get_params(cmg_learned* net, float* host, int n);
 int cmg_learned_set_params(cmg_learned* net, const float* host, int n); /* also resets Adam */
-int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target);
+/* training/evaluation tiles: rho, diag, types, target [n][512]; optional (NULL: absent, the
+ * inputs read 0): faces [n][3][512], the -x/-y/-z face coefficients of each cell; halo
+ * [n][768], the residual across the tile's six faces (value of face r, side s, cell (a, b) at
+ * r*128 + s*64 + a*8 + b, then the same layout of 1/0 flags for cells that exist and are
+ * INTERIOR).  In the solve the net reads both from the grid itself. */
+int cmg_learned_set_samples(cmg_learned* net, int n, const float* rho, const float* diag, const uint8_t* types, const float* target,
+                            const float* faces, const float* halo);
 /* correction (S/D) f on INTERIOR cells (0 elsewhere) of samples first..first+n-1 */
 int cmg_learned_forward(cmg_learned* net, int first, int n, float* out);
+/* The net on the grid itself, as the learned solve applies it: on the LEAF tiles of `level`,
+ * rho = channel r_ch - channel az_ch (az_ch < 0: r_ch holds rho), the face coefficients from
+ * coeff_ch..coeff_ch+2 and the diagonal from coeff_ch+3, the halo from same-level LEAF
+ * neighbours; out_ch += the correction (= with overwrite) on INTERIOR cells. */
+int cmg_learned_apply_grid(cmg_learned* net, cmg_grid* g, int level, int r_ch, int az_ch, int coeff_ch, int out_ch, int overwrite);
 /* inference kernel of every net in the process: 0 (default) mma.sync, 1 tcgen05.mma with
  * TMEM accumulators; both compute the same network (FP32 accumulation, BF16 operands).  With
  * 8 output channels the tcgen05 MMAs are M = 64, N = 8 and measured slower than mma.sync. */

@@ -4,9 +4,12 @@ Imported by tests/ -- never by the product.  The reference has no learned precon
 this module restates the network that cirrus-amg_b200/csrc/learned.cu runs on BF16 tensor
 cores, so that its forward pass, loss and gradients can be checked:
 
-  features per 8^3 tile (channels-last, zero padding outside the tile):
+  features per 8^3 tile (channels-last) with a 1-cell border:
       0: rho / S (S = RMS of rho over INTERIOR cells)   1: INTERIOR   2: DIRICHLET
-      3: diag / D on INTERIOR cells (D = max |diag| over INTERIOR cells)   4-7: 0
+      3: diag / D on INTERIOR cells (D = max |diag| over INTERIOR cells)
+      4-6: the -x/-y/-z face coefficients / D on INTERIOR cells (0 without face data)   7: 0
+      border: channel 0 the neighbour's rho / S and channel 1 its flag across each face (the
+      sample's halo), 0 without halo data; the hidden layers are zero-padded
   a1 = relu(conv(x, W1) + b1); a2 = relu(conv(a1, W2) + b2); f = conv(a2, W3)
   correction = (S / D) f on INTERIOR cells
   loss = sum over tiles and INTERIOR cells of (f - target D / S)^2 / (n 512), or with the
@@ -50,11 +53,20 @@ def _taps():
     return [(t // 9, (t // 3) % 3, t % 3) for t in range(27)]
 
 
-def conv(x, W):
-    """x [n, 8, 8, 8, Cin], W [Cout, 27, Cin] -> [n, 8, 8, 8, Cout]; out[v] = sum_t x[v + off(t)] W[:, t]."""
-    n = x.shape[0]
-    xp = np.zeros((n, 10, 10, 10, x.shape[4]))
+def _padded(x):
+    """x [n, 8, 8, 8, C] zero-padded to [n, 10, 10, 10, C]; an x already [n, 10, ...] as is."""
+    if x.shape[1] == 10:
+        return x
+    xp = np.zeros((x.shape[0], 10, 10, 10, x.shape[4]))
     xp[:, 1:9, 1:9, 1:9] = x
+    return xp
+
+
+def conv(x, W):
+    """x [n, 8, 8, 8, Cin] (or padded [n, 10, 10, 10, Cin]), W [Cout, 27, Cin] -> [n, 8, 8, 8, Cout];
+    out[v] = sum_t x[v + off(t)] W[:, t]."""
+    n = x.shape[0]
+    xp = _padded(x)
     out = np.zeros((n, 8, 8, 8, W.shape[0]))
     for t, (dx, dy, dz) in enumerate(_taps()):
         out += np.einsum("sijkc,nc->sijkn", xp[:, dx:dx + 8, dy:dy + 8, dz:dz + 8], W[:, t, :])
@@ -74,19 +86,33 @@ def conv_input_grad(d, W):
 
 def conv_weight_grad(x, d):
     """Gradient of conv's weights: gW[n, t, c] = sum_v x[v + off(t), c] d[v, n]."""
-    xp = np.zeros((x.shape[0], 10, 10, 10, x.shape[4]))
-    xp[:, 1:9, 1:9, 1:9] = x
+    xp = _padded(x)
     g = np.zeros((d.shape[4], 27, x.shape[4]))
     for t, (dx, dy, dz) in enumerate(_taps()):
         g[:, t, :] = np.einsum("sijkc,sijkn->nc", xp[:, dx:dx + 8, dy:dy + 8, dz:dz + 8], d)
     return g
 
 
-def features(rho, diag, types, emulate_bf16=True):
-    """Per-tile features; rho, diag [n, 512] float32, types [n, 512] uint8 (cell i*64 + j*8 + k)."""
+def halo_positions():
+    """Padded-grid index (i, j, k) of halo entry r*128 + side*64 + a*8 + b: the cell (a, b) of
+    the face of axis r on side `side` (0: -, 1: +)."""
+    pos = np.zeros((384, 3), np.int64)
+    for r in range(3):
+        for side in range(2):
+            for a in range(8):
+                for b in range(8):
+                    e = 9 if side else 0
+                    pos[r * 128 + side * 64 + a * 8 + b] = [(e, a + 1, b + 1), (a + 1, e, b + 1), (a + 1, b + 1, e)][r]
+    return pos
+
+
+def features(rho, diag, types, emulate_bf16=True, faces=None, halo=None):
+    """Per-tile features as a padded [n, 10, 10, 10, 8] volume; rho, diag [n, 512] float32,
+    types [n, 512] uint8 (cell i*64 + j*8 + k); faces [n, 3, 512], halo [n, 768] (optional)."""
     rho = np.asarray(rho, dtype=np.float32).reshape(-1, 512)
     diag = np.asarray(diag, dtype=np.float32).reshape(-1, 512)
     types = np.asarray(types, dtype=np.uint8).reshape(-1, 512)
+    n = rho.shape[0]
     inter = (types & INTERIOR) != 0
     r = np.where(inter, rho, 0.0).astype(np.float64)
     cnt = inter.sum(1)
@@ -94,21 +120,33 @@ def features(rho, diag, types, emulate_bf16=True):
     ss = (r * r).sum(1)
     ok = (cnt > 0) & (ss > 0) & (D > 0)
     S = np.where(ok, np.sqrt(ss / np.maximum(cnt, 1)), 0.0)
-    x = np.zeros((rho.shape[0], 512, 8))
+    x = np.zeros((n, 512, 8))
     Ssafe = np.where(ok, S, 1.0)[:, None]
     Dsafe = np.where(ok, D, 1.0)[:, None]
     x[:, :, 0] = r / Ssafe
     x[:, :, 1] = inter
     x[:, :, 2] = (types & DIRICHLET) != 0
     x[:, :, 3] = np.where(inter, diag / Dsafe, 0.0)
+    if faces is not None:
+        fc = np.asarray(faces, dtype=np.float32).reshape(n, 3, 512).astype(np.float64)
+        for a in range(3):
+            x[:, :, 4 + a] = np.where(inter, fc[:, a] / Dsafe, 0.0)
+    xp = np.zeros((n, 10, 10, 10, 8))
+    xp[:, 1:9, 1:9, 1:9] = x.reshape(n, 8, 8, 8, 8)
+    if halo is not None:
+        hl = np.asarray(halo, dtype=np.float32).reshape(n, 768).astype(np.float64)
+        pos = halo_positions()
+        val, flag = hl[:, :384], hl[:, 384:]
+        xp[:, pos[:, 0], pos[:, 1], pos[:, 2], 0] = np.where(flag != 0, val / Ssafe, 0.0)
+        xp[:, pos[:, 0], pos[:, 1], pos[:, 2], 1] = flag
     if emulate_bf16:
-        x = bf16(x)
-    return x.reshape(-1, 8, 8, 8, 8), S, D, inter, ok
+        xp = bf16(xp)
+    return xp, S, D, inter, ok
 
 
-def forward(p, H, rho, diag, types, emulate_bf16=True):
+def forward(p, H, rho, diag, types, emulate_bf16=True, faces=None, halo=None):
     """Correction (S/D) f on INTERIOR cells, [n, 512]."""
-    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16)
+    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16, faces, halo)
     f, _ = _forward_net(p, H, x, emulate_bf16)
     sc = np.where(ok, S / np.where(ok, D, 1.0), 0.0)[:, None]
     return np.where(inter & ok[:, None], sc * f.reshape(-1, 512), 0.0)
@@ -134,10 +172,10 @@ def tile_laplacian(e):
     return (6.0 * g - nb).reshape(-1, 512)
 
 
-def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True, kind=0):
+def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True, kind=0, faces=None, halo=None):
     """Mean loss and its gradient (layout of `layout(H)`); kind 0: sum e^2 per tile,
     kind 1: e^T L e with L = tile_laplacian."""
-    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16)
+    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16, faces, halo)
     n = x.shape[0]
     f, (x, a1, a2, W1, W2, W3) = _forward_net(p, H, x, emulate_bf16)
     r = bf16 if emulate_bf16 else (lambda a: a)

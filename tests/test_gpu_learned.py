@@ -82,6 +82,97 @@ def test_gradient_matches_oracle(H, kind):
     assert np.all(gw1[:, :, 4:] == 0)
 
 
+def random_extra(n, seed):
+    """Face coefficients (negative, cut faces smaller) and a residual halo with about a third of
+    its cells absent (flag 0, value 0)."""
+    rng = np.random.default_rng(seed)
+    faces = (-rng.uniform(0.05, 1.0, (n, 3, 512)) / 64.0).astype(np.float32)
+    val = (rng.standard_normal((n, 384)) * 10.0 ** rng.uniform(-3, 3, (n, 1))).astype(np.float32)
+    flag = (rng.uniform(size=(n, 384)) > 0.33).astype(np.float32)
+    return faces, np.concatenate([val * flag, flag], axis=1)
+
+
+@pytest.mark.parametrize("H,kind", [(8, "tcgen05"), (16, "tcgen05"), (8, "mma.sync"), (16, "mma.sync")])
+def test_forward_with_faces_and_halo_matches_oracle(H, kind):
+    """The net's face-coefficient channels and the residual's 1-cell halo, both kernels."""
+    rho, diag, types, target = random_samples(12, 50 + H)
+    faces, halo = random_extra(12, 60 + H)
+    net = cmg.LearnedNet(H, seed=1)
+    p = random_params(H, 70 + H)
+    net.set_params(p)
+    net.set_samples(rho, diag, types, target, faces, halo)
+    cmg.set_learned_inference(kind)
+    try:
+        out = net.forward()
+    finally:
+        cmg.set_learned_inference("mma.sync")
+    ref = LO.forward(p, H, rho, diag, types, faces=faces, halo=halo)
+    plain = LO.forward(p, H, rho, diag, types)
+    assert np.all(out[(types & cmg.INTERIOR) == 0] == 0)
+    moved = 0
+    for s in range(out.shape[0]):
+        m = np.abs(ref[s]).max()
+        if m == 0:
+            continue
+        assert np.abs(out[s] - ref[s]).max() <= 1e-2 * m, s
+        moved += np.abs(ref[s] - plain[s]).max() > 0.05 * m  # the extra inputs change the output
+    assert moved >= 6
+
+
+@pytest.mark.parametrize("H", [8, 16])
+def test_gradient_with_faces_and_halo_matches_oracle(H):
+    rho, diag, types, target = random_samples(10, 80 + H)
+    faces, halo = random_extra(10, 90 + H)
+    net = cmg.LearnedNet(H, seed=2)
+    p = random_params(H, 100 + H)
+    net.set_params(p)
+    net.set_loss("energy")
+    net.set_samples(rho, diag, types, target, faces, halo)
+    loss, g = net.gradient()
+    rl, rg = LO.loss_and_grad(p, H, rho, diag, types, target, kind=1, faces=faces, halo=halo)
+    assert abs(loss - rl) <= 1e-3 * rl
+    L = LO.layout(H)
+    for a, b in [("W1", "B1"), ("B1", "W2"), ("W2", "B2"), ("B2", "W3"), ("W3", "n")]:
+        gs, rs = g[L[a]:L[b]], rg[L[a]:L[b]]
+        assert np.linalg.norm(gs - rs) <= 2e-2 * np.linalg.norm(rs) + 1e-12, a
+    # the face channels 4..6 now carry gradient; channel 7 stays unused
+    gw1 = g[L["W1"]:L["B1"]].reshape(H, 27, 8)
+    assert np.any(gw1[:, :, 4:7] != 0) and np.all(gw1[:, :, 7] == 0)
+
+
+@pytest.mark.parametrize("kind", ["mma.sync", "tcgen05"])
+def test_net_on_the_grid_equals_net_on_samples(kind):
+    """The learned solve's inputs read on the grid (face coefficients, the residual across faces
+    from same-level LEAF neighbours) equal the training samples' (learned.collect_pairs), bit
+    for bit: the same kernel on the same values."""
+    from workloads import setup_shell, shell_params
+
+    G, _, S = setup_shell(shell_params(coarse=3, mid=4, fine=5), with_oracle=False)
+    lv, ijk, ty = G.tiles()
+    L = int(lv.max())
+    nb, _ = G.tables()
+    types = G.download_cell_types()
+    rng = np.random.default_rng(3)
+    leaf = ty == cmg.LEAF
+    inter = (types & cmg.INTERIOR) != 0
+    r = np.where(inter & leaf[:, None], rng.standard_normal((G.num_tiles, 512)), 0.0).astype(np.float32)
+    G.upload(1, r)
+    net = cmg.LearnedNet(16, seed=5)
+    net.set_params(random_params(16, 6))
+    cmg.set_learned_inference(kind)
+    try:
+        net.apply_grid(G, L, 1, -1, COEFF, 4, overwrite=True)
+        sel = learned.finest_leaf_tiles(G)
+        faces = np.stack([G.download(COEFF + a) for a in range(3)], axis=1)[sel]
+        halo = learned.tile_halo(r, types, ty, nb, sel)
+        assert halo[:, 384:].sum() > 0  # the octree has LEAF neighbours across tile faces
+        net.set_samples(r[sel], G.download(COEFF + 3)[sel], types[sel], None, faces, halo)
+        out = net.forward()
+    finally:
+        cmg.set_learned_inference("mma.sync")
+    assert np.array_equal(G.download(4)[sel], out)
+
+
 def test_inference_kernels_agree():
     """tcgen05 and mma.sync inference on 300 tiles: the same products, summed in different orders."""
     rho, diag, types, target = random_samples(300, 77)
