@@ -460,10 +460,10 @@ def collect_training_pairs(cmg, spec, S):
 
 
 def learned_block(cmg, torch, spec, steps, world, dev):
-    """The learned finest-level smoother on one workload: pairs from plain solves of other
-    right-hand sides of the same octree, trained on the GPU, then the timed rhs solved plain
-    and learned, each timed over `steps` solves with CUDA events (the learned solve's
-    true-residual judge included)."""
+    """The learned finest-level smoother on one workload: pairs from plain solves on random
+    octrees like the workload's (collect_training_pairs), trained on the GPU, then the timed
+    rhs solved plain and learned, each timed over `steps` solves with CUDA events (the
+    learned solve's true-residual judge included)."""
     import learned
 
     S = make_solver(cmg)
@@ -624,7 +624,7 @@ def run_sequence(args, rank, world, local_rank):
             "plain_pcg_iters": [min(plain_it), max(plain_it)], "octree_setup_s_per_step": round(setup_s / max(args.steps, 1), 3),
             "learned_preconditioner": {
                 "hidden": LEARNED["hidden"], "loss": LEARNED["loss"], "damping": LEARNED["damping"],
-                "inference_kernel": LEARNED_INFERENCE[0], "trained_on": "position 0, 10 other right-hand sides", "train_and_collect_s": round(train_s, 3),
+                "inference_kernel": LEARNED_INFERENCE[0], "trained_on": "3 random sphere octrees, 10 right-hand sides (none of the sequence's)", "train_and_collect_s": round(train_s, 3),
                 "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
                 "ms_mean": round(ml, 4), "learned_pcg_iters": [min(learned_it), max(learned_it)], "fell_back": fallbacks,
                 "rel_residual_true_max": float(max(true_rel)), "plain_ms_mean": round(mp, 4)},
