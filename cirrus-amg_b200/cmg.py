@@ -55,7 +55,7 @@ EXPORTS = [
     "cmg_amg_solver_autotune", "cmg_amg_solver_set_finest_iters", "cmg_amg_solver_learned_status",
     "cmg_amg_solver_set_residual_replacement", "cmg_amg_solver_residual_replacements", "cmg_amg_solver_set_coarsest_direct", "cmg_amg_solver_set_cycle_bf16",
     "cmg_batch_create", "cmg_batch_destroy", "cmg_batch_set_schedule", "cmg_batch_schedule", "cmg_batch_solve", "cmg_batch_autotune",
-    "cmg_amg_vcycle", "cmg_amg_mu_cycle", "cmg_amg_fas_f_cycle",
+    "cmg_amg_vcycle", "cmg_amg_mu_cycle", "cmg_amg_fas_f_cycle", "cmg_set_dependent_launch",
 ]
 
 TARGET_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int)
@@ -134,6 +134,7 @@ def lib():
             "cmg_amg_last_solve_launches": (I, [P, P]),
             "cmg_amg_solve_batch": (I, [P, P, I, P, P, I, D, I, I, I, I, P, P, P]),
             "cmg_amg_vcycle": (I, [P, P, I, I, I, I, I]),
+            "cmg_set_dependent_launch": (I, [I]),
             "cmg_amg_mu_cycle": (I, [P, P, I, I, I, I, I, I]),
             "cmg_amg_fas_f_cycle": (I, [P, P, I, I, I, I, I]),
             "cmg_batch_create": (I, [P, P, I, P]),
@@ -674,6 +675,12 @@ def default_tune_candidates():
             for ci in (2, 5, 10)]
     grid += [(om, 1, li, ci, fi) for om in (1.0, 1.2, 1.3) for li in (2, 3, 4) for ci in (5, 10) for fi in (1, 2) if fi < li]
     return grid
+
+
+def set_dependent_launch(on):
+    """Launch the pipelined smoothing passes as programmatic dependents of the kernel before
+    them (default on; same results either way).  Takes effect for graphs built afterwards."""
+    _check(lib().cmg_set_dependent_launch(int(bool(on))), "set_dependent_launch")
 
 
 def set_learned_inference(kind):

@@ -869,6 +869,10 @@ int cmg_amg_fas_f_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, in
     return cmg::check_cuda(cudaGetLastError(), "fas_f_cycle");
     GUARD_END
 }
+int cmg_set_dependent_launch(int on) {
+    cmg::gs_pipe_set_dependent_launch(on != 0);
+    return CMG_OK;
+}
 int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms) {
     if (!s || !ms) return fail(CMG_ERR_INVALID, "null argument");
     *ms = s->s.last_ms;

@@ -29,6 +29,7 @@
 
 #include <cstddef>
 #include <type_traits>
+#include <utility>
 
 #include "kernels.hpp"
 
@@ -203,18 +204,18 @@ __device__ __forceinline__ void load_desc(const DevGrid& g, int t, int side, int
     for (int r = 0; r < 3; ++r) d[r] = __ldg(g.nbx + 8 * t + r + 3 * side);
 }
 
-// start the copies of tile t into stage S (mbarrier mb takes the bulk part)
+// start the copies of tile t into stage S (mbarrier mb takes the bulk part), in two halves:
+// issue_static moves what no kernel of a solve writes (the operator planes, the cell types,
+// the neighbours' face coefficients), issue_dynamic x, rhs and the halo x
 template <typename CT, typename XT>
-__device__ __forceinline__ void issue(PipeStage<CT, XT>& S, unsigned mb, const DevGrid& g, int t, const XT* X, const XT* B,
-                                      const CT* C0, const CT* C1, const CT* C2, const CT* C3, const int d[3], int q, float h) {
+__device__ __forceinline__ void issue_static(PipeStage<CT, XT>& S, unsigned mb, const DevGrid& g, int t, const CT* C0, const CT* C1,
+                                             const CT* C2, const CT* C3, const int d[3], int q, float h) {
     const size_t tb = (size_t)t * kCells;
     if (q == 0) {
         constexpr unsigned kX = kCells * sizeof(XT), kC = kCells * sizeof(CT), kT = kCells;
         // the stage was last read through ordinary loads; order them before the async writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect(mb, 2 * kX + 4 * kC + kT);
-        bulk_g2s(S.x, X + tb, kX, mb);
-        bulk_g2s(S.b, B + tb, kX, mb);
         bulk_g2s(S.d, C3 + tb, kC, mb);
         bulk_g2s(S.c0, C0 + tb, kC, mb);
         bulk_g2s(S.c1, C1 + tb, kC, mb);
@@ -222,23 +223,40 @@ __device__ __forceinline__ void issue(PipeStage<CT, XT>& S, unsigned mb, const D
         bulk_g2s(S.ty, g.ctype + tb, kT, mb);
     }
     const int side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
-    const int e = side ? 0 : 7;  // the neighbour's cell next to the shared face
-    const int nl[3] = {cell_index(e, fa, fb), cell_index(fa, e, fb), cell_index(fa, fb, e)};
+    if (!side) return;
+    const int nl[3] = {cell_index(0, fa, fb), cell_index(fa, 0, fb), cell_index(fa, fb, 0)};
     unsigned* hc[3] = {&S.c0h[fa * 8 + fb], &S.c1h[fa * 8 + fb], &S.c2h[fa * 8 + fb]};
     const CT* Cr[3] = {C0, C1, C2};
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
+        if (d[r] != 0) Coef<CT>::cp_face(hc[r], Cr[r], (size_t)((d[r] >> 3) - 1) * kCells + nl[r]);
+        else *hc[r] = Coef<CT>::word(h);
+    }
+}
+template <typename CT, typename XT>
+__device__ __forceinline__ void issue_dynamic(PipeStage<CT, XT>& S, unsigned mb, int t, const XT* X, const XT* B, const int d[3], int q) {
+    const size_t tb = (size_t)t * kCells;
+    if (q == 0) {
+        constexpr unsigned kX = kCells * sizeof(XT);
+        bulk_g2s(S.x, X + tb, kX, mb);
+        bulk_g2s(S.b, B + tb, kX, mb);
+    }
+    const int side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
+    const int e = side ? 0 : 7;  // the neighbour's cell next to the shared face
+    const int nl[3] = {cell_index(e, fa, fb), cell_index(fa, e, fb), cell_index(fa, fb, e)};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
         unsigned* hxd = &S.hx[r * 128 + q];
-        if (d[r] != 0) {
-            const size_t o = (size_t)((d[r] >> 3) - 1) * kCells + nl[r];
-            XStore<XT>::cp_halo(hxd, X, o);
-            if (side) Coef<CT>::cp_face(hc[r], Cr[r], o);
-        } else {
-            *hxd = 0u;
-            if (side) *hc[r] = Coef<CT>::word(h);
-        }
+        if (d[r] != 0) XStore<XT>::cp_halo(hxd, X, (size_t)((d[r] >> 3) - 1) * kCells + nl[r]);
+        else *hxd = 0u;
     }
     cp_commit();
+}
+template <typename CT, typename XT>
+__device__ __forceinline__ void issue(PipeStage<CT, XT>& S, unsigned mb, const DevGrid& g, int t, const XT* X, const XT* B,
+                                      const CT* C0, const CT* C1, const CT* C2, const CT* C3, const int d[3], int q, float h) {
+    issue_static(S, mb, g, t, C0, C1, C2, C3, d, q, h);
+    issue_dynamic(S, mb, t, X, B, d, q);
 }
 
 // The masked snapshot of the staged tile in SX: own cells (x is 0 on cells that are not
@@ -458,7 +476,12 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, XT* X, const XT* 
     load_desc(g, tcur, side, dcur);
     int tnext = tcur + stride;
     if (tnext < tend) load_desc(g, tnext, side, dnext);
-    issue(sm.st[0], mb0, g, tcur, X, B, C0, C1, C2, C3, dcur, q, h);
+    // Launched as a programmatic dependent of the previous kernel, the block may start while
+    // that kernel still runs: the first tile's static planes go out now, x and rhs only once
+    // the previous kernel has finished (a no-op for an ordinary launch).
+    issue_static(sm.st[0], mb0, g, tcur, C0, C1, C2, C3, dcur, q, h);
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    issue_dynamic(sm.st[0], mb0, tcur, X, B, dcur, q);
     bool pending_other = false;  // bulk copies in flight into the other stage
     for (int k = 0;; ++k) {
         const int s = k & 1;
@@ -468,6 +491,9 @@ __global__ void __launch_bounds__(128, 6) k_gs_pipe(DevGrid g, XT* X, const XT* 
         const int tn2 = tnext + stride;
         int dn2[3] = {0, 0, 0};
         if (tn2 < tend) load_desc(g, tn2, side, dn2);
+        // on its last tile the block lets the next pass be scheduled (it reads nothing of this
+        // one before its own wait); a block that exits counts as triggered
+        if (tnext >= tend) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
         cp_wait_prev();
         // stage s is the (k >> 1)-th use of its mbarrier
         const bool ok = mbar_wait(mb0 + 8 * s, (unsigned)(k >> 1) & 1u);
@@ -504,6 +530,25 @@ __global__ void k_coeff16(const float* __restrict__ C, CT* __restrict__ out, siz
 }
 
 int g_pipe_blocks = 0;  // resident blocks of k_gs_pipe on the device
+int g_pipe_dependent = 1;  // launch the passes as programmatic dependents of the previous kernel
+
+// A pass launched as a programmatic dependent starts its blocks as soon as the previous
+// kernel's blocks have all started (or exited) and resources free up, instead of after that
+// kernel has drained: the launch latency and the first tile's static copies overlap its tail.
+template <typename... P, typename... A>
+void launch_pass_kernel(void (*kernel)(P...), int blocks, size_t smem, cudaStream_t st, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pipe_dependent ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 using bf16 = __nv_bfloat16;
 
@@ -520,13 +565,16 @@ template <typename CT, typename XT>
 void launch_pass(int blocks, cudaStream_t st, const DevGrid& g, XT* X, const XT* B, const PipeArgs& A) {
     const size_t sm = sizeof(PipeSmem<CT, XT>);
     if (A.exact == kRelaxRef)
-        k_gs_pipe<CT, 0, kRelaxRef, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
+        launch_pass_kernel(k_gs_pipe<CT, 0, kRelaxRef, XT>, blocks, sm, st, g, X, B, A);
     else
-        k_gs_pipe<CT, 0, kRelaxDouble, XT><<<blocks, 128, sm, st>>>(g, X, B, A);
+        launch_pass_kernel(k_gs_pipe<CT, 0, kRelaxDouble, XT>, blocks, sm, st, g, X, B, A);
 }
 int g_restrict_blocks = 0;  // resident blocks of the restriction pass
 
 }  // namespace
+
+void gs_pipe_set_dependent_launch(bool on) { g_pipe_dependent = on ? 1 : 0; }
+bool gs_pipe_dependent_launch() { return g_pipe_dependent != 0; }
 
 int gs_pipe_take_error() {
     int v = 0, z = 0;
@@ -615,11 +663,12 @@ void launch_restrict_pipe(const DevGrid& g, int t0, int nt, const void* X, const
     const int blocks = nt < g_restrict_blocks ? nt : g_restrict_blocks;
     note_kernel_launch();
     if (!x16) {
-        k_gs_pipe<float, 1><<<blocks, 128, sizeof(PipeSmemR<float>), st>>>(g, (float*)X, (const float*)B, A);
+        launch_pass_kernel(k_gs_pipe<float, 1>, blocks, sizeof(PipeSmemR<float>), st, g, (float*)X, (const float*)B, A);
     } else if (p16) {
-        k_gs_pipe<float, 1, kRelaxRef, bf16, bf16><<<blocks, 128, sizeof(PipeSmemR<bf16>), st>>>(g, (bf16*)X, (const bf16*)B, A);
+        launch_pass_kernel(k_gs_pipe<float, 1, kRelaxRef, bf16, bf16>, blocks, sizeof(PipeSmemR<bf16>), st, g, (bf16*)X, (const bf16*)B, A);
     } else {
-        k_gs_pipe<float, 1, kRelaxRef, bf16, float><<<blocks, 128, sizeof(PipeSmemR<bf16>), st>>>(g, (bf16*)X, (const bf16*)B, A);
+        launch_pass_kernel(k_gs_pipe<float, 1, kRelaxRef, bf16, float>, blocks, sizeof(PipeSmemR<bf16>), st, g, (bf16*)X, (const bf16*)B,
+                           A);
     }
 }
 
@@ -694,7 +743,7 @@ void launch_fas_pipe_x16(const DevGrid& g, int t0, int nt, const void* X, void* 
     A.x0p = X0;
     const int blocks = nt < g_restrict_blocks ? nt : g_restrict_blocks;
     note_kernel_launch();
-    k_gs_pipe<float, 2, kRelaxRef, bf16><<<blocks, 128, sizeof(PipeSmemR<bf16>), st>>>(g, (bf16*)X, (const bf16*)RHS, A);
+    launch_pass_kernel(k_gs_pipe<float, 2, kRelaxRef, bf16>, blocks, sizeof(PipeSmemR<bf16>), st, g, (bf16*)X, (const bf16*)RHS, A);
 }
 
 }  // namespace cmg

@@ -47,6 +47,9 @@ void launch_accumulate_cells(const DevGrid& g, int t0, int nt, int types, const 
 int gs_pipe_init();
 // 1 if a pipelined sweep gave up waiting for its bulk copies since the last call (then cleared)
 int gs_pipe_take_error();
+// launch the pipelined passes as programmatic dependents of the previous kernel (default on)
+void gs_pipe_set_dependent_launch(bool on);
+bool gs_pipe_dependent_launch();
 // Storage of the operator planes the pipelined smoother reads: the float channels, or a
 // BF16 / FP16 copy (coeff16: four planes of num_tiles*512 elements, made by launch_coeff16).
 constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;

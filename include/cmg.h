@@ -443,6 +443,12 @@ int cmg_amg_fas_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, i
 int cmg_amg_vcycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters);
 int cmg_amg_mu_cycle(cmg_amg_solver* s, cmg_grid* g, int repeat_times, int x_ch, int f_ch, int rhs_ch, int level_iters, int coarsest_iters);
 int cmg_amg_fas_f_cycle(cmg_amg_solver* s, cmg_grid* g, int x_ch, int rhs_ch, int x0_ch, int level_iters, int coarsest_iters);
+/* Process-wide: launch the pipelined smoothing and restriction passes as programmatic
+ * dependent launches of the kernel before them (1, the default), so that each pass's blocks
+ * start as the previous kernel drains and copy their first tile's operator planes meanwhile;
+ * 0: ordinary launches.  Results are the same bits either way.  Applies to solves whose CUDA
+ * graph is built afterwards. */
+int cmg_set_dependent_launch(int on);
 /* device time of the last cmg_amg_solve, milliseconds (CUDA events) */
 int cmg_amg_last_solve_ms(cmg_amg_solver* s, float* ms);
 /* number of this library's kernels the last cmg_amg_solve executed (counted

@@ -114,6 +114,27 @@ def test_cycle_variants_match_oracle(cycle, shell):
         assert np.array_equal(G.download(11), f)  # f is read only
 
 
+@pytest.mark.parametrize("graph", [True, False])
+def test_dependent_launch_gives_the_same_bits(graph):
+    """The pipelined passes launched as programmatic dependents (the default) or as ordinary
+    launches: the same iterations, residual and x, in graph and in stream launch mode."""
+    G, _, solver = setup_shell(shell_params(coarse=3, mid=4, fine=5), with_oracle=False)
+    b = G.download(1)
+    out = []
+    try:
+        for on in (True, False):
+            cmg.set_dependent_launch(on)
+            s = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+            s.set_launch_mode(use_graph=graph)
+            G.upload(1, b)
+            it, rel = s.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+            out.append((it, rel, G.download(0)))
+    finally:
+        cmg.set_dependent_launch(True)
+    assert out[0][:2] == out[1][:2]
+    assert np.array_equal(out[0][2], out[1][2])
+
+
 @pytest.mark.parametrize("mu", [2, 1])
 def test_uniform_solve_matches_oracle_and_fp64(mu):
     G, g, solver, b = setup_uniform(3)
