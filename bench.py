@@ -421,6 +421,11 @@ def training_rhs(cmg, G, spec, n):
 LEARNED_INFERENCE = ["mma.sync"]  # set from --learned-inference
 LEARNED = dict(hidden=8, epochs=30, batch=256, lr=2e-3, damping=0.5, loss="energy", iters=(1, 2, 3, 5), rhs=10, max_tiles=1250,
                octrees=3)
+# the network as the learned-preconditioner spec states it: conv 8->32, four residual blocks of
+# two 3x3x3 convs at 32 channels, conv 32->1, inference and training on tcgen05
+LEARNED_DEEP = dict(LEARNED, hidden=32, epochs=20, lr=1e-3, damping=0.25)
+NETWORKS = {8: "conv 8->8, conv 8->8, conv 8->1 (3x3x3, BF16 operands)",
+            32: "conv 8->32, 4 residual blocks of two 3x3x3 convs at 32 channels, conv 32->1 (BF16 operands)"}
 
 
 def random_octree_specs(spec, k, seed=300):
@@ -459,20 +464,22 @@ def collect_training_pairs(cmg, spec, S):
     return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
 
 
-def learned_block(cmg, torch, spec, steps, world, dev):
+def learned_block(cmg, torch, spec, steps, world, dev, cfg=LEARNED, pairs=None):
     """The learned finest-level smoother on one workload: pairs from plain solves on random
-    octrees like the workload's (collect_training_pairs), trained on the GPU, then the timed
-    rhs solved plain and learned, each timed over `steps` solves with CUDA events (the
-    learned solve's true-residual judge included)."""
+    octrees like the workload's (collect_training_pairs, or the given pairs), trained on the
+    GPU with the settings cfg, then the timed rhs solved plain and learned, each timed over
+    `steps` solves with CUDA events (the learned solve's true-residual judge included).
+    Returns the result and the pairs."""
     import learned
 
     S = make_solver(cmg)
     t0 = time.perf_counter()
-    pairs = collect_training_pairs(cmg, spec, S)
+    if pairs is None:
+        pairs = collect_training_pairs(cmg, spec, S)
     G = build_grid(cmg, spec)
     t1 = time.perf_counter()
-    net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
-                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
+    net, losses = learned.train(pairs, hidden=cfg["hidden"], epochs=cfg["epochs"], batch=cfg["batch"], lr=cfg["lr"], seed=0,
+                                damping=cfg["damping"], loss=cfg["loss"])
     torch.cuda.synchronize()
     t2 = time.perf_counter()
 
@@ -497,14 +504,15 @@ def learned_block(cmg, torch, spec, steps, world, dev):
     S.set_learned(None)
     _, _, ty = G.tiles()
     lm = ty == cmg.LEAF
-    return {"hidden": LEARNED["hidden"], "loss": LEARNED["loss"], "inference_kernel": LEARNED_INFERENCE[0],
-            "damping": LEARNED["damping"], "train_pairs": int(pairs["rho"].shape[0]), "collect_s": round(t1 - t0, 3),
-            "train_s": round(t2 - t1, 3), "epochs": LEARNED["epochs"], "loss_first_epoch": float(losses[0]),
+    return {"hidden": cfg["hidden"], "network": NETWORKS[cfg["hidden"]], "loss": cfg["loss"],
+            "kernels": "tcgen05 inference and training" if cfg["hidden"] == 32 else LEARNED_INFERENCE[0] + " inference, mma.sync training",
+            "damping": cfg["damping"], "train_pairs": int(pairs["rho"].shape[0]), "collect_s": round(t1 - t0, 3),
+            "train_s": round(t2 - t1, 3), "epochs": cfg["epochs"], "loss_first_epoch": float(losses[0]),
             "loss_last_epoch": float(losses[-1]), "plain_ms": round(plain_ms, 4), "plain_pcg_iters": plain_it,
             "learned_ms": round(ms, 4), "pcg_iters": it, "learned_pcg_iters": learned_it, "fell_back": fell_back,
             "rel_residual_true": true_rel,
             "rel_l2_vs_plain_solution": float(np.linalg.norm((xl - xp)[lm].astype(np.float64)) /
-                                              np.linalg.norm(xp[lm].astype(np.float64)))}
+                                              np.linalg.norm(xp[lm].astype(np.float64)))}, pairs
 
 
 def learned_on_tuned(cmg, torch, G, S2, best, spec, steps, world, dev):
@@ -731,8 +739,11 @@ def run_ours(args, rank, world, local_rank):
     learned_res = []
     if not args.no_learned:
         for name in dict.fromkeys(["uniform64", args.workload]):
-            learned_res.append(dict(learned_block(cmg, torch, dict(instance_specs(name)[0], name=name), args.steps, world, dev),
-                                    workload=WORKLOADS[name]))
+            spec_n = dict(instance_specs(name)[0], name=name)
+            res, pairs = learned_block(cmg, torch, spec_n, args.steps, world, dev)
+            learned_res.append(dict(res, workload=WORKLOADS[name]))
+            res, _ = learned_block(cmg, torch, spec_n, args.steps, world, dev, cfg=LEARNED_DEEP, pairs=pairs)
+            learned_res.append(dict(res, workload=WORKLOADS[name]))
 
     # true residual of the last solution, FP32 operator apply on the device
     x = G.download(0)

@@ -482,7 +482,8 @@ int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage) {
 }
 int cmg_learned_create(int hidden, unsigned long long seed, cmg_learned** out) {
     GUARD_BEGIN
-    if (!out || (hidden != 8 && hidden != 16)) return fail(CMG_ERR_INVALID, "cmg_learned_create: hidden must be 8 or 16");
+    if (!out || (hidden != 8 && hidden != 16 && hidden != 32))
+        return fail(CMG_ERR_INVALID, "cmg_learned_create: hidden must be 8, 16 or 32");
     *out = nullptr;
     auto* n = new cmg_learned();
     if (int rc = n->n.init(hidden, seed)) {

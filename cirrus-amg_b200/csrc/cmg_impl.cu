@@ -412,14 +412,14 @@ int Solver::set_learned(const Net* net) {
         dfree(lnet.bias);
         lnet.H = 0;
         CK(cudaMalloc(&lnet.pack, sizeof(uint16_t) * (size_t)net_pack_elems(net->H)));
-        CK(cudaMalloc(&lnet.bias, sizeof(float) * 2 * net->H));
+        CK(cudaMalloc(&lnet.bias, sizeof(float) * net_bias_elems(net->H)));
         lnet.H = net->H;
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
         graphs.clear();
     }
     CK(cudaStreamSynchronize(net->st));
     CK(cudaMemcpy(lnet.pack, net->pack, sizeof(uint16_t) * (size_t)net_pack_elems(net->H), cudaMemcpyDeviceToDevice));
-    CK(cudaMemcpy(lnet.bias, net->bias, sizeof(float) * 2 * net->H, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(lnet.bias, net->bias, sizeof(float) * net_bias_elems(net->H), cudaMemcpyDeviceToDevice));
     lnet.enabled = true;
     return 0;
 }

@@ -266,11 +266,12 @@ struct Net {
     float* diag = nullptr;
     uint8_t* types = nullptr;
     float* target = nullptr;
-    float* grad = nullptr;  // per batch slot
+    float* grad = nullptr;  // per batch slot (the residual net: per training block)
     float* loss = nullptr;  // per sample
     float* gsum = nullptr;
     int* idx = nullptr;
     int batch_cap = 0;
+    void* scratch = nullptr;  // the residual net's per-block training scratch
     cudaStream_t st = nullptr;
     ~Net();
     int init(int hidden, unsigned long long seed);

@@ -56,13 +56,17 @@ constexpr int kStorageFP32 = 0, kStorageBF16 = 1, kStorageFP16 = 2;
 void launch_gs_pipe(const DevGrid& g, int t0, int nt, void* X, const void* B, bool x16, int coeff_ch, int color, double omega,
                     cudaStream_t st, int storage, const void* coeff16);
 size_t coeff16_bytes(const DevGrid& g);
-// learned finest-level smoother: per-tile conv net, hidden width H = 8 or 16 (learned.cu)
+// learned finest-level smoother: per-tile conv net, hidden width H = 8 or 16 (learned.cu), or
+// H = 32, the residual net of four blocks of two 32-channel convs (learned_deep.cu)
 int net_params(int H);      // fp32 parameters
 int net_pack_elems(int H);  // bf16 elements of the packed operands
+int net_bias_elems(int H);  // fp32 elements of the bias vector the kernels read
+size_t net_train_scratch_bytes(int H, int nb);  // device scratch a training launch of nb samples needs
+int net_train_rows(int H, int nb);              // gradient rows it writes (summed by launch_net_reduce_adam)
 bool net_init();
 void net_set_inference_kind(int kind);  // 0: mma.sync (default), 1: tcgen05
 int net_inference_kind();
-int net_take_tc_error();  // 1 if a tcgen05 inference launch timed out waiting for its MMAs (then cleared)
+int net_take_tc_error();  // 1 if a tcgen05 launch (any inference, the residual net's training) timed out waiting (then cleared)
 void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaStream_t st);
 // Optional inputs of the net beyond rho, the cell types and the diagonal: the -x/-y/-z face
 // coefficients (face a of tile t at faces + a*fstride + t*ftile), and the residual's 1-cell
@@ -81,7 +85,21 @@ void launch_net_forward(int H, const float* r, const float* az, const float* dia
                         const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st, const NetExtra& ex = NetExtra{});
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
                       const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st,
-                      const NetExtra& ex = NetExtra{});
+                      const NetExtra& ex = NetExtra{}, void* scratch = nullptr);
+// the residual net (learned_deep.cu), dispatched to by the net_* / launch_net_* functions for H = 32
+int deep_params();
+int deep_pack_elems();
+int deep_bias_elems();
+size_t deep_scratch_bytes();
+int deep_train_blocks(int nb);
+bool deep_init();
+int deep_take_error();
+void launch_deep_pack(const float* params, void* pack, float* bias, cudaStream_t st);
+void launch_deep_forward(const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
+                         const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st, const NetExtra& ex);
+void launch_deep_train(const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
+                       const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st, const NetExtra& ex,
+                       void* scratch);
 void launch_net_reduce_adam(const float* grad, int nb, int np, float scale, float* gout, float* p, float* m, float* v, float lr, int step,
                             bool update, cudaStream_t st);
 // flexible-CG beta (Polak-Ribiere): gamma = r.z, beta = -alpha (Ap.z) / gamma_old

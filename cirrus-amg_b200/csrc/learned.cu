@@ -35,18 +35,11 @@
 #include <cmath>
 #include <type_traits>
 
-#include "kernels.hpp"
+#include "net_common.cuh"
 
 namespace cmg {
 
 namespace {
-
-constexpr int kNetThreads = 128;
-constexpr int kPadVox = 1000;  // 10^3 padded voxels per tile
-
-// tap = dx*9 + dy*3 + dz (each 0..2), offset in the padded voxel grid
-__device__ __forceinline__ int tap_off(int tap) { return (tap / 9 - 1) * 100 + ((tap / 3) % 3 - 1) * 10 + (tap % 3 - 1); }
-__device__ __forceinline__ int pad_vox(int i, int j, int k) { return (i + 1) * 100 + (j + 1) * 10 + (k + 1); }
 
 // element offset of (voxel v, first channel of 8-channel group grp) in an activation buffer of CG groups
 template <int CG>
@@ -54,8 +47,6 @@ __device__ __forceinline__ int act_off(int v, int grp) {
     if constexpr (CG == 2) return v * 16 + ((grp ^ ((v >> 2) & 1)) << 3);
     else return v * 8;
 }
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void ldsm_x4(uint32_t a, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n" : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
@@ -259,144 +250,6 @@ __device__ __forceinline__ void bias_grad(const __nv_bfloat16* d, float* red, fl
     __syncthreads();
 }
 
-// fixed-order block reductions over 128 threads
-__device__ __forceinline__ float block_sum_f(float v, float* red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    const float r = (red[0] + red[1]) + (red[2] + red[3]);
-    __syncthreads();
-    return r;
-}
-__device__ __forceinline__ float block_max_f(float v, float* red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    const float r = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
-    __syncthreads();
-    return r;
-}
-
-// Where one tile's inputs come from: sample s is tile (idx ? idx[s] : t0 + s) of planes of
-// 512 floats; rho = r - az (az may be null: r already holds rho).  ex: the face coefficients
-// and the residual's 1-cell halo (NetExtra), each optional.
-struct NetIn {
-    const float* r;
-    const float* az;
-    const float* diag;
-    const uint8_t* types;
-    const float* target;
-    const int* idx;
-    int t0;
-    NetExtra ex;
-};
-
-struct Staged {
-    float rho[4];
-    float tgt[4];
-    bool in[4];
-    float S, D;  // S = 0: nothing to do on this tile
-};
-
-// Stage one tile's features into x0 (8-channel layout); thread q owns cells 4q..4q+3.
-__device__ __forceinline__ Staged stage_features(const NetIn& I, int s, __nv_bfloat16* x0, float* red) {
-    Staged o;
-    const int t = I.idx ? I.idx[s] : I.t0 + s;
-    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
-    float4 r4 = ldcg4(I.r + base);
-    if (I.az) {
-        const float4 a4 = ldcg4(I.az + base);
-        r4 = make_float4(__fsub_rn(r4.x, a4.x), __fsub_rn(r4.y, a4.y), __fsub_rn(r4.z, a4.z), __fsub_rn(r4.w, a4.w));
-    }
-    const float4 dg = ldcg4(I.diag + base);
-    const uchar4 ty = ldt4(I.types + base);
-    const float rr[4] = {r4.x, r4.y, r4.z, r4.w}, dd[4] = {dg.x, dg.y, dg.z, dg.w};
-    const uint8_t tt[4] = {ty.x, ty.y, ty.z, ty.w};
-    float ss = 0.0f, dm = 0.0f, cnt = 0.0f;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        o.in[u] = (tt[u] & dInterior) != 0;
-        o.rho[u] = o.in[u] ? rr[u] : 0.0f;
-        ss = __fmaf_rn(o.rho[u], o.rho[u], ss);
-        if (o.in[u]) {
-            dm = fmaxf(dm, fabsf(dd[u]));
-            cnt += 1.0f;
-        }
-    }
-    if (I.target) {
-        const float4 tg = ldcg4(I.target + base);
-        o.tgt[0] = tg.x, o.tgt[1] = tg.y, o.tgt[2] = tg.z, o.tgt[3] = tg.w;
-    }
-    const float sum = block_sum_f(ss, red), n = block_sum_f(cnt, red);
-    o.D = block_max_f(dm, red);
-    o.S = (n > 0.0f && sum > 0.0f && o.D > 0.0f) ? sqrtf(sum / n) : 0.0f;
-    if (o.S == 0.0f) return o;
-    // the -x, -y, -z face coefficients (cut cells: scaled by their face fractions)
-    float fc[3][4] = {};
-    if (I.ex.faces) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float4 f4 = ldcg4(I.ex.faces + (size_t)a * I.ex.fstride + (size_t)t * I.ex.ftile + 4 * threadIdx.x);
-            fc[a][0] = f4.x, fc[a][1] = f4.y, fc[a][2] = f4.z, fc[a][3] = f4.w;
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int cell = 4 * threadIdx.x + u;
-        const int v = pad_vox(cell >> 6, (cell >> 3) & 7, cell & 7);
-        __nv_bfloat162 f[4];
-        f[0] = __floats2bfloat162_rn(o.rho[u] / o.S, o.in[u] ? 1.0f : 0.0f);
-        f[1] = __floats2bfloat162_rn((tt[u] & dDirichlet) ? 1.0f : 0.0f, o.in[u] ? dd[u] / o.D : 0.0f);
-        f[2] = __floats2bfloat162_rn(o.in[u] ? fc[0][u] / o.D : 0.0f, o.in[u] ? fc[1][u] / o.D : 0.0f);
-        f[3] = __floats2bfloat162_rn(o.in[u] ? fc[2][u] / o.D : 0.0f, 0.0f);
-        *reinterpret_cast<uint4*>(x0 + v * 8) = *reinterpret_cast<const uint4*>(f);
-    }
-    // the residual's 1-cell halo: thread q owns cell (fa, fb) of the face of axis r on side
-    // q >> 6 for r = 0, 1, 2 (channel 0: rho / S of the neighbour cell, channel 1: 1 when it
-    // is an INTERIOR cell of a LEAF neighbour tile, else both 0)
-    if (I.ex.halo || I.ex.nbx) {
-        const int q = threadIdx.x, side = q >> 6, fa = (q >> 3) & 7, fb = q & 7;
-        const int e = side ? 0 : 7, hx = side ? 8 : -1;
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            float hv = 0.0f, ok = 0.0f;
-            if (I.ex.halo) {
-                const float* hs = I.ex.halo + (size_t)t * 768;
-                hv = __ldcg(hs + r * 128 + q);
-                ok = __ldcg(hs + 384 + r * 128 + q);
-            } else {
-                const int d = I.ex.nbx[8 * t + r + 3 * side];
-                if (d != 0 && (d & 7) == dLeaf) {
-                    const size_t on = (size_t)((d >> 3) - 1) * kCells +
-                                      (r == 0 ? cell_index(e, fa, fb) : r == 1 ? cell_index(fa, e, fb) : cell_index(fa, fb, e));
-                    if (I.types[on] & dInterior) {
-                        hv = __ldcg(I.r + on);
-                        if (I.az) hv = __fsub_rn(hv, __ldcg(I.az + on));
-                        ok = 1.0f;
-                    }
-                }
-            }
-            const int v = r == 0 ? pad_vox(hx, fa, fb) : r == 1 ? pad_vox(fa, hx, fb) : pad_vox(fa, fb, hx);
-            __nv_bfloat162 f[4];
-            f[0] = __floats2bfloat162_rn(ok != 0.0f ? hv / o.S : 0.0f, ok);
-            f[1] = f[2] = f[3] = __floats2bfloat162_rn(0.0f, 0.0f);
-            *reinterpret_cast<uint4*>(x0 + v * 8) = *reinterpret_cast<const uint4*>(f);
-        }
-    }
-    return o;
-}
-// zero the face halo voxels of an 8-channel buffer (whose other use needs zero padding)
-__device__ __forceinline__ void clear_face_halo(__nv_bfloat16* x0) {
-    const int q = threadIdx.x, side = q >> 6, fa = (q >> 3) & 7, fb = q & 7, hx = side ? 8 : -1;
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const int v = r == 0 ? pad_vox(hx, fa, fb) : r == 1 ? pad_vox(fa, hx, fb) : pad_vox(fa, fb, hx);
-        *reinterpret_cast<uint4*>(x0 + v * 8) = make_uint4(0, 0, 0, 0);
-    }
-}
-
 template <int H>
 struct NetDims {
     static constexpr int CG = H / 8;
@@ -415,10 +268,6 @@ __device__ __forceinline__ void copy_weights(__nv_bfloat16* dst, const __nv_bflo
     for (int i = threadIdx.x; i < n / 8; i += kNetThreads) reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
     if (threadIdx.x < 2 * H) bias[threadIdx.x] = bsrc[threadIdx.x];
 }
-__device__ __forceinline__ void zero_smem(void* p, int bytes) {
-    for (int i = threadIdx.x; i < bytes / 16; i += kNetThreads) reinterpret_cast<uint4*>(p)[i] = make_uint4(0, 0, 0, 0);
-}
-
 // Forward pass over samples; out (z) += (S/D) * f on INTERIOR cells, or, with overwrite, out = (S/D) * f.
 template <int H>
 __global__ void __launch_bounds__(kNetThreads) k_net_forward(NetIn I, int ns, const __nv_bfloat16* __restrict__ pack,
@@ -488,8 +337,6 @@ __global__ void __launch_bounds__(kNetThreads) k_net_forward(NetIn I, int ns, co
 // The accumulator of plane p occupies TMEM columns p*N .. p*N+N-1; row r of an M = 64 MMA
 // lives in TMEM lane (r % 16) + 32 (r / 16), so warp w reads rows 16w .. 16w+15 through
 // its own 32-lane quarter.
-constexpr int kTcVox = 1008;  // padded voxels per group plane (16 beyond the grid: K padding reads there)
-
 __device__ int g_net_tc_error;  // set when an MMA completion wait gives up
 
 template <int H>
@@ -503,82 +350,29 @@ struct TcDims {
     static constexpr int kActElems = 2 * kAct;
 };
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) |
-           (1ull << 46);  // no swizzle, version 1
-}
-// kind::f16 instruction descriptor: F32 accumulator, BF16 A and B, both K-major, M = 64
-__host__ __device__ constexpr uint32_t umma_idesc(int N) { return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | (4u << 24); }
-
-__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
-    uint32_t done;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-                 : "=r"(done)
-                 : "r"(mbar), "r"(parity)
-                 : "memory");
-    return done != 0;
-}
-// bounded wait for an MMA completion phase
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int i = 0; i < (1 << 20); ++i)
-        if (mbar_try(mbar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
-          "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
 // Issue one layer (thread 0): for each i-plane p and K step s, D[p] (+)= A(p, s) B(s).
 // CGI: 8-channel groups of the input; N: output columns; steps: K steps of 16.
 template <int CGI, int N>
 __device__ __forceinline__ void tc_issue_layer(uint32_t in_s, uint32_t w_s, int steps, uint32_t taddr) {
     constexpr uint32_t idesc = umma_idesc(N);
-    const uint32_t b_lbo = N * 16, b_sbo = 128;
+    // descriptors as a base plus the start-address offset in 16-byte units (the low field;
+    // shared addresses stay below 256 KB, so nothing carries into the other fields)
+    const uint64_t a_base = umma_desc(in_s + (uint32_t)pad_vox(0, 0, 0) * 16u, CGI == 2 ? kTcVox * 16 : 16u, 160u);
+    const uint64_t b_base = umma_desc(w_s, N * 16, 128);
 #pragma unroll 1
     for (int st = 0; st < steps; ++st) {  // K outer, planes inner: 8 independent accumulators in flight
-        int t0, lbo;
+        uint64_t a;
         if constexpr (CGI == 2) {
-            t0 = st;
-            lbo = kTcVox * 16;
-        } else {
-            t0 = 2 * st;
-            lbo = (t0 + 1 <= 26 ? tap_off(t0 + 1) - tap_off(t0) : 1) * 16;  // tap 27: zero weights
+            a = a_base + (uint64_t)(int64_t)tap_off(st);
+        } else {  // tap 27: zero weights
+            const int t0 = 2 * st;
+            const int lbo = t0 + 1 <= 26 ? tap_off(t0 + 1) - tap_off(t0) : 1;
+            a = (a_base & ~(0x3FFFull << 16)) + ((uint64_t)lbo << 16) + (uint64_t)(int64_t)tap_off(t0);
         }
-        const uint64_t b = umma_desc(w_s + (uint32_t)(st * 2 * N * 8 * 2), b_lbo, b_sbo);
-        const uint32_t a0 = in_s + (uint32_t)(pad_vox(0, 0, 0) + tap_off(t0)) * 16u;
+        const uint64_t b = b_base + (uint64_t)(st * (2 * N * 8 * 2 / 16));
+        const uint32_t acc = st > 0 ? 1u : 0u;
 #pragma unroll
-        for (int p = 0; p < 8; ++p) {
-            const uint64_t a = umma_desc(a0 + (uint32_t)(p * 100 * 16), (uint32_t)lbo, 160u);
-            umma_f16(taddr + (uint32_t)(p * N), a, b, idesc, st > 0 ? 1u : 0u);
-        }
+        for (int p = 0; p < 8; ++p) umma_f16(taddr + (uint32_t)(p * N), a + (uint64_t)(p * 100), b, idesc, acc);
     }
 }
 
@@ -780,36 +574,12 @@ __global__ void __launch_bounds__(kNetThreads) k_net_train(NetIn I, int nb, cons
             store_output(acc, ys);
         }
         __syncthreads();
-        // e = f - target D/S on INTERIOR cells (0 elsewhere).  Loss kind 0: sum e^2, dL/df = 2 e.
-        // Kind 1 (energy): e^T L e with L the 7-point Laplacian of the tile (6 on the diagonal,
-        // -1 per neighbour inside the tile, zero outside), dL/df = 2 (L e) on INTERIOR cells.
-        const float sc = st.D / st.S;
-        float e[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) e[u] = st.in[u] ? __fsub_rn(ys[4 * threadIdx.x + u], __fmul_rn(st.tgt[u], sc)) : 0.0f;
-        if (loss_kind == 1) {
-            __syncthreads();  // every thread has read its f
-#pragma unroll
-            for (int u = 0; u < 4; ++u) ys[4 * threadIdx.x + u] = e[u];
-            __syncthreads();
-        }
-        float l = 0.0f;
+        float g[4];
+        const float l = tile_loss_grad(st, ys, loss_kind, g);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int cell = 4 * threadIdx.x + u, ci = cell >> 6, cj = (cell >> 3) & 7, ck = cell & 7;
-            float g = e[u];
-            if (loss_kind == 1) {
-                float nbs = 0.0f;
-                if (ci > 0) nbs += ys[cell - 64];
-                if (ci < 7) nbs += ys[cell + 64];
-                if (cj > 0) nbs += ys[cell - 8];
-                if (cj < 7) nbs += ys[cell + 8];
-                if (ck > 0) nbs += ys[cell - 1];
-                if (ck < 7) nbs += ys[cell + 1];
-                g = st.in[u] ? __fsub_rn(6.0f * e[u], nbs) : 0.0f;
-            }
-            l = __fmaf_rn(e[u], g, l);
-            dy[pad_vox(ci, cj, ck) * 8] = __float2bfloat16_rn(2.0f * g);
+            const int cell = 4 * threadIdx.x + u;
+            dy[pad_vox(cell >> 6, (cell >> 3) & 7, cell & 7) * 8] = __float2bfloat16_rn(2.0f * g[u]);
         }
         const float lt = block_sum_f(l, red);  // synchronises: dy is complete
         if (threadIdx.x == 0) loss[b] = lt;
@@ -901,11 +671,14 @@ int g_infer_kind = 0;             // 0: mma.sync inference kernel (measured fast
 
 }  // namespace
 
-int net_params(int H) { return H == 16 ? NetDims<16>::kParams : NetDims<8>::kParams; }
-int net_pack_elems(int H) { return H == 16 ? NetDims<16>::kPack : NetDims<8>::kPack; }
+int net_params(int H) { return H == 32 ? deep_params() : H == 16 ? NetDims<16>::kParams : NetDims<8>::kParams; }
+int net_pack_elems(int H) { return H == 32 ? deep_pack_elems() : H == 16 ? NetDims<16>::kPack : NetDims<8>::kPack; }
+int net_bias_elems(int H) { return H == 32 ? deep_bias_elems() : 2 * H; }
+int net_train_rows(int H, int nb) { return H == 32 ? deep_train_blocks(nb) : nb; }
+size_t net_train_scratch_bytes(int H, int nb) { return H == 32 ? deep_scratch_bytes() * (size_t)deep_train_blocks(nb) : 0; }
 
 bool net_init() {
-    bool ok = true;
+    bool ok = deep_init();
     ok = ok && cudaFuncSetAttribute(k_net_forward<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<8>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_net_forward<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<16>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_net_train<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem<8>()) == cudaSuccess;
@@ -934,6 +707,10 @@ static int num_sms() {
 }
 
 void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaStream_t st) {
+    if (H == 32) {
+        launch_deep_pack(params, pack, bias, st);
+        return;
+    }
     const int n = net_pack_elems(H);
     note_kernel_launch();
     if (H == 16) k_net_pack<16><<<(n + 255) / 256, 256, 0, st>>>(params, (__nv_bfloat16*)pack, bias);
@@ -943,6 +720,10 @@ void launch_net_pack(int H, const float* params, void* pack, float* bias, cudaSt
 void launch_net_forward(int H, const float* r, const float* az, const float* diag, const uint8_t* types, const int* idx, int t0, int ns,
                         const void* pack, const float* bias, float* out, bool overwrite, cudaStream_t st, const NetExtra& ex) {
     if (ns <= 0) return;
+    if (H == 32) {
+        launch_deep_forward(r, az, diag, types, idx, t0, ns, pack, bias, out, overwrite, st, ex);
+        return;
+    }
     const NetIn I{r, az, diag, types, nullptr, idx, t0, ex};
     if (g_infer_kind == 1) {
         // resident blocks per SM from shared memory (1 KB reserved per block) and TMEM (512 columns)
@@ -979,12 +760,18 @@ int net_take_tc_error() {
     int v = 0, z = 0;
     if (cudaMemcpyFromSymbol(&v, g_net_tc_error, sizeof(int)) != cudaSuccess) return -1;
     if (v) cudaMemcpyToSymbol(g_net_tc_error, &z, sizeof(int));
-    return v;
+    const int d = deep_take_error();
+    return d < 0 ? -1 : (v | d);
 }
 
 void launch_net_train(int H, const float* rho, const float* diag, const uint8_t* types, const float* target, const int* idx, int nb,
-                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st, const NetExtra& ex) {
+                      const void* pack, const float* bias, float* grad, float* loss, int loss_kind, cudaStream_t st, const NetExtra& ex,
+                      void* scratch) {
     if (nb <= 0) return;
+    if (H == 32) {
+        launch_deep_train(rho, diag, types, target, idx, nb, pack, bias, grad, loss, loss_kind, st, ex, scratch);
+        return;
+    }
     const NetIn I{rho, nullptr, diag, types, target, idx, 0, ex};
     const int sms = num_sms();
     const int blocks = nb < sms ? nb : sms;

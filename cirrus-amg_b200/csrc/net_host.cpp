@@ -56,6 +56,7 @@ Net::~Net() {
     nfree(loss);
     nfree(gsum);
     nfree(idx);
+    if (scratch) cudaFree(scratch);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -75,9 +76,25 @@ int Net::init(int hidden, unsigned long long seed) {
     NCK(cudaMalloc(&v, sizeof(float) * np));
     NCK(cudaMalloc(&gsum, sizeof(float) * np));
     NCK(cudaMalloc(&pack, sizeof(uint16_t) * (size_t)net_pack_elems(H)));
-    NCK(cudaMalloc(&bias, sizeof(float) * 2 * H));
+    NCK(cudaMalloc(&bias, sizeof(float) * net_bias_elems(H)));
     std::vector<float> h(np, 0.0f);
     SplitMix rng{seed};
+    if (H == 32) {
+        // residual net: He-normal W0 (7 feature channels in use) and Wa; Wb at a tenth of He so
+        // that each block starts close to the identity; zero biases; a small output layer
+        const int C = 32, blk = 2 * C * 27 * C + 2 * C, wo = C * 216 + C + 4 * blk;
+        const double s0 = std::sqrt(2.0 / (27.0 * 7.0)), sh = std::sqrt(2.0 / (27.0 * C)), so = 0.1 * std::sqrt(1.0 / (27.0 * C));
+        for (int n = 0; n < C; ++n)
+            for (int t = 0; t < 27; ++t)
+                for (int c = 0; c < 8; ++c) h[(n * 27 + t) * 8 + c] = c < 7 ? (float)(s0 * rng.normal()) : 0.0f;
+        for (int k = 0; k < 4; ++k) {
+            const int wa = C * 216 + C + k * blk, wb = wa + C * 27 * C + C;
+            for (int e = 0; e < C * 27 * C; ++e) h[wa + e] = (float)(sh * rng.normal());
+            for (int e = 0; e < C * 27 * C; ++e) h[wb + e] = (float)(0.1 * sh * rng.normal());
+        }
+        for (int e = wo; e < np; ++e) h[e] = (float)(so * rng.normal());
+        return set_params(h.data());
+    }
     const int w1 = 0, b1 = w1 + H * 216, w2 = b1 + H, b2 = w2 + H * 27 * H, w3 = b2 + H;
     const double s1 = std::sqrt(2.0 / (27.0 * 4.0)), s2 = std::sqrt(2.0 / (27.0 * H)), s3 = 0.1 * std::sqrt(1.0 / (27.0 * H));
     for (int n = 0; n < H; ++n)
@@ -144,8 +161,15 @@ int Net::set_samples(int n, const float* hr, const float* hd, const uint8_t* ht,
 int Net::ensure_batch(int nb) {
     if (nb <= batch_cap) return 0;
     nfree(grad);
+    if (scratch) cudaFree(scratch);
+    scratch = nullptr;
     batch_cap = 0;
-    NCK(cudaMalloc(&grad, sizeof(float) * (size_t)nb * np));
+    NCK(cudaMalloc(&grad, sizeof(float) * (size_t)net_train_rows(H, nb) * np));
+    if (const size_t sb = net_train_scratch_bytes(H, nb)) {
+        // the activation planes' borders are never written: they stay zero
+        NCK(cudaMalloc(&scratch, sb));
+        NCK(cudaMemsetAsync(scratch, 0, sb, st));
+    }
     batch_cap = nb;
     return 0;
 }
@@ -181,9 +205,13 @@ int Net::forward(int first, int n, float* out_host) {
 int Net::gradient(int first, int n, double* loss_out, float* grad_host) {
     if (int rc = ensure_batch(n)) return rc;
     const size_t o = (size_t)first * kCells;
-    launch_net_train(H, rho + o, diag + o, types + o, target + o, nullptr, n, pack, bias, grad, loss, loss_kind, st, extra(first));
+    launch_net_train(H, rho + o, diag + o, types + o, target + o, nullptr, n, pack, bias, grad, loss, loss_kind, st, extra(first), scratch);
     const float scale = 1.0f / ((float)n * kCells);
-    launch_net_reduce_adam(grad, n, np, scale, gsum, p, m, v, 0.0f, 0, false, st);
+    launch_net_reduce_adam(grad, net_train_rows(H, n), np, scale, gsum, p, m, v, 0.0f, 0, false, st);
+    if (net_take_tc_error() == 1) {
+        set_error("learned gradient: a tensor-core MMA or bulk copy did not complete in time");
+        return 2;
+    }
     std::vector<float> l(n);
     NCK(cudaMemcpyAsync(l.data(), loss, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
     if (grad_host) NCK(cudaMemcpyAsync(grad_host, gsum, sizeof(float) * np, cudaMemcpyDeviceToHost, st));
@@ -214,12 +242,17 @@ int Net::train(int epochs, int batch, float lr, unsigned long long seed, float* 
         NCK(cudaMemcpyAsync(idx, perm.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
         for (int b0 = 0; b0 < ns; b0 += batch) {
             const int nb = ns - b0 < batch ? ns - b0 : batch;
-            launch_net_train(H, rho, diag, types, target, idx + b0, nb, pack, bias, grad, loss + b0, loss_kind, st, extra(0));
-            launch_net_reduce_adam(grad, nb, np, 1.0f / ((float)nb * kCells), nullptr, p, m, v, lr, ++adam_step, true, st);
+            launch_net_train(H, rho, diag, types, target, idx + b0, nb, pack, bias, grad, loss + b0, loss_kind, st, extra(0), scratch);
+            launch_net_reduce_adam(grad, net_train_rows(H, nb), np, 1.0f / ((float)nb * kCells), nullptr, p, m, v, lr, ++adam_step, true,
+                                   st);
             launch_net_pack(H, p, pack, bias, st);
         }
         NCK(cudaMemcpyAsync(l.data(), loss, sizeof(float) * ns, cudaMemcpyDeviceToHost, st));
         NCK(cudaStreamSynchronize(st));
+        if (net_take_tc_error() == 1) {
+            set_error("learned train: a tensor-core MMA or bulk copy did not complete in time");
+            return 2;
+        }
         double s = 0.0;
         for (int i = 0; i < ns; ++i) s += l[i];
         if (epoch_loss) epoch_loss[e] = (float)(s / ((double)ns * kCells));

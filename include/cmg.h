@@ -274,7 +274,9 @@ int cmg_amg_solver_set_launch_mode(cmg_amg_solver* s, int flags);
 #define CMG_STORAGE_FP16 2
 int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage);
 /* Learned finest-level smoother (no counterpart in the reference).  A per-tile 3-D conv
- * net (conv3x3x3 8->H, ReLU, H->H, ReLU, H->1; H = 8 or 16) on BF16 tensor cores adds
+ * net on BF16 tensor cores, hidden = 8 or 16 (conv3x3x3 8->H, ReLU, H->H, ReLU, H->1) or
+ * 32 (conv 8->32, ReLU, four residual blocks x = relu(x + conv(relu(conv(x))))) at 32
+ * channels, conv 32->1; tcgen05 MMAs with TMEM accumulators for inference and training), adds
  * (S/D) f(rho/S, INTERIOR, DIRICHLET, diag/D) to z on the finest level's LEAF tiles after
  * each mu-cycle, rho = r - A z being the residual the cycle leaves (S: its RMS on the
  * tile, D: the tile's largest diagonal).  The solve then runs flexible CG (Polak-Ribiere
@@ -288,7 +290,9 @@ typedef struct cmg_learned cmg_learned;
 int cmg_learned_create(int hidden, unsigned long long seed, cmg_learned** out);
 int cmg_learned_destroy(cmg_learned* net);
 int cmg_learned_num_params(cmg_learned* net, int* n);
-/* fp32 parameters: W1[H][27][8], b1[H], W2[H][27][H], b2[H], W3[27][H]; tap = dx*9+dy*3+dz */
+/* fp32 parameters: W1[H][27][8], b1[H], W2[H][27][H], b2[H], W3[27][H]; tap = dx*9+dy*3+dz.
+ * hidden = 32: W0[32][27][8], b0[32], per block k = 0..3 Wa[32][27][32], ba[32], Wb[32][27][32],
+ * bb[32], then Wo[27][32] (229,248 in all) */
 int cmg_learned_get_params(cmg_learned* net, float* host, int n);
 int cmg_learned_set_params(cmg_learned* net, const float* host, int n); /* also resets Adam */
 /* training/evaluation tiles: rho, diag, types, target [n][512]; optional (NULL: absent, the

@@ -195,3 +195,98 @@ def loss_and_grad(p, H, rho, diag, types, target, emulate_bf16=True, kind=0, fac
     gb1 = dz1.sum((0, 1, 2, 3))
     g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel()]) * scale
     return loss, g
+
+
+# ---------------------------------------------------------------------------------------
+# The residual network (hidden = 32): conv 8->32, four residual blocks of two 3x3x3 convs
+# at 32 channels, conv 32->1.
+#   x1 = relu(conv(x0, W0) + b0)
+#   block k: h_k = relu(conv(x_k, Wa_k) + ba_k); x_{k+1} = relu(x_k + conv(h_k, Wb_k) + bb_k)
+#   f = conv(x5, Wo)
+# The GPU rounds x0, the weights, x_k, h_k, 2 (f - t) and every back-propagated gradient
+# that enters a convolution (the ReLU-masked pre-activation gradients) to BF16.
+# ---------------------------------------------------------------------------------------
+DEEP_BLOCKS = 4
+DEEP_C = 32
+
+
+def layout_deep():
+    C, o = DEEP_C, {}
+    o["W0"] = 0
+    o["B0"] = C * 216
+    base = o["B0"] + C
+    blk = 2 * (C * 27 * C) + 2 * C
+    for k in range(DEEP_BLOCKS):
+        o[f"Wa{k}"] = base + k * blk
+        o[f"Ba{k}"] = o[f"Wa{k}"] + C * 27 * C
+        o[f"Wb{k}"] = o[f"Ba{k}"] + C
+        o[f"Bb{k}"] = o[f"Wb{k}"] + C * 27 * C
+    o["WO"] = base + DEEP_BLOCKS * blk
+    o["n"] = o["WO"] + 27 * C
+    return o
+
+
+def unpack_deep(p):
+    L, C = layout_deep(), DEEP_C
+    p = np.asarray(p, dtype=np.float64)
+    W0 = p[L["W0"]:L["B0"]].reshape(C, 27, 8)
+    b0 = p[L["B0"]:L["B0"] + C]
+    blocks = []
+    for k in range(DEEP_BLOCKS):
+        blocks.append((p[L[f"Wa{k}"]:L[f"Ba{k}"]].reshape(C, 27, C), p[L[f"Ba{k}"]:L[f"Wb{k}"]],
+                       p[L[f"Wb{k}"]:L[f"Bb{k}"]].reshape(C, 27, C), p[L[f"Bb{k}"]:L[f"Bb{k}"] + C]))
+    Wo = p[L["WO"]:L["n"]].reshape(1, 27, C)
+    return W0, b0, blocks, Wo
+
+
+def _forward_deep(p, x0, emulate_bf16):
+    W0, b0, blocks, Wo = unpack_deep(p)
+    r = bf16 if emulate_bf16 else (lambda a: a)
+    W0, Wo = r(W0), r(Wo)
+    blocks = [(r(Wa), ba, r(Wb), bb) for Wa, ba, Wb, bb in blocks]
+    xs = [r(np.maximum(conv(x0, W0) + b0, 0.0))]
+    hs = []
+    for Wa, ba, Wb, bb in blocks:
+        h = r(np.maximum(conv(xs[-1], Wa) + ba, 0.0))
+        hs.append(h)
+        xs.append(r(np.maximum(conv(h, Wb) + bb + xs[-1], 0.0)))
+    f = conv(xs[-1], Wo)[..., 0]
+    return f, (W0, blocks, Wo, xs, hs)
+
+
+def forward_deep(p, rho, diag, types, emulate_bf16=True, faces=None, halo=None):
+    """Correction (S/D) f of the residual network on INTERIOR cells, [n, 512]."""
+    x, S, D, inter, ok = features(rho, diag, types, emulate_bf16, faces, halo)
+    f, _ = _forward_deep(p, x, emulate_bf16)
+    sc = np.where(ok, S / np.where(ok, D, 1.0), 0.0)[:, None]
+    return np.where(inter & ok[:, None], sc * f.reshape(-1, 512), 0.0)
+
+
+def loss_and_grad_deep(p, rho, diag, types, target, emulate_bf16=True, kind=0, faces=None, halo=None):
+    """Mean loss of the residual network and its gradient (layout of `layout_deep()`)."""
+    x0, S, D, inter, ok = features(rho, diag, types, emulate_bf16, faces, halo)
+    n = x0.shape[0]
+    f, (W0, blocks, Wo, xs, hs) = _forward_deep(p, x0, emulate_bf16)
+    r = bf16 if emulate_bf16 else (lambda a: a)
+    tgt = np.asarray(target, dtype=np.float64).reshape(-1, 512) * np.where(ok, D / np.where(ok, S, 1.0), 0.0)[:, None]
+    m = inter & ok[:, None]
+    e = np.where(m, f.reshape(-1, 512) - tgt, 0.0)
+    g = np.where(m, tile_laplacian(e), 0.0) if kind == 1 else e
+    scale = 1.0 / (n * 512)
+    loss = (e * g).sum() * scale
+    dy = r(2.0 * g).reshape(n, 8, 8, 8, 1)
+    L = layout_deep()
+    grad = np.zeros(L["n"])
+    grad[L["WO"]:L["n"]] = conv_weight_grad(xs[-1], dy).ravel()
+    d = r(conv_input_grad(dy, Wo) * (xs[-1] > 0))  # gradient of block 3's pre-activation
+    for k in range(DEEP_BLOCKS - 1, -1, -1):
+        Wa, ba, Wb, bb = blocks[k]
+        grad[L[f"Bb{k}"]:L[f"Bb{k}"] + DEEP_C] = d.sum((0, 1, 2, 3))
+        grad[L[f"Wb{k}"]:L[f"Bb{k}"]] = conv_weight_grad(hs[k], d).ravel()
+        da = r(conv_input_grad(d, Wb) * (hs[k] > 0))
+        grad[L[f"Ba{k}"]:L[f"Wb{k}"]] = da.sum((0, 1, 2, 3))
+        grad[L[f"Wa{k}"]:L[f"Ba{k}"]] = conv_weight_grad(xs[k], da).ravel()
+        d = r((d + conv_input_grad(da, Wa)) * (xs[k] > 0))
+    grad[L["B0"]:L["B0"] + DEEP_C] = d.sum((0, 1, 2, 3))
+    grad[L["W0"]:L["B0"]] = conv_weight_grad(x0, d).ravel()
+    return loss, grad * scale

@@ -99,7 +99,7 @@ def test_learned_entry_points_reject_bad_arguments():
     """The learned smoother's entry points validate their arguments before touching the GPU."""
     L = cmg.lib()
     out = ctypes.c_void_p()
-    assert L.cmg_learned_create(12, 0, ctypes.byref(out)) == 1  # hidden must be 8 or 16
+    assert L.cmg_learned_create(12, 0, ctypes.byref(out)) == 1  # hidden must be 8, 16 or 32
     assert L.cmg_learned_create(8, 0, None) == 1
     assert L.cmg_learned_set_inference(2) == 1
     assert L.cmg_learned_set_loss(None, 0) == 1

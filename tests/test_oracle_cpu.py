@@ -482,3 +482,32 @@ def test_oracle_cycle_variants_reduce_the_residual(cycle, case):
     assert np.linalg.norm(r[m]) < 0.2 * np.linalg.norm(f[m])
     if cycle != "fcycle":
         assert np.array_equal(g.channel(11), f)
+
+
+def test_deep_oracle_gradient_matches_finite_differences():
+    """The residual net's FP64 restatement (hidden = 32): its analytic gradient against central
+    differences of its loss, on parameters of every layer (both loss kinds)."""
+    import numpy as np
+
+    from oracle import learned_oracle as LO
+
+    L = LO.layout_deep()
+    assert L["n"] == 229248
+    rng = np.random.default_rng(0)
+    p = rng.normal(size=L["n"]) * 0.05
+    rho = rng.normal(size=(2, 512)).astype(np.float32)
+    diag = (6 + rng.random((2, 512))).astype(np.float32)
+    types = np.full((2, 512), 2, np.uint8)
+    types[0, :10] = 1
+    tg = rng.normal(size=(2, 512)).astype(np.float32)
+    for kind in (0, 1):
+        _, g = LO.loss_and_grad_deep(p, rho, diag, types, tg, emulate_bf16=False, kind=kind)
+        for idx in (L["W0"] + 9, L["B0"] + 3, L["Wa0"] + 100, L["Ba1"] + 5, L["Wb2"] + 7, L["Bb3"] + 2, L["WO"] + 40):
+            e = 1e-6
+            pp, pm = p.copy(), p.copy()
+            pp[idx] += e
+            pm[idx] -= e
+            lp, _ = LO.loss_and_grad_deep(pp, rho, diag, types, tg, emulate_bf16=False, kind=kind)
+            lm, _ = LO.loss_and_grad_deep(pm, rho, diag, types, tg, emulate_bf16=False, kind=kind)
+            fd = (lp - lm) / (2 * e)
+            assert abs(fd - g[idx]) <= 1e-6 + 1e-5 * abs(fd), (kind, idx, fd, g[idx])
