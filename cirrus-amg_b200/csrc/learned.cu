@@ -326,17 +326,18 @@ __global__ void __launch_bounds__(kNetThreads) k_net_forward(NetIn I, int ns, co
 // Inference on the 5th-generation tensor cores (tcgen05.mma, accumulators in TMEM)
 // ---------------------------------------------------------------------------
 // Activations are channel-group-major planes: element (voxel v, channel c) of a buffer with
-// CG groups sits at ((c >> 3) * kTcVox + v) * 8 + (c & 7), 16 bytes per voxel and group.  One
-// MMA computes one i-plane of the tile (M = 64 voxels: 8 rows j of 8 voxels k) against N
-// output channels for one 16-wide K step.  In the no-swizzle K-major operand layout the
-// 8-voxel rows are core matrices (128 contiguous bytes), the 8 rows sit 10 voxels (160 B)
-// apart (the stride-dimension offset) and the two K halves are the two channel groups
+// CG groups sits at ((c >> 3) * kTcVox + v) * 8 + (c & 7), 16 bytes per voxel and group.  In
+// the no-swizzle K-major operand layout the 8-voxel rows of the padded grid are core matrices
+// (128 contiguous bytes) that follow one another 10 voxels (160 B) apart through the planes
+// (the stride-dimension offset): row R = 10 i + j, j = 0..9.  One M = 128 MMA takes 16
+// consecutive rows against N output channels for one 16-wide K step, so 5 MMAs (tiles m =
+// 0..4, rows 16m..16m+15) cover the tile's 80 rows; the rows j = 8, 9 are border rows of the
+// padded grid, computed and never stored.  The two K halves are the two channel groups
 // (kTcVox voxels apart) or, with 8 input channels, the next tap (the leading-dimension
 // offset).  A tap's shifted operand is therefore only a different start address: no im2col.
 // Weights are stored per K step as [K half][n][8] (core matrices of 8 output channels).
-// The accumulator of plane p occupies TMEM columns p*N .. p*N+N-1; row r of an M = 64 MMA
-// lives in TMEM lane (r % 16) + 32 (r / 16), so warp w reads rows 16w .. 16w+15 through
-// its own 32-lane quarter.
+// The accumulator of tile m occupies TMEM columns m*N .. m*N+N-1, row r in lane r.
+constexpr int kTcTiles = 5;
 __device__ int g_net_tc_error;  // set when an MMA completion wait gives up
 
 template <int H>
@@ -345,7 +346,7 @@ struct TcDims {
     static constexpr int S1 = 14, SH = CG == 2 ? 27 : 14;  // K steps of 16
     static constexpr int W1 = 0, W2 = W1 + S1 * 2 * H * 8, W3 = W2 + SH * 2 * H * 8, kW = W3 + SH * 2 * 8 * 8;  // bf16 elements
     static constexpr int kAct = kTcVox * H;
-    static constexpr int kCols = H == 16 ? 128 : 64;  // TMEM columns: 8 planes x N
+    static constexpr int kCols = H == 16 ? 128 : 64;  // TMEM columns: 5 tiles x N, rounded up to a power of 2
     // shared memory: a1 | x0 and a2 in the same place (x0 is dead once layer 1 has run) | weights
     static constexpr int kActElems = 2 * kAct;
 };
@@ -354,13 +355,13 @@ struct TcDims {
 // CGI: 8-channel groups of the input; N: output columns; steps: K steps of 16.
 template <int CGI, int N>
 __device__ __forceinline__ void tc_issue_layer(uint32_t in_s, uint32_t w_s, int steps, uint32_t taddr) {
-    constexpr uint32_t idesc = umma_idesc(N);
+    constexpr uint32_t idesc = (umma_idesc(N) & ~(0x1Fu << 24)) | (8u << 24);  // M = 128
     // descriptors as a base plus the start-address offset in 16-byte units (the low field;
     // shared addresses stay below 256 KB, so nothing carries into the other fields)
     const uint64_t a_base = umma_desc(in_s + (uint32_t)pad_vox(0, 0, 0) * 16u, CGI == 2 ? kTcVox * 16 : 16u, 160u);
     const uint64_t b_base = umma_desc(w_s, N * 16, 128);
 #pragma unroll 1
-    for (int st = 0; st < steps; ++st) {  // K outer, planes inner: 8 independent accumulators in flight
+    for (int st = 0; st < steps; ++st) {  // K outer, tiles inner: 5 independent accumulators in flight
         uint64_t a;
         if constexpr (CGI == 2) {
             a = a_base + (uint64_t)(int64_t)tap_off(st);
@@ -372,8 +373,14 @@ __device__ __forceinline__ void tc_issue_layer(uint32_t in_s, uint32_t w_s, int 
         const uint64_t b = b_base + (uint64_t)(st * (2 * N * 8 * 2 / 16));
         const uint32_t acc = st > 0 ? 1u : 0u;
 #pragma unroll
-        for (int p = 0; p < 8; ++p) umma_f16(taddr + (uint32_t)(p * N), a + (uint64_t)(p * 100), b, idesc, acc);
+        for (int m = 0; m < kTcTiles; ++m) umma_f16(taddr + (uint32_t)(m * N), a + (uint64_t)(m * 160), b, idesc, acc);
     }
+}
+
+// voxel of TMEM lane `row` of tile m (-1: a border row of the padded grid, not stored)
+__device__ __forceinline__ int tc_tile_voxel(int m, int row) {
+    const int R = 16 * m + (row >> 3), i = R / 10, j = R - 10 * i;
+    return j < 8 ? pad_vox(i, j, row & 7) : -1;
 }
 
 // Hidden-layer epilogue from TMEM: all eight planes' accumulators loaded before one wait, then
@@ -382,25 +389,24 @@ __device__ __forceinline__ void tc_issue_layer(uint32_t in_s, uint32_t w_s, int 
 template <int H>
 __device__ __forceinline__ void tc_epilogue_hidden(uint32_t lane_base, int warp, int lane, const float* bias, __nv_bfloat16* out) {
     constexpr int CG = H / 8;
-    float v[8][H];
+    float v[kTcTiles][H];
 #pragma unroll
-    for (int pl = 0; pl < 8; ++pl) {
-        if constexpr (H == 16) tmem_ld16(lane_base + pl * H, v[pl]);
-        else tmem_ld8(lane_base + pl * H, v[pl]);
+    for (int m = 0; m < kTcTiles; ++m) {
+        if constexpr (H == 16) tmem_ld16(lane_base + m * H, v[m]);
+        else tmem_ld8(lane_base + m * H, v[m]);
     }
     tmem_wait_ld();
-    if (lane >= 16) return;
-    const int r = 16 * warp + lane;
 #pragma unroll
-    for (int pl = 0; pl < 8; ++pl) {
-        const int vx = pad_vox(pl, r >> 3, r & 7);
+    for (int m = 0; m < kTcTiles; ++m) {
+        const int vx = tc_tile_voxel(m, 32 * warp + lane);
+        if (vx < 0) continue;
 #pragma unroll
         for (int g = 0; g < CG; ++g) {
             __nv_bfloat162 o[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e)
-                o[e] = __floats2bfloat162_rn(fmaxf(__fadd_rn(v[pl][8 * g + 2 * e], bias[8 * g + 2 * e]), 0.0f),
-                                             fmaxf(__fadd_rn(v[pl][8 * g + 2 * e + 1], bias[8 * g + 2 * e + 1]), 0.0f));
+                o[e] = __floats2bfloat162_rn(fmaxf(__fadd_rn(v[m][8 * g + 2 * e], bias[8 * g + 2 * e]), 0.0f),
+                                             fmaxf(__fadd_rn(v[m][8 * g + 2 * e + 1], bias[8 * g + 2 * e + 1]), 0.0f));
             *reinterpret_cast<uint4*>(out + (g * kTcVox + vx) * 8) = *reinterpret_cast<const uint4*>(o);
         }
     }
@@ -495,13 +501,14 @@ __global__ void __launch_bounds__(kNetThreads) k_net_forward_tc(NetIn I, int ns,
         ok = run_layer(std::integral_constant<int, CG>{}, std::integral_constant<int, 8>{}, smem_u32(a2), smem_u32(wt + Tc::W3), Tc::SH);
         if (!ok) break;
         {
-            float v[8][8];
+            float v[kTcTiles][8];
 #pragma unroll
-            for (int pl = 0; pl < 8; ++pl) tmem_ld8(lane_base + pl * 8, v[pl]);
+            for (int m = 0; m < kTcTiles; ++m) tmem_ld8(lane_base + m * 8, v[m]);
             tmem_wait_ld();
-            if (lane < 16) {
 #pragma unroll
-                for (int pl = 0; pl < 8; ++pl) ys[pl * 64 + 16 * warp + lane] = v[pl][0];
+            for (int m = 0; m < kTcTiles; ++m) {
+                const int R = 16 * m + ((32 * warp + lane) >> 3), i = R / 10, j = R - 10 * i;
+                if (j < 8) ys[i * 64 + j * 8 + (lane & 7)] = v[m][0];
             }
         }
         tc_fence_before();

@@ -13,12 +13,13 @@
 // One CTA of 128 threads per SM (191 KB of shared memory) loops over tiles.  Activations
 // are channel-group-major planes, element (voxel v, channel c) at ((c >> 3) * kTcVox + v)
 // * 8 + (c & 7): 16 bytes per voxel and 8-channel group, the padded 10^3 voxel grid.
-//   * A convolution is one MMA per i-plane of the tile (M = 64 voxels: 8 rows j of 8
-//     voxels k) and 16-wide K step: K-major A operand straight from the activation buffer
-//     (the 8-voxel rows are 128-byte core matrices 160 B apart, the K halves are channel
-//     groups or, with 8 input channels, the next tap), so a tap's shifted operand is only a
-//     start address (no im2col).  Weights per K step as [K half][n][8].  The 8 planes' FP32
-//     accumulators (N = 32 columns each) sit side by side in TMEM.
+//   * A convolution is five M = 128 MMAs per 16-wide K step: K-major A operand straight from
+//     the activation buffer (the 8-voxel rows are 128-byte core matrices 160 B apart through
+//     the padded grid's planes, 16 of them per MMA, the two border rows of each plane
+//     computed and discarded; the K halves are channel groups or, with 8 input channels, the
+//     next tap), so a tap's shifted operand is only a start address (no im2col).  Weights
+//     per K step as [K half][n][8].  The five tiles' FP32 accumulators (N = 32 columns
+//     each) sit side by side in TMEM.
 //   * The weights of each convolution (55 KB) stream into one shared buffer with a bulk
 //     copy (cp.async.bulk onto an mbarrier) as soon as the previous convolution's MMAs have
 //     completed, overlapping the epilogue.
@@ -92,6 +93,9 @@ constexpr size_t kScrBytes = kScrG + kBufB;
 
 __device__ int g_deep_error;  // set when an mbarrier wait gives up
 
+constexpr int kConvTiles = 5;  // M = 128 tiles of a convolution (rows R = 0..79)
+// kind::f16, M = 128, both operands K-major (the convolutions)
+__host__ __device__ constexpr uint32_t umma_idesc_m128(int N) { return (umma_idesc(N) & ~(0x1Fu << 24)) | (8u << 24); }
 // kind::f16, M = 64, both operands MN-major (the weight-gradient MMAs)
 __host__ __device__ constexpr uint32_t umma_idesc_mn(int N) { return umma_idesc(N) | (1u << 15) | (1u << 16); }
 
@@ -105,15 +109,20 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
 }
 __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
-// Convolution (thread 0): D[plane p] (+)= A(p, step) B(step) for the 8 i-planes.
+// Convolution (thread 0): D[tile m] (+)= A(m, step) B(step) for the 5 row tiles.
 // CGI = 4: 54 K steps (tap, channel-group pair); CGI = 1: 14 steps of two taps (tap 27 zero).
+// M = 128: the 8-voxel rows of the padded grid follow one another 10 voxels (160 B) apart
+// through the planes, row R = 10 i + j for j = 0..9, so 16 consecutive rows are one operand;
+// tile m holds rows 16m..16m+15, and the rows j = 8, 9 (the border rows of the padded grid)
+// are computed and never stored.  80 rows in 5 MMAs instead of 64 in 8 M = 64 MMAs: the
+// per-instruction cost of these small MMAs, not their arithmetic, bounds a convolution.
 // A descriptor's start address is its low 14 bits in 16-byte units, so each MMA's operand
 // descriptor is a base descriptor plus an offset (no field can carry: shared addresses stay
 // below 256 KB); the issuing thread spends a couple of instructions per MMA.
 template <int CGI, int N>
 __device__ __forceinline__ void dc_issue_conv(uint32_t in_s, uint32_t w_s, uint32_t taddr) {
     constexpr int kSteps = CGI == 4 ? 54 : 14;
-    constexpr uint32_t idesc = umma_idesc(N);
+    constexpr uint32_t idesc = umma_idesc_m128(N);
     const uint64_t a_base = umma_desc(in_s + (uint32_t)pad_vox(0, 0, 0) * 16u, CGI == 4 ? kGrpB : 16u, 160u);
     const uint64_t b_base = umma_desc(w_s, N * 16, 128);
 #pragma unroll 1
@@ -129,7 +138,7 @@ __device__ __forceinline__ void dc_issue_conv(uint32_t in_s, uint32_t w_s, uint3
         const uint64_t b = b_base + (uint64_t)(st * (2 * N * 8 * 2 / 16));
         const uint32_t acc = st > 0 ? 1u : 0u;
 #pragma unroll
-        for (int p = 0; p < 8; ++p) umma_f16(taddr + (uint32_t)(p * N), a + (uint64_t)(p * 100), b, idesc, acc);
+        for (int m = 0; m < kConvTiles; ++m) umma_f16(taddr + (uint32_t)(m * N), a + (uint64_t)(m * 160), b, idesc, acc);
     }
 }
 
@@ -171,22 +180,26 @@ __device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
     return u;
 }
 
-// Hidden-layer epilogues: accumulator row r = 16 warp + lane (lanes 0-15) of plane pl is voxel
-// (pl, r >> 3, r & 7); the result goes to the buffer at dst and, if scr, to the same place in
-// the CTA's scratch.
+// voxel of TMEM lane `row` of convolution tile m (-1: a border row, not stored)
+__device__ __forceinline__ int dc_tile_voxel(int m, int row) {
+    const int R = 16 * m + (row >> 3), i = R / 10, j = R - 10 * i;
+    return j < 8 ? pad_vox(i, j, row & 7) : -1;
+}
+
+// Hidden-layer epilogues: TMEM lane 32 warp + lane of tile m is voxel dc_tile_voxel; the result
+// goes to the buffer at dst and, if scr, to the same place in the CTA's scratch.
 enum { kEpReluBias, kEpResid, kEpMaskSelf, kEpResidMask };
 template <int kOp>
 __device__ __forceinline__ void dc_epilogue(uint32_t lane_base, int warp, int lane, unsigned char* dst, const float* bias,
                                             unsigned char* scr, const unsigned char* mask_src) {
 #pragma unroll 1
-    for (int pl = 0; pl < 8; ++pl) {
+    for (int mt = 0; mt < kConvTiles; ++mt) {
         float v[2][16];
-        tmem_ld16(lane_base + (uint32_t)(pl * 32), v[0]);
-        tmem_ld16(lane_base + (uint32_t)(pl * 32 + 16), v[1]);
+        tmem_ld16(lane_base + (uint32_t)(mt * 32), v[0]);
+        tmem_ld16(lane_base + (uint32_t)(mt * 32 + 16), v[1]);
         tmem_wait_ld();
-        if (lane >= 16) continue;
-        const int r = 16 * warp + lane;
-        const int vx = pad_vox(pl, r >> 3, r & 7);
+        const int vx = dc_tile_voxel(mt, 32 * warp + lane);
+        if (vx < 0) continue;
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
             uint4* d = reinterpret_cast<uint4*>(dst + g * kGrpB + vx * 16);
@@ -398,10 +411,11 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_net_deep(NetIn I, int ns, co
         else load_w(kPF0, kWs8);  // the next tile's first layer
         {
             float v[8];
-            for (int pl = 0; pl < 8; ++pl) {
-                tmem_ld8(lane_base + (uint32_t)(pl * 8), v);
+            for (int mt = 0; mt < kConvTiles; ++mt) {
+                tmem_ld8(lane_base + (uint32_t)(mt * 8), v);
                 tmem_wait_ld();
-                if (lane < 16) ys[pl * 64 + 16 * warp + lane] = v[0];
+                const int R = 16 * mt + ((32 * warp + lane) >> 3), i = R / 10, j = R - 10 * i;
+                if (j < 8) ys[i * 64 + j * 8 + (lane & 7)] = v[0];
             }
         }
         tc_fence_before();
