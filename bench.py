@@ -572,8 +572,9 @@ def run_sequence(args, rank, world, local_rank):
     S = make_solver(cmg)
     t0 = time.perf_counter()
     pairs = collect_training_pairs(cmg, spec0, S)  # random sphere octrees, not the sequence's
-    net, losses = learned.train(pairs, hidden=LEARNED["hidden"], epochs=LEARNED["epochs"], batch=LEARNED["batch"],
-                                lr=LEARNED["lr"], seed=0, damping=LEARNED["damping"], loss=LEARNED["loss"])
+    cfg = LEARNED_DEEP if args.learned_net == "residual" else LEARNED
+    net, losses = learned.train(pairs, hidden=cfg["hidden"], epochs=cfg["epochs"], batch=cfg["batch"], lr=cfg["lr"], seed=0,
+                                damping=cfg["damping"], loss=cfg["loss"])
     train_s = time.perf_counter() - t0
     G = build_grid(cmg, spec0)
     rhs = training_rhs(cmg, G, spec0, 1)
@@ -631,8 +632,8 @@ def run_sequence(args, rank, world, local_rank):
             "l2": "inputs larger than L2: ~550 MB of channel planes per octree",
             "plain_pcg_iters": [min(plain_it), max(plain_it)], "octree_setup_s_per_step": round(setup_s / max(args.steps, 1), 3),
             "learned_preconditioner": {
-                "hidden": LEARNED["hidden"], "loss": LEARNED["loss"], "damping": LEARNED["damping"],
-                "inference_kernel": LEARNED_INFERENCE[0], "trained_on": "3 random sphere octrees, 10 right-hand sides (none of the sequence's)", "train_and_collect_s": round(train_s, 3),
+                "hidden": cfg["hidden"], "network": NETWORKS[cfg["hidden"]], "loss": cfg["loss"], "damping": cfg["damping"],
+                "inference_kernel": "tcgen05" if cfg["hidden"] == 32 else LEARNED_INFERENCE[0], "trained_on": "3 random sphere octrees, 10 right-hand sides (none of the sequence's)", "train_and_collect_s": round(train_s, 3),
                 "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
                 "ms_mean": round(ml, 4), "learned_pcg_iters": [min(learned_it), max(learned_it)], "fell_back": fallbacks,
                 "rel_residual_true_max": float(max(true_rel)), "plain_ms_mean": round(mp, 4)},
@@ -1121,6 +1122,8 @@ def main():
     ap.add_argument("--learned-inference", default="mma.sync", choices=["mma.sync", "tcgen05"],
                     help="inference kernel of the learned smoother")
     ap.add_argument("--workload", default="sphere", choices=sorted(WORKLOADS))
+    ap.add_argument("--learned-net", default="small", choices=["small", "residual"],
+                    help="moving_sphere: the learned smoother's net (small: 3 convs at 8 channels; residual: 4 residual blocks at 32)")
     ap.add_argument("--streams", type=int, default=BATCH_STREAMS, help="streams of the batched workload")
     ap.add_argument("--batch-instances", type=int, default=64, help="batched workload: solve only its first N octrees (profiling)")
     ap.add_argument("--batch-schedule", default=None,
