@@ -71,6 +71,8 @@ struct BCtx {
 template <class Ctx>
 __device__ bool group_sync(const Ctx& C) {
     __syncthreads();
+    // a group of one block: the block barrier already orders its threads' global memory
+    if (C.G == 1) return *(volatile unsigned int*)C.err == 0;
     if (threadIdx.x == 0) {
         volatile unsigned int* gen = C.gbar + 1;
         const unsigned int g0 = *gen;
