@@ -685,7 +685,7 @@ int net_train_rows(int H, int nb) { return H == 32 ? deep_train_blocks(nb) : nb;
 size_t net_train_scratch_bytes(int H, int nb) { return H == 32 ? deep_scratch_bytes() * (size_t)deep_train_blocks(nb) : 0; }
 
 bool net_init() {
-    bool ok = deep_init();
+    bool ok = true;
     ok = ok && cudaFuncSetAttribute(k_net_forward<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<8>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_net_forward<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<16>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_net_train<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem<8>()) == cudaSuccess;

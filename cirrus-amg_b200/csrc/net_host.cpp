@@ -68,6 +68,13 @@ int Net::init(int hidden, unsigned long long seed) {
         set_error("learned: the network kernels cannot be configured on this device");
         return 2;
     }
+    if (hidden == 32) {
+        static const bool deep_ok = deep_init();
+        if (!deep_ok) {
+            set_error("learned: the residual network's kernels cannot be configured on this device");
+            return 2;
+        }
+    }
     H = hidden;
     np = net_params(H);
     NCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
