@@ -70,10 +70,11 @@ BYTES_PER_CELL = dict(
 )
 
 
-def solve_algorithmic_bytes(G, mu, level_iters, iters):
+def solve_algorithmic_bytes(G, mu, level_iters, iters, finest_iters=-1):
     """Algorithmic DRAM bytes of one plain solve of octree G that took `iters` PCG iterations:
     every tile step of the FAS mu-cycle (a level-l step runs mu^(top-l) times per cycle) and
-    of the PCG vector updates, each plane read or written once per step."""
+    of the PCG vector updates, each plane read or written once per step.  finest_iters >= 0:
+    the sweeps of the finest level (the autotuner's setting), else level_iters."""
     lv, _, ty = G.tiles()
     import cmg
 
@@ -86,7 +87,9 @@ def solve_algorithmic_bytes(G, mu, level_iters, iters):
     cycle = 0.0
     for l in range(2, top + 1):
         v = mu ** (top - l)
-        step = 2 * level_iters * act[l] * BYTES_PER_CELL_GS + act[l] * B["restrict"] + nonleaf[l - 1] * B["fas"] + alll[l] * B["prolong"]
+        li = finest_iters if (l == top and finest_iters >= 0) else level_iters
+        # li sweeps before and li after the coarse correction, two colour passes each
+        step = 4 * li * act[l] * BYTES_PER_CELL_GS + act[l] * B["restrict"] + nonleaf[l - 1] * B["fas"] + alll[l] * B["prolong"]
         cycle += v * step * c
     cycle += (mu ** max(top - 1, 0)) * 9 * c * B["coarse"] + len(lv) * c * B["fill"]
     leaf_iter = nleaf * c * (B["apply"] + B["xr"] + B["dot"] + B["pupdate"])
@@ -853,7 +856,16 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roofline_entry(launch_ms, achieved, alg_bytes, L, active, cells, peak, peak_kind, tpc),
             "clocks": clocks,
         }
+        # the whole solve against the HBM roofline: algorithmic bytes of every cycle and PCG step
+        # (solve_algorithmic_bytes) over the solve's time, of the measured copy bandwidth
+        sb = solve_algorithmic_bytes(G, SOLVE["mu"], SOLVE["level_iters"], iters[-1])
+        result["config"]["whole_solve_hbm"] = {
+            "algorithmic_bytes": int(sb), "ms": round(per_solve, 4), "achieved_gbs": round(sb / per_solve / 1e6, 1),
+            "per_vcycle_hbm_frac": round(sb / per_solve / 1e6 / peak, 4), "peak_gbs": peak, "peak_kind": peak_kind}
         if tuned is not None:
+            tb = solve_algorithmic_bytes(G, tuned["mu"], tuned["level_iters"], tuned["pcg_iters"], tuned["finest_iters"])
+            tuned["whole_solve_hbm"] = {"algorithmic_bytes": int(tb), "achieved_gbs": round(tb / tuned["ms"] / 1e6, 1),
+                                        "per_vcycle_hbm_frac": round(tb / tuned["ms"] / 1e6 / peak, 4)}
             tuned["speedup_vs_plain"] = round(per_solve / tuned["ms"], 3)
             tuned["speedup_vs_plain_bf16_storage"] = round(per_solve / tuned["ms_bf16_storage"], 3)
             tuned["speedup_vs_plain_bf16_operator_x_rhs"] = round(per_solve / tuned["ms_bf16_operator_x_rhs"], 3)
