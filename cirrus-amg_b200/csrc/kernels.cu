@@ -286,29 +286,48 @@ __global__ void __launch_bounds__(128) k_true_residual(DevGrid g, const int* lea
     if (blockIdx.x == 0 && threadIdx.x == 0) ++s->replaced;
 }
 
-__global__ void __launch_bounds__(128) k_xr_update(DevGrid g, const int* leaf, float* X, float* R, const float* P, const float* AP,
-                                                   ReduceScratch rs, cudaGraphConditionalHandle loop_h,
+__global__ void __launch_bounds__(128) k_xr_update(DevGrid g, const int* leaf, int nleaf, float* X, float* R, const float* P,
+                                                   const float* AP, ReduceScratch rs, cudaGraphConditionalHandle loop_h,
                                                    cudaGraphConditionalHandle body_h, int use_handles) {
     __shared__ double red[4];
-    const int t = leaf[blockIdx.x];
-    const Quad Q(t, threadIdx.x);
     const float alpha = (float)rs.s->alpha;
-    float4 x = ld4(X + Q.base), r = ld4(R + Q.base);
-    const float4 p = ld4(P + Q.base), ap = ld4(AP + Q.base);
-    const uchar4 ty = ldt4(g.ctype + Q.base);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        if (t4get(ty, u) & dInterior) {
-            f4set(x, u, __fmaf_rn(alpha, f4get(p, u), f4get(x, u)));
-            f4set(r, u, __fmaf_rn(-alpha, f4get(ap, u), f4get(r, u)));
+    // the block walks the leaf list with stride gridDim.x, the next tile's planes in flight
+    // while it finishes the current one; tile i's partial is what one block per tile gives
+    int i = blockIdx.x;
+    Quad Q(leaf[i], threadIdx.x);
+    float4 x = ld4(X + Q.base), r = ld4(R + Q.base), p = ld4(P + Q.base), ap = ld4(AP + Q.base);
+    uchar4 ty = ldt4(g.ctype + Q.base);
+    for (;;) {
+        const int in = i + gridDim.x;
+        const bool more = in < nleaf;
+        const Quad Qn(more ? leaf[in] : 0, threadIdx.x);
+        float4 xn = x, rn = r, pn = p, apn = ap;
+        uchar4 tyn = ty;
+        if (more) {
+            xn = ld4(X + Qn.base);
+            rn = ld4(R + Qn.base);
+            pn = ld4(P + Qn.base);
+            apn = ld4(AP + Qn.base);
+            tyn = ldt4(g.ctype + Qn.base);
         }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (t4get(ty, u) & dInterior) {
+                f4set(x, u, __fmaf_rn(alpha, f4get(p, u), f4get(x, u)));
+                f4set(r, u, __fmaf_rn(-alpha, f4get(ap, u), f4get(r, u)));
+            }
+        }
+        st4(X + Q.base, x);
+        st4(R + Q.base, r);
+        const double bs = block_sum128(dot4(r, r), red);
+        if (threadIdx.x == 0) rs.partial[i] = bs;
+        if (!more) break;
+        i = in;
+        Q = Qn;
+        x = xn, r = rn, p = pn, ap = apn, ty = tyn;
     }
-    st4(X + Q.base, x);
-    st4(R + Q.base, r);
-    const double bs = block_sum128(dot4(r, r), red);
-    if (threadIdx.x == 0) rs.partial[blockIdx.x] = bs;
     if (last_block(&rs.s->counter[1])) {
-        const double rr = sum_partials(rs.partial, gridDim.x, red);
+        const double rr = sum_partials(rs.partial, nleaf, red);
         if (threadIdx.x == 0) {
             PcgScalars* s = rs.s;
             s->rr = rr;
@@ -328,14 +347,31 @@ __global__ void __launch_bounds__(128) k_xr_update(DevGrid g, const int* leaf, f
     }
 }
 
-__global__ void __launch_bounds__(128) k_dot(const int* leaf, const float* A, const float* B, int mode, double* out, ReduceScratch rs) {
+__global__ void __launch_bounds__(128) k_dot(const int* leaf, int nleaf, const float* A, const float* B, int mode, double* out,
+                                             ReduceScratch rs) {
     __shared__ double red[4];
-    const int t = leaf[blockIdx.x];
-    const size_t base = (size_t)t * kCells + 4 * threadIdx.x;
-    const double bs = block_sum128(dot4(ld4(A + base), ld4(B + base)), red);
-    if (threadIdx.x == 0) rs.partial[blockIdx.x] = bs;
+    // grid-stride over the leaf list, the next tile's loads in flight; per-tile partials as
+    // with one block per tile
+    int i = blockIdx.x;
+    size_t base = (size_t)leaf[i] * kCells + 4 * threadIdx.x;
+    float4 a = ld4(A + base), b = ld4(B + base);
+    for (;;) {
+        const int in = i + gridDim.x;
+        const bool more = in < nleaf;
+        float4 an = a, bn = b;
+        if (more) {
+            base = (size_t)leaf[in] * kCells + 4 * threadIdx.x;
+            an = ld4(A + base);
+            bn = ld4(B + base);
+        }
+        const double bs = block_sum128(dot4(a, b), red);
+        if (threadIdx.x == 0) rs.partial[i] = bs;
+        if (!more) break;
+        i = in;
+        a = an, b = bn;
+    }
     if (last_block(&rs.s->counter[2])) {
-        const double d = sum_partials(rs.partial, gridDim.x, red);
+        const double d = sum_partials(rs.partial, nleaf, red);
         if (threadIdx.x == 0) {
             PcgScalars* s = rs.s;
             if (mode == kDotStore) *out = d;
@@ -1011,15 +1047,27 @@ void launch_true_residual(const DevGrid& g, const int* leaf, int nleaf, const fl
                           PcgScalars* s, int every, cudaStream_t st) {
     if (nleaf > 0 && every > 0) count_launch(), k_true_residual<<<nleaf, 128, 0, st>>>(g, leaf, X, B, R, coeff_ch, s, every);
 }
+// blocks of the grid-stride PCG vector kernels: 8 per SM (a block keeps two tiles' loads in flight)
+static int vec_blocks(int nleaf) {
+    static int per = 0;
+    if (!per) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        per = 8 * (sms > 0 ? sms : 1);
+    }
+    return nleaf < per ? nleaf : per;
+}
 void launch_xr_update(const DevGrid& g, const int* leaf, int nleaf, float* X, float* R, const float* P, const float* AP,
                       ReduceScratch rs, cudaGraphConditionalHandle loop_h, cudaGraphConditionalHandle body_h, bool use_handles,
                       cudaStream_t st) {
-    if (nleaf > 0) count_launch(), k_xr_update<<<nleaf, 128, 0, st>>>(g, leaf, X, R, P, AP, rs, loop_h, body_h, use_handles ? 1 : 0);
+    if (nleaf > 0)
+        count_launch(), k_xr_update<<<vec_blocks(nleaf), 128, 0, st>>>(g, leaf, nleaf, X, R, P, AP, rs, loop_h, body_h, use_handles ? 1 : 0);
 }
 void launch_dot(const DevGrid& g, const int* leaf, int nleaf, const float* A, const float* B, int mode, double* out, ReduceScratch rs,
                 cudaStream_t st) {
     (void)g;
-    if (nleaf > 0) count_launch(), k_dot<<<nleaf, 128, 0, st>>>(leaf, A, B, mode, out, rs);
+    if (nleaf > 0) count_launch(), k_dot<<<vec_blocks(nleaf), 128, 0, st>>>(leaf, nleaf, A, B, mode, out, rs);
 }
 void launch_dot_flex(const DevGrid& g, const int* leaf, int nleaf, const float* R, const float* Z, const float* AP, ReduceScratch rs,
                      cudaStream_t st) {
