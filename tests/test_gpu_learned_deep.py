@@ -158,3 +158,33 @@ def test_deep_trained_net_against_plain(capsys):
     ip, tp, il, tl, tr, fb, dx = rows[-1]
     assert not fb and tr <= 4e-6 and dx <= 1e-4
     assert il <= ip, rows
+
+
+def test_deep_nonfinite_net_falls_back_to_plain():
+    """The residual net with overflowing parameters makes the learned solve non-finite; the
+    plain solve takes over and gives the plain result bit for bit."""
+    from workloads import setup_uniform
+
+    G, _, solver, b = setup_uniform(2, seed=3, with_oracle=False)
+    ip, _ = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    xp = G.download(0)
+    net = cmg.LearnedNet(32, seed=6)
+    net.set_params(np.full(net.num_params, 3e37, np.float32))
+    solver.set_learned(net)
+    G.upload(1, b)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    tr, fb, _ = solver.learned_status()
+    assert fb and it == ip and rel < 1e-6
+    assert np.array_equal(G.download(0), xp)
+
+
+def test_deep_untrained_net_in_the_solve_matches_plain():
+    """An untrained residual net inside flexible PCG: the solve reaches the tolerance under the
+    true-residual judge and x agrees with the plain solve."""
+    from workloads import setup_uniform
+
+    G, _, solver, b = setup_uniform(3, seed=0, with_oracle=False)
+    net = cmg.LearnedNet(32, seed=5)
+    rows = learned.compare(G, solver, net, [b])
+    ip, tp, il, tl, tr, fb, dx = rows[0]
+    assert tr <= 4e-6 and dx <= 1e-4, rows
