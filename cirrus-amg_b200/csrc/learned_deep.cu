@@ -10,7 +10,7 @@
 // operands (weights, x0, X_k, H_k and the back-propagated gradients that enter a
 // convolution) and FP32 accumulation in TMEM.
 //
-// One CTA of 128 threads per SM (191 KB of shared memory) loops over tiles.  Activations
+// One CTA of 128 threads per SM (194 KB of shared memory) loops over tiles.  Activations
 // are channel-group-major planes, element (voxel v, channel c) at ((c >> 3) * kTcVox + v)
 // * 8 + (c & 7): 16 bytes per voxel and 8-channel group, the padded 10^3 voxel grid.
 //   * A convolution is five M = 128 MMAs per 16-wide K step: K-major A operand straight from
