@@ -1030,6 +1030,8 @@ int Solver::solve_begin(Grid& G, int max_iters, double tol, int level_iters, int
     }
     std::memset(h_s, 0, sizeof(PcgScalars));
     h_s->max_iters = max_iters;
+    // the learned solve falls back to the plain one when its residual stalls
+    h_s->stall_window = learned_active() ? kLearnedStallWindow : 0;
     h_s->sync_stride = sync_stride;
     h_s->thr = -1.0;
     h_s->tol = tol;  // the gate kernel turns it into max(tol^2 rr0, DBL_MIN)

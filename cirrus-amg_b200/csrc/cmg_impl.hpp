@@ -189,6 +189,9 @@ struct Solver {
     int last_fallback = 0, last_learned_iters = 0;
     bool learned_active() const { return lnet.enabled && kind == kAMG && !learned_suspended; }
     int set_learned(const Net* net);
+    // a learned solve stops as stalled (and the plain solve takes over) when its residual norm
+    // has fallen by less than 2x over this many iterations
+    static constexpr int kLearnedStallWindow = 4;
     // a learned solve passes when its true relative residual is at most this many times tol:
     // the FP32 operator apply itself leaves the plain solve of the adaptive sphere octree at
     // 3.5 tol, so a tighter bound would reject sound solves

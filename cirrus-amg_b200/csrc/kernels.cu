@@ -334,7 +334,14 @@ __global__ void __launch_bounds__(128) k_xr_update(DevGrid g, const int* leaf, i
             const int it = ++s->iter;
             const bool bad = !isfinite(rr) || !isfinite(s->alpha);
             const bool conv = s->sync_stride > 0 && (it % s->sync_stride) == 0 && rr < s->thr;
-            const bool done = conv || bad || it >= s->max_iters;
+            bool stalled = false;
+            if (s->stall_window > 0 && s->sync_stride > 0) {
+                const int w = s->stall_window, h = it % w;
+                stalled = it > w && !conv && rr > 0.25 * s->rr_hist[h];
+                s->rr_hist[h] = rr;
+            }
+            s->stalled = stalled;
+            const bool done = conv || bad || stalled || it >= s->max_iters;
             s->converged = conv;
             s->nonfinite = bad;
             s->done = done;

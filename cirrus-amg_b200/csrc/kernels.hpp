@@ -16,6 +16,10 @@ struct PcgScalars {
     int replaced;  // true-residual replacements made by the solve
     int max_iters, sync_stride;
     unsigned int counter[8];
+    // stall test of the learned solve (window 0: off): the solve stops, not converged, when the
+    // residual norm has fallen by less than 2x over the last `stall_window` iterations
+    double rr_hist[4];
+    int stall_window, stalled;
 };
 
 struct ReduceScratch {

@@ -281,7 +281,8 @@ int cmg_amg_solver_set_storage(cmg_amg_solver* s, int storage);
  * each mu-cycle, rho = r - A z being the residual the cycle leaves (S: its RMS on the
  * tile, D: the tile's largest diagonal).  The solve then runs flexible CG (Polak-Ribiere
  * beta), judges the result by the true residual |b - A x| / |b| and falls back to the
- * plain solve when that exceeds 10 tol or the solve does not converge.
+ * plain solve when that exceeds 10 tol, the solve does not converge, or its residual stalls
+ * (its norm falls by less than 2x over 4 iterations).
  * Samples are tiles of 512 cells (cell i*64 + j*8 + k): rho, the diagonal of A (the
  * coefficient channel coeff+3), cell types and the target error d = A^-1 rho.
  * The net keeps its parameters, Adam state and samples on the device; training runs

@@ -257,6 +257,26 @@ def test_learned_solve_matches_plain():
     assert il <= 100
 
 
+def test_stalled_learned_solve_falls_back_to_plain():
+    """A net whose correction swamps the cycle's (output layer x 1000) leaves the residual where
+    it is: the solve stops as stalled after a few iterations (the residual norm fell by less
+    than 2x over 4 of them), and the plain solve takes over with the plain result."""
+    G, _, solver, b = setup_uniform(3, seed=0, with_oracle=False)
+    ip, _ = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    xp = G.download(0)
+    net = cmg.LearnedNet(8, seed=3)
+    p = net.params()
+    p[-27 * 8:] *= 1000.0
+    net.set_params(p)
+    solver.set_learned(net)
+    G.upload(1, b)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    tr, fb, lit = solver.learned_status()
+    solver.set_learned(None)
+    assert fb and lit <= 8, (fb, lit)
+    assert it == ip and rel < 1e-6 and np.array_equal(G.download(0), xp)
+
+
 def test_nonfinite_net_falls_back_to_plain():
     """A net whose output overflows makes the learned solve non-finite; the plain solve takes over."""
     G, _, solver, b = setup_uniform(2, seed=3, with_oracle=False)
