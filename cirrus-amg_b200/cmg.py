@@ -568,7 +568,8 @@ class AMGSolver:
     def autotune(self, grid, candidates=None, max_iters=100, relative_tolerance=1e-6, repeats=2):
         """Time solves of the grid's current rhs (channel 1) under each candidate
         (omega, mu, level_iters, coarsest_iters[, finest_iters]) and keep the fastest that
-        converges.  Sets omega, mu_cycle_repeat_times and finest_iters; returns (best candidate
+        converges (among those within 3 % of the fastest, the one with the fewest
+        iterations, then the smallest final residual).  Sets omega, mu_cycle_repeat_times and finest_iters; returns (best candidate
         as a 5-tuple or None, table of (candidate, ms or None, iters))."""
         if candidates is None:
             candidates = default_tune_candidates()

@@ -60,6 +60,17 @@ static cudaError_t plane_pool(int dev, cudaMemPool_t* out) {
     *out = pool;
     return cudaSuccess;
 }
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    cudaMemPool_t pool;
+    if (e == cudaSuccess) e = plane_pool(dev, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+void pool_release(void* p, cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st);
+}
 template <class T>
 static cudaError_t pool_alloc(T** p, size_t bytes, int dev, cudaStream_t st) {
     cudaMemPool_t pool;
@@ -69,22 +80,30 @@ static cudaError_t pool_alloc(T** p, size_t bytes, int dev, cudaStream_t st) {
 }
 template <class T>
 static void pool_free(T*& p, cudaStream_t st) {
-    if (p) cudaFreeAsync((void*)p, st);
+    pool_release((void*)p, st);
     p = nullptr;
+}
+
+static int plane_class_tiles(int n) {
+    if (n <= 64) return n;
+    int p = 64;
+    while (p * 2 <= n) p *= 2;
+    const int q = p / 16;
+    return (n + q - 1) / q * q;
 }
 
 Grid::~Grid() {
     // cudaFree synchronised the device here before the planes came from a pool; keep that,
     // so that no work of the grid's stream still reads them, then free on the legacy stream
     // (the caller's stream may be gone by now)
-    if (chan || ctype) cudaDeviceSynchronize();
+    if (chan || ctype || meta) cudaDeviceSynchronize();
     pool_free(chan, nullptr);
     pool_free(ctype, nullptr);
-    dfree(meta);
-    dfree(nb);
-    dfree(child);
-    dfree(nbx);
-    dfree(leaf);
+    pool_free(meta, nullptr);
+    pool_free(nb, nullptr);
+    pool_free(child, nullptr);
+    pool_free(nbx, nullptr);
+    pool_free(leaf, nullptr);
     dfree(spheres);
     dfree(modes);
     dfree(dot_out);
@@ -182,15 +201,21 @@ int Grid::ensure_device() {
     float* chan_new = nullptr;
     uint8_t* ct_new = nullptr;
     const size_t cells = (size_t)n_new * kCells;
+    // the allocations are rounded up to a size class (a sixteenth of the power of two at or
+    // below the tile count, at most 6 % more): octrees of nearly the same size, rebuilt one
+    // after another, then ask the pool for the same sizes and take back the same blocks
+    const size_t cap_cells = (size_t)plane_class_tiles(n_new) * kCells;
     if (device < 0) CK(cudaGetDevice(&device));
-    CK(pool_alloc(&chan_new, sizeof(float) * cells * nch + 16, device, stream));
-    CK(pool_alloc(&ct_new, cells + 16, device, stream));
+    CK(pool_alloc(&chan_new, sizeof(float) * cap_cells * nch + 16, device, stream));
+    CK(pool_alloc(&ct_new, cap_cells + 16, device, stream));
+    // the tables come from the pool too, and the copies are stream-ordered (a pageable
+    // source is staged before cudaMemcpyAsync returns)
     int2* d_map = nullptr;
     int4* d_meta = nullptr;
-    CK(cudaMalloc(&d_map, sizeof(int2) * (n_new + 1)));
-    CK(cudaMalloc(&d_meta, sizeof(int4) * (n_new + 1)));
-    CK(cudaMemcpy(d_map, src_of_new.data(), sizeof(int2) * n_new, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_meta, hm.data(), sizeof(int4) * n_new, cudaMemcpyHostToDevice));
+    CK(pool_alloc(&d_map, sizeof(int2) * (n_new + 1), device, stream));
+    CK(pool_alloc(&d_meta, sizeof(int4) * (n_new + 1), device, stream));
+    CK(cudaMemcpyAsync(d_map, src_of_new.data(), sizeof(int2) * n_new, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_meta, hm.data(), sizeof(int4) * n_new, cudaMemcpyHostToDevice, stream));
     if (n_old > 0) {
         launch_remap(chan, chan_new, d_map, d_meta, n_new, nch, n_old, stream);
         launch_remap_types(ctype, ct_new, d_map, d_meta, n_new, stream);
@@ -200,7 +225,10 @@ int Grid::ensure_device() {
     }
     CK(cudaStreamSynchronize(stream));
     CK(cudaGetLastError());
-    cudaFree(d_map);
+    pool_free(d_map, stream);
+    // the old planes and tables may still be read by work on other streams (a solver's, a
+    // net's): wait for the device, as cudaFree did, before they go back to the pool
+    if (chan || meta) CK(cudaDeviceSynchronize());
     pool_free(chan, stream);
     pool_free(ctype, stream);
     chan = chan_new;
@@ -212,20 +240,22 @@ int Grid::ensure_device() {
             const int q = topo.nb[8 * t + f];
             if (q >= 0) hx[8 * t + f] = ((q + 1) << 3) | topo.tiles()[q].type;
         }
-    dfree(meta);
+    pool_free(meta, stream);
     meta = d_meta;
-    dfree(nb);
-    dfree(child);
-    dfree(nbx);
-    dfree(leaf);
-    CK(cudaMalloc(&nbx, sizeof(int) * 8 * (n_new + 1)));
-    CK(cudaMemcpy(nbx, hx.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&nb, sizeof(int) * 8 * (n_new + 1)));
-    CK(cudaMalloc(&child, sizeof(int) * 8 * (n_new + 1)));
-    CK(cudaMalloc(&leaf, sizeof(int) * (topo.leaf_list.size() + 1)));
-    CK(cudaMemcpy(nb, topo.nb.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(child, topo.child.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(leaf, topo.leaf_list.data(), sizeof(int) * topo.leaf_list.size(), cudaMemcpyHostToDevice));
+    pool_free(nb, stream);
+    pool_free(child, stream);
+    pool_free(nbx, stream);
+    pool_free(leaf, stream);
+    CK(pool_alloc(&nbx, sizeof(int) * 8 * (n_new + 1), device, stream));
+    CK(cudaMemcpyAsync(nbx, hx.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice, stream));
+    CK(pool_alloc(&nb, sizeof(int) * 8 * (n_new + 1), device, stream));
+    CK(pool_alloc(&child, sizeof(int) * 8 * (n_new + 1), device, stream));
+    CK(pool_alloc(&leaf, sizeof(int) * (topo.leaf_list.size() + 1), device, stream));
+    CK(cudaMemcpyAsync(nb, topo.nb.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(child, topo.child.data(), sizeof(int) * 8 * n_new, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(leaf, topo.leaf_list.data(), sizeof(int) * topo.leaf_list.size(), cudaMemcpyHostToDevice, stream));
+    // callers read the tables on other streams or from the host right after this
+    CK(cudaStreamSynchronize(stream));
     n = n_new;
     nleaf = (int)topo.leaf_list.size();
     dev_keys.swap(keys);
@@ -1178,6 +1208,8 @@ int Solver::solve(Grid& G, bool verbose, int max_iters, double tol, int level_it
     return rc;
 }
 
+constexpr float kTuneTie = 0.03f;
+
 int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, double tol, int repeats, float* ms, int* iters, int* best) {
     *best = -1;
     if (int rc = ensure_aux(G)) return rc;  // bsave keeps the rhs between the timed solves
@@ -1187,6 +1219,7 @@ int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, doub
     const int mu0 = mu, fi0 = finest_iters;
     auto restore = [&]() { omega = omega0, mu = mu0, finest_iters = fi0; };
     float best_ms = 0.0f;
+    std::vector<double> rel_end(n, 0.0);
     for (int i = 0; i < n; ++i) {
         omega = c[i].omega;
         mu = c[i].mu;
@@ -1194,6 +1227,7 @@ int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, doub
         float tmin = -1.0f;
         bool ok = true;
         int it = 0;
+        double rel_last = 0.0;
         for (int r = 0; r <= repeats; ++r) {  // the first solve builds the graph and is not counted
             CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
             if (int rc = solve_begin(G, max_iters, tol, c[i].level_iters, c[i].coarsest_iters, 1, false)) {
@@ -1202,6 +1236,7 @@ int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, doub
             }
             double rel = 0.0;
             const int rc = solve_finish(false, &it, &rel);
+            rel_last = rel;
             if (rc == 5) ok = false;  // non-finite: this setting diverges
             else if (rc) {
                 restore();
@@ -1217,10 +1252,23 @@ int Solver::autotune(Grid& G, int n, const TuneCandidate* c, int max_iters, doub
         }
         ms[i] = ok ? tmin : -1.0f;
         iters[i] = it;
+        rel_end[i] = rel_last;
         if (ok && (*best < 0 || tmin < best_ms)) {
             *best = i;
             best_ms = tmin;
         }
+    }
+    // near-ties (within kTuneTie of the fastest) go to the candidate with the fewest
+    // iterations, then to the one whose last iteration reached the smallest residual:
+    // timing noise then does not decide between settings of nearly equal cost, and the
+    // cycle that converges fastest carries over best to other right-hand sides and octrees
+    if (*best >= 0) {
+        int pick = *best;
+        for (int i = 0; i < n; ++i) {
+            if (ms[i] < 0.0f || ms[i] > (1.0f + kTuneTie) * best_ms) continue;
+            if (iters[i] < iters[pick] || (iters[i] == iters[pick] && rel_end[i] < rel_end[pick])) pick = i;
+        }
+        *best = pick;
     }
     CK(cudaMemcpyAsync(G.plane(1), bsave, bytes, cudaMemcpyDeviceToDevice, G.stream));
     CK(cudaStreamSynchronize(G.stream));

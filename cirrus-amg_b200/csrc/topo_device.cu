@@ -342,23 +342,15 @@ cudaError_t device_leaf_cell_types(const int4* meta, uint8_t* ctype, const int* 
     return cudaGetLastError();
 }
 
-DeviceTopoBuilder::~DeviceTopoBuilder() { release(); }
+DeviceTopoBuilder::~DeviceTopoBuilder() {
+    st = nullptr;  // the owner's stream may be gone; its work has been waited for
+    release();
+}
 
 void DeviceTopoBuilder::release() {
-    cudaFree(hk);
-    cudaFree(hv);
-    cudaFree(rec);
-    cudaFree(rec2);
-    cudaFree(type0);
-    cudaFree(flag);
-    cudaFree(keys);
-    cudaFree(keys2);
-    cudaFree(idx);
-    cudaFree(idx2);
-    cudaFree(nb);
-    cudaFree(child);
-    cudaFree(scal);
-    cudaFree(sort_tmp);
+    for (void* p : {(void*)hk, (void*)hv, (void*)rec, (void*)rec2, (void*)type0, (void*)flag, (void*)keys, (void*)keys2, (void*)idx,
+                    (void*)idx2, (void*)nb, (void*)child, (void*)scal, sort_tmp})
+        pool_release(p, st);
     hk = nullptr;
     hv = nullptr;
     rec = rec2 = nullptr;
@@ -379,7 +371,7 @@ cudaError_t DeviceTopoBuilder::reserve(int need) {
     while (h < 2u * (unsigned)c) h <<= 1;
     cudaError_t e = cudaSuccess;
     auto A = [&](void** p, size_t bytes) {
-        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = pool_malloc(p, bytes, st);
     };
     A((void**)&hk, sizeof(unsigned long long) * h);
     A((void**)&hv, sizeof(int) * h);
@@ -418,6 +410,7 @@ int device_refine_case(DeviceTopoBuilder& B, Topology& topo, int case_id, const 
     if (n == 0) return 1;
     // scal: [0] count, [1] error, [2] refined in this step, [3] max level
     int need = n < 1024 ? 1024 : 2 * n;
+    B.st = st;
     for (;;) {
         if (B.reserve(need) != cudaSuccess) return 2;
         std::vector<int4> h(n);

@@ -212,7 +212,10 @@ typedef struct cmg_tune_candidate {
  * under each of n candidate settings to tol, `repeats` timed solves each after one untimed
  * solve (a candidate whose first solve is slower than 1.5x the best so far, or does not
  * converge, is not timed further; its ms[i] is that first solve's), and keeps the fastest
- * setting that converges: ms[i] (-1: did not converge), iters[i], *best (-1: none).  The
+ * setting that converges, except that among the settings within 3 % of the fastest time
+ * the one with the fewest iterations wins, and among those the one whose last iteration
+ * reached the smallest relative residual: ms[i] (-1: did not converge),
+ * iters[i], *best (-1: none).  The
  * solver takes the best candidate's omega, mu and finest_iters; pass its
  * level_iters and coarsest_iters to cmg_amg_solve.  Channel 1 is restored, channel 0 holds
  * the last solution.  Tune on a right-hand side other than the ones to be timed. */

@@ -1,5 +1,7 @@
 """The smoother-parameter autotuner (cmg_amg_solver_autotune): it keeps the fastest setting
-that converges, restores the right-hand side, and the tuned solve agrees with the plain one."""
+that converges (near-ties within 3 % going to the fewest iterations, then the smallest
+final residual), restores the right-hand side, and the tuned solve agrees with the plain
+one."""
 import numpy as np
 import pytest
 
@@ -18,7 +20,10 @@ def test_autotune_keeps_fastest_converging_setting():
     best, table = solver.autotune(G, cands, max_iters=7, relative_tolerance=1e-6, repeats=2)
     assert best is not None
     conv = [t for t in table if t[1] is not None]
-    assert best == min(conv, key=lambda t: t[1])[0]
+    fastest = min(t[1] for t in conv)
+    near = [t for t in conv if t[1] <= 1.03 * fastest]
+    # the final residuals that break ties at equal iterations are not reported
+    assert best in [t[0] for t in near if t[2] == min(u[2] for u in near)]
     for cand, ms, it in table:
         if ms is None:
             assert it == 7  # ran out of iterations
