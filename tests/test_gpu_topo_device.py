@@ -68,3 +68,29 @@ def test_device_built_octree_solves_identically():
         it, rel = S.solve(G, False, 100, 1e-6, 2, 10, 1, False)
         out.append((it, rel, G.download(0)))
     assert out[0][:2] == out[1][:2] and np.array_equal(out[0][2], out[1][2])
+
+
+def test_rebuilt_octrees_reuse_pool_memory():
+    """Octrees rebuilt one after another around a moving sphere (each one built while the
+    previous one still exists, then the previous one destroyed) take back the pool blocks
+    that earlier ones freed: the tile counts differ, but the planes are allocated in size
+    classes.  Device memory grows by less than one octree's planes after the first octrees,
+    and not at all when the sphere moves back over positions already seen."""
+    import torch
+
+    free, counts, G = [], [], None
+    ks = list(range(10)) + list(range(9, -1, -1))
+    for k in ks:
+        c = (0.42 + 0.02 * k, 0.5, 0.5)
+        Gn = _grid(cmg.CASE_SHELL, shell_params(3, 4, 5, center=c), True)
+        Gn.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
+        Gn.synchronize()
+        G = Gn
+        del Gn
+        counts.append(G.num_tiles)
+        free.append(torch.cuda.mem_get_info()[0])
+    assert len(set(counts)) > 1, counts
+    planes = 16 * 512 * 4 * min(counts)
+    grown = [free[3] - f for f in free]
+    assert max(grown[3:10]) < planes, (grown, planes)
+    assert free[-1] == free[9], grown
