@@ -60,11 +60,9 @@ static cudaError_t plane_pool(int dev, cudaMemPool_t* out) {
     *out = pool;
     return cudaSuccess;
 }
-cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t st) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+cudaError_t pool_malloc(void** p, size_t bytes, int dev, cudaStream_t st) {
     cudaMemPool_t pool;
-    if (e == cudaSuccess) e = plane_pool(dev, &pool);
+    cudaError_t e = plane_pool(dev, &pool);
     if (e != cudaSuccess) return e;
     return cudaMallocFromPoolAsync(p, bytes, pool, st);
 }
@@ -138,6 +136,11 @@ int Grid::refine_case_device(int case_id, const double* params, int nparams, int
         return rebuild();
     }
     if (!topo_builder) topo_builder = new DeviceTopoBuilder();
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) {
+        set_error("refine_case_device: no CUDA device");
+        return 2;
+    }
+    topo_builder->dev = device;
     const int rc = device_refine_case(*topo_builder, topo, case_id, params, nparams, stream, steps);
     if (rc == 1) {
         set_error("refine_case_device: bad parameters");

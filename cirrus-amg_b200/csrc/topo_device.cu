@@ -371,7 +371,7 @@ cudaError_t DeviceTopoBuilder::reserve(int need) {
     while (h < 2u * (unsigned)c) h <<= 1;
     cudaError_t e = cudaSuccess;
     auto A = [&](void** p, size_t bytes) {
-        if (e == cudaSuccess) e = pool_malloc(p, bytes, st);
+        if (e == cudaSuccess) e = pool_malloc(p, bytes, dev, st);
     };
     A((void**)&hk, sizeof(unsigned long long) * h);
     A((void**)&hv, sizeof(int) * h);

@@ -11,7 +11,7 @@ constexpr int kDevTopoMaxParams = 64;
 
 // Device memory from the per-device stream-ordered pool that also holds the grids' channel
 // planes and tables; freed memory stays in the pool for the next octree (cmg_impl.cu).
-cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t st);
+cudaError_t pool_malloc(void** p, size_t bytes, int dev, cudaStream_t st);
 void pool_release(void* p, cudaStream_t st);
 
 // Device work space of the builder: tile pool, hash table, sort buffers (grow-only).
@@ -25,6 +25,7 @@ struct DeviceTopoBuilder {
     void* sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
     cudaStream_t st = nullptr;  // the stream the builder's work and its allocations run on
+    int dev = 0;                // the device of the grid that owns the builder
     cudaError_t reserve(int tiles);
     void release();
     ~DeviceTopoBuilder();
