@@ -213,6 +213,46 @@ def test_shell_solve_matches_oracle_and_fp64():
     assert rel_l2(x[rt, rc], xs) <= 1e-5
 
 
+@pytest.mark.parametrize("seed", [3, 11])
+def test_random_multi_sphere_octree_solve_matches_oracle_and_fp64(seed):
+    """A random octree of the batched workload's kind: two or three spheres at random
+    centres and radii, refined around each to level 5 from level 3, cut-cell faces of every
+    sphere, rhs the divergence of Fourier modes; the same set-up on the GPU and in the
+    oracle (bitwise), then the solve against the oracle and the FP64 solution."""
+    from workloads import fourier_modes
+
+    rng = np.random.default_rng(seed)
+    ns = int(rng.integers(2, 4))
+    sph = [tuple(float(v) for v in rng.uniform(0.25, 0.75, 3)) + (float(rng.uniform(0.06, 0.14)),) for _ in range(ns)]
+    prm = [3, 5, 0.05, ns] + [v for s_ in sph for v in s_]
+    k, amp, ph = fourier_modes(100 + seed)
+    G = build_product(cmg.CASE_MULTI_SPHERE, prm)
+    G.set_leaf_cell_types_case(cmg.CASE_UNIFORM)
+    G.cutcell_sphere_coeffs(COEFF, sph, 0.5)
+    G.face_velocity_fourier(U, k, amp, ph)
+    G.divergence(U, COEFF, 1)
+    g = build_oracle(cmg.CASE_MULTI_SPHERE, prm)
+    g.set_leaf_cell_types_case(O.CASE_UNIFORM)
+    g.cutcell_sphere_coeffs(COEFF, sph, 0.5)
+    g.face_velocity_fourier(U, k, amp, ph)
+    g.divergence(U, COEFF, 1)
+    assert np.array_equal(G.download_cell_types(), g.cell_types())
+    for a in range(4):
+        assert same_bits(G.download(COEFF + a), g.channel(COEFF + a)), f"coefficient channel {a}"
+    b = G.download(1)
+    assert np.abs(b).max() > 0
+    g.channel(1)[:] = b
+    solver = cmg.AMGSolver(COEFF, 0.5, 1.0, 1.0)
+    it, rel = solver.solve(G, False, 100, 1e-6, 2, 10, 1, False)
+    ito, relo = g.amg_solve(COEFF, max_iters=100, tol=1e-6)
+    assert rel <= 1e-6 and relo <= 1e-6 and abs(it - ito) <= 1, (it, ito, rel, relo)
+    m = leaf_mask(G)
+    x = G.download(0)
+    assert rel_l2(x[m], g.channel(0)[m]) <= 1e-5
+    xs, rt, rc = fp64_solution(g, b, 1)
+    assert rel_l2(x[rt, rc], xs) <= 1e-5
+
+
 @pytest.mark.parametrize("case_id,prm", [(cmg.CASE_SPHERE_SOLID, [2, 4]), (cmg.CASE_STAR_EMPTY, [2, 4]), (cmg.CASE_CENTER_POINT, [2, 5])])
 def test_reference_test_grids_solve(case_id, prm):
     """Octrees of tests/TestGrids.cuh solved by both sides (Dirichlet walls, random rhs on INTERIOR cells)."""
